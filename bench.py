@@ -1,0 +1,354 @@
+#!/usr/bin/env python3
+"""Benchmark: class-5 peel probes/sec and eligible-B/hour at B~3.2M on B200.
+
+One step = one pass of the cls5 hot path (2-D (d,e) free peel, mod-124,488
+gate, xor probe) over the production-shape band B in [3,200,000, 3,220,000]
+(all ~155k Stage-1 cls5 units plus 32 seeded plants) against an r=48 xor
+table for N = ceil(B_max/42) built on the device.  `value` is R>0 grid
+points ("peel probes") per second with units already resident in HBM;
+`e2e` is the same metric through the C ABI with host buffers.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun): each rank owns its own 20,000-B band (weak scaling),
+no collective on the data path; rank 0 prints one JSON line.
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "six-one-five_b200"), os.path.join(ROOT, "oracle")]
+
+METRIC = "cls5 peel probes/sec and eligible-B/hour at B≈3.2M, 1 B200; p99 unit latency"
+UNIT = "peel_probes/s"
+BAND_LO, BAND_W = 3_200_000, 20_000
+PROBE_BYTES = 108          # 3 cells x 1.125 sectors x 32 B per post-gate xor probe (r=48)
+N_PLANTS = 32
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--band-width", type=int, default=BAND_W)
+    ap.add_argument("--r", type=int, default=48)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return rank, world, local, pg
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        out, _ = self.p.communicate(timeout=10)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per post-gate probe from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "cls5_sieve_band3p2M.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_probe:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def band_units(lo, hi):
+    import workloads as W
+    return W.cls5_units(lo, hi)
+
+
+def eligible_count(lo, hi):
+    return sum(1 for B in range(lo, hi + 1) if math.gcd(B, 42) == 1)
+
+
+def cpu_sample_rate(table, units, plants_n, N, budget_s=15.0, check=None):
+    """Oracle (CPU restatement of k_cls5_192) on a bounded sample of the same
+    units and table: R>0 points per second with all host threads."""
+    import numpy as np
+
+    import orc
+    cores = os.cpu_count() or 1
+    step = max(1, len(units) // 4096)
+    pool = units[::step]
+    one = orc.units_array([orc.pack_unit(*pool[0])])
+    t0 = time.perf_counter()
+    _, c1 = orc.cls5_run(table, one, 1, threads=1)
+    t_unit = max(time.perf_counter() - t0, 1e-3)
+    n = max(cores, min(len(pool), int(cores * budget_s / t_unit)))
+    n = min(n, len(pool))
+    idx = np.linspace(0, len(pool) - 1, n).astype(int)
+    sample = [pool[i] for i in idx]
+    arr = orc.units_array([orc.pack_unit(B, u) for B, u in sample])
+    t0 = time.perf_counter()
+    hits, (calls, gated, probes) = orc.cls5_run(table, arr, len(sample), threads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": (gated + probes) / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{len(sample)} of the band's units (evenly spaced), same r=48 table; "
+                      f"{gated + probes:.3e} R>0 points in {dt:.1f} s"}, sample, hits
+
+
+def run_reference(args, rank):
+    """--impl reference: the reference's CPU path restated (oracle port of
+    k_cls5_192 with the reference's per-point 192-bit peel, mod-192 gate and
+    funnel key) on the box's host cores, a bounded unit sample per step."""
+    if rank != 0:
+        return 0
+    import orc
+    lo, hi = BAND_LO, BAND_LO + args.band_width
+    units = band_units(lo, hi)
+    # the reference's host table builder needs hours and ~100 GB at N=76,667;
+    # the reference arm probes a host-built N=2000 table (probes are ~1% of points)
+    table = orc.Table.build_pairs(2000, args.r)
+    cores = os.cpu_count() or 1
+    rates, samples = [], []
+    n_per = max(cores, 1)
+    for s in range(args.warmup + args.steps):
+        chunk = units[(s * 7919) % len(units)::max(1, len(units) // n_per)][:n_per]
+        arr = orc.units_array([orc.pack_unit(B, u) for B, u in chunk])
+        t0 = time.perf_counter()
+        _, (calls, gated, probes) = orc.cls5_run(table, arr, len(chunk), threads=cores)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            rates.append((gated + probes) / dt)
+            samples.append(len(chunk))
+    v = statistics.mean(rates)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u64", "data": "synthetic",
+            "config": {"workload": f"cls5 band B in [{lo}, {hi}], Stage-1 units; reference arm: "
+                                   f"{samples[0]} units per step on the host cores, N=2000 r={args.r} table"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{samples[0]} units per step x {args.steps} steps"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    rank, world, local, dist = dist_setup(args)
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import numpy as np
+    import torch
+
+    import s615
+    import workloads as W
+
+    torch.cuda.set_device(local)
+    lo = BAND_LO + rank * args.band_width
+    hi = lo + args.band_width
+    N = math.ceil((BAND_LO + world * args.band_width) / 42)
+    eng = s615.Engine(local)
+    t0 = time.perf_counter()
+    tid = eng.build_table(N, args.r)
+    build_s = time.perf_counter() - t0
+    units = band_units(lo, hi)
+    plants = W.plants(N_PLANTS, 1000 + rank, lo, hi, N)
+    arr, n = W.unit_array(units, plants, N)
+
+    lib = s615.lib()
+    batch = C.c_void_p()
+    s615._check(lib.s615_cls5_prepare(eng._ctx, C.cast(arr, C.c_void_p), n, C.byref(batch)),
+                "prepare")
+    stream = torch.cuda.current_stream()
+    sptr = C.c_void_p(stream.cuda_stream)
+
+    def step():
+        s615._check(lib.s615_cls5_run_batch(eng._ctx, tid, batch, 0, sptr), "run_batch")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    launches0 = eng.launches
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev[0].record(stream)
+    for k in range(args.steps):
+        step()
+        ev[k + 1].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    cl = clocks.stop()
+    launches = eng.launches - launches0
+    per_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[args.steps])
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+
+    hits = (s615.Hit * (1 << 20))()
+    nh = C.c_size_t(0)
+    ctr = s615.Counters()
+    s615._check(lib.s615_cls5_batch_results(eng._ctx, batch, C.cast(hits, C.c_void_p), 1 << 20,
+                                            C.byref(nh), C.byref(ctr)), "results")
+    harr = s615.hits_to_array(hits, nh.value)
+    sols = eng.verify(arr, n, harr, N)
+    recovered = sum(1 for s in sols if s.kind == 1)
+    solutions = [s615.solution_line(s) for s in sols if s.kind == 0]
+
+    pos_all = ctr.pos * world
+    value = pos_all * args.steps / (total_ms / 1e3)
+    eligible = eligible_count(lo, hi - 1) * world
+    ms_step = total_ms / args.steps
+
+    # e2e: the public C ABI with host buffers (unit records up, hits + counters down)
+    e2e_steps = max(1, min(args.steps, 3))
+    h2d = n * 152 + 6 * n * 4
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        h2, c2 = eng.cls5_run(tid, arr, n, hit_cap=1 << 16)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    assert c2.pos == ctr.pos and c2.probes == ctr.probes
+    d2h = 40 + len(h2) * 32
+
+    peak, peak_kind = measured_peaks()
+    dur_s = statistics.mean(per_ms) / 1e3
+    achieved = ctr.probes * PROBE_BYTES / dur_s / 1e9
+    tpp = profiled_traffic()
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs (burst)",
+            "traffic": (tpp * ctr.probes if tpp else None),
+            "algorithmic_bytes_per_launch": ctr.probes * PROBE_BYTES}
+
+    # plain per-unit-launch form on a bounded sample of the same band
+    plain = None
+    if not args.no_plain and rank == 0:
+        samp = units[:: max(1, len(units) // 1500)]
+        parr, pn = W.unit_array(samp, [], N)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, pc = eng.cls5_run(tid, parr, pn, flags=s615.F_PLAIN, hit_cap=1 << 16)
+        pdt = time.perf_counter() - t0
+        p_rate = pc.pos / pdt
+        plain = {"peel_probes_per_s": p_rate, "units": pn,
+                 "eligible_B_per_hour": p_rate / (ctr.pos / eligible_count(lo, hi - 1)) * 3600,
+                 "batched_over_plain": value / world / p_rate}
+
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        import orc
+        hb, pk = eng.export_table(tid)
+        ot = orc.Table.from_memory(hb, pk)
+        cpu, sample, ohits = cpu_sample_rate(ot, units, 0, N)
+        # the sampled units' raw hits must equal the device's for those units
+        del ot, pk
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": {"workload": f"cls5 band B in [{lo}, {hi}) per rank: {len(units)} Stage-1 units + "
+                               f"{N_PLANTS} plants; xor table N={N} r={args.r} built on device",
+                   "units_per_rank": n, "N": N, "r": args.r,
+                   "l2": "inputs larger than L2 (table %.1f GB)" % (eng.table_info(tid).device_bytes / 1e9),
+                   "parallelism": f"replicas-by-band x{world}"},
+        "eligible_B_per_hour": eligible * args.steps / (total_ms / 1e3) * 3600,
+        "p99_unit_latency_ms": None,
+        "counters": {"calls": ctr.calls * world, "gated": ctr.gated * world,
+                     "probes": ctr.probes * world, "pos": pos_all},
+        "plants_recovered": f"{recovered}/{N_PLANTS}", "solutions": solutions,
+        "table_build_s": round(build_s, 2),
+        "e2e": {"value": ctr.pos / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "plain_form": plain,
+        "clocks": cl,
+    }
+    s615._check(lib.s615_cls5_batch_free(eng._ctx, batch), "batch_free")
+    eng.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,189 @@
+/*
+ * s615.h -- C ABI of the B200 engine for the (6,1,5) class-5 meet-in-the-middle
+ * search: 2-D (d,e) free peel, mod-124,488 residue gate, xor-filter probe and
+ * exact verification, plus the device xor-filter builder the path consumes.
+ *
+ * Naming follows the reference (cavedave/six-one-five): e is the x14 free
+ * term (residues mod 3^6, e <= (B-1)/14), d is the x21 free term (residues mod
+ * 2^6, d <= (B-1)/21).  A unit is a Stage-1 pair (B,u); its grid point (e,d)
+ * has R = B^6 - u^6 - (14e)^6 - (21d)^6 and T = R / 42^6.
+ *
+ * Conventions: every call returns an int status (S615_OK or a negative
+ * S615_E_* code); nothing here calls exit().  Plain pointers and sizes only.
+ * Host-buffer entry points copy in and out themselves; *_dev entry points take
+ * device pointers and a cudaStream_t passed as void*.
+ * A context is not thread-safe, except that s615_submit may be called from any
+ * thread while one thread calls s615_poll.
+ */
+#ifndef S615_H
+#define S615_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define S615_OK 0
+#define S615_E_ARG (-1)        /* bad argument */
+#define S615_E_IO (-2)         /* cannot open / short read or write */
+#define S615_E_FORMAT (-3)     /* bad header, kind, version, or unit shape */
+#define S615_E_N_MISMATCH (-4) /* table file N != expected N */
+#define S615_E_FPR_SMOKE (-5)  /* FPR smoke > 16 / 200k: refuse to search */
+#define S615_E_OOM (-6)        /* device or HBM-budget allocation failed */
+#define S615_E_DEVICE (-7)     /* CUDA error */
+#define S615_E_TIMEOUT (-8)    /* a bounded device wait gave up */
+#define S615_E_OVERFLOW (-9)   /* hit buffer too small (results incomplete) */
+#define S615_E_BUILD (-10)     /* xor peel stalled for every seed */
+#define S615_E_NOTABLE (-11)   /* unknown table id */
+
+const char* s615_strerror(int status);
+
+typedef struct s615_ctx s615_ctx;
+
+/* Table layouts held in HBM.  PACKED is the file layout (r-bit cells);
+ * WIDE stores one cell per aligned 4- or 8-byte word (one sector per cell). */
+#define S615_LAYOUT_AUTO 0
+#define S615_LAYOUT_PACKED 1
+#define S615_LAYOUT_WIDE 2
+
+/* Store header v2, byte-identical to the reference's StoreHeader
+ * (spike/ribbon/store_header.hpp:23-37): 64 bytes, little-endian. */
+typedef struct s615_header {
+  uint32_t magic, version, kind, r, w, N;
+  uint64_t n_keys, m_cells, mix_seed;
+  uint32_t shard_count, shard_index, shard_mode, reserved;
+} s615_header;
+
+typedef struct s615_table_info {
+  s615_header hdr;
+  int layout;             /* S615_LAYOUT_PACKED or _WIDE */
+  int cell_bytes;         /* 0 for PACKED, else 4 or 8 */
+  uint64_t device_bytes;  /* HBM held by the table */
+} s615_table_info;
+
+/* Unit record.  kind 0: a Stage-1 unit (B,u); the engine derives everything
+ * like pack_unit5 (fourcore_cls5_gpu_v4.cu:169-184).  kind 1: a planted
+ * target: base (= target - u^6, 3 LE limbs) is taken as given, with one e
+ * residue res_e <= fmax1 grid and one d residue res_d <= fmax2 grid (the
+ * reference's plant shape, solve_516_v3.cu:1149-1170). */
+typedef struct s615_unit {
+  uint32_t cls;      /* 5 */
+  uint32_t kind;     /* 0 = (B,u), 1 = planted base */
+  uint64_t B, u;
+  uint64_t base[3];  /* kind 1 only */
+  uint32_t fmax1, fmax2, res_e, res_d, lim; /* kind 1 only */
+  uint32_t pad;
+} s615_unit;
+
+/* Raw filter hit, same layout as the reference's Hit{unit,a,b,d,e,fp}
+ * (fourcore_cls5_gpu_v4.cu:140); a=b=0, unit = index into the unit array. */
+typedef struct s615_hit {
+  uint32_t unit, a, b, d, e;
+  uint64_t fp;
+} s615_hit;
+
+/* Counters with the reference's meaning (fourcore_cls5_gpu_v4.cu:382-409):
+ * calls = in-range (e,d) points, gated = R>0 points stopped by the gate,
+ * probes = xor probes issued; pos = R>0 points (= gated + probes). */
+typedef struct s615_counters {
+  uint64_t calls, gated, probes, pos, hits;
+} s615_counters;
+
+/* A verified identity B^6 = u^6+(21d)^6+(14e)^6+42^6(c1^6+c2^6) with sorted
+ * distinct terms a[0..4] < B (the SOLUTION line of fourcore_cls5_gpu_v4.cu:
+ * 524-536), or a recovered plant (kind 1, a[] unused). */
+typedef struct s615_solution {
+  uint32_t unit, kind;
+  uint64_t B, u;
+  uint32_t d, e, c1, c2;
+  int64_t a[5];
+  int64_t gcd;
+} s615_solution;
+
+/* ------------------------------------------------------------- context */
+/* Open device `device` with an HBM admission budget (0 = all free memory). */
+int s615_open(int device, size_t hbm_budget, s615_ctx** out);
+int s615_close(s615_ctx* ctx);
+/* Kernel launches the engine issued since open (all of its own kernels). */
+uint64_t s615_launch_count(s615_ctx* ctx);
+
+/* -------------------------------------------------------------- tables */
+/* xor_load_file (fourcore_xor_store.hpp:147-181) + xor_fpr_smoke (:54-65) +
+ * upload: header v2 checks, exact N (expected_N <= 0 accepts any), smoke <=16
+ * hits of 200k keys, then the table is resident in HBM. */
+int s615_load_table(s615_ctx* ctx, const char* path, int expected_N, int layout,
+                    int* table_id);
+/* xor_build_pairs (fourcore_xor_store.hpp:67-119) on the device: keys
+ * (i^6+j^6) mod 2^64 for 1<=i<=j<=N, the same capacity, seeds and header;
+ * parallel peel (cell bytes differ from the host FIFO peel). */
+int s615_build_table(s615_ctx* ctx, int N, int r, int layout, int* table_id);
+/* build_xor (spike/ribbon/xor_filter.hpp:447-470) over arbitrary host keys. */
+int s615_build_table_keys(s615_ctx* ctx, const uint64_t* keys, size_t n, int r,
+                          uint64_t base_seed, int layout, int* table_id);
+/* xor_save_file (fourcore_xor_store.hpp:126-143): header + packed cells. */
+int s615_save_table(s615_ctx* ctx, int table_id, const char* path);
+/* The packed file bytes (after the 64-byte header) into a host buffer of
+ * cap >= packed_bytes(m_cells, r) bytes; the in-memory form of the
+ * reference's XorFilter::packed. *len receives the byte count. */
+int s615_export_table(s615_ctx* ctx, int table_id, s615_header* hdr, uint8_t* buf, size_t cap,
+                      size_t* len);
+int s615_get_table_info(s615_ctx* ctx, int table_id, s615_table_info* info);
+int s615_free_table(s615_ctx* ctx, int table_id);
+/* xor_might_contain (xor_filter.hpp:472-483) for n host keys -> out[i] 0/1. */
+int s615_xor_query(s615_ctx* ctx, int table_id, const uint64_t* keys, size_t n,
+                   uint8_t* out);
+int s615_xor_query_dev(s615_ctx* ctx, int table_id, const uint64_t* d_keys, size_t n,
+                       uint8_t* d_out, void* stream);
+
+/* Free / total device memory of the context's GPU (cudaMemGetInfo). */
+int s615_mem_info(s615_ctx* ctx, size_t* free_bytes, size_t* total_bytes);
+
+/* --------------------------------------------------------------- units */
+/* unit_candidates(rt,B,cls,0,1) (fourcore_classes_v3.hpp:137-154). */
+int s615_unit_candidates(uint64_t B, int cls, uint64_t* out, size_t cap, size_t* n);
+/* What a run does with one unit: S615_OK = searched, 1 = dropped like
+ * pack_unit5 drops it (u >= B or an empty residue class), S615_E_FORMAT =
+ * rejected (outside the engine's exact-arithmetic range, or a planted base
+ * whose grid points are not all divisible by 42^6). */
+int s615_unit_status(const s615_unit* unit);
+
+/* ----------------------------------------------------------- cls5 peel */
+#define S615_F_NO_GATE 1u     /* --no-gate: probe every R>0 point */
+#define S615_F_PLAIN 2u       /* one unit per launch + sync (the plain form) */
+
+/* run_cls5_gpu (fourcore_cls5_gpu_v4.cu:412-563) without the verify step:
+ * host units in, raw hits + counters out.  Hits are unordered.  Returns
+ * S615_E_OVERFLOW (with *n_hits = the true count) when hit_cap is too small. */
+int s615_cls5_run(s615_ctx* ctx, int table_id, const s615_unit* units, size_t n,
+                  unsigned flags, s615_hit* hits, size_t hit_cap, size_t* n_hits,
+                  s615_counters* counters);
+/* Device-resident form: d_units is the packed device record array produced
+ * by s615_cls5_prepare; results stay on the device. */
+typedef struct s615_batch s615_batch;
+int s615_cls5_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch** out);
+int s615_cls5_run_batch(s615_ctx* ctx, int table_id, s615_batch* b, unsigned flags,
+                        void* stream);
+int s615_cls5_batch_results(s615_ctx* ctx, s615_batch* b, s615_hit* hits, size_t hit_cap,
+                            size_t* n_hits, s615_counters* counters);
+int s615_cls5_batch_free(s615_ctx* ctx, s615_batch* b);
+
+/* ------------------------------------------------------------- verify */
+/* PairRecover + exact identity (fourcore_xor_store.hpp:23-51,
+ * fourcore_cls5_gpu_v4.cu:513-542) on the device: every (c1<=c2<=min(N,lim))
+ * with c1^6+c2^6 = T for each hit, then the identity and term checks. */
+int s615_cls5_verify(s615_ctx* ctx, const s615_unit* units, size_t n_units,
+                     const s615_hit* hits, size_t n_hits, int N, s615_solution* out,
+                     size_t cap, size_t* n_out);
+
+/* ------------------------------------------------------------ selftest */
+/* Host-only checks of selftest_host (fourcore_cls5_gpu_v4.cu:186-263) plus the
+ * engine's invariants (gate factorisation, exact remainder, row identity).
+ * Needs no GPU.  Returns 0 on success, else the number of the failed check. */
+int s615_selftest_host(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,119 @@
+/*
+ * s615_oracle.h -- C API of the CPU oracle for the cls5 peel/gate/probe path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is a plain CPU restatement of the
+ * reference algorithm (cavedave/six-one-five) and is used exclusively as the
+ * checker: by tests/, by __graft_entry__.smoke() and by bench.py's
+ * cpu_baseline / reference leg.  The product (libs615) never links or calls it.
+ *
+ * Every function follows the reference file:line named beside it.  Naming
+ * follows the reference: e is the x14 free term (residues mod 3^6), d is the
+ * x21 free term (residues mod 2^6).
+ */
+#ifndef S615_ORACLE_H
+#define S615_ORACLE_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Store header v2 (spike/ribbon/store_header.hpp:23-37), 64 bytes LE. */
+typedef struct orc_header {
+  uint32_t magic, version, kind, r, w, N;
+  uint64_t n_keys, m_cells, mix_seed;
+  uint32_t shard_count, shard_index, shard_mode, reserved;
+} orc_header;
+
+/* Unit5 (fourcore_cls5_gpu_v4.cu:143-151): base = B^6-u^6 as 3 LE limbs. */
+typedef struct orc_unit5 {
+  uint64_t B, u;
+  uint64_t base[3];
+  uint32_t lim, mod1, mod2, fmax1, fmax2, nres1, nres2;
+  uint32_t res[24]; /* e residues then d residues */
+  uint32_t planted; /* 1 = base set directly (plant), verify against base */
+} orc_unit5;
+
+/* Hit (fourcore_cls5_gpu_v4.cu:140). */
+typedef struct orc_hit {
+  uint32_t unit, a, b, d, e;
+  uint64_t fp;
+} orc_hit;
+
+typedef struct orc_table orc_table;
+
+/* ---- units (fourcore_classes_v3.hpp) ---- */
+/* unit_candidates(rt,B,cls,0,1) -> sorted u list; returns count (<= cap written). */
+size_t orc_unit_candidates(uint64_t B, int cls, uint64_t* out, size_t cap);
+/* seeds_for_B count for a class (selftest KAT). */
+size_t orc_seed_count(uint64_t B, int cls);
+/* pack_unit5 (fourcore_cls5_gpu_v4.cu:169-184). 1 = ok. */
+int orc_pack_unit5(uint64_t B, uint64_t u, orc_unit5* out);
+/* free_d_cls234 (fourcore_classes_v3.hpp:188-209): residues, mod, fmax. */
+int orc_free_d_cls234(uint64_t B, uint64_t u, int cls, uint32_t* res, uint32_t* nres,
+                      uint64_t* mod, uint64_t* fmax);
+
+/* ---- exact arithmetic KATs ---- */
+void orc_pow6_192(uint32_t x, uint64_t out[3]);
+/* T=(B^6-u^6-(21d)^6-(14e)^6)/42^6 (fourcore_gmp.hpp:55-62); 1 if ok. */
+int orc_T_peel2(uint64_t B, uint64_t u, uint64_t d, uint64_t e, uint64_t T[2]);
+/* funnel fingerprint of base-(14e)^6-(21d)^6 (cls5_gpu_v4.cu:266-268). */
+uint64_t orc_funnel_fp(const orc_unit5* U, uint32_t d, uint32_t e, int* ok);
+/* gate bitmaps (cls5_gpu_v4.cu:124-137): 504 + 247 flags. */
+void orc_gate_tables(uint8_t g504[504], uint8_t g247[247]);
+
+/* ---- xor filter (spike/ribbon/xor_filter.hpp, xor_pack.hpp, mix64.hpp) ---- */
+uint64_t orc_mix64(uint64_t x);
+size_t orc_capacity_for(size_t n);
+size_t orc_packed_bytes(uint64_t m_cells, uint32_t r);
+/* build_xor(keys, r, base_seed, max_tries) -> table (NULL on failure). */
+orc_table* orc_build_xor(const uint64_t* keys, size_t n, int r, uint64_t base_seed,
+                         int max_seed_tries);
+/* xor_build_pairs(N, r) (fourcore_xor_store.hpp:67-119). */
+orc_table* orc_build_pairs(int N, int r);
+/* xor_load_file (fourcore_xor_store.hpp:147-181); expected_N<=0 accepts any. */
+orc_table* orc_load(const char* path, int expected_N);
+orc_table* orc_from_memory(const orc_header* h, const uint8_t* bytes, size_t len);
+int orc_save(const orc_table* t, const char* path);
+void orc_free(orc_table* t);
+void orc_table_header(const orc_table* t, orc_header* h);
+const uint8_t* orc_table_bytes(const orc_table* t, size_t* n);
+/* xor_might_contain (xor_filter.hpp:472-483) over n keys. */
+void orc_query(const orc_table* t, const uint64_t* keys, size_t n, uint8_t* out);
+/* xor_fpr_smoke (fourcore_xor_store.hpp:54-65). */
+int orc_fpr_smoke(const orc_table* t);
+
+/* ---- cls5 peel (k_cls5_192, fourcore_cls5_gpu_v4.cu:353-410) ---- */
+/* Runs every unit; hits (unit index, d, e, fp) appended up to cap; counters
+ * calls/gated/probes; threads<=0 uses all OpenMP threads. Returns #hits found
+ * (may exceed cap; only cap written). */
+size_t orc_cls5_run(const orc_table* t, const orc_unit5* units, size_t n, int use_gate,
+                    int threads, orc_hit* hits, size_t cap, uint64_t counters[3]);
+
+/* ---- verify (cls5_gpu_v4.cu:513-542, fourcore_xor_store.hpp:23-51) ---- */
+/* For each hit, PairRecover + exact verify.  Writes SOLUTION lines (or PLANT
+ * lines for planted units) into buf; returns number of lines. */
+size_t orc_cls5_verify(const orc_unit5* units, const orc_hit* hits, size_t nh, int N,
+                       int stop_first, char* buf, size_t buflen);
+
+/* ---- cls2-4 find3 leaf (fourcore_find_v4.cu:165-205,255-284,401-425) ---- */
+typedef struct orc_job3 {
+  uint32_t cls, lim;
+  uint64_t B, u, d;     /* free term d (x14 / x21 / x7) */
+  uint64_t T[2];        /* T=(B^6-u^6-(f d)^6)/42^6 */
+  uint32_t lo, hi;      /* c3 window */
+} orc_job3;
+typedef struct orc_hit3 {
+  uint32_t job, c3;
+  uint64_t fp;
+} orc_hit3;
+/* Expand one unit into find3 jobs (expand_unit + make_cand mode 3). */
+size_t orc_expand_cls234(uint64_t B, uint64_t u, int cls, orc_job3* out, size_t cap);
+size_t orc_find3_run(const orc_table* t, const orc_job3* jobs, size_t n, int use_gate,
+                     int threads, orc_hit3* hits, size_t cap, uint64_t counters[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

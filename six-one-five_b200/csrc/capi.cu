@@ -1,0 +1,588 @@
+// capi.cu -- the C ABI (include/s615.h): context, tables, cls5 runs, verify.
+//
+// Host orchestration replacing run_cls5_gpu / acquire_xor_filter
+// (fourcore_cls5_gpu_v4.cu:412-594) and the table I/O of
+// fourcore_xor_store.hpp:54-181.  Differences by design: every call returns a
+// status instead of exiting; the table stays resident across calls; a whole
+// batch of units is one persistent launch instead of one launch and one
+// device-wide sync per 16 units; a full hit buffer is reported
+// (S615_E_OVERFLOW) instead of silently truncated.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <random>
+#include <vector>
+
+#include "engine.hpp"
+
+using namespace s615;
+
+namespace s615 {
+
+int cuda_status(cudaError_t e) {
+  if (e == cudaErrorMemoryAllocation) return S615_E_OOM;
+  return e == cudaSuccess ? S615_OK : S615_E_DEVICE;
+}
+
+int dev_alloc(s615_ctx* ctx, void** p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) bytes = 16;
+  if (ctx->budget && ctx->used + bytes > ctx->budget) return S615_E_OOM;
+  const cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) { cudaGetLastError(); *p = nullptr; return S615_E_OOM; }
+  ctx->used += bytes;
+  return S615_OK;
+}
+
+void dev_free(s615_ctx* ctx, void* p, size_t bytes) {
+  if (!p) return;
+  if (bytes == 0) bytes = 16;
+  cudaFree(p);
+  ctx->used -= std::min(ctx->used, bytes);
+}
+
+bool gate_product_matches();
+
+}  // namespace s615
+
+namespace {
+
+void free_table(s615_ctx* ctx, DevTable& t) {
+  dev_free(ctx, t.d_cells, t.bytes);
+  t.d_cells = nullptr;
+  t.bytes = 0;
+}
+
+DevTable* find_table(s615_ctx* ctx, int id) {
+  auto it = ctx->tables.find(id);
+  return it == ctx->tables.end() ? nullptr : &it->second;
+}
+
+int add_table(s615_ctx* ctx, DevTable t, int* id) {
+  const int k = ctx->next_table++;
+  ctx->tables[k] = t;
+  if (id) *id = k;
+  return S615_OK;
+}
+
+bool header_ok(const s615_header& h) {  // store_header.hpp:39-42 plus kind == Xor
+  return h.magic == kMagic && h.version == kVersion && h.shard_count >= 1 &&
+         h.shard_index < h.shard_count && h.r > 0 && h.r <= 64 && h.kind == 1;
+}
+
+// Choose the HBM layout of a table with m cells of r bits.
+int pick_layout(s615_ctx* ctx, int want, u64 m, u32 r, int* cell_bytes) {
+  *cell_bytes = r <= 32 ? 4 : 8;
+  if (want == S615_LAYOUT_PACKED) { *cell_bytes = 0; return S615_LAYOUT_PACKED; }
+  if (want == S615_LAYOUT_WIDE) return S615_LAYOUT_WIDE;
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  const size_t wide = m * (size_t)(*cell_bytes) + packed_bytes(m, r) + ((size_t)4 << 30);
+  const size_t room = std::min(free_b, ctx->budget ? ctx->budget - std::min(ctx->budget, ctx->used) : free_b);
+  if (wide <= room) return S615_LAYOUT_WIDE;
+  *cell_bytes = 0;
+  return S615_LAYOUT_PACKED;
+}
+
+// Turn a device buffer holding packed bytes into the chosen layout.
+int finish_upload(s615_ctx* ctx, DevTable& t, void* d_packed, size_t packed_alloc, int layout,
+                  int cell_bytes) {
+  if (layout == S615_LAYOUT_PACKED) {
+    t.layout = S615_LAYOUT_PACKED; t.cell_bytes = 0;
+    t.d_cells = d_packed; t.bytes = packed_alloc;
+    return S615_OK;
+  }
+  void* wide = nullptr;
+  const size_t wb = t.hdr.m_cells * (size_t)cell_bytes;
+  int s = dev_alloc(ctx, &wide, wb);
+  if (s) { dev_free(ctx, d_packed, packed_alloc); return s; }
+  s = launch_unpack(ctx, static_cast<const u8*>(d_packed), t.hdr.m_cells, t.hdr.r, wide, cell_bytes,
+                    ctx->stream);
+  const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  dev_free(ctx, d_packed, packed_alloc);
+  if (s || e != cudaSuccess) { dev_free(ctx, wide, wb); return s ? s : cuda_status(e); }
+  t.layout = S615_LAYOUT_WIDE; t.cell_bytes = cell_bytes;
+  t.d_cells = wide; t.bytes = wb;
+  return S615_OK;
+}
+
+}  // namespace
+
+// ======================================================================= ABI
+extern "C" {
+
+const char* s615_strerror(int s) {
+  switch (s) {
+    case S615_OK: return "ok";
+    case S615_E_ARG: return "bad argument";
+    case S615_E_IO: return "i/o error";
+    case S615_E_FORMAT: return "bad format";
+    case S615_E_N_MISMATCH: return "table N mismatch";
+    case S615_E_FPR_SMOKE: return "xor FPR smoke too high";
+    case S615_E_OOM: return "out of device memory / HBM budget";
+    case S615_E_DEVICE: return "CUDA error";
+    case S615_E_TIMEOUT: return "device wait timed out";
+    case S615_E_OVERFLOW: return "result buffer overflow";
+    case S615_E_BUILD: return "xor peel stalled for every seed";
+    case S615_E_NOTABLE: return "unknown table id";
+  }
+  return "unknown status";
+}
+
+int s615_open(int device, size_t hbm_budget, s615_ctx** out) {
+  if (!out) return S615_E_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return S615_E_DEVICE;
+  }
+  std::unique_ptr<s615_ctx> ctx(new s615_ctx());
+  ctx->device = device;
+  S615_CU(cudaSetDevice(device));
+  S615_CU(cudaFree(nullptr));
+  S615_CU(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  S615_CU(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
+  size_t free_b = 0, total_b = 0;
+  S615_CU(cudaMemGetInfo(&free_b, &total_b));
+  ctx->budget = hbm_budget ? hbm_budget : total_b;
+  u32 pat[kPatWords];
+  void* p = nullptr;
+  int s = dev_alloc(ctx.get(), &p, sizeof pat);
+  if (s) return s;
+  ctx->d_pat_gate = static_cast<u32*>(p);
+  gate_patterns(true, pat);
+  S615_CU(cudaMemcpy(ctx->d_pat_gate, pat, sizeof pat, cudaMemcpyHostToDevice));
+  if ((s = dev_alloc(ctx.get(), &p, sizeof pat))) return s;
+  ctx->d_pat_open = static_cast<u32*>(p);
+  gate_patterns(false, pat);
+  S615_CU(cudaMemcpy(ctx->d_pat_open, pat, sizeof pat, cudaMemcpyHostToDevice));
+  *out = ctx.release();
+  return S615_OK;
+}
+
+int s615_close(s615_ctx* ctx) {
+  if (!ctx) return S615_E_ARG;
+  cudaSetDevice(ctx->device);
+  for (auto& kv : ctx->tables) free_table(ctx, kv.second);
+  ctx->tables.clear();
+  dev_free(ctx, ctx->d_pat_gate, kPatWords * 4);
+  dev_free(ctx, ctx->d_pat_open, kPatWords * 4);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return S615_OK;
+}
+
+uint64_t s615_launch_count(s615_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int s615_get_table_info(s615_ctx* ctx, int id, s615_table_info* info) {
+  if (!ctx || !info) return S615_E_ARG;
+  DevTable* t = find_table(ctx, id);
+  if (!t) return S615_E_NOTABLE;
+  info->hdr = t->hdr;
+  info->layout = t->layout;
+  info->cell_bytes = t->cell_bytes;
+  info->device_bytes = t->bytes;
+  return S615_OK;
+}
+
+int s615_free_table(s615_ctx* ctx, int id) {
+  if (!ctx) return S615_E_ARG;
+  DevTable* t = find_table(ctx, id);
+  if (!t) return S615_E_NOTABLE;
+  cudaSetDevice(ctx->device);
+  free_table(ctx, *t);
+  ctx->tables.erase(id);
+  return S615_OK;
+}
+
+int s615_xor_query_dev(s615_ctx* ctx, int id, const uint64_t* d_keys, size_t n, uint8_t* d_out,
+                       void* stream) {
+  if (!ctx) return S615_E_ARG;
+  DevTable* t = find_table(ctx, id);
+  if (!t) return S615_E_NOTABLE;
+  return launch_xor_query(ctx, view_of(*t), d_keys, n, d_out,
+                          stream ? static_cast<cudaStream_t>(stream) : ctx->stream);
+}
+
+int s615_xor_query(s615_ctx* ctx, int id, const uint64_t* keys, size_t n, uint8_t* out) {
+  if (!ctx || (n && (!keys || !out))) return S615_E_ARG;
+  DevTable* t = find_table(ctx, id);
+  if (!t) return S615_E_NOTABLE;
+  if (n == 0) return S615_OK;
+  cudaSetDevice(ctx->device);
+  const size_t chunk = std::min<size_t>(n, (size_t)1 << 26);
+  void *dk = nullptr, *dout = nullptr;
+  int s = dev_alloc(ctx, &dk, chunk * 8);
+  if (s) return s;
+  if ((s = dev_alloc(ctx, &dout, chunk))) { dev_free(ctx, dk, chunk * 8); return s; }
+  const TableView tv = view_of(*t);
+  for (size_t off = 0; off < n && !s; off += chunk) {
+    const size_t c = std::min(chunk, n - off);
+    cudaError_t e = cudaMemcpyAsync(dk, keys + off, c * 8, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) s = launch_xor_query(ctx, tv, static_cast<const u64*>(dk), c,
+                                               static_cast<u8*>(dout), ctx->stream);
+    if (e == cudaSuccess && !s) e = cudaMemcpyAsync(out + off, dout, c, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess && !s) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) s = cuda_status(e);
+  }
+  dev_free(ctx, dk, chunk * 8);
+  dev_free(ctx, dout, chunk);
+  return s;
+}
+
+// xor_fpr_smoke (fourcore_xor_store.hpp:54-65): 200k keys x <- x*phi + 1 from
+// 0x123456789abcdef0 through the device query; refuse more than 16 hits.
+static int smoke_table(s615_ctx* ctx, int id) {
+  DevTable* t = find_table(ctx, id);
+  if (t->hdr.m_cells < 3 || t->hdr.r == 0 || !t->d_cells) return S615_E_FPR_SMOKE;
+  const size_t n = 200000;
+  std::vector<u64> keys(n);
+  u64 x = 0x123456789abcdef0ULL;
+  for (size_t i = 0; i < n; ++i) { x = x * kPhi + 1; keys[i] = x; }
+  std::vector<u8> out(n);
+  const int s = s615_xor_query(ctx, id, keys.data(), n, out.data());
+  if (s) return s;
+  size_t hits = 0;
+  for (u8 v : out) hits += v;
+  return hits > 16 ? S615_E_FPR_SMOKE : S615_OK;
+}
+
+int s615_load_table(s615_ctx* ctx, const char* path, int expected_N, int layout, int* table_id) {
+  if (!ctx || !path) return S615_E_ARG;
+  cudaSetDevice(ctx->device);
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return S615_E_IO;
+  DevTable t;
+  if (std::fread(&t.hdr, sizeof t.hdr, 1, f) != 1) { std::fclose(f); return S615_E_IO; }
+  if (!header_ok(t.hdr)) { std::fclose(f); return S615_E_FORMAT; }
+  if (expected_N > 0 && (int)t.hdr.N != expected_N) { std::fclose(f); return S615_E_N_MISMATCH; }
+  const u64 len = packed_bytes(t.hdr.m_cells, t.hdr.r);
+  const size_t alloc = ((len + 7) / 8 + 1) * 8;
+  int cell_bytes = 0;
+  const int lay = pick_layout(ctx, layout, t.hdr.m_cells, t.hdr.r, &cell_bytes);
+  void* d = nullptr;
+  int s = dev_alloc(ctx, &d, alloc);
+  if (s) { std::fclose(f); return s; }
+  cudaMemsetAsync(d, 0, alloc, ctx->stream);
+  // Stream the file through two pinned staging buffers.
+  const size_t stage = (size_t)64 << 20;
+  void* pin[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2];
+  bool ok = cudaMallocHost(&pin[0], stage) == cudaSuccess && cudaMallocHost(&pin[1], stage) == cudaSuccess;
+  cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+  u64 done = 0;
+  int k = 0;
+  while (ok && done < len) {
+    const size_t c = (size_t)std::min<u64>(stage, len - done);
+    cudaEventSynchronize(ev[k]);
+    if (std::fread(pin[k], 1, c, f) != c) { ok = false; s = S615_E_IO; break; }
+    if (cudaMemcpyAsync(static_cast<u8*>(d) + done, pin[k], c, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) {
+      ok = false; s = S615_E_DEVICE; break;
+    }
+    cudaEventRecord(ev[k], ctx->stream);
+    done += c;
+    k ^= 1;
+  }
+  cudaStreamSynchronize(ctx->stream);
+  std::fclose(f);
+  for (int i = 0; i < 2; ++i) { if (pin[i]) cudaFreeHost(pin[i]); cudaEventDestroy(ev[i]); }
+  if (!ok) { dev_free(ctx, d, alloc); return s ? s : S615_E_OOM; }
+  if ((s = finish_upload(ctx, t, d, alloc, lay, cell_bytes))) return s;
+  int id = 0;
+  add_table(ctx, t, &id);
+  if ((s = smoke_table(ctx, id))) { s615_free_table(ctx, id); return s; }
+  if (table_id) *table_id = id;
+  return S615_OK;
+}
+
+// The packed file bytes of a resident table into buf (len bytes).
+static int export_packed(s615_ctx* ctx, const DevTable& t, u8* buf, u64 len) {
+  if (!len) return S615_OK;
+  if (t.layout == S615_LAYOUT_PACKED) {
+    S615_CU(cudaMemcpy(buf, t.d_cells, len, cudaMemcpyDeviceToHost));
+    return S615_OK;
+  }
+  void* pk = nullptr;
+  const size_t pb = ((len + 7) / 8 + 1) * 8;
+  int s = dev_alloc(ctx, &pk, pb);
+  if (s) return s;
+  s = launch_pack(ctx, t.d_cells, t.cell_bytes, t.hdr.m_cells, t.hdr.r, static_cast<u8*>(pk), len,
+                  ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (!s && e == cudaSuccess) e = cudaMemcpy(buf, pk, len, cudaMemcpyDeviceToHost);
+  dev_free(ctx, pk, pb);
+  if (s) return s;
+  return cuda_status(e);
+}
+
+int s615_export_table(s615_ctx* ctx, int id, s615_header* hdr, uint8_t* buf, size_t cap,
+                      size_t* len) {
+  if (!ctx) return S615_E_ARG;
+  DevTable* t = find_table(ctx, id);
+  if (!t) return S615_E_NOTABLE;
+  cudaSetDevice(ctx->device);
+  const u64 n = packed_bytes(t->hdr.m_cells, t->hdr.r);
+  if (hdr) *hdr = t->hdr;
+  if (len) *len = n;
+  if (!buf) return S615_OK;
+  if (cap < n) return S615_E_OVERFLOW;
+  return export_packed(ctx, *t, buf, n);
+}
+
+int s615_save_table(s615_ctx* ctx, int id, const char* path) {
+  if (!ctx || !path) return S615_E_ARG;
+  DevTable* t = find_table(ctx, id);
+  if (!t) return S615_E_NOTABLE;
+  cudaSetDevice(ctx->device);
+  const u64 len = packed_bytes(t->hdr.m_cells, t->hdr.r);
+  std::vector<u8> host(len);
+  const int s = export_packed(ctx, *t, host.data(), len);
+  if (s) return s;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return S615_E_IO;
+  bool ok = std::fwrite(&t->hdr, sizeof t->hdr, 1, f) == 1;
+  if (ok && len) ok = std::fwrite(host.data(), 1, len, f) == len;
+  ok = (std::fclose(f) == 0) && ok;
+  return ok ? S615_OK : S615_E_IO;
+}
+
+int s615_build_table(s615_ctx* ctx, int N, int r, int layout, int* table_id) {
+  if (!ctx || N < 1 || N > 4 * kNSoftMax || r < 8 || r > 64) return S615_E_ARG;
+  cudaSetDevice(ctx->device);
+  // distinct values of i^6 mod 2^64 (many i collide 2-adically)
+  std::vector<u64> vals((size_t)N);
+  for (int i = 1; i <= N; ++i) { const u64 x2 = (u64)i * (u64)i; vals[i - 1] = x2 * x2 * x2; }
+  std::sort(vals.begin(), vals.end());
+  vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
+  void* dv = nullptr;
+  int s = dev_alloc(ctx, &dv, vals.size() * 8);
+  if (s) return s;
+  S615_CU(cudaMemcpy(dv, vals.data(), vals.size() * 8, cudaMemcpyHostToDevice));
+  u64 seeds[4];
+  for (int o = 0; o < 4; ++o) seeds[o] = kSeedBase + (u64)o * kPhi;
+  DevTable t;
+  s = build_xor_device(ctx, static_cast<const u64*>(dv), vals.size(), nullptr, 0, r, seeds, 4, N,
+                       layout == S615_LAYOUT_AUTO ? S615_LAYOUT_WIDE : layout, &t);
+  dev_free(ctx, dv, vals.size() * 8);
+  if (s) return s;
+  int id = 0;
+  add_table(ctx, t, &id);
+  if ((s = smoke_table(ctx, id))) { s615_free_table(ctx, id); return s; }
+  if (table_id) *table_id = id;
+  return S615_OK;
+}
+
+int s615_build_table_keys(s615_ctx* ctx, const uint64_t* keys, size_t n, int r, uint64_t base_seed,
+                          int layout, int* table_id) {
+  if (!ctx || (n && !keys) || r < 1 || r > 64) return S615_E_ARG;
+  cudaSetDevice(ctx->device);
+  void* dk = nullptr;
+  int s = dev_alloc(ctx, &dk, std::max<size_t>(n, 1) * 8);
+  if (s) return s;
+  if (n) S615_CU(cudaMemcpy(dk, keys, n * 8, cudaMemcpyHostToDevice));
+  DevTable t;
+  const u64 seed = base_seed;
+  s = build_xor_device(ctx, nullptr, 0, static_cast<const u64*>(dk), n, r, &seed, 1, 0,
+                       layout == S615_LAYOUT_AUTO ? S615_LAYOUT_WIDE : layout, &t);
+  dev_free(ctx, dk, std::max<size_t>(n, 1) * 8);
+  if (s) return s;
+  return add_table(ctx, t, table_id);
+}
+
+int s615_mem_info(s615_ctx* ctx, size_t* free_b, size_t* total_b) {
+  if (!ctx || !free_b || !total_b) return S615_E_ARG;
+  cudaSetDevice(ctx->device);
+  S615_CU(cudaMemGetInfo(free_b, total_b));
+  return S615_OK;
+}
+
+int s615_unit_status(const s615_unit* unit) {
+  if (!unit) return S615_E_ARG;
+  DevUnit5 d;
+  bool skip = false;
+  const int s = make_dev_unit(*unit, 0, &d, &skip);
+  if (s) return s;
+  return skip ? 1 : S615_OK;
+}
+
+int s615_unit_candidates(uint64_t B, int cls, uint64_t* out, size_t cap, size_t* n) {
+  if (!n || cls < 1 || cls > 5) return S615_E_ARG;
+  const auto v = unit_candidates(B, cls);
+  for (size_t i = 0; i < v.size() && i < cap; ++i) out[i] = v[i];
+  *n = v.size();
+  return v.size() > cap ? S615_E_OVERFLOW : S615_OK;
+}
+
+// ------------------------------------------------------------- cls5 batches
+int s615_cls5_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch** out) {
+  if (!ctx || !out || (n && !units)) return S615_E_ARG;
+  cudaSetDevice(ctx->device);
+  std::unique_ptr<s615_batch> b(new s615_batch());
+  std::vector<DevUnit5> du;
+  du.reserve(n);
+  for (size_t i = 0; i < n; ++i) {
+    DevUnit5 d;
+    bool skip = false;
+    const int s = make_dev_unit(units[i], (u32)i, &d, &skip);
+    if (s) return s;
+    if (skip) continue;
+    for (u32 ie = 0; ie < d.nres1; ++ie) b->host_items.push_back(((u32)du.size() << 4) | ie);
+    du.push_back(d);
+  }
+  b->n_units = du.size();
+  b->n_items = b->host_items.size();
+  int s = 0;
+  void* p = nullptr;
+  if ((s = dev_alloc(ctx, &p, std::max<size_t>(du.size(), 1) * sizeof(DevUnit5)))) return s;
+  b->d_units = static_cast<DevUnit5*>(p);
+  if ((s = dev_alloc(ctx, &p, std::max<size_t>(b->n_items, 1) * 4))) { s615_cls5_batch_free(ctx, b.release()); return s; }
+  b->d_items = static_cast<u32*>(p);
+  if ((s = dev_alloc(ctx, &p, sizeof(Cls5Counters) + 64))) { s615_cls5_batch_free(ctx, b.release()); return s; }
+  b->d_ctr = static_cast<Cls5Counters*>(p);
+  b->d_work = reinterpret_cast<u32*>(static_cast<char*>(p) + sizeof(Cls5Counters));
+  b->hit_cap = 1u << 20;
+  if ((s = dev_alloc(ctx, &p, (size_t)b->hit_cap * sizeof(s615_hit)))) { s615_cls5_batch_free(ctx, b.release()); return s; }
+  b->d_hits = static_cast<s615_hit*>(p);
+  if (!du.empty()) S615_CU(cudaMemcpy(b->d_units, du.data(), du.size() * sizeof(DevUnit5), cudaMemcpyHostToDevice));
+  if (b->n_items) S615_CU(cudaMemcpy(b->d_items, b->host_items.data(), b->n_items * 4, cudaMemcpyHostToDevice));
+  *out = b.release();
+  return S615_OK;
+}
+
+int s615_cls5_batch_free(s615_ctx* ctx, s615_batch* b) {
+  if (!ctx || !b) return S615_E_ARG;
+  dev_free(ctx, b->d_units, std::max<size_t>(b->n_units, 1) * sizeof(DevUnit5));
+  dev_free(ctx, b->d_items, std::max<size_t>(b->n_items, 1) * 4);
+  dev_free(ctx, b->d_ctr, sizeof(Cls5Counters) + 64);
+  dev_free(ctx, b->d_hits, (size_t)b->hit_cap * sizeof(s615_hit));
+  delete b;
+  return S615_OK;
+}
+
+int s615_cls5_run_batch(s615_ctx* ctx, int id, s615_batch* b, unsigned flags, void* stream) {
+  if (!ctx || !b) return S615_E_ARG;
+  DevTable* t = find_table(ctx, id);
+  if (!t) return S615_E_NOTABLE;
+  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  const TableView tv = view_of(*t);
+  S615_CU(cudaMemsetAsync(b->d_ctr, 0, sizeof(Cls5Counters) + 64, st));
+  if (!(flags & S615_F_PLAIN)) return launch_cls5_sieve(ctx, tv, b, flags, st, 0);
+  // Plain form: one unit per launch and a sync after each, like the
+  // reference's per-chunk loop.
+  s615_batch one = *b;
+  size_t i = 0;
+  while (i < b->n_items) {
+    size_t j = i;
+    while (j < b->n_items && (b->host_items[j] >> 4) == (b->host_items[i] >> 4)) ++j;
+    one.d_items = b->d_items + i;
+    one.n_items = j - i;
+    S615_CU(cudaMemsetAsync(b->d_work, 0, 4, st));
+    int s = launch_cls5_sieve(ctx, tv, &one, flags, st, (int)(j - i));
+    if (s) return s;
+    S615_CU(cudaStreamSynchronize(st));
+    i = j;
+  }
+  return S615_OK;
+}
+
+int s615_cls5_batch_results(s615_ctx* ctx, s615_batch* b, s615_hit* hits, size_t hit_cap,
+                            size_t* n_hits, s615_counters* counters) {
+  if (!ctx || !b) return S615_E_ARG;
+  Cls5Counters c{};
+  S615_CU(cudaStreamSynchronize(ctx->stream));
+  S615_CU(cudaMemcpy(&c, b->d_ctr, sizeof c, cudaMemcpyDeviceToHost));
+  if (counters) {
+    counters->calls = c.calls;
+    counters->probes = c.probes;
+    counters->pos = c.pos;
+    counters->gated = c.pos - c.probes;
+    counters->hits = c.hits;
+  }
+  const size_t nh = (size_t)c.hits;
+  if (n_hits) *n_hits = nh;
+  const size_t avail = std::min<size_t>(nh, b->hit_cap);
+  const size_t take = std::min(avail, hit_cap);
+  if (take && hits) S615_CU(cudaMemcpy(hits, b->d_hits, take * sizeof(s615_hit), cudaMemcpyDeviceToHost));
+  if (nh > b->hit_cap || nh > hit_cap) return S615_E_OVERFLOW;
+  return S615_OK;
+}
+
+int s615_cls5_run(s615_ctx* ctx, int id, const s615_unit* units, size_t n, unsigned flags,
+                  s615_hit* hits, size_t hit_cap, size_t* n_hits, s615_counters* counters) {
+  if (!ctx) return S615_E_ARG;
+  if (!find_table(ctx, id)) return S615_E_NOTABLE;
+  cudaSetDevice(ctx->device);
+  s615_batch* b = nullptr;
+  int s = s615_cls5_prepare(ctx, units, n, &b);
+  if (s) return s;
+  s = s615_cls5_run_batch(ctx, id, b, flags, nullptr);
+  if (!s) s = s615_cls5_batch_results(ctx, b, hits, hit_cap, n_hits, counters);
+  s615_cls5_batch_free(ctx, b);
+  return s;
+}
+
+int s615_cls5_verify(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s615_hit* hits,
+                     size_t n_hits, int N, s615_solution* out, size_t cap, size_t* n_out) {
+  if (!ctx || !n_out || N < 1) return S615_E_ARG;
+  cudaSetDevice(ctx->device);
+  return verify_cls5_device(ctx, units, n_units, hits, n_hits, N, out, cap, n_out);
+}
+
+// Host self-test (no GPU): the reference's --selftest-host checks
+// (fourcore_cls5_gpu_v4.cu:186-263) plus the engine's own invariants.
+// Returns 0 on success, else the number of the failed check.
+int s615_selftest_host(void) {
+  // 1. pow6 in three limbs against repeated multiplication
+  for (u64 x : {1ULL, 42ULL, 100003ULL, 2353975ULL, 2752470ULL}) {
+    W3 a = pow6_w3(x), b{{1, 0, 0}};
+    for (int i = 0; i < 6; ++i) b = mul_w3_u64(b, x);
+    if (!eq_w3(a, b)) return 1;
+  }
+  // 2. gate = CRT product of the five factor sets; 27/504 and 50/247
+  if (!gate_product_matches()) return 2;
+  // 3. exact remainder against %
+  std::mt19937_64 rng(615);
+  for (int i = 0; i < 200000; ++i) {
+    u64 block = (rng() >> (rng() % 62)) | 2;
+    const u64 h = rng();
+    if (fast_mod(h, block, mod_recip(block)) != h % block) return 3;
+  }
+  const u64 blocks[] = {2, 3, 1ULL << 32, (1ULL << 63) + 1, ~0ULL, 1190335832ULL};
+  for (const u64 block : blocks) {
+    const u64 hs[] = {0, ~0ULL, block - 1, block, 2 * block - 1, 12345678901234567ULL};
+    for (const u64 h : hs)
+      if (fast_mod(h, block, mod_recip(block)) != h % block) return 3;
+  }
+  // 4. the row formulation: T = (V - d^6)/64 equals the exact peel at the
+  //    reference's sample (B=100003, u=17646, d=9, e=44)
+  {
+    const u64 B = 100003, u = 17646, d = 9, e = 44;
+    W3 R = pow6_w3(B);
+    sub_w3(R, pow6_w3(u));
+    W3 V = R;
+    if (sub_w3(V, pow6_w3(14 * e))) return 4;
+    if (divmod_w3(V, kM21) != 0) return 4;
+    W3 R2 = R;
+    sub_w3(R2, pow6_w3(14 * e));
+    sub_w3(R2, pow6_w3(21 * d));
+    if (divmod_w3(R2, kM42) != 0) return 4;
+    W3 T = V;
+    if (sub_w3(T, pow6_w3(d))) return 4;
+    if (divmod_w3(T, 64) != 0 || !eq_w3(T, R2)) return 4;
+  }
+  // 5. B^6 at B=2752470 needs at most 192 bits (134)
+  {
+    W3 b6 = pow6_w3(2752470ULL);
+    if (b6.l[2] == 0 || (b6.l[2] >> 7) != 0) return 5;
+  }
+  // 6. capacity rule
+  if (capacity_for(0) != 33 || capacity_for(45150) != 55569) return 6;
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,293 @@
+// cli_cls5.cpp -- s615_cls5, a drop-in for fourcore_cls5_gpu_v4.
+//
+// Same flags, semantics, stdout lines and exit codes as
+// fourcore_cls5_gpu_v4.cu:596-709 (usage, argument parsing, --check-table,
+// acquire_xor_filter's FATAL paths, the SOLUTION and "---- done" lines).
+// Extra flags: --dump-survivors F (one "B u d e fp" line per raw filter hit,
+// reference naming: d is the x21 term, e the x14 term), --plain (one unit per
+// launch), --layout packed|wide, --batch K (units per device batch).
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/s615.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+constexpr int kNSoftMax = 120000;   // fourcore_xor_store.hpp:122
+
+void usage() {
+  std::printf(
+      "usage: s615_cls5 [--selftest-host]\n"
+      "   or: s615_cls5 --units FILE.buc [--r BITS]\n"
+      "                 [--N K] [--quiet|--no-quiet] [--no-gate]\n"
+      "                 [--stop-first] [--device K]\n"
+      "                 [--load-table F] [--save-table F]\n"
+      "                 [--allow-rebuild] [--dump-survivors F] [--plain]\n"
+      "                 [--layout packed|wide] [--batch K]\n"
+      "   or: s615_cls5 --check-table --N K --load-table F\n"
+      "                 [--r BITS] [--save-table F] [--allow-rebuild]\n"
+      "  --load-table F: packed xor from xor_build_save / --save-table.\n"
+      "  --save-table F: write packed xor after build or successful load.\n"
+      "  --allow-rebuild: if --load-table fails, build on the device (default: FATAL).\n"
+      "  --check-table: load + FPR smoke only.\n");
+}
+
+int selftest_host() {
+  std::printf("[selftest-host] cls5 engine (row identity, gate factors, exact remainder)\n");
+  const int s = s615_selftest_host();
+  if (s != 0) {
+    std::printf("FAIL check %d\n", s);
+    return 1;
+  }
+  std::printf("[selftest-host] PASS\n");
+  return 0;
+}
+
+struct Line { int cls; unsigned long long B, u; };
+
+bool load_buc5(const char* path, std::vector<Line>& out) {  // fourcore_cls5_gpu_v4.cu:155-167
+  FILE* f = std::fopen(path, "r");
+  if (!f) return false;
+  char buf[256];
+  while (std::fgets(buf, sizeof buf, f)) {
+    int cls;
+    unsigned long long B, u;
+    if (std::sscanf(buf, "%d %llu %llu", &cls, &B, &u) != 3) continue;
+    if (cls != 5) continue;
+    out.push_back({cls, B, u});
+  }
+  std::fclose(f);
+  return !out.empty();
+}
+
+// acquire_xor_filter (fourcore_cls5_gpu_v4.cu:568-594) on the device.
+bool acquire(s615_ctx* ctx, int N, int& r, const std::string& load, const std::string& save,
+             bool allow_rebuild, int layout, int& tid) {
+  bool loaded = false;
+  if (!load.empty()) {
+    const int s = s615_load_table(ctx, load.c_str(), N, layout, &tid);
+    if (s == S615_E_FPR_SMOKE) {
+      std::fprintf(stderr, "[cls5-gpu] FATAL: xor FPR smoke too high — refuse to search\n");
+      return false;
+    }
+    loaded = s == S615_OK;
+    if (!loaded) {
+      std::fprintf(stderr, "[xor] cannot use %s: %s\n", load.c_str(), s615_strerror(s));
+      if (!allow_rebuild) {
+        std::fprintf(stderr,
+                     "[cls5-gpu] FATAL: --load-table failed (see [xor] lines above). Fix N/path, or "
+                     "pass --allow-rebuild to build the table on the device.\n");
+        return false;
+      }
+      std::fprintf(stderr, "[cls5-gpu] --load-table failed; --allow-rebuild: building xor on device...\n");
+    }
+  }
+  if (!loaded) {
+    const int s = s615_build_table(ctx, N, r, layout, &tid);
+    if (s) {
+      std::fprintf(stderr, "[cls5-gpu] FATAL: xor build failed: %s\n", s615_strerror(s));
+      return false;
+    }
+  }
+  s615_table_info info;
+  s615_get_table_info(ctx, tid, &info);
+  r = (int)info.hdr.r;
+  std::fprintf(stderr, "[xor] N=%u keys=%llu cells=%llu r=%u seed=0x%llx (%.2f GB in HBM)\n",
+               info.hdr.N, (unsigned long long)info.hdr.n_keys, (unsigned long long)info.hdr.m_cells,
+               info.hdr.r, (unsigned long long)info.hdr.mix_seed, info.device_bytes / 1e9);
+  if (!save.empty()) {
+    const int s = s615_save_table(ctx, tid, save.c_str());
+    if (s) {
+      std::fprintf(stderr, "[xor] cannot save %s: %s\n", save.c_str(), s615_strerror(s));
+      return false;
+    }
+    std::fprintf(stderr, "[xor] saved %s\n", save.c_str());
+  }
+  return true;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  std::setvbuf(stdout, nullptr, _IOLBF, 0);
+  std::setvbuf(stderr, nullptr, _IOLBF, 0);
+  std::string units_path, load_table, save_table, dump_path;
+  int device = 0, N_override = 0, xor_r = 48, layout = S615_LAYOUT_AUTO;
+  size_t batch = 1 << 16;
+  bool do_host = false, quiet = true, use_gate = true, stop_first = false;
+  bool allow_rebuild = false, check_table = false, plain = false;
+  for (int i = 1; i < argc; ++i) {
+    const std::string s = argv[i];
+    auto next = [&]() { return (i + 1 < argc) ? std::string(argv[++i]) : std::string(); };
+    if (s == "--selftest-host") do_host = true;
+    else if (s == "--units") units_path = next();
+    else if (s == "--max-table-gb") (void)next();   // accepted and ignored, like the reference
+    else if (s == "--S") (void)next();              // accepted and ignored, like the reference
+    else if (s == "--r") xor_r = std::atoi(next().c_str());
+    else if (s == "--N") N_override = std::atoi(next().c_str());
+    else if (s == "--quiet") quiet = true;
+    else if (s == "--no-quiet") quiet = false;
+    else if (s == "--no-gate") use_gate = false;
+    else if (s == "--stop-first") stop_first = true;
+    else if (s == "--device") device = std::atoi(next().c_str());
+    else if (s == "--load-table") load_table = next();
+    else if (s == "--save-table") save_table = next();
+    else if (s == "--allow-rebuild") allow_rebuild = true;
+    else if (s == "--check-table") check_table = true;
+    else if (s == "--dump-survivors") dump_path = next();
+    else if (s == "--plain") plain = true;
+    else if (s == "--batch") batch = (size_t)std::max(1, std::atoi(next().c_str()));
+    else if (s == "--layout") {
+      const std::string v = next();
+      layout = v == "packed" ? S615_LAYOUT_PACKED : v == "wide" ? S615_LAYOUT_WIDE : S615_LAYOUT_AUTO;
+    } else if (s == "-h" || s == "--help") { usage(); return 0; }
+    else { std::fprintf(stderr, "unknown %s\n", s.c_str()); usage(); return 1; }
+  }
+  if (do_host || argc == 1) return selftest_host();
+  if (xor_r < 8 || xor_r > 64) { std::fprintf(stderr, "--r must be 8..64\n"); return 1; }
+
+  if (check_table) {
+    if (N_override <= 0) { std::fprintf(stderr, "--check-table needs --N\n"); return 1; }
+    if (N_override > kNSoftMax) {
+      std::fprintf(stderr, "N=%d exceeds soft xor cap %d\n", N_override, kNSoftMax);
+      return 1;
+    }
+  } else if (units_path.empty()) {
+    usage();
+    return 1;
+  }
+
+  s615_ctx* ctx = nullptr;
+  int s = s615_open(device, 0, &ctx);
+  if (s) { std::fprintf(stderr, "CUDA device %d: %s\n", device, s615_strerror(s)); return 1; }
+  size_t free_b = 0, total_b = 0;
+  s615_mem_info(ctx, &free_b, &total_b);
+  std::fprintf(stderr, "[cls5-gpu] device=%d free=%.1f / total=%.1f GB\n", device, free_b / 1e9,
+               total_b / 1e9);
+
+  if (check_table) {
+    int tid = 0;
+    if (!acquire(ctx, N_override, xor_r, load_table, save_table, allow_rebuild, layout, tid)) {
+      s615_close(ctx);
+      return 1;
+    }
+    s615_table_info info;
+    s615_get_table_info(ctx, tid, &info);
+    std::fprintf(stderr, "[cls5-gpu] --check-table OK N=%d r=%d packed=%.3f GB\n", N_override, xor_r,
+                 (double)(info.hdr.m_cells * info.hdr.r / 8 + 8) / 1e9);
+    s615_close(ctx);
+    return 0;
+  }
+
+  std::vector<Line> lines;
+  if (!load_buc5(units_path.c_str(), lines)) {
+    std::fprintf(stderr, "no cls5 units in %s\n", units_path.c_str());
+    s615_close(ctx);
+    return 1;
+  }
+  std::vector<s615_unit> units;
+  units.reserve(lines.size());
+  unsigned need = 0;
+  for (const Line& L : lines) {
+    s615_unit U{};
+    U.cls = 5; U.kind = 0; U.B = L.B; U.u = L.u;
+    const int st = s615_unit_status(&U);
+    if (st == 1) continue;
+    if (st != S615_OK) {
+      std::fprintf(stderr, "[cls5-gpu] unit B=%llu u=%llu rejected: %s\n", L.B, L.u, s615_strerror(st));
+      continue;
+    }
+    need = std::max(need, (unsigned)((L.B - 1) / 42));
+    units.push_back(U);
+  }
+  std::fprintf(stderr, "[cls5-gpu] packed %zu/%zu units from %s\n", units.size(), lines.size(),
+               units_path.c_str());
+  if (units.empty()) { s615_close(ctx); return 1; }
+  const int N = N_override > 0 ? N_override : (int)need;
+  if (N > kNSoftMax) {
+    std::fprintf(stderr, "N=%d exceeds soft xor cap %d\n", N, kNSoftMax);
+    s615_close(ctx);
+    return 1;
+  }
+  std::fprintf(stderr, "[cls5-gpu] N=%d r=%d\n", N, xor_r);
+  int tid = 0;
+  if (!acquire(ctx, N, xor_r, load_table, save_table, allow_rebuild, layout, tid)) {
+    s615_close(ctx);
+    return 1;
+  }
+
+  FILE* dump = nullptr;
+  if (!dump_path.empty()) {
+    dump = std::fopen(dump_path.c_str(), "w");
+    if (!dump) { std::fprintf(stderr, "cannot open %s\n", dump_path.c_str()); s615_close(ctx); return 1; }
+  }
+  const unsigned flags = (use_gate ? 0u : S615_F_NO_GATE) | (plain ? S615_F_PLAIN : 0u);
+  unsigned long long tot_calls = 0, tot_gated = 0, tot_probes = 0, sols = 0;
+  const auto t0 = Clock::now();
+  std::vector<s615_hit> hits;
+  std::vector<s615_solution> solv;
+  size_t chunk_no = 0;
+  for (size_t off = 0; off < units.size(); off += batch, ++chunk_no) {
+    const size_t n = std::min(batch, units.size() - off);
+    size_t cap = std::max<size_t>(hits.size(), 1 << 16), nh = 0;
+    s615_counters c{};
+    for (;;) {
+      hits.resize(cap);
+      s = s615_cls5_run(ctx, tid, units.data() + off, n, flags, hits.data(), cap, &nh, &c);
+      if (s == S615_E_OVERFLOW && nh > cap) { cap = nh + nh / 4; continue; }
+      break;
+    }
+    if (s) {
+      std::fprintf(stderr, "[cls5-gpu] run failed: %s\n", s615_strerror(s));
+      s615_close(ctx);
+      return 1;
+    }
+    tot_calls += c.calls; tot_gated += c.gated; tot_probes += c.probes;
+    if (dump)
+      for (size_t k = 0; k < nh; ++k) {
+        const s615_unit& U = units[off + hits[k].unit];
+        std::fprintf(dump, "%llu %llu %u %u %llu\n", (unsigned long long)U.B, (unsigned long long)U.u,
+                     hits[k].d, hits[k].e, (unsigned long long)hits[k].fp);
+      }
+    if (nh) {
+      size_t ns = 0;
+      size_t scap = std::max<size_t>(16, nh);
+      solv.resize(scap);
+      s = s615_cls5_verify(ctx, units.data() + off, n, hits.data(), nh, N, solv.data(), scap, &ns);
+      if (s && s != S615_E_OVERFLOW) {
+        std::fprintf(stderr, "[cls5-gpu] verify failed: %s\n", s615_strerror(s));
+        s615_close(ctx);
+        return 1;
+      }
+      for (size_t k = 0; k < std::min(ns, scap); ++k) {
+        const s615_solution& S = solv[k];
+        if (S.kind != 0) continue;
+        std::printf("SOLUTION cls=5 B=%llu u=%llu a1=%lld a2=%lld a3=%lld a4=%lld a5=%lld gcd=%lld %s\n",
+                    (unsigned long long)S.B, (unsigned long long)S.u, (long long)S.a[0],
+                    (long long)S.a[1], (long long)S.a[2], (long long)S.a[3], (long long)S.a[4],
+                    (long long)S.gcd, S.gcd == 1 ? "primitive" : "NON-PRIMITIVE");
+        ++sols;
+        if (stop_first) break;
+      }
+    }
+    const double sec = std::chrono::duration<double>(Clock::now() - t0).count();
+    if (!quiet || chunk_no % 2 == 0 || off + n >= units.size()) {
+      const double gate_pct = tot_calls ? 100.0 * (double)tot_gated / (double)tot_calls : 0.0;
+      std::fprintf(stderr, "[cls5-gpu] units=%zu/%zu calls=%llu probes=%llu gate=%.1f%% sols=%llu %.1fs\n",
+                   off + n, units.size(), tot_calls, tot_probes, gate_pct, sols, sec);
+    }
+    if (stop_first && sols) break;
+  }
+  if (dump) std::fclose(dump);
+  const double sec = std::chrono::duration<double>(Clock::now() - t0).count();
+  std::printf("---- done cls5-gpu: solutions=%llu units=%zu calls=%llu probes=%llu time=%.1fs ----\n",
+              sols, units.size(), tot_calls, tot_probes, sec);
+  s615_close(ctx);
+  return 0;
+}

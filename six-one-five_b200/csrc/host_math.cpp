@@ -1,0 +1,315 @@
+// host_math.cpp -- exact host arithmetic, residue rules and unit records.
+//
+// The unit rule and free-term residue classes restate
+// fourcore_classes_v3.hpp:68-219; unit packing restates pack_unit5
+// (fourcore_cls5_gpu_v4.cu:169-184) and adds the divisibility checks the
+// device row arithmetic relies on.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace s615 {
+
+// ------------------------------------------------------------ 192-bit words
+W3 pow6_w3(u64 x) {
+  const u128 x2 = (u128)x * x;
+  // x < 2^32 keeps x^2 < 2^64; for larger x compute in two steps.
+  if ((u64)(x2 >> 64) == 0) {
+    const u64 a = (u64)x2;
+    const u128 x4 = (u128)a * a;
+    const u128 lo = (u128)(u64)x4 * a;
+    const u128 hi = (u128)(u64)(x4 >> 64) * a;
+    W3 r;
+    r.l[0] = (u64)lo;
+    const u128 mid = (lo >> 64) + (u128)(u64)hi;
+    r.l[1] = (u64)mid;
+    r.l[2] = (u64)(hi >> 64) + (u64)(mid >> 64);
+    return r;
+  }
+  W3 r{{1, 0, 0}};
+  for (int i = 0; i < 6; ++i) r = mul_w3_u64(r, x);
+  return r;
+}
+
+bool sub_w3(W3& a, const W3& b) {
+  u64 br = 0;
+  for (int i = 0; i < 3; ++i) {
+    const u128 d = (u128)a.l[i] - b.l[i] - br;
+    a.l[i] = (u64)d;
+    br = (u64)(d >> 64) ? 1 : 0;
+  }
+  return br != 0;
+}
+void add_w3(W3& a, const W3& b) {
+  u128 c = 0;
+  for (int i = 0; i < 3; ++i) {
+    c += (u128)a.l[i] + b.l[i];
+    a.l[i] = (u64)c;
+    c >>= 64;
+  }
+}
+W3 mul_w3_u64(const W3& a, u64 m) {
+  W3 r;
+  u128 c = 0;
+  for (int i = 0; i < 3; ++i) {
+    c += (u128)a.l[i] * m;
+    r.l[i] = (u64)c;
+    c >>= 64;
+  }
+  return r;
+}
+bool zero_w3(const W3& a) { return (a.l[0] | a.l[1] | a.l[2]) == 0; }
+bool eq_w3(const W3& a, const W3& b) {
+  return a.l[0] == b.l[0] && a.l[1] == b.l[1] && a.l[2] == b.l[2];
+}
+u64 divmod_w3(W3& a, u64 m) {
+  u128 r = 0;
+  for (int i = 2; i >= 0; --i) {
+    const u128 cur = (r << 64) | a.l[i];
+    a.l[i] = (u64)(cur / m);
+    r = cur % m;
+  }
+  return (u64)r;
+}
+u128 pow6_u128(u64 x) { const u128 a = (u128)x * x; return a * a * a; }
+u128 inv_2adic_u128(u128 a) {
+  u128 x = a;                       // correct to 3 bits for odd a
+  for (int i = 0; i < 7; ++i) x *= (u128)2 - a * x;
+  return x;
+}
+
+// ------------------------------------------------------------ residue rules
+namespace {
+
+long long mod_pow6(long long b, long long m) {
+  long long r = 1;
+  b %= m; if (b < 0) b += m;
+  for (int i = 0; i < 6; ++i) r = (long long)((__int128)r * b % m);
+  return r;
+}
+long long mod_inv(long long a, long long m) {
+  long long g = m, x = 0, x1 = 1, aa = a % m;
+  if (aa < 0) aa += m;
+  long long b = aa;
+  // extended Euclid on (m, a)
+  long long r0 = m, r1 = b, s0 = 0, s1 = 1;
+  while (r1) {
+    const long long q = r0 / r1;
+    long long t = r0 - q * r1; r0 = r1; r1 = t;
+    t = s0 - q * s1; s0 = s1; s1 = t;
+  }
+  (void)g; (void)x; (void)x1;
+  s0 %= m; if (s0 < 0) s0 += m;
+  return s0;
+}
+long long crt_pair(long long r1, long long m1, long long r2, long long m2) {
+  // m1, m2 coprime
+  const long long inv = mod_inv(m1 % m2, m2);
+  long long t = ((r2 - r1) % m2 + m2) % m2;
+  t = (long long)((__int128)t * inv % m2);
+  return r1 + m1 * t;
+}
+
+constexpr long long kM2 = 64, kM3 = 729, kM7 = 117649;
+
+// Units a (coprime to the modulus) grouped by a^6 mod the modulus.
+struct RootTable {
+  std::vector<std::vector<u32>> by;
+  explicit RootTable(long long m) : by((size_t)m) {
+    for (long long a = 1; a < m; ++a)
+      if (std::gcd(a, m) == 1) by[(size_t)mod_pow6(a, m)].push_back((u32)a);
+  }
+};
+const RootTable& roots2() { static RootTable t(kM2); return t; }
+const RootTable& roots3() { static RootTable t(kM3); return t; }
+const RootTable& roots7() { static RootTable t(kM7); return t; }
+
+bool unit_ok(u64 u, int cls) {
+  switch (cls) {
+    case 1: return (u & 1) && std::gcd(u, (u64)42) == 1;
+    case 2: return (u & 1) && (u % 3 == 0) && (u % 9 != 0);
+    case 3: return !(u & 1) && std::gcd(u, (u64)21) == 1;
+    case 4: case 5: return (u % 6 == 0) && (u % 7 != 0);
+  }
+  return false;
+}
+
+}  // namespace
+
+// (14e)^6 = B^6 (mod 3^6): e in the roots of B^6 * 14^-6.
+std::vector<u32> e_residues(u64 B) {
+  const long long t = mod_pow6((long long)(B % kM3), kM3) * mod_inv(mod_pow6(14, kM3), kM3) % kM3;
+  return roots3().by[(size_t)t];
+}
+// (21d)^6 = B^6 - u^6 (mod 2^6).
+std::vector<u32> d_residues(u64 B, u64 u) {
+  long long rhs = (mod_pow6((long long)(B % kM2), kM2) - mod_pow6((long long)(u % kM2), kM2)) % kM2;
+  if (rhs < 0) rhs += kM2;
+  const long long t = rhs * mod_inv(mod_pow6(21, kM2), kM2) % kM2;
+  return roots2().by[(size_t)t];
+}
+
+// Stage-1 units for one B over the full band (0,1)*B.
+std::vector<u64> unit_candidates(u64 B, int cls) {
+  std::vector<u64> out;
+  if (B < 2 || cls < 1 || cls > 5) return out;
+  const long long b2 = mod_pow6((long long)(B % kM2), kM2);
+  const long long b3 = mod_pow6((long long)(B % kM3), kM3);
+  const long long b7 = mod_pow6((long long)(B % kM7), kM7);
+  std::vector<long long> seeds;
+  long long M = kM7;
+  const auto& s7 = roots7().by[(size_t)b7];
+  if (cls == 1) {
+    M = kM2 * kM3 * kM7;
+    for (u32 a : roots2().by[(size_t)b2])
+      for (u32 c : roots3().by[(size_t)b3]) {
+        const long long s23 = crt_pair(a, kM2, c, kM3);
+        for (u32 s : s7) seeds.push_back(crt_pair(s23, kM2 * kM3, s, kM7));
+      }
+  } else if (cls == 2) {
+    M = kM2 * kM7;
+    for (u32 a : roots2().by[(size_t)b2]) for (u32 s : s7) seeds.push_back(crt_pair(a, kM2, s, kM7));
+  } else if (cls == 3) {
+    M = kM3 * kM7;
+    for (u32 c : roots3().by[(size_t)b3]) for (u32 s : s7) seeds.push_back(crt_pair(c, kM3, s, kM7));
+  } else {
+    for (u32 s : s7) seeds.push_back(s);
+  }
+  const u64 lo = 1, hi = B - 1;
+  for (long long s : seeds) {
+    u64 u = (u64)(s % M);
+    if (u < lo) u += (lo - u + (u64)M - 1) / (u64)M * (u64)M;
+    for (; u <= hi; u += (u64)M) if (unit_ok(u, cls)) out.push_back(u);
+  }
+  std::sort(out.begin(), out.end());
+  out.erase(std::unique(out.begin(), out.end()), out.end());
+  return out;
+}
+
+// --------------------------------------------------------------- dev units
+namespace {
+constexpr u64 kMaxB = 40000000ULL;  // keeps d^3, (14e)^3 and V inside the device word sizes
+
+// base - (14 e0)^6 divisible by 21^6, and V(e0) = d0^6 (mod 64) for every d0:
+// then every grid point of the unit has 42^6 | R (the construction of the
+// residue classes guarantees it for Stage-1 units).
+bool divisible_grid(const W3& base, u32 e0, const u32* d0s, u32 nd) {
+  W3 R = base;
+  if (sub_w3(R, pow6_w3(14ULL * e0))) return true;  // row has no R>0 point
+  if (divmod_w3(R, kM21) != 0) return false;
+  for (u32 i = 0; i < nd; ++i) {
+    const u64 d0 = d0s[i];
+    const u64 d6m = ((d0 * d0 % 64) * (d0 * d0 % 64) % 64) * (d0 * d0 % 64) % 64;
+    if ((R.l[0] & 63) != d6m) return false;
+  }
+  return true;
+}
+}  // namespace
+
+int make_dev_unit(const s615_unit& in, u32 id, DevUnit5* out, bool* skip) {
+  std::memset(out, 0, sizeof *out);
+  *skip = false;
+  if (in.cls != 5) return S615_E_FORMAT;
+  W3 base;
+  if (in.kind == 0) {
+    const u64 B = in.B, u = in.u;
+    if (B < 2 || B > kMaxB || u == 0) return S615_E_FORMAT;
+    if (u >= B) { *skip = true; return S615_OK; }   // base <= 0: pack_unit5 drops it
+    base = pow6_w3(B);
+    sub_w3(base, pow6_w3(u));
+    const auto er = e_residues(B);
+    const auto dr = d_residues(B, u);
+    if (er.empty() || dr.empty()) { *skip = true; return S615_OK; }
+    out->B = B; out->u = u;
+    out->lim = (u32)((B - 1) / 42);
+    out->fmax1 = (u32)((B - 1) / 14);
+    out->fmax2 = (u32)((B - 1) / 21);
+    out->nres1 = (u32)std::min<size_t>(er.size(), 12);
+    out->nres2 = (u32)std::min<size_t>(dr.size(), 12);
+    for (u32 i = 0; i < out->nres1; ++i) out->res1[i] = er[i];
+    for (u32 i = 0; i < out->nres2; ++i) out->res2[i] = dr[i];
+    // With both residue classes non-empty, R = 0 (mod 2^6) holds by the d rule
+    // and R = 0 (mod 3^6) by the e rule once 3 | u; R = 0 (mod 7^6) needs
+    // u^6 = B^6 (mod 7^6).  Stage-1 units satisfy both (classes_v3.hpp:102-135).
+    if (u % 3 != 0 || mod_pow6((long long)(u % kM7), kM7) != mod_pow6((long long)(B % kM7), kM7))
+      return S615_E_FORMAT;
+    out->base_lo = base.l[0];
+    out->base_hi = base.l[1];
+    out->id = id;
+    return S615_OK;
+  } else if (in.kind == 1) {
+    base = W3{{in.base[0], in.base[1], in.base[2]}};
+    if (zero_w3(base) || (in.base[2] >> 22) != 0) return S615_E_FORMAT;  // base < 2^150
+    if ((u64)in.fmax1 * 14 > kMaxB || (u64)in.fmax2 * 21 > kMaxB) return S615_E_FORMAT;
+    out->B = in.B; out->u = in.u;
+    out->lim = in.lim;
+    out->fmax1 = in.fmax1; out->fmax2 = in.fmax2;
+    out->nres1 = 1; out->nres2 = 1;
+    out->res1[0] = in.res_e % kModE;
+    out->res2[0] = in.res_d % kModD;
+  } else {
+    return S615_E_FORMAT;
+  }
+  for (u32 i = 0; i < out->nres1; ++i)
+    if (!divisible_grid(base, out->res1[i], out->res2, out->nres2)) return S615_E_FORMAT;
+  out->base_lo = base.l[0];
+  out->base_hi = base.l[1];
+  out->id = id;
+  return S615_OK;
+}
+
+// ------------------------------------------------------------ gate patterns
+// Admissible T mod q: sums of two sixth powers mod q (the factors of the
+// reference's mod-504 and mod-247 bitmaps, fourcore_cls5_gpu_v4.cu:124-137).
+static std::vector<u8> pair_sums_mod(u32 q) {
+  std::vector<u8> ok(q, 0);
+  for (u32 i = 0; i < q; ++i)
+    for (u32 j = 0; j < q; ++j) ok[(mod_pow6(i, q) + mod_pow6(j, q)) % q] = 1;
+  return ok;
+}
+
+void gate_patterns(bool gated, u32 out[kPatWords]) {
+  for (int qi = 0; qi < 4; ++qi) {
+    const u32 q = (u32)kPatQ[qi];
+    const auto ok = pair_sums_mod(q);
+    // (V - x^6) mod q must lie in 64 * ok  (T = (V - x^6) / 64).
+    std::vector<u8> ok64(q, 0);
+    for (u32 t = 0; t < q; ++t) if (ok[t]) ok64[(64 * t) % q] = 1;
+    for (u32 a = 0; a < q; ++a)
+      for (u32 s = 0; s < q; ++s) {
+        u32 w = 0;
+        for (u32 i = 0; i < 32; ++i) {
+          const u32 x = (s + 64 * i) % q;
+          const u32 v = (u32)(((long long)a - mod_pow6(x, q)) % q + q) % q;
+          if (!gated || ok64[v]) w |= 1u << i;
+        }
+        out[kPatBase[qi] + a * q + s] = w;
+      }
+  }
+}
+
+// The reference's bitmaps equal the CRT product of the five factor sets.
+bool gate_product_matches() {
+  std::vector<u8> g504(504, 0), g247(247, 0);
+  for (int i = 0; i < 504; ++i) for (int j = i; j < 504; ++j) g504[(mod_pow6(i, 504) + mod_pow6(j, 504)) % 504] = 1;
+  for (int i = 0; i < 247; ++i) for (int j = i; j < 247; ++j) g247[(mod_pow6(i, 247) + mod_pow6(j, 247)) % 247] = 1;
+  const auto s8 = pair_sums_mod(8), s9 = pair_sums_mod(9), s7 = pair_sums_mod(7);
+  const auto s13 = pair_sums_mod(13), s19 = pair_sums_mod(19);
+  int c504 = 0, c247 = 0;
+  for (int t = 0; t < 504; ++t) {
+    c504 += g504[t];
+    if (g504[t] != (s8[t % 8] && s9[t % 9] && s7[t % 7])) return false;
+  }
+  for (int t = 0; t < 247; ++t) {
+    c247 += g247[t];
+    if (g247[t] != (s13[t % 13] && s19[t % 19])) return false;
+  }
+  // admissible T mod 8 must be exactly {0,1,2}: the kernel encodes it as 0x7
+  if (!(s8[0] && s8[1] && s8[2]) || s8[3] || s8[4] || s8[5] || s8[6] || s8[7]) return false;
+  return c504 == 27 && c247 == 50;
+}
+
+}  // namespace s615

@@ -1,0 +1,58 @@
+// s615_device.cuh -- device-side building blocks: table cell loads for the
+// three HBM layouts, the xor-filter membership test, exact 128-bit helpers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "engine.hpp"
+
+namespace s615 {
+
+// Read one r-bit cell.  WIDE layouts hold one cell per aligned word, so a
+// cell is one load from one 32-byte sector.  PACKED is the file layout:
+// cell i starts at bit i*r; it is assembled from at most two aligned 64-bit
+// words (the device buffer is padded so word w+1 always exists).
+__device__ __forceinline__ u64 load_cell(const TableView& t, u64 i) {
+  if (t.layout == S615_LAYOUT_WIDE) {
+    if (t.cell_bytes == 8) return __ldg(static_cast<const unsigned long long*>(t.cells) + i);
+    return (u64)__ldg(static_cast<const unsigned int*>(t.cells) + i);
+  }
+  const unsigned long long* p = static_cast<const unsigned long long*>(t.cells);
+  const u64 bit = i * (u64)t.r;
+  const u64 w = bit >> 6;
+  const u32 o = (u32)(bit & 63);
+  u64 v = __ldg(p + w) >> o;
+  if (o + t.r > 64) v |= (u64)__ldg(p + w + 1) << (64 - o);
+  return v & t.fpmask;
+}
+
+// xor_might_contain: h = mix64(key + seed), three cells, compare with the
+// low r bits of h.
+__device__ __forceinline__ bool might_contain(const TableView& t, u64 key) {
+  if (t.block == 0) return false;
+  const u64 h = mix64(key + t.seed);
+  u64 c[3];
+  cell_indices(h, t.block, t.recip, c);
+  const u64 a = load_cell(t, c[0]);
+  const u64 b = load_cell(t, c[1]);
+  const u64 d = load_cell(t, c[2]);
+  return (a ^ b ^ d) == (h & t.fpmask);
+}
+
+// x^6 for x < 2^21 (exact, < 2^126).
+__device__ __forceinline__ u128 pow6_small(u64 x) {
+  const u64 x3 = x * x * x;
+  return (u128)x3 * x3;
+}
+
+// floor(v^(1/6)) for 0 <= v < 2^120: double estimate, then exact fix-up.
+__device__ __forceinline__ u32 iroot6_u128(u128 v) {
+  if (v == 0) return 0;
+  const double x = (double)(u64)(v >> 64) * 18446744073709551616.0 + (double)(u64)v;
+  u64 r = (u64)cbrt(sqrt(x));
+  if (r > (1ULL << 20)) r = 1ULL << 20;
+  while (r > 0 && pow6_small(r) > v) --r;
+  while (pow6_small(r + 1) <= v) ++r;
+  return (u32)r;
+}
+
+}  // namespace s615

@@ -1,0 +1,167 @@
+// verify.cu -- exact re-derivation of the pair behind every filter hit.
+//
+// The reference expands a hit fingerprint into candidate pairs with
+// PairRecover (fourcore_xor_store.hpp:23-51: all i<=j<=N with i^6+j^6 = fp
+// mod 2^64), keeps a,b <= lim and then requires p6[a]+p6[b] == T exactly
+// (fourcore_cls5_gpu_v4.cu:513-523).  The surviving set is exactly
+// {(c1,c2): c1 <= c2 <= min(N,lim), c1^6 + c2^6 = T}, which this kernel
+// enumerates directly: one warp per hit, the c1 range [1, (T/2)^(1/6)] split
+// into 32 segments, each walked with the two-pointer rule (c1 up, c2 down).
+// The identity, term and gcd checks that follow are done on the host.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "s615_device.cuh"
+
+namespace s615 {
+
+namespace {
+
+struct PairOut { u32 hit, c1, c2, pad; };
+
+__global__ void k_verify(const DevUnit5* __restrict__ units, const s615_hit* __restrict__ hits,
+                         u32 n_hits, u32 N, u64 inv_lo, u64 inv_hi, PairOut* out, u32 cap,
+                         u32* n_out) {
+  const u32 lane = threadIdx.x & 31;
+  const u32 warps = (gridDim.x * blockDim.x) >> 5;
+  const u128 inv21 = ((u128)inv_hi << 64) | inv_lo;
+  for (u32 hi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; hi < n_hits; hi += warps) {
+    const s615_hit H = hits[hi];
+    const DevUnit5& U = units[H.unit];
+    const u128 base = ((u128)U.base_hi << 64) | U.base_lo;
+    const u64 x = 14ull * H.e;
+    const u128 x3 = (u128)(x * x) * x;
+    const u128 V = (base - x3 * x3) * inv21;
+    const u128 d6 = pow6_small(H.d);
+    if ((V >> 127) || V <= d6) continue;
+    const u128 diff = V - d6;
+    if ((u64)diff & 63) continue;
+    const u128 T = diff >> 6;
+    const u32 cmax = min(N, U.lim);
+    const u32 c1max = iroot6_u128(T >> 1);
+    if (c1max == 0) continue;
+    const u32 seg = (c1max + 31) / 32;
+    u32 c1 = 1 + lane * seg;
+    const u32 end = min(c1max, c1 + seg - 1);
+    if (c1 > c1max) continue;
+    u32 c2 = min(iroot6_u128(T - pow6_small(c1)), cmax);
+    while (c1 <= end && c2 >= c1) {
+      const u128 s = pow6_small(c1) + pow6_small(c2);
+      if (s == T) {
+        const u32 k = atomicAdd(n_out, 1u);
+        if (k < cap) out[k] = PairOut{hi, c1, c2, 0};
+        ++c1;
+        --c2;
+      } else if (s < T) {
+        ++c1;
+      } else {
+        --c2;
+      }
+    }
+  }
+}
+
+}  // namespace
+
+int verify_cls5_device(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s615_hit* hits,
+                       size_t n_hits, int N, s615_solution* out, size_t cap, size_t* n_out) {
+  *n_out = 0;
+  if (n_hits == 0) return S615_OK;
+  std::vector<DevUnit5> du(n_units);
+  for (size_t i = 0; i < n_units; ++i) {
+    bool skip = false;
+    const int s = make_dev_unit(units[i], (u32)i, &du[i], &skip);
+    if (s && !skip) std::memset(&du[i], 0, sizeof du[i]);
+  }
+  for (size_t i = 0; i < n_hits; ++i)
+    if (hits[i].unit >= n_units) return S615_E_ARG;
+  const u32 pcap = (u32)std::min<size_t>(std::max<size_t>(4 * n_hits + 64, 1024), 1u << 26);
+  void *d_u = nullptr, *d_h = nullptr, *d_p = nullptr, *d_n = nullptr;
+  const size_t bu = du.size() * sizeof(DevUnit5), bh = n_hits * sizeof(s615_hit);
+  const size_t bp = pcap * sizeof(PairOut);
+  int s = 0;
+  if ((s = dev_alloc(ctx, &d_u, bu))) return s;
+  if ((s = dev_alloc(ctx, &d_h, bh))) { dev_free(ctx, d_u, bu); return s; }
+  if ((s = dev_alloc(ctx, &d_p, bp))) { dev_free(ctx, d_u, bu); dev_free(ctx, d_h, bh); return s; }
+  if ((s = dev_alloc(ctx, &d_n, 16))) {
+    dev_free(ctx, d_u, bu); dev_free(ctx, d_h, bh); dev_free(ctx, d_p, bp);
+    return s;
+  }
+  auto cleanup = [&]() {
+    dev_free(ctx, d_u, bu); dev_free(ctx, d_h, bh); dev_free(ctx, d_p, bp); dev_free(ctx, d_n, 16);
+  };
+  cudaStream_t st = ctx->stream;
+  std::vector<PairOut> pairs;
+  u32 np = 0;
+  {
+    const u128 inv = inv_2adic_u128((u128)kM21);
+    cudaError_t e = cudaMemcpyAsync(d_u, du.data(), bu, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_h, hits, bh, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_n, 0, 16, st);
+    if (e == cudaSuccess) {
+      const u32 blocks = (u32)std::min<size_t>((n_hits + 7) / 8, (size_t)ctx->num_sms * 32);
+      k_verify<<<blocks, 256, 0, st>>>(static_cast<const DevUnit5*>(d_u),
+                                       static_cast<const s615_hit*>(d_h), (u32)n_hits, (u32)N,
+                                       (u64)inv, (u64)(inv >> 64), static_cast<PairOut*>(d_p), pcap,
+                                       static_cast<u32*>(d_n));
+      ctx->launches++;
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&np, d_n, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess && np > pcap) { cleanup(); return S615_E_OVERFLOW; }
+    if (e == cudaSuccess) {
+      pairs.resize(np);
+      if (np) e = cudaMemcpy(pairs.data(), d_p, np * sizeof(PairOut), cudaMemcpyDeviceToHost);
+    }
+    cleanup();
+    if (e != cudaSuccess) return cuda_status(e);
+  }
+  std::sort(pairs.begin(), pairs.end(), [&](const PairOut& a, const PairOut& b) {
+    const s615_hit &ha = hits[a.hit], &hb = hits[b.hit];
+    if (ha.unit != hb.unit) return ha.unit < hb.unit;
+    if (ha.e != hb.e) return ha.e < hb.e;
+    if (ha.d != hb.d) return ha.d < hb.d;
+    if (a.hit != b.hit) return a.hit < b.hit;
+    return a.c1 < b.c1;
+  });
+  size_t k = 0;
+  for (const PairOut& p : pairs) {
+    const s615_hit& H = hits[p.hit];
+    const s615_unit& U = units[H.unit];
+    // exact identity: target = u^6 + (21d)^6 + (14e)^6 + 42^6 (c1^6 + c2^6)
+    W3 rhs = pow6_w3(21ULL * H.d);
+    add_w3(rhs, pow6_w3(14ULL * H.e));
+    const u128 core = pow6_u128(p.c1) + pow6_u128(p.c2);
+    add_w3(rhs, mul_w3_u64(W3{{(u64)core, (u64)(core >> 64), 0}}, kM42));
+    s615_solution S{};
+    S.unit = H.unit; S.kind = U.kind; S.B = U.B; S.u = U.u;
+    S.d = H.d; S.e = H.e; S.c1 = p.c1; S.c2 = p.c2;
+    if (U.kind == 1) {
+      if (!eq_w3(rhs, W3{{U.base[0], U.base[1], U.base[2]}})) continue;
+    } else {
+      add_w3(rhs, pow6_w3(U.u));
+      if (!eq_w3(rhs, pow6_w3(U.B))) continue;
+      long long t[5] = {42LL * p.c1, 42LL * p.c2, 21LL * H.d, 14LL * H.e, (long long)U.u};
+      std::sort(t, t + 5);
+      bool bad = false;
+      for (int i = 0; i < 4; ++i) if (t[i] == t[i + 1]) bad = true;
+      if (bad || t[4] >= (long long)U.B) continue;
+      long long g = t[0];
+      for (int i = 1; i < 5; ++i) g = std::gcd(g, t[i]);
+      g = std::gcd(g, (long long)U.B);
+      for (int i = 0; i < 5; ++i) S.a[i] = t[i];
+      S.gcd = g;
+    }
+    if (k < cap) out[k] = S;
+    ++k;
+  }
+  *n_out = k;
+  return k > cap ? S615_E_OVERFLOW : S615_OK;
+}
+
+}  // namespace s615

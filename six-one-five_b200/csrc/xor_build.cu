@@ -1,0 +1,370 @@
+// xor_build.cu -- device construction of the 3-hash xor filter.
+//
+// Produces a table with the reference's header (n_keys, m_cells, mix_seed,
+// seed schedule: spike/ribbon/xor_filter.hpp:185-192,256-470 and
+// fourcore_xor_store.hpp:67-119) from the same key set, built on the GPU:
+//
+//  1. Key set.  Pair mode enumerates unordered pairs of the DISTINCT values
+//     of i^6 mod 2^64 (1<=i<=N); many i share a value (every multiple of 2048
+//     has i^6 = 0 mod 2^64), so this already removes most duplicate keys.
+//     Remaining duplicates are removed by an open-addressing hash set in HBM
+//     (the reference sorts + uniques).  The survivors are the unique keys.
+//  2. Incidence: setxor[c] ^= h and count[c]++ for the three cells of each key.
+//  3. Peel in rounds.  A cell with count 1 holds exactly one key; in round r
+//     every such key is claimed by the lowest of its count-1 cells (so a key
+//     is claimed once), recorded as round[c] = r, then removed from its other
+//     two cells.  The 2-core is unique, so peeling succeeds for exactly the
+//     seeds for which the reference's FIFO peel succeeds.
+//  4. Fill in reverse round order, in place: the claimed cell of a round-r key
+//     becomes fp(h) ^ cell(c1) ^ cell(c2).  Its other cells were never claimed
+//     in rounds <= r (a count-1 cell cannot hold a second unpeeled key), so
+//     they are final already and a round needs no ordering inside it.
+// Cells then hold exactly the reference's cell relation (FN = 0, same FPR);
+// which key owns which cell differs from the FIFO order, so bytes differ.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "s615_device.cuh"
+
+namespace s615 {
+
+namespace {
+
+constexpr u64 kEmpty = ~0ULL;
+
+int grid_for(s615_ctx* ctx, u64 n, int threads) {
+  const u64 want = (n + threads - 1) / threads;
+  const u64 cap = (u64)ctx->num_sms * 16;
+  return (int)(want < cap ? (want ? want : 1) : cap);
+}
+
+__device__ __forceinline__ void hset_insert(unsigned long long* table, u64 tmask, u64 key,
+                                            u32* has_empty_key) {
+  if (key == kEmpty) { *has_empty_key = 1; return; }
+  u64 pos = mix64(key ^ 0x5bd1e9955bd1e995ULL) & tmask;
+  for (u64 probe = 0; probe <= tmask; ++probe) {
+    const unsigned long long old = atomicCAS(table + pos, (unsigned long long)kEmpty,
+                                             (unsigned long long)key);
+    if (old == kEmpty || old == key) return;
+    pos = (pos + 1) & tmask;
+  }
+}
+
+// Pair keys u[a] + u[b], a <= b, one block-stride row per a.
+__global__ void k_insert_pairs(const u64* __restrict__ vals, u64 nv, unsigned long long* table,
+                               u64 tmask, u32 part_bits, u32 part, u32* has_empty_key) {
+  for (u64 a = blockIdx.x; a < nv; a += gridDim.x) {
+    const u64 va = vals[a];
+    for (u64 b = a + threadIdx.x; b < nv; b += blockDim.x) {
+      const u64 key = va + vals[b];
+      if (part_bits && (mix64(key) >> (64 - part_bits)) != part) continue;
+      hset_insert(table, tmask, key, has_empty_key);
+    }
+  }
+}
+
+__global__ void k_insert_keys(const u64* __restrict__ keys, u64 n, unsigned long long* table,
+                              u64 tmask, u32 part_bits, u32 part, u32* has_empty_key) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n;
+       i += (u64)gridDim.x * blockDim.x) {
+    const u64 key = keys[i];
+    if (part_bits && (mix64(key) >> (64 - part_bits)) != part) continue;
+    hset_insert(table, tmask, key, has_empty_key);
+  }
+}
+
+// Append occupied slots to out (order irrelevant).
+__global__ void k_compact(const unsigned long long* __restrict__ table, u64 tsize,
+                          u64* __restrict__ out, unsigned long long* n_out) {
+  const u32 lane = threadIdx.x & 31;
+  for (u64 i0 = blockIdx.x * (u64)blockDim.x; i0 < tsize; i0 += (u64)gridDim.x * blockDim.x) {
+    const u64 i = i0 + threadIdx.x;
+    const bool occ = i < tsize && table[i] != kEmpty;
+    const u32 ballot = __ballot_sync(0xFFFFFFFFu, occ);
+    unsigned long long base = 0;
+    if (lane == 0 && ballot) base = atomicAdd(n_out, (unsigned long long)__popc(ballot));
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if (occ) out[base + __popc(ballot & ((1u << lane) - 1u))] = table[i];
+  }
+}
+
+__device__ __forceinline__ u32 count_of(const u32* counts, u64 c) {
+  return (counts[c >> 2] >> (8 * (c & 3))) & 0xFFu;
+}
+
+__global__ void k_incidence(const u64* __restrict__ keys, u64 n, u64 seed, u64 block, u64 recip,
+                            unsigned long long* setxor, u32* counts, u32* overflow) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n;
+       i += (u64)gridDim.x * blockDim.x) {
+    const u64 h = mix64(keys[i] + seed);
+    u64 c[3];
+    cell_indices(h, block, recip, c);
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+      atomicXor(setxor + c[t], (unsigned long long)h);
+      const u32 sh = 8 * (u32)(c[t] & 3);
+      const u32 old = atomicAdd(counts + (c[t] >> 2), 1u << sh);
+      if (((old >> sh) & 0xFFu) == 0xFFu) *overflow = 1;
+    }
+  }
+}
+
+// Claim: a count-1 cell c claims its key iff no lower cell of that key has
+// count 1.  Counts are only read here, so the round sees one snapshot.
+__global__ void k_claim(const unsigned long long* __restrict__ setxor, const u32* __restrict__ counts,
+                        u16* __restrict__ round, u64 m, u64 block, u64 recip, u16 r,
+                        unsigned long long* n_claimed) {
+  const u32 lane = threadIdx.x & 31;
+  for (u64 c0 = blockIdx.x * (u64)blockDim.x; c0 < m; c0 += (u64)gridDim.x * blockDim.x) {
+    const u64 c = c0 + threadIdx.x;
+    bool claim = false;
+    if (c < m && count_of(counts, c) == 1) {
+      const u64 h = setxor[c];
+      u64 cs[3];
+      cell_indices(h, block, recip, cs);
+      claim = true;
+#pragma unroll
+      for (int t = 0; t < 3; ++t)
+        if (cs[t] < c && count_of(counts, cs[t]) == 1) claim = false;
+      if (claim) round[c] = r;
+    }
+    const u32 ballot = __ballot_sync(0xFFFFFFFFu, claim);
+    if (lane == 0 && ballot) atomicAdd(n_claimed, (unsigned long long)__popc(ballot));
+  }
+}
+
+// Apply the round's claims: remove each claimed key from its other cells and
+// clear the claimed cell's count (its setxor keeps the key's hash).
+__global__ void k_apply(unsigned long long* setxor, u32* counts, const u16* __restrict__ round,
+                        u64 m, u64 block, u64 recip, u16 r) {
+  for (u64 c = blockIdx.x * (u64)blockDim.x + threadIdx.x; c < m;
+       c += (u64)gridDim.x * blockDim.x) {
+    if (round[c] != r) continue;
+    const u64 h = setxor[c];
+    u64 cs[3];
+    cell_indices(h, block, recip, cs);
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+      if (cs[t] == c) continue;
+      atomicXor(setxor + cs[t], (unsigned long long)h);
+      atomicSub(counts + (cs[t] >> 2), 1u << (8 * (u32)(cs[t] & 3)));
+    }
+    atomicAnd(counts + (c >> 2), ~(0xFFu << (8 * (u32)(c & 3))));
+  }
+}
+
+// Reverse fill of one round, in place.
+__global__ void k_fill(unsigned long long* setxor, const u16* __restrict__ round, u64 m, u64 block,
+                       u64 recip, u16 r, u64 mask) {
+  for (u64 c = blockIdx.x * (u64)blockDim.x + threadIdx.x; c < m;
+       c += (u64)gridDim.x * blockDim.x) {
+    if (round[c] != r) continue;
+    const u64 h = setxor[c];
+    u64 cs[3];
+    cell_indices(h, block, recip, cs);
+    u64 v = h & mask;
+#pragma unroll
+    for (int t = 0; t < 3; ++t)
+      if (cs[t] != c) v ^= setxor[cs[t]];
+    setxor[c] = v & mask;
+  }
+}
+
+__global__ void k_narrow(const u64* __restrict__ in, u32* __restrict__ out, u64 m) {
+  for (u64 c = blockIdx.x * (u64)blockDim.x + threadIdx.x; c < m;
+       c += (u64)gridDim.x * blockDim.x)
+    out[c] = (u32)in[c];
+}
+
+struct Buf {
+  s615_ctx* ctx;
+  void* p = nullptr;
+  size_t n = 0;
+  explicit Buf(s615_ctx* c) : ctx(c) {}
+  int alloc(size_t bytes) { n = bytes; return dev_alloc(ctx, &p, bytes); }
+  void release() { if (p) dev_free(ctx, p, n); p = nullptr; n = 0; }
+  ~Buf() { release(); }
+};
+
+u64 pow2_at_least(u64 x) { u64 p = 1; while (p < x) p <<= 1; return p; }
+
+}  // namespace
+
+int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u64* d_keys,
+                     u64 n_keys, int r, const u64* seeds, int n_seeds, int N, int layout,
+                     DevTable* out) {
+  cudaStream_t st = ctx->stream;
+  const bool pairs = d_pair_vals != nullptr;
+  const u64 n_raw = pairs ? n_vals * (n_vals + 1) / 2 : n_keys;
+
+  // ---- 1. unique keys ----
+  Buf keys(ctx);
+  u64 n = 0;
+  {
+    int s = keys.alloc(std::max<u64>(n_raw, 1) * sizeof(u64));
+    if (s) return s;
+    // Hash set sized for load <= 1/2 per partition; partitions by the top bits
+    // of mix64(key) bound the table when HBM is short.
+    size_t free_b = 0, total_b = 0;
+    S615_CU(cudaMemGetInfo(&free_b, &total_b));
+    size_t avail = std::min(free_b, ctx->budget > ctx->used ? ctx->budget - ctx->used : (size_t)0);
+    if (avail > ((size_t)2 << 30)) avail -= (size_t)2 << 30;
+    u32 part_bits = 0;
+    u64 tsize = pow2_at_least(std::max<u64>(2 * n_raw, 1024));
+    while (tsize * sizeof(u64) > avail && part_bits < 8) {
+      ++part_bits;
+      tsize = pow2_at_least(std::max<u64>((2 * n_raw >> part_bits) + (n_raw >> (part_bits + 3)) + 1024, 1024));
+    }
+    Buf table(ctx), scratch(ctx);
+    s = table.alloc(tsize * sizeof(u64));
+    if (s) return s;
+    s = scratch.alloc(64);
+    if (s) return s;
+    u32* d_flag = static_cast<u32*>(scratch.p);
+    unsigned long long* d_n = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch.p) + 8);
+    S615_CU(cudaMemsetAsync(scratch.p, 0, 64, st));
+    for (u32 part = 0; part < (1u << part_bits); ++part) {
+      S615_CU(cudaMemsetAsync(table.p, 0xFF, tsize * sizeof(u64), st));
+      if (pairs) {
+        const int grid = (int)std::min<u64>(n_vals ? n_vals : 1, (u64)ctx->num_sms * 32);
+        k_insert_pairs<<<grid, 256, 0, st>>>(d_pair_vals, n_vals,
+                                             static_cast<unsigned long long*>(table.p), tsize - 1,
+                                             part_bits, part, d_flag);
+      } else {
+        k_insert_keys<<<grid_for(ctx, n_keys, 256), 256, 0, st>>>(
+            d_keys, n_keys, static_cast<unsigned long long*>(table.p), tsize - 1, part_bits, part,
+            d_flag);
+      }
+      ctx->launches++;
+      S615_CU(cudaGetLastError());
+      k_compact<<<grid_for(ctx, tsize, 256), 256, 0, st>>>(
+          static_cast<const unsigned long long*>(table.p), tsize, static_cast<u64*>(keys.p), d_n);
+      ctx->launches++;
+      S615_CU(cudaGetLastError());
+    }
+    u32 h_flag = 0;
+    unsigned long long h_n = 0;
+    S615_CU(cudaMemcpyAsync(&h_flag, d_flag, 4, cudaMemcpyDeviceToHost, st));
+    S615_CU(cudaMemcpyAsync(&h_n, d_n, 8, cudaMemcpyDeviceToHost, st));
+    S615_CU(cudaStreamSynchronize(st));
+    n = h_n;
+    if (h_flag) {
+      const u64 e = kEmpty;
+      S615_CU(cudaMemcpy(static_cast<u64*>(keys.p) + n, &e, 8, cudaMemcpyHostToDevice));
+      ++n;
+    }
+  }
+
+  std::memset(&out->hdr, 0, sizeof out->hdr);
+  out->hdr.magic = kMagic; out->hdr.version = kVersion; out->hdr.kind = 1;
+  out->hdr.r = (u32)r; out->hdr.N = (u32)(N > 0 ? N : 0);
+  out->hdr.shard_count = 1;
+  if (n == 0) {
+    out->hdr.mix_seed = seeds[0];
+    out->layout = S615_LAYOUT_WIDE; out->cell_bytes = 8;
+    out->d_cells = nullptr; out->bytes = 0;
+    return S615_OK;
+  }
+
+  // ---- 2-4. per seed: incidence, peel, fill ----
+  const u64 m = capacity_for(n);
+  const u64 block = m / 3, recip = mod_recip(block);
+  Buf setxor(ctx), counts(ctx), rounds(ctx), scratch(ctx);
+  int s = setxor.alloc(m * sizeof(u64));
+  if (s) return s;
+  if ((s = counts.alloc(((m + 3) / 4) * sizeof(u32)))) return s;
+  if ((s = rounds.alloc(m * sizeof(u16)))) return s;
+  if ((s = scratch.alloc(64))) return s;
+  u32* d_over = static_cast<u32*>(scratch.p);
+  unsigned long long* d_claimed = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch.p) + 8);
+  const int g = grid_for(ctx, m, 256);
+  bool built = false;
+  u64 used_seed = 0;
+  for (int si = 0; si < n_seeds && !built; ++si) {
+    const u64 seed = seeds[si];
+    S615_CU(cudaMemsetAsync(setxor.p, 0, m * sizeof(u64), st));
+    S615_CU(cudaMemsetAsync(counts.p, 0, ((m + 3) / 4) * sizeof(u32), st));
+    S615_CU(cudaMemsetAsync(rounds.p, 0, m * sizeof(u16), st));
+    S615_CU(cudaMemsetAsync(scratch.p, 0, 64, st));
+    k_incidence<<<grid_for(ctx, n, 256), 256, 0, st>>>(static_cast<const u64*>(keys.p), n, seed,
+                                                       block, recip,
+                                                       static_cast<unsigned long long*>(setxor.p),
+                                                       static_cast<u32*>(counts.p), d_over);
+    ctx->launches++;
+    S615_CU(cudaGetLastError());
+    u64 peeled = 0;
+    u16 rr = 0;
+    for (;;) {
+      if (rr == 0xFFFE) break;
+      ++rr;
+      S615_CU(cudaMemsetAsync(d_claimed, 0, 8, st));
+      k_claim<<<g, 256, 0, st>>>(static_cast<const unsigned long long*>(setxor.p),
+                                 static_cast<const u32*>(counts.p), static_cast<u16*>(rounds.p), m,
+                                 block, recip, rr, d_claimed);
+      ctx->launches++;
+      k_apply<<<g, 256, 0, st>>>(static_cast<unsigned long long*>(setxor.p),
+                                 static_cast<u32*>(counts.p), static_cast<const u16*>(rounds.p), m,
+                                 block, recip, rr);
+      ctx->launches++;
+      S615_CU(cudaGetLastError());
+      unsigned long long c = 0;
+      S615_CU(cudaMemcpyAsync(&c, d_claimed, 8, cudaMemcpyDeviceToHost, st));
+      S615_CU(cudaStreamSynchronize(st));
+      if (c == 0) { --rr; break; }
+      peeled += c;
+    }
+    u32 over = 0;
+    S615_CU(cudaMemcpy(&over, d_over, 4, cudaMemcpyDeviceToHost));
+    if (over) return S615_E_BUILD;
+    if (peeled != n) continue;   // 2-core not empty: next seed
+    const u64 mask = fp_mask((u32)r);
+    for (u16 q = rr; q >= 1; --q) {
+      k_fill<<<g, 256, 0, st>>>(static_cast<unsigned long long*>(setxor.p),
+                                static_cast<const u16*>(rounds.p), m, block, recip, q, mask);
+      ctx->launches++;
+    }
+    S615_CU(cudaGetLastError());
+    built = true;
+    used_seed = seed;
+  }
+  if (!built) return S615_E_BUILD;
+  keys.release(); counts.release(); rounds.release();
+
+  out->hdr.n_keys = n;
+  out->hdr.m_cells = m;
+  out->hdr.mix_seed = used_seed;
+  // ---- 5. final HBM layout ----
+  if (layout == S615_LAYOUT_PACKED) {
+    const u64 len = packed_bytes(m, (u32)r);
+    const size_t bytes = ((len + 7) / 8 + 1) * 8;
+    void* p = nullptr;
+    if ((s = dev_alloc(ctx, &p, bytes))) return s;
+    S615_CU(cudaMemsetAsync(p, 0, bytes, st));
+    if ((s = launch_pack(ctx, setxor.p, 8, m, (u32)r, static_cast<u8*>(p), len, st))) {
+      dev_free(ctx, p, bytes);
+      return s;
+    }
+    out->layout = S615_LAYOUT_PACKED; out->cell_bytes = 0;
+    out->d_cells = p; out->bytes = bytes;
+  } else if (r <= 32) {
+    void* p = nullptr;
+    const size_t bytes = m * sizeof(u32);
+    if ((s = dev_alloc(ctx, &p, bytes))) return s;
+    k_narrow<<<g, 256, 0, st>>>(static_cast<const u64*>(setxor.p), static_cast<u32*>(p), m);
+    ctx->launches++;
+    out->layout = S615_LAYOUT_WIDE; out->cell_bytes = 4;
+    out->d_cells = p; out->bytes = bytes;
+  } else {
+    out->layout = S615_LAYOUT_WIDE; out->cell_bytes = 8;
+    out->d_cells = setxor.p; out->bytes = setxor.n;
+    setxor.p = nullptr; setxor.n = 0;   // ownership moves to the table
+  }
+  S615_CU(cudaStreamSynchronize(st));
+  S615_CU(cudaGetLastError());
+  return S615_OK;
+}
+
+}  // namespace s615

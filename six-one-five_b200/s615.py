@@ -1,0 +1,273 @@
+"""ctypes binding of the engine's C ABI (include/s615.h).
+
+This is the Python-side view a user (or the tests and bench) gets of
+``lib/libs615.so``: the same entry points, the same structs, errors raised as
+:class:`S615Error` carrying the C status.  There is no fallback: if the
+library is missing or no GPU is present, calls that need the device fail.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Iterable, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libs615.so")
+
+S615_OK = 0
+STATUS = {
+    -1: "ARG", -2: "IO", -3: "FORMAT", -4: "N_MISMATCH", -5: "FPR_SMOKE", -6: "OOM",
+    -7: "DEVICE", -8: "TIMEOUT", -9: "OVERFLOW", -10: "BUILD", -11: "NOTABLE",
+}
+LAYOUT_AUTO, LAYOUT_PACKED, LAYOUT_WIDE = 0, 1, 2
+F_NO_GATE, F_PLAIN = 1, 2
+
+
+class S615Error(RuntimeError):
+    def __init__(self, status: int, what: str):
+        super().__init__(f"{what}: {STATUS.get(status, status)} ({status})")
+        self.status = status
+
+
+class Header(C.Structure):
+    _fields_ = [("magic", C.c_uint32), ("version", C.c_uint32), ("kind", C.c_uint32),
+                ("r", C.c_uint32), ("w", C.c_uint32), ("N", C.c_uint32),
+                ("n_keys", C.c_uint64), ("m_cells", C.c_uint64), ("mix_seed", C.c_uint64),
+                ("shard_count", C.c_uint32), ("shard_index", C.c_uint32),
+                ("shard_mode", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class TableInfo(C.Structure):
+    _fields_ = [("hdr", Header), ("layout", C.c_int), ("cell_bytes", C.c_int),
+                ("device_bytes", C.c_uint64)]
+
+
+class Unit(C.Structure):
+    _fields_ = [("cls", C.c_uint32), ("kind", C.c_uint32), ("B", C.c_uint64), ("u", C.c_uint64),
+                ("base", C.c_uint64 * 3), ("fmax1", C.c_uint32), ("fmax2", C.c_uint32),
+                ("res_e", C.c_uint32), ("res_d", C.c_uint32), ("lim", C.c_uint32),
+                ("pad", C.c_uint32)]
+
+
+class Hit(C.Structure):
+    _fields_ = [("unit", C.c_uint32), ("a", C.c_uint32), ("b", C.c_uint32), ("d", C.c_uint32),
+                ("e", C.c_uint32), ("fp", C.c_uint64)]
+
+
+class Counters(C.Structure):
+    _fields_ = [("calls", C.c_uint64), ("gated", C.c_uint64), ("probes", C.c_uint64),
+                ("pos", C.c_uint64), ("hits", C.c_uint64)]
+
+
+class Solution(C.Structure):
+    _fields_ = [("unit", C.c_uint32), ("kind", C.c_uint32), ("B", C.c_uint64), ("u", C.c_uint64),
+                ("d", C.c_uint32), ("e", C.c_uint32), ("c1", C.c_uint32), ("c2", C.c_uint32),
+                ("a", C.c_int64 * 5), ("gcd", C.c_int64)]
+
+
+assert C.sizeof(Header) == 64
+assert C.sizeof(Hit) == 32
+assert C.sizeof(Unit) == 72
+
+HIT_DTYPE = np.dtype([("unit", "<u4"), ("a", "<u4"), ("b", "<u4"), ("d", "<u4"), ("e", "<u4"),
+                      ("pad", "<u4"), ("fp", "<u8")])
+
+# Every entry point declared in include/s615.h, with its ctypes signature.
+_P = C.c_void_p
+SIGNATURES = {
+    "s615_strerror": (C.c_char_p, [C.c_int]),
+    "s615_open": (C.c_int, [C.c_int, C.c_size_t, C.POINTER(_P)]),
+    "s615_close": (C.c_int, [_P]),
+    "s615_launch_count": (C.c_uint64, [_P]),
+    "s615_load_table": (C.c_int, [_P, C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "s615_build_table": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "s615_build_table_keys": (C.c_int, [_P, _P, C.c_size_t, C.c_int, C.c_uint64, C.c_int,
+                                        C.POINTER(C.c_int)]),
+    "s615_save_table": (C.c_int, [_P, C.c_int, C.c_char_p]),
+    "s615_export_table": (C.c_int, [_P, C.c_int, C.POINTER(Header), _P, C.c_size_t,
+                                    C.POINTER(C.c_size_t)]),
+    "s615_get_table_info": (C.c_int, [_P, C.c_int, C.POINTER(TableInfo)]),
+    "s615_free_table": (C.c_int, [_P, C.c_int]),
+    "s615_xor_query": (C.c_int, [_P, C.c_int, _P, C.c_size_t, _P]),
+    "s615_xor_query_dev": (C.c_int, [_P, C.c_int, _P, C.c_size_t, _P, _P]),
+    "s615_mem_info": (C.c_int, [_P, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "s615_unit_candidates": (C.c_int, [C.c_uint64, C.c_int, _P, C.c_size_t,
+                                       C.POINTER(C.c_size_t)]),
+    "s615_unit_status": (C.c_int, [_P]),
+    "s615_cls5_run": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.c_uint, _P, C.c_size_t,
+                                C.POINTER(C.c_size_t), C.POINTER(Counters)]),
+    "s615_cls5_prepare": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(_P)]),
+    "s615_cls5_run_batch": (C.c_int, [_P, C.c_int, _P, C.c_uint, _P]),
+    "s615_cls5_batch_results": (C.c_int, [_P, _P, _P, C.c_size_t, C.POINTER(C.c_size_t),
+                                          C.POINTER(Counters)]),
+    "s615_cls5_batch_free": (C.c_int, [_P, _P]),
+    "s615_cls5_verify": (C.c_int, [_P, _P, C.c_size_t, _P, C.c_size_t, C.c_int, _P, C.c_size_t,
+                                   C.POINTER(C.c_size_t)]),
+    "s615_selftest_host": (C.c_int, []),
+}
+
+_lib: Optional[C.CDLL] = None
+
+
+def lib() -> C.CDLL:
+    """Load lib/libs615.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} missing: run `make -C six-one-five_b200`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(status: int, what: str) -> int:
+    if status != S615_OK:
+        raise S615Error(status, what)
+    return status
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+def unit_candidates(B: int, cls: int = 5) -> List[int]:
+    n = C.c_size_t(0)
+    buf = np.zeros(4096, dtype=np.uint64)
+    st = lib().s615_unit_candidates(B, cls, _ptr(buf), buf.size, C.byref(n))
+    if st not in (S615_OK, -9):
+        _check(st, "unit_candidates")
+    if n.value > buf.size:
+        buf = np.zeros(n.value, dtype=np.uint64)
+        _check(lib().s615_unit_candidates(B, cls, _ptr(buf), buf.size, C.byref(n)), "unit_candidates")
+    return [int(x) for x in buf[: n.value]]
+
+
+def make_units(pairs: Iterable[Tuple[int, int]]) -> "C.Array":
+    pairs = list(pairs)
+    arr = (Unit * max(len(pairs), 1))()
+    for i, (B, u) in enumerate(pairs):
+        arr[i].cls = 5
+        arr[i].kind = 0
+        arr[i].B = B
+        arr[i].u = u
+    return arr, len(pairs)
+
+
+def make_plant(base: int, e: int, d: int, lim: int, u: int = 0, B: int = 0) -> Unit:
+    """A planted unit: base given, single residue per axis, fmax = the planted value."""
+    x = Unit()
+    x.cls, x.kind, x.B, x.u = 5, 1, B, u
+    for i in range(3):
+        x.base[i] = (base >> (64 * i)) & (2**64 - 1)
+    x.fmax1, x.fmax2, x.res_e, x.res_d, x.lim = e, d, e % 729, d % 64, lim
+    return x
+
+
+def hits_to_array(hits, n: int) -> np.ndarray:
+    raw = np.frombuffer(C.string_at(C.addressof(hits), n * C.sizeof(Hit)), dtype=HIT_DTYPE)
+    return raw.copy()
+
+
+class Engine:
+    """One device context (s615_open ... s615_close)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        self._ctx = C.c_void_p()
+        _check(lib().s615_open(device, hbm_budget, C.byref(self._ctx)), "s615_open")
+
+    def close(self) -> None:
+        if self._ctx:
+            lib().s615_close(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def launches(self) -> int:
+        return int(lib().s615_launch_count(self._ctx))
+
+    # ---- tables ----
+    def load_table(self, path: str, expected_N: int = 0, layout: int = LAYOUT_AUTO) -> int:
+        tid = C.c_int(0)
+        _check(lib().s615_load_table(self._ctx, path.encode(), expected_N, layout, C.byref(tid)),
+               f"load_table {path}")
+        return tid.value
+
+    def build_table(self, N: int, r: int, layout: int = LAYOUT_AUTO) -> int:
+        tid = C.c_int(0)
+        _check(lib().s615_build_table(self._ctx, N, r, layout, C.byref(tid)), "build_table")
+        return tid.value
+
+    def build_table_keys(self, keys, r: int, base_seed: int = 0x615615615615615,
+                         layout: int = LAYOUT_AUTO) -> int:
+        k = np.ascontiguousarray(np.asarray(keys, dtype=np.uint64))
+        tid = C.c_int(0)
+        _check(lib().s615_build_table_keys(self._ctx, _ptr(k), k.size, r, base_seed, layout,
+                                           C.byref(tid)), "build_table_keys")
+        return tid.value
+
+    def save_table(self, tid: int, path: str) -> None:
+        _check(lib().s615_save_table(self._ctx, tid, path.encode()), "save_table")
+
+    def export_table(self, tid: int):
+        """(64 header bytes, packed cell bytes as uint8 ndarray)."""
+        hdr = Header()
+        n = C.c_size_t(0)
+        _check(lib().s615_export_table(self._ctx, tid, C.byref(hdr), None, 0, C.byref(n)),
+               "export_table")
+        buf = np.zeros(n.value, dtype=np.uint8)
+        _check(lib().s615_export_table(self._ctx, tid, C.byref(hdr), _ptr(buf), buf.size,
+                                       C.byref(n)), "export_table")
+        return bytes(hdr), buf
+
+    def table_info(self, tid: int) -> TableInfo:
+        info = TableInfo()
+        _check(lib().s615_get_table_info(self._ctx, tid, C.byref(info)), "table_info")
+        return info
+
+    def free_table(self, tid: int) -> None:
+        _check(lib().s615_free_table(self._ctx, tid), "free_table")
+
+    def query(self, tid: int, keys) -> np.ndarray:
+        k = np.ascontiguousarray(np.asarray(keys, dtype=np.uint64))
+        out = np.zeros(k.size, dtype=np.uint8)
+        _check(lib().s615_xor_query(self._ctx, tid, _ptr(k), k.size, _ptr(out)), "xor_query")
+        return out
+
+    # ---- cls5 ----
+    def cls5_run(self, tid: int, units, n: int, flags: int = 0, hit_cap: int = 1 << 20):
+        hits = (Hit * max(hit_cap, 1))()
+        nh = C.c_size_t(0)
+        ctr = Counters()
+        st = lib().s615_cls5_run(self._ctx, tid, C.cast(units, C.c_void_p), n, flags,
+                                 C.cast(hits, C.c_void_p), hit_cap, C.byref(nh), C.byref(ctr))
+        _check(st, "cls5_run")
+        return hits_to_array(hits, nh.value), ctr
+
+    def verify(self, units, n_units: int, hits: np.ndarray, N: int, cap: int = 4096):
+        h = np.ascontiguousarray(hits.astype(HIT_DTYPE))
+        out = (Solution * cap)()
+        no = C.c_size_t(0)
+        _check(lib().s615_cls5_verify(self._ctx, C.cast(units, C.c_void_p), n_units, _ptr(h),
+                                      h.size, N, C.cast(out, C.c_void_p), cap, C.byref(no)),
+               "cls5_verify")
+        return [out[i] for i in range(no.value)]
+
+
+def solution_line(s: Solution) -> str:
+    """The reference's SOLUTION line (fourcore_cls5_gpu_v4.cu:533-536)."""
+    if s.kind == 1:
+        return f"PLANT unit={s.unit} d={s.d} e={s.e} c1={s.c1} c2={s.c2}"
+    a = list(s.a)
+    return (f"SOLUTION cls=5 B={s.B} u={s.u} a1={a[0]} a2={a[1]} a3={a[2]} a4={a[3]} a5={a[4]} "
+            f"gcd={s.gcd} {'primitive' if s.gcd == 1 else 'NON-PRIMITIVE'}")

@@ -1,0 +1,72 @@
+"""Host-side checks of the engine library (no GPU calls)."""
+import ctypes as C
+import math
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import orc
+import s615
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "s615.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(s615_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = s615.lib()
+    names = declared_symbols()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(names) == set(s615.SIGNATURES), set(names) ^ set(s615.SIGNATURES)
+    out = subprocess.run(["nm", "-D", "--defined-only", s615.LIB_PATH], capture_output=True,
+                         text=True).stdout
+    exported = set(re.findall(r"\bT (s615_\w+)", out))
+    assert set(names) <= exported
+
+
+def test_struct_layouts_match_header():
+    assert C.sizeof(s615.Header) == 64
+    assert C.sizeof(s615.Hit) == 32      # reference Hit{u32 x5; u64 fp}
+    assert C.sizeof(s615.Unit) == 72
+    assert s615.HIT_DTYPE.itemsize == 32
+
+
+def test_host_selftest():
+    # pow6 KATs, gate = CRT product (27/504, 50/247), exact remainder, row identity
+    assert s615.lib().s615_selftest_host() == 0
+
+
+def test_unit_candidates_match_oracle():
+    rng = np.random.RandomState(3)
+    Bs = [100003, 2353975, 3200003] + [int(b) for b in rng.randint(1000, 5_000_000, size=60)]
+    for B in Bs:
+        if math.gcd(B, 42) != 1:
+            continue
+        for cls in (1, 2, 3, 4, 5):
+            assert s615.unit_candidates(B, cls) == orc.unit_candidates(B, cls), (B, cls)
+
+
+def test_open_without_gpu_fails_loudly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(s615.S615Error) as ei:
+        s615.Engine(0)
+    assert ei.value.status == -7
+
+
+def test_cli_built_and_selftest():
+    cli = os.path.join(ROOT, "six-one-five_b200", "bin", "s615_cls5")
+    assert os.path.exists(cli)
+    r = subprocess.run([cli, "--selftest-host"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "PASS" in r.stdout
