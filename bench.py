@@ -40,6 +40,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--band-width", type=int, default=BAND_W)
+    ap.add_argument("--band-lo", type=int, default=BAND_LO,
+                    help="first B of rank 0's band (a smaller band/table for profiling)")
+    ap.add_argument("--N", type=int, default=0, help="table N (default ceil(B_max/42))")
     ap.add_argument("--r", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -126,6 +129,10 @@ def profiled_traffic():
     return None
 
 
+def log(msg):
+    print(f"[bench] {msg}", file=sys.stderr, flush=True)
+
+
 def band_units(lo, hi):
     import workloads as W
     return W.cls5_units(lo, hi)
@@ -168,7 +175,7 @@ def run_reference(args, rank):
     if rank != 0:
         return 0
     import orc
-    lo, hi = BAND_LO, BAND_LO + args.band_width
+    lo, hi = args.band_lo, args.band_lo + args.band_width
     units = band_units(lo, hi)
     # the reference's host table builder needs hours and ~100 GB at N=76,667;
     # the reference arm probes a host-built N=2000 table (probes are ~1% of points)
@@ -212,14 +219,16 @@ def main():
     import workloads as W
 
     torch.cuda.set_device(local)
-    lo = BAND_LO + rank * args.band_width
+    lo = args.band_lo + rank * args.band_width
     hi = lo + args.band_width
-    N = math.ceil((BAND_LO + world * args.band_width) / 42)
+    N = args.N or math.ceil((args.band_lo + world * args.band_width) / 42)
     eng = s615.Engine(local)
     t0 = time.perf_counter()
     tid = eng.build_table(N, args.r)
     build_s = time.perf_counter() - t0
+    log(f"rank {rank}: table N={N} r={args.r} built in {build_s:.1f} s")
     units = band_units(lo, hi)
+    log(f"rank {rank}: {len(units)} units in [{lo}, {hi})")
     plants = W.plants(N_PLANTS, 1000 + rank, lo, hi, N)
     arr, n = W.unit_array(units, plants, N)
 
@@ -227,7 +236,9 @@ def main():
     batch = C.c_void_p()
     s615._check(lib.s615_cls5_prepare(eng._ctx, C.cast(arr, C.c_void_p), n, C.byref(batch)),
                 "prepare")
-    stream = torch.cuda.current_stream()
+    # a real stream handle: the engine launches on it and the events below are
+    # recorded on it (handle 0 would mean "the engine's own stream")
+    stream = torch.cuda.Stream()
     sptr = C.c_void_p(stream.cuda_stream)
 
     def step():
@@ -266,8 +277,13 @@ def main():
     s615._check(lib.s615_cls5_batch_results(eng._ctx, batch, C.cast(hits, C.c_void_p), 1 << 20,
                                             C.byref(nh), C.byref(ctr)), "results")
     harr = s615.hits_to_array(hits, nh.value)
+    log(f"timed {args.steps} steps: {total_ms:.1f} ms; pos={ctr.pos} probes={ctr.probes} hits={nh.value}")
     sols = eng.verify(arr, n, harr, N)
-    recovered = sum(1 for s in sols if s.kind == 1)
+    # a plant counts when its exact planted (d, e, c1, c2) is among the verified
+    # identities (an even d can add a second, equally valid identity 21d = 42c)
+    got = {(s.unit, s.d, s.e, s.c1, s.c2) for s in sols if s.kind == 1}
+    recovered = sum(1 for j, p in enumerate(plants)
+                    if (len(units) + j, p.d, p.e, p.c1, p.c2) in got)
     solutions = [s615.solution_line(s) for s in sols if s.kind == 0]
 
     pos_all = ctr.pos * world
@@ -282,6 +298,7 @@ def main():
     for _ in range(e2e_steps):
         h2, c2 = eng.cls5_run(tid, arr, n, hit_cap=1 << 16)
     e2e_s = (time.perf_counter() - t0) / e2e_steps
+    log(f"e2e through s615_cls5_run: {e2e_s * 1e3:.1f} ms per step (device step {total_ms / args.steps:.1f} ms)")
     assert c2.pos == ctr.pos and c2.probes == ctr.probes
     d2h = 40 + len(h2) * 32
 

@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <random>
@@ -420,7 +421,7 @@ int s615_unit_candidates(uint64_t B, int cls, uint64_t* out, size_t cap, size_t*
 
 // ------------------------------------------------------------- cls5 batches
 int s615_cls5_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch** out) {
-  if (!ctx || !out || (n && !units)) return S615_E_ARG;
+  if (!ctx || !out || (n && !units) || n > kMaxBatchUnits) return S615_E_ARG;
   cudaSetDevice(ctx->device);
   std::unique_ptr<s615_batch> b(new s615_batch());
   std::vector<DevUnit5> du;
@@ -431,7 +432,13 @@ int s615_cls5_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batc
     const int s = make_dev_unit(units[i], (u32)i, &d, &skip);
     if (s) return s;
     if (skip) continue;
-    for (u32 ie = 0; ie < d.nres1; ++ie) b->host_items.push_back(((u32)du.size() << 4) | ie);
+    for (u32 ie = 0; ie < d.nres1; ++ie) {
+      u32 jmin = 0, jend = 0;
+      e_rows(d.res1[ie], d.fmax1, &jmin, &jend);
+      const u32 rows = jend > jmin ? jend - jmin : 0;
+      for (u32 c = 0; c * kItemRows < rows; ++c)
+        b->host_items.push_back(make_item((u32)du.size(), ie, c));
+    }
     du.push_back(d);
   }
   b->n_units = du.size();
@@ -478,11 +485,11 @@ int s615_cls5_run_batch(s615_ctx* ctx, int id, s615_batch* b, unsigned flags, vo
   size_t i = 0;
   while (i < b->n_items) {
     size_t j = i;
-    while (j < b->n_items && (b->host_items[j] >> 4) == (b->host_items[i] >> 4)) ++j;
+    while (j < b->n_items && item_unit(b->host_items[j]) == item_unit(b->host_items[i])) ++j;
     one.d_items = b->d_items + i;
     one.n_items = j - i;
     S615_CU(cudaMemsetAsync(b->d_work, 0, 4, st));
-    int s = launch_cls5_sieve(ctx, tv, &one, flags, st, (int)(j - i));
+    int s = launch_cls5_sieve(ctx, tv, &one, flags, st, 0);
     if (s) return s;
     S615_CU(cudaStreamSynchronize(st));
     i = j;

@@ -17,12 +17,13 @@
 //    each factor is periodic in k.  A lane evaluates the gate for 32
 //    consecutive k at once as the AND of one row constant (mod 8) and four
 //    32-bit pattern words from shared memory (mod 9, 7, 13, 19).
-//  * Compaction before probing.  Gate survivors (~1.08%) go to a per-warp
-//    shared-memory ring; each full batch of 32 is probed by all 32 lanes
-//    together: three independent cell loads per lane in flight.
-//  * One persistent grid drains a device work queue of (unit, e-residue)
-//    items; within an item the warps pull (d-residue, 1024-k tile, 64-row
-//    block) tasks from a block-local counter.
+//  * Compaction before probing.  Gate survivors go to a per-warp ring in
+//    shared memory; each full batch of 32 is probed by all 32 lanes together
+//    (three independent L2-only cell loads per lane in flight).
+//  * Warps are independent workers: each pulls (unit, e residue, 64-row
+//    chunk) items from one device-wide queue, sets its rows up in its own
+//    slice of shared memory and sieves every d residue and k tile of them.
+//    Nothing waits at a block barrier, so a slow item delays only its warp.
 #include <cuda_runtime.h>
 
 #include "s615_device.cuh"
@@ -33,10 +34,9 @@ namespace {
 
 constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
-constexpr int kRowChunk = 512;   // e-rows set up per pass
-constexpr int kMaxD = 4;         // d residues sieved per pass
-constexpr int kRowBlock = 64;    // rows per task
-constexpr int kQ = 64;           // warp ring capacity (power of two)
+constexpr u32 kRows = kItemRows;  // e-rows per item (64)
+constexpr u32 kMaxD = 4;          // d residues per pass
+constexpr u32 kQ = 64;            // warp ring capacity (power of two)
 constexpr u32 kNoRow = 0xFFFFFFFFu;
 
 struct __align__(16) RowRec {
@@ -44,6 +44,14 @@ struct __align__(16) RowRec {
   u32 D;          // iroot6(V-1)
   u32 v512;       // V mod 512, or kNoRow when V <= 0 (no R>0 point)
   u16 off[4];     // pattern-table word offset per q for a = V mod q
+};
+
+struct WarpSmem {                 // one warp's private slice
+  RowRec rows[kRows];             // 2048 B
+  u16 K[kMaxD][kRows];            // in-row k limit per d residue (k < 2^16)
+  u8 M4[kMaxD][kRows];            // mod-8 admissibility of k = 0..3 (mod 4)
+  u32 ring[kQ];
+  u32 d0s[kMaxD];                 // d residues of the current pass
 };
 
 struct SieveParams {
@@ -61,10 +69,7 @@ struct SieveParams {
 };
 
 constexpr size_t kSmemPat = kPatWords * sizeof(u32);                // 2640
-constexpr size_t kSmemRows = kRowChunk * sizeof(RowRec);            // 16384
-constexpr size_t kSmemK = kMaxD * kRowChunk * sizeof(u32);          // 8192
-constexpr size_t kSmemQ = kWarps * kQ * sizeof(u32);                // 2048
-constexpr size_t kSmemTotal = kSmemPat + kSmemRows + 2 * kSmemK + kSmemQ;
+constexpr size_t kSmemTotal = kSmemPat + kWarps * sizeof(WarpSmem);
 
 __device__ __forceinline__ u32 lanemask_lt() {
   u32 m;
@@ -91,15 +96,17 @@ __device__ __forceinline__ u32 pow6_mod512(u32 x) {
   return (x3 * x3) & 511;
 }
 
-// Probe the first `cnt` entries of the warp ring (one per lane).
-__device__ __forceinline__ void probe_batch(const SieveParams& P, const u32* ring, u32 head,
-                                            u32 cnt, const RowRec* rows, u32 d0, u32 e0,
-                                            u32 jc, u32 unit_id, u32 lane) {
+// Ring entry: k (16 bits) | row (6 bits) << 16 | d-residue slot (2 bits) << 22.
+__device__ __forceinline__ u32 entry(u32 di, u32 r, u32 k) { return (di << 22) | (r << 16) | k; }
+
+// Probe the ring entries [head, head+cnt) (one per lane).
+__device__ __forceinline__ void probe_batch(const SieveParams& P, const WarpSmem& W, u32 head,
+                                            u32 cnt, u32 e0, u32 j0, u32 unit_id, u32 lane) {
   if (lane >= cnt) return;
-  const u32 ent = ring[(head + lane) & (kQ - 1)];
-  const u32 r = ent >> 16, k = ent & 0xFFFFu;
-  const RowRec& R = rows[r];
-  const u64 d = (u64)d0 + 64ull * k;
+  const u32 ent = W.ring[(head + lane) & (kQ - 1)];
+  const u32 k = ent & 0xFFFFu, r = (ent >> 16) & 63u, di = ent >> 22;
+  const RowRec& R = W.rows[r];
+  const u64 d = (u64)W.d0s[di] + 64ull * k;
   const u128 V = ((u128)R.vhi << 64) | R.vlo;
   const u128 diff = V - pow6_small(d);
   const u64 key = (u64)(diff >> 6);
@@ -109,139 +116,114 @@ __device__ __forceinline__ void probe_batch(const SieveParams& P, const u32* rin
       s615_hit h;
       h.unit = unit_id; h.a = 0; h.b = 0;
       h.d = (u32)d;
-      h.e = e0 + 729u * (jc + r);
+      h.e = e0 + 729u * (j0 + r);
       h.fp = key;
       P.hits[idx] = h;
     }
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_cls5_sieve(SieveParams P) {
+__global__ void __launch_bounds__(kThreads, 6) k_cls5_sieve(SieveParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   u32* s_pat = reinterpret_cast<u32*>(smem);
-  RowRec* s_rows = reinterpret_cast<RowRec*>(smem + kSmemPat);
-  u32* s_K = reinterpret_cast<u32*>(smem + kSmemPat + kSmemRows);
-  u32* s_M8 = s_K + kMaxD * kRowChunk;
-  u32* s_ring = s_M8 + kMaxD * kRowChunk;
-  __shared__ u32 s_item, s_task;
-  __shared__ unsigned long long s_acc[3];
-
   const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  u32* ring = s_ring + warp * kQ;
+  WarpSmem& W = reinterpret_cast<WarpSmem*>(smem + kSmemPat)[warp];
   for (u32 i = tid; i < (u32)kPatWords; i += kThreads) s_pat[i] = P.pat[i];
-  if (tid < 3) s_acc[tid] = 0;
+  __syncthreads();   // the only block barrier: pattern tables are shared
 
   const u128 inv21 = ((u128)P.inv21_hi << 64) | P.inv21_lo;
   u64 my_calls = 0, my_pos = 0, my_probes = 0;
 
   for (;;) {
-    __syncthreads();
-    if (tid == 0) s_item = atomicAdd(P.work, 1u);
-    __syncthreads();
-    const u32 it = s_item;
+    u32 it = 0;
+    if (lane == 0) it = atomicAdd(P.work, 1u);
+    it = __shfl_sync(0xFFFFFFFFu, it, 0);
     if (it >= P.n_items) break;
-    const u32 packed_item = P.items[it];
-    const DevUnit5* U = P.units + (packed_item >> 4);
-    const u32 ie = packed_item & 15u;
-    const u32 e0 = U->res1[ie];
-    const u32 fmax1 = U->fmax1, fmax2 = U->fmax2, nres2 = U->nres2, unit_id = U->id;
+    const u32 packed = P.items[it];
+    const DevUnit5* U = P.units + item_unit(packed);
+    const u32 e0 = U->res1[item_eres(packed)];
+    const u32 fmax2 = U->fmax2, nres2 = U->nres2, unit_id = U->id;
+    u32 jmin, jend;
+    e_rows(e0, U->fmax1, &jmin, &jend);
+    const u32 j0 = jmin + item_chunk(packed) * kRows;
+    const u32 nrows = min(kRows, jend - j0);
     const u128 base = ((u128)U->base_hi << 64) | U->base_lo;
-    const u32 jmin = (e0 == 0) ? 1u : 0u;
-    const u32 jend = (e0 <= fmax1) ? (fmax1 - e0) / 729u + 1u : 0u;
 
-    // calls: every in-range (e,d) of this e-residue (counted once per item).
-    if (tid == 0 && jend > jmin) {
-      u64 dcount = 0;
-      for (u32 di = 0; di < nres2; ++di) {
-        const u32 d0 = U->res2[di];
-        if (d0 <= fmax2) dcount += (fmax2 - d0) / 64u + 1u - (d0 == 0 ? 1u : 0u);
+    // ---- row set-up: V, D and the residues of V (two rows per lane) ----
+    for (u32 r = lane; r < nrows; r += 32) {
+      const u64 x = 14ull * ((u64)e0 + 729ull * (j0 + r));
+      const u128 x3 = (u128)(x * x) * x;           // (14e)^3 < 2^78
+      const u128 V = (base - x3 * x3) * inv21;    // exact mod 2^128
+      RowRec R;
+      R.vlo = (u64)V; R.vhi = (u64)(V >> 64);
+      if ((R.vhi >> 63) || V == 0) {
+        R.D = 0; R.v512 = kNoRow;
+        R.off[0] = R.off[1] = R.off[2] = R.off[3] = 0;
+      } else {
+        R.D = iroot6_u128(V - 1);
+        R.v512 = (u32)(R.vlo & 511u);
+        R.off[0] = (u16)(kPatB9 + 9 * mod_small<9>(R.vhi, R.vlo));
+        R.off[1] = (u16)(kPatB7 + 7 * mod_small<7>(R.vhi, R.vlo));
+        R.off[2] = (u16)(kPatB13 + 13 * mod_small<13>(R.vhi, R.vlo));
+        R.off[3] = (u16)(kPatB19 + 19 * mod_small<19>(R.vhi, R.vlo));
       }
-      my_calls += (u64)(jend - jmin) * dcount;
+      W.rows[r] = R;
     }
+    u32 head = 0, qlen = 0;
 
-    for (u32 jc = jmin; jc < jend; jc += kRowChunk) {
-      const u32 nrows = min((u32)kRowChunk, jend - jc);
-      // ---- row set-up: V, D, residues of V ----
-      for (u32 r = tid; r < nrows; r += kThreads) {
-        const u64 x = 14ull * ((u64)e0 + 729ull * (jc + r));
-        const u128 x3 = (u128)(x * x) * x;           // (14e)^3 < 2^78
-        const u128 V = (base - x3 * x3) * inv21;    // exact mod 2^128
-        RowRec R;
-        R.vlo = (u64)V; R.vhi = (u64)(V >> 64);
-        if ((R.vhi >> 63) || V == 0) {
-          R.D = 0; R.v512 = kNoRow;
-          R.off[0] = R.off[1] = R.off[2] = R.off[3] = 0;
-        } else {
-          R.D = iroot6_u128(V - 1);
-          R.v512 = (u32)(R.vlo & 511u);
-          R.off[0] = (u16)(kPatB9 + 9 * mod_small<9>(R.vhi, R.vlo));
-          R.off[1] = (u16)(kPatB7 + 7 * mod_small<7>(R.vhi, R.vlo));
-          R.off[2] = (u16)(kPatB13 + 13 * mod_small<13>(R.vhi, R.vlo));
-          R.off[3] = (u16)(kPatB19 + 19 * mod_small<19>(R.vhi, R.vlo));
-        }
-        s_rows[r] = R;
-      }
-      __syncthreads();
-
-      for (u32 dg = 0; dg < nres2; dg += kMaxD) {
-        const u32 nd = min((u32)kMaxD, nres2 - dg);
-        // ---- per (row, d residue): in-row limit and the mod-8 row mask ----
-        for (u32 idx = tid; idx < nd * nrows; idx += kThreads) {
-          const u32 di = idx / nrows, r = idx - di * nrows;
-          const u32 d0 = U->res2[dg + di];
-          const RowRec& R = s_rows[r];
-          const u32 kcap = (d0 <= fmax2) ? (fmax2 - d0) / 64u + 1u : 0u;
-          const u32 kpos = (R.v512 != kNoRow && R.D >= d0) ? (R.D - d0) / 64u + 1u : 0u;
-          const u32 kend = min(kcap, kpos);
-          const u32 kmin = (d0 == 0) ? 1u : 0u;
-          if (kend > kmin) my_pos += kend - kmin;
-          u32 m4 = 0;
-          if (R.v512 != kNoRow) {
+    for (u32 dg = 0; dg < nres2; dg += kMaxD) {
+      const u32 nd = min(kMaxD, nres2 - dg);
+      __syncwarp();
+      if (lane < kMaxD) W.d0s[lane] = lane < nd ? U->res2[dg + lane] : 0u;
+      __syncwarp();
+      // ---- per (row, d residue): in-row limit and the mod-8 row mask ----
+      u32 kmax = 0;
+      for (u32 idx = lane; idx < nd * kRows; idx += 32) {
+        const u32 di = idx / kRows, r = idx % kRows;
+        if (r >= nrows) continue;
+        const u32 d0 = W.d0s[di];
+        const RowRec& R = W.rows[r];
+        const u32 kcap = (d0 <= fmax2) ? (fmax2 - d0) / 64u + 1u : 0u;
+        const u32 kpos = (R.v512 != kNoRow && R.D >= d0) ? (R.D - d0) / 64u + 1u : 0u;
+        const u32 kend = min(kcap, kpos);
+        const u32 kmin = (d0 == 0) ? 1u : 0u;
+        if (kend > kmin) my_pos += kend - kmin;
+        if (r == 0) my_calls += (u64)nrows * (kcap > kmin ? kcap - kmin : 0u);
+        kmax = max(kmax, kend);
+        u32 m4 = 0;
+        if (R.v512 != kNoRow) {
 #pragma unroll
-            for (u32 i = 0; i < 4; ++i) {
-              const u32 t8 = ((R.v512 - pow6_mod512(d0 + 64u * i)) & 511u) >> 6;
-              m4 |= ((P.s8 >> t8) & 1u) << i;
-            }
+          for (u32 i = 0; i < 4; ++i) {
+            const u32 t8 = ((R.v512 - pow6_mod512(d0 + 64u * i)) & 511u) >> 6;
+            m4 |= ((P.s8 >> t8) & 1u) << i;
           }
-          s_K[di * kRowChunk + r] = kend;
-          s_M8[di * kRowChunk + r] = m4 * 0x11111111u;
         }
-        if (tid == 0) s_task = 0;
-        __syncthreads();
+        W.K[di][r] = (u16)kend;
+        W.M4[di][r] = (u8)m4;
+      }
+#pragma unroll
+      for (int o = 16; o; o >>= 1) kmax = max(kmax, __shfl_xor_sync(0xFFFFFFFFu, kmax, o));
+      __syncwarp();
 
-        // ---- sieve + probe: warps pull (d residue, k tile, row block) tasks ----
-        u32 kmax = 0;
-        for (u32 di = 0; di < nd; ++di) kmax = max(kmax, s_K[di * kRowChunk]);
-        const u32 ntiles = (kmax + 1023u) / 1024u;
-        const u32 nrb = (nrows + kRowBlock - 1) / kRowBlock;
-        const u32 ntasks = nd * ntiles * nrb;
-        for (;;) {
-          u32 t = 0;
-          if (lane == 0) t = atomicAdd(&s_task, 1u);
-          t = __shfl_sync(0xFFFFFFFFu, t, 0);
-          if (t >= ntasks) break;
-          const u32 di = t / (ntiles * nrb);
-          const u32 rem = t - di * ntiles * nrb;
-          const u32 wt = rem / nrb, rb = rem - wt * nrb;
-          const u32 d0 = U->res2[dg + di];
+      // ---- sieve: lanes cover 32 words (1024 k) of a tile, rows in order ----
+      const u32 ntiles = (kmax + 1023u) / 1024u;
+      for (u32 di = 0; di < nd; ++di) {
+        const u32 d0 = W.d0s[di];
+        const u32 lowmask0 = (d0 == 0) ? ~1u : ~0u;
+        for (u32 wt = 0; wt < ntiles; ++wt) {
           const u32 w = wt * 32u + lane;
           const u32 kbase = w * 32u;
-          // lane phases: d mod q at the first k of this lane's word
           const u64 dstart = (u64)d0 + 64ull * kbase;
           const u32 s9 = (u32)(dstart % 9), s7 = (u32)(dstart % 7);
           const u32 s13 = (u32)(dstart % 13), s19 = (u32)(dstart % 19);
-          const u32 lowmask = (kbase == 0 && d0 == 0) ? ~1u : ~0u;
-          const u32* Krow = s_K + di * kRowChunk;
-          const u32* Mrow = s_M8 + di * kRowChunk;
-          const u32 r1 = min(nrows, (rb + 1) * (u32)kRowBlock);
-          u32 head = 0, qlen = 0;
-          for (u32 r = rb * kRowBlock; r < r1; ++r) {
-            const u32 kend = Krow[r];
+          const u32 lowmask = (kbase == 0) ? lowmask0 : ~0u;
+          for (u32 r = 0; r < nrows; ++r) {
+            const u32 kend = W.K[di][r];
             if (kend <= wt * 1024u) break;
             u32 m = 0;
             if (kbase < kend) {
-              const uint2 offs = *reinterpret_cast<const uint2*>(&s_rows[r].off[0]);
-              m = Mrow[r] & s_pat[(offs.x & 0xFFFFu) + s9] & s_pat[(offs.x >> 16) + s7] &
+              const uint2 offs = *reinterpret_cast<const uint2*>(&W.rows[r].off[0]);
+              m = ((u32)W.M4[di][r] * 0x11111111u) & s_pat[(offs.x & 0xFFFFu) + s9] & s_pat[(offs.x >> 16) + s7] &
                   s_pat[(offs.y & 0xFFFFu) + s13] & s_pat[(offs.y >> 16) + s19];
               const u32 n = kend - kbase;
               if (n < 32u) m &= (1u << n) - 1u;
@@ -253,35 +235,40 @@ __global__ void __launch_bounds__(kThreads) k_cls5_sieve(SieveParams P) {
               const u32 bit = has ? (u32)(__ffs(m) - 1) : 0u;
               m &= m - 1u;
               const u32 ballot = __ballot_sync(0xFFFFFFFFu, has);
-              if (has) ring[(head + qlen + __popc(ballot & lanemask_lt())) & (kQ - 1)] = (r << 16) | (kbase + bit);
+              if (has)
+                W.ring[(head + qlen + __popc(ballot & lanemask_lt())) & (kQ - 1)] =
+                    entry(di, r, kbase + bit);
               qlen += __popc(ballot);
               if (qlen >= 32u) {
                 __syncwarp();
-                probe_batch(P, ring, head, 32u, s_rows, d0, e0, jc, unit_id, lane);
+                probe_batch(P, W, head, 32u, e0, j0, unit_id, lane);
                 __syncwarp();
                 head = (head + 32u) & (kQ - 1);
                 qlen -= 32u;
               }
             }
           }
-          __syncwarp();
-          probe_batch(P, ring, head, qlen, s_rows, d0, e0, jc, unit_id, lane);
-          __syncwarp();
         }
-        __syncthreads();
       }
+      __syncwarp();
+      probe_batch(P, W, head, qlen, e0, j0, unit_id, lane);   // drain before d0s change
+      head = 0;
+      qlen = 0;
+      __syncwarp();
     }
   }
 
-  // ---- counters: one atomic per block ----
-  atomicAdd(&s_acc[0], (unsigned long long)my_calls);
-  atomicAdd(&s_acc[1], (unsigned long long)my_pos);
-  atomicAdd(&s_acc[2], (unsigned long long)my_probes);
-  __syncthreads();
-  if (tid == 0) {
-    atomicAdd(&P.ctr->calls, s_acc[0]);
-    atomicAdd(&P.ctr->pos, s_acc[1]);
-    atomicAdd(&P.ctr->probes, s_acc[2]);
+  // ---- counters: warp reduce, one atomic per warp ----
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    my_calls += __shfl_xor_sync(0xFFFFFFFFu, my_calls, o);
+    my_pos += __shfl_xor_sync(0xFFFFFFFFu, my_pos, o);
+    my_probes += __shfl_xor_sync(0xFFFFFFFFu, my_probes, o);
+  }
+  if (lane == 0) {
+    atomicAdd(&P.ctr->calls, (unsigned long long)my_calls);
+    atomicAdd(&P.ctr->pos, (unsigned long long)my_pos);
+    atomicAdd(&P.ctr->probes, (unsigned long long)my_probes);
   }
 }
 
@@ -318,7 +305,8 @@ int launch_cls5_sieve(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigne
                                                           kSmemTotal));
     grid = ctx->num_sms * (per_sm > 0 ? per_sm : 1);
   }
-  if ((size_t)grid > b->n_items) grid = (int)b->n_items;
+  const size_t need = (b->n_items + kWarps - 1) / kWarps;
+  if ((size_t)grid > need) grid = (int)need;
   k_cls5_sieve<<<grid, kThreads, kSmemTotal, st>>>(P);
   ctx->launches++;
   S615_CU(cudaGetLastError());

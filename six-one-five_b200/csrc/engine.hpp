@@ -55,6 +55,20 @@ struct Cls5Counters {  // device accumulators (u64 atomics)
   unsigned long long calls, probes, pos, hits;
 };
 
+// Work items of the sieve: (unit, e residue, chunk of kItemRows e-rows),
+// packed as unit << 12 | e-residue index << 8 | chunk.
+constexpr u32 kItemRows = 64;
+constexpr u32 kMaxBatchUnits = 1u << 20;
+S615_HD u32 make_item(u32 unit, u32 ie, u32 chunk) { return (unit << 12) | (ie << 8) | chunk; }
+S615_HD u32 item_unit(u32 it) { return it >> 12; }
+S615_HD u32 item_eres(u32 it) { return (it >> 8) & 15u; }
+S615_HD u32 item_chunk(u32 it) { return it & 255u; }
+// e-rows of one residue: e = e0 + 729 j for j in [jmin, jend).
+S615_HD void e_rows(u32 e0, u32 fmax1, u32* jmin, u32* jend) {
+  *jmin = (e0 == 0) ? 1u : 0u;
+  *jend = (e0 <= fmax1) ? (fmax1 - e0) / 729u + 1u : 0u;
+}
+
 }  // namespace s615
 
 struct s615_batch {

@@ -11,17 +11,32 @@ namespace s615 {
 // cell is one load from one 32-byte sector.  PACKED is the file layout:
 // cell i starts at bit i*r; it is assembled from at most two aligned 64-bit
 // words (the device buffer is padded so word w+1 always exists).
+// Table reads are random and never reused: they skip L1 (.cg) and cap the
+// L2 miss fill at 64 bytes (.L2::64B).  Without the cap every miss fills a
+// 128-byte line from DRAM; random-access throughput is bound by the HBM
+// access rate either way, so the cap halves DRAM bytes at the same speed.
+__device__ __forceinline__ u64 ld_cell64(const unsigned long long* p) {
+  u64 v;
+  asm("ld.global.cg.L2::64B.u64 %0, [%1];" : "=l"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ u32 ld_cell32(const unsigned int* p) {
+  u32 v;
+  asm("ld.global.cg.L2::64B.u32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+
 __device__ __forceinline__ u64 load_cell(const TableView& t, u64 i) {
   if (t.layout == S615_LAYOUT_WIDE) {
-    if (t.cell_bytes == 8) return __ldg(static_cast<const unsigned long long*>(t.cells) + i);
-    return (u64)__ldg(static_cast<const unsigned int*>(t.cells) + i);
+    if (t.cell_bytes == 8) return ld_cell64(static_cast<const unsigned long long*>(t.cells) + i);
+    return (u64)ld_cell32(static_cast<const unsigned int*>(t.cells) + i);
   }
   const unsigned long long* p = static_cast<const unsigned long long*>(t.cells);
   const u64 bit = i * (u64)t.r;
   const u64 w = bit >> 6;
   const u32 o = (u32)(bit & 63);
-  u64 v = __ldg(p + w) >> o;
-  if (o + t.r > 64) v |= (u64)__ldg(p + w + 1) << (64 - o);
+  u64 v = ld_cell64(p + w) >> o;
+  if (o + t.r > 64) v |= ld_cell64(p + w + 1) << (64 - o);
   return v & t.fpmask;
 }
 

@@ -204,7 +204,8 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
   Buf keys(ctx);
   u64 n = 0;
   {
-    int s = keys.alloc(std::max<u64>(n_raw, 1) * sizeof(u64));
+    // +1: the all-ones key is kept out of the hash set and appended last
+    int s = keys.alloc((n_raw + 1) * sizeof(u64));
     if (s) return s;
     // Hash set sized for load <= 1/2 per partition; partitions by the top bits
     // of mix64(key) bound the table when HBM is short.
