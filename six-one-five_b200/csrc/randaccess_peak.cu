@@ -1,0 +1,73 @@
+// randaccess_peak.cu -- the B200's random 8-byte read rate, the ceiling of the
+// xor probe (three random cells per probe).
+//
+// Reads `iters` 8-byte words at hashed (uniform, always in-bounds) positions of
+// a 2 GiB buffer with several load forms and prints reads/s.  The result is the
+// denominator for the probe kernel's random-access roofline.
+//   bin/randaccess_peak            (run under ncu with dram__sectors_read.sum to
+//                                   see the bytes each form moves per read)
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+
+typedef unsigned long long u64;
+
+__device__ __forceinline__ u64 mix(u64 x) {
+  x ^= x >> 33; x *= 0xff51afd7ed558ccdULL;
+  x ^= x >> 33; x *= 0xc4ceb9fe1a85ec53ULL;
+  x ^= x >> 33;
+  return x;
+}
+
+template <int V>
+__global__ void k_random_reads(const u64* __restrict__ p, u64 n, u64 iters, u64* out) {
+  u64 acc = 0;
+  const u64 tid = blockIdx.x * (u64)blockDim.x + threadIdx.x, nt = (u64)gridDim.x * blockDim.x;
+  for (u64 i = tid; i < iters; i += nt) {
+    const u64 j = mix(i * 0x9E3779B97F4A7C15ULL + V) % n;
+    u64 v;
+    if (V == 0) v = __ldg(p + j);                                   // L1-allocating, read-only
+    else if (V == 1) v = __ldcg(p + j);                             // L2 only
+    else asm volatile("ld.global.cg.L2::64B.u64 %0, [%1];" : "=l"(v) : "l"(p + j));  // L2 only, 64 B fill
+    acc ^= v;
+  }
+  if (acc == 0x123456789ULL) out[0] = acc;
+}
+
+int main() {
+  const u64 n = (2ull << 30) / 8;
+  const u64 iters = 1ull << 27;
+  u64 *p = nullptr, *o = nullptr;
+  if (cudaMalloc(&p, n * 8) != cudaSuccess || cudaMalloc(&o, 8) != cudaSuccess) {
+    std::printf("alloc failed\n");
+    return 1;
+  }
+  cudaMemset(p, 1, n * 8);
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const char* names[3] = {"ld.global.nc (L1)", "ld.global.cg", "ld.global.cg.L2::64B"};
+  for (int v = 0; v < 3; ++v) {
+    auto launch = [&]() {
+      if (v == 0) k_random_reads<0><<<sms * 8, 256>>>(p, n, iters, o);
+      else if (v == 1) k_random_reads<1><<<sms * 8, 256>>>(p, n, iters, o);
+      else k_random_reads<2><<<sms * 8, 256>>>(p, n, iters, o);
+    };
+    launch();
+    cudaEventRecord(a);
+    launch();
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    std::printf("%-24s %.3f ms  %.3e random reads/s\n", names[v], ms, iters / (ms * 1e-3));
+  }
+  const cudaError_t e = cudaGetLastError();
+  std::printf("status: %s\n", cudaGetErrorString(e));
+  cudaFree(p);
+  cudaFree(o);
+  return e == cudaSuccess ? 0 : 1;
+}
