@@ -169,6 +169,23 @@ int s615_cls5_batch_results(s615_ctx* ctx, s615_batch* b, s615_hit* hits, size_t
                             size_t* n_hits, s615_counters* counters);
 int s615_cls5_batch_free(s615_ctx* ctx, s615_batch* b);
 
+/* No counterpart in the reference.  s615_cls5_run for callers that cannot
+ * allocate device memory when they search: their free HBM is owned by another
+ * allocator, cudaMalloc's latency and implicit device synchronisation are not
+ * acceptable on their thread, or their host forbids new device allocations.
+ * It allocates no device memory: unit records, work items, counters, the
+ * queue cursor and hits live in one fixed device array of the library
+ * (about 1.4 MB, held by every GPU that loads the library until exit).
+ * Limits: n <= 4096 units, <= 65536 work items (S615_E_ARG beyond either),
+ * <= 16384 raw hits (S615_E_OVERFLOW beyond, *n_hits = true count); flags may
+ * only hold S615_F_NO_GATE.  The first call on a device looks up the array's
+ * device address; make that first call before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU race; each call clears the
+ * counters and cursor it needs and waits for its own results. */
+int s615_cls5_run_noalloc(s615_ctx* ctx, int table_id, const s615_unit* units, size_t n,
+                          unsigned flags, s615_hit* hits, size_t hit_cap, size_t* n_hits,
+                          s615_counters* counters);
+
 /* ------------------------------------------------------------- verify */
 /* PairRecover + exact identity (fourcore_xor_store.hpp:23-51,
  * fourcore_cls5_gpu_v4.cu:513-542) on the device: every (c1<=c2<=min(N,lim))

@@ -98,6 +98,8 @@ SIGNATURES = {
     "s615_unit_status": (C.c_int, [_P]),
     "s615_cls5_run": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.c_uint, _P, C.c_size_t,
                                 C.POINTER(C.c_size_t), C.POINTER(Counters)]),
+    "s615_cls5_run_noalloc": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.c_uint, _P, C.c_size_t,
+                                        C.POINTER(C.c_size_t), C.POINTER(Counters)]),
     "s615_cls5_prepare": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(_P)]),
     "s615_cls5_run_batch": (C.c_int, [_P, C.c_int, _P, C.c_uint, _P]),
     "s615_cls5_batch_results": (C.c_int, [_P, _P, _P, C.c_size_t, C.POINTER(C.c_size_t),
