@@ -234,7 +234,7 @@ def main():
 
     lib = s615.lib()
     batch = C.c_void_p()
-    s615._check(lib.s615_cls5_prepare(eng._ctx, C.cast(arr, C.c_void_p), n, C.byref(batch)),
+    s615._check(lib.s615_prepare(eng._ctx, C.cast(arr, C.c_void_p), n, C.byref(batch)),
                 "prepare")
     # a real stream handle: the engine launches on it and the events below are
     # recorded on it (handle 0 would mean "the engine's own stream")
@@ -242,7 +242,7 @@ def main():
     sptr = C.c_void_p(stream.cuda_stream)
 
     def step():
-        s615._check(lib.s615_cls5_run_batch(eng._ctx, tid, batch, 0, sptr), "run_batch")
+        s615._check(lib.s615_run_batch(eng._ctx, tid, batch, 0, sptr), "run_batch")
 
     for _ in range(args.warmup):
         step()
@@ -274,7 +274,7 @@ def main():
     hits = (s615.Hit * (1 << 20))()
     nh = C.c_size_t(0)
     ctr = s615.Counters()
-    s615._check(lib.s615_cls5_batch_results(eng._ctx, batch, C.cast(hits, C.c_void_p), 1 << 20,
+    s615._check(lib.s615_batch_results(eng._ctx, batch, C.cast(hits, C.c_void_p), 1 << 20,
                                             C.byref(nh), C.byref(ctr)), "results")
     harr = s615.hits_to_array(hits, nh.value)
     log(f"timed {args.steps} steps: {total_ms:.1f} ms; pos={ctr.pos} probes={ctr.probes} hits={nh.value}")
@@ -357,7 +357,7 @@ def main():
         "plain_form": plain,
         "clocks": cl,
     }
-    s615._check(lib.s615_cls5_batch_free(eng._ctx, batch), "batch_free")
+    s615._check(lib.s615_batch_free(eng._ctx, batch), "batch_free")
     eng.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

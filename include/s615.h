@@ -63,13 +63,17 @@ typedef struct s615_table_info {
   uint64_t device_bytes;  /* HBM held by the table */
 } s615_table_info;
 
-/* Unit record.  kind 0: a Stage-1 unit (B,u); the engine derives everything
- * like pack_unit5 (fourcore_cls5_gpu_v4.cu:169-184).  kind 1: a planted
- * target: base (= target - u^6, 3 LE limbs) is taken as given, with one e
- * residue res_e <= fmax1 grid and one d residue res_d <= fmax2 grid (the
- * reference's plant shape, solve_516_v3.cu:1149-1170). */
+/* Unit record.  cls 5: the 2-D (e,d) peel; cls 2, 3, 4: one free term d
+ * (x14, x21, x7) and the find3 leaf over c3 (fourcore_find_v4.cu:165-205).
+ * kind 0: a Stage-1 unit (B,u); the engine derives everything like
+ * pack_unit5 (fourcore_cls5_gpu_v4.cu:169-184) / free_d_cls234
+ * (fourcore_classes_v3.hpp:188-209).  kind 1: a planted target: base
+ * (= target - u^6, 3 LE limbs) is taken as given with a single residue per
+ * axis and fmax equal to the planted value (the reference's plant shape,
+ * solve_516_v3.cu:1130-1170): cls 5 uses res_e/fmax1 and res_d/fmax2;
+ * cls 2-4 use res_d/fmax1. */
 typedef struct s615_unit {
-  uint32_t cls;      /* 5 */
+  uint32_t cls;      /* 2, 3, 4 or 5 */
   uint32_t kind;     /* 0 = (B,u), 1 = planted base */
   uint64_t B, u;
   uint64_t base[3];  /* kind 1 only */
@@ -78,7 +82,10 @@ typedef struct s615_unit {
 } s615_unit;
 
 /* Raw filter hit, same layout as the reference's Hit{unit,a,b,d,e,fp}
- * (fourcore_cls5_gpu_v4.cu:140); a=b=0, unit = index into the unit array. */
+ * (fourcore_cls5_gpu_v4.cu:140); a=b=0, unit = index into the unit array.
+ * cls 5: d is the x21 term and e the x14 term.  cls 2-4: d is the free term
+ * and e carries c3 (the reference's find3 Hit puts c3 in its third field,
+ * fourcore_find_device.cuh:70-77). */
 typedef struct s615_hit {
   uint32_t unit, a, b, d, e;
   uint64_t fp;
@@ -91,11 +98,14 @@ typedef struct s615_counters {
   uint64_t calls, gated, probes, pos, hits;
 } s615_counters;
 
-/* A verified identity B^6 = u^6+(21d)^6+(14e)^6+42^6(c1^6+c2^6) with sorted
- * distinct terms a[0..4] < B (the SOLUTION line of fourcore_cls5_gpu_v4.cu:
- * 524-536), or a recovered plant (kind 1, a[] unused). */
+/* A verified identity with sorted distinct terms a[0..4] < B and their gcd
+ * with B (the SOLUTION line of fourcore_cls5_gpu_v4.cu:524-536 and
+ * fourcore_find_v4.cu:427-457), or a recovered plant (kind 1, a[] unused):
+ *   cls 5  : B^6 = u^6 + (21d)^6 + (14e)^6 + 42^6 (c1^6 + c2^6)
+ *   cls 2-4: B^6 = u^6 + (f d)^6 + 42^6 (c1^6 + c2^6 + c3^6), f = 14, 21, 7
+ * (for plants the left side is base + u^6). */
 typedef struct s615_solution {
-  uint32_t unit, kind;
+  uint32_t unit, kind, cls, c3;
   uint64_t B, u;
   uint32_t d, e, c1, c2;
   int64_t a[5];
@@ -149,25 +159,33 @@ int s615_unit_candidates(uint64_t B, int cls, uint64_t* out, size_t cap, size_t*
  * whose grid points are not all divisible by 42^6). */
 int s615_unit_status(const s615_unit* unit);
 
-/* ----------------------------------------------------------- cls5 peel */
+/* ---------------------------------------------------------- free peels */
 #define S615_F_NO_GATE 1u     /* --no-gate: probe every R>0 point */
 #define S615_F_PLAIN 2u       /* one unit per launch + sync (the plain form) */
 
+/* The peel of a mixed batch of units (classes 2-5) in one persistent launch:
+ * run_cls5_gpu's chunk loop (fourcore_cls5_gpu_v4.cu:472-512) for cls 5 and
+ * run_batch mode 3 (fourcore_find_v4.cu:460-513) for cls 2-4, without the
+ * verify step.  Host units in, raw hits + counters out (hits unordered).
+ * Returns S615_E_OVERFLOW (*n_hits = the true count) when hit_cap is too
+ * small; at most 2^24 units per call. */
+int s615_run(s615_ctx* ctx, int table_id, const s615_unit* units, size_t n, unsigned flags,
+             s615_hit* hits, size_t hit_cap, size_t* n_hits, s615_counters* counters);
 /* run_cls5_gpu (fourcore_cls5_gpu_v4.cu:412-563) without the verify step:
- * host units in, raw hits + counters out.  Hits are unordered.  Returns
- * S615_E_OVERFLOW (with *n_hits = the true count) when hit_cap is too small. */
+ * s615_run restricted to class-5 units (S615_E_FORMAT for any other). */
 int s615_cls5_run(s615_ctx* ctx, int table_id, const s615_unit* units, size_t n,
                   unsigned flags, s615_hit* hits, size_t hit_cap, size_t* n_hits,
                   s615_counters* counters);
-/* Device-resident form: d_units is the packed device record array produced
- * by s615_cls5_prepare; results stay on the device. */
+/* Device-resident form: the units are packed and uploaded once
+ * (s615_prepare); each s615_run_batch is one launch on the caller's stream
+ * (NULL = the context's stream); results stay on the device until
+ * s615_batch_results. */
 typedef struct s615_batch s615_batch;
-int s615_cls5_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch** out);
-int s615_cls5_run_batch(s615_ctx* ctx, int table_id, s615_batch* b, unsigned flags,
-                        void* stream);
-int s615_cls5_batch_results(s615_ctx* ctx, s615_batch* b, s615_hit* hits, size_t hit_cap,
-                            size_t* n_hits, s615_counters* counters);
-int s615_cls5_batch_free(s615_ctx* ctx, s615_batch* b);
+int s615_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch** out);
+int s615_run_batch(s615_ctx* ctx, int table_id, s615_batch* b, unsigned flags, void* stream);
+int s615_batch_results(s615_ctx* ctx, s615_batch* b, s615_hit* hits, size_t hit_cap,
+                       size_t* n_hits, s615_counters* counters);
+int s615_batch_free(s615_ctx* ctx, s615_batch* b);
 
 /* No counterpart in the reference.  s615_cls5_run for callers that cannot
  * allocate device memory when they search: their free HBM is owned by another
@@ -175,7 +193,7 @@ int s615_cls5_batch_free(s615_ctx* ctx, s615_batch* b);
  * acceptable on their thread, or their host forbids new device allocations.
  * It allocates no device memory: unit records, work items, counters, the
  * queue cursor and hits live in one fixed device array of the library
- * (about 1.4 MB, held by every GPU that loads the library until exit).
+ * (about 1.9 MB, held by every GPU that loads the library until exit).
  * Limits: n <= 4096 units, <= 65536 work items (S615_E_ARG beyond either),
  * <= 16384 raw hits (S615_E_OVERFLOW beyond, *n_hits = true count); flags may
  * only hold S615_F_NO_GATE.  The first call on a device looks up the array's
@@ -187,9 +205,15 @@ int s615_cls5_run_noalloc(s615_ctx* ctx, int table_id, const s615_unit* units, s
                           s615_counters* counters);
 
 /* ------------------------------------------------------------- verify */
-/* PairRecover + exact identity (fourcore_xor_store.hpp:23-51,
- * fourcore_cls5_gpu_v4.cu:513-542) on the device: every (c1<=c2<=min(N,lim))
- * with c1^6+c2^6 = T for each hit, then the identity and term checks. */
+/* PairRecover + exact identity on the device for hits of any class
+ * (fourcore_xor_store.hpp:23-51; fourcore_cls5_gpu_v4.cu:513-542;
+ * fourcore_find_v4.cu:516-560): every pair c1 <= c2 with c1^6 + c2^6 equal to
+ * the hit's exact remainder (cls 5: T, c2 <= min(N, lim); cls 2-4: T - c3^6,
+ * c2 <= min(N, c3)), then the identity, distinct-term, < B and gcd checks.
+ * Solutions come sorted by (unit, e, d, c1). */
+int s615_verify(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s615_hit* hits,
+                size_t n_hits, int N, s615_solution* out, size_t cap, size_t* n_out);
+/* s615_verify restricted to class-5 units (S615_E_FORMAT for any other). */
 int s615_cls5_verify(s615_ctx* ctx, const s615_unit* units, size_t n_units,
                      const s615_hit* hits, size_t n_hits, int N, s615_solution* out,
                      size_t cap, size_t* n_out);

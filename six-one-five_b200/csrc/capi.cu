@@ -150,17 +150,17 @@ int s615_open(int device, size_t hbm_budget, s615_ctx** out) {
   size_t free_b = 0, total_b = 0;
   S615_CU(cudaMemGetInfo(&free_b, &total_b));
   ctx->budget = hbm_budget ? hbm_budget : total_b;
-  u32 pat[kPatWords];
+  // gate pattern sets: [gate cls5 | open cls5 | gate find3 | open find3]
+  std::vector<u32> pat(4 * kPatWords);
+  gate_patterns(true, 0, pat.data());
+  gate_patterns(false, 0, pat.data() + kPatWords);
+  gate_patterns(true, 1, pat.data() + 2 * kPatWords);
+  gate_patterns(false, 1, pat.data() + 3 * kPatWords);
   void* p = nullptr;
-  int s = dev_alloc(ctx.get(), &p, sizeof pat);
+  const int s = dev_alloc(ctx.get(), &p, pat.size() * sizeof(u32));
   if (s) return s;
-  ctx->d_pat_gate = static_cast<u32*>(p);
-  gate_patterns(true, pat);
-  S615_CU(cudaMemcpy(ctx->d_pat_gate, pat, sizeof pat, cudaMemcpyHostToDevice));
-  if ((s = dev_alloc(ctx.get(), &p, sizeof pat))) return s;
-  ctx->d_pat_open = static_cast<u32*>(p);
-  gate_patterns(false, pat);
-  S615_CU(cudaMemcpy(ctx->d_pat_open, pat, sizeof pat, cudaMemcpyHostToDevice));
+  ctx->d_pat = static_cast<u32*>(p);
+  S615_CU(cudaMemcpy(ctx->d_pat, pat.data(), pat.size() * sizeof(u32), cudaMemcpyHostToDevice));
   *out = ctx.release();
   return S615_OK;
 }
@@ -170,8 +170,7 @@ int s615_close(s615_ctx* ctx) {
   cudaSetDevice(ctx->device);
   for (auto& kv : ctx->tables) free_table(ctx, kv.second);
   ctx->tables.clear();
-  dev_free(ctx, ctx->d_pat_gate, kPatWords * 4);
-  dev_free(ctx, ctx->d_pat_open, kPatWords * 4);
+  dev_free(ctx, ctx->d_pat, 4 * kPatWords * sizeof(u32));
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return S615_OK;
@@ -404,7 +403,7 @@ int s615_mem_info(s615_ctx* ctx, size_t* free_b, size_t* total_b) {
 
 int s615_unit_status(const s615_unit* unit) {
   if (!unit) return S615_E_ARG;
-  DevUnit5 d;
+  DevUnit d;
   bool skip = false;
   const int s = make_dev_unit(*unit, 0, &d, &skip);
   if (s) return s;
@@ -419,66 +418,68 @@ int s615_unit_candidates(uint64_t B, int cls, uint64_t* out, size_t cap, size_t*
   return v.size() > cap ? S615_E_OVERFLOW : S615_OK;
 }
 
-// ------------------------------------------------------------- cls5 batches
-int s615_cls5_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch** out) {
+// ---------------------------------------------------------- peel batches
+int s615_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch** out) {
   if (!ctx || !out || (n && !units) || n > kMaxBatchUnits) return S615_E_ARG;
   cudaSetDevice(ctx->device);
   std::unique_ptr<s615_batch> b(new s615_batch());
-  std::vector<DevUnit5> du;
+  std::vector<DevUnit> du;
   du.reserve(n);
   for (size_t i = 0; i < n; ++i) {
-    DevUnit5 d;
+    DevUnit d;
     bool skip = false;
     const int s = make_dev_unit(units[i], (u32)i, &d, &skip);
     if (s) return s;
     if (skip) continue;
-    for (u32 ie = 0; ie < d.nres1; ++ie) {
-      u32 jmin = 0, jend = 0;
-      e_rows(d.res1[ie], d.fmax1, &jmin, &jend);
-      const u32 rows = jend > jmin ? jend - jmin : 0;
-      for (u32 c = 0; c * kItemRows < rows; ++c)
-        b->host_items.push_back(make_item((u32)du.size(), ie, c));
-    }
+    unit_items(d, (u32)du.size(), b->host_items);
     du.push_back(d);
   }
   b->n_units = du.size();
   b->n_items = b->host_items.size();
   int s = 0;
   void* p = nullptr;
-  if ((s = dev_alloc(ctx, &p, std::max<size_t>(du.size(), 1) * sizeof(DevUnit5)))) return s;
-  b->d_units = static_cast<DevUnit5*>(p);
-  if ((s = dev_alloc(ctx, &p, std::max<size_t>(b->n_items, 1) * 4))) { s615_cls5_batch_free(ctx, b.release()); return s; }
-  b->d_items = static_cast<u32*>(p);
-  if ((s = dev_alloc(ctx, &p, sizeof(Cls5Counters) + 64))) { s615_cls5_batch_free(ctx, b.release()); return s; }
+  if ((s = dev_alloc(ctx, &p, std::max<size_t>(du.size(), 1) * sizeof(DevUnit)))) return s;
+  b->d_units = static_cast<DevUnit*>(p);
+  if ((s = dev_alloc(ctx, &p, std::max<size_t>(b->n_items, 1) * sizeof(u64)))) {
+    s615_batch_free(ctx, b.release());
+    return s;
+  }
+  b->d_items = static_cast<u64*>(p);
+  if ((s = dev_alloc(ctx, &p, sizeof(Cls5Counters) + 64))) { s615_batch_free(ctx, b.release()); return s; }
   b->d_ctr = static_cast<Cls5Counters*>(p);
   b->d_work = reinterpret_cast<u32*>(static_cast<char*>(p) + sizeof(Cls5Counters));
   b->hit_cap = 1u << 20;
-  if ((s = dev_alloc(ctx, &p, (size_t)b->hit_cap * sizeof(s615_hit)))) { s615_cls5_batch_free(ctx, b.release()); return s; }
+  if ((s = dev_alloc(ctx, &p, (size_t)b->hit_cap * sizeof(s615_hit)))) {
+    s615_batch_free(ctx, b.release());
+    return s;
+  }
   b->d_hits = static_cast<s615_hit*>(p);
-  if (!du.empty()) S615_CU(cudaMemcpy(b->d_units, du.data(), du.size() * sizeof(DevUnit5), cudaMemcpyHostToDevice));
-  if (b->n_items) S615_CU(cudaMemcpy(b->d_items, b->host_items.data(), b->n_items * 4, cudaMemcpyHostToDevice));
+  if (!du.empty())
+    S615_CU(cudaMemcpy(b->d_units, du.data(), du.size() * sizeof(DevUnit), cudaMemcpyHostToDevice));
+  if (b->n_items)
+    S615_CU(cudaMemcpy(b->d_items, b->host_items.data(), b->n_items * sizeof(u64), cudaMemcpyHostToDevice));
   *out = b.release();
   return S615_OK;
 }
 
-int s615_cls5_batch_free(s615_ctx* ctx, s615_batch* b) {
+int s615_batch_free(s615_ctx* ctx, s615_batch* b) {
   if (!ctx || !b) return S615_E_ARG;
-  dev_free(ctx, b->d_units, std::max<size_t>(b->n_units, 1) * sizeof(DevUnit5));
-  dev_free(ctx, b->d_items, std::max<size_t>(b->n_items, 1) * 4);
+  dev_free(ctx, b->d_units, std::max<size_t>(b->n_units, 1) * sizeof(DevUnit));
+  dev_free(ctx, b->d_items, std::max<size_t>(b->n_items, 1) * sizeof(u64));
   dev_free(ctx, b->d_ctr, sizeof(Cls5Counters) + 64);
   dev_free(ctx, b->d_hits, (size_t)b->hit_cap * sizeof(s615_hit));
   delete b;
   return S615_OK;
 }
 
-int s615_cls5_run_batch(s615_ctx* ctx, int id, s615_batch* b, unsigned flags, void* stream) {
+int s615_run_batch(s615_ctx* ctx, int id, s615_batch* b, unsigned flags, void* stream) {
   if (!ctx || !b) return S615_E_ARG;
   DevTable* t = find_table(ctx, id);
   if (!t) return S615_E_NOTABLE;
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
   const TableView tv = view_of(*t);
   S615_CU(cudaMemsetAsync(b->d_ctr, 0, sizeof(Cls5Counters) + 64, st));
-  if (!(flags & S615_F_PLAIN)) return launch_cls5_sieve(ctx, tv, b, flags, st, 0);
+  if (!(flags & S615_F_PLAIN)) return launch_peel(ctx, tv, b, flags, st, 0);
   // Plain form: one unit per launch and a sync after each, like the
   // reference's per-chunk loop.
   s615_batch one = *b;
@@ -489,7 +490,7 @@ int s615_cls5_run_batch(s615_ctx* ctx, int id, s615_batch* b, unsigned flags, vo
     one.d_items = b->d_items + i;
     one.n_items = j - i;
     S615_CU(cudaMemsetAsync(b->d_work, 0, 4, st));
-    int s = launch_cls5_sieve(ctx, tv, &one, flags, st, 0);
+    int s = launch_peel(ctx, tv, &one, flags, st, 0);
     if (s) return s;
     S615_CU(cudaStreamSynchronize(st));
     i = j;
@@ -497,8 +498,8 @@ int s615_cls5_run_batch(s615_ctx* ctx, int id, s615_batch* b, unsigned flags, vo
   return S615_OK;
 }
 
-int s615_cls5_batch_results(s615_ctx* ctx, s615_batch* b, s615_hit* hits, size_t hit_cap,
-                            size_t* n_hits, s615_counters* counters) {
+int s615_batch_results(s615_ctx* ctx, s615_batch* b, s615_hit* hits, size_t hit_cap,
+                       size_t* n_hits, s615_counters* counters) {
   if (!ctx || !b) return S615_E_ARG;
   Cls5Counters c{};
   S615_CU(cudaStreamSynchronize(ctx->stream));
@@ -519,25 +520,39 @@ int s615_cls5_batch_results(s615_ctx* ctx, s615_batch* b, s615_hit* hits, size_t
   return S615_OK;
 }
 
-int s615_cls5_run(s615_ctx* ctx, int id, const s615_unit* units, size_t n, unsigned flags,
-                  s615_hit* hits, size_t hit_cap, size_t* n_hits, s615_counters* counters) {
+int s615_run(s615_ctx* ctx, int id, const s615_unit* units, size_t n, unsigned flags,
+             s615_hit* hits, size_t hit_cap, size_t* n_hits, s615_counters* counters) {
   if (!ctx) return S615_E_ARG;
   if (!find_table(ctx, id)) return S615_E_NOTABLE;
   cudaSetDevice(ctx->device);
   s615_batch* b = nullptr;
-  int s = s615_cls5_prepare(ctx, units, n, &b);
+  int s = s615_prepare(ctx, units, n, &b);
   if (s) return s;
-  s = s615_cls5_run_batch(ctx, id, b, flags, nullptr);
-  if (!s) s = s615_cls5_batch_results(ctx, b, hits, hit_cap, n_hits, counters);
-  s615_cls5_batch_free(ctx, b);
+  s = s615_run_batch(ctx, id, b, flags, nullptr);
+  if (!s) s = s615_batch_results(ctx, b, hits, hit_cap, n_hits, counters);
+  s615_batch_free(ctx, b);
   return s;
+}
+
+int s615_cls5_run(s615_ctx* ctx, int id, const s615_unit* units, size_t n, unsigned flags,
+                  s615_hit* hits, size_t hit_cap, size_t* n_hits, s615_counters* counters) {
+  for (size_t i = 0; i < n; ++i)
+    if (units[i].cls != 5) return S615_E_FORMAT;
+  return s615_run(ctx, id, units, n, flags, hits, hit_cap, n_hits, counters);
+}
+
+int s615_verify(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s615_hit* hits,
+                size_t n_hits, int N, s615_solution* out, size_t cap, size_t* n_out) {
+  if (!ctx || !n_out || N < 1) return S615_E_ARG;
+  cudaSetDevice(ctx->device);
+  return verify_device(ctx, units, n_units, hits, n_hits, N, out, cap, n_out);
 }
 
 int s615_cls5_verify(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s615_hit* hits,
                      size_t n_hits, int N, s615_solution* out, size_t cap, size_t* n_out) {
-  if (!ctx || !n_out || N < 1) return S615_E_ARG;
-  cudaSetDevice(ctx->device);
-  return verify_cls5_device(ctx, units, n_units, hits, n_hits, N, out, cap, n_out);
+  for (size_t i = 0; i < n_units; ++i)
+    if (units[i].cls != 5) return S615_E_FORMAT;
+  return s615_verify(ctx, units, n_units, hits, n_hits, N, out, cap, n_out);
 }
 
 // Host self-test (no GPU): the reference's --selftest-host checks

@@ -13,22 +13,29 @@
 namespace s615 {
 
 // ------------------------------------------------------------ device unit
-// One class-5 unit as the sieve kernel consumes it.  Only base mod 2^128 is
-// needed: every row quantity V(e) = (base - (14e)^6) / 21^6 is exact and
-// below 2^112, so it is recovered from the low 128 bits by the 2-adic
-// inverse of 21^6 (the host checks the divisibility this relies on).
-struct DevUnit5 {
+// One unit as the peel kernel consumes it.  Only base mod 2^128 is needed:
+// every row quantity is an exact integer below 2^122 recovered from the low
+// 128 bits with the 2-adic inverse of 21^6 (the host checks the
+// divisibility this relies on).
+//   cls 5  : rows are e = res1[i] + 729 j (e <= fmax1), columns
+//            d = res2[k] + 64 t (d <= fmax2); row value V = (base-(14e)^6)/21^6.
+//   cls 2-4: rows are d = res1[i] + mod1 j (d <= fmax1), free factor f; row
+//            value T = (base-(f d)^6)/42^6, columns c3 over the find3 window.
+struct DevUnit {
   u64 base_lo, base_hi;
   u64 B, u;
-  u32 fmax1, fmax2, lim, nres1, nres2, id;
-  u32 res1[12];
+  u32 cls, fmax1, fmax2, lim;
+  u32 nres1, nres2, mod1, f;
+  u32 id, pad0, pad1, pad2;
+  u32 res1[24];
   u32 res2[12];
 };
-static_assert(sizeof(DevUnit5) == 152, "DevUnit5 layout");
+static_assert(sizeof(DevUnit) == 224, "DevUnit layout");
 
-// Gate pattern tables: for q in {9,7,13,19} and a,s in [0,q), bit i of word
-// pat[base_q + a*q + s] says whether T = (V - x^6)/64 is an admissible pair
-// sum mod q when V = a (mod q) and x = s + 64 i (mod q).
+// Gate pattern tables.  For q in {9,7,13,19} and a,s in [0,q), bit i of word
+// pat[base_q + a*q + s] says whether (W - x^6)/scale is an admissible pair sum
+// mod q when W = a (mod q) and x = s + step*i (mod q).  Two sets: the cls5
+// columns (step 64, scale 64) and the find3 columns (step 1, scale 1).
 constexpr int kPatQ[4] = {9, 7, 13, 19};
 constexpr int kPatBase[4] = {0, 81, 130, 299};
 constexpr int kPatB9 = 0, kPatB7 = 81, kPatB13 = 130, kPatB19 = 299;  // usable in device code
@@ -55,32 +62,32 @@ struct Cls5Counters {  // device accumulators (u64 atomics)
   unsigned long long calls, probes, pos, hits;
 };
 
-// Work items of the sieve: (unit, e residue, chunk of kItemRows e-rows),
-// packed as unit << 12 | e-residue index << 8 | chunk.
+// Work items: (unit, residue index, chunk of kItemRows rows) packed in a u64.
 constexpr u32 kItemRows = 64;
-constexpr u32 kMaxBatchUnits = 1u << 20;
-S615_HD u32 make_item(u32 unit, u32 ie, u32 chunk) { return (unit << 12) | (ie << 8) | chunk; }
-S615_HD u32 item_unit(u32 it) { return it >> 12; }
-S615_HD u32 item_eres(u32 it) { return (it >> 8) & 15u; }
-S615_HD u32 item_chunk(u32 it) { return it & 255u; }
-// e-rows of one residue: e = e0 + 729 j for j in [jmin, jend).
-S615_HD void e_rows(u32 e0, u32 fmax1, u32* jmin, u32* jend) {
-  *jmin = (e0 == 0) ? 1u : 0u;
-  *jend = (e0 <= fmax1) ? (fmax1 - e0) / 729u + 1u : 0u;
+constexpr u32 kMaxBatchUnits = 1u << 24;
+S615_HD u64 make_item(u32 unit, u32 ires, u32 chunk) {
+  return ((u64)unit << 32) | ((u64)ires << 24) | chunk;
+}
+S615_HD u32 item_unit(u64 it) { return (u32)(it >> 32); }
+S615_HD u32 item_res(u64 it) { return (u32)(it >> 24) & 255u; }
+S615_HD u32 item_chunk(u64 it) { return (u32)it & 0xFFFFFFu; }
+// Rows of one residue class: x = r0 + mod j for j in [jmin, jend), x <= fmax.
+S615_HD void class_rows(u32 r0, u32 mod, u32 fmax, u32* jmin, u32* jend) {
+  *jmin = (r0 == 0) ? 1u : 0u;
+  *jend = (r0 <= fmax) ? (fmax - r0) / mod + 1u : 0u;
 }
 
 }  // namespace s615
 
 struct s615_batch {
   size_t n_units = 0, n_items = 0;
-  s615::DevUnit5* d_units = nullptr;
-  s615::u32* d_items = nullptr;
+  s615::DevUnit* d_units = nullptr;
+  s615::u64* d_items = nullptr;
   s615_hit* d_hits = nullptr;
   s615::u32 hit_cap = 0;
   s615::Cls5Counters* d_ctr = nullptr;
   s615::u32* d_work = nullptr;   // persistent-queue cursor
-  std::vector<s615::u32> unit_ids;
-  std::vector<s615::u32> host_items;
+  std::vector<s615::u64> host_items;
 };
 
 struct s615_ctx {
@@ -89,8 +96,7 @@ struct s615_ctx {
   cudaStream_t stream = nullptr;
   std::map<int, s615::DevTable> tables;
   int next_table = 1;
-  s615::u32* d_pat_gate = nullptr;
-  s615::u32* d_pat_open = nullptr;
+  s615::u32* d_pat = nullptr;   // [gate cls5 | open cls5 | gate find3 | open find3]
   int num_sms = 0;
   unsigned long long launches = 0;
   std::mutex mu;
@@ -113,8 +119,8 @@ void dev_free(s615_ctx* ctx, void* p, size_t bytes);
 TableView view_of(const DevTable& t);
 
 // Kernel launchers (each returns a status and counts its launches).
-int launch_cls5_sieve(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
-                      cudaStream_t st, int grid_blocks);
+int launch_peel(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
+                cudaStream_t st, int grid_blocks);
 int launch_xor_query(s615_ctx* ctx, const TableView& tv, const u64* d_keys, size_t n,
                      u8* d_out, cudaStream_t st);
 int launch_unpack(s615_ctx* ctx, const u8* d_packed, u64 m, u32 r, void* d_wide, int cell_bytes,
@@ -128,9 +134,8 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
                      DevTable* out);
 
 // Device verifier; see verify.cu.
-int verify_cls5_device(s615_ctx* ctx, const s615_unit* units, size_t n_units,
-                       const s615_hit* hits, size_t n_hits, int N, s615_solution* out,
-                       size_t cap, size_t* n_out);
+int verify_device(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s615_hit* hits,
+                  size_t n_hits, int N, s615_solution* out, size_t cap, size_t* n_out);
 
 // Host math shared by the C ABI and the CLI.
 struct W3 { u64 l[3]; };
@@ -147,13 +152,17 @@ u128 inv_2adic_u128(u128 a);  // a odd
 // Residue classes (free-term rules of fourcore_classes_v3.hpp:156-219).
 std::vector<u32> e_residues(u64 B);
 std::vector<u32> d_residues(u64 B, u64 u);
+std::vector<u32> d_residues_cls234(u64 B, u64 u, int cls, u32* mod, u32* fmax);
 std::vector<u64> unit_candidates(u64 B, int cls);
+int free_factor(int cls);
 
-// Build the device record of one caller unit; returns S615_OK, or
-// S615_E_FORMAT when the unit cannot be searched (reference pack_unit5 drops
-// it) -- *skip is set for units that are dropped rather than rejected.
-int make_dev_unit(const s615_unit& in, u32 id, DevUnit5* out, bool* skip);
+// Build the device record of one caller unit; returns S615_OK (with *skip
+// set for units the reference drops) or S615_E_FORMAT for units the engine
+// cannot search exactly.
+int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip);
+// Work items of one packed unit (appended to out).
+void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out);
 
-void gate_patterns(bool gated, u32 out[kPatWords]);
+void gate_patterns(bool gated, int shape, u32 out[kPatWords]);
 
 }  // namespace s615

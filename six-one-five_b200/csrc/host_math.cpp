@@ -90,20 +90,16 @@ long long mod_pow6(long long b, long long m) {
   for (int i = 0; i < 6; ++i) r = (long long)((__int128)r * b % m);
   return r;
 }
+// Inverse of a modulo m (a coprime to m) by the extended Euclidean algorithm.
 long long mod_inv(long long a, long long m) {
-  long long g = m, x = 0, x1 = 1, aa = a % m;
-  if (aa < 0) aa += m;
-  long long b = aa;
-  // extended Euclid on (m, a)
-  long long r0 = m, r1 = b, s0 = 0, s1 = 1;
+  long long r0 = m, r1 = ((a % m) + m) % m, s0 = 0, s1 = 1;
   while (r1) {
     const long long q = r0 / r1;
     long long t = r0 - q * r1; r0 = r1; r1 = t;
     t = s0 - q * s1; s0 = s1; s1 = t;
   }
-  (void)g; (void)x; (void)x1;
-  s0 %= m; if (s0 < 0) s0 += m;
-  return s0;
+  s0 %= m;
+  return s0 < 0 ? s0 + m : s0;
 }
 long long crt_pair(long long r1, long long m1, long long r2, long long m2) {
   // m1, m2 coprime
@@ -191,12 +187,11 @@ std::vector<u64> unit_candidates(u64 B, int cls) {
 
 // --------------------------------------------------------------- dev units
 namespace {
-constexpr u64 kMaxB = 40000000ULL;  // keeps d^3, (14e)^3 and V inside the device word sizes
+constexpr u64 kMaxB = 40000000ULL;  // keeps d^3, (14e)^3 and the row values inside device words
 
 // base - (14 e0)^6 divisible by 21^6, and V(e0) = d0^6 (mod 64) for every d0:
-// then every grid point of the unit has 42^6 | R (the construction of the
-// residue classes guarantees it for Stage-1 units).
-bool divisible_grid(const W3& base, u32 e0, const u32* d0s, u32 nd) {
+// then every grid point of the unit has 42^6 | R.
+bool divisible_grid5(const W3& base, u32 e0, const u32* d0s, u32 nd) {
   W3 R = base;
   if (sub_w3(R, pow6_w3(14ULL * e0))) return true;  // row has no R>0 point
   if (divmod_w3(R, kM21) != 0) return false;
@@ -207,62 +202,125 @@ bool divisible_grid(const W3& base, u32 e0, const u32* d0s, u32 nd) {
   }
   return true;
 }
+
+// 42^6 | base - (f d0)^6; every d = d0 (mod mod) then follows (the modulus
+// supplies the prime powers that f^6 lacks).
+bool divisible_row234(const W3& base, u32 f, u32 d0) {
+  W3 R = base;
+  if (sub_w3(R, pow6_w3((u64)f * d0))) return true;   // no R>0 row in this class
+  return divmod_w3(R, kM42) == 0;
+}
 }  // namespace
 
-int make_dev_unit(const s615_unit& in, u32 id, DevUnit5* out, bool* skip) {
+int free_factor(int cls) { return cls == 2 ? 14 : cls == 3 ? 21 : cls == 4 ? 7 : 0; }
+
+// free_d_cls234 (fourcore_classes_v3.hpp:188-209): residues, modulus, fmax.
+std::vector<u32> d_residues_cls234(u64 B, u64 u, int cls, u32* mod, u32* fmax) {
+  std::vector<u32> r;
+  if (cls == 2) {
+    const long long t = mod_pow6((long long)(B % kM3), kM3) * mod_inv(mod_pow6(14, kM3), kM3) % kM3;
+    r = roots3().by[(size_t)t];
+    *mod = (u32)kM3; *fmax = (u32)((B - 1) / 14);
+  } else if (cls == 3) {
+    r = d_residues(B, u);
+    *mod = (u32)kM2; *fmax = (u32)((B - 1) / 21);
+  } else if (cls == 4) {
+    const long long t2 = mod_pow6((long long)(B % kM2), kM2) * mod_inv(mod_pow6(7, kM2), kM2) % kM2;
+    const long long t3 = mod_pow6((long long)(B % kM3), kM3) * mod_inv(mod_pow6(7, kM3), kM3) % kM3;
+    for (u32 a : roots2().by[(size_t)t2])
+      for (u32 b : roots3().by[(size_t)t3]) r.push_back((u32)crt_pair(a, kM2, b, kM3));
+    std::sort(r.begin(), r.end());
+    *mod = (u32)(kM2 * kM3); *fmax = (u32)((B - 1) / 7);
+  }
+  return r;
+}
+
+int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip) {
   std::memset(out, 0, sizeof *out);
   *skip = false;
-  if (in.cls != 5) return S615_E_FORMAT;
+  const u32 cls = in.cls;
+  if (cls < 2 || cls > 5) return S615_E_FORMAT;
   W3 base;
+  out->cls = cls;
+  out->f = (u32)free_factor((int)cls);
   if (in.kind == 0) {
     const u64 B = in.B, u = in.u;
     if (B < 2 || B > kMaxB || u == 0) return S615_E_FORMAT;
-    if (u >= B) { *skip = true; return S615_OK; }   // base <= 0: pack_unit5 drops it
+    if (u >= B) { *skip = true; return S615_OK; }   // base <= 0: the reference drops it
     base = pow6_w3(B);
     sub_w3(base, pow6_w3(u));
-    const auto er = e_residues(B);
-    const auto dr = d_residues(B, u);
-    if (er.empty() || dr.empty()) { *skip = true; return S615_OK; }
     out->B = B; out->u = u;
     out->lim = (u32)((B - 1) / 42);
-    out->fmax1 = (u32)((B - 1) / 14);
-    out->fmax2 = (u32)((B - 1) / 21);
-    out->nres1 = (u32)std::min<size_t>(er.size(), 12);
-    out->nres2 = (u32)std::min<size_t>(dr.size(), 12);
-    for (u32 i = 0; i < out->nres1; ++i) out->res1[i] = er[i];
-    for (u32 i = 0; i < out->nres2; ++i) out->res2[i] = dr[i];
-    // With both residue classes non-empty, R = 0 (mod 2^6) holds by the d rule
-    // and R = 0 (mod 3^6) by the e rule once 3 | u; R = 0 (mod 7^6) needs
-    // u^6 = B^6 (mod 7^6).  Stage-1 units satisfy both (classes_v3.hpp:102-135).
-    if (u % 3 != 0 || mod_pow6((long long)(u % kM7), kM7) != mod_pow6((long long)(B % kM7), kM7))
-      return S615_E_FORMAT;
-    out->base_lo = base.l[0];
-    out->base_hi = base.l[1];
-    out->id = id;
-    return S615_OK;
+    if (cls == 5) {
+      const auto er = e_residues(B);
+      const auto dr = d_residues(B, u);
+      if (er.empty() || dr.empty()) { *skip = true; return S615_OK; }
+      out->mod1 = kModE;
+      out->fmax1 = (u32)((B - 1) / 14);
+      out->fmax2 = (u32)((B - 1) / 21);
+      out->nres1 = (u32)std::min<size_t>(er.size(), 12);
+      out->nres2 = (u32)std::min<size_t>(dr.size(), 12);
+      for (u32 i = 0; i < out->nres1; ++i) out->res1[i] = er[i];
+      for (u32 i = 0; i < out->nres2; ++i) out->res2[i] = dr[i];
+      // With both residue classes non-empty, R = 0 (mod 2^6) holds by the d
+      // rule and R = 0 (mod 3^6) by the e rule once 3 | u; R = 0 (mod 7^6)
+      // needs u^6 = B^6 (mod 7^6).  Stage-1 units satisfy both
+      // (classes_v3.hpp:102-135).
+      if (u % 3 != 0 || mod_pow6((long long)(u % kM7), kM7) != mod_pow6((long long)(B % kM7), kM7))
+        return S615_E_FORMAT;
+    } else {
+      u32 mod = 0, fmax = 0;
+      const auto dr = d_residues_cls234(B, u, (int)cls, &mod, &fmax);
+      if (dr.empty()) { *skip = true; return S615_OK; }
+      out->mod1 = mod;
+      out->fmax1 = fmax;
+      out->nres1 = (u32)std::min<size_t>(dr.size(), 24);
+      for (u32 i = 0; i < out->nres1; ++i) out->res1[i] = dr[i];
+      for (u32 i = 0; i < out->nres1; ++i)
+        if (!divisible_row234(base, out->f, out->res1[i])) return S615_E_FORMAT;
+    }
   } else if (in.kind == 1) {
     base = W3{{in.base[0], in.base[1], in.base[2]}};
     if (zero_w3(base) || (in.base[2] >> 22) != 0) return S615_E_FORMAT;  // base < 2^150
-    if ((u64)in.fmax1 * 14 > kMaxB || (u64)in.fmax2 * 21 > kMaxB) return S615_E_FORMAT;
     out->B = in.B; out->u = in.u;
     out->lim = in.lim;
-    out->fmax1 = in.fmax1; out->fmax2 = in.fmax2;
-    out->nres1 = 1; out->nres2 = 1;
-    out->res1[0] = in.res_e % kModE;
-    out->res2[0] = in.res_d % kModD;
+    out->nres1 = 1;
+    if (cls == 5) {
+      if ((u64)in.fmax1 * 14 > kMaxB || (u64)in.fmax2 * 21 > kMaxB) return S615_E_FORMAT;
+      out->mod1 = kModE;
+      out->fmax1 = in.fmax1; out->fmax2 = in.fmax2;
+      out->nres2 = 1;
+      out->res1[0] = in.res_e % kModE;
+      out->res2[0] = in.res_d % kModD;
+      if (!divisible_grid5(base, out->res1[0], out->res2, 1)) return S615_E_FORMAT;
+    } else {
+      const u32 mod = cls == 2 ? (u32)kM3 : cls == 3 ? (u32)kM2 : (u32)(kM2 * kM3);
+      if ((u64)in.fmax1 * out->f > kMaxB) return S615_E_FORMAT;
+      out->mod1 = mod;
+      out->fmax1 = in.fmax1;
+      out->res1[0] = in.res_d % mod;
+      if (!divisible_row234(base, out->f, out->res1[0])) return S615_E_FORMAT;
+    }
   } else {
     return S615_E_FORMAT;
   }
-  for (u32 i = 0; i < out->nres1; ++i)
-    if (!divisible_grid(base, out->res1[i], out->res2, out->nres2)) return S615_E_FORMAT;
   out->base_lo = base.l[0];
   out->base_hi = base.l[1];
   out->id = id;
   return S615_OK;
 }
 
+void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out) {
+  for (u32 ir = 0; ir < d.nres1; ++ir) {
+    u32 jmin = 0, jend = 0;
+    class_rows(d.res1[ir], d.mod1, d.fmax1, &jmin, &jend);
+    const u32 rows = jend > jmin ? jend - jmin : 0;
+    for (u32 c = 0; c * kItemRows < rows; ++c) out.push_back(make_item(unit_index, ir, c));
+  }
+}
+
 // ------------------------------------------------------------ gate patterns
-// Admissible T mod q: sums of two sixth powers mod q (the factors of the
+// Admissible values mod q: sums of two sixth powers mod q (the factors of the
 // reference's mod-504 and mod-247 bitmaps, fourcore_cls5_gpu_v4.cu:124-137).
 static std::vector<u8> pair_sums_mod(u32 q) {
   std::vector<u8> ok(q, 0);
@@ -271,20 +329,22 @@ static std::vector<u8> pair_sums_mod(u32 q) {
   return ok;
 }
 
-void gate_patterns(bool gated, u32 out[kPatWords]) {
+// shape 0: cls5 columns, x = s + 64 i, value (W - x^6)/64;
+// shape 1: find3 columns, x = s + i, value W - x^6.
+void gate_patterns(bool gated, int shape, u32 out[kPatWords]) {
+  const u32 step = shape == 0 ? 64 : 1, scale = shape == 0 ? 64 : 1;
   for (int qi = 0; qi < 4; ++qi) {
     const u32 q = (u32)kPatQ[qi];
     const auto ok = pair_sums_mod(q);
-    // (V - x^6) mod q must lie in 64 * ok  (T = (V - x^6) / 64).
-    std::vector<u8> ok64(q, 0);
-    for (u32 t = 0; t < q; ++t) if (ok[t]) ok64[(64 * t) % q] = 1;
+    std::vector<u8> okw(q, 0);   // admissible (W - x^6) mod q
+    for (u32 t = 0; t < q; ++t) if (ok[t]) okw[(scale * t) % q] = 1;
     for (u32 a = 0; a < q; ++a)
       for (u32 s = 0; s < q; ++s) {
         u32 w = 0;
         for (u32 i = 0; i < 32; ++i) {
-          const u32 x = (s + 64 * i) % q;
+          const u32 x = (s + step * i) % q;
           const u32 v = (u32)(((long long)a - mod_pow6(x, q)) % q + q) % q;
-          if (!gated || ok64[v]) w |= 1u << i;
+          if (!gated || okw[v]) w |= 1u << i;
         }
         out[kPatBase[qi] + a * q + s] = w;
       }

@@ -27,14 +27,14 @@ constexpr size_t kMaxItems = 65536;
 constexpr size_t kMaxHits = 16384;
 
 struct Scratch {
-  DevUnit5 units[kMaxUnits];
-  u32 items[kMaxItems];
+  DevUnit units[kMaxUnits];
+  u64 items[kMaxItems];
   s615_hit hits[kMaxHits];
   Cls5Counters ctr;
   u32 work;
 };
 
-// The scratch: every GPU that loads the library holds these ~1.4 MB until the
+// The scratch: every GPU that loads the library holds these ~1.9 MB until the
 // process exits.  All calls share it; it keeps the last call's contents.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(Scratch)];
 
@@ -81,30 +81,31 @@ extern "C" int s615_cls5_run_noalloc(s615_ctx* ctx, int table_id, const s615_uni
 
   // Unit records and work items, staged through small stack buffers (the
   // pageable copies have consumed a buffer by the time they return).
-  DevUnit5 ustage[32];
-  u32 istage[512];
+  DevUnit ustage[32];
+  u64 istage[256];
   size_t nu = 0, ni = 0, us = 0, is = 0;
   auto flush_units = [&]() -> int {
     if (!us) return S615_OK;
-    S615_CU(cudaMemcpyAsync(S->units + nu - us, ustage, us * sizeof(DevUnit5),
+    S615_CU(cudaMemcpyAsync(S->units + nu - us, ustage, us * sizeof(DevUnit),
                             cudaMemcpyHostToDevice, st));
     us = 0;
     return S615_OK;
   };
   auto flush_items = [&]() -> int {
     if (!is) return S615_OK;
-    S615_CU(cudaMemcpyAsync(S->items + ni - is, istage, is * sizeof(u32), cudaMemcpyHostToDevice, st));
+    S615_CU(cudaMemcpyAsync(S->items + ni - is, istage, is * sizeof(u64), cudaMemcpyHostToDevice, st));
     is = 0;
     return S615_OK;
   };
   for (size_t i = 0; i < n; ++i) {
-    DevUnit5 d;
+    if (units[i].cls != 5) return S615_E_FORMAT;
+    DevUnit d;
     bool skip = false;
     if ((s = make_dev_unit(units[i], (u32)i, &d, &skip))) return s;
     if (skip) continue;
     for (u32 ie = 0; ie < d.nres1; ++ie) {
       u32 jmin = 0, jend = 0;
-      e_rows(d.res1[ie], d.fmax1, &jmin, &jend);
+      class_rows(d.res1[ie], d.mod1, d.fmax1, &jmin, &jend);
       const u32 rows = jend > jmin ? jend - jmin : 0;
       for (u32 c = 0; c * kItemRows < rows; ++c) {
         if (ni == kMaxItems) return S615_E_ARG;
@@ -131,7 +132,7 @@ extern "C" int s615_cls5_run_noalloc(s615_ctx* ctx, int table_id, const s615_uni
   b.hit_cap = (u32)kMaxHits;
   b.d_ctr = &S->ctr;
   b.d_work = &S->work;
-  if ((s = launch_cls5_sieve(ctx, view_of(it->second), &b, flags, st, 0))) return s;
+  if ((s = launch_peel(ctx, view_of(it->second), &b, flags, st, 0))) return s;
 
   Cls5Counters c{};
   S615_CU(cudaMemcpyAsync(&c, &S->ctr, sizeof c, cudaMemcpyDeviceToHost, st));

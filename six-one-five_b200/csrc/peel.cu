@@ -1,0 +1,410 @@
+// peel.cu -- the free peels of classes 2-5: exact row set-up, the residue
+// gate as a sieve, compaction and the xor probe, in one persistent kernel.
+//
+// Class 5 replaces k_cls5_192 (fourcore_cls5_gpu_v4.cu:353-410); classes 2-4
+// replace the find3 leaf (expand_unit + make_cand mode 3 + k_find3,
+// fourcore_find_v4.cu:165-205,401-425,255-284).  Both give the reference's
+// raw hits and calls/gated/probes counters.
+//
+//  * Exact rows, no per-point big integers.
+//      cls5 row e:   V(e) = (base - (14e)^6) / 21^6 (exact, < 2^112);
+//                    at column d, T = (V - d^6) / 64, and R > 0 <=> d <= D(e)
+//                    with D(e) = iroot6(V - 1).
+//      cls2-4 row d: T(d) = (base - (f d)^6) / 42^6 (exact, < 2^122); the
+//                    column c3 runs over [lo, hi] with 3 lo^6 >= T and
+//                    hi = min(iroot6(T), lim); the point value is T - c3^6.
+//    Row values come from base mod 2^128 and the 2-adic inverse of 21^6.
+//  * The gate as a sieve.  The reference keeps a value iff it is a sum of
+//    two sixth powers mod 504 and mod 247.  Those sets are products over
+//    8, 9, 7, 13, 19, and along a row each factor is periodic in the column,
+//    so a lane evaluates 32 consecutive columns at once: one row constant for
+//    mod 8 AND four 32-bit pattern words from shared memory.
+//  * Compaction: gate survivors go to a per-warp ring; each full batch of 32
+//    is probed by all lanes together (three L2-only cell loads per lane).
+//  * Warps are independent workers pulling (unit, residue, 64-row chunk)
+//    items from one device-wide queue; nothing waits at a block barrier.
+#include <cuda_runtime.h>
+
+#include "s615_device.cuh"
+
+namespace s615 {
+
+namespace {
+
+constexpr int kWarps = 8;
+constexpr int kThreads = kWarps * 32;
+constexpr u32 kRows = kItemRows;  // rows per item (64)
+constexpr u32 kMaxD = 4;          // cls5 d residues per pass
+constexpr u32 kQ = 64;            // warp ring capacity (power of two)
+constexpr u32 kNoRow = 0xFFFFFFFFu;
+constexpr u32 kLenMask = 0x0FFFFFFFu;
+
+struct __align__(16) RowRec {
+  u64 wlo, whi;   // row value W mod 2^128 (cls5: V(e); cls2-4: T(d))
+  u32 a;          // cls5: D = iroot6(V-1);   cls2-4: window start lo
+  u32 b;          // cls5: V mod 512 or kNoRow; cls2-4: window length | m4 << 28
+  u16 off[4];     // pattern-table word offset per q for W mod q
+};
+
+struct WarpSmem {                 // one warp's private slice
+  RowRec rows[kRows];
+  u16 K[kMaxD][kRows];            // cls5: in-row d limit per d residue
+  u8 M4[kMaxD][kRows];            // cls5: mod-8 admissibility of k mod 4
+  u32 ring[kQ];
+  u32 d0s[kMaxD];                 // cls5: d residues of the current pass
+};
+
+struct PeelParams {
+  TableView tv;
+  const DevUnit* units;
+  const u64* items;
+  u32 n_items;
+  u32* work;
+  s615_hit* hits;
+  u32 hit_cap;
+  Cls5Counters* ctr;
+  const u32* pat5;         // cls5 column patterns (step 64, scale 64)
+  const u32* pat3;         // find3 column patterns (step 1, scale 1)
+  u64 inv21_lo, inv21_hi;  // (21^6)^-1 mod 2^128
+  u32 s8;                  // admissible values mod 8, as a bitmask
+};
+
+constexpr size_t kSmemPat = 2 * kPatWords * sizeof(u32);
+constexpr size_t kSmemTotal = kSmemPat + kWarps * sizeof(WarpSmem);
+
+__device__ __forceinline__ u32 lanemask_lt() {
+  u32 m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// (hi * 2^64 + lo) mod Q for a small constant Q.
+constexpr u32 two64_mod(u32 q) {
+  u64 r = 1;
+  for (int i = 0; i < 64; ++i) r = (r * 2) % q;
+  return (u32)r;
+}
+template <u32 Q>
+__device__ __forceinline__ u32 mod_small(u64 hi, u64 lo) {
+  return (u32)(((hi % Q) * two64_mod(Q) + lo % Q) % Q);
+}
+
+__device__ __forceinline__ void set_offsets(RowRec& R) {
+  R.off[0] = (u16)(kPatB9 + 9 * mod_small<9>(R.whi, R.wlo));
+  R.off[1] = (u16)(kPatB7 + 7 * mod_small<7>(R.whi, R.wlo));
+  R.off[2] = (u16)(kPatB13 + 13 * mod_small<13>(R.whi, R.wlo));
+  R.off[3] = (u16)(kPatB19 + 19 * mod_small<19>(R.whi, R.wlo));
+}
+
+// x^6 mod 512 for small x.
+__device__ __forceinline__ u32 pow6_mod512(u32 x) {
+  x &= 511;
+  const u32 x2 = (x * x) & 511;
+  const u32 x3 = (x2 * x) & 511;
+  return (x3 * x3) & 511;
+}
+
+// Ring entry: column k (18 bits) | row (6 bits) << 18 | pass slot (2 bits) << 24.
+__device__ __forceinline__ u32 entry(u32 di, u32 r, u32 k) { return (di << 24) | (r << 18) | k; }
+
+// The gate word of one lane: bits for 32 consecutive columns.
+__device__ __forceinline__ u32 gate_word(const u32* pat, const RowRec& R, u32 s9, u32 s7, u32 s13,
+                                         u32 s19) {
+  const uint2 offs = *reinterpret_cast<const uint2*>(&R.off[0]);
+  return pat[(offs.x & 0xFFFFu) + s9] & pat[(offs.x >> 16) + s7] & pat[(offs.y & 0xFFFFu) + s13] &
+         pat[(offs.y >> 16) + s19];
+}
+
+struct ItemCtx {
+  u32 cls, unit_id, r0, mod, j0, f;
+};
+
+// Probe the ring entries [head, head+cnt) (one per lane).
+__device__ __forceinline__ void probe_batch(const PeelParams& P, const WarpSmem& W, u32 head,
+                                            u32 cnt, const ItemCtx& I, u32 lane) {
+  if (lane >= cnt) return;
+  const u32 ent = W.ring[(head + lane) & (kQ - 1)];
+  const u32 k = ent & 0x3FFFFu, r = (ent >> 18) & 63u, di = ent >> 24;
+  const RowRec& R = W.rows[r];
+  const u128 Wv = ((u128)R.whi << 64) | R.wlo;
+  u64 key, x;
+  u32 rowval;
+  if (I.cls == 5) {
+    x = (u64)W.d0s[di] + 64ull * k;                 // d
+    key = (u64)((Wv - pow6_small(x)) >> 6);         // T = (V - d^6)/64
+    rowval = I.r0 + I.mod * (I.j0 + r);             // e
+  } else {
+    x = (u64)R.a + k;                               // c3
+    key = R.wlo - (u64)pow6_small(x);               // T - c3^6 mod 2^64
+    rowval = I.r0 + I.mod * (I.j0 + r);             // d
+  }
+  if (might_contain(P.tv, key)) {
+    const unsigned long long idx = atomicAdd(&P.ctr->hits, 1ull);
+    if (idx < P.hit_cap) {
+      s615_hit h;
+      h.unit = I.unit_id; h.a = 0; h.b = 0;
+      if (I.cls == 5) { h.d = (u32)x; h.e = rowval; }
+      else { h.d = rowval; h.e = (u32)x; }
+      h.fp = key;
+      P.hits[idx] = h;
+    }
+  }
+}
+
+// Push the set bits of m into the ring; probe every full batch of 32.
+__device__ __forceinline__ void push_bits(const PeelParams& P, WarpSmem& W, u32 m, u32 di, u32 r,
+                                          u32 kbase, u32& head, u32& qlen, const ItemCtx& I,
+                                          u32 lane) {
+  while (__any_sync(0xFFFFFFFFu, m != 0)) {
+    const bool has = m != 0;
+    const u32 bit = has ? (u32)(__ffs(m) - 1) : 0u;
+    m &= m - 1u;
+    const u32 ballot = __ballot_sync(0xFFFFFFFFu, has);
+    if (has) W.ring[(head + qlen + __popc(ballot & lanemask_lt())) & (kQ - 1)] = entry(di, r, kbase + bit);
+    qlen += __popc(ballot);
+    if (qlen >= 32u) {
+      __syncwarp();
+      probe_batch(P, W, head, 32u, I, lane);
+      __syncwarp();
+      head = (head + 32u) & (kQ - 1);
+      qlen -= 32u;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 5) k_peel(PeelParams P) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  u32* s_pat5 = reinterpret_cast<u32*>(smem);
+  u32* s_pat3 = s_pat5 + kPatWords;
+  const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  WarpSmem& W = reinterpret_cast<WarpSmem*>(smem + kSmemPat)[warp];
+  for (u32 i = tid; i < (u32)kPatWords; i += kThreads) {
+    s_pat5[i] = P.pat5[i];
+    s_pat3[i] = P.pat3[i];
+  }
+  __syncthreads();   // the only block barrier: pattern tables are shared
+
+  const u128 inv21 = ((u128)P.inv21_hi << 64) | P.inv21_lo;
+  u64 my_calls = 0, my_pos = 0, my_probes = 0;
+
+  for (;;) {
+    u32 it = 0;
+    if (lane == 0) it = atomicAdd(P.work, 1u);
+    it = __shfl_sync(0xFFFFFFFFu, it, 0);
+    if (it >= P.n_items) break;
+    const u64 packed = P.items[it];
+    const DevUnit* U = P.units + item_unit(packed);
+    ItemCtx I;
+    I.cls = U->cls;
+    I.unit_id = U->id;
+    I.r0 = U->res1[item_res(packed)];
+    I.mod = U->mod1;
+    I.f = U->f;
+    u32 jmin, jend;
+    class_rows(I.r0, I.mod, U->fmax1, &jmin, &jend);
+    I.j0 = jmin + item_chunk(packed) * kRows;
+    const u32 nrows = min(kRows, jend - I.j0);
+    const u128 base = ((u128)U->base_hi << 64) | U->base_lo;
+    const u32 lim = U->lim;
+    u32 head = 0, qlen = 0;
+    __syncwarp();
+
+    if (I.cls == 5) {
+      // ---- cls5 rows: V, D and the residues of V (two rows per lane) ----
+      for (u32 r = lane; r < nrows; r += 32) {
+        const u64 x = 14ull * ((u64)I.r0 + (u64)I.mod * (I.j0 + r));
+        const u128 x3 = (u128)(x * x) * x;           // (14e)^3 < 2^78
+        const u128 V = (base - x3 * x3) * inv21;    // exact mod 2^128
+        RowRec R;
+        R.wlo = (u64)V; R.whi = (u64)(V >> 64);
+        if ((R.whi >> 63) || V == 0) {
+          R.a = 0; R.b = kNoRow;
+          R.off[0] = R.off[1] = R.off[2] = R.off[3] = 0;
+        } else {
+          R.a = iroot6_u128(V - 1);
+          R.b = (u32)(R.wlo & 511u);
+          set_offsets(R);
+        }
+        W.rows[r] = R;
+      }
+      const u32 fmax2 = U->fmax2, nres2 = U->nres2;
+      for (u32 dg = 0; dg < nres2; dg += kMaxD) {
+        const u32 nd = min(kMaxD, nres2 - dg);
+        __syncwarp();
+        if (lane < kMaxD) W.d0s[lane] = lane < nd ? U->res2[dg + lane] : 0u;
+        __syncwarp();
+        // per (row, d residue): in-row limit and the mod-8 row mask
+        u32 kmax = 0;
+        for (u32 idx = lane; idx < nd * kRows; idx += 32) {
+          const u32 di = idx / kRows, r = idx % kRows;
+          if (r >= nrows) continue;
+          const u32 d0 = W.d0s[di];
+          const RowRec& R = W.rows[r];
+          const u32 kcap = (d0 <= fmax2) ? (fmax2 - d0) / 64u + 1u : 0u;
+          const u32 kpos = (R.b != kNoRow && R.a >= d0) ? (R.a - d0) / 64u + 1u : 0u;
+          const u32 kend = min(kcap, kpos);
+          const u32 kmin = (d0 == 0) ? 1u : 0u;
+          if (kend > kmin) my_pos += kend - kmin;
+          if (r == 0) my_calls += (u64)nrows * (kcap > kmin ? kcap - kmin : 0u);
+          kmax = max(kmax, kend);
+          u32 m4 = 0;
+          if (R.b != kNoRow) {
+#pragma unroll
+            for (u32 i = 0; i < 4; ++i) {
+              const u32 t8 = ((R.b - pow6_mod512(d0 + 64u * i)) & 511u) >> 6;
+              m4 |= ((P.s8 >> t8) & 1u) << i;
+            }
+          }
+          W.K[di][r] = (u16)kend;
+          W.M4[di][r] = (u8)m4;
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) kmax = max(kmax, __shfl_xor_sync(0xFFFFFFFFu, kmax, o));
+        __syncwarp();
+        const u32 ntiles = (kmax + 1023u) / 1024u;
+        for (u32 di = 0; di < nd; ++di) {
+          const u32 d0 = W.d0s[di];
+          const u32 lowmask0 = (d0 == 0) ? ~1u : ~0u;
+          for (u32 wt = 0; wt < ntiles; ++wt) {
+            const u32 kbase = (wt * 32u + lane) * 32u;
+            const u64 dstart = (u64)d0 + 64ull * kbase;
+            const u32 s9 = (u32)(dstart % 9), s7 = (u32)(dstart % 7);
+            const u32 s13 = (u32)(dstart % 13), s19 = (u32)(dstart % 19);
+            const u32 lowmask = (kbase == 0) ? lowmask0 : ~0u;
+            for (u32 r = 0; r < nrows; ++r) {
+              const u32 kend = W.K[di][r];
+              if (kend <= wt * 1024u) break;          // rows shorten as e grows
+              u32 m = 0;
+              if (kbase < kend) {
+                m = ((u32)W.M4[di][r] * 0x11111111u) & gate_word(s_pat5, W.rows[r], s9, s7, s13, s19);
+                const u32 n = kend - kbase;
+                if (n < 32u) m &= (1u << n) - 1u;
+                m &= lowmask;
+              }
+              my_probes += __popc(m);
+              push_bits(P, W, m, di, r, kbase, head, qlen, I, lane);
+            }
+          }
+        }
+        __syncwarp();
+        probe_batch(P, W, head, qlen, I, lane);   // drain before d0s change
+        head = 0;
+        qlen = 0;
+        __syncwarp();
+      }
+    } else {
+      // ---- cls2-4 rows: T(d) and its find3 window [lo, hi] ----
+      for (u32 r = lane; r < nrows; r += 32) {
+        const u64 x = (u64)I.f * ((u64)I.r0 + (u64)I.mod * (I.j0 + r));
+        const u128 x3 = (u128)(x * x) * x;
+        const u128 Rm = base - x3 * x3;                         // R mod 2^128
+        const u128 T = ((Rm >> 6) * inv21) & ((~(u128)0) >> 6);  // T mod 2^122
+        RowRec R;
+        R.wlo = (u64)T; R.whi = (u64)(T >> 64);
+        R.a = 0; R.b = 0;
+        R.off[0] = R.off[1] = R.off[2] = R.off[3] = 0;
+        if (T != 0 && (T >> 121) == 0) {
+          const u32 hi = min(iroot6_u128(T), lim);
+          const u128 third = T / 3 + ((T % 3) ? 1 : 0);         // ceil(T/3) >= 1
+          const u32 lo = iroot6_u128(third - 1) + 1;            // least c with 3 c^6 >= T
+          if (lo <= hi) {
+            const u32 len = hi - lo + 1;
+            u32 m4 = 0;
+#pragma unroll
+            for (u32 i = 0; i < 4; ++i) {
+              const u32 odd = (lo + i) & 1u;                    // c^6 mod 8 = c odd ? 1 : 0
+              const u32 t8 = ((u32)R.wlo - odd) & 7u;
+              m4 |= ((P.s8 >> t8) & 1u) << i;
+            }
+            R.a = lo;
+            R.b = len | (m4 << 28);
+            set_offsets(R);
+            my_calls += len;
+            my_pos += len;
+          }
+        }
+        W.rows[r] = R;
+      }
+      __syncwarp();
+      for (u32 r = 0; r < nrows; ++r) {
+        const RowRec& R = W.rows[r];
+        const u32 len = R.b & kLenMask;
+        if (len == 0) continue;
+        const u32 m8 = (R.b >> 28) * 0x11111111u;
+        const u32 ntiles = (len + 1023u) / 1024u;
+        for (u32 wt = 0; wt < ntiles; ++wt) {
+          const u32 kbase = (wt * 32u + lane) * 32u;
+          u32 m = 0;
+          if (kbase < len) {
+            const u32 xs = R.a + kbase;
+            m = m8 & gate_word(s_pat3, R, xs % 9, xs % 7, xs % 13, xs % 19);
+            const u32 n = len - kbase;
+            if (n < 32u) m &= (1u << n) - 1u;
+          }
+          my_probes += __popc(m);
+          push_bits(P, W, m, 0, r, kbase, head, qlen, I, lane);
+        }
+      }
+      __syncwarp();
+      probe_batch(P, W, head, qlen, I, lane);
+      __syncwarp();
+    }
+  }
+
+  // ---- counters: warp reduce, one atomic per warp ----
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    my_calls += __shfl_xor_sync(0xFFFFFFFFu, my_calls, o);
+    my_pos += __shfl_xor_sync(0xFFFFFFFFu, my_pos, o);
+    my_probes += __shfl_xor_sync(0xFFFFFFFFu, my_probes, o);
+  }
+  if (lane == 0) {
+    atomicAdd(&P.ctr->calls, (unsigned long long)my_calls);
+    atomicAdd(&P.ctr->pos, (unsigned long long)my_pos);
+    atomicAdd(&P.ctr->probes, (unsigned long long)my_probes);
+  }
+}
+
+}  // namespace
+
+int launch_peel(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
+                cudaStream_t st, int grid_blocks) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    S615_CU(cudaFuncSetAttribute(k_peel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kSmemTotal));
+    attr_set = true;
+  }
+  PeelParams P{};
+  P.tv = tv;
+  P.units = b->d_units;
+  P.items = b->d_items;
+  P.n_items = (u32)b->n_items;
+  P.work = b->d_work;
+  P.hits = b->d_hits;
+  P.hit_cap = b->hit_cap;
+  P.ctr = b->d_ctr;
+  const bool gated = !(flags & S615_F_NO_GATE);
+  // ctx->d_pat = [gate cls5 | open cls5 | gate find3 | open find3]
+  P.pat5 = ctx->d_pat + (gated ? 0 : kPatWords);
+  P.pat3 = ctx->d_pat + 2 * kPatWords + (gated ? 0 : kPatWords);
+  const u128 inv = inv_2adic_u128((u128)kM21);
+  P.inv21_lo = (u64)inv;
+  P.inv21_hi = (u64)(inv >> 64);
+  P.s8 = gated ? 0x7u : 0xFFu;
+  if (b->n_items == 0) return S615_OK;
+  int grid = grid_blocks;
+  if (grid <= 0) {
+    int per_sm = 0;
+    S615_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel, kThreads, kSmemTotal));
+    grid = ctx->num_sms * (per_sm > 0 ? per_sm : 1);
+  }
+  const size_t need = (b->n_items + kWarps - 1) / kWarps;
+  if ((size_t)grid > need) grid = (int)need;
+  k_peel<<<grid, kThreads, kSmemTotal, st>>>(P);
+  ctx->launches++;
+  S615_CU(cudaGetLastError());
+  return S615_OK;
+}
+
+}  // namespace s615

@@ -1,13 +1,15 @@
-// verify.cu -- exact re-derivation of the pair behind every filter hit.
+// verify.cu -- exact re-derivation of the pairs behind filter hits.
 //
 // The reference expands a hit fingerprint into candidate pairs with
 // PairRecover (fourcore_xor_store.hpp:23-51: all i<=j<=N with i^6+j^6 = fp
-// mod 2^64), keeps a,b <= lim and then requires p6[a]+p6[b] == T exactly
-// (fourcore_cls5_gpu_v4.cu:513-523).  The surviving set is exactly
-// {(c1,c2): c1 <= c2 <= min(N,lim), c1^6 + c2^6 = T}, which this kernel
-// enumerates directly: one warp per hit, the c1 range [1, (T/2)^(1/6)] split
-// into 32 segments, each walked with the two-pointer rule (c1 up, c2 down).
-// The identity, term and gcd checks that follow are done on the host.
+// mod 2^64) and keeps those whose exact sixth powers add up:
+//   cls 5  : a,b <= lim and p6[a]+p6[b] == T          (cls5_gpu_v4.cu:513-523)
+//   cls 2-4: b <= c3 and p6[a]+p6[b]+p6[c3] == T       (find_v4.cu:538-543)
+// The surviving set is exactly {(c1,c2): c1 <= c2 <= cmax, c1^6 + c2^6 = S}
+// with S the hit's exact remainder and cmax = min(N, lim) or min(N, c3); this
+// kernel enumerates it directly: one warp per hit, the c1 range
+// [1, (S/2)^(1/6)] split into 32 segments, each walked with the two-pointer
+// rule (c1 up, c2 down).  Identity, term and gcd checks run on the host.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -23,7 +25,7 @@ namespace {
 
 struct PairOut { u32 hit, c1, c2, pad; };
 
-__global__ void k_verify(const DevUnit5* __restrict__ units, const s615_hit* __restrict__ hits,
+__global__ void k_verify(const DevUnit* __restrict__ units, const s615_hit* __restrict__ hits,
                          u32 n_hits, u32 N, u64 inv_lo, u64 inv_hi, PairOut* out, u32 cap,
                          u32* n_out) {
   const u32 lane = threadIdx.x & 31;
@@ -31,32 +33,44 @@ __global__ void k_verify(const DevUnit5* __restrict__ units, const s615_hit* __r
   const u128 inv21 = ((u128)inv_hi << 64) | inv_lo;
   for (u32 hi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; hi < n_hits; hi += warps) {
     const s615_hit H = hits[hi];
-    const DevUnit5& U = units[H.unit];
+    const DevUnit& U = units[H.unit];
     const u128 base = ((u128)U.base_hi << 64) | U.base_lo;
-    const u64 x = 14ull * H.e;
-    const u128 x3 = (u128)(x * x) * x;
-    const u128 V = (base - x3 * x3) * inv21;
-    const u128 d6 = pow6_small(H.d);
-    if ((V >> 127) || V <= d6) continue;
-    const u128 diff = V - d6;
-    if ((u64)diff & 63) continue;
-    const u128 T = diff >> 6;
-    const u32 cmax = min(N, U.lim);
-    const u32 c1max = iroot6_u128(T >> 1);
+    u128 S;
+    u32 cmax;
+    if (U.cls == 5) {
+      const u64 x = 14ull * H.e;
+      const u128 x3 = (u128)(x * x) * x;
+      const u128 V = (base - x3 * x3) * inv21;
+      const u128 d6 = pow6_small(H.d);
+      if ((V >> 127) || V <= d6) continue;
+      const u128 diff = V - d6;
+      if ((u64)diff & 63) continue;
+      S = diff >> 6;
+      cmax = min(N, U.lim);
+    } else {
+      const u64 x = (u64)U.f * H.d;
+      const u128 x3 = (u128)(x * x) * x;
+      const u128 T = (((base - x3 * x3) >> 6) * inv21) & ((~(u128)0) >> 6);
+      const u128 c6 = pow6_small(H.e);
+      if ((T >> 121) || T <= c6) continue;
+      S = T - c6;
+      cmax = min(N, H.e);
+    }
+    const u32 c1max = iroot6_u128(S >> 1);
     if (c1max == 0) continue;
     const u32 seg = (c1max + 31) / 32;
     u32 c1 = 1 + lane * seg;
     const u32 end = min(c1max, c1 + seg - 1);
     if (c1 > c1max) continue;
-    u32 c2 = min(iroot6_u128(T - pow6_small(c1)), cmax);
+    u32 c2 = min(iroot6_u128(S - pow6_small(c1)), cmax);
     while (c1 <= end && c2 >= c1) {
       const u128 s = pow6_small(c1) + pow6_small(c2);
-      if (s == T) {
+      if (s == S) {
         const u32 k = atomicAdd(n_out, 1u);
         if (k < cap) out[k] = PairOut{hi, c1, c2, 0};
         ++c1;
         --c2;
-      } else if (s < T) {
+      } else if (s < S) {
         ++c1;
       } else {
         --c2;
@@ -67,11 +81,11 @@ __global__ void k_verify(const DevUnit5* __restrict__ units, const s615_hit* __r
 
 }  // namespace
 
-int verify_cls5_device(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s615_hit* hits,
-                       size_t n_hits, int N, s615_solution* out, size_t cap, size_t* n_out) {
+int verify_device(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s615_hit* hits,
+                  size_t n_hits, int N, s615_solution* out, size_t cap, size_t* n_out) {
   *n_out = 0;
   if (n_hits == 0) return S615_OK;
-  std::vector<DevUnit5> du(n_units);
+  std::vector<DevUnit> du(n_units);
   for (size_t i = 0; i < n_units; ++i) {
     bool skip = false;
     const int s = make_dev_unit(units[i], (u32)i, &du[i], &skip);
@@ -81,7 +95,7 @@ int verify_cls5_device(s615_ctx* ctx, const s615_unit* units, size_t n_units, co
     if (hits[i].unit >= n_units) return S615_E_ARG;
   const u32 pcap = (u32)std::min<size_t>(std::max<size_t>(4 * n_hits + 64, 1024), 1u << 26);
   void *d_u = nullptr, *d_h = nullptr, *d_p = nullptr, *d_n = nullptr;
-  const size_t bu = du.size() * sizeof(DevUnit5), bh = n_hits * sizeof(s615_hit);
+  const size_t bu = du.size() * sizeof(DevUnit), bh = n_hits * sizeof(s615_hit);
   const size_t bp = pcap * sizeof(PairOut);
   int s = 0;
   if ((s = dev_alloc(ctx, &d_u, bu))) return s;
@@ -104,7 +118,7 @@ int verify_cls5_device(s615_ctx* ctx, const s615_unit* units, size_t n_units, co
     if (e == cudaSuccess) e = cudaMemsetAsync(d_n, 0, 16, st);
     if (e == cudaSuccess) {
       const u32 blocks = (u32)std::min<size_t>((n_hits + 7) / 8, (size_t)ctx->num_sms * 32);
-      k_verify<<<blocks, 256, 0, st>>>(static_cast<const DevUnit5*>(d_u),
+      k_verify<<<blocks, 256, 0, st>>>(static_cast<const DevUnit*>(d_u),
                                        static_cast<const s615_hit*>(d_h), (u32)n_hits, (u32)N,
                                        (u64)inv, (u64)(inv >> 64), static_cast<PairOut*>(d_p), pcap,
                                        static_cast<u32*>(d_n));
@@ -133,24 +147,36 @@ int verify_cls5_device(s615_ctx* ctx, const s615_unit* units, size_t n_units, co
   for (const PairOut& p : pairs) {
     const s615_hit& H = hits[p.hit];
     const s615_unit& U = units[H.unit];
-    // exact identity: target = u^6 + (21d)^6 + (14e)^6 + 42^6 (c1^6 + c2^6)
-    W3 rhs = pow6_w3(21ULL * H.d);
-    add_w3(rhs, pow6_w3(14ULL * H.e));
-    const u128 core = pow6_u128(p.c1) + pow6_u128(p.c2);
-    add_w3(rhs, mul_w3_u64(W3{{(u64)core, (u64)(core >> 64), 0}}, kM42));
     s615_solution S{};
-    S.unit = H.unit; S.kind = U.kind; S.B = U.B; S.u = U.u;
-    S.d = H.d; S.e = H.e; S.c1 = p.c1; S.c2 = p.c2;
+    S.unit = H.unit; S.kind = U.kind; S.cls = U.cls; S.B = U.B; S.u = U.u;
+    S.c1 = p.c1; S.c2 = p.c2;
+    W3 rhs;   // the peeled terms plus 42^6 times the core
+    long long t[5];
+    if (U.cls == 5) {
+      S.d = H.d; S.e = H.e;
+      rhs = pow6_w3(21ULL * H.d);
+      add_w3(rhs, pow6_w3(14ULL * H.e));
+      const u128 core = pow6_u128(p.c1) + pow6_u128(p.c2);
+      add_w3(rhs, mul_w3_u64(W3{{(u64)core, (u64)(core >> 64), 0}}, kM42));
+      t[0] = 42LL * p.c1; t[1] = 42LL * p.c2; t[2] = 21LL * H.d; t[3] = 14LL * H.e;
+    } else {
+      const u64 f = (u64)free_factor((int)U.cls);
+      S.d = H.d; S.c3 = H.e;
+      rhs = pow6_w3(f * H.d);
+      const u128 core = pow6_u128(p.c1) + pow6_u128(p.c2) + pow6_u128(H.e);
+      add_w3(rhs, mul_w3_u64(W3{{(u64)core, (u64)(core >> 64), 0}}, kM42));
+      t[0] = 42LL * p.c1; t[1] = 42LL * p.c2; t[2] = 42LL * H.e; t[3] = (long long)(f * H.d);
+    }
     if (U.kind == 1) {
       if (!eq_w3(rhs, W3{{U.base[0], U.base[1], U.base[2]}})) continue;
     } else {
       add_w3(rhs, pow6_w3(U.u));
       if (!eq_w3(rhs, pow6_w3(U.B))) continue;
-      long long t[5] = {42LL * p.c1, 42LL * p.c2, 21LL * H.d, 14LL * H.e, (long long)U.u};
+      t[4] = (long long)U.u;
       std::sort(t, t + 5);
       bool bad = false;
       for (int i = 0; i < 4; ++i) if (t[i] == t[i + 1]) bad = true;
-      if (bad || t[4] >= (long long)U.B) continue;
+      if (bad || t[4] >= (long long)U.B || t[0] < 1) continue;
       long long g = t[0];
       for (int i = 1; i < 5; ++i) g = std::gcd(g, t[i]);
       g = std::gcd(g, (long long)U.B);

@@ -62,7 +62,8 @@ class Counters(C.Structure):
 
 
 class Solution(C.Structure):
-    _fields_ = [("unit", C.c_uint32), ("kind", C.c_uint32), ("B", C.c_uint64), ("u", C.c_uint64),
+    _fields_ = [("unit", C.c_uint32), ("kind", C.c_uint32), ("cls", C.c_uint32), ("c3", C.c_uint32),
+                ("B", C.c_uint64), ("u", C.c_uint64),
                 ("d", C.c_uint32), ("e", C.c_uint32), ("c1", C.c_uint32), ("c2", C.c_uint32),
                 ("a", C.c_int64 * 5), ("gcd", C.c_int64)]
 
@@ -96,15 +97,19 @@ SIGNATURES = {
     "s615_unit_candidates": (C.c_int, [C.c_uint64, C.c_int, _P, C.c_size_t,
                                        C.POINTER(C.c_size_t)]),
     "s615_unit_status": (C.c_int, [_P]),
+    "s615_run": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.c_uint, _P, C.c_size_t,
+                           C.POINTER(C.c_size_t), C.POINTER(Counters)]),
     "s615_cls5_run": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.c_uint, _P, C.c_size_t,
                                 C.POINTER(C.c_size_t), C.POINTER(Counters)]),
     "s615_cls5_run_noalloc": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.c_uint, _P, C.c_size_t,
                                         C.POINTER(C.c_size_t), C.POINTER(Counters)]),
-    "s615_cls5_prepare": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(_P)]),
-    "s615_cls5_run_batch": (C.c_int, [_P, C.c_int, _P, C.c_uint, _P]),
-    "s615_cls5_batch_results": (C.c_int, [_P, _P, _P, C.c_size_t, C.POINTER(C.c_size_t),
-                                          C.POINTER(Counters)]),
-    "s615_cls5_batch_free": (C.c_int, [_P, _P]),
+    "s615_prepare": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(_P)]),
+    "s615_run_batch": (C.c_int, [_P, C.c_int, _P, C.c_uint, _P]),
+    "s615_batch_results": (C.c_int, [_P, _P, _P, C.c_size_t, C.POINTER(C.c_size_t),
+                                     C.POINTER(Counters)]),
+    "s615_batch_free": (C.c_int, [_P, _P]),
+    "s615_verify": (C.c_int, [_P, _P, C.c_size_t, _P, C.c_size_t, C.c_int, _P, C.c_size_t,
+                              C.POINTER(C.c_size_t)]),
     "s615_cls5_verify": (C.c_int, [_P, _P, C.c_size_t, _P, C.c_size_t, C.c_int, _P, C.c_size_t,
                                    C.POINTER(C.c_size_t)]),
     "s615_selftest_host": (C.c_int, []),
@@ -162,12 +167,25 @@ def make_units(pairs: Iterable[Tuple[int, int]]) -> "C.Array":
 
 
 def make_plant(base: int, e: int, d: int, lim: int, u: int = 0, B: int = 0) -> Unit:
-    """A planted unit: base given, single residue per axis, fmax = the planted value."""
+    """A planted cls5 unit: base given, single residue per axis, fmax = the planted value."""
     x = Unit()
     x.cls, x.kind, x.B, x.u = 5, 1, B, u
     for i in range(3):
         x.base[i] = (base >> (64 * i)) & (2**64 - 1)
     x.fmax1, x.fmax2, x.res_e, x.res_d, x.lim = e, d, e % 729, d % 64, lim
+    return x
+
+
+CLS234_MOD = {2: 729, 3: 64, 4: 46656}
+
+
+def make_plant234(cls: int, base: int, d: int, lim: int, u: int = 0, B: int = 0) -> Unit:
+    """A planted cls2-4 unit: base given, one free-term residue, fmax = d."""
+    x = Unit()
+    x.cls, x.kind, x.B, x.u = cls, 1, B, u
+    for i in range(3):
+        x.base[i] = (base >> (64 * i)) & (2**64 - 1)
+    x.fmax1, x.res_d, x.lim = d, d % CLS234_MOD[cls], lim
     return x
 
 
@@ -246,30 +264,36 @@ class Engine:
         _check(lib().s615_xor_query(self._ctx, tid, _ptr(k), k.size, _ptr(out)), "xor_query")
         return out
 
-    # ---- cls5 ----
-    def cls5_run(self, tid: int, units, n: int, flags: int = 0, hit_cap: int = 1 << 20):
+    # ---- peels (classes 2-5) ----
+    def run(self, tid: int, units, n: int, flags: int = 0, hit_cap: int = 1 << 20,
+            entry: str = "s615_run"):
         hits = (Hit * max(hit_cap, 1))()
         nh = C.c_size_t(0)
         ctr = Counters()
-        st = lib().s615_cls5_run(self._ctx, tid, C.cast(units, C.c_void_p), n, flags,
-                                 C.cast(hits, C.c_void_p), hit_cap, C.byref(nh), C.byref(ctr))
-        _check(st, "cls5_run")
+        st = getattr(lib(), entry)(self._ctx, tid, C.cast(units, C.c_void_p), n, flags,
+                                   C.cast(hits, C.c_void_p), hit_cap, C.byref(nh), C.byref(ctr))
+        _check(st, entry)
         return hits_to_array(hits, nh.value), ctr
+
+    def cls5_run(self, tid: int, units, n: int, flags: int = 0, hit_cap: int = 1 << 20):
+        return self.run(tid, units, n, flags, hit_cap, entry="s615_cls5_run")
 
     def verify(self, units, n_units: int, hits: np.ndarray, N: int, cap: int = 4096):
         h = np.ascontiguousarray(hits.astype(HIT_DTYPE))
         out = (Solution * cap)()
         no = C.c_size_t(0)
-        _check(lib().s615_cls5_verify(self._ctx, C.cast(units, C.c_void_p), n_units, _ptr(h),
-                                      h.size, N, C.cast(out, C.c_void_p), cap, C.byref(no)),
-               "cls5_verify")
+        _check(lib().s615_verify(self._ctx, C.cast(units, C.c_void_p), n_units, _ptr(h), h.size, N,
+                                 C.cast(out, C.c_void_p), cap, C.byref(no)), "verify")
         return [out[i] for i in range(no.value)]
 
 
 def solution_line(s: Solution) -> str:
-    """The reference's SOLUTION line (fourcore_cls5_gpu_v4.cu:533-536)."""
+    """The reference's SOLUTION line (fourcore_cls5_gpu_v4.cu:533-536,
+    fourcore_find_v4.cu:450-453); plants print a PLANT line."""
     if s.kind == 1:
-        return f"PLANT unit={s.unit} d={s.d} e={s.e} c1={s.c1} c2={s.c2}"
+        if s.cls == 5:
+            return f"PLANT unit={s.unit} d={s.d} e={s.e} c1={s.c1} c2={s.c2}"
+        return f"PLANT cls={s.cls} unit={s.unit} d={s.d} c1={s.c1} c2={s.c2} c3={s.c3}"
     a = list(s.a)
-    return (f"SOLUTION cls=5 B={s.B} u={s.u} a1={a[0]} a2={a[1]} a3={a[2]} a4={a[3]} a5={a[4]} "
-            f"gcd={s.gcd} {'primitive' if s.gcd == 1 else 'NON-PRIMITIVE'}")
+    return (f"SOLUTION cls={s.cls} B={s.B} u={s.u} a1={a[0]} a2={a[1]} a3={a[2]} a4={a[3]} "
+            f"a5={a[4]} gcd={s.gcd} {'primitive' if s.gcd == 1 else 'NON-PRIMITIVE'}")
