@@ -44,7 +44,19 @@ class OrcHit3(C.Structure):
     _fields_ = [("job", C.c_uint32), ("c3", C.c_uint32), ("fp", C.c_uint64)]
 
 
+class OrcCand617(C.Structure):
+    _fields_ = [("base", C.c_uint64 * 2), ("B", C.c_uint32), ("u", C.c_uint32), ("w", C.c_uint32),
+                ("lim", C.c_uint32), ("mod1", C.c_uint32), ("fmax1", C.c_uint32),
+                ("nres1", C.c_uint32), ("pad", C.c_uint32), ("res", C.c_uint32 * 24)]
+
+
+class OrcHit617(C.Structure):
+    _fields_ = [("cand", C.c_uint32), ("a", C.c_uint32), ("b", C.c_uint32), ("c", C.c_uint32),
+                ("d", C.c_uint32), ("e", C.c_uint32), ("fp", C.c_uint64)]
+
+
 assert C.sizeof(OrcUnit5) == 168 and C.sizeof(OrcHit) == 32
+assert C.sizeof(OrcCand617) == 144 and C.sizeof(OrcHit617) == 32
 
 _P = C.c_void_p
 _SIG = {
@@ -72,6 +84,11 @@ _SIG = {
     "orc_cls5_verify": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_char_p, C.c_size_t]),
     "orc_expand_cls234": (C.c_size_t, [C.c_uint64, C.c_uint64, C.c_int, _P, C.c_size_t]),
     "orc_find3_run": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_int, _P, C.c_size_t, _P]),
+    "orc_617_cands": (C.c_size_t, [C.c_uint64, _P, C.c_size_t]),
+    "orc_617_run": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_int, _P,
+                                 C.c_size_t, _P]),
+    "orc_617_verify": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_char_p, C.c_size_t,
+                                    _P]),
 }
 
 _lib = None
@@ -224,3 +241,52 @@ def unit_candidates(B: int, cls: int = 5):
 
 def seed_count(B: int, cls: int) -> int:
     return int(lib().orc_seed_count(B, cls))
+
+
+HIT617_DTYPE = np.dtype([("cand", "<u4"), ("a", "<u4"), ("b", "<u4"), ("c", "<u4"), ("d", "<u4"),
+                         ("e", "<u4"), ("fp", "<u8")])
+
+
+def cands617(B: int):
+    """gen_class_cands(cls=5) of solve_617_v1.cu:885-906 for one B (full u band)."""
+    n = lib().orc_617_cands(B, None, 0)
+    arr = (OrcCand617 * max(n, 1))()
+    lib().orc_617_cands(B, C.cast(arr, C.c_void_p), n)
+    return arr, n
+
+
+def concat617(parts):
+    """One candidate array from [(array, count), ...]."""
+    n = sum(k for _, k in parts)
+    out = (OrcCand617 * max(n, 1))()
+    i = 0
+    for arr, k in parts:
+        C.memmove(C.byref(out, i * C.sizeof(OrcCand617)), arr, k * C.sizeof(OrcCand617))
+        i += k
+    return out, n
+
+
+def run617(table: Table, cands, n: int, use_gate: bool = True, use_tri: bool = True,
+           zmax: int = 1, threads: int = 0, cap: int = 1 << 20):
+    """k_find4_cls5 semantics: (hits, [calls, gated, probes, tri_total, tri_skipped])."""
+    hits = (OrcHit617 * cap)()
+    ctr = np.zeros(5, dtype=np.uint64)
+    nh = lib().orc_617_run(table.h, C.cast(cands, C.c_void_p), n, int(use_gate), int(use_tri),
+                           zmax, threads, C.cast(hits, C.c_void_p), cap, _ptr(ctr))
+    if nh > cap:
+        raise RuntimeError("oracle hit buffer overflow")
+    raw = np.frombuffer(C.string_at(C.addressof(hits), nh * C.sizeof(OrcHit617)),
+                        dtype=HIT617_DTYPE)
+    return raw.copy(), [int(x) for x in ctr]
+
+
+def verify617(cands, hits: np.ndarray, N: int, planted: bool = False, stats: list = None):
+    """SOLUTION (or PLANT617) lines; stats, if given, receives [exact, fp_false]."""
+    h = np.ascontiguousarray(hits.astype(HIT617_DTYPE))
+    buf = C.create_string_buffer(1 << 20)
+    st = np.zeros(2, dtype=np.uint64)
+    lib().orc_617_verify(C.cast(cands, C.c_void_p), _ptr(h), h.size, N, int(planted), buf, len(buf),
+                         _ptr(st))
+    if stats is not None:
+        stats[:] = [int(st[0]), int(st[1])]
+    return [l for l in buf.value.decode().splitlines() if l]

@@ -13,6 +13,7 @@
 #include "s615_oracle.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -786,6 +787,244 @@ size_t orc_find3_run(const orc_table* t, const orc_job3* jobs, size_t n, int use
   }
   counters[0] = c0; counters[1] = c1; counters[2] = c2;
   return nh;
+}
+
+}  // extern "C"
+
+// ===================================================== (6,1,7) Branch-A cls5
+// Restates solve_617_v1.cu: gen_class_cands(cls=5) (:885-906),
+// k_find4_cls5 (:563-657) and verify_hit (:1040-1110).
+namespace {
+
+typedef __int128 i128;
+
+// scaled comparisons of solve_617_v1.cu:405-452 in exact u128 arithmetic: a
+// product that overflows 128 bits counts as larger than any R.
+bool o617_scaled_gt(u128 R, u64 c, u64 scale) {       // scale*c^6 > R
+  const u128 c6 = pow6_u128(c);
+  if (c6 > (~(u128)0) / scale) return true;
+  return c6 * scale > R;
+}
+bool o617_scaled_lt(u128 R, u64 c, u64 scale) {       // R > scale*c^6
+  const u128 c6 = pow6_u128(c);
+  if (c6 > (~(u128)0) / scale) return false;
+  return R > c6 * scale;
+}
+// iroot6_fix: largest r with scale*r^6 <= R (double estimate + exact fix-up).
+u32 o617_iroot6_fix(u128 R, u64 scale) {
+  const double d = (double)(u64)(R >> 64) * 18446744073709551616.0 + (double)(u64)R;
+  u64 r = (u64)std::pow(d / (double)scale, 1.0 / 6.0) + 2;
+  while (r > 0 && o617_scaled_gt(R, r, scale)) --r;
+  while (!o617_scaled_gt(R, r + 1, scale)) ++r;
+  return (u32)r;
+}
+// min_c_fix: least c >= 1 with !(R > 3*scale*c^6).
+u32 o617_min_c_fix(u128 R, u32 r_hi, u64 scale) {
+  u64 c = (u64)(r_hi * 0.8326831149);
+  if (c < 1) c = 1;
+  while (o617_scaled_lt(R, c, 3 * scale)) ++c;
+  while (c > 1 && !o617_scaled_lt(R, c - 1, 3 * scale)) --c;
+  return (u32)c;
+}
+
+// {(a^6 + b^6 + c^6) mod m} (build_tri_set, solve_617_v1.cu:334-342).
+std::vector<uint8_t> tri_set(int m) {
+  std::vector<uint8_t> sp(m, 0), p2(m, 0), p3(m, 0);
+  for (int i = 0; i < m; ++i) sp[mod_pow6(i, m)] = 1;
+  for (int a = 0; a < m; ++a) if (sp[a]) for (int c = 0; c < m; ++c) if (sp[c]) p2[(a + c) % m] = 1;
+  for (int a = 0; a < m; ++a) if (p2[a]) for (int c = 0; c < m; ++c) if (sp[c]) p3[(a + c) % m] = 1;
+  return p3;
+}
+
+// lift residue classes (mod m) to the values <= maxv (gen_class_cands :815-824).
+std::vector<long long> lift617(const std::vector<long long>& res, long long m, long long maxv) {
+  std::vector<long long> v;
+  for (long long r : res) {
+    long long x = r % m;
+    if (x == 0) x = m;
+    for (; x <= maxv; x += m) v.push_back(x);
+  }
+  std::sort(v.begin(), v.end());
+  return v;
+}
+
+// roots of (scale*x)^6 = b6 (mod mod) (scaled_roots, solve_617_v1.cu:217-221).
+std::vector<long long> scaled_roots617(const std::vector<std::vector<long long>>& tab, long long b6,
+                                       long long scale, long long mod) {
+  return tab[b6 * mod_inv(mod_pow6(scale, mod), mod) % mod];
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t orc_617_cands(uint64_t B, orc_cand617* out, size_t cap) {
+  const Roots& rt = roots();
+  const long long lo = 1, hi = (long long)B - 1;
+  const u128 B6 = pow6_u128(B);
+  const u32 lim = (u32)((B - 1) / 42);
+  const auto wres = scaled_roots617(rt.r2, mod_pow6((long long)B, kM2), 21, kM2);
+  const auto ures = classes_d_cls2((long long)B);                       // (14u')^6 = B^6 (3^6)
+  const auto vres = scaled_roots617(rt.r7, mod_pow6((long long)B, kM7), 6, kM7);  // (6v')^6 = B^6 (7^6)
+  size_t k = 0;
+  for (long long up : lift617(ures, kM3, ((long long)B - 1) / 14)) {
+    const long long u = 14 * up;
+    if (u < lo || u > hi) continue;
+    const u128 u6 = pow6_u128((u64)u);
+    for (long long vp : lift617(vres, kM7, ((long long)B - 1) / 6)) {
+      const i128 base = (i128)B6 - (i128)u6 - (i128)pow6_u128((u64)(6 * vp));
+      if (base <= 0) continue;
+      orc_cand617 C{};
+      C.base[0] = (u64)(u128)base; C.base[1] = (u64)((u128)base >> 64);
+      C.B = (u32)B; C.u = (u32)u; C.w = (u32)(6 * vp); C.lim = lim;
+      C.mod1 = (u32)kM2; C.fmax1 = (u32)((B - 1) / 21);
+      C.nres1 = (u32)std::min<size_t>(wres.size(), 24);
+      for (u32 i = 0; i < C.nres1; ++i) C.res[i] = (u32)wres[i];
+      if (k < cap) out[k] = C;
+      ++k;
+    }
+  }
+  return k;
+}
+
+size_t orc_617_run(const orc_table* t, const orc_cand617* cands, size_t n, int use_gate,
+                   int use_tri, int zmax, int threads, orc_hit617* hits, size_t cap,
+                   uint64_t counters[5]) {
+  static const PeelCtx PC;
+  const Gate& G = gate();
+  static const std::vector<uint8_t> t504 = tri_set(504), t247 = tri_set(247);
+  u64 c_calls = 0, c_gated = 0, c_tri_tot = 0, c_tri_skip = 0;
+  size_t nh = 0;
+#ifdef _OPENMP
+  const int nt = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt) reduction(+ : c_calls, c_gated, c_tri_tot, c_tri_skip)
+#endif
+  for (long long ci = 0; ci < (long long)n; ++ci) {
+    const orc_cand617& C = cands[ci];
+    const u128 base = ((u128)C.base[1] << 64) | C.base[0];
+    const u32 kmax = C.fmax1 / C.mod1 + 1;
+    std::vector<orc_hit617> local;
+    for (u32 tt = 0; tt < C.nres1 * kmax; ++tt) {
+      const u32 d = C.res[tt % C.nres1] + (tt / C.nres1) * C.mod1;
+      if (d == 0 || d > C.fmax1) continue;
+      const i128 Rs = (i128)base - (i128)pow6_u128(21ULL * d);
+      if (Rs <= 0) continue;
+      const u128 R = (u128)Rs;
+      u32 hi4 = o617_iroot6_fix(R, kM42);
+      if (hi4 > C.lim) hi4 = C.lim;
+      if (hi4 < 1) continue;
+      const u32 lo4 = o617_min_c_fix(R, hi4, kM42);
+      if (lo4 > hi4) continue;
+      // T = R/42^6 residues (once per d, reused per c4)
+      const u32 q504 = (u32)((u64)(R % (u128)(504ULL * kM42)) / kM42 % 504);
+      const u32 q247 = (u32)((u64)(R % 247) * PC.inv42_247 % 247);
+      for (u32 c4 = lo4; c4 <= hi4; ++c4) {
+        // visits of this c4 by the reference's c4 tiles of 2048 (gpu_run :960-968)
+        const u64 mult = zmax <= 1 ? 1 : std::min<u64>((u64)zmax, (c4 - lo4) / 2048 + 1);
+        const u32 t4504 = (q504 + 504 - G.p6504[c4 % 504]) % 504;
+        const u32 t4247 = (q247 + 247 - G.p6247[c4 % 247]) % 247;
+        if (use_tri) {
+          c_tri_tot += mult;
+          if (!t504[t4504] || !t247[t4247]) { c_tri_skip += mult; continue; }
+        }
+        const u128 c6 = pow6_u128(c4);
+        if (c6 > (~(u128)0) / kM42) continue;
+        const u128 m = c6 * kM42;
+        if (m >= R) continue;
+        const u128 R2 = R - m;
+        u32 hi3 = o617_iroot6_fix(R2, kM42);
+        const u32 capm = C.lim < c4 ? C.lim : c4;
+        if (hi3 > capm) hi3 = capm;
+        if (hi3 < 1) continue;
+        const u32 lo3 = o617_min_c_fix(R2, hi3, kM42);
+        const u64 tfp = ((u64)R2 >> 6 | (u64)(R2 >> 64) << 58) * PC.inv216;   // funnel_fp
+        for (u32 c3 = lo3; c3 <= hi3; ++c3) {
+          if (use_gate) {
+            const u32 x = (t4504 + 504 - G.p6504[c3 % 504]) % 504;
+            const u32 y = (t4247 + 247 - G.p6247[c3 % 247]) % 247;
+            if (!(G.g504[x] && G.g247[y])) { c_gated += mult; continue; }
+          }
+          c_calls += mult;
+          const u64 c3_2 = (u64)c3 * c3;
+          const u64 key = tfp - c3_2 * c3_2 * c3_2;
+          if (might_contain(*t, key))
+            for (u64 k = 0; k < mult; ++k) local.push_back(orc_hit617{(u32)ci, 0, 0, c3, c4, d, key});
+        }
+      }
+    }
+    if (!local.empty()) {
+#pragma omp critical(orc_hits617)
+      {
+        for (const auto& h : local) { if (nh < cap) hits[nh] = h; ++nh; }
+      }
+    }
+  }
+  counters[0] = c_calls; counters[1] = c_gated; counters[2] = 3 * c_calls;
+  counters[3] = c_tri_tot; counters[4] = c_tri_skip;
+  return nh;
+}
+
+size_t orc_617_verify(const orc_cand617* cands, const orc_hit617* hits, size_t nh, int N,
+                      int planted, char* buf, size_t buflen, uint64_t stats[2]) {
+  u64 n_exact = 0, n_false = 0;
+  PairRecover pr(N);
+  std::vector<std::pair<u32, u32>> pairs;
+  std::vector<std::array<long long, 7>> reported;
+  std::string text;
+  size_t lines = 0;
+  for (size_t k = 0; k < nh; ++k) {
+    const orc_hit617& H = hits[k];
+    const orc_cand617& C = cands[H.cand];
+    const u128 q = ((u128)C.base[1] << 64) | C.base[0];
+    pr.recover(H.fp, pairs);
+    for (auto [a, b] : pairs) {
+      const u128 g6 = pow6_u128(21ULL * H.e);
+      bool exact = false;
+      if (g6 <= q) {
+        const u128 rhs = q - g6;
+        exact = rhs % kM42 == 0 &&
+                pow6_u128(a) + pow6_u128(b) + pow6_u128(H.c) + pow6_u128(H.d) == rhs / kM42;
+      }
+      if (!exact) { ++n_false; continue; }
+      ++n_exact;
+      char line[256];
+      if (planted) {
+        std::snprintf(line, sizeof line, "PLANT617 cand=%u e=%u a=%u b=%u c=%u d=%u\n", H.cand, H.e,
+                      a, b, H.c, H.d);
+        text += line;
+        ++lines;
+        continue;
+      }
+      std::array<long long, 7> t = {42LL * a, 42LL * b, 42LL * H.c, 42LL * H.d, 21LL * H.e,
+                                    (long long)C.u, (long long)C.w};
+      std::sort(t.begin(), t.end());
+      bool bad = false;
+      for (int i = 0; i < 6; ++i) if (t[i] == t[i + 1]) bad = true;
+      if (bad || t[6] >= (long long)C.B || t[0] < 1) continue;
+      i128 lhs = (i128)pow6_u128(C.B);
+      for (long long x : t) { lhs -= (i128)pow6_u128((u64)x); if (lhs < 0) break; }
+      if (lhs != 0) continue;
+      if (std::find(reported.begin(), reported.end(), t) != reported.end()) continue;
+      reported.push_back(t);
+      long long g = std::gcd(t[0], t[1]);
+      for (int i = 2; i < 7; ++i) g = std::gcd(g, t[i]);
+      g = std::gcd(g, (long long)C.B);
+      std::snprintf(line, sizeof line,
+                    "SOLUTION cls=5 B=%u a1=%lld a2=%lld a3=%lld a4=%lld a5=%lld a6=%lld a7=%lld "
+                    "(anchor=%u) gcd=%lld %s\n",
+                    C.B, t[0], t[1], t[2], t[3], t[4], t[5], t[6], C.u, g,
+                    g == 1 ? "primitive" : "NON-PRIMITIVE");
+      text += line;
+      ++lines;
+    }
+  }
+  if (stats) { stats[0] = n_exact; stats[1] = n_false; }
+  if (buf && buflen) {
+    const size_t c = std::min(buflen - 1, text.size());
+    std::memcpy(buf, text.data(), c);
+    buf[c] = 0;
+  }
+  return lines;
 }
 
 }  // extern "C"

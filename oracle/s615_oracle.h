@@ -113,6 +113,35 @@ size_t orc_expand_cls234(uint64_t B, uint64_t u, int cls, orc_job3* out, size_t 
 size_t orc_find3_run(const orc_table* t, const orc_job3* jobs, size_t n, int use_gate,
                      int threads, orc_hit3* hits, size_t cap, uint64_t counters[3]);
 
+/* ---- (6,1,7) Branch-A class 5 (solve_617_v1.cu) ---- */
+typedef struct orc_cand617 {
+  uint64_t base[2];        /* B^6 - u^6 - w^6 (i128; B <= 2,353,973) */
+  uint32_t B, u, w, lim;   /* u = 14u', w = 6v' */
+  uint32_t mod1, fmax1, nres1, pad;
+  uint32_t res[24];        /* d residues mod 64 (the 21d term) */
+} orc_cand617;
+typedef struct orc_hit617 {
+  uint32_t cand, a, b, c, d, e;   /* c = c3, d = c4, e = the x21 term */
+  uint64_t fp;
+} orc_hit617;
+/* gen_class_cands(cls=5) (solve_617_v1.cu:885-906), full u band. */
+size_t orc_617_cands(uint64_t B, orc_cand617* out, size_t cap);
+/* k_find4_cls5 (solve_617_v1.cu:563-657): counters[0..4] = calls (post-gate
+ * probes), gated, probes (3 slot reads per probe), tri_total, tri_skipped.
+ * zmax <= 1 visits every (d, c4, c3) once.  zmax > 1 restates the reference
+ * launch with grid.z = zmax (gpu_run, solve_617_v1.cu:960-968): block z walks
+ * c4 from lo4 + 2048 z to hi4, so c4 is visited min(zmax, (c4-lo4)/2048 + 1)
+ * times and every count and hit is repeated that often. */
+size_t orc_617_run(const orc_table* t, const orc_cand617* cands, size_t n, int use_gate,
+                   int use_tri, int zmax, int threads, orc_hit617* hits, size_t cap,
+                   uint64_t counters[5]);
+/* expand_xor_hits + verify_hit (solve_617_v1.cu:1019-1110): SOLUTION lines
+ * (distinct tuples only); plants (u=14, w=6 dummies) print PLANT617 lines.
+ * stats (may be NULL) gets the campaign's exact / fp-false counts
+ * (:1949-1950): expanded (hit, pair) records with / without the identity. */
+size_t orc_617_verify(const orc_cand617* cands, const orc_hit617* hits, size_t nh, int N,
+                      int planted, char* buf, size_t buflen, uint64_t stats[2]);
+
 #ifdef __cplusplus
 }
 #endif

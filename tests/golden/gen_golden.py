@@ -20,6 +20,7 @@ import tempfile
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 REF_BIN = os.path.join(ROOT, "oracle", "_ref")
+REF = "/root/reference"
 OUT = os.path.join(ROOT, "tests", "golden", "golden.json")
 
 
@@ -96,6 +97,37 @@ def main():
     def pair_sums(q):
         return sorted({(i**6 + j**6) % q for i in range(q) for j in range(i, q)})
     g["gate"] = {"504": len(pair_sums(504)), "247": len(pair_sums(247))}
+
+    # -- triple-sum gate sizes (build_tri_set, solve_617_v1.cu:334-345; its
+    #    selftest requires 64 residues mod 504, :1382)
+    def tri_sums(q):
+        p = {pow(i, 6, q) for i in range(q)}
+        p2 = {(a + b) % q for a in p for b in p}
+        return sorted({(a + b) % q for a in p2 for b in p})
+    g["tri_gate"] = {"504": len(tri_sums(504)), "247": len(tri_sums(247))}
+
+    # -- known (6,1,7) identities of the Branch-A class-5 shape, read from the
+    #    reference's 617-solutions-clean.txt: 7 does not divide B, four terms
+    #    42c, one term 21d, u = 14u' and w = 6v' (the other two terms)
+    known = []
+    with open(os.path.join(REF, "617-solutions-clean.txt")) as f:
+        for line in f:
+            m = re.match(r"\s*(\d+)\s*=\s*([\d\s+]+)\|", line)
+            if not m:
+                continue
+            B = int(m.group(1))
+            t = sorted(int(x) for x in m.group(2).split("+"))
+            assert sum(x**6 for x in t) == B**6
+            if B % 7 == 0:
+                continue
+            c = [x for x in t if x % 42 == 0]
+            d = [x for x in t if x % 21 == 0 and x % 42 != 0]
+            u = [x for x in t if x % 14 == 0 and x % 42 != 0]
+            w = [x for x in t if x % 6 == 0 and x % 42 != 0]
+            if len(c) == 4 and len(d) == 1 and len(u) == 1 and len(w) == 1:
+                known.append({"B": B, "terms": t, "u": u[0], "w": w[0], "d": d[0] // 21,
+                              "c": [x // 42 for x in c]})
+    g["known617_cls5"] = [k for k in known if k["B"] < 200000]
 
     with open(OUT, "w") as f:
         json.dump(g, f, indent=1, sort_keys=True)

@@ -1,0 +1,68 @@
+#!/usr/bin/env python3
+"""Record the reference's own (6,1,7) Branch-A class-5 counts as a fixture.
+
+Runs the reference GPU binary oracle/_ref/solve_617_v1 (built from the
+reference sources by `make -C oracle ref`) on a few small B ranges and writes
+what its summary prints (candidates, probes, exact / fp-false, gate-kill,
+tri-skip counts, SOLUTION lines) to a JSON file.  It needs a GPU; run it on a
+GPU machine and copy the output to tests/golden/ref617.json, which
+tests/test_oracle617.py compares with the oracle on the same inputs.
+
+  python tests/golden/gen_ref617.py [out.json]
+"""
+import json
+import os
+import re
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+BIN = os.path.join(ROOT, "oracle", "_ref", "solve_617_v1")
+
+# (B_lo, B_hi, r, gate, tri)
+CASES = [
+    (54301, 54400, 48, True, True),
+    (54301, 54400, 16, True, True),
+    (59801, 59900, 20, True, True),
+    (63601, 63700, 48, True, True),
+    (54301, 54400, 48, True, False),
+    (54301, 54340, 20, False, True),
+]
+
+SUMMARY = re.compile(
+    r"cls5: cands=(\d+) probes=(\S+) kernel=\S+ rate=\S+ probes/s exact=(\d+) fp-false=(\d+) "
+    r"gate-kill=([\d.]+)%(?: tri-skip=[\d.]+% \((\d+)/(\d+) c4\))?")
+
+
+def main():
+    out = sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "ref617.json")
+    cases = []
+    for lo, hi, r, gate, tri in CASES:
+        cmd = [BIN, str(lo), str(hi), "5", "--branch-a-only", "--r", str(r), "--quiet"]
+        if not gate:
+            cmd.append("--no-gate")
+        if not tri:
+            cmd.append("--no-tri-gate")
+        p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+        case = {"B_lo": lo, "B_hi": hi, "r": r, "gate": gate, "tri": tri, "rc": p.returncode,
+                "cmd": " ".join(["oracle/_ref/solve_617_v1"] + cmd[1:])}
+        m = SUMMARY.search(p.stderr)
+        if p.returncode != 0 or not m:
+            case["error"] = p.stderr.strip().splitlines()[-3:]
+        else:
+            case.update(cands=int(m.group(1)), probes=m.group(2), exact=int(m.group(3)),
+                        fp_false=int(m.group(4)), gate_kill=m.group(5))
+            if m.group(6):
+                case.update(tri_skipped=int(m.group(6)), tri_total=int(m.group(7)))
+            case["solutions"] = [l for l in p.stdout.splitlines() if l.startswith("SOLUTION")]
+        cases.append(case)
+        print(json.dumps(case)[:300])
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    with open(out, "w") as f:
+        json.dump({"binary": "solve_617_v1 (reference sources, nvcc sm_100a)", "cases": cases}, f,
+                  indent=1)
+    return 0 if all("error" not in c for c in cases) else 1
+
+
+if __name__ == "__main__":
+    sys.exit(main())
