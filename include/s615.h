@@ -65,50 +65,71 @@ typedef struct s615_table_info {
 
 /* Unit record.  cls 5: the 2-D (e,d) peel; cls 2, 3, 4: one free term d
  * (x14, x21, x7) and the find3 leaf over c3 (fourcore_find_v4.cu:165-205).
+ * cls 7 (S615_CLS_617): the (6,1,7) Branch-A class-5 candidate of
+ * solve_617_v1.cu:885-906, B^6 = u^6 + w^6 + (21d)^6 + 42^6 (c1^6+..+c4^6)
+ * with u = 14u', w = 6v', d over residues mod 2^6 (d <= (B-1)/21) and the
+ * c4 / c3 windows of k_find4_cls5 (solve_617_v1.cu:563-657).
  * kind 0: a Stage-1 unit (B,u); the engine derives everything like
  * pack_unit5 (fourcore_cls5_gpu_v4.cu:169-184) / free_d_cls234
  * (fourcore_classes_v3.hpp:188-209).  kind 1: a planted target: base
  * (= target - u^6, 3 LE limbs) is taken as given with a single residue per
  * axis and fmax equal to the planted value (the reference's plant shape,
  * solve_516_v3.cu:1130-1170): cls 5 uses res_e/fmax1 and res_d/fmax2;
- * cls 2-4 use res_d/fmax1. */
+ * cls 2-4 and 7 use res_d/fmax1.  cls 7 kind 0 needs 14 | u, 6 | w,
+ * u^6 = B^6 (mod 3^6), w^6 = B^6 (mod 7^6) and B <= 2,353,973 (B^6 < 2^127);
+ * units with base <= 0 are dropped like the reference drops them.  A cls 7
+ * plant (solve_617_v1.cu:1564-1582) has base < 2^127 and lim < 65536. */
+#define S615_CLS_617 7
 typedef struct s615_unit {
-  uint32_t cls;      /* 2, 3, 4 or 5 */
-  uint32_t kind;     /* 0 = (B,u), 1 = planted base */
+  uint32_t cls;      /* 2, 3, 4, 5 or 7 */
+  uint32_t kind;     /* 0 = (B,u) or (B,u,w), 1 = planted base */
   uint64_t B, u;
   uint64_t base[3];  /* kind 1 only */
   uint32_t fmax1, fmax2, res_e, res_d, lim; /* kind 1 only */
-  uint32_t pad;
+  uint32_t w;        /* cls 7: the x6 anchor term 6v'; otherwise 0 */
 } s615_unit;
 
 /* Raw filter hit, same layout as the reference's Hit{unit,a,b,d,e,fp}
  * (fourcore_cls5_gpu_v4.cu:140); a=b=0, unit = index into the unit array.
  * cls 5: d is the x21 term and e the x14 term.  cls 2-4: d is the free term
  * and e carries c3 (the reference's find3 Hit puts c3 in its third field,
- * fourcore_find_device.cuh:70-77). */
+ * fourcore_find_device.cuh:70-77).  cls 7: d is the x21 term, e carries c3
+ * and c4 carries c4 (the reference's Hit{cand,a,b,c,d,e} of
+ * solve_617_v1.cu:364 holds them as e, c and d).  c4 is 0 for other classes
+ * and sits in what is padding in the reference's record. */
 typedef struct s615_hit {
-  uint32_t unit, a, b, d, e;
+  uint32_t unit, a, b, d, e, c4;
   uint64_t fp;
 } s615_hit;
 
 /* Counters with the reference's meaning (fourcore_cls5_gpu_v4.cu:382-409):
  * calls = in-range (e,d) points, gated = R>0 points stopped by the gate,
- * probes = xor probes issued; pos = R>0 points (= gated + probes). */
+ * probes = xor probes issued; pos = R>0 points (= gated + probes).
+ * cls 2-4 and 7 count c3 window points as calls and pos.  The (6,1,7)
+ * counters of solve_617_v1.cu:985-995 are: its calls = probes, its gated =
+ * gated, its probes = 3 * probes, and tri_total / tri_skipped = c4 values
+ * that reached / failed the triple-sum gate (0 with S615_F_NO_TRI). */
 typedef struct s615_counters {
   uint64_t calls, gated, probes, pos, hits;
+  uint64_t tri_total, tri_skipped;
 } s615_counters;
 
-/* A verified identity with sorted distinct terms a[0..4] < B and their gcd
- * with B (the SOLUTION line of fourcore_cls5_gpu_v4.cu:524-536 and
- * fourcore_find_v4.cu:427-457), or a recovered plant (kind 1, a[] unused):
- *   cls 5  : B^6 = u^6 + (21d)^6 + (14e)^6 + 42^6 (c1^6 + c2^6)
- *   cls 2-4: B^6 = u^6 + (f d)^6 + 42^6 (c1^6 + c2^6 + c3^6), f = 14, 21, 7
- * (for plants the left side is base + u^6). */
+/* A verified identity with sorted distinct terms a[0..n-1] < B and their gcd
+ * with B (the SOLUTION line of fourcore_cls5_gpu_v4.cu:524-536,
+ * fourcore_find_v4.cu:427-457 and solve_617_v1.cu:1096-1106), or a recovered
+ * plant (kind 1, a[] unused):
+ *   cls 5  : B^6 = u^6 + (21d)^6 + (14e)^6 + 42^6 (c1^6 + c2^6)           n = 5
+ *   cls 2-4: B^6 = u^6 + (f d)^6 + 42^6 (c1^6 + c2^6 + c3^6), f = 14, 21, 7 n = 5
+ *   cls 7  : B^6 = u^6 + w^6 + (21d)^6 + 42^6 (c1^6 + .. + c4^6)         n = 7
+ * (for plants the left side is base + u^6, or base + u^6 + w^6).  cls 7
+ * reports each distinct 7-tuple once per call, like the reference's reported
+ * set (solve_617_v1.cu:1096). */
 typedef struct s615_solution {
   uint32_t unit, kind, cls, c3;
   uint64_t B, u;
   uint32_t d, e, c1, c2;
-  int64_t a[5];
+  uint32_t c4, w;
+  int64_t a[7];
   int64_t gcd;
 } s615_solution;
 
@@ -162,11 +183,14 @@ int s615_unit_status(const s615_unit* unit);
 /* ---------------------------------------------------------- free peels */
 #define S615_F_NO_GATE 1u     /* --no-gate: probe every R>0 point */
 #define S615_F_PLAIN 2u       /* one unit per launch + sync (the plain form) */
+#define S615_F_NO_TRI 4u      /* cls 7: --no-tri-gate, every c4 of the window */
 
-/* The peel of a mixed batch of units (classes 2-5) in one persistent launch:
- * run_cls5_gpu's chunk loop (fourcore_cls5_gpu_v4.cu:472-512) for cls 5 and
- * run_batch mode 3 (fourcore_find_v4.cu:460-513) for cls 2-4, without the
- * verify step.  Host units in, raw hits + counters out (hits unordered).
+/* The peel of a mixed batch of units (classes 2-5 and 7) in one persistent
+ * launch per kernel: run_cls5_gpu's chunk loop (fourcore_cls5_gpu_v4.cu:
+ * 472-512) for cls 5, run_batch mode 3 (fourcore_find_v4.cu:460-513) for
+ * cls 2-4 and gpu_run (solve_617_v1.cu:924-1006) for cls 7, without the
+ * verify step.  Class-7 units go to their own persistent kernel, launched
+ * after the first on the same stream.  Host units in, raw hits + counters out (hits unordered).
  * Returns S615_E_OVERFLOW (*n_hits = the true count) when hit_cap is too
  * small; at most 2^24 units per call. */
 int s615_run(s615_ctx* ctx, int table_id, const s615_unit* units, size_t n, unsigned flags,
@@ -209,8 +233,9 @@ int s615_cls5_run_noalloc(s615_ctx* ctx, int table_id, const s615_unit* units, s
  * (fourcore_xor_store.hpp:23-51; fourcore_cls5_gpu_v4.cu:513-542;
  * fourcore_find_v4.cu:516-560): every pair c1 <= c2 with c1^6 + c2^6 equal to
  * the hit's exact remainder (cls 5: T, c2 <= min(N, lim); cls 2-4: T - c3^6,
- * c2 <= min(N, c3)), then the identity, distinct-term, < B and gcd checks.
- * Solutions come sorted by (unit, e, d, c1). */
+ * c2 <= min(N, c3); cls 7: T - c4^6 - c3^6, c2 <= N as in expand_xor_hits,
+ * solve_617_v1.cu:1019-1036), then the identity, distinct-term, < B and gcd
+ * checks.  Solutions come sorted by (unit, e, d, c4, c1). */
 int s615_verify(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s615_hit* hits,
                 size_t n_hits, int N, s615_solution* out, size_t cap, size_t* n_out);
 /* s615_verify restricted to class-5 units (S615_E_FORMAT for any other). */

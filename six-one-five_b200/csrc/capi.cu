@@ -150,16 +150,19 @@ int s615_open(int device, size_t hbm_budget, s615_ctx** out) {
   size_t free_b = 0, total_b = 0;
   S615_CU(cudaMemGetInfo(&free_b, &total_b));
   ctx->budget = hbm_budget ? hbm_budget : total_b;
-  // gate pattern sets: [gate cls5 | open cls5 | gate find3 | open find3]
-  std::vector<u32> pat(4 * kPatWords);
+  // gate pattern sets: [gate cls5 | open cls5 | gate find3 | open find3],
+  // then the triple-sum gate block of the (6,1,7) kernel
+  std::vector<u32> pat(4 * kPatWords + kTriWords);
   gate_patterns(true, 0, pat.data());
   gate_patterns(false, 0, pat.data() + kPatWords);
   gate_patterns(true, 1, pat.data() + 2 * kPatWords);
   gate_patterns(false, 1, pat.data() + 3 * kPatWords);
+  tri_tables(pat.data() + 4 * kPatWords);
   void* p = nullptr;
   const int s = dev_alloc(ctx.get(), &p, pat.size() * sizeof(u32));
   if (s) return s;
   ctx->d_pat = static_cast<u32*>(p);
+  ctx->d_tri = ctx->d_pat + 4 * kPatWords;
   S615_CU(cudaMemcpy(ctx->d_pat, pat.data(), pat.size() * sizeof(u32), cudaMemcpyHostToDevice));
   *out = ctx.release();
   return S615_OK;
@@ -170,7 +173,7 @@ int s615_close(s615_ctx* ctx) {
   cudaSetDevice(ctx->device);
   for (auto& kv : ctx->tables) free_table(ctx, kv.second);
   ctx->tables.clear();
-  dev_free(ctx, ctx->d_pat, 4 * kPatWords * sizeof(u32));
+  dev_free(ctx, ctx->d_pat, (4 * kPatWords + kTriWords) * sizeof(u32));
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return S615_OK;
@@ -425,16 +428,19 @@ int s615_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch** o
   std::unique_ptr<s615_batch> b(new s615_batch());
   std::vector<DevUnit> du;
   du.reserve(n);
+  std::vector<u64> items617;   // the (6,1,7) kernel's items go after the others
   for (size_t i = 0; i < n; ++i) {
     DevUnit d;
     bool skip = false;
     const int s = make_dev_unit(units[i], (u32)i, &d, &skip);
     if (s) return s;
     if (skip) continue;
-    unit_items(d, (u32)du.size(), b->host_items);
+    unit_items(d, (u32)du.size(), d.cls == S615_CLS_617 ? items617 : b->host_items);
     du.push_back(d);
   }
   b->n_units = du.size();
+  b->n_main = b->host_items.size();
+  b->host_items.insert(b->host_items.end(), items617.begin(), items617.end());
   b->n_items = b->host_items.size();
   int s = 0;
   void* p = nullptr;
@@ -482,14 +488,20 @@ int s615_run_batch(s615_ctx* ctx, int id, s615_batch* b, unsigned flags, void* s
   if (!(flags & S615_F_PLAIN)) return launch_peel(ctx, tv, b, flags, st, 0);
   // Plain form: one unit per launch and a sync after each, like the
   // reference's per-chunk loop.
-  s615_batch one = *b;
+  s615_batch one;   // a view of one unit's items; its vectors stay empty
+  one.d_units = b->d_units;
+  one.d_hits = b->d_hits;
+  one.hit_cap = b->hit_cap;
+  one.d_ctr = b->d_ctr;
+  one.d_work = b->d_work;
   size_t i = 0;
   while (i < b->n_items) {
     size_t j = i;
     while (j < b->n_items && item_unit(b->host_items[j]) == item_unit(b->host_items[i])) ++j;
     one.d_items = b->d_items + i;
     one.n_items = j - i;
-    S615_CU(cudaMemsetAsync(b->d_work, 0, 4, st));
+    one.n_main = i < b->n_main ? j - i : 0;   // a unit's items are all of one kernel
+    S615_CU(cudaMemsetAsync(b->d_work, 0, 8, st));
     int s = launch_peel(ctx, tv, &one, flags, st, 0);
     if (s) return s;
     S615_CU(cudaStreamSynchronize(st));
@@ -510,6 +522,8 @@ int s615_batch_results(s615_ctx* ctx, s615_batch* b, s615_hit* hits, size_t hit_
     counters->pos = c.pos;
     counters->gated = c.pos - c.probes;
     counters->hits = c.hits;
+    counters->tri_total = c.tri_total;
+    counters->tri_skipped = c.tri_skipped;
   }
   const size_t nh = (size_t)c.hits;
   if (n_hits) *n_hits = nh;

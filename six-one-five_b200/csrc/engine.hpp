@@ -21,12 +21,15 @@ namespace s615 {
 //            d = res2[k] + 64 t (d <= fmax2); row value V = (base-(14e)^6)/21^6.
 //   cls 2-4: rows are d = res1[i] + mod1 j (d <= fmax1), free factor f; row
 //            value T = (base-(f d)^6)/42^6, columns c3 over the find3 window.
+//   cls 7  : the (6,1,7) class-5 shape: base = B^6-u^6-w^6 (< 2^127), rows
+//            d = res1[i] + 64 j (d <= fmax1), f = 21; each row's c4 window
+//            opens find3 rows T' = T - c4^6 over c3.
 struct DevUnit {
   u64 base_lo, base_hi;
   u64 B, u;
   u32 cls, fmax1, fmax2, lim;
   u32 nres1, nres2, mod1, f;
-  u32 id, pad0, pad1, pad2;
+  u32 id, w, pad1, pad2;
   u32 res1[24];
   u32 res2[12];
 };
@@ -40,6 +43,11 @@ constexpr int kPatQ[4] = {9, 7, 13, 19};
 constexpr int kPatBase[4] = {0, 81, 130, 299};
 constexpr int kPatB9 = 0, kPatB7 = 81, kPatB13 = 130, kPatB19 = 299;  // usable in device code
 constexpr int kPatWords = 660;
+
+// Triple-sum gate of solve_617_v1.cu:334-345 for the c4 step, as one
+// 400-word block: bitmaps of {a^6+b^6+c^6 mod 504} (16 words) and mod 247
+// (8 words), then c^6 mod 504 (504 u16) and c^6 mod 247 (247 u16).
+constexpr int kTriT504 = 0, kTriT247 = 16, kTriP504 = 24, kTriWords = 400;
 
 // Table resident in HBM.
 struct DevTable {
@@ -60,6 +68,7 @@ struct TableView {
 
 struct Cls5Counters {  // device accumulators (u64 atomics)
   unsigned long long calls, probes, pos, hits;
+  unsigned long long tri_total, tri_skipped;
 };
 
 // Work items: (unit, residue index, chunk of kItemRows rows) packed in a u64.
@@ -81,12 +90,13 @@ S615_HD void class_rows(u32 r0, u32 mod, u32 fmax, u32* jmin, u32* jend) {
 
 struct s615_batch {
   size_t n_units = 0, n_items = 0;
+  size_t n_main = 0;             // items [0, n_main) are classes 2-5, the rest cls 7
   s615::DevUnit* d_units = nullptr;
   s615::u64* d_items = nullptr;
   s615_hit* d_hits = nullptr;
   s615::u32 hit_cap = 0;
   s615::Cls5Counters* d_ctr = nullptr;
-  s615::u32* d_work = nullptr;   // persistent-queue cursor
+  s615::u32* d_work = nullptr;   // persistent-queue cursors [classes 2-5, cls 7]
   std::vector<s615::u64> host_items;
 };
 
@@ -97,6 +107,7 @@ struct s615_ctx {
   std::map<int, s615::DevTable> tables;
   int next_table = 1;
   s615::u32* d_pat = nullptr;   // [gate cls5 | open cls5 | gate find3 | open find3]
+  s615::u32* d_tri = nullptr;   // triple-sum gate block (kTriWords)
   int num_sms = 0;
   unsigned long long launches = 0;
   std::mutex mu;
@@ -119,8 +130,12 @@ void dev_free(s615_ctx* ctx, void* p, size_t bytes);
 TableView view_of(const DevTable& t);
 
 // Kernel launchers (each returns a status and counts its launches).
+// Launches k_peel over items [0, n_main) and, when present, the (6,1,7)
+// kernel over [n_main, n_items), in that order on st.
 int launch_peel(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
                 cudaStream_t st, int grid_blocks);
+int launch_peel617(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
+                   cudaStream_t st, int grid_blocks);
 int launch_xor_query(s615_ctx* ctx, const TableView& tv, const u64* d_keys, size_t n,
                      u8* d_out, cudaStream_t st);
 int launch_unpack(s615_ctx* ctx, const u8* d_packed, u64 m, u32 r, void* d_wide, int cell_bytes,
@@ -164,5 +179,6 @@ int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip);
 void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out);
 
 void gate_patterns(bool gated, int shape, u32 out[kPatWords]);
+void tri_tables(u32 out[kTriWords]);
 
 }  // namespace s615

@@ -188,6 +188,7 @@ std::vector<u64> unit_candidates(u64 B, int cls) {
 // --------------------------------------------------------------- dev units
 namespace {
 constexpr u64 kMaxB = 40000000ULL;  // keeps d^3, (14e)^3 and the row values inside device words
+constexpr u64 kMaxB617 = 2353973ULL; // largest B with B^6 < 2^127 (solve_617_v1.cu B_HARD_MAX)
 
 // base - (14 e0)^6 divisible by 21^6, and V(e0) = d0^6 (mod 64) for every d0:
 // then every grid point of the unit has 42^6 | R.
@@ -235,10 +236,60 @@ std::vector<u32> d_residues_cls234(u64 B, u64 u, int cls, u32* mod, u32* fmax) {
   return r;
 }
 
+// cls 7: the (6,1,7) class-5 candidate (gen_class_cands, solve_617_v1.cu:
+// 885-906).  Every row d then has 42^6 | base - (21d)^6: mod 2^6 by the d
+// residues (u, w even), mod 3^6 by u^6 = B^6 (w, 21d divisible by 3), mod 7^6
+// by w^6 = B^6 (u, 21d divisible by 7).
+static int make_dev_unit617(const s615_unit& in, DevUnit* out, bool* skip) {
+  out->cls = S615_CLS_617;
+  out->f = 21;
+  out->mod1 = (u32)kM2;
+  W3 base;
+  if (in.kind == 0) {
+    const u64 B = in.B, u = in.u, w = in.w;
+    if (B < 2 || B > kMaxB617 || u == 0 || w == 0) return S615_E_FORMAT;
+    if (u % 14 != 0 || w % 6 != 0) return S615_E_FORMAT;
+    if (mod_pow6((long long)(u % kM3), kM3) != mod_pow6((long long)(B % kM3), kM3) ||
+        mod_pow6((long long)(w % kM7), kM7) != mod_pow6((long long)(B % kM7), kM7))
+      return S615_E_FORMAT;
+    if (u >= B || w >= B) { *skip = true; return S615_OK; }
+    base = pow6_w3(B);
+    sub_w3(base, pow6_w3(u));
+    if (sub_w3(base, pow6_w3(w)) || zero_w3(base)) { *skip = true; return S615_OK; }  // base <= 0
+    const auto dr = d_residues(B, u);
+    if (dr.empty()) { *skip = true; return S615_OK; }
+    out->B = B; out->u = u; out->w = (u32)w;
+    out->lim = (u32)((B - 1) / 42);
+    out->fmax1 = (u32)((B - 1) / 21);
+    out->nres1 = (u32)std::min<size_t>(dr.size(), 24);
+    for (u32 i = 0; i < out->nres1; ++i) out->res1[i] = dr[i];
+  } else if (in.kind == 1) {
+    base = W3{{in.base[0], in.base[1], in.base[2]}};
+    if (zero_w3(base) || base.l[2] != 0 || (base.l[1] >> 63) != 0) return S615_E_FORMAT;
+    if (in.lim >= 65536 || (u64)in.fmax1 * 21 > kMaxB617) return S615_E_FORMAT;
+    out->B = in.B; out->u = in.u; out->w = in.w;
+    out->lim = in.lim;
+    out->fmax1 = in.fmax1;
+    out->nres1 = 1;
+    out->res1[0] = in.res_d % (u32)kM2;
+    if (!divisible_row234(base, 21, out->res1[0])) return S615_E_FORMAT;
+  } else {
+    return S615_E_FORMAT;
+  }
+  out->base_lo = base.l[0];
+  out->base_hi = base.l[1];
+  return S615_OK;
+}
+
 int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip) {
   std::memset(out, 0, sizeof *out);
   *skip = false;
   const u32 cls = in.cls;
+  if (cls == S615_CLS_617) {
+    const int s = make_dev_unit617(in, out, skip);
+    out->id = id;
+    return s;
+  }
   if (cls < 2 || cls > 5) return S615_E_FORMAT;
   W3 base;
   out->cls = cls;
@@ -349,6 +400,27 @@ void gate_patterns(bool gated, int shape, u32 out[kPatWords]) {
         out[kPatBase[qi] + a * q + s] = w;
       }
   }
+}
+
+// Triple-sum gate block (build_tri_set, solve_617_v1.cu:334-345): bit x of
+// the first bitmap is set iff x = a^6 + b^6 + c^6 (mod 504) for some a, b, c;
+// likewise mod 247; then the tables c^6 mod 504 and mod 247 as u16 pairs.
+void tri_tables(u32 out[kTriWords]) {
+  std::memset(out, 0, kTriWords * sizeof(u32));
+  auto tri = [](u32 m, u32* bits) {
+    std::vector<u8> sp(m, 0), p2(m, 0);
+    for (u32 i = 0; i < m; ++i) sp[(size_t)mod_pow6(i, m)] = 1;
+    for (u32 a = 0; a < m; ++a) if (sp[a]) for (u32 c = 0; c < m; ++c) if (sp[c]) p2[(a + c) % m] = 1;
+    for (u32 a = 0; a < m; ++a) if (p2[a]) for (u32 c = 0; c < m; ++c) if (sp[c]) {
+      const u32 x = (a + c) % m;
+      bits[x >> 5] |= 1u << (x & 31);
+    }
+  };
+  tri(504, out + kTriT504);
+  tri(247, out + kTriT247);
+  u16* p6 = reinterpret_cast<u16*>(out + kTriP504);
+  for (u32 c = 0; c < 504; ++c) p6[c] = (u16)mod_pow6(c, 504);
+  for (u32 c = 0; c < 247; ++c) p6[504 + c] = (u16)mod_pow6(c, 247);
 }
 
 // The reference's bitmaps equal the CRT product of the five factor sets.

@@ -126,6 +126,7 @@ extern "C" int s615_cls5_run_noalloc(s615_ctx* ctx, int table_id, const s615_uni
   s615_batch b;   // a view of the scratch; its vectors stay empty
   b.n_units = nu;
   b.n_items = ni;
+  b.n_main = ni;   // class 5 only: every item is for k_peel
   b.d_units = S->units;
   b.d_items = S->items;
   b.d_hits = S->hits;
@@ -150,6 +151,8 @@ extern "C" int s615_cls5_run_noalloc(s615_ctx* ctx, int table_id, const s615_uni
     counters->pos = c.pos;
     counters->gated = c.pos - c.probes;
     counters->hits = c.hits;
+    counters->tri_total = 0;
+    counters->tri_skipped = 0;
   }
   return (nh > kMaxHits || nh > hit_cap) ? S615_E_OVERFLOW : S615_OK;
 }

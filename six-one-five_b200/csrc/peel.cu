@@ -25,7 +25,7 @@
 //    items from one device-wide queue; nothing waits at a block barrier.
 #include <cuda_runtime.h>
 
-#include "s615_device.cuh"
+#include "peel_common.cuh"
 
 namespace s615 {
 
@@ -38,13 +38,6 @@ constexpr u32 kMaxD = 4;          // cls5 d residues per pass
 constexpr u32 kQ = 64;            // warp ring capacity (power of two)
 constexpr u32 kNoRow = 0xFFFFFFFFu;
 constexpr u32 kLenMask = 0x0FFFFFFFu;
-
-struct __align__(16) RowRec {
-  u64 wlo, whi;   // row value W mod 2^128 (cls5: V(e); cls2-4: T(d))
-  u32 a;          // cls5: D = iroot6(V-1);   cls2-4: window start lo
-  u32 b;          // cls5: V mod 512 or kNoRow; cls2-4: window length | m4 << 28
-  u16 off[4];     // pattern-table word offset per q for W mod q
-};
 
 struct WarpSmem {                 // one warp's private slice
   RowRec rows[kRows];
@@ -72,30 +65,6 @@ struct PeelParams {
 constexpr size_t kSmemPat = 2 * kPatWords * sizeof(u32);
 constexpr size_t kSmemTotal = kSmemPat + kWarps * sizeof(WarpSmem);
 
-__device__ __forceinline__ u32 lanemask_lt() {
-  u32 m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-  return m;
-}
-
-// (hi * 2^64 + lo) mod Q for a small constant Q.
-constexpr u32 two64_mod(u32 q) {
-  u64 r = 1;
-  for (int i = 0; i < 64; ++i) r = (r * 2) % q;
-  return (u32)r;
-}
-template <u32 Q>
-__device__ __forceinline__ u32 mod_small(u64 hi, u64 lo) {
-  return (u32)(((hi % Q) * two64_mod(Q) + lo % Q) % Q);
-}
-
-__device__ __forceinline__ void set_offsets(RowRec& R) {
-  R.off[0] = (u16)(kPatB9 + 9 * mod_small<9>(R.whi, R.wlo));
-  R.off[1] = (u16)(kPatB7 + 7 * mod_small<7>(R.whi, R.wlo));
-  R.off[2] = (u16)(kPatB13 + 13 * mod_small<13>(R.whi, R.wlo));
-  R.off[3] = (u16)(kPatB19 + 19 * mod_small<19>(R.whi, R.wlo));
-}
-
 // x^6 mod 512 for small x.
 __device__ __forceinline__ u32 pow6_mod512(u32 x) {
   x &= 511;
@@ -106,14 +75,6 @@ __device__ __forceinline__ u32 pow6_mod512(u32 x) {
 
 // Ring entry: column k (18 bits) | row (6 bits) << 18 | pass slot (2 bits) << 24.
 __device__ __forceinline__ u32 entry(u32 di, u32 r, u32 k) { return (di << 24) | (r << 18) | k; }
-
-// The gate word of one lane: bits for 32 consecutive columns.
-__device__ __forceinline__ u32 gate_word(const u32* pat, const RowRec& R, u32 s9, u32 s7, u32 s13,
-                                         u32 s19) {
-  const uint2 offs = *reinterpret_cast<const uint2*>(&R.off[0]);
-  return pat[(offs.x & 0xFFFFu) + s9] & pat[(offs.x >> 16) + s7] & pat[(offs.y & 0xFFFFu) + s13] &
-         pat[(offs.y >> 16) + s19];
-}
 
 struct ItemCtx {
   u32 cls, unit_id, r0, mod, j0, f;
@@ -142,7 +103,7 @@ __device__ __forceinline__ void probe_batch(const PeelParams& P, const WarpSmem&
     const unsigned long long idx = atomicAdd(&P.ctr->hits, 1ull);
     if (idx < P.hit_cap) {
       s615_hit h;
-      h.unit = I.unit_id; h.a = 0; h.b = 0;
+      h.unit = I.unit_id; h.a = 0; h.b = 0; h.c4 = 0;
       if (I.cls == 5) { h.d = (u32)x; h.e = rowval; }
       else { h.d = rowval; h.e = (u32)x; }
       h.fp = key;
@@ -365,10 +326,9 @@ __global__ void __launch_bounds__(kThreads, 5) k_peel(PeelParams P) {
   }
 }
 
-}  // namespace
-
-int launch_peel(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
-                cudaStream_t st, int grid_blocks) {
+// k_peel over items [0, n) of the batch.
+int launch_main(s615_ctx* ctx, const TableView& tv, const s615_batch* b, size_t n,
+                unsigned flags, cudaStream_t st, int grid_blocks) {
   static bool attr_set = false;
   if (!attr_set) {
     S615_CU(cudaFuncSetAttribute(k_peel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -379,7 +339,7 @@ int launch_peel(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flag
   P.tv = tv;
   P.units = b->d_units;
   P.items = b->d_items;
-  P.n_items = (u32)b->n_items;
+  P.n_items = (u32)n;
   P.work = b->d_work;
   P.hits = b->d_hits;
   P.hit_cap = b->hit_cap;
@@ -392,18 +352,30 @@ int launch_peel(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flag
   P.inv21_lo = (u64)inv;
   P.inv21_hi = (u64)(inv >> 64);
   P.s8 = gated ? 0x7u : 0xFFu;
-  if (b->n_items == 0) return S615_OK;
+  if (n == 0) return S615_OK;
   int grid = grid_blocks;
   if (grid <= 0) {
     int per_sm = 0;
     S615_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel, kThreads, kSmemTotal));
     grid = ctx->num_sms * (per_sm > 0 ? per_sm : 1);
   }
-  const size_t need = (b->n_items + kWarps - 1) / kWarps;
+  const size_t need = (n + kWarps - 1) / kWarps;
   if ((size_t)grid > need) grid = (int)need;
   k_peel<<<grid, kThreads, kSmemTotal, st>>>(P);
   ctx->launches++;
   S615_CU(cudaGetLastError());
+  return S615_OK;
+}
+
+}  // namespace
+
+int launch_peel(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
+                cudaStream_t st, int grid_blocks) {
+  if (b->n_main) {
+    const int s = launch_main(ctx, tv, b, b->n_main, flags, st, grid_blocks);
+    if (s) return s;
+  }
+  if (b->n_items > b->n_main) return launch_peel617(ctx, tv, b, flags, st, grid_blocks);
   return S615_OK;
 }
 

@@ -5,14 +5,16 @@
 // mod 2^64) and keeps those whose exact sixth powers add up:
 //   cls 5  : a,b <= lim and p6[a]+p6[b] == T          (cls5_gpu_v4.cu:513-523)
 //   cls 2-4: b <= c3 and p6[a]+p6[b]+p6[c3] == T       (find_v4.cu:538-543)
+//   cls 7  : a,b <= N and a^6+b^6+c3^6+c4^6 == T       (solve_617_v1.cu:1083-1088)
 // The surviving set is exactly {(c1,c2): c1 <= c2 <= cmax, c1^6 + c2^6 = S}
-// with S the hit's exact remainder and cmax = min(N, lim) or min(N, c3); this
+// with S the hit's exact remainder and cmax = min(N, lim), min(N, c3) or N; this
 // kernel enumerates it directly: one warp per hit, the c1 range
 // [1, (S/2)^(1/6)] split into 32 segments, each walked with the two-pointer
 // rule (c1 up, c2 down).  Identity, term and gcd checks run on the host.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cstring>
 #include <numeric>
 #include <vector>
@@ -55,6 +57,12 @@ __global__ void k_verify(const DevUnit* __restrict__ units, const s615_hit* __re
       if ((T >> 121) || T <= c6) continue;
       S = T - c6;
       cmax = min(N, H.e);
+      if (U.cls == S615_CLS_617) {   // T - c3^6 - c4^6; pairs up to N
+        const u128 c46 = pow6_small(H.c4);
+        if (S <= c46) continue;
+        S -= c46;
+        cmax = N;
+      }
     }
     const u32 c1max = iroot6_u128(S >> 1);
     if (c1max == 0) continue;
@@ -140,10 +148,12 @@ int verify_device(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s
     if (ha.unit != hb.unit) return ha.unit < hb.unit;
     if (ha.e != hb.e) return ha.e < hb.e;
     if (ha.d != hb.d) return ha.d < hb.d;
+    if (ha.c4 != hb.c4) return ha.c4 < hb.c4;
     if (a.hit != b.hit) return a.hit < b.hit;
     return a.c1 < b.c1;
   });
   size_t k = 0;
+  std::vector<std::array<long long, 7>> reported;   // cls 7: distinct 7-tuples only
   for (const PairOut& p : pairs) {
     const s615_hit& H = hits[p.hit];
     const s615_unit& U = units[H.unit];
@@ -152,6 +162,35 @@ int verify_device(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s
     S.c1 = p.c1; S.c2 = p.c2;
     W3 rhs;   // the peeled terms plus 42^6 times the core
     long long t[5];
+    if (U.cls == S615_CLS_617) {
+      S.d = H.d; S.c3 = H.e; S.c4 = H.c4; S.w = U.w;
+      rhs = pow6_w3(21ULL * H.d);
+      const u128 core = pow6_u128(p.c1) + pow6_u128(p.c2) + pow6_u128(H.e) + pow6_u128(H.c4);
+      add_w3(rhs, mul_w3_u64(W3{{(u64)core, (u64)(core >> 64), 0}}, kM42));
+      if (U.kind == 1) {
+        if (!eq_w3(rhs, W3{{U.base[0], U.base[1], U.base[2]}})) continue;
+      } else {
+        add_w3(rhs, pow6_w3(U.u));
+        add_w3(rhs, pow6_w3(U.w));
+        if (!eq_w3(rhs, pow6_w3(U.B))) continue;
+        std::array<long long, 7> t7 = {42LL * p.c1, 42LL * p.c2, 42LL * H.e, 42LL * H.c4,
+                                       21LL * H.d, (long long)U.u, (long long)U.w};
+        std::sort(t7.begin(), t7.end());
+        bool bad = false;
+        for (int i = 0; i < 6; ++i) if (t7[i] == t7[i + 1]) bad = true;
+        if (bad || t7[6] >= (long long)U.B || t7[0] < 1) continue;
+        if (std::find(reported.begin(), reported.end(), t7) != reported.end()) continue;
+        reported.push_back(t7);
+        long long g = t7[0];
+        for (int i = 1; i < 7; ++i) g = std::gcd(g, t7[i]);
+        g = std::gcd(g, (long long)U.B);
+        for (int i = 0; i < 7; ++i) S.a[i] = t7[i];
+        S.gcd = g;
+      }
+      if (k < cap) out[k] = S;
+      ++k;
+      continue;
+    }
     if (U.cls == 5) {
       S.d = H.d; S.e = H.e;
       rhs = pow6_w3(21ULL * H.d);

@@ -22,7 +22,8 @@ STATUS = {
     -7: "DEVICE", -8: "TIMEOUT", -9: "OVERFLOW", -10: "BUILD", -11: "NOTABLE",
 }
 LAYOUT_AUTO, LAYOUT_PACKED, LAYOUT_WIDE = 0, 1, 2
-F_NO_GATE, F_PLAIN = 1, 2
+F_NO_GATE, F_PLAIN, F_NO_TRI = 1, 2, 4
+S615_CLS_617 = 7
 
 
 class S615Error(RuntimeError):
@@ -48,32 +49,35 @@ class Unit(C.Structure):
     _fields_ = [("cls", C.c_uint32), ("kind", C.c_uint32), ("B", C.c_uint64), ("u", C.c_uint64),
                 ("base", C.c_uint64 * 3), ("fmax1", C.c_uint32), ("fmax2", C.c_uint32),
                 ("res_e", C.c_uint32), ("res_d", C.c_uint32), ("lim", C.c_uint32),
-                ("pad", C.c_uint32)]
+                ("w", C.c_uint32)]
 
 
 class Hit(C.Structure):
     _fields_ = [("unit", C.c_uint32), ("a", C.c_uint32), ("b", C.c_uint32), ("d", C.c_uint32),
-                ("e", C.c_uint32), ("fp", C.c_uint64)]
+                ("e", C.c_uint32), ("c4", C.c_uint32), ("fp", C.c_uint64)]
 
 
 class Counters(C.Structure):
     _fields_ = [("calls", C.c_uint64), ("gated", C.c_uint64), ("probes", C.c_uint64),
-                ("pos", C.c_uint64), ("hits", C.c_uint64)]
+                ("pos", C.c_uint64), ("hits", C.c_uint64), ("tri_total", C.c_uint64),
+                ("tri_skipped", C.c_uint64)]
 
 
 class Solution(C.Structure):
     _fields_ = [("unit", C.c_uint32), ("kind", C.c_uint32), ("cls", C.c_uint32), ("c3", C.c_uint32),
                 ("B", C.c_uint64), ("u", C.c_uint64),
                 ("d", C.c_uint32), ("e", C.c_uint32), ("c1", C.c_uint32), ("c2", C.c_uint32),
-                ("a", C.c_int64 * 5), ("gcd", C.c_int64)]
+                ("c4", C.c_uint32), ("w", C.c_uint32), ("a", C.c_int64 * 7), ("gcd", C.c_int64)]
 
 
 assert C.sizeof(Header) == 64
 assert C.sizeof(Hit) == 32
 assert C.sizeof(Unit) == 72
+assert C.sizeof(Counters) == 56
+assert C.sizeof(Solution) == 120
 
 HIT_DTYPE = np.dtype([("unit", "<u4"), ("a", "<u4"), ("b", "<u4"), ("d", "<u4"), ("e", "<u4"),
-                      ("pad", "<u4"), ("fp", "<u8")])
+                      ("c4", "<u4"), ("fp", "<u8")])
 
 # Every entry point declared in include/s615.h, with its ctypes signature.
 _P = C.c_void_p
@@ -189,6 +193,26 @@ def make_plant234(cls: int, base: int, d: int, lim: int, u: int = 0, B: int = 0)
     return x
 
 
+def make_units617(triples: Iterable[Tuple[int, int, int]]) -> "C.Array":
+    """(6,1,7) Branch-A class-5 candidates (B, u = 14u', w = 6v')."""
+    triples = list(triples)
+    arr = (Unit * max(len(triples), 1))()
+    for i, (B, u, w) in enumerate(triples):
+        arr[i].cls, arr[i].kind, arr[i].B, arr[i].u, arr[i].w = S615_CLS_617, 0, B, u, w
+    return arr, len(triples)
+
+
+def make_plant617(base: int, d: int, lim: int, B: int = 0, u: int = 14, w: int = 6) -> Unit:
+    """A planted (6,1,7) class-5 target (solve_617_v1.cu:1564-1582): base
+    given, one x21 residue, fmax = d, c4 and c3 capped by lim."""
+    x = Unit()
+    x.cls, x.kind, x.B, x.u, x.w = S615_CLS_617, 1, B, u, w
+    for i in range(3):
+        x.base[i] = (base >> (64 * i)) & (2**64 - 1)
+    x.fmax1, x.res_d, x.lim = d, d % 64, lim
+    return x
+
+
 def hits_to_array(hits, n: int) -> np.ndarray:
     raw = np.frombuffer(C.string_at(C.addressof(hits), n * C.sizeof(Hit)), dtype=HIT_DTYPE)
     return raw.copy()
@@ -289,11 +313,19 @@ class Engine:
 
 def solution_line(s: Solution) -> str:
     """The reference's SOLUTION line (fourcore_cls5_gpu_v4.cu:533-536,
-    fourcore_find_v4.cu:450-453); plants print a PLANT line."""
+    fourcore_find_v4.cu:450-453, solve_617_v1.cu:1101-1103; the (6,1,7)
+    class-5 shape prints as cls=5 there); plants print a PLANT line."""
     if s.kind == 1:
         if s.cls == 5:
             return f"PLANT unit={s.unit} d={s.d} e={s.e} c1={s.c1} c2={s.c2}"
+        if s.cls == S615_CLS_617:
+            return (f"PLANT cls=7 unit={s.unit} d={s.d} c1={s.c1} c2={s.c2} c3={s.c3} "
+                    f"c4={s.c4}")
         return f"PLANT cls={s.cls} unit={s.unit} d={s.d} c1={s.c1} c2={s.c2} c3={s.c3}"
     a = list(s.a)
+    if s.cls == S615_CLS_617:
+        terms = " ".join(f"a{i + 1}={a[i]}" for i in range(7))
+        return (f"SOLUTION cls=5 B={s.B} {terms} (anchor={s.u}) gcd={s.gcd} "
+                f"{'primitive' if s.gcd == 1 else 'NON-PRIMITIVE'}")
     return (f"SOLUTION cls={s.cls} B={s.B} u={s.u} a1={a[0]} a2={a[1]} a3={a[2]} a4={a[3]} "
             f"a5={a[4]} gcd={s.gcd} {'primitive' if s.gcd == 1 else 'NON-PRIMITIVE'}")
