@@ -127,7 +127,10 @@ typedef struct orc_hit617 {
 /* gen_class_cands(cls=5) (solve_617_v1.cu:885-906), full u band. */
 size_t orc_617_cands(uint64_t B, orc_cand617* out, size_t cap);
 /* k_find4_cls5 (solve_617_v1.cu:563-657): counters[0..4] = calls (post-gate
- * probes), gated, probes (3 slot reads per probe), tri_total, tri_skipped.
+ * probes), gated, probes (3 slot reads per probe), tri_total, tri_skipped
+ * (c4 values that reached / failed the triple-sum gate; the reference's own
+ * tri counters are 32 times these, since each of the 32 threads of the warp
+ * that walks a c4 counts it, :604-614).
  * zmax <= 1 visits every (d, c4, c3) once.  zmax > 1 restates the reference
  * launch with grid.z = zmax (gpu_run, solve_617_v1.cu:960-968): block z walks
  * c4 from lo4 + 2048 z to hi4, so c4 is visited min(zmax, (c4-lo4)/2048 + 1)
