@@ -174,6 +174,13 @@ int s615_mem_info(s615_ctx* ctx, size_t* free_bytes, size_t* total_bytes);
 /* --------------------------------------------------------------- units */
 /* unit_candidates(rt,B,cls,0,1) (fourcore_classes_v3.hpp:137-154). */
 int s615_unit_candidates(uint64_t B, int cls, uint64_t* out, size_t cap, size_t* n);
+/* gen_class_cands(cls=5) of the (6,1,7) solver (solve_617_v1.cu:885-906) over
+ * the full u band: the cls 7 units (B, u = 14u', w = 6v') with
+ * u^6 + w^6 < B^6, u' over the 6 classes with (14u')^6 = B^6 (mod 3^6), v' over
+ * the 6 classes with (6v')^6 = B^6 (mod 7^6), in the reference's order (u,
+ * then w, ascending).  Writes min(cap, count) records; *n = count;
+ * S615_E_OVERFLOW when cap is short; S615_E_ARG for B > 2,353,973. */
+int s615_617_candidates(uint64_t B, s615_unit* out, size_t cap, size_t* n);
 /* What a run does with one unit: S615_OK = searched, 1 = dropped like
  * pack_unit5 drops it (u >= B or an empty residue class), S615_E_FORMAT =
  * rejected (outside the engine's exact-arithmetic range, or a planted base

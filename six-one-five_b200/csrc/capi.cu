@@ -421,6 +421,22 @@ int s615_unit_candidates(uint64_t B, int cls, uint64_t* out, size_t cap, size_t*
   return v.size() > cap ? S615_E_OVERFLOW : S615_OK;
 }
 
+int s615_617_candidates(uint64_t B, s615_unit* out, size_t cap, size_t* n) {
+  if (!n || B > 2353973ULL || (cap && !out)) return S615_E_ARG;
+  const auto v = candidates617(B);
+  for (size_t i = 0; i < v.size() && i < cap; ++i) {
+    s615_unit x{};
+    x.cls = S615_CLS_617;
+    x.kind = 0;
+    x.B = B;
+    x.u = v[i].first;
+    x.w = (uint32_t)v[i].second;
+    out[i] = x;
+  }
+  *n = v.size();
+  return v.size() > cap ? S615_E_OVERFLOW : S615_OK;
+}
+
 // ---------------------------------------------------------- peel batches
 int s615_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch** out) {
   if (!ctx || !out || (n && !units) || n > kMaxBatchUnits) return S615_E_ARG;

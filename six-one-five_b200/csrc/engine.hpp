@@ -169,6 +169,8 @@ std::vector<u32> e_residues(u64 B);
 std::vector<u32> d_residues(u64 B, u64 u);
 std::vector<u32> d_residues_cls234(u64 B, u64 u, int cls, u32* mod, u32* fmax);
 std::vector<u64> unit_candidates(u64 B, int cls);
+// (u, w) anchor pairs of the (6,1,7) class-5 candidates of one B.
+std::vector<std::pair<u64, u64>> candidates617(u64 B);
 int free_factor(int cls);
 
 // Build the device record of one caller unit; returns S615_OK (with *skip

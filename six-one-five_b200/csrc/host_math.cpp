@@ -185,6 +185,36 @@ std::vector<u64> unit_candidates(u64 B, int cls) {
   return out;
 }
 
+// gen_class_cands(cls=5), solve_617_v1.cu:885-906: u = 14u' with (14u')^6 =
+// B^6 (mod 3^6) (the e rule of the (6,1,5) search), w = 6v' with (6v')^6 = B^6
+// (mod 7^6); residues lifted to every value <= (B-1)/14, (B-1)/6; pairs with
+// B^6 - u^6 - w^6 > 0, u ascending then w ascending.
+std::vector<std::pair<u64, u64>> candidates617(u64 B) {
+  std::vector<std::pair<u64, u64>> out;
+  if (B < 2) return out;
+  auto lift = [](const std::vector<u32>& res, u64 m, u64 maxv) {
+    std::vector<u64> v;
+    for (u32 r : res)
+      for (u64 x = (r % m) ? r % m : m; x <= maxv; x += m) v.push_back(x);
+    std::sort(v.begin(), v.end());
+    return v;
+  };
+  const long long t7 = mod_pow6((long long)(B % kM7), kM7) * mod_inv(mod_pow6(6, kM7), kM7) % kM7;
+  const auto us = lift(e_residues(B), (u64)kM3, (B - 1) / 14);
+  const auto vs = lift(roots7().by[(size_t)t7], (u64)kM7, (B - 1) / 6);
+  const u128 B6 = pow6_u128(B);
+  for (u64 up : us) {
+    const u64 u = 14 * up;
+    if (u < 1 || u > B - 1) continue;
+    const u128 u6 = pow6_u128(u);
+    for (u64 vp : vs) {
+      const u128 w6 = pow6_u128(6 * vp);
+      if (u6 < B6 && w6 < B6 - u6) out.emplace_back(u, 6 * vp);
+    }
+  }
+  return out;
+}
+
 // --------------------------------------------------------------- dev units
 namespace {
 constexpr u64 kMaxB = 40000000ULL;  // keeps d^3, (14e)^3 and the row values inside device words

@@ -101,6 +101,7 @@ SIGNATURES = {
     "s615_unit_candidates": (C.c_int, [C.c_uint64, C.c_int, _P, C.c_size_t,
                                        C.POINTER(C.c_size_t)]),
     "s615_unit_status": (C.c_int, [_P]),
+    "s615_617_candidates": (C.c_int, [C.c_uint64, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
     "s615_run": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.c_uint, _P, C.c_size_t,
                            C.POINTER(C.c_size_t), C.POINTER(Counters)]),
     "s615_cls5_run": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.c_uint, _P, C.c_size_t,
@@ -191,6 +192,18 @@ def make_plant234(cls: int, base: int, d: int, lim: int, u: int = 0, B: int = 0)
         x.base[i] = (base >> (64 * i)) & (2**64 - 1)
     x.fmax1, x.res_d, x.lim = d, d % CLS234_MOD[cls], lim
     return x
+
+
+def candidates617(B: int):
+    """s615_617_candidates: the (6,1,7) class-5 units of one B (array, count)."""
+    n = C.c_size_t(0)
+    st = lib().s615_617_candidates(B, None, 0, C.byref(n))
+    if st not in (S615_OK, -9):
+        _check(st, "617_candidates")
+    arr = (Unit * max(n.value, 1))()
+    _check(lib().s615_617_candidates(B, C.cast(arr, C.c_void_p), n.value, C.byref(n)),
+           "617_candidates")
+    return arr, n.value
 
 
 def make_units617(triples: Iterable[Tuple[int, int, int]]) -> "C.Array":

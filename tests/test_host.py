@@ -37,6 +37,8 @@ def test_struct_layouts_match_header():
     assert C.sizeof(s615.Header) == 64
     assert C.sizeof(s615.Hit) == 32      # reference Hit{u32 x5; u64 fp}
     assert C.sizeof(s615.Unit) == 72
+    assert C.sizeof(s615.Counters) == 56
+    assert C.sizeof(s615.Solution) == 120
     assert s615.HIT_DTYPE.itemsize == 32
 
 
@@ -53,6 +55,22 @@ def test_unit_candidates_match_oracle():
             continue
         for cls in (1, 2, 3, 4, 5):
             assert s615.unit_candidates(B, cls) == orc.unit_candidates(B, cls), (B, cls)
+
+
+def test_617_candidates_match_oracle():
+    # s615_617_candidates against the oracle's gen_class_cands(cls=5)
+    rng = np.random.RandomState(17)
+    Bs = [54347, 400471, 2353973] + [int(b) for b in rng.randint(12, 2_353_973, size=30)]
+    for B in Bs:
+        if B % 2 == 0 or B % 3 == 0 or B % 7 == 0:
+            continue
+        arr, n = s615.candidates617(B)
+        oarr, on = orc.cands617(B)
+        assert n == on, B
+        assert [(arr[i].u, arr[i].w) for i in range(n)] == [(oarr[i].u, oarr[i].w) for i in range(on)]
+        assert all(arr[i].cls == s615.S615_CLS_617 and arr[i].B == B for i in range(n))
+    with pytest.raises(s615.S615Error):
+        s615.candidates617(2353975)
 
 
 def test_open_without_gpu_fails_loudly():
