@@ -12,6 +12,15 @@ points ("peel probes") per second with units already resident in HBM;
 
 Multi-GPU (torchrun): each rank owns its own 20,000-B band (weak scaling),
 no collective on the data path; rank 0 prints one JSON line.
+
+  python bench.py --workload cls617 [--impl ours|reference]
+
+measures the (6,1,7) Branch-A class-5 search instead: one step is every
+candidate of the eligible B in [400,401, 400,441) (a slice of the band
+B in [400,000, 440,000]) plus 128 plants, against the N=10,476 r=48 table;
+`value` counts probes the way the reference's summary does (3 per post-gate
+xor probe).  Its reference arm runs the reference's own GPU binary
+(oracle/_ref/solve_617_v1, built from the reference sources) on the same band.
 """
 import argparse
 import ctypes as C
@@ -46,6 +55,7 @@ def parse():
     ap.add_argument("--r", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--workload", default="cls5", choices=["cls5", "cls617"])
     return ap.parse_args()
 
 
@@ -206,9 +216,227 @@ def run_reference(args, rank):
     return 0
 
 
+# ------------------------------------------------ (6,1,7) class-5 workload
+METRIC617 = "(6,1,7) Branch-A cls5 probes/sec (3 per post-gate xor probe), B in [400k,440k], 1 B200"
+UNIT617 = "probes/s"
+LO617, W617, N617, PLANTS617 = 400_401, 40, 10_476, 128
+
+
+def eligible617(B):
+    return B >= 11 and B % 2 == 1 and B % 3 != 0 and B % 7 != 0
+
+
+def plants617(n, seed, N):
+    """Planted 7-term bases in the reference's plant shape
+    (solve_617_v1.cu:1564-1582), drawn so that the planted c4 and c3 lie in
+    the windows k_find4_cls5 searches (3 c4^6 >= T, 3 c3^6 >= T - c4^6)."""
+    import numpy as np
+    rng = np.random.RandomState(seed)
+    out = []
+    while len(out) < n:
+        c = sorted(int(x) for x in rng.choice(np.arange(1, N + 1), 4, replace=False))
+        T = sum(x**6 for x in c)
+        if 3 * c[3] ** 6 < T or 3 * c[2] ** 6 < T - c[3] ** 6:
+            continue
+        d = int(rng.randint(1, 281))
+        out.append((c, d, (21 * d) ** 6 + 42**6 * T))
+    return out
+
+
+def run617(args, rank, world, local, dist):
+    import numpy as np
+    import torch
+
+    import s615
+
+    torch.cuda.set_device(local)
+    width = args.band_width if args.band_width != BAND_W else W617
+    lo = (args.band_lo if args.band_lo != BAND_LO else LO617) + rank * width
+    hi = lo + width
+    N = args.N or N617
+    eng = s615.Engine(local)
+    t0 = time.perf_counter()
+    tid = eng.build_table(N, args.r)
+    build_s = time.perf_counter() - t0
+    Bs = [B for B in range(lo, hi) if eligible617(B)]
+    cands = []
+    for B in Bs:
+        arr, n = s615.candidates617(B)
+        cands += [arr[i] for i in range(n)]
+    plants = plants617(PLANTS617, 617 + rank, N)
+    n = len(cands) + len(plants)
+    units = (s615.Unit * n)()
+    for i, x in enumerate(cands):
+        units[i] = x
+    for j, (c, d, base) in enumerate(plants):
+        units[len(cands) + j] = s615.make_plant617(base, d, N, B=42 * N + 1)
+    log(f"rank {rank}: {len(Bs)} B in [{lo}, {hi}): {len(cands)} candidates + {len(plants)} plants")
+
+    lib = s615.lib()
+    batch = C.c_void_p()
+    s615._check(lib.s615_prepare(eng._ctx, C.cast(units, C.c_void_p), n, C.byref(batch)), "prepare")
+    stream = torch.cuda.Stream()
+    sptr = C.c_void_p(stream.cuda_stream)
+
+    def step():
+        s615._check(lib.s615_run_batch(eng._ctx, tid, batch, 0, sptr), "run_batch")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    launches0 = eng.launches
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev[0].record(stream)
+    for k in range(args.steps):
+        step()
+        ev[k + 1].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    cl = clocks.stop()
+    launches = eng.launches - launches0
+    per_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[args.steps])
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+
+    hits = (s615.Hit * (1 << 20))()
+    nh = C.c_size_t(0)
+    ctr = s615.Counters()
+    s615._check(lib.s615_batch_results(eng._ctx, batch, C.cast(hits, C.c_void_p), 1 << 20,
+                                       C.byref(nh), C.byref(ctr)), "results")
+    harr = s615.hits_to_array(hits, nh.value)
+    sols = eng.verify(units, n, harr, N)
+    got = {(s.unit, tuple(sorted((s.c1, s.c2, s.c3, s.c4))), s.d) for s in sols if s.kind == 1}
+    recovered = sum(1 for j, (c, d, _) in enumerate(plants)
+                    if (len(cands) + j, tuple(c), d) in got)
+    solutions = [s615.solution_line(s) for s in sols if s.kind == 0]
+    ref_probes = 3 * ctr.probes                     # the reference's "probes" (3 per call)
+    value = ref_probes * world * args.steps / (total_ms / 1e3)
+    step_s = total_ms / args.steps / 1e3
+
+    # e2e: s615_run with host unit records in and hits + counters out
+    e2e_steps = max(1, min(args.steps, 2))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        h2, c2 = eng.run(tid, units, n, hit_cap=1 << 16)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    assert c2.probes == ctr.probes and c2.tri_total == ctr.tri_total
+
+    peak, peak_kind = measured_peaks()
+    achieved = ctr.probes * PROBE_BYTES / (statistics.mean(per_ms) / 1e3) / 1e9
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs (burst)",
+            "traffic": None, "algorithmic_bytes_per_launch": ctr.probes * PROBE_BYTES}
+
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        import orc
+        hb, pk = eng.export_table(tid)
+        ot = orc.Table.from_memory(hb, pk)
+        cores = os.cpu_count() or 1
+        # a bounded sample: 2 candidates per host thread, evenly spaced over the
+        # step's candidates, one OpenMP run over them
+        allc = orc.concat617([orc.cands617(B) for B in Bs])
+        idx = np.linspace(0, allc[1] - 1, min(allc[1], 2 * cores)).astype(int)
+        samp = (orc.OrcCand617 * len(idx))()
+        for k, i in enumerate(idx):
+            samp[k] = allc[0][i]
+        t0 = time.perf_counter()
+        _, c = orc.run617(ot, samp, len(idx), threads=cores)
+        took = time.perf_counter() - t0
+        cpu = {"value": 3 * c[0] / took, "unit": UNIT617, "cores": cores, "kind": "port",
+               "sample": f"{len(idx)} evenly spaced candidates of the step ({c[0]} post-gate probes "
+                         f"in {took:.1f} s; oracle restatement of k_find4_cls5)"}
+        del ot, pk
+
+    line = {
+        "metric": METRIC617, "value": value, "unit": UNIT617, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u128", "data": "synthetic",
+        "config": {"workload": f"(6,1,7) cls5: every candidate of the {len(Bs)} eligible B in "
+                               f"[{lo}, {hi}) per rank ({len(cands)} candidates) + {len(plants)} plants; "
+                               f"xor table N={N} r={args.r} built on device",
+                   "N": N, "r": args.r,
+                   "l2": "table %.2f GB, larger than L2" % (eng.table_info(tid).device_bytes / 1e9),
+                   "parallelism": f"replicas-by-band x{world}"},
+        "B_per_hour": len(Bs) * world / step_s * 3600,
+        "c3_points_per_s": ctr.pos * world / step_s,
+        "counters": {"c3_points": ctr.pos, "gated": ctr.gated, "post_gate_probes": ctr.probes,
+                     "tri_total": ctr.tri_total, "tri_skipped": ctr.tri_skipped, "hits": ctr.hits},
+        "plants_recovered": f"{recovered}/{len(plants)}", "solutions": solutions,
+        "table_build_s": round(build_s, 2),
+        "e2e": {"value": ref_probes / e2e_s, "unit": UNIT617,
+                "h2d_bytes_per_step": n * C.sizeof(s615.Unit), "d2h_bytes_per_step": 56 + len(h2) * 32},
+        "gpu_launches": launches,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": cl,
+    }
+    s615._check(lib.s615_batch_free(eng._ctx, batch), "batch_free")
+    eng.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run617_reference(args, rank):
+    """--workload cls617 --impl reference: the reference's own GPU binary
+    (solve_617_v1, compiled from the reference sources into oracle/_ref) on
+    the same band; its summary's kernel time and probe rate."""
+    if rank != 0:
+        return 0
+    exe = os.path.join(ROOT, "oracle", "_ref", "solve_617_v1")
+    width = args.band_width if args.band_width != BAND_W else W617
+    lo = args.band_lo if args.band_lo != BAND_LO else LO617
+    hi = lo + width - 1
+    base = {"impl": "reference", "metric": METRIC617, "unit": UNIT617}
+    if not os.path.exists(exe):
+        print(json.dumps({**base, "unavailable": "oracle/_ref/solve_617_v1 not built"}), flush=True)
+        return 0
+    rates, secs = [], []
+    for s in range(max(1, args.steps)):
+        p = subprocess.run([exe, str(lo), str(hi), "5", "--branch-a-only", "--r", str(args.r),
+                            "--quiet"], capture_output=True, text=True, timeout=3600)
+        import re
+        m = re.search(r"cls5: cands=(\d+) probes=(\S+) kernel=([\d.]+)s rate=(\S+) probes/s", p.stderr)
+        if p.returncode != 0 or not m:
+            print(json.dumps({**base, "unavailable": "solve_617_v1 failed: " +
+                              " ".join(p.stderr.strip().splitlines()[-2:])}), flush=True)
+            return 0
+        rates.append(float(m.group(4)))
+        secs.append(float(m.group(3)))
+    v = statistics.mean(rates)
+    line = {**base, "value": v, "n_gpus": 1, "steps": len(rates), "warmup": 0,
+            "ms_per_step": statistics.mean(secs) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u128", "data": "synthetic",
+            "config": {"workload": f"(6,1,7) cls5 band B in [{lo}, {hi}], reference solve_617_v1 "
+                                   f"--branch-a-only --r {args.r} (table N={hi // 42} built on the host)"},
+            "cpu_baseline": None,
+            "e2e": {"value": v, "unit": UNIT617, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "kernel time as the reference's summary prints it (k_find4_cls5 launches only)"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     rank, world, local, dist = dist_setup(args)
+    if args.workload == "cls617":
+        if args.impl == "reference":
+            return run617_reference(args, rank)
+        return run617(args, rank, world, local, dist)
     if args.impl == "reference":
         return run_reference(args, rank)
 
