@@ -129,7 +129,7 @@ def measured_peaks():
 
 def profiled_traffic():
     """DRAM bytes per post-gate probe from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "cls5_sieve_band3p2M.md")
+    path = os.path.join(ROOT, "profiles", "k_peel_cls5_band3p2M.md")
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_probe:"):

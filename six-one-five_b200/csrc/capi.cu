@@ -454,6 +454,10 @@ int s615_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch** o
     unit_items(d, (u32)du.size(), d.cls == S615_CLS_617 ? items617 : b->host_items);
     du.push_back(d);
   }
+  // heaviest first: a candidate's first rows (smallest d) have the largest T
+  // and windows, so every candidate's chunk 0 goes out before any chunk 1
+  std::stable_sort(items617.begin(), items617.end(),
+                   [](u64 a, u64 b) { return item_chunk(a) < item_chunk(b); });
   b->n_units = du.size();
   b->n_main = b->host_items.size();
   b->host_items.insert(b->host_items.end(), items617.begin(), items617.end());
@@ -503,7 +507,8 @@ int s615_run_batch(s615_ctx* ctx, int id, s615_batch* b, unsigned flags, void* s
   S615_CU(cudaMemsetAsync(b->d_ctr, 0, sizeof(Cls5Counters) + 64, st));
   if (!(flags & S615_F_PLAIN)) return launch_peel(ctx, tv, b, flags, st, 0);
   // Plain form: one unit per launch and a sync after each, like the
-  // reference's per-chunk loop.
+  // reference's per-chunk loop.  (cls 7 items go out heaviest first, so a
+  // cls 7 unit's items are not contiguous: each run of them is one launch.)
   s615_batch one;   // a view of one unit's items; its vectors stay empty
   one.d_units = b->d_units;
   one.d_hits = b->d_hits;

@@ -73,6 +73,10 @@ struct Cls5Counters {  // device accumulators (u64 atomics)
 
 // Work items: (unit, residue index, chunk of kItemRows rows) packed in a u64.
 constexpr u32 kItemRows = 64;
+// (6,1,7) rows carry a whole c4 window each: 8 rows per item keep the
+// heaviest item short next to a pass.
+constexpr u32 kItemRows617 = 8;
+S615_HD u32 item_rows(u32 cls) { return cls == 7u ? kItemRows617 : kItemRows; }
 constexpr u32 kMaxBatchUnits = 1u << 24;
 S615_HD u64 make_item(u32 unit, u32 ires, u32 chunk) {
   return ((u64)unit << 32) | ((u64)ires << 24) | chunk;

@@ -392,11 +392,12 @@ int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip) {
 }
 
 void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out) {
+  const u32 per = item_rows(d.cls);
   for (u32 ir = 0; ir < d.nres1; ++ir) {
     u32 jmin = 0, jend = 0;
     class_rows(d.res1[ir], d.mod1, d.fmax1, &jmin, &jend);
     const u32 rows = jend > jmin ? jend - jmin : 0;
-    for (u32 c = 0; c * kItemRows < rows; ++c) out.push_back(make_item(unit_index, ir, c));
+    for (u32 c = 0; c * per < rows; ++c) out.push_back(make_item(unit_index, ir, c));
   }
 }
 

@@ -4,7 +4,8 @@
 // launches with one block per (candidate, d) and c4 tiles of 2048, and gives
 // its raw hits and its calls / gated / tri_total / tri_skipped counters.
 //
-//  * Rows d (the x21 term, one lane each, 64 per work item):
+//  * Rows d (the x21 term, one lane each, 8 per work item; items are handed
+//    out smallest d first, where T and both windows are largest):
 //      T = (base - (21d)^6) / 42^6, exact (< 2^95) from base mod 2^128 and
 //      the 2-adic inverse of 21^6; the c4 window [lo4, hi4] with
 //      hi4 = min(iroot6(T), lim) and lo4 the least c with 3 c^6 >= T
@@ -251,8 +252,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_peel617(Peel617Params P) {
     I.lim = U->lim;
     u32 jmin, jend;
     class_rows(I.r0, I.mod, U->fmax1, &jmin, &jend);
-    I.j0 = jmin + item_chunk(packed) * kItemRows;
-    const u32 nrows = min(kItemRows, jend - I.j0);
+    I.j0 = jmin + item_chunk(packed) * kItemRows617;
+    const u32 nrows = min(kItemRows617, jend - I.j0);
     const u128 base = ((u128)U->base_hi << 64) | U->base_lo;
     S.nbuf = 0; S.head = 0; S.qlen = 0;
     __syncwarp();
