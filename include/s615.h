@@ -13,7 +13,7 @@
  * Host-buffer entry points copy in and out themselves; *_dev entry points take
  * device pointers and a cudaStream_t passed as void*.
  * A context is not thread-safe, except that s615_submit may be called from any
- * thread while one thread calls s615_poll.
+ * thread while one thread calls s615_poll (serving, below).
  */
 #ifndef S615_H
 #define S615_H
@@ -37,6 +37,7 @@ extern "C" {
 #define S615_E_OVERFLOW (-9)   /* hit buffer too small (results incomplete) */
 #define S615_E_BUILD (-10)     /* xor peel stalled for every seed */
 #define S615_E_NOTABLE (-11)   /* unknown table id */
+#define S615_E_BUSY (-12)      /* the context is serving: stop it first */
 
 const char* s615_strerror(int status);
 
@@ -255,6 +256,43 @@ int s615_cls5_verify(s615_ctx* ctx, const s615_unit* units, size_t n_units,
  * engine's invariants (gate factorisation, exact remainder, row identity).
  * Needs no GPU.  Returns 0 on success, else the number of the failed check. */
 int s615_selftest_host(void);
+
+/* ------------------------------------------------------------- serving */
+/* A long-running request loop on one context (no counterpart in the
+ * reference, which runs one campaign per process).  s615_submit queues a copy
+ * of the caller's units and returns a ticket; a worker thread takes every
+ * pending request for the same (table, flags) -- up to max_batch_units units
+ * -- as one batch, launches it on one of `slots` streams as soon as a stream
+ * is free and its buffers fit the HBM budget (requests that arrive meanwhile
+ * join the next batch: continuous batching), verifies its hits and splits the
+ * results back per request.  A request's hits and solutions are the same as
+ * those of s615_run + s615_verify on its units alone.  While serving, calls
+ * that allocate or launch on the context (s615_run, s615_prepare,
+ * s615_verify, table loads/builds/frees) return S615_E_BUSY. */
+typedef struct s615_result {
+  uint64_t ticket;
+  int32_t status;                  /* S615_OK or the batch's error status */
+  int32_t table_id;
+  uint64_t n_units;
+  uint64_t n_hits, n_solutions;
+  const s615_hit* hits;            /* unit = index into this request's units */
+  const s615_solution* solutions;  /* both owned by the library until s615_release */
+  s615_counters counters;          /* of the whole batch that carried the request */
+  uint32_t batch_requests;         /* requests in that batch */
+  uint32_t pad;
+  double queued_ms;                /* submit -> launch */
+  double latency_ms;               /* submit -> result ready (verified) */
+} s615_result;
+/* slots: batches in flight (1..16); max_batch_units: 0 = 2^20. */
+int s615_serve_start(s615_ctx* ctx, int slots, size_t max_batch_units);
+int s615_submit(s615_ctx* ctx, int table_id, const s615_unit* units, size_t n, unsigned flags,
+                uint64_t* ticket);
+/* Finished requests, oldest first; waits up to wait_ms for the first one. */
+int s615_poll(s615_ctx* ctx, s615_result* out, size_t cap, size_t* n, int wait_ms);
+int s615_release(s615_ctx* ctx, uint64_t ticket);
+/* Stops accepting requests, finishes every submitted one, joins the worker;
+ * finished results stay readable until released or s615_close. */
+int s615_serve_stop(s615_ctx* ctx);
 
 #ifdef __cplusplus
 }

@@ -129,6 +129,7 @@ const char* s615_strerror(int s) {
     case S615_E_OVERFLOW: return "result buffer overflow";
     case S615_E_BUILD: return "xor peel stalled for every seed";
     case S615_E_NOTABLE: return "unknown table id";
+    case S615_E_BUSY: return "context is serving";
   }
   return "unknown status";
 }
@@ -171,6 +172,7 @@ int s615_open(int device, size_t hbm_budget, s615_ctx** out) {
 int s615_close(s615_ctx* ctx) {
   if (!ctx) return S615_E_ARG;
   cudaSetDevice(ctx->device);
+  server_destroy(ctx);
   for (auto& kv : ctx->tables) free_table(ctx, kv.second);
   ctx->tables.clear();
   dev_free(ctx, ctx->d_pat, (4 * kPatWords + kTriWords) * sizeof(u32));
@@ -194,6 +196,7 @@ int s615_get_table_info(s615_ctx* ctx, int id, s615_table_info* info) {
 
 int s615_free_table(s615_ctx* ctx, int id) {
   if (!ctx) return S615_E_ARG;
+  if (serving_blocks(ctx)) return S615_E_BUSY;
   DevTable* t = find_table(ctx, id);
   if (!t) return S615_E_NOTABLE;
   cudaSetDevice(ctx->device);
@@ -256,6 +259,7 @@ static int smoke_table(s615_ctx* ctx, int id) {
 
 int s615_load_table(s615_ctx* ctx, const char* path, int expected_N, int layout, int* table_id) {
   if (!ctx || !path) return S615_E_ARG;
+  if (serving_blocks(ctx)) return S615_E_BUSY;
   cudaSetDevice(ctx->device);
   FILE* f = std::fopen(path, "rb");
   if (!f) return S615_E_IO;
@@ -356,6 +360,7 @@ int s615_save_table(s615_ctx* ctx, int id, const char* path) {
 
 int s615_build_table(s615_ctx* ctx, int N, int r, int layout, int* table_id) {
   if (!ctx || N < 1 || N > 4 * kNSoftMax || r < 8 || r > 64) return S615_E_ARG;
+  if (serving_blocks(ctx)) return S615_E_BUSY;
   cudaSetDevice(ctx->device);
   // distinct values of i^6 mod 2^64 (many i collide 2-adically)
   std::vector<u64> vals((size_t)N);
@@ -383,6 +388,7 @@ int s615_build_table(s615_ctx* ctx, int N, int r, int layout, int* table_id) {
 int s615_build_table_keys(s615_ctx* ctx, const uint64_t* keys, size_t n, int r, uint64_t base_seed,
                           int layout, int* table_id) {
   if (!ctx || (n && !keys) || r < 1 || r > 64) return S615_E_ARG;
+  if (serving_blocks(ctx)) return S615_E_BUSY;
   cudaSetDevice(ctx->device);
   void* dk = nullptr;
   int s = dev_alloc(ctx, &dk, std::max<size_t>(n, 1) * 8);
@@ -440,6 +446,7 @@ int s615_617_candidates(uint64_t B, s615_unit* out, size_t cap, size_t* n) {
 // ---------------------------------------------------------- peel batches
 int s615_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch** out) {
   if (!ctx || !out || (n && !units) || n > kMaxBatchUnits) return S615_E_ARG;
+  if (serving_blocks(ctx)) return S615_E_BUSY;
   cudaSetDevice(ctx->device);
   std::unique_ptr<s615_batch> b(new s615_batch());
   std::vector<DevUnit> du;
@@ -579,6 +586,7 @@ int s615_cls5_run(s615_ctx* ctx, int id, const s615_unit* units, size_t n, unsig
 int s615_verify(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s615_hit* hits,
                 size_t n_hits, int N, s615_solution* out, size_t cap, size_t* n_out) {
   if (!ctx || !n_out || N < 1) return S615_E_ARG;
+  if (serving_blocks(ctx)) return S615_E_BUSY;
   cudaSetDevice(ctx->device);
   return verify_device(ctx, units, n_units, hits, n_hits, N, out, cap, n_out);
 }

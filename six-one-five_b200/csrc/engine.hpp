@@ -92,6 +92,10 @@ S615_HD void class_rows(u32 r0, u32 mod, u32 fmax, u32* jmin, u32* jend) {
 
 }  // namespace s615
 
+namespace s615 {
+struct Server;   // serve.cpp
+}
+
 struct s615_batch {
   size_t n_units = 0, n_items = 0;
   size_t n_main = 0;             // items [0, n_main) are classes 2-5, the rest cls 7
@@ -115,6 +119,7 @@ struct s615_ctx {
   int num_sms = 0;
   unsigned long long launches = 0;
   std::mutex mu;
+  s615::Server* server = nullptr;   // the serving loop, when started
 };
 
 namespace s615 {
@@ -126,6 +131,11 @@ int cuda_status(cudaError_t e);
     cudaError_t _e = (x);                            \
     if (_e != cudaSuccess) return ::s615::cuda_status(_e); \
   } while (0)
+
+// Serving: true when a request loop owns the context and the caller is not
+// its worker thread (calls that allocate or launch then return S615_E_BUSY).
+bool serving_blocks(s615_ctx* ctx);
+void server_destroy(s615_ctx* ctx);   // stops the loop (draining it) and frees it
 
 // Budgeted device allocation.
 int dev_alloc(s615_ctx* ctx, void** p, size_t bytes);

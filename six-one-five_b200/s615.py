@@ -19,7 +19,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libs615.so")
 S615_OK = 0
 STATUS = {
     -1: "ARG", -2: "IO", -3: "FORMAT", -4: "N_MISMATCH", -5: "FPR_SMOKE", -6: "OOM",
-    -7: "DEVICE", -8: "TIMEOUT", -9: "OVERFLOW", -10: "BUILD", -11: "NOTABLE",
+    -7: "DEVICE", -8: "TIMEOUT", -9: "OVERFLOW", -10: "BUILD", -11: "NOTABLE", -12: "BUSY",
 }
 LAYOUT_AUTO, LAYOUT_PACKED, LAYOUT_WIDE = 0, 1, 2
 F_NO_GATE, F_PLAIN, F_NO_TRI = 1, 2, 4
@@ -70,6 +70,14 @@ class Solution(C.Structure):
                 ("c4", C.c_uint32), ("w", C.c_uint32), ("a", C.c_int64 * 7), ("gcd", C.c_int64)]
 
 
+class Result(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("status", C.c_int32), ("table_id", C.c_int32),
+                ("n_units", C.c_uint64), ("n_hits", C.c_uint64), ("n_solutions", C.c_uint64),
+                ("hits", C.POINTER(Hit)), ("solutions", C.POINTER(Solution)),
+                ("counters", Counters), ("batch_requests", C.c_uint32), ("pad", C.c_uint32),
+                ("queued_ms", C.c_double), ("latency_ms", C.c_double)]
+
+
 assert C.sizeof(Header) == 64
 assert C.sizeof(Hit) == 32
 assert C.sizeof(Unit) == 72
@@ -118,6 +126,11 @@ SIGNATURES = {
     "s615_cls5_verify": (C.c_int, [_P, _P, C.c_size_t, _P, C.c_size_t, C.c_int, _P, C.c_size_t,
                                    C.POINTER(C.c_size_t)]),
     "s615_selftest_host": (C.c_int, []),
+    "s615_serve_start": (C.c_int, [_P, C.c_int, C.c_size_t]),
+    "s615_submit": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.c_uint, C.POINTER(C.c_uint64)]),
+    "s615_poll": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(C.c_size_t), C.c_int]),
+    "s615_release": (C.c_int, [_P, C.c_uint64]),
+    "s615_serve_stop": (C.c_int, [_P]),
 }
 
 _lib: Optional[C.CDLL] = None
@@ -226,6 +239,13 @@ def make_plant617(base: int, d: int, lim: int, B: int = 0, u: int = 14, w: int =
     return x
 
 
+def s615_hits_copy(ptr, n: int) -> np.ndarray:
+    if n == 0:
+        return np.zeros(0, dtype=HIT_DTYPE)
+    raw = C.string_at(C.cast(ptr, C.c_void_p), n * C.sizeof(Hit))
+    return np.frombuffer(raw, dtype=HIT_DTYPE).copy()
+
+
 def hits_to_array(hits, n: int) -> np.ndarray:
     raw = np.frombuffer(C.string_at(C.addressof(hits), n * C.sizeof(Hit)), dtype=HIT_DTYPE)
     return raw.copy()
@@ -314,6 +334,38 @@ class Engine:
 
     def cls5_run(self, tid: int, units, n: int, flags: int = 0, hit_cap: int = 1 << 20):
         return self.run(tid, units, n, flags, hit_cap, entry="s615_cls5_run")
+
+    # ---- serving (s615_serve_start / submit / poll / release / serve_stop)
+    def serve_start(self, slots: int = 2, max_batch_units: int = 0) -> None:
+        _check(lib().s615_serve_start(self._ctx, slots, max_batch_units), "serve_start")
+
+    def submit(self, tid: int, units, n: int, flags: int = 0) -> int:
+        t = C.c_uint64(0)
+        _check(lib().s615_submit(self._ctx, tid, C.cast(units, C.c_void_p), n, flags, C.byref(t)),
+               "submit")
+        return t.value
+
+    def poll(self, cap: int = 64, wait_ms: int = 100):
+        """Finished requests: list of dicts with the hits and solutions copied
+        out (the library's copies are released)."""
+        out = (Result * cap)()
+        n = C.c_size_t(0)
+        _check(lib().s615_poll(self._ctx, C.cast(out, C.c_void_p), cap, C.byref(n), wait_ms), "poll")
+        res = []
+        for i in range(n.value):
+            r = out[i]
+            hits = (s615_hits_copy(r.hits, r.n_hits))
+            sols = [Solution.from_buffer_copy(r.solutions[k]) for k in range(r.n_solutions)]
+            res.append({"ticket": r.ticket, "status": r.status, "table_id": r.table_id,
+                        "n_units": r.n_units, "hits": hits, "solutions": sols,
+                        "counters": Counters.from_buffer_copy(r.counters),
+                        "batch_requests": r.batch_requests, "queued_ms": r.queued_ms,
+                        "latency_ms": r.latency_ms})
+            _check(lib().s615_release(self._ctx, r.ticket), "release")
+        return res
+
+    def serve_stop(self) -> None:
+        _check(lib().s615_serve_stop(self._ctx), "serve_stop")
 
     def verify(self, units, n_units: int, hits: np.ndarray, N: int, cap: int = 4096):
         h = np.ascontiguousarray(hits.astype(HIT_DTYPE))
