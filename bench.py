@@ -143,6 +143,57 @@ def log(msg):
     print(f"[bench] {msg}", file=sys.stderr, flush=True)
 
 
+def batch_h2d(lib, batch):
+    """Bytes s615_prepare copied host-to-device for this batch (unit records +
+    work items), the same the C-ABI entry points copy per call."""
+    nu, ni, hb = C.c_size_t(0), C.c_size_t(0), C.c_size_t(0)
+    lib.s615_batch_size(batch, C.byref(nu), C.byref(ni), C.byref(hb))
+    return hb.value
+
+
+def serve_latency(eng, tid, units, N, rate=5000.0, secs=4.0, req_units=50, seed=5):
+    """Per-unit latency under a Poisson stream of requests through the serving
+    loop (s615_submit / s615_poll): `rate` units/s in requests of `req_units`
+    units drawn from the band; a unit's latency is its request's
+    submit-to-verified-result time."""
+    import numpy as np
+
+    import s615
+    import workloads as W
+    rng = np.random.RandomState(seed)
+    eng.serve_start(slots=2)
+    lat, batch_reqs, sent = [], [], 0
+    try:
+        t0 = time.perf_counter()
+        nxt = t0
+        done = 0
+        while time.perf_counter() - t0 < secs:
+            now = time.perf_counter()
+            while nxt <= now:
+                pick = [units[i] for i in rng.randint(0, len(units), size=req_units)]
+                arr, n = W.unit_array(pick, [], N)
+                eng.submit(tid, arr, n)
+                sent += 1
+                nxt += rng.exponential(req_units / rate)
+            for r in eng.poll(wait_ms=1):
+                lat += [r["latency_ms"]] * r["n_units"]
+                batch_reqs.append(r["batch_requests"])
+                done += 1
+            time.sleep(max(0.0, min(0.001, nxt - time.perf_counter())))
+        while done < sent:
+            for r in eng.poll(wait_ms=100):
+                lat += [r["latency_ms"]] * r["n_units"]
+                batch_reqs.append(r["batch_requests"])
+                done += 1
+    finally:
+        eng.serve_stop()
+    lat = np.array(lat)
+    return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "units": int(lat.size), "requests": sent, "offered_units_per_s": rate,
+            "request_units": req_units, "mean_requests_per_batch": float(np.mean(batch_reqs)),
+            "loop": "s615_serve_start(slots=2) + s615_submit/s615_poll, Poisson arrivals"}
+
+
 def band_units(lo, hi):
     import workloads as W
     return W.cls5_units(lo, hi)
@@ -337,6 +388,12 @@ def run617(args, rank, world, local, dist):
             "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs (burst)",
             "traffic": None, "algorithmic_bytes_per_launch": ctr.probes * PROBE_BYTES}
 
+    # per-unit latency through the serving loop under a config-5-like stream
+    serve = None
+    if rank == 0 and not args.no_plain:
+        serve = serve_latency(eng, tid, units, N)
+        log(f"serving: p50 {serve['p50_ms']:.1f} ms, p99 {serve['p99_ms']:.1f} ms per unit")
+
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         import orc
@@ -375,7 +432,8 @@ def run617(args, rank, world, local, dist):
         "plants_recovered": f"{recovered}/{len(plants)}", "solutions": solutions,
         "table_build_s": round(build_s, 2),
         "e2e": {"value": ref_probes / e2e_s, "unit": UNIT617,
-                "h2d_bytes_per_step": n * C.sizeof(s615.Unit), "d2h_bytes_per_step": 56 + len(h2) * 32},
+                "h2d_bytes_per_step": batch_h2d(lib, batch),
+                "d2h_bytes_per_step": C.sizeof(s615.Counters) + len(h2) * 32},
         "gpu_launches": launches,
         "roofline": roof,
         "cpu_baseline": cpu,
@@ -521,14 +579,14 @@ def main():
 
     # e2e: the public C ABI with host buffers (unit records up, hits + counters down)
     e2e_steps = max(1, min(args.steps, 3))
-    h2d = n * 152 + 6 * n * 4
+    h2d = batch_h2d(lib, batch)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         h2, c2 = eng.cls5_run(tid, arr, n, hit_cap=1 << 16)
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     log(f"e2e through s615_cls5_run: {e2e_s * 1e3:.1f} ms per step (device step {total_ms / args.steps:.1f} ms)")
     assert c2.pos == ctr.pos and c2.probes == ctr.probes
-    d2h = 40 + len(h2) * 32
+    d2h = C.sizeof(s615.Counters) + len(h2) * 32
 
     peak, peak_kind = measured_peaks()
     dur_s = statistics.mean(per_ms) / 1e3
@@ -553,6 +611,12 @@ def main():
                  "eligible_B_per_hour": p_rate / (ctr.pos / eligible_count(lo, hi - 1)) * 3600,
                  "batched_over_plain": value / world / p_rate}
 
+    # per-unit latency through the serving loop under a config-5-like stream
+    serve = None
+    if rank == 0 and not args.no_plain:
+        serve = serve_latency(eng, tid, units, N)
+        log(f"serving: p50 {serve['p50_ms']:.1f} ms, p99 {serve['p99_ms']:.1f} ms per unit")
+
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         import orc
@@ -572,7 +636,9 @@ def main():
                    "l2": "inputs larger than L2 (table %.1f GB)" % (eng.table_info(tid).device_bytes / 1e9),
                    "parallelism": f"replicas-by-band x{world}"},
         "eligible_B_per_hour": eligible * args.steps / (total_ms / 1e3) * 3600,
-        "p99_unit_latency_ms": None,
+        "p99_unit_latency_ms": serve["p99_ms"] if serve else None,
+        "p50_unit_latency_ms": serve["p50_ms"] if serve else None,
+        "serving": serve,
         "counters": {"calls": ctr.calls * world, "gated": ctr.gated * world,
                      "probes": ctr.probes * world, "pos": pos_all},
         "plants_recovered": f"{recovered}/{N_PLANTS}", "solutions": solutions,

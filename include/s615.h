@@ -218,6 +218,9 @@ int s615_run_batch(s615_ctx* ctx, int table_id, s615_batch* b, unsigned flags, v
 int s615_batch_results(s615_ctx* ctx, s615_batch* b, s615_hit* hits, size_t hit_cap,
                        size_t* n_hits, s615_counters* counters);
 int s615_batch_free(s615_ctx* ctx, s615_batch* b);
+/* What s615_prepare copied to the device: unit records, work items and the
+ * host-to-device bytes of both (no counterpart in the reference). */
+int s615_batch_size(const s615_batch* b, size_t* n_units, size_t* n_items, size_t* h2d_bytes);
 
 /* No counterpart in the reference.  s615_cls5_run for callers that cannot
  * allocate device memory when they search: their free HBM is owned by another

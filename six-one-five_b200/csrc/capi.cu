@@ -495,6 +495,14 @@ int s615_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch** o
   return S615_OK;
 }
 
+int s615_batch_size(const s615_batch* b, size_t* n_units, size_t* n_items, size_t* h2d_bytes) {
+  if (!b) return S615_E_ARG;
+  if (n_units) *n_units = b->n_units;
+  if (n_items) *n_items = b->n_items;
+  if (h2d_bytes) *h2d_bytes = b->n_units * sizeof(DevUnit) + b->n_items * sizeof(u64);
+  return S615_OK;
+}
+
 int s615_batch_free(s615_ctx* ctx, s615_batch* b) {
   if (!ctx || !b) return S615_E_ARG;
   dev_free(ctx, b->d_units, std::max<size_t>(b->n_units, 1) * sizeof(DevUnit));

@@ -121,6 +121,8 @@ SIGNATURES = {
     "s615_batch_results": (C.c_int, [_P, _P, _P, C.c_size_t, C.POINTER(C.c_size_t),
                                      C.POINTER(Counters)]),
     "s615_batch_free": (C.c_int, [_P, _P]),
+    "s615_batch_size": (C.c_int, [_P, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
+                                  C.POINTER(C.c_size_t)]),
     "s615_verify": (C.c_int, [_P, _P, C.c_size_t, _P, C.c_size_t, C.c_int, _P, C.c_size_t,
                               C.POINTER(C.c_size_t)]),
     "s615_cls5_verify": (C.c_int, [_P, _P, C.c_size_t, _P, C.c_size_t, C.c_int, _P, C.c_size_t,
