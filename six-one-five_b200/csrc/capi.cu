@@ -173,6 +173,7 @@ int s615_close(s615_ctx* ctx) {
   if (!ctx) return S615_E_ARG;
   cudaSetDevice(ctx->device);
   server_destroy(ctx);
+  for (int k = 0; k < 4; ++k) dev_free(ctx, ctx->arena[k], ctx->arena_cap[k]);
   for (auto& kv : ctx->tables) free_table(ctx, kv.second);
   ctx->tables.clear();
   dev_free(ctx, ctx->d_pat, (4 * kPatWords + kTriWords) * sizeof(u32));
@@ -444,11 +445,28 @@ int s615_617_candidates(uint64_t B, s615_unit* out, size_t cap, size_t* n) {
 }
 
 // ---------------------------------------------------------- peel batches
-int s615_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch** out) {
-  if (!ctx || !out || (n && !units) || n > kMaxBatchUnits) return S615_E_ARG;
-  if (serving_blocks(ctx)) return S615_E_BUSY;
-  cudaSetDevice(ctx->device);
-  std::unique_ptr<s615_batch> b(new s615_batch());
+}  // extern "C"
+
+namespace s615 {
+
+int arena_get(s615_ctx* ctx, int k, size_t bytes, void** p) {
+  if (bytes > ctx->arena_cap[k]) {
+    dev_free(ctx, ctx->arena[k], ctx->arena_cap[k]);
+    ctx->arena[k] = nullptr;
+    ctx->arena_cap[k] = 0;
+    const size_t want = std::max<size_t>(bytes + bytes / 4, 4096);
+    void* q = nullptr;
+    const int s = dev_alloc(ctx, &q, want);
+    if (s) return s;
+    ctx->arena[k] = q;
+    ctx->arena_cap[k] = want;
+  }
+  *p = ctx->arena[k];
+  return S615_OK;
+}
+
+int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
+  b->host_items.clear();
   std::vector<DevUnit> du;
   du.reserve(n);
   std::vector<u64> items617;   // the (6,1,7) kernel's items go after the others
@@ -471,26 +489,53 @@ int s615_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch** o
   b->n_items = b->host_items.size();
   int s = 0;
   void* p = nullptr;
-  if ((s = dev_alloc(ctx, &p, std::max<size_t>(du.size(), 1) * sizeof(DevUnit)))) return s;
-  b->d_units = static_cast<DevUnit*>(p);
-  if ((s = dev_alloc(ctx, &p, std::max<size_t>(b->n_items, 1) * sizeof(u64)))) {
-    s615_batch_free(ctx, b.release());
-    return s;
+  if (!b->d_units || du.size() > b->cap_units) {
+    dev_free(ctx, b->d_units, b->cap_units * sizeof(DevUnit));
+    b->d_units = nullptr;
+    const size_t cap = std::max<size_t>(du.size(), 1);
+    if ((s = dev_alloc(ctx, &p, cap * sizeof(DevUnit)))) { b->cap_units = 0; return s; }
+    b->d_units = static_cast<DevUnit*>(p);
+    b->cap_units = cap;
   }
-  b->d_items = static_cast<u64*>(p);
-  if ((s = dev_alloc(ctx, &p, sizeof(Cls5Counters) + 64))) { s615_batch_free(ctx, b.release()); return s; }
-  b->d_ctr = static_cast<Cls5Counters*>(p);
-  b->d_work = reinterpret_cast<u32*>(static_cast<char*>(p) + sizeof(Cls5Counters));
-  b->hit_cap = 1u << 20;
-  if ((s = dev_alloc(ctx, &p, (size_t)b->hit_cap * sizeof(s615_hit)))) {
-    s615_batch_free(ctx, b.release());
-    return s;
+  if (!b->d_items || b->n_items > b->cap_items) {
+    dev_free(ctx, b->d_items, b->cap_items * sizeof(u64));
+    b->d_items = nullptr;
+    const size_t cap = std::max<size_t>(b->n_items, 1);
+    if ((s = dev_alloc(ctx, &p, cap * sizeof(u64)))) { b->cap_items = 0; return s; }
+    b->d_items = static_cast<u64*>(p);
+    b->cap_items = cap;
   }
-  b->d_hits = static_cast<s615_hit*>(p);
+  if (!b->d_ctr) {
+    if ((s = dev_alloc(ctx, &p, sizeof(Cls5Counters) + 64))) return s;
+    b->d_ctr = static_cast<Cls5Counters*>(p);
+    b->d_work = reinterpret_cast<u32*>(static_cast<char*>(p) + sizeof(Cls5Counters));
+  }
+  if (!b->d_hits) {
+    if ((s = dev_alloc(ctx, &p, (size_t)(1u << 20) * sizeof(s615_hit)))) return s;
+    b->d_hits = static_cast<s615_hit*>(p);
+    b->hit_cap = 1u << 20;
+  }
   if (!du.empty())
     S615_CU(cudaMemcpy(b->d_units, du.data(), du.size() * sizeof(DevUnit), cudaMemcpyHostToDevice));
   if (b->n_items)
     S615_CU(cudaMemcpy(b->d_items, b->host_items.data(), b->n_items * sizeof(u64), cudaMemcpyHostToDevice));
+  return S615_OK;
+}
+
+}  // namespace s615
+
+extern "C" {
+
+int s615_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch** out) {
+  if (!ctx || !out || (n && !units) || n > kMaxBatchUnits) return S615_E_ARG;
+  if (serving_blocks(ctx)) return S615_E_BUSY;
+  cudaSetDevice(ctx->device);
+  std::unique_ptr<s615_batch> b(new s615_batch());
+  const int s = fill_batch(ctx, units, n, b.get());
+  if (s) {
+    s615_batch_free(ctx, b.release());
+    return s;
+  }
   *out = b.release();
   return S615_OK;
 }
@@ -505,8 +550,8 @@ int s615_batch_size(const s615_batch* b, size_t* n_units, size_t* n_items, size_
 
 int s615_batch_free(s615_ctx* ctx, s615_batch* b) {
   if (!ctx || !b) return S615_E_ARG;
-  dev_free(ctx, b->d_units, std::max<size_t>(b->n_units, 1) * sizeof(DevUnit));
-  dev_free(ctx, b->d_items, std::max<size_t>(b->n_items, 1) * sizeof(u64));
+  dev_free(ctx, b->d_units, b->cap_units * sizeof(DevUnit));
+  dev_free(ctx, b->d_items, b->cap_items * sizeof(u64));
   dev_free(ctx, b->d_ctr, sizeof(Cls5Counters) + 64);
   dev_free(ctx, b->d_hits, (size_t)b->hit_cap * sizeof(s615_hit));
   delete b;

@@ -103,6 +103,7 @@ struct s615_batch {
   s615::u64* d_items = nullptr;
   s615_hit* d_hits = nullptr;
   s615::u32 hit_cap = 0;
+  size_t cap_units = 0, cap_items = 0;   // device capacity (a reused batch only grows)
   s615::Cls5Counters* d_ctr = nullptr;
   s615::u32* d_work = nullptr;   // persistent-queue cursors [classes 2-5, cls 7]
   std::vector<s615::u64> host_items;
@@ -120,6 +121,8 @@ struct s615_ctx {
   unsigned long long launches = 0;
   std::mutex mu;
   s615::Server* server = nullptr;   // the serving loop, when started
+  void* arena[4] = {};              // verify scratch, grow-only (units, hits, pairs, count)
+  size_t arena_cap[4] = {};
 };
 
 namespace s615 {
@@ -140,6 +143,12 @@ void server_destroy(s615_ctx* ctx);   // stops the loop (draining it) and frees 
 // Budgeted device allocation.
 int dev_alloc(s615_ctx* ctx, void** p, size_t bytes);
 void dev_free(s615_ctx* ctx, void* p, size_t bytes);
+// Grow-only scratch slot k of the context (no free, so no device-wide sync
+// once it is large enough).
+int arena_get(s615_ctx* ctx, int k, size_t bytes, void** p);
+// Pack units into batch b (new or reused: its device buffers only grow) and
+// copy them to the device.
+int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b);
 
 TableView view_of(const DevTable& t);
 

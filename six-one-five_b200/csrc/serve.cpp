@@ -19,6 +19,8 @@
 //    s615_poll and stay readable until s615_release.
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -53,6 +55,8 @@ struct Done {
 };
 
 struct Flight {
+  Clock::time_point t_take, t_launched;
+  double prep_ms = 0;
   std::vector<Req> reqs;
   std::vector<s615_unit> all;
   s615_batch* b = nullptr;
@@ -81,7 +85,9 @@ struct Server {
   uint64_t next_ticket = 1;
   std::vector<cudaStream_t> streams;
   std::vector<bool> busy;
+  std::vector<s615_batch*> slot_batch;   // one reused batch per stream slot
   std::thread th;
+  bool trace = std::getenv("S615_TRACE") != nullptr;   // per-batch phase times on stderr
 
   void complete(std::vector<Req>& reqs, int status, const Flight* f,
                 const std::vector<s615_hit>* hits, const std::vector<s615_solution>* sols,
@@ -131,14 +137,17 @@ struct Server {
 
   // Download, verify and split one finished batch.
   void finish(Flight& f, int status) {
+    const auto t_done = Clock::now();
     std::vector<s615_hit> hits;
     std::vector<s615_solution> sols;
     s615_counters ctr{};
-    if (status == S615_OK) {
-      hits.resize(f.b->hit_cap);
+    if (status == S615_OK) {   // counters first, then exactly the hits there are
       size_t nh = 0;
-      status = s615_batch_results(ctx, f.b, hits.data(), hits.size(), &nh, &ctr);
-      hits.resize(std::min(nh, hits.size()));
+      status = s615_batch_results(ctx, f.b, nullptr, 0, &nh, &ctr);
+      if (status == S615_E_OVERFLOW && nh <= f.b->hit_cap) {
+        hits.resize(nh);
+        status = s615_batch_results(ctx, f.b, hits.data(), nh, &nh, &ctr);
+      }
     }
     if (status == S615_OK && !hits.empty()) {
       const DevTable* t = nullptr;
@@ -154,8 +163,13 @@ struct Server {
         sols.resize(std::min(ns, sols.size()));
       }
     }
-    if (f.b) s615_batch_free(ctx, f.b);
-    f.b = nullptr;
+    const auto t_verified = Clock::now();
+    if (trace)
+      std::fprintf(stderr,
+                   "[s615 serve] batch of %zu requests / %zu units: prepare %.2f ms, "
+                   "device %.2f ms, results+verify %.2f ms, free %.2f ms\n",
+                   f.reqs.size(), f.all.size(), f.prep_ms, ms_between(f.t_launched, t_done),
+                   ms_between(t_done, t_verified), ms_between(t_verified, Clock::now()));
     if (f.ev) cudaEventDestroy(f.ev);
     f.ev = nullptr;
     busy[f.slot] = false;
@@ -209,7 +223,13 @@ struct Server {
         Flight f;
         if (!take_batch(f)) break;
         for (const Req& q : f.reqs) f.all.insert(f.all.end(), q.units.begin(), q.units.end());
-        int s = s615_prepare(ctx, f.all.data(), f.all.size(), &f.b);
+        int slot = 0;
+        while (busy[slot]) ++slot;
+        if (!slot_batch[slot]) slot_batch[slot] = new s615_batch();
+        f.t_take = Clock::now();
+        f.b = slot_batch[slot];
+        int s = fill_batch(ctx, f.all.data(), f.all.size(), f.b);
+        f.prep_ms = ms_between(f.t_take, Clock::now());
         if (s == S615_E_OOM && !flights.empty()) {   // wait for memory to free up
           put_back(f);
           break;
@@ -218,8 +238,6 @@ struct Server {
           complete(f.reqs, s, nullptr, nullptr, nullptr, nullptr);
           continue;
         }
-        int slot = 0;
-        while (busy[slot]) ++slot;
         f.slot = slot;
         busy[slot] = true;
         const auto now = Clock::now();
@@ -228,6 +246,7 @@ struct Server {
         if (s == S615_OK && cudaEventCreateWithFlags(&f.ev, cudaEventDisableTiming) != cudaSuccess)
           s = S615_E_DEVICE;
         if (s == S615_OK && cudaEventRecord(f.ev, streams[slot]) != cudaSuccess) s = S615_E_DEVICE;
+        f.t_launched = Clock::now();
         if (s != S615_OK) {
           cudaStreamSynchronize(streams[slot]);
           finish(f, s);
@@ -251,6 +270,8 @@ bool serving_blocks(s615_ctx* ctx) { return ctx && ctx->server && ctx->server->r
 void server_destroy(s615_ctx* ctx) {
   if (!ctx || !ctx->server) return;
   s615_serve_stop(ctx);
+  for (s615_batch* b : ctx->server->slot_batch)
+    if (b) s615_batch_free(ctx, b);
   for (cudaStream_t s : ctx->server->streams) cudaStreamDestroy(s);
   delete ctx->server;
   ctx->server = nullptr;
@@ -272,6 +293,7 @@ int s615_serve_start(s615_ctx* ctx, int slots, size_t max_batch_units) {
   sv->slots = slots;
   sv->max_units = max_batch_units ? std::min<size_t>(max_batch_units, kMaxBatchUnits) : (1u << 20);
   sv->busy.assign(slots, false);
+  sv->slot_batch.assign(slots, nullptr);
   for (int i = 0; i < slots; ++i) {
     cudaStream_t s = nullptr;
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {

@@ -102,20 +102,15 @@ int verify_device(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s
   for (size_t i = 0; i < n_hits; ++i)
     if (hits[i].unit >= n_units) return S615_E_ARG;
   const u32 pcap = (u32)std::min<size_t>(std::max<size_t>(4 * n_hits + 64, 1024), 1u << 26);
+  // scratch from the context's grow-only arena: no cudaFree, so no
+  // device-wide sync against kernels running on other streams
   void *d_u = nullptr, *d_h = nullptr, *d_p = nullptr, *d_n = nullptr;
   const size_t bu = du.size() * sizeof(DevUnit), bh = n_hits * sizeof(s615_hit);
   const size_t bp = pcap * sizeof(PairOut);
   int s = 0;
-  if ((s = dev_alloc(ctx, &d_u, bu))) return s;
-  if ((s = dev_alloc(ctx, &d_h, bh))) { dev_free(ctx, d_u, bu); return s; }
-  if ((s = dev_alloc(ctx, &d_p, bp))) { dev_free(ctx, d_u, bu); dev_free(ctx, d_h, bh); return s; }
-  if ((s = dev_alloc(ctx, &d_n, 16))) {
-    dev_free(ctx, d_u, bu); dev_free(ctx, d_h, bh); dev_free(ctx, d_p, bp);
+  if ((s = arena_get(ctx, 0, bu, &d_u)) || (s = arena_get(ctx, 1, bh, &d_h)) ||
+      (s = arena_get(ctx, 2, bp, &d_p)) || (s = arena_get(ctx, 3, 16, &d_n)))
     return s;
-  }
-  auto cleanup = [&]() {
-    dev_free(ctx, d_u, bu); dev_free(ctx, d_h, bh); dev_free(ctx, d_p, bp); dev_free(ctx, d_n, 16);
-  };
   cudaStream_t st = ctx->stream;
   std::vector<PairOut> pairs;
   u32 np = 0;
@@ -135,12 +130,12 @@ int verify_device(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(&np, d_n, 4, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e == cudaSuccess && np > pcap) { cleanup(); return S615_E_OVERFLOW; }
+    if (e == cudaSuccess && np > pcap) return S615_E_OVERFLOW;
     if (e == cudaSuccess) {
       pairs.resize(np);
-      if (np) e = cudaMemcpy(pairs.data(), d_p, np * sizeof(PairOut), cudaMemcpyDeviceToHost);
+      if (np) e = cudaMemcpyAsync(pairs.data(), d_p, np * sizeof(PairOut), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     }
-    cleanup();
     if (e != cudaSuccess) return cuda_status(e);
   }
   std::sort(pairs.begin(), pairs.end(), [&](const PairOut& a, const PairOut& b) {
