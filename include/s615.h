@@ -161,6 +161,10 @@ int s615_save_table(s615_ctx* ctx, int table_id, const char* path);
  * reference's XorFilter::packed. *len receives the byte count. */
 int s615_export_table(s615_ctx* ctx, int table_id, s615_header* hdr, uint8_t* buf, size_t cap,
                       size_t* len);
+/* xor_fpr_smoke (fourcore_xor_store.hpp:54-65) on a resident table: hits
+ * among 200,000 fixed non-member keys (the loaders refuse > 16; the (6,1,7)
+ * solver refuses > 8, solve_617_v1.cu:1829-1833). */
+int s615_fpr_smoke(s615_ctx* ctx, int table_id, int* hits);
 int s615_get_table_info(s615_ctx* ctx, int table_id, s615_table_info* info);
 int s615_free_table(s615_ctx* ctx, int table_id);
 /* xor_might_contain (xor_filter.hpp:472-483) for n host keys -> out[i] 0/1. */

@@ -242,10 +242,13 @@ int s615_xor_query(s615_ctx* ctx, int id, const uint64_t* keys, size_t n, uint8_
 }
 
 // xor_fpr_smoke (fourcore_xor_store.hpp:54-65): 200k keys x <- x*phi + 1 from
-// 0x123456789abcdef0 through the device query; refuse more than 16 hits.
-static int smoke_table(s615_ctx* ctx, int id) {
+// 0x123456789abcdef0 through the device query; the number of hits.
+int s615_fpr_smoke(s615_ctx* ctx, int id, int* hits) {
+  if (!ctx || !hits) return S615_E_ARG;
   DevTable* t = find_table(ctx, id);
-  if (t->hdr.m_cells < 3 || t->hdr.r == 0 || !t->d_cells) return S615_E_FPR_SMOKE;
+  if (!t) return S615_E_NOTABLE;
+  *hits = 200000;
+  if (t->hdr.m_cells < 3 || t->hdr.r == 0 || !t->d_cells) return S615_OK;
   const size_t n = 200000;
   std::vector<u64> keys(n);
   u64 x = 0x123456789abcdef0ULL;
@@ -253,8 +256,17 @@ static int smoke_table(s615_ctx* ctx, int id) {
   std::vector<u8> out(n);
   const int s = s615_xor_query(ctx, id, keys.data(), n, out.data());
   if (s) return s;
-  size_t hits = 0;
-  for (u8 v : out) hits += v;
+  int c = 0;
+  for (u8 v : out) c += v;
+  *hits = c;
+  return S615_OK;
+}
+
+// Refuse more than 16 hits (fourcore_cls5_gpu_v4.cu:576-579).
+static int smoke_table(s615_ctx* ctx, int id) {
+  int hits = 0;
+  const int s = s615_fpr_smoke(ctx, id, &hits);
+  if (s) return s;
   return hits > 16 ? S615_E_FPR_SMOKE : S615_OK;
 }
 

@@ -103,6 +103,7 @@ SIGNATURES = {
                                     C.POINTER(C.c_size_t)]),
     "s615_get_table_info": (C.c_int, [_P, C.c_int, C.POINTER(TableInfo)]),
     "s615_free_table": (C.c_int, [_P, C.c_int]),
+    "s615_fpr_smoke": (C.c_int, [_P, C.c_int, C.POINTER(C.c_int)]),
     "s615_xor_query": (C.c_int, [_P, C.c_int, _P, C.c_size_t, _P]),
     "s615_xor_query_dev": (C.c_int, [_P, C.c_int, _P, C.c_size_t, _P, _P]),
     "s615_mem_info": (C.c_int, [_P, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
