@@ -237,7 +237,7 @@ def run_reference(args, rank):
         return 0
     import orc
     lo, hi = args.band_lo, args.band_lo + args.band_width
-    units = band_units(lo, hi)
+    units = band_units(lo, hi - 1)
     # the reference's host table builder needs hours and ~100 GB at N=76,667;
     # the reference arm probes a host-built N=2000 table (probes are ~1% of points)
     table = orc.Table.build_pairs(2000, args.r)
@@ -354,10 +354,6 @@ def run617(args, rank, world, local, dist):
     launches = eng.launches - launches0
     per_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
     total_ms = ev[0].elapsed_time(ev[args.steps])
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
 
     hits = (s615.Hit * (1 << 20))()
     nh = C.c_size_t(0)
@@ -370,8 +366,11 @@ def run617(args, rank, world, local, dist):
     recovered = sum(1 for j, (c, d, _) in enumerate(plants)
                     if (len(cands) + j, tuple(c), d) in got)
     solutions = [s615.solution_line(s) for s in sols if s.kind == 0]
+    import shard
+    total_ms, tot = shard.merge(dist, "cuda", total_ms,
+                                {"probes": ctr.probes, "pos": ctr.pos, "B": len(Bs)})
     ref_probes = 3 * ctr.probes                     # the reference's "probes" (3 per call)
-    value = ref_probes * world * args.steps / (total_ms / 1e3)
+    value = 3 * tot["probes"] * args.steps / (total_ms / 1e3)
     step_s = total_ms / args.steps / 1e3
 
     # e2e: s615_run with host unit records in and hits + counters out
@@ -425,8 +424,8 @@ def run617(args, rank, world, local, dist):
                    "N": N, "r": args.r,
                    "l2": "table %.2f GB, larger than L2" % (eng.table_info(tid).device_bytes / 1e9),
                    "parallelism": f"replicas-by-band x{world}"},
-        "B_per_hour": len(Bs) * world / step_s * 3600,
-        "c3_points_per_s": ctr.pos * world / step_s,
+        "B_per_hour": tot["B"] / step_s * 3600,
+        "c3_points_per_s": tot["pos"] / step_s,
         "counters": {"c3_points": ctr.pos, "gated": ctr.gated, "post_gate_probes": ctr.probes,
                      "tri_total": ctr.tri_total, "tri_skipped": ctr.tri_skipped, "hits": ctr.hits},
         "plants_recovered": f"{recovered}/{len(plants)}", "solutions": solutions,
@@ -502,18 +501,18 @@ def main():
     import torch
 
     import s615
+    import shard
     import workloads as W
 
     torch.cuda.set_device(local)
-    lo = args.band_lo + rank * args.band_width
-    hi = lo + args.band_width
-    N = args.N or math.ceil((args.band_lo + world * args.band_width) / 42)
+    lo, hi = shard.rank_band(args.band_lo, args.band_width, rank)
+    N = args.N or shard.table_N(args.band_lo, args.band_width, world)
     eng = s615.Engine(local)
     t0 = time.perf_counter()
     tid = eng.build_table(N, args.r)
     build_s = time.perf_counter() - t0
     log(f"rank {rank}: table N={N} r={args.r} built in {build_s:.1f} s")
-    units = band_units(lo, hi)
+    units = band_units(lo, hi - 1)   # B in [lo, hi): bands of ranks do not overlap
     log(f"rank {rank}: {len(units)} units in [{lo}, {hi})")
     plants = W.plants(N_PLANTS, 1000 + rank, lo, hi, N)
     arr, n = W.unit_array(units, plants, N)
@@ -552,16 +551,16 @@ def main():
     launches = eng.launches - launches0
     per_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
     total_ms = ev[0].elapsed_time(ev[args.steps])
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
 
     hits = (s615.Hit * (1 << 20))()
     nh = C.c_size_t(0)
     ctr = s615.Counters()
     s615._check(lib.s615_batch_results(eng._ctx, batch, C.cast(hits, C.c_void_p), 1 << 20,
                                             C.byref(nh), C.byref(ctr)), "results")
+    # slowest rank's time, counters summed over ranks
+    total_ms, tot = shard.merge(dist, "cuda", total_ms,
+                                {"calls": ctr.calls, "gated": ctr.gated, "probes": ctr.probes,
+                                 "pos": ctr.pos, "eligible": eligible_count(lo, hi - 1)})
     harr = s615.hits_to_array(hits, nh.value)
     log(f"timed {args.steps} steps: {total_ms:.1f} ms; pos={ctr.pos} probes={ctr.probes} hits={nh.value}")
     sols = eng.verify(arr, n, harr, N)
@@ -572,9 +571,9 @@ def main():
                     if (len(units) + j, p.d, p.e, p.c1, p.c2) in got)
     solutions = [s615.solution_line(s) for s in sols if s.kind == 0]
 
-    pos_all = ctr.pos * world
+    pos_all = tot["pos"]
     value = pos_all * args.steps / (total_ms / 1e3)
-    eligible = eligible_count(lo, hi - 1) * world
+    eligible = tot["eligible"]
     ms_step = total_ms / args.steps
 
     # e2e: the public C ABI with host buffers (unit records up, hits + counters down)
@@ -639,8 +638,8 @@ def main():
         "p99_unit_latency_ms": serve["p99_ms"] if serve else None,
         "p50_unit_latency_ms": serve["p50_ms"] if serve else None,
         "serving": serve,
-        "counters": {"calls": ctr.calls * world, "gated": ctr.gated * world,
-                     "probes": ctr.probes * world, "pos": pos_all},
+        "counters": {"calls": tot["calls"], "gated": tot["gated"], "probes": tot["probes"],
+                     "pos": pos_all},
         "plants_recovered": f"{recovered}/{N_PLANTS}", "solutions": solutions,
         "table_build_s": round(build_s, 2),
         "e2e": {"value": ctr.pos / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
