@@ -5,7 +5,11 @@
 // acquire_xor_filter's FATAL paths, the SOLUTION and "---- done" lines).
 // Extra flags: --dump-survivors F (one "B u d e fp" line per raw filter hit,
 // reference naming: d is the x21 term, e the x14 term), --plain (one unit per
-// launch), --layout packed|wide, --batch K (units per device batch).
+// launch), --layout packed|wide, --batch K (units per device batch),
+// --plant COUNT[:SEED] (adds planted targets in the reference's plant shape,
+// solve_516_v3.cu:1130-1170, and reports how many were recovered) and
+// --serve (reads .buc lines from stdin and runs them through the serving
+// loop as they arrive, printing SOLUTION lines as their requests finish).
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -29,7 +33,8 @@ void usage() {
       "                 [--stop-first] [--device K]\n"
       "                 [--load-table F] [--save-table F]\n"
       "                 [--allow-rebuild] [--dump-survivors F] [--plain]\n"
-      "                 [--layout packed|wide] [--batch K]\n"
+      "                 [--layout packed|wide] [--batch K] [--plant COUNT[:SEED]]\n"
+      "   or: s615_cls5 --serve --N K [--load-table F] [--r BITS] [--batch K] < units.buc\n"
       "   or: s615_cls5 --check-table --N K --load-table F\n"
       "                 [--r BITS] [--save-table F] [--allow-rebuild]\n"
       "  --load-table F: packed xor from xor_build_save / --save-table.\n"
@@ -50,6 +55,56 @@ int selftest_host() {
 }
 
 struct Line { int cls; unsigned long long B, u; };
+
+using u64 = unsigned long long;
+using u128 = unsigned __int128;
+struct W3 { u64 l[3]; };
+W3 pow6_w3(u64 x) {   // x < 2^32
+  const u128 x2 = (u128)x * x, x4 = x2 * x2;
+  const u128 lo = (u128)(u64)x4 * (u64)x2, hi = (u128)(u64)(x4 >> 64) * (u64)x2;
+  const u128 mid = (lo >> 64) + (u128)(u64)hi;
+  return W3{{(u64)lo, (u64)mid, (u64)(hi >> 64) + (u64)(mid >> 64)}};
+}
+void add_w3(W3& a, const W3& b) {
+  u128 c = 0;
+  for (int i = 0; i < 3; ++i) { c += (u128)a.l[i] + b.l[i]; a.l[i] = (u64)c; c >>= 64; }
+}
+W3 mul_w3(const W3& a, u64 m) {
+  W3 r;
+  u128 c = 0;
+  for (int i = 0; i < 3; ++i) { c += (u128)a.l[i] * m; r.l[i] = (u64)c; c >>= 64; }
+  return r;
+}
+
+// Planted class-5 targets: base = (14e)^6 + (21d)^6 + 42^6 (c1^6 + c2^6), one
+// residue per axis and fmax = the planted value, c1 < c2 <= N.
+struct Plant { unsigned e, d, c1, c2; };
+std::vector<Plant> make_plants(int count, u64 seed, u64 B_max, int N, std::vector<s615_unit>& out) {
+  std::vector<Plant> ps;
+  u64 x = seed * 0x9E3779B97F4A7C15ULL + 615;
+  auto rnd = [&](u64 m) { x = x * 6364136223846793005ULL + 1442695040888963407ULL; return (x >> 17) % m; };
+  while ((int)ps.size() < count) {
+    Plant p;
+    p.e = 1 + (unsigned)rnd((B_max - 1) / 14);
+    p.d = 1 + (unsigned)rnd((B_max - 1) / 21);
+    p.c1 = 1 + (unsigned)rnd(N);
+    p.c2 = 1 + (unsigned)rnd(N);
+    if (p.c1 >= p.c2) continue;
+    W3 base = pow6_w3(14ULL * p.e);
+    add_w3(base, pow6_w3(21ULL * p.d));
+    W3 core = pow6_w3(p.c1);
+    add_w3(core, pow6_w3(p.c2));
+    add_w3(base, mul_w3(core, 5489031744ULL));   // 42^6
+    s615_unit U{};
+    U.cls = 5; U.kind = 1;
+    for (int i = 0; i < 3; ++i) U.base[i] = base.l[i];
+    U.fmax1 = p.e; U.fmax2 = p.d; U.res_e = p.e % 729; U.res_d = p.d % 64; U.lim = (unsigned)N;
+    if (s615_unit_status(&U) != S615_OK) continue;
+    out.push_back(U);
+    ps.push_back(p);
+  }
+  return ps;
+}
 
 bool load_buc5(const char* path, std::vector<Line>& out) {  // fourcore_cls5_gpu_v4.cu:155-167
   FILE* f = std::fopen(path, "r");
@@ -121,7 +176,9 @@ int main(int argc, char** argv) {
   int device = 0, N_override = 0, xor_r = 48, layout = S615_LAYOUT_AUTO;
   size_t batch = 1 << 16;
   bool do_host = false, quiet = true, use_gate = true, stop_first = false;
-  bool allow_rebuild = false, check_table = false, plain = false;
+  bool allow_rebuild = false, check_table = false, plain = false, serve = false;
+  int plant_count = 0;
+  u64 plant_seed = 0;
   for (int i = 1; i < argc; ++i) {
     const std::string s = argv[i];
     auto next = [&]() { return (i + 1 < argc) ? std::string(argv[++i]) : std::string(); };
@@ -142,6 +199,13 @@ int main(int argc, char** argv) {
     else if (s == "--check-table") check_table = true;
     else if (s == "--dump-survivors") dump_path = next();
     else if (s == "--plain") plain = true;
+    else if (s == "--serve") serve = true;
+    else if (s == "--plant") {
+      const std::string v = next();
+      plant_count = std::atoi(v.c_str());
+      const size_t c = v.find(':');
+      if (c != std::string::npos) plant_seed = std::strtoull(v.c_str() + c + 1, nullptr, 10);
+    }
     else if (s == "--batch") batch = (size_t)std::max(1, std::atoi(next().c_str()));
     else if (s == "--layout") {
       const std::string v = next();
@@ -158,6 +222,8 @@ int main(int argc, char** argv) {
       std::fprintf(stderr, "N=%d exceeds soft xor cap %d\n", N_override, kNSoftMax);
       return 1;
     }
+  } else if (serve) {
+    if (N_override <= 0) { std::fprintf(stderr, "--serve needs --N\n"); return 1; }
   } else if (units_path.empty()) {
     usage();
     return 1;
@@ -181,6 +247,74 @@ int main(int argc, char** argv) {
     s615_get_table_info(ctx, tid, &info);
     std::fprintf(stderr, "[cls5-gpu] --check-table OK N=%d r=%d packed=%.3f GB\n", N_override, xor_r,
                  (double)(info.hdr.m_cells * info.hdr.r / 8 + 8) / 1e9);
+    s615_close(ctx);
+    return 0;
+  }
+
+  if (serve) {   // units stream in on stdin; one request per --batch lines (or at EOF)
+    int tid = 0;
+    if (!acquire(ctx, N_override, xor_r, load_table, save_table, allow_rebuild, layout, tid)) {
+      s615_close(ctx);
+      return 1;
+    }
+    const unsigned flags = use_gate ? 0u : S615_F_NO_GATE;
+    if ((s = s615_serve_start(ctx, 2, 0))) {
+      std::fprintf(stderr, "[cls5-gpu] serve: %s\n", s615_strerror(s));
+      s615_close(ctx);
+      return 1;
+    }
+    std::vector<s615_unit> pend;
+    size_t submitted = 0, finished = 0, n_units = 0;
+    unsigned long long sols = 0, calls = 0, probes = 0;
+    std::vector<s615_result> res(64);
+    auto drain = [&](int wait_ms) {
+      size_t k = 0;
+      s615_poll(ctx, res.data(), res.size(), &k, wait_ms);
+      for (size_t i = 0; i < k; ++i) {
+        const s615_result& R = res[i];
+        if (R.status) std::fprintf(stderr, "[cls5-gpu] request %llu: %s\n", (u64)R.ticket, s615_strerror(R.status));
+        for (u64 j = 0; j < R.n_solutions; ++j) {
+          const s615_solution& S = R.solutions[j];
+          if (S.kind != 0) continue;
+          std::printf("SOLUTION cls=5 B=%llu u=%llu a1=%lld a2=%lld a3=%lld a4=%lld a5=%lld gcd=%lld %s\n",
+                      (u64)S.B, (u64)S.u, (long long)S.a[0], (long long)S.a[1], (long long)S.a[2],
+                      (long long)S.a[3], (long long)S.a[4], (long long)S.gcd,
+                      S.gcd == 1 ? "primitive" : "NON-PRIMITIVE");
+          ++sols;
+        }
+        if (!quiet)
+          std::fprintf(stderr, "[cls5-gpu] request %llu: %llu units, %.1f ms\n", (u64)R.ticket,
+                       (u64)R.n_units, R.latency_ms);
+        s615_release(ctx, R.ticket);
+        ++finished;
+      }
+    };
+    auto submit = [&]() {
+      if (pend.empty()) return;
+      uint64_t t = 0;
+      if (s615_submit(ctx, tid, pend.data(), pend.size(), flags, &t) == S615_OK) ++submitted;
+      n_units += pend.size();
+      pend.clear();
+    };
+    const auto t0 = Clock::now();
+    char buf[256];
+    while (std::fgets(buf, sizeof buf, stdin)) {
+      int cls;
+      u64 B, u;
+      if (std::sscanf(buf, "%d %llu %llu", &cls, &B, &u) != 3 || cls != 5) continue;
+      s615_unit U{};
+      U.cls = 5; U.B = B; U.u = u;
+      if (s615_unit_status(&U) != S615_OK) continue;
+      pend.push_back(U);
+      if (pend.size() >= batch) submit();
+      drain(0);
+    }
+    submit();
+    while (finished < submitted) drain(100);
+    s615_serve_stop(ctx);
+    (void)calls; (void)probes;
+    std::printf("---- done cls5-gpu serve: solutions=%llu units=%zu requests=%zu time=%.1fs ----\n", sols,
+                n_units, submitted, std::chrono::duration<double>(Clock::now() - t0).count());
     s615_close(ctx);
     return 0;
   }
@@ -216,6 +350,15 @@ int main(int argc, char** argv) {
     return 1;
   }
   std::fprintf(stderr, "[cls5-gpu] N=%d r=%d\n", N, xor_r);
+  std::vector<Plant> plants;
+  const size_t n_stage1 = units.size();
+  if (plant_count > 0) {
+    u64 bmax = 0;
+    for (size_t i = 0; i < n_stage1; ++i) bmax = std::max<u64>(bmax, units[i].B);
+    plants = make_plants(plant_count, plant_seed, bmax, N, units);
+    std::fprintf(stderr, "[plant] %d planted targets after %zu units\n", plant_count, n_stage1);
+  }
+  std::vector<char> plant_got(plants.size(), 0);
   int tid = 0;
   if (!acquire(ctx, N, xor_r, load_table, save_table, allow_rebuild, layout, tid)) {
     s615_close(ctx);
@@ -267,6 +410,14 @@ int main(int argc, char** argv) {
       }
       for (size_t k = 0; k < std::min(ns, scap); ++k) {
         const s615_solution& S = solv[k];
+        if (S.kind == 1) {   // a recovered plant: its exact planted (e, d, c1, c2)?
+          const size_t pi = off + S.unit - n_stage1;
+          if (off + S.unit >= n_stage1 && pi < plants.size()) {
+            const Plant& P = plants[pi];
+            if (S.e == P.e && S.d == P.d && S.c1 == P.c1 && S.c2 == P.c2) plant_got[pi] = 1;
+          }
+          continue;
+        }
         if (S.kind != 0) continue;
         std::printf("SOLUTION cls=5 B=%llu u=%llu a1=%lld a2=%lld a3=%lld a4=%lld a5=%lld gcd=%lld %s\n",
                     (unsigned long long)S.B, (unsigned long long)S.u, (long long)S.a[0],
@@ -285,6 +436,11 @@ int main(int argc, char** argv) {
     if (stop_first && sols) break;
   }
   if (dump) std::fclose(dump);
+  if (!plants.empty()) {
+    size_t got = 0;
+    for (char g : plant_got) got += g;
+    std::fprintf(stderr, "[plant] recovered %zu/%zu\n", got, plants.size());
+  }
   const double sec = std::chrono::duration<double>(Clock::now() - t0).count();
   std::printf("---- done cls5-gpu: solutions=%llu units=%zu calls=%llu probes=%llu time=%.1fs ----\n",
               sols, units.size(), tot_calls, tot_probes, sec);

@@ -82,3 +82,23 @@ def test_cls5_cli_counters_equal_oracle(tmp_path, oracle_table):
     _, (calls, gated, probes) = orc.cls5_run(t, arr, len(units))
     assert (int(m.group(2)), int(m.group(3)), int(m.group(4))) == (len(units), calls, probes)
     assert int(m.group(1)) == 0 and "SOLUTION" not in p.stdout
+
+
+def test_cls5_cli_plants_and_serve(tmp_path, oracle_table):
+    N = 715
+    _, path = oracle_table(N, 48)
+    units = W.cls5_units(1000, 30000)
+    buc = tmp_path / "u.buc"
+    W.write_buc(str(buc), units)
+    p = subprocess.run([BIN5, "--units", str(buc), "--N", str(N), "--load-table", path,
+                        "--plant", "16:3"], capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr
+    assert "[plant] recovered 16/16" in p.stderr
+    # the same units streamed through the serving loop, 100 per request
+    with open(buc) as f:
+        p = subprocess.run([BIN5, "--serve", "--N", str(N), "--load-table", path, "--batch", "100"],
+                           stdin=f, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr
+    m = re.search(r"---- done cls5-gpu serve: solutions=(\d+) units=(\d+) requests=(\d+)", p.stdout)
+    assert m and int(m.group(2)) == len(units) and int(m.group(3)) == (len(units) + 99) // 100
+    assert int(m.group(1)) == 0
