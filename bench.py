@@ -151,6 +151,27 @@ def batch_h2d(lib, batch):
     return hb.value
 
 
+def timed_steps(lib, eng, tid, batch, stream, flags, steps):
+    """CUDA-event time of `steps` back-to-back s615_run_batch calls (ms) and
+    the counters of the last one."""
+    import torch
+
+    import s615
+    sptr = C.c_void_p(stream.cuda_stream)
+    s615._check(lib.s615_run_batch(eng._ctx, tid, batch, flags, sptr), "run_batch")   # warm
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        s615._check(lib.s615_run_batch(eng._ctx, tid, batch, flags, sptr), "run_batch")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ctr = s615.Counters()
+    nh = C.c_size_t(0)
+    lib.s615_batch_results(eng._ctx, batch, None, 0, C.byref(nh), C.byref(ctr))
+    return e0.elapsed_time(e1), ctr
+
+
 def serve_latency(eng, tid, units, N, rate=5000.0, secs=4.0, req_units=50, seed=5):
     """Per-unit latency under a Poisson stream of requests through the serving
     loop (s615_submit / s615_poll): `rate` units/s in requests of `req_units`
@@ -381,11 +402,28 @@ def run617(args, rank, world, local, dist):
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     assert c2.probes == ctr.probes and c2.tri_total == ctr.tri_total
 
+    sharp = None
+    if rank == 0:
+        sms, sctr = timed_steps(lib, eng, tid, batch, stream, s615.F_SHARP, 1)
+        sharp = {"value": 3 * sctr.probes / (sms / 1e3), "ms_per_step": sms,
+                 "post_gate_probes": sctr.probes, "c3_points_per_s": sctr.pos / (sms / 1e3),
+                 "flag": "S615_F_SHARP (extra sound residue tests; raw hits a subset)"}
+
     peak, peak_kind = measured_peaks()
     achieved = ctr.probes * PROBE_BYTES / (statistics.mean(per_ms) / 1e3) / 1e9
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs (burst)",
             "traffic": None, "algorithmic_bytes_per_launch": ctr.probes * PROBE_BYTES}
+
+    # the opt-in sharper gate (S615_F_SHARP) on the same batch: same points,
+    # fewer probes, the same verified solutions (tests/test_gpu_sharp.py)
+    sharp = None
+    if rank == 0 and not args.no_plain:
+        sms, sctr = timed_steps(lib, eng, tid, batch, stream, s615.F_SHARP, 2)
+        sharp = {"value": sctr.pos * 2 / (sms / 1e3), "unit": UNIT, "ms_per_step": sms / 2,
+                 "post_gate_probes": sctr.probes, "pos": sctr.pos,
+                 "flag": "S615_F_SHARP (extra sound residue tests; raw hits a subset)"}
+        log(f"sharp gate: {sms / 2:.1f} ms per step, probes {sctr.probes}")
 
     # per-unit latency through the serving loop under a config-5-like stream
     serve = None
@@ -436,6 +474,7 @@ def run617(args, rank, world, local, dist):
         "gpu_launches": launches,
         "roofline": roof,
         "cpu_baseline": cpu,
+        "sharp_gate": sharp,
         "clocks": cl,
     }
     s615._check(lib.s615_batch_free(eng._ctx, batch), "batch_free")
@@ -610,6 +649,16 @@ def main():
                  "eligible_B_per_hour": p_rate / (ctr.pos / eligible_count(lo, hi - 1)) * 3600,
                  "batched_over_plain": value / world / p_rate}
 
+    # the opt-in sharper gate (S615_F_SHARP) on the same batch: same points,
+    # fewer probes, the same verified solutions (tests/test_gpu_sharp.py)
+    sharp = None
+    if rank == 0 and not args.no_plain:
+        sms, sctr = timed_steps(lib, eng, tid, batch, stream, s615.F_SHARP, 2)
+        sharp = {"value": sctr.pos * 2 / (sms / 1e3), "unit": UNIT, "ms_per_step": sms / 2,
+                 "post_gate_probes": sctr.probes, "pos": sctr.pos,
+                 "flag": "S615_F_SHARP (extra sound residue tests; raw hits a subset)"}
+        log(f"sharp gate: {sms / 2:.1f} ms per step, probes {sctr.probes}")
+
     # per-unit latency through the serving loop under a config-5-like stream
     serve = None
     if rank == 0 and not args.no_plain:
@@ -648,6 +697,7 @@ def main():
         "roofline": roof,
         "cpu_baseline": cpu,
         "plain_form": plain,
+        "sharp_gate": sharp,
         "clocks": cl,
     }
     s615._check(lib.s615_batch_free(eng._ctx, batch), "batch_free")

@@ -153,17 +153,21 @@ int s615_open(int device, size_t hbm_budget, s615_ctx** out) {
   ctx->budget = hbm_budget ? hbm_budget : total_b;
   // gate pattern sets: [gate cls5 | open cls5 | gate find3 | open find3],
   // then the triple-sum gate block of the (6,1,7) kernel
-  std::vector<u32> pat(4 * kPatWords + kTriWords);
+  std::vector<u32> pat(4 * kPatWords + kTriWords + 2 * kSharpWords);
   gate_patterns(true, 0, pat.data());
   gate_patterns(false, 0, pat.data() + kPatWords);
   gate_patterns(true, 1, pat.data() + 2 * kPatWords);
   gate_patterns(false, 1, pat.data() + 3 * kPatWords);
   tri_tables(pat.data() + 4 * kPatWords);
+  gate_patterns_sharp(0, pat.data() + 4 * kPatWords + kTriWords);
+  gate_patterns_sharp(1, pat.data() + 4 * kPatWords + kTriWords + kSharpWords);
   void* p = nullptr;
   const int s = dev_alloc(ctx.get(), &p, pat.size() * sizeof(u32));
   if (s) return s;
   ctx->d_pat = static_cast<u32*>(p);
   ctx->d_tri = ctx->d_pat + 4 * kPatWords;
+  ctx->d_sharp = ctx->d_tri + kTriWords;
+  ctx->p64 = pair_sums_mask64();
   S615_CU(cudaMemcpy(ctx->d_pat, pat.data(), pat.size() * sizeof(u32), cudaMemcpyHostToDevice));
   *out = ctx.release();
   return S615_OK;
@@ -176,7 +180,7 @@ int s615_close(s615_ctx* ctx) {
   for (int k = 0; k < 4; ++k) dev_free(ctx, ctx->arena[k], ctx->arena_cap[k]);
   for (auto& kv : ctx->tables) free_table(ctx, kv.second);
   ctx->tables.clear();
-  dev_free(ctx, ctx->d_pat, (4 * kPatWords + kTriWords) * sizeof(u32));
+  dev_free(ctx, ctx->d_pat, (4 * kPatWords + kTriWords + 2 * kSharpWords) * sizeof(u32));
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return S615_OK;

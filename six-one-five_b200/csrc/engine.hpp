@@ -44,6 +44,16 @@ constexpr int kPatBase[4] = {0, 81, 130, 299};
 constexpr int kPatB9 = 0, kPatB7 = 81, kPatB13 = 130, kPatB19 = 299;  // usable in device code
 constexpr int kPatWords = 660;
 
+// Sharper sound gate (S615_F_SHARP, no counterpart in the reference): T must
+// also be a sum of two sixth powers mod 64 (a 32-column mask per row), 27 and
+// 49 (in place of 9 and 7), 13, 19, 31, 37 and 43 (pattern words as above).
+// Pattern blocks per q in this order; 7,839 words per column shape.
+constexpr int kSharpQ[7] = {27, 49, 13, 19, 31, 37, 43};
+constexpr int kSharpBase[7] = {0, 729, 3130, 3299, 3660, 4621, 5990};
+constexpr int kSB27 = 0, kSB49 = 729, kSB13 = 3130, kSB19 = 3299, kSB31 = 3660, kSB37 = 4621,
+              kSB43 = 5990;
+constexpr int kSharpWords = 7839;
+
 // Triple-sum gate of solve_617_v1.cu:334-345 for the c4 step, as one
 // 400-word block: bitmaps of {a^6+b^6+c^6 mod 504} (16 words) and mod 247
 // (8 words), then c^6 mod 504 (504 u16) and c^6 mod 247 (247 u16).
@@ -117,6 +127,8 @@ struct s615_ctx {
   int next_table = 1;
   s615::u32* d_pat = nullptr;   // [gate cls5 | open cls5 | gate find3 | open find3]
   s615::u32* d_tri = nullptr;   // triple-sum gate block (kTriWords)
+  s615::u32* d_sharp = nullptr; // sharp patterns [cls5 shape | find3 shape]
+  unsigned long long p64 = 0;   // bit t: t is a sum of two sixth powers mod 64
   int num_sms = 0;
   unsigned long long launches = 0;
   std::mutex mu;
@@ -205,5 +217,7 @@ void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out);
 
 void gate_patterns(bool gated, int shape, u32 out[kPatWords]);
 void tri_tables(u32 out[kTriWords]);
+void gate_patterns_sharp(int shape, u32 out[kSharpWords]);
+u64 pair_sums_mask64();
 
 }  // namespace s615

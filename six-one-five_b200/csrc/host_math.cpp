@@ -433,6 +433,36 @@ void gate_patterns(bool gated, int shape, u32 out[kPatWords]) {
   }
 }
 
+// Sharp pattern blocks: for q in kSharpQ, the same construction as
+// gate_patterns (shape 0: x = s + 64 i, value (W - x^6)/64; shape 1: x = s + i,
+// value W - x^6), always gated.
+void gate_patterns_sharp(int shape, u32 out[kSharpWords]) {
+  const u32 step = shape == 0 ? 64 : 1, scale = shape == 0 ? 64 : 1;
+  for (int qi = 0; qi < 7; ++qi) {
+    const u32 q = (u32)kSharpQ[qi];
+    const auto ok = pair_sums_mod(q);
+    std::vector<u8> okw(q, 0);   // admissible (W - x^6) mod q
+    for (u32 t = 0; t < q; ++t) if (ok[t]) okw[(scale * t) % q] = 1;
+    for (u32 a = 0; a < q; ++a)
+      for (u32 s = 0; s < q; ++s) {
+        u32 w = 0;
+        for (u32 i = 0; i < 32; ++i) {
+          const u32 x = (s + step * i) % q;
+          const u32 v = (u32)(((long long)a - mod_pow6(x, q)) % q + q) % q;
+          if (okw[v]) w |= 1u << i;
+        }
+        out[kSharpBase[qi] + a * q + s] = w;
+      }
+  }
+}
+
+u64 pair_sums_mask64() {
+  const auto ok = pair_sums_mod(64);
+  u64 m = 0;
+  for (u32 t = 0; t < 64; ++t) if (ok[t]) m |= 1ULL << t;
+  return m;
+}
+
 // Triple-sum gate block (build_tri_set, solve_617_v1.cu:334-345): bit x of
 // the first bitmap is set iff x = a^6 + b^6 + c^6 (mod 504) for some a, b, c;
 // likewise mod 247; then the tables c^6 mod 504 and mod 247 as u16 pairs.

@@ -25,6 +25,8 @@
 //    items from one device-wide queue; nothing waits at a block barrier.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "peel_common.cuh"
 
 namespace s615 {
@@ -47,6 +49,15 @@ struct WarpSmem {                 // one warp's private slice
   u32 d0s[kMaxD];                 // cls5: d residues of the current pass
 };
 
+// With the sharp gate a cls5 row also carries the offsets for 31, 37, 43 and
+// a 32-column mod-64 mask per d residue (T mod 64 has period 32 in k).
+struct WarpSmemSharp : WarpSmem {
+  u16 offx[kRows][4];
+  u32 M32[kMaxD][kRows];
+};
+template <bool kSharp>
+using WarpT = typename std::conditional<kSharp, WarpSmemSharp, WarpSmem>::type;
+
 struct PeelParams {
   TableView tv;
   const DevUnit* units;
@@ -60,10 +71,17 @@ struct PeelParams {
   const u32* pat3;         // find3 column patterns (step 1, scale 1)
   u64 inv21_lo, inv21_hi;  // (21^6)^-1 mod 2^128
   u32 s8;                  // admissible values mod 8, as a bitmask
+  u64 p64;                 // sharp gate: admissible values mod 64, as a bitmask
 };
 
-constexpr size_t kSmemPat = 2 * kPatWords * sizeof(u32);
-constexpr size_t kSmemTotal = kSmemPat + kWarps * sizeof(WarpSmem);
+// cls5 pattern words (sharp or not) then the find3 ones, then the warp slices
+// (which start on a 16-byte boundary: the row records are 16-byte aligned).
+template <bool kSharp>
+constexpr size_t smem_pat() {
+  return ((size_t)((kSharp ? kSharpWords : kPatWords) + kPatWords) * sizeof(u32) + 15) / 16 * 16;
+}
+template <bool kSharp>
+constexpr size_t smem_total() { return smem_pat<kSharp>() + kWarps * sizeof(WarpT<kSharp>); }
 
 // x^6 mod 512 for small x.
 __device__ __forceinline__ u32 pow6_mod512(u32 x) {
@@ -133,16 +151,16 @@ __device__ __forceinline__ void push_bits(const PeelParams& P, WarpSmem& W, u32 
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 5) k_peel(PeelParams P) {
+template <bool kSharp>
+__global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
+  constexpr u32 kP5 = kSharp ? (u32)kSharpWords : (u32)kPatWords;
   u32* s_pat5 = reinterpret_cast<u32*>(smem);
-  u32* s_pat3 = s_pat5 + kPatWords;
+  u32* s_pat3 = s_pat5 + kP5;
   const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  WarpSmem& W = reinterpret_cast<WarpSmem*>(smem + kSmemPat)[warp];
-  for (u32 i = tid; i < (u32)kPatWords; i += kThreads) {
-    s_pat5[i] = P.pat5[i];
-    s_pat3[i] = P.pat3[i];
-  }
+  WarpT<kSharp>& W = reinterpret_cast<WarpT<kSharp>*>(smem + smem_pat<kSharp>())[warp];
+  for (u32 i = tid; i < kP5; i += kThreads) s_pat5[i] = P.pat5[i];
+  for (u32 i = tid; i < (u32)kPatWords; i += kThreads) s_pat3[i] = P.pat3[i];
   __syncthreads();   // the only block barrier: pattern tables are shared
 
   const u128 inv21 = ((u128)P.inv21_hi << 64) | P.inv21_lo;
@@ -184,7 +202,8 @@ __global__ void __launch_bounds__(kThreads, 5) k_peel(PeelParams P) {
         } else {
           R.a = iroot6_u128(V - 1);
           R.b = (u32)(R.wlo & 511u);
-          set_offsets(R);
+          if constexpr (kSharp) set_offsets_sharp(R, W.offx[r]);
+          else set_offsets(R);
         }
         W.rows[r] = R;
       }
@@ -208,16 +227,29 @@ __global__ void __launch_bounds__(kThreads, 5) k_peel(PeelParams P) {
           if (kend > kmin) my_pos += kend - kmin;
           if (r == 0) my_calls += (u64)nrows * (kcap > kmin ? kcap - kmin : 0u);
           kmax = max(kmax, kend);
-          u32 m4 = 0;
-          if (R.b != kNoRow) {
-#pragma unroll
-            for (u32 i = 0; i < 4; ++i) {
-              const u32 t8 = ((R.b - pow6_mod512(d0 + 64u * i)) & 511u) >> 6;
-              m4 |= ((P.s8 >> t8) & 1u) << i;
+          if constexpr (kSharp) {
+            // T = (V - d^6)/64 mod 64 from (V - d^6) mod 4096, d = d0 + 64 i
+            u32 m32 = 0;
+            if (R.b != kNoRow) {
+              const u32 v12 = (u32)R.wlo & 4095u;
+              for (u32 i = 0; i < 32; ++i) {
+                const u32 t = ((v12 - pow6_mod4096(d0 + 64u * i)) & 4095u) >> 6;
+                m32 |= (u32)((P.p64 >> t) & 1ull) << i;
+              }
             }
+            W.M32[di][r] = m32;
+          } else {
+            u32 m4 = 0;
+            if (R.b != kNoRow) {
+#pragma unroll
+              for (u32 i = 0; i < 4; ++i) {
+                const u32 t8 = ((R.b - pow6_mod512(d0 + 64u * i)) & 511u) >> 6;
+                m4 |= ((P.s8 >> t8) & 1u) << i;
+              }
+            }
+            W.M4[di][r] = (u8)m4;
           }
           W.K[di][r] = (u16)kend;
-          W.M4[di][r] = (u8)m4;
         }
 #pragma unroll
         for (int o = 16; o; o >>= 1) kmax = max(kmax, __shfl_xor_sync(0xFFFFFFFFu, kmax, o));
@@ -229,15 +261,23 @@ __global__ void __launch_bounds__(kThreads, 5) k_peel(PeelParams P) {
           for (u32 wt = 0; wt < ntiles; ++wt) {
             const u32 kbase = (wt * 32u + lane) * 32u;
             const u64 dstart = (u64)d0 + 64ull * kbase;
-            const u32 s9 = (u32)(dstart % 9), s7 = (u32)(dstart % 7);
+            const u32 s9 = (u32)(dstart % (kSharp ? 27 : 9)), s7 = (u32)(dstart % (kSharp ? 49 : 7));
             const u32 s13 = (u32)(dstart % 13), s19 = (u32)(dstart % 19);
+            u32 s31 = 0, s37 = 0, s43 = 0;
+            if constexpr (kSharp) {
+              s31 = (u32)(dstart % 31); s37 = (u32)(dstart % 37); s43 = (u32)(dstart % 43);
+            }
             const u32 lowmask = (kbase == 0) ? lowmask0 : ~0u;
             for (u32 r = 0; r < nrows; ++r) {
               const u32 kend = W.K[di][r];
               if (kend <= wt * 1024u) break;          // rows shorten as e grows
               u32 m = 0;
               if (kbase < kend) {
-                m = ((u32)W.M4[di][r] * 0x11111111u) & gate_word(s_pat5, W.rows[r], s9, s7, s13, s19);
+                if constexpr (kSharp)
+                  m = W.M32[di][r] & gate_word(s_pat5, W.rows[r], s9, s7, s13, s19) &
+                      gate_word3(s_pat5, W.offx[r], s31, s37, s43);
+                else
+                  m = ((u32)W.M4[di][r] * 0x11111111u) & gate_word(s_pat5, W.rows[r], s9, s7, s13, s19);
                 const u32 n = kend - kbase;
                 if (n < 32u) m &= (1u << n) - 1u;
                 m &= lowmask;
@@ -327,11 +367,13 @@ __global__ void __launch_bounds__(kThreads, 5) k_peel(PeelParams P) {
 }
 
 // k_peel over items [0, n) of the batch.
+template <bool kSharp>
 int launch_main(s615_ctx* ctx, const TableView& tv, const s615_batch* b, size_t n,
                 unsigned flags, cudaStream_t st, int grid_blocks) {
   static bool attr_set = false;
+  constexpr size_t kSmemTotal = smem_total<kSharp>();
   if (!attr_set) {
-    S615_CU(cudaFuncSetAttribute(k_peel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    S615_CU(cudaFuncSetAttribute(k_peel<kSharp>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kSmemTotal));
     attr_set = true;
   }
@@ -346,7 +388,8 @@ int launch_main(s615_ctx* ctx, const TableView& tv, const s615_batch* b, size_t 
   P.ctr = b->d_ctr;
   const bool gated = !(flags & S615_F_NO_GATE);
   // ctx->d_pat = [gate cls5 | open cls5 | gate find3 | open find3]
-  P.pat5 = ctx->d_pat + (gated ? 0 : kPatWords);
+  P.pat5 = kSharp ? ctx->d_sharp : ctx->d_pat + (gated ? 0 : kPatWords);
+  P.p64 = ctx->p64;
   P.pat3 = ctx->d_pat + 2 * kPatWords + (gated ? 0 : kPatWords);
   const u128 inv = inv_2adic_u128((u128)kM21);
   P.inv21_lo = (u64)inv;
@@ -356,12 +399,12 @@ int launch_main(s615_ctx* ctx, const TableView& tv, const s615_batch* b, size_t 
   int grid = grid_blocks;
   if (grid <= 0) {
     int per_sm = 0;
-    S615_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel, kThreads, kSmemTotal));
+    S615_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel<kSharp>, kThreads, kSmemTotal));
     grid = ctx->num_sms * (per_sm > 0 ? per_sm : 1);
   }
   const size_t need = (n + kWarps - 1) / kWarps;
   if ((size_t)grid > need) grid = (int)need;
-  k_peel<<<grid, kThreads, kSmemTotal, st>>>(P);
+  k_peel<kSharp><<<grid, kThreads, kSmemTotal, st>>>(P);
   ctx->launches++;
   S615_CU(cudaGetLastError());
   return S615_OK;
@@ -372,7 +415,9 @@ int launch_main(s615_ctx* ctx, const TableView& tv, const s615_batch* b, size_t 
 int launch_peel(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
                 cudaStream_t st, int grid_blocks) {
   if (b->n_main) {
-    const int s = launch_main(ctx, tv, b, b->n_main, flags, st, grid_blocks);
+    const bool sharp = (flags & S615_F_SHARP) && !(flags & S615_F_NO_GATE);
+    const int s = sharp ? launch_main<true>(ctx, tv, b, b->n_main, flags, st, grid_blocks)
+                        : launch_main<false>(ctx, tv, b, b->n_main, flags, st, grid_blocks);
     if (s) return s;
   }
   if (b->n_items > b->n_main) return launch_peel617(ctx, tv, b, flags, st, grid_blocks);

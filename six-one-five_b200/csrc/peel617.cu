@@ -28,6 +28,8 @@
 //    (B above about 514,000); its counters and raw hits then repeat those c4.
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "peel_common.cuh"
 
 namespace s615 {
@@ -50,6 +52,15 @@ struct WarpSmem617 {
   u32 ring[kQ];          // probe ring: column (18 bits) | buffer row << 18
 };
 
+// With the sharp gate a row also carries the offsets for 31, 37, 43 and a
+// 32-column mod-64 mask (c^6 mod 64 has period 32 in c).
+struct WarpSmem617Sharp : WarpSmem617 {
+  u16 offx[kBuf][4];
+  u32 m32[kBuf];
+};
+template <bool kSharp>
+using Warp617T = typename std::conditional<kSharp, WarpSmem617Sharp, WarpSmem617>::type;
+
 struct Peel617Params {
   TableView tv;
   const DevUnit* units;
@@ -64,11 +75,19 @@ struct Peel617Params {
   u64 inv21_lo, inv21_hi;  // (21^6)^-1 mod 2^128
   u32 s8;                  // admissible values mod 8, as a bitmask
   u32 use_tri;
+  u64 p64;                 // sharp gate: admissible values mod 64, as a bitmask
 };
 
-constexpr size_t kSmemPat = kPatWords * sizeof(u32);
+// Pattern words, the triple-sum block, then the warp slices (16-byte aligned:
+// the row records are).
+template <bool kSharp>
+constexpr size_t smem_pat617() {
+  return ((size_t)(kSharp ? kSharpWords : kPatWords) * sizeof(u32) + 15) / 16 * 16;
+}
 constexpr size_t kSmemTri = kTriWords * sizeof(u32);
-constexpr size_t kSmemTotal = kSmemPat + kSmemTri + kWarps * sizeof(WarpSmem617);
+static_assert(kSmemTri % 16 == 0, "warp slices must start 16-byte aligned");
+template <bool kSharp>
+constexpr size_t smem_total617() { return smem_pat617<kSharp>() + kSmemTri + kWarps * sizeof(Warp617T<kSharp>); }
 
 struct Item617 {
   u32 unit_id, r0, mod, j0, lim;
@@ -106,7 +125,8 @@ __device__ __forceinline__ void probe_batch(const Peel617Params& P, const WarpSm
 }
 
 // Sieve every buffered row, probe the survivors, empty the buffer.
-__device__ __forceinline__ void flush_rows(const Peel617Params& P, WarpSmem617& W,
+template <bool kSharp>
+__device__ __forceinline__ void flush_rows(const Peel617Params& P, Warp617T<kSharp>& W,
                                            const u32* s_pat, State617& S, const Item617& I,
                                            u32 lane) {
   const u32 nbuf = S.nbuf;
@@ -139,7 +159,11 @@ __device__ __forceinline__ void flush_rows(const Peel617Params& P, WarpSmem617& 
       kbase = (g - W.pre[r]) << 5;
       const u32 len = R.b & kLenMask;
       const u32 xs = R.a + kbase;
-      m = ((R.b >> 28) * 0x11111111u) & gate_word(s_pat, R, xs % 9u, xs % 7u, xs % 13u, xs % 19u);
+      if constexpr (kSharp)
+        m = W.m32[r] & gate_word(s_pat, R, xs % 27u, xs % 49u, xs % 13u, xs % 19u) &
+            gate_word3(s_pat, W.offx[r], xs % 31u, xs % 37u, xs % 43u);
+      else
+        m = ((R.b >> 28) * 0x11111111u) & gate_word(s_pat, R, xs % 9u, xs % 7u, xs % 13u, xs % 19u);
       const u32 n = len - kbase;
       if (n < 32u) m &= (1u << n) - 1u;
     }
@@ -170,7 +194,8 @@ __device__ __forceinline__ void flush_rows(const Peel617Params& P, WarpSmem617& 
 }
 
 // Turn cnt queued c4 (from cq[ch]) into find3 rows, one per lane.
-__device__ __forceinline__ void make_rows(const Peel617Params& P, WarpSmem617& W,
+template <bool kSharp>
+__device__ __forceinline__ void make_rows(const Peel617Params& P, Warp617T<kSharp>& W,
                                           const u32* s_pat, State617& S, const Item617& I,
                                           u32 lane, u32 ch, u32 cnt, u32 h, u64 tl, u64 th) {
   const bool act = lane < cnt;
@@ -179,6 +204,8 @@ __device__ __forceinline__ void make_rows(const Peel617Params& P, WarpSmem617& W
   const u32 c4 = e & 0xFFFFu;
   const u64 Tl = __shfl_sync(kFull, tl, src), Th = __shfl_sync(kFull, th, src);
   RowRec R;
+  u16 offx[4] = {0, 0, 0, 0};
+  u32 m32 = 0;
   bool ok = false;
   u32 len = 0;
   if (act) {
@@ -201,7 +228,15 @@ __device__ __forceinline__ void make_rows(const Peel617Params& P, WarpSmem617& W
           }
           R.a = lo3;
           R.b = len | (m4 << 28);
-          set_offsets(R);
+          if constexpr (kSharp) {
+            set_offsets_sharp(R, offx);
+            for (u32 i = 0; i < 32; ++i) {
+              const u32 t = ((u32)R.wlo - pow6_mod4096(lo3 + i)) & 63u;
+              m32 |= (u32)((P.p64 >> t) & 1ull) << i;
+            }
+          } else {
+            set_offsets(R);
+          }
           ok = true;
         }
       }
@@ -210,10 +245,14 @@ __device__ __forceinline__ void make_rows(const Peel617Params& P, WarpSmem617& W
   __syncwarp();
   const u32 bal = __ballot_sync(kFull, ok);
   const u32 nnew = __popc(bal);
-  if (S.nbuf + nnew > kBuf) flush_rows(P, W, s_pat, S, I, lane);
+  if (S.nbuf + nnew > kBuf) flush_rows<kSharp>(P, W, s_pat, S, I, lane);
   if (ok) {
     const u32 slot = S.nbuf + __popc(bal & lanemask_lt());
     W.rows[slot] = R;
+    if constexpr (kSharp) {
+      W.m32[slot] = m32;
+      for (int k = 0; k < 4; ++k) W.offx[slot][k] = offx[k];
+    }
     W.aux[slot] = c4 | ((h + src) << 16);
     S.pos += len;
   }
@@ -221,13 +260,15 @@ __device__ __forceinline__ void make_rows(const Peel617Params& P, WarpSmem617& W
   __syncwarp();
 }
 
-__global__ void __launch_bounds__(kThreads, 4) k_peel617(Peel617Params P) {
+template <bool kSharp>
+__global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Params P) {
   extern __shared__ __align__(16) unsigned char smem[];
+  constexpr u32 kPW = kSharp ? (u32)kSharpWords : (u32)kPatWords;
   u32* s_pat = reinterpret_cast<u32*>(smem);
-  u32* s_tri = s_pat + kPatWords;
+  u32* s_tri = s_pat + kPW;
   const u32 tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  WarpSmem617& W = reinterpret_cast<WarpSmem617*>(smem + kSmemPat + kSmemTri)[warp];
-  for (u32 i = tid; i < (u32)kPatWords; i += kThreads) s_pat[i] = P.pat3[i];
+  Warp617T<kSharp>& W = reinterpret_cast<Warp617T<kSharp>*>(smem + smem_pat617<kSharp>() + kSmemTri)[warp];
+  for (u32 i = tid; i < kPW; i += kThreads) s_pat[i] = P.pat3[i];
   for (u32 i = tid; i < (u32)kTriWords; i += kThreads) s_tri[i] = P.tri[i];
   __syncthreads();   // the only block barrier: the tables are shared
   const u16* p6_504 = reinterpret_cast<const u16*>(s_tri + kTriP504);
@@ -307,7 +348,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_peel617(Peel617Params P) {
           cl += __popc(bal);
           if (cl >= 32u) {
             __syncwarp();
-            make_rows(P, W, s_pat, S, I, lane, ch, 32u, h, tl, th);
+            make_rows<kSharp>(P, W, s_pat, S, I, lane, ch, 32u, h, tl, th);
             ch = (ch + 32u) & (kCQ - 1);
             cl -= 32u;
           }
@@ -315,10 +356,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_peel617(Peel617Params P) {
       }
       if (cl) {   // the queue refers to this half's lane rows: empty it now
         __syncwarp();
-        make_rows(P, W, s_pat, S, I, lane, ch, cl, h, tl, th);
+        make_rows<kSharp>(P, W, s_pat, S, I, lane, ch, cl, h, tl, th);
       }
     }
-    flush_rows(P, W, s_pat, S, I, lane);
+    flush_rows<kSharp>(P, W, s_pat, S, I, lane);
   }
 
   // ---- counters: warp reduce, one atomic per warp ----
@@ -341,11 +382,15 @@ __global__ void __launch_bounds__(kThreads, 4) k_peel617(Peel617Params P) {
 
 }  // namespace
 
-int launch_peel617(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
-                   cudaStream_t st, int grid_blocks) {
+namespace {
+
+template <bool kSharp>
+int launch617(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
+              cudaStream_t st, int grid_blocks) {
   static bool attr_set = false;
+  constexpr size_t kSmemTotal = smem_total617<kSharp>();
   if (!attr_set) {
-    S615_CU(cudaFuncSetAttribute(k_peel617, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    S615_CU(cudaFuncSetAttribute(k_peel617<kSharp>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kSmemTotal));
     attr_set = true;
   }
@@ -361,7 +406,8 @@ int launch_peel617(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned f
   P.hit_cap = b->hit_cap;
   P.ctr = b->d_ctr;
   const bool gated = !(flags & S615_F_NO_GATE);
-  P.pat3 = ctx->d_pat + 2 * kPatWords + (gated ? 0 : kPatWords);
+  P.pat3 = kSharp ? ctx->d_sharp + kSharpWords : ctx->d_pat + 2 * kPatWords + (gated ? 0 : kPatWords);
+  P.p64 = ctx->p64;
   P.tri = ctx->d_tri;
   const u128 inv = inv_2adic_u128((u128)kM21);
   P.inv21_lo = (u64)inv;
@@ -371,15 +417,24 @@ int launch_peel617(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned f
   int grid = grid_blocks;
   if (grid <= 0) {
     int per_sm = 0;
-    S615_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel617, kThreads, kSmemTotal));
+    S615_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel617<kSharp>, kThreads, kSmemTotal));
     grid = ctx->num_sms * (per_sm > 0 ? per_sm : 1);
   }
   const size_t need = (n + kWarps - 1) / kWarps;
   if ((size_t)grid > need) grid = (int)need;
-  k_peel617<<<grid, kThreads, kSmemTotal, st>>>(P);
+  k_peel617<kSharp><<<grid, kThreads, kSmemTotal, st>>>(P);
   ctx->launches++;
   S615_CU(cudaGetLastError());
   return S615_OK;
+}
+
+}  // namespace
+
+int launch_peel617(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
+                   cudaStream_t st, int grid_blocks) {
+  if ((flags & S615_F_SHARP) && !(flags & S615_F_NO_GATE))
+    return launch617<true>(ctx, tv, b, flags, st, grid_blocks);
+  return launch617<false>(ctx, tv, b, flags, st, grid_blocks);
 }
 
 }  // namespace s615

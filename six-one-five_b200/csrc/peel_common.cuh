@@ -39,6 +39,31 @@ __device__ __forceinline__ void set_offsets(RowRec& R) {
   R.off[3] = (u16)(kPatB19 + 19 * mod_small<19>(R.whi, R.wlo));
 }
 
+// Sharp gate offsets: q = 27, 49, 13, 19 in the row record, 31, 37, 43 in offx.
+__device__ __forceinline__ void set_offsets_sharp(RowRec& R, u16* offx) {
+  R.off[0] = (u16)(kSB27 + 27 * mod_small<27>(R.whi, R.wlo));
+  R.off[1] = (u16)(kSB49 + 49 * mod_small<49>(R.whi, R.wlo));
+  R.off[2] = (u16)(kSB13 + 13 * mod_small<13>(R.whi, R.wlo));
+  R.off[3] = (u16)(kSB19 + 19 * mod_small<19>(R.whi, R.wlo));
+  offx[0] = (u16)(kSB31 + 31 * mod_small<31>(R.whi, R.wlo));
+  offx[1] = (u16)(kSB37 + 37 * mod_small<37>(R.whi, R.wlo));
+  offx[2] = (u16)(kSB43 + 43 * mod_small<43>(R.whi, R.wlo));
+}
+
+// The three extra sharp words of one lane.
+__device__ __forceinline__ u32 gate_word3(const u32* pat, const u16* offx, u32 s31, u32 s37,
+                                          u32 s43) {
+  return pat[offx[0] + s31] & pat[offx[1] + s37] & pat[offx[2] + s43];
+}
+
+// x^6 mod 4096 (and so mod 64) for x < 2^32.
+__device__ __forceinline__ u32 pow6_mod4096(u32 x) {
+  x &= 4095u;
+  const u32 x2 = (x * x) & 4095u;
+  const u32 x3 = (x2 * x) & 4095u;
+  return (x3 * x3) & 4095u;
+}
+
 // The gate word of one lane: bits for 32 consecutive columns.
 __device__ __forceinline__ u32 gate_word(const u32* pat, const RowRec& R, u32 s9, u32 s7, u32 s13,
                                          u32 s19) {

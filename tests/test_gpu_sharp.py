@@ -1,0 +1,128 @@
+"""The sharper gate (S615_F_SHARP) on the device (GPU).
+
+It adds sound residue tests (sums of two sixth powers mod 64, 27, 49, 31, 37,
+43), so against the default run on the same units: the same in-range and R>0
+point counts, fewer probes, raw hits a subset, and exactly the same verified
+solutions and recovered plants.  cls 2-4 units are not affected.
+"""
+import numpy as np
+import pytest
+
+import orc
+import s615
+import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def hit_set(h):
+    return {(int(x["unit"]), int(x["d"]), int(x["e"]), int(x["c4"]), int(x["fp"])) for x in h}
+
+
+def sol_set(sols):
+    return {(s.unit, s.kind, s.cls, s.d, s.e, s.c1, s.c2, s.c3, s.c4, tuple(s.a)) for s in sols}
+
+
+def both(engine, tid, arr, n, N, flags=0):
+    h0, c0 = engine.run(tid, arr, n, flags)
+    h1, c1 = engine.run(tid, arr, n, flags | s615.F_SHARP)
+    return (h0, c0, sol_set(engine.verify(arr, n, h0, N))), (h1, c1, sol_set(engine.verify(arr, n, h1, N)))
+
+
+@pytest.mark.parametrize("r", [16, 48])
+def test_sharp_cls5_config1(engine, oracle_table, r):
+    N = 715
+    _, path = oracle_table(N, r)
+    tid = engine.load_table(path, N)
+    try:
+        units = W.cls5_units(1000, 30000)
+        plants = W.plants(16, 1, 1000, 30000, N)
+        arr, n = W.unit_array(units, plants, N)
+        (h0, c0, s0), (h1, c1, s1) = both(engine, tid, arr, n, N)
+        assert (c1.calls, c1.pos) == (c0.calls, c0.pos)
+        assert c1.probes < c0.probes and c1.gated == c1.pos - c1.probes
+        assert hit_set(h1) <= hit_set(h0)
+        assert s1 == s0 and len([s for s in s1 if s[1] == 1]) >= len(plants)
+        if r == 16:
+            assert len(hit_set(h1)) < len(hit_set(h0))   # some filter false positives skipped
+    finally:
+        engine.free_table(tid)
+
+
+def test_sharp_cls5_band_sample(engine):
+    N = 76300
+    tid = engine.build_table(N, 48)
+    try:
+        units = W.cls5_units(3200000, 3200400)
+        plants = W.plants(32, 2, 3200000, 3200400, N)
+        arr, n = W.unit_array(units, plants, N)
+        (h0, c0, s0), (h1, c1, s1) = both(engine, tid, arr, n, N)
+        assert c1.pos == c0.pos and c1.probes * 2 < c0.probes
+        assert hit_set(h1) <= hit_set(h0)
+        assert s1 == s0
+        got = {(s[0], s[3], s[4], s[5], s[6]) for s in s1 if s[1] == 1}
+        assert all((len(units) + j, p.d, p.e, p.c1, p.c2) in got for j, p in enumerate(plants))
+    finally:
+        engine.free_table(tid)
+
+
+def test_sharp_617(engine, oracle_table):
+    N = 54400 // 42
+    _, path = oracle_table(N, 16)
+    tid = engine.load_table(path, N)
+    try:
+        trip = []
+        for B in range(54301, 54401):
+            if B % 2 and B % 3 and B % 7:
+                arr, k = s615.candidates617(B)
+                trip += [(arr[i].B, arr[i].u, arr[i].w) for i in range(k)]
+        arr, n = s615.make_units617(trip)
+        (h0, c0, s0), (h1, c1, s1) = both(engine, tid, arr, n, N)
+        assert (c1.tri_total, c1.tri_skipped, c1.pos) == (c0.tri_total, c0.tri_skipped, c0.pos)
+        assert c1.probes < c0.probes
+        assert hit_set(h1) <= hit_set(h0) and s1 == s0
+        lines = [s615.solution_line(s) for s in engine.verify(arr, n, h1, N)]
+        assert any("B=54347 a1=2100 a2=3150 a3=19467 a4=32748 a5=33376 a6=46032 a7=48846" in l
+                   for l in lines)
+    finally:
+        engine.free_table(tid)
+
+
+def test_sharp_617_plants(engine):
+    N = 600
+    tid = engine.build_table(N, 48)
+    try:
+        rng = np.random.RandomState(9)
+        units, want = [], []
+        while len(units) < 64:
+            c = sorted(int(x) for x in rng.choice(np.arange(1, N + 1), 4, replace=False))
+            T = sum(x**6 for x in c)
+            if 3 * c[3] ** 6 < T or 3 * c[2] ** 6 < T - c[3] ** 6:
+                continue
+            d = int(rng.randint(1, 281))
+            units.append(s615.make_plant617((21 * d) ** 6 + 42**6 * T, d, N, B=42 * N + 1))
+            want.append((d, tuple(c)))
+        arr = (s615.Unit * len(units))(*units)
+        h1, _ = engine.run(tid, arr, len(units), s615.F_SHARP)
+        got = {(s.unit, s.d, tuple(sorted((s.c1, s.c2, s.c3, s.c4))))
+               for s in engine.verify(arr, len(units), h1, N)}
+        assert all((i, d, c) in got for i, (d, c) in enumerate(want))
+    finally:
+        engine.free_table(tid)
+
+
+def test_sharp_leaves_cls234_alone(engine, oracle_table):
+    N = 2000
+    _, path = oracle_table(N, 16)
+    tid = engine.load_table(path, N)
+    try:
+        units = [(c, B, u) for B in range(400000, 400600) if W.eligible(B)
+                 for c in (2, 3, 4) for u in s615.unit_candidates(B, c)]
+        arr = (s615.Unit * len(units))()
+        for i, (c, B, u) in enumerate(units):
+            arr[i].cls, arr[i].B, arr[i].u = c, B, u
+        (h0, c0, s0), (h1, c1, s1) = both(engine, tid, arr, len(units), N)
+        assert (c1.calls, c1.probes) == (c0.calls, c0.probes)
+        assert hit_set(h1) == hit_set(h0) and s1 == s0
+    finally:
+        engine.free_table(tid)
