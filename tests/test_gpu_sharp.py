@@ -43,8 +43,6 @@ def test_sharp_cls5_config1(engine, oracle_table, r):
         assert c1.probes < c0.probes and c1.gated == c1.pos - c1.probes
         assert hit_set(h1) <= hit_set(h0)
         assert s1 == s0 and len([s for s in s1 if s[1] == 1]) >= len(plants)
-        if r == 16:
-            assert len(hit_set(h1)) < len(hit_set(h0))   # some filter false positives skipped
     finally:
         engine.free_table(tid)
 
