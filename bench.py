@@ -415,22 +415,6 @@ def run617(args, rank, world, local, dist):
             "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs (burst)",
             "traffic": None, "algorithmic_bytes_per_launch": ctr.probes * PROBE_BYTES}
 
-    # the opt-in sharper gate (S615_F_SHARP) on the same batch: same points,
-    # fewer probes, the same verified solutions (tests/test_gpu_sharp.py)
-    sharp = None
-    if rank == 0 and not args.no_plain:
-        sms, sctr = timed_steps(lib, eng, tid, batch, stream, s615.F_SHARP, 2)
-        sharp = {"value": sctr.pos * 2 / (sms / 1e3), "unit": UNIT, "ms_per_step": sms / 2,
-                 "post_gate_probes": sctr.probes, "pos": sctr.pos,
-                 "flag": "S615_F_SHARP (extra sound residue tests; raw hits a subset)"}
-        log(f"sharp gate: {sms / 2:.1f} ms per step, probes {sctr.probes}")
-
-    # per-unit latency through the serving loop under a config-5-like stream
-    serve = None
-    if rank == 0 and not args.no_plain:
-        serve = serve_latency(eng, tid, units, N)
-        log(f"serving: p50 {serve['p50_ms']:.1f} ms, p99 {serve['p99_ms']:.1f} ms per unit")
-
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         import orc
