@@ -55,7 +55,9 @@ def parse():
     ap.add_argument("--r", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
-    ap.add_argument("--workload", default="cls5", choices=["cls5", "cls617"])
+    ap.add_argument("--workload", default="cls5", choices=["cls5", "cls617", "mix", "serve"])
+    ap.add_argument("--units", type=int, default=0, help="mix: units per step (default 200,000)")
+    ap.add_argument("--seconds", type=float, default=10.0, help="serve: seconds of arrivals")
     return ap.parse_args()
 
 
@@ -510,9 +512,194 @@ def run617_reference(args, rank):
     return 0
 
 
+# ------------------------------------------------ mixed classes and serving
+METRIC_MIX = "mixed-class units/s (classes 2:4%/3:1%/4:48%/5:47%, B log-uniform [1M,4M]), 1 B200"
+METRIC_SERVE = "per-unit latency p50/p99 through the serving loop (Poisson 5,000 units/s), 1 B200"
+
+
+def run_mix(args, rank, world, local, dist):
+    """200,000 Stage-1 units of classes 2-5 in one persistent batch (the mixed
+    queue), B log-uniform on [1M, 4M], 64 plants, N = 95,239 (B <= 4M)."""
+    import numpy as np
+    import torch
+
+    import s615
+    import workloads as W
+    torch.cuda.set_device(local)
+    n_units = args.units or 200_000
+    N = args.N or math.ceil(4_000_000 / 42)
+    eng = s615.Engine(local)
+    t0 = time.perf_counter()
+    tid = eng.build_table(N, args.r)
+    build_s = time.perf_counter() - t0
+    units = W.mixed_units(n_units, 3 + rank, 1_000_000, 4_000_000)
+    p5 = W.plants(32, 33 + rank, 1_000_000, 4_000_000, N)
+    p24 = W.plants234(32, 34 + rank, 1_000_000, 4_000_000, N)
+    arr, n = W.mixed_unit_array(units, p5, p24, N)
+    lib = s615.lib()
+    batch = C.c_void_p()
+    s615._check(lib.s615_prepare(eng._ctx, C.cast(arr, C.c_void_p), n, C.byref(batch)), "prepare")
+    stream = torch.cuda.Stream()
+    sptr = C.c_void_p(stream.cuda_stream)
+    for _ in range(args.warmup):
+        s615._check(lib.s615_run_batch(eng._ctx, tid, batch, 0, sptr), "run_batch")
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    launches0 = eng.launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        s615._check(lib.s615_run_batch(eng._ctx, tid, batch, 0, sptr), "run_batch")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    cl = clocks.stop()
+    launches = eng.launches - launches0
+    ms = e0.elapsed_time(e1)
+    hits = (s615.Hit * (1 << 20))()
+    nh = C.c_size_t(0)
+    ctr = s615.Counters()
+    s615._check(lib.s615_batch_results(eng._ctx, batch, C.cast(hits, C.c_void_p), 1 << 20,
+                                       C.byref(nh), C.byref(ctr)), "results")
+    sols = eng.verify(arr, n, s615.hits_to_array(hits, nh.value), N, cap=65536)
+    k5 = len(units)
+    got5 = {(s.unit, s.d, s.e, s.c1, s.c2) for s in sols if s.kind == 1 and s.cls == 5}
+    rec5 = sum((k5 + j, p.d, p.e, p.c1, p.c2) in got5 for j, p in enumerate(p5))
+    got24 = {(s.unit, s.d, (s.c1, s.c2, s.c3)) for s in sols if s.kind == 1 and s.cls != 5}
+    rec24 = sum((k5 + len(p5) + j, d, c) in got24 for j, (_, _, d, c, _) in enumerate(p24))
+    t0 = time.perf_counter()
+    h2, c2 = eng.run(tid, arr, n, hit_cap=1 << 16)
+    e2e_s = time.perf_counter() - t0
+    assert c2.pos == ctr.pos and c2.probes == ctr.probes
+    import collections
+    mix = collections.Counter(c for c, _, _ in units)
+    step_s = ms / args.steps / 1e3
+    line = {"metric": METRIC_MIX, "value": n / step_s, "unit": "units/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic",
+            "config": {"workload": f"{len(units)} Stage-1 units {dict(sorted(mix.items()))} + 64 plants, "
+                                   f"one persistent batch; xor table N={N} r={args.r} on device",
+                       "N": N, "r": args.r,
+                       "l2": "table %.1f GB, larger than L2" % (eng.table_info(tid).device_bytes / 1e9)},
+            "points_per_s": ctr.pos / step_s,
+            "counters": {"calls": ctr.calls, "gated": ctr.gated, "probes": ctr.probes, "pos": ctr.pos},
+            "plants_recovered": f"{rec5 + rec24}/{len(p5) + len(p24)}",
+            "solutions": [s615.solution_line(s) for s in sols if s.kind == 0],
+            "table_build_s": round(build_s, 2),
+            "e2e": {"value": n / e2e_s, "unit": "units/s", "h2d_bytes_per_step": batch_h2d(lib, batch),
+                    "d2h_bytes_per_step": C.sizeof(s615.Counters) + len(h2) * C.sizeof(s615.Hit)},
+            "gpu_launches": launches, "roofline": None, "cpu_baseline": None, "clocks": cl}
+    s615._check(lib.s615_batch_free(eng._ctx, batch), "batch_free")
+    eng.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serve(args, rank, world, local, dist):
+    """Serving with four resident tables: requests of 50 units arrive as a
+    Poisson stream (5,000 units/s); B uniform on [1M, 5M], classes mixed
+    2:4%/3:1%/4:48%/5:47%; each request goes to the smallest table whose N
+    covers its B; 256 planted targets ride in the stream; the context's HBM
+    admission budget is 150 GB."""
+    import numpy as np
+
+    import s615
+    import workloads as W
+    if rank != 0:
+        return 0
+    eng = s615.Engine(local)
+    Ns = [24_000, 48_000, 76_000, 120_000]
+    tids, builds = {}, {}
+    for N in sorted(Ns, reverse=True):      # the largest build needs the most scratch
+        t0 = time.perf_counter()
+        try:
+            tids[N] = eng.build_table(N, args.r, layout=s615.LAYOUT_PACKED)
+            builds[N] = round(time.perf_counter() - t0, 2)
+        except s615.S615Error as e:
+            log(f"table N={N}: {e}")
+    resident = sum(eng.table_info(t).device_bytes for t in tids.values())
+    s615._check(s615.lib().s615_set_budget(eng._ctx, 150_000_000_000), "set_budget")
+    ranges = []
+    lo = 1_000_000
+    for N in sorted(tids):
+        hi = min(5_000_000, 42 * N + 1)
+        if hi > lo:
+            ranges.append((N, lo, hi))
+            lo = hi + 1
+    rng = np.random.RandomState(55)
+    widths = np.array([hi - lo for _, lo, hi in ranges], dtype=float)
+    p_tab = widths / widths.sum()
+    rate, req_units, secs = 5000.0, 50, args.seconds
+    plants_left = 256
+    planted = {}          # (ticket, index) -> expected solution key
+    eng.serve_start(slots=2)
+    lat, sent, done, got_plants = [], 0, 0, 0
+    t_start = time.perf_counter()
+    nxt = t_start
+    try:
+        while time.perf_counter() - t_start < secs:
+            now = time.perf_counter()
+            while nxt <= now:
+                ti = int(rng.choice(len(ranges), p=p_tab))
+                N, blo, bhi = ranges[ti]
+                us = W.mixed_units(req_units, int(rng.randint(1 << 30)), blo, bhi, log_uniform=False)
+                p5 = []
+                if plants_left > 0 and rng.rand() < 0.5:
+                    p5 = W.plants(1, int(rng.randint(1 << 30)), blo, bhi, N)
+                arr, n = W.mixed_unit_array(us, p5, [], N)
+                t = eng.submit(tids[N], arr, n)
+                if p5:
+                    p = p5[0]
+                    planted[t] = (len(us), p.d, p.e, p.c1, p.c2)
+                    plants_left -= 1
+                sent += 1
+                nxt += rng.exponential(req_units / rate)
+            for r in eng.poll(wait_ms=1):
+                lat += [r["latency_ms"]] * r["n_units"]
+                done += 1
+                if r["ticket"] in planted:
+                    got = {(s.unit, s.d, s.e, s.c1, s.c2) for s in r["solutions"] if s.kind == 1}
+                    got_plants += planted[r["ticket"]] in got
+            time.sleep(max(0.0, min(0.001, nxt - time.perf_counter())))
+        while done < sent:
+            for r in eng.poll(wait_ms=100):
+                lat += [r["latency_ms"]] * r["n_units"]
+                done += 1
+                if r["ticket"] in planted:
+                    got = {(s.unit, s.d, s.e, s.c1, s.c2) for s in r["solutions"] if s.kind == 1}
+                    got_plants += planted[r["ticket"]] in got
+    finally:
+        eng.serve_stop()
+    wall = time.perf_counter() - t_start
+    lat = np.array(lat)
+    line = {"metric": METRIC_SERVE, "value": float(np.percentile(lat, 99)), "unit": "ms",
+            "n_gpus": 1, "steps": sent, "warmup": 0, "ms_per_step": None, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": f"Poisson {rate:.0f} units/s for {secs:.0f} s in {req_units}-unit requests, "
+                                   "classes 2:4%/3:1%/4:48%/5:47%, B uniform [1M,5M]; resident tables "
+                                   + ", ".join(f"N={N}" for N in sorted(tids)) + " (packed, r=%d)" % args.r,
+                       "hbm_budget_gb": 150, "resident_table_gb": round(resident / 1e9, 2)},
+            "p50_unit_latency_ms": float(np.percentile(lat, 50)),
+            "p99_unit_latency_ms": float(np.percentile(lat, 99)),
+            "units_completed": int(lat.size), "requests": sent,
+            "completed_units_per_s": lat.size / wall,
+            "plants_recovered": f"{got_plants}/{len(planted)}",
+            "table_build_s": builds,
+            "e2e": None, "gpu_launches": eng.launches, "roofline": None, "cpu_baseline": None}
+    eng.close()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     rank, world, local, dist = dist_setup(args)
+    if args.workload == "mix":
+        return run_mix(args, rank, world, local, dist)
+    if args.workload == "serve":
+        return run_serve(args, rank, world, local, dist)
     if args.workload == "cls617":
         if args.impl == "reference":
             return run617_reference(args, rank)

@@ -138,6 +138,10 @@ typedef struct s615_solution {
 /* Open device `device` with an HBM admission budget (0 = all free memory). */
 int s615_open(int device, size_t hbm_budget, s615_ctx** out);
 int s615_close(s615_ctx* ctx);
+/* Change the HBM admission budget of an open context (0 = all device memory):
+ * allocations that would take the context's total above it fail with
+ * S615_E_OOM (a serving loop then waits for running batches to finish). */
+int s615_set_budget(s615_ctx* ctx, size_t hbm_budget);
 /* Kernel launches the engine issued since open (all of its own kernels). */
 uint64_t s615_launch_count(s615_ctx* ctx);
 

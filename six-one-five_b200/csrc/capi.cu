@@ -188,6 +188,16 @@ int s615_close(s615_ctx* ctx) {
 
 uint64_t s615_launch_count(s615_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+int s615_set_budget(s615_ctx* ctx, size_t hbm_budget) {
+  if (!ctx) return S615_E_ARG;
+  if (serving_blocks(ctx)) return S615_E_BUSY;
+  size_t free_b = 0, total_b = 0;
+  cudaSetDevice(ctx->device);
+  S615_CU(cudaMemGetInfo(&free_b, &total_b));
+  ctx->budget = hbm_budget ? hbm_budget : total_b;
+  return S615_OK;
+}
+
 int s615_get_table_info(s615_ctx* ctx, int id, s615_table_info* info) {
   if (!ctx || !info) return S615_E_ARG;
   DevTable* t = find_table(ctx, id);

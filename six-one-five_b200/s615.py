@@ -94,6 +94,7 @@ SIGNATURES = {
     "s615_open": (C.c_int, [C.c_int, C.c_size_t, C.POINTER(_P)]),
     "s615_close": (C.c_int, [_P]),
     "s615_launch_count": (C.c_uint64, [_P]),
+    "s615_set_budget": (C.c_int, [_P, C.c_size_t]),
     "s615_load_table": (C.c_int, [_P, C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_int)]),
     "s615_build_table": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)]),
     "s615_build_table_keys": (C.c_int, [_P, _P, C.c_size_t, C.c_int, C.c_uint64, C.c_int,
