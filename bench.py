@@ -821,6 +821,20 @@ def main():
                  "eligible_B_per_hour": p_rate / (ctr.pos / eligible_count(lo, hi - 1)) * 3600,
                  "batched_over_plain": value / world / p_rate}
 
+    # the band form: units generated and packed on the device from (B_lo, B_hi)
+    band_e2e = None
+    if rank == 0 and not args.no_plain:
+        t0 = time.perf_counter()
+        _, bn, bh, bctr = eng.run_band(tid, lo, hi - 1, hit_cap=1 << 16)
+        bs = time.perf_counter() - t0
+        band_e2e = {"value": bctr.pos / bs, "unit": UNIT, "units": bn, "seconds": bs,
+                    # per-B and per-unit counts/offsets for the two prefix sums
+                    "h2d_bytes_per_step": 4 * (hi - lo) + 4 * bn,
+                    "d2h_bytes_per_step": 4 * (hi - lo) + 4 * bn + 16 * bn
+                    + C.sizeof(s615.Counters) + 32 * len(bh),
+                    "call": "s615_prepare_band + s615_batch_units + s615_run_batch + s615_batch_results"}
+        log(f"band form (device Stage-1): {bs * 1e3:.1f} ms for {bn} units")
+
     # the opt-in sharper gate (S615_F_SHARP) on the same batch: same points,
     # fewer probes, the same verified solutions (tests/test_gpu_sharp.py)
     sharp = None

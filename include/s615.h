@@ -234,6 +234,17 @@ int s615_run_batch(s615_ctx* ctx, int table_id, s615_batch* b, unsigned flags, v
 int s615_batch_results(s615_ctx* ctx, s615_batch* b, s615_hit* hits, size_t hit_cap,
                        size_t* n_hits, s615_counters* counters);
 int s615_batch_free(s615_ctx* ctx, s615_batch* b);
+/* Stage-1 on the device: the class-5 units of every eligible B in
+ * [B_lo, B_hi] (gcd(B, 42) = 1; the rule of unit_candidates,
+ * fourcore_classes_v3.hpp:114-154, as fourcore_hunt_v3.cpp:371-381 emits it)
+ * generated and packed (pack_unit5, fourcore_cls5_gpu_v4.cu:169-184) by device
+ * kernels straight into a batch, in the same order as s615_prepare on the
+ * host list (B ascending, u ascending).  No unit records cross from the host.
+ * B_hi <= 40,000,000 and B_hi - B_lo < 2^26. */
+int s615_prepare_band(s615_ctx* ctx, uint64_t B_lo, uint64_t B_hi, s615_batch** out);
+/* The (cls, B, u) records of a batch's units, in batch order (to verify or
+ * report the hits of a device-generated batch). */
+int s615_batch_units(s615_ctx* ctx, const s615_batch* b, s615_unit* out, size_t cap, size_t* n);
 /* What s615_prepare copied to the device: unit records, work items and the
  * host-to-device bytes of both (no counterpart in the reference). */
 int s615_batch_size(const s615_batch* b, size_t* n_units, size_t* n_items, size_t* h2d_bytes);

@@ -178,6 +178,7 @@ int s615_close(s615_ctx* ctx) {
   cudaSetDevice(ctx->device);
   server_destroy(ctx);
   for (int k = 0; k < 4; ++k) dev_free(ctx, ctx->arena[k], ctx->arena_cap[k]);
+  dev_free(ctx, ctx->d_roots, ctx->roots_bytes);
   for (auto& kv : ctx->tables) free_table(ctx, kv.second);
   ctx->tables.clear();
   dev_free(ctx, ctx->d_pat, (4 * kPatWords + kTriWords + 2 * kSharpWords) * sizeof(u32));

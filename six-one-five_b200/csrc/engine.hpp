@@ -134,6 +134,8 @@ struct s615_ctx {
   std::mutex mu;
   s615::Server* server = nullptr;   // the serving loop, when started
   void* arena[4] = {};              // verify scratch, grow-only (units, hits, pairs, count)
+  s615::u32* d_roots = nullptr;     // device Stage-1 root tables (stage1.cu)
+  size_t roots_bytes = 0;
   size_t arena_cap[4] = {};
 };
 
@@ -204,6 +206,8 @@ std::vector<u32> e_residues(u64 B);
 std::vector<u32> d_residues(u64 B, u64 u);
 std::vector<u32> d_residues_cls234(u64 B, u64 u, int cls, u32* mod, u32* fmax);
 std::vector<u64> unit_candidates(u64 B, int cls);
+void root_csr(int which, std::vector<u32>& off, std::vector<u32>& roots);
+u32 inv_pow6_mod(u32 f, u32 m);   // (f^6)^-1 mod m
 // (u, w) anchor pairs of the (6,1,7) class-5 candidates of one B.
 std::vector<std::pair<u64, u64>> candidates617(u64 B);
 int free_factor(int cls);

@@ -135,6 +135,20 @@ bool unit_ok(u64 u, int cls) {
 
 }  // namespace
 
+// Root lists as CSR arrays for the device: off[t]..off[t+1] index the units a
+// with a^6 = t (mod m), ascending.  which: 2, 3 or 7 (moduli 2^6, 3^6, 7^6).
+void root_csr(int which, std::vector<u32>& off, std::vector<u32>& roots) {
+  const RootTable& t = which == 2 ? roots2() : which == 3 ? roots3() : roots7();
+  off.assign(t.by.size() + 1, 0);
+  roots.clear();
+  for (size_t i = 0; i < t.by.size(); ++i) {
+    off[i] = (u32)roots.size();
+    roots.insert(roots.end(), t.by[i].begin(), t.by[i].end());
+  }
+  off[t.by.size()] = (u32)roots.size();
+}
+u32 inv_pow6_mod(u32 f, u32 m) { return (u32)mod_inv(mod_pow6(f, m), m); }
+
 // (14e)^6 = B^6 (mod 3^6): e in the roots of B^6 * 14^-6.
 std::vector<u32> e_residues(u64 B) {
   const long long t = mod_pow6((long long)(B % kM3), kM3) * mod_inv(mod_pow6(14, kM3), kM3) % kM3;

@@ -125,6 +125,8 @@ SIGNATURES = {
     "s615_batch_free": (C.c_int, [_P, _P]),
     "s615_batch_size": (C.c_int, [_P, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
                                   C.POINTER(C.c_size_t)]),
+    "s615_prepare_band": (C.c_int, [_P, C.c_uint64, C.c_uint64, C.POINTER(_P)]),
+    "s615_batch_units": (C.c_int, [_P, _P, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
     "s615_verify": (C.c_int, [_P, _P, C.c_size_t, _P, C.c_size_t, C.c_int, _P, C.c_size_t,
                               C.POINTER(C.c_size_t)]),
     "s615_cls5_verify": (C.c_int, [_P, _P, C.c_size_t, _P, C.c_size_t, C.c_int, _P, C.c_size_t,
@@ -335,6 +337,27 @@ class Engine:
                                    C.cast(hits, C.c_void_p), hit_cap, C.byref(nh), C.byref(ctr))
         _check(st, entry)
         return hits_to_array(hits, nh.value), ctr
+
+    def run_band(self, tid: int, B_lo: int, B_hi: int, flags: int = 0, hit_cap: int = 1 << 20):
+        """Stage-1 class-5 units of B in [B_lo, B_hi] generated on the device
+        (s615_prepare_band), one run: (unit array, n, hits, counters)."""
+        b = C.c_void_p()
+        _check(lib().s615_prepare_band(self._ctx, B_lo, B_hi, C.byref(b)), "prepare_band")
+        try:
+            n = C.c_size_t(0)
+            lib().s615_batch_units(self._ctx, b, None, 0, C.byref(n))
+            units = (Unit * max(n.value, 1))()
+            _check(lib().s615_batch_units(self._ctx, b, C.cast(units, C.c_void_p), n.value,
+                                          C.byref(n)), "batch_units")
+            _check(lib().s615_run_batch(self._ctx, tid, b, flags, None), "run_batch")
+            hits = (Hit * max(hit_cap, 1))()
+            nh = C.c_size_t(0)
+            ctr = Counters()
+            _check(lib().s615_batch_results(self._ctx, b, C.cast(hits, C.c_void_p), hit_cap,
+                                            C.byref(nh), C.byref(ctr)), "batch_results")
+            return units, n.value, hits_to_array(hits, nh.value), ctr
+        finally:
+            lib().s615_batch_free(self._ctx, b)
 
     def cls5_run(self, tid: int, units, n: int, flags: int = 0, hit_cap: int = 1 << 20):
         return self.run(tid, units, n, flags, hit_cap, entry="s615_cls5_run")
