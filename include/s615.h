@@ -66,6 +66,10 @@ typedef struct s615_table_info {
 
 /* Unit record.  cls 5: the 2-D (e,d) peel; cls 2, 3, 4: one free term d
  * (x14, x21, x7) and the find3 leaf over c3 (fourcore_find_v4.cu:165-205).
+ * cls 1: the find4 unit of fourcore_find_v4 (expand_unit + make_cand mode 4
+ * + k_find4, fourcore_find_v4.cu:165-176,406-420,287-338),
+ * B^6 = u^6 + 42^6 (c1^6 + c2^6 + c3^6 + c4^6); a cls 1 plant has
+ * base = 42^6 (c1^6 + .. + c4^6) and lim < 2^21.
  * cls 7 (S615_CLS_617): the (6,1,7) Branch-A class-5 candidate of
  * solve_617_v1.cu:885-906, B^6 = u^6 + w^6 + (21d)^6 + 42^6 (c1^6+..+c4^6)
  * with u = 14u', w = 6v', d over residues mod 2^6 (d <= (B-1)/21) and the
@@ -82,7 +86,7 @@ typedef struct s615_table_info {
  * plant (solve_617_v1.cu:1564-1582) has base < 2^127 and lim < 65536. */
 #define S615_CLS_617 7
 typedef struct s615_unit {
-  uint32_t cls;      /* 2, 3, 4, 5 or 7 */
+  uint32_t cls;      /* 1, 2, 3, 4, 5 or 7 */
   uint32_t kind;     /* 0 = (B,u) or (B,u,w), 1 = planted base */
   uint64_t B, u;
   uint64_t base[3];  /* kind 1 only */
@@ -94,7 +98,8 @@ typedef struct s615_unit {
  * (fourcore_cls5_gpu_v4.cu:140); a=b=0, unit = index into the unit array.
  * cls 5: d is the x21 term and e the x14 term.  cls 2-4: d is the free term
  * and e carries c3 (the reference's find3 Hit puts c3 in its third field,
- * fourcore_find_device.cuh:70-77).  cls 7: d is the x21 term, e carries c3
+ * fourcore_find_device.cuh:70-77).  cls 1: d = 0, e carries c3 and c4 carries
+ * c4 (k_find4's Hit holds them as c and d).  cls 7: d is the x21 term, e carries c3
  * and c4 carries c4 (the reference's Hit{cand,a,b,c,d,e} of
  * solve_617_v1.cu:364 holds them as e, c and d).  c4 is 0 for other classes
  * and sits in what is padding in the reference's record. */

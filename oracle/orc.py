@@ -44,6 +44,11 @@ class OrcHit3(C.Structure):
     _fields_ = [("job", C.c_uint32), ("c3", C.c_uint32), ("fp", C.c_uint64)]
 
 
+class OrcHit4(C.Structure):
+    _fields_ = [("job", C.c_uint32), ("c3", C.c_uint32), ("c4", C.c_uint32), ("pad", C.c_uint32),
+                ("fp", C.c_uint64)]
+
+
 class OrcCand617(C.Structure):
     _fields_ = [("base", C.c_uint64 * 2), ("B", C.c_uint32), ("u", C.c_uint32), ("w", C.c_uint32),
                 ("lim", C.c_uint32), ("mod1", C.c_uint32), ("fmax1", C.c_uint32),
@@ -84,6 +89,9 @@ _SIG = {
     "orc_cls5_verify": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_char_p, C.c_size_t]),
     "orc_expand_cls234": (C.c_size_t, [C.c_uint64, C.c_uint64, C.c_int, _P, C.c_size_t]),
     "orc_find3_run": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_int, _P, C.c_size_t, _P]),
+    "orc_expand_cls1": (C.c_size_t, [C.c_uint64, C.c_uint64, _P, C.c_size_t]),
+    "orc_find4_run": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_int, _P, C.c_size_t,
+                                   _P]),
     "orc_617_cands": (C.c_size_t, [C.c_uint64, _P, C.c_size_t]),
     "orc_617_run": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_int, _P,
                                  C.c_size_t, _P]),
@@ -290,3 +298,33 @@ def verify617(cands, hits: np.ndarray, N: int, planted: bool = False, stats: lis
     if stats is not None:
         stats[:] = [int(st[0]), int(st[1])]
     return [l for l in buf.value.decode().splitlines() if l]
+
+
+HIT4_DTYPE = np.dtype([("job", "<u4"), ("c3", "<u4"), ("c4", "<u4"), ("pad", "<u4"), ("fp", "<u8")])
+
+
+def jobs_cls1(units):
+    """expand_unit(cls 1) + make_cand(mode 4) for (B, u) pairs: (jobs, n, unit index per job)."""
+    buf = (OrcJob3 * 1)()
+    jobs, origin = [], []
+    for k, (B, u) in enumerate(units):
+        if lib().orc_expand_cls1(B, u, C.cast(buf, C.c_void_p), 1):
+            jobs.append(OrcJob3.from_buffer_copy(buf[0]))
+            origin.append(k)
+    arr = (OrcJob3 * max(len(jobs), 1))()
+    for i, J in enumerate(jobs):
+        arr[i] = J
+    return arr, len(jobs), origin
+
+
+def run_find4(table: Table, jobs, n: int, use_gate: bool = True, ref_tiles: bool = False,
+              threads: int = 0, cap: int = 1 << 20):
+    """k_find4 semantics: (hits, [calls, gated, probes])."""
+    hits = (OrcHit4 * cap)()
+    ctr = np.zeros(3, dtype=np.uint64)
+    nh = lib().orc_find4_run(table.h, C.cast(jobs, C.c_void_p), n, int(use_gate), int(ref_tiles),
+                             threads, C.cast(hits, C.c_void_p), cap, _ptr(ctr))
+    if nh > cap:
+        raise RuntimeError("oracle hit buffer overflow")
+    raw = np.frombuffer(C.string_at(C.addressof(hits), nh * C.sizeof(OrcHit4)), dtype=HIT4_DTYPE)
+    return raw.copy(), [int(x) for x in ctr]

@@ -751,6 +751,90 @@ size_t orc_expand_cls234(uint64_t B, uint64_t u, int cls, orc_job3* out, size_t 
   return k;
 }
 
+// iroot6_host (fourcore_find_v4.cu:115-123): double estimate then exact fix-up.
+static u32 iroot6_find(u128 T) {
+  const double x = std::ldexp((double)(u64)(T >> 64), 64) + (double)(u64)T;
+  u64 a = x < 1.0 ? 0 : (u64)std::pow(x, 1.0 / 6.0);
+  while (pow6_u128(a + 1) <= T && a < 0xffffffffULL - 2) ++a;
+  while (a && pow6_u128(a) > T) --a;
+  return (u32)a;
+}
+
+size_t orc_expand_cls1(uint64_t B, uint64_t u, orc_job3* out, size_t cap) {
+  if (u >= B) return 0;                                  // compute_T_gmp (fourcore_gmp.hpp:34-42)
+  W3 R = w3_pow6(B);
+  if (w3_sub(R, w3_pow6(u)) || w3_zero(R)) return 0;
+  if (w3_divmod(R, kM42) != 0 || !w3_fits128(R)) return 0;
+  const u128 T = w3_to128(R);
+  const u32 lim = (u32)((B - 1) / 42);
+  const u32 hi = std::min(iroot6_find(T), lim);          // make_cand mode 4 (:415-419)
+  u64 lo = 1;
+  while (lo <= hi && pow6_u128(lo) * 4 < T) ++lo;
+  if (lo > hi) return 0;                                 // run_batch drops empty windows (:486)
+  orc_job3 J{};
+  J.cls = 1; J.lim = lim; J.B = B; J.u = u; J.d = 0;
+  J.T[0] = (u64)T; J.T[1] = (u64)(T >> 64);
+  J.lo = (u32)lo; J.hi = hi;
+  if (cap) out[0] = J;
+  return 1;
+}
+
+size_t orc_find4_run(const orc_table* t, const orc_job3* jobs, size_t n, int use_gate,
+                     int ref_tiles, int threads, orc_hit4* hits, size_t cap, uint64_t counters[3]) {
+  const Gate& G = gate();
+  u64 c0 = 0, c1 = 0, c2 = 0;
+  size_t nh = 0;
+#ifdef _OPENMP
+  const int nt = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt) reduction(+ : c0, c1, c2)
+#endif
+  for (long long i = 0; i < (long long)n; ++i) {
+    const orc_job3& J = jobs[i];
+    const u128 T = ((u128)J.T[1] << 64) | J.T[0];
+    const u32 t504 = (u32)(T % 504), t247 = (u32)(T % 247);
+    std::vector<orc_hit4> local;
+    for (u64 c4 = J.lo; c4 <= J.hi; ++c4) {              // k_find4 (:287-338)
+      if (c4 < 1 || c4 > J.lim) continue;
+      const u64 mult = ref_tiles ? (c4 - J.lo) / 2048 + 1 : 1;
+      const u128 c46 = pow6_u128(c4);
+      if (c46 >= T) continue;                            // R' <= 0
+      const u128 R2 = T - c46;
+      u32 hi3 = iroot6_find(R2);
+      const u32 capm = J.lim < c4 ? J.lim : (u32)c4;
+      if (hi3 > capm) hi3 = capm;
+      if (hi3 < 1) continue;
+      u32 lo3 = (u32)(hi3 * 0.8);
+      if (lo3 < 1) lo3 = 1;
+      if (lo3 > hi3) continue;
+      const u64 tfp = J.T[0] - (u64)pow6_u128(c4);
+      const u32 r4_504 = G.p6504[c4 % 504], r4_247 = G.p6247[c4 % 247];
+      for (u64 c3 = lo3; c3 <= hi3; ++c3) {
+        c0 += mult;
+        if (use_gate) {
+          u32 r504 = t504 + 1008 - r4_504 - G.p6504[c3 % 504];
+          while (r504 >= 504) r504 -= 504;
+          u32 r247 = t247 + 494 - r4_247 - G.p6247[c3 % 247];
+          while (r247 >= 247) r247 -= 247;
+          if (!(G.g504[r504] && G.g247[r247])) { c1 += mult; continue; }
+        }
+        c2 += mult;
+        const u64 c32 = c3 * c3;
+        const u64 fp = tfp - c32 * c32 * c32;
+        if (might_contain(*t, fp))
+          for (u64 k = 0; k < mult; ++k) local.push_back(orc_hit4{(u32)i, (u32)c3, (u32)c4, 0, fp});
+      }
+    }
+    if (!local.empty()) {
+#pragma omp critical(orc_hits4)
+      {
+        for (const auto& h : local) { if (nh < cap) hits[nh] = h; ++nh; }
+      }
+    }
+  }
+  counters[0] = c0; counters[1] = c1; counters[2] = c2;
+  return nh;
+}
+
 // k_find3 (fourcore_find_v4.cu:255-284) with u64 cell indices (xor_filter.hpp:53-60).
 size_t orc_find3_run(const orc_table* t, const orc_job3* jobs, size_t n, int use_gate,
                      int threads, orc_hit3* hits, size_t cap, uint64_t counters[3]) {

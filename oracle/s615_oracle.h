@@ -113,6 +113,21 @@ size_t orc_expand_cls234(uint64_t B, uint64_t u, int cls, orc_job3* out, size_t 
 size_t orc_find3_run(const orc_table* t, const orc_job3* jobs, size_t n, int use_gate,
                      int threads, orc_hit3* hits, size_t cap, uint64_t counters[3]);
 
+/* ---- cls1 find4 (fourcore_find_v4.cu:165-176,406-420,287-338) ---- */
+typedef struct orc_hit4 {
+  uint32_t job, c3, c4, pad;
+  uint64_t fp;
+} orc_hit4;
+/* expand_unit(cls 1) + make_cand(mode 4): one job with T = (B^6-u^6)/42^6 and
+ * the c4 window [lo, hi] (hi = min(iroot6(T), lim), lo least with 4 lo^6 >= T);
+ * returns 0 when compute_T fails or the window is empty (run_batch drops it). */
+size_t orc_expand_cls1(uint64_t B, uint64_t u, orc_job3* out, size_t cap);
+/* k_find4: per c4 the c3 window [max(1, (u32)(0.8 hi3)), hi3], hi3 = min(iroot6(T - c4^6),
+ * lim, c4); counters calls / gated / probes.  ref_tiles != 0 repeats each c4 as the
+ * reference's y tiles of 2048 do (block y walks c4 >= lo + 2048 y to hi). */
+size_t orc_find4_run(const orc_table* t, const orc_job3* jobs, size_t n, int use_gate,
+                     int ref_tiles, int threads, orc_hit4* hits, size_t cap, uint64_t counters[3]);
+
 /* ---- (6,1,7) Branch-A class 5 (solve_617_v1.cu) ---- */
 typedef struct orc_cand617 {
   uint64_t base[2];        /* B^6 - u^6 - w^6 (i128; B <= 2,353,973) */

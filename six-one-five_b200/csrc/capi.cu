@@ -503,7 +503,8 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
     const int s = make_dev_unit(units[i], (u32)i, &d, &skip);
     if (s) return s;
     if (skip) continue;
-    unit_items(d, (u32)du.size(), d.cls == S615_CLS_617 ? items617 : b->host_items);
+    // classes 1 and 7 (c4 windows) run in the second kernel
+    unit_items(d, (u32)du.size(), (d.cls == S615_CLS_617 || d.cls == 1) ? items617 : b->host_items);
     du.push_back(d);
   }
   // heaviest first: a candidate's first rows (smallest d) have the largest T

@@ -21,6 +21,9 @@ namespace s615 {
 //            d = res2[k] + 64 t (d <= fmax2); row value V = (base-(14e)^6)/21^6.
 //   cls 2-4: rows are d = res1[i] + mod1 j (d <= fmax1), free factor f; row
 //            value T = (base-(f d)^6)/42^6, columns c3 over the find3 window.
+//   cls 1  : the find4 unit (fourcore_find_v4.cu:287-338): base holds
+//            T = (B^6-u^6)/42^6 itself, fmax2..fmax1 the c4 window [lo4, hi4];
+//            items are chunks of kC4Chunk c4 values.
 //   cls 7  : the (6,1,7) class-5 shape: base = B^6-u^6-w^6 (< 2^127), rows
 //            d = res1[i] + 64 j (d <= fmax1), f = 21; each row's c4 window
 //            opens find3 rows T' = T - c4^6 over c3.
@@ -87,6 +90,7 @@ constexpr u32 kItemRows = 64;
 // heaviest item short next to a pass.
 constexpr u32 kItemRows617 = 8;
 S615_HD u32 item_rows(u32 cls) { return cls == 7u ? kItemRows617 : kItemRows; }
+constexpr u32 kC4Chunk = 128;   // cls 1: c4 values per work item
 constexpr u32 kMaxBatchUnits = 1u << 24;
 S615_HD u64 make_item(u32 unit, u32 ires, u32 chunk) {
   return ((u64)unit << 32) | ((u64)ires << 24) | chunk;

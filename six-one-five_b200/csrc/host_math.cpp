@@ -5,6 +5,7 @@
 // (fourcore_cls5_gpu_v4.cu:169-184) and adds the divisibility checks the
 // device row arithmetic relies on.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <numeric>
 #include <vector>
@@ -325,10 +326,71 @@ static int make_dev_unit617(const s615_unit& in, DevUnit* out, bool* skip) {
   return S615_OK;
 }
 
+// floor(T^(1/6)) and the least c >= 1 with k c^6 >= T, exactly (T < 2^126).
+static u32 iroot6_exact(u128 T) {
+  const double x = (double)(u64)(T >> 64) * 18446744073709551616.0 + (double)(u64)T;
+  u64 a = x < 1.0 ? 0 : (u64)std::pow(x, 1.0 / 6.0);
+  while (pow6_u128(a + 1) <= T) ++a;
+  while (a && pow6_u128(a) > T) --a;
+  return (u32)a;
+}
+static u32 least_c_k(u128 T, u32 k) {
+  const double x = (double)(u64)(T >> 64) * 18446744073709551616.0 + (double)(u64)T;
+  u64 c = (u64)std::pow(x / k, 1.0 / 6.0);
+  if (c < 1) c = 1;
+  while ((u128)k * pow6_u128(c) < T) ++c;
+  while (c > 1 && (u128)k * pow6_u128(c - 1) >= T) --c;
+  return (u32)c;
+}
+
+// cls 1: the find4 unit of fourcore_find_v4 (expand_unit :172-176, make_cand
+// mode 4 :415-419): T = (B^6 - u^6)/42^6 exact, c4 window [lo4, hi4] with
+// hi4 = min(iroot6(T), lim), lo4 the least c with 4 c^6 >= T; an empty window
+// is dropped like run_batch drops it (:486).
+static int make_dev_unit1(const s615_unit& in, DevUnit* out, bool* skip) {
+  out->cls = 1;
+  out->f = 0;
+  W3 R;
+  u32 lim = 0;
+  if (in.kind == 0) {
+    const u64 B = in.B, u = in.u;
+    if (B < 2 || B > kMaxB || u == 0) return S615_E_FORMAT;
+    if (u >= B) { *skip = true; return S615_OK; }
+    R = pow6_w3(B);
+    sub_w3(R, pow6_w3(u));
+    lim = (u32)((B - 1) / 42);
+  } else if (in.kind == 1) {
+    R = W3{{in.base[0], in.base[1], in.base[2]}};
+    if (in.lim >= (1u << 21)) return S615_E_FORMAT;
+    lim = in.lim;
+  } else {
+    return S615_E_FORMAT;
+  }
+  if (zero_w3(R) || divmod_w3(R, kM42) != 0 || R.l[2] != 0 || (R.l[1] >> 62) != 0)
+    return S615_E_FORMAT;   // not a class-1 target, or T outside exact device range
+  const u128 T = ((u128)R.l[1] << 64) | R.l[0];
+  const u32 hi4 = std::min(iroot6_exact(T), lim);
+  const u32 lo4 = least_c_k(T, 4);
+  if (hi4 < 1 || lo4 > hi4) { *skip = true; return S615_OK; }
+  out->B = in.B; out->u = in.u;
+  out->lim = lim;
+  out->base_lo = (u64)T;
+  out->base_hi = (u64)(T >> 64);
+  out->fmax1 = hi4;
+  out->fmax2 = lo4;
+  out->nres1 = 1;
+  return S615_OK;
+}
+
 int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip) {
   std::memset(out, 0, sizeof *out);
   *skip = false;
   const u32 cls = in.cls;
+  if (cls == 1) {
+    const int s = make_dev_unit1(in, out, skip);
+    out->id = id;
+    return s;
+  }
   if (cls == S615_CLS_617) {
     const int s = make_dev_unit617(in, out, skip);
     out->id = id;
@@ -406,6 +468,11 @@ int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip) {
 }
 
 void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out) {
+  if (d.cls == 1) {   // chunks of the c4 window
+    const u32 n = (d.fmax1 - d.fmax2) / kC4Chunk + 1;
+    for (u32 c = 0; c < n; ++c) out.push_back(make_item(unit_index, 0, c));
+    return;
+  }
   const u32 per = item_rows(d.cls);
   for (u32 ir = 0; ir < d.nres1; ++ir) {
     u32 jmin = 0, jend = 0;

@@ -43,12 +43,14 @@ constexpr u32 kQ = 64;              // probe ring capacity (power of two)
 constexpr u32 kCQ = 64;             // c4 queue capacity (power of two)
 constexpr u32 kLenMask = 0x0FFFFFFFu;
 constexpr u32 kFull = 0xFFFFFFFFu;
+constexpr u32 kC4Bits = 21;         // c4 <= lim < 2^21 (B <= 40,000,000)
+constexpr u32 kC4Mask = (1u << kC4Bits) - 1u;
 
 struct WarpSmem617 {
   RowRec rows[kBuf];     // W = T', a = lo3, b = len | m4 << 28
-  u32 aux[kBuf];         // c4 | (row index in the item) << 16
+  u32 aux[kBuf];         // c4 | (row index in the item) << kC4Bits
   u32 pre[kBuf + 1];     // first 32-column chunk of each buffered row
-  u32 cq[kCQ];           // c4 queue: c4 | (lane holding the row) << 16
+  u32 cq[kCQ];           // c4 queue: c4 | (lane holding the row) << kC4Bits
   u32 ring[kQ];          // probe ring: column (18 bits) | buffer row << 18
 };
 
@@ -90,7 +92,7 @@ template <bool kSharp>
 constexpr size_t smem_total617() { return smem_pat617<kSharp>() + kSmemTri + kWarps * sizeof(Warp617T<kSharp>); }
 
 struct Item617 {
-  u32 unit_id, r0, mod, j0, lim;
+  u32 unit_id, r0, mod, j0, lim, cls;
 };
 
 // Per-warp state carried through one item.
@@ -115,9 +117,9 @@ __device__ __forceinline__ void probe_batch(const Peel617Params& P, const WarpSm
       const u32 aux = W.aux[r];
       s615_hit h;
       h.unit = I.unit_id; h.a = 0; h.b = 0;
-      h.d = I.r0 + I.mod * (I.j0 + (aux >> 16));   // the x21 term
+      h.d = I.r0 + I.mod * (I.j0 + (aux >> kC4Bits));   // the x21 term (0 for cls 1)
       h.e = c3;
-      h.c4 = aux & 0xFFFFu;
+      h.c4 = aux & kC4Mask;
       h.fp = key;
       P.hits[idx] = h;
     }
@@ -200,8 +202,8 @@ __device__ __forceinline__ void make_rows(const Peel617Params& P, Warp617T<kShar
                                           u32 lane, u32 ch, u32 cnt, u32 h, u64 tl, u64 th) {
   const bool act = lane < cnt;
   const u32 e = W.cq[(ch + lane) & (kCQ - 1)];
-  const u32 src = act ? (e >> 16) & 31u : 0u;
-  const u32 c4 = e & 0xFFFFu;
+  const u32 src = act ? (e >> kC4Bits) & 31u : 0u;
+  const u32 c4 = e & kC4Mask;
   const u64 Tl = __shfl_sync(kFull, tl, src), Th = __shfl_sync(kFull, th, src);
   RowRec R;
   u16 offx[4] = {0, 0, 0, 0};
@@ -215,7 +217,10 @@ __device__ __forceinline__ void make_rows(const Peel617Params& P, Warp617T<kShar
       const u128 T2 = T - c6;
       const u32 hi3 = min(min(iroot6_u128(T2), I.lim), c4);
       if (hi3 >= 1) {
-        const u32 lo3 = least_c_3c6(T2);
+        // cls 7: least c with 3 c^6 >= T' (min_c_fix); cls 1: (u32)(0.8 hi3), at
+        // least 1 (k_find4, fourcore_find_v4.cu:312-314; 0.8 hi3 never lands within
+        // 2^-20 of an integer, so the integer form is the same)
+        const u32 lo3 = I.cls == 1 ? max(1u, (4u * hi3) / 5u) : least_c_3c6(T2);
         if (lo3 <= hi3) {
           len = hi3 - lo3 + 1u;
           R.wlo = (u64)T2; R.whi = (u64)(T2 >> 64);
@@ -253,7 +258,7 @@ __device__ __forceinline__ void make_rows(const Peel617Params& P, Warp617T<kShar
       W.m32[slot] = m32;
       for (int k = 0; k < 4; ++k) W.offx[slot][k] = offx[k];
     }
-    W.aux[slot] = c4 | ((h + src) << 16);
+    W.aux[slot] = c4 | ((h + src) << kC4Bits);
     S.pos += len;
   }
   S.nbuf += nnew;
@@ -288,13 +293,21 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Par
     const DevUnit* U = P.units + item_unit(packed);
     Item617 I;
     I.unit_id = U->id;
-    I.r0 = U->res1[item_res(packed)];
-    I.mod = U->mod1;
+    I.cls = U->cls;
     I.lim = U->lim;
-    u32 jmin, jend;
-    class_rows(I.r0, I.mod, U->fmax1, &jmin, &jend);
-    I.j0 = jmin + item_chunk(packed) * kItemRows617;
-    const u32 nrows = min(kItemRows617, jend - I.j0);
+    u32 nrows;
+    if (I.cls == 1) {   // one row, T = base; this item's c4 are a chunk of [fmax2, fmax1]
+      I.r0 = 0; I.mod = 0; I.j0 = 0;
+      nrows = 1;
+    } else {
+      I.r0 = U->res1[item_res(packed)];
+      I.mod = U->mod1;
+      u32 jmin, jend;
+      class_rows(I.r0, I.mod, U->fmax1, &jmin, &jend);
+      I.j0 = jmin + item_chunk(packed) * kItemRows617;
+      nrows = min(kItemRows617, jend - I.j0);
+    }
+    const bool tri = P.use_tri && I.cls != 1;   // cls 1 (k_find4) has no triple-sum gate
     const u128 base = ((u128)U->base_hi << 64) | U->base_lo;
     S.nbuf = 0; S.head = 0; S.qlen = 0;
     __syncwarp();
@@ -303,7 +316,16 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Par
       // ---- the row of this lane: T(d), its c4 window and T mod 504 / 247 ----
       u64 tl = 0, th = 0;
       u32 lo4 = 0, len4 = 0, q504 = 0, q247 = 0;
-      if (h + lane < nrows) {
+      if (I.cls == 1) {
+        if (lane == 0) {
+          const u32 c0 = U->fmax2 + item_chunk(packed) * kC4Chunk;
+          if (c0 <= U->fmax1) {
+            tl = U->base_lo; th = U->base_hi;
+            lo4 = c0;
+            len4 = min(kC4Chunk, U->fmax1 - c0 + 1u);
+          }
+        }
+      } else if (h + lane < nrows) {
         const u64 x = 21ull * ((u64)I.r0 + (u64)I.mod * (I.j0 + h + lane));
         const u128 x3 = (u128)(x * x) * x;
         const u128 Rm = base - x3 * x3;                          // R mod 2^128
@@ -322,7 +344,7 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Par
           }
         }
       }
-      if (P.use_tri) my_tri += len4;
+      if (tri) my_tri += len4;
       // ---- c4 step: triple-sum gate, survivors to the c4 queue ----
       u32 ch = 0, cl = 0;
       const u32 nd = min(32u, nrows - h);
@@ -334,7 +356,7 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Par
         for (u32 c0 = 0; c0 < L; c0 += 32u) {
           const u32 c4 = lo + c0 + lane;
           bool pass = c0 + lane < L;
-          if (pass && P.use_tri) {
+          if (pass && tri) {
             u32 x = a504 + 504u - p6_504[c4 % 504u];
             if (x >= 504u) x -= 504u;
             u32 y = a247 + 247u - p6_247[c4 % 247u];
@@ -344,7 +366,7 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Par
             if (!pass) ++my_skip;
           }
           const u32 bal = __ballot_sync(kFull, pass);
-          if (pass) W.cq[(ch + cl + __popc(bal & lanemask_lt())) & (kCQ - 1)] = c4 | (j << 16);
+          if (pass) W.cq[(ch + cl + __popc(bal & lanemask_lt())) & (kCQ - 1)] = c4 | (j << kC4Bits);
           cl += __popc(bal);
           if (cl >= 32u) {
             __syncwarp();

@@ -39,7 +39,13 @@ __global__ void k_verify(const DevUnit* __restrict__ units, const s615_hit* __re
     const u128 base = ((u128)U.base_hi << 64) | U.base_lo;
     u128 S;
     u32 cmax;
-    if (U.cls == 5) {
+    if (U.cls == 1) {   // base holds T; S = T - c4^6 - c3^6, pairs up to N
+      const u128 T = base;
+      const u128 c46 = pow6_small(H.c4) + pow6_small(H.e);
+      if (T <= c46) continue;
+      S = T - c46;
+      cmax = N;
+    } else if (U.cls == 5) {
       const u64 x = 14ull * H.e;
       const u128 x3 = (u128)(x * x) * x;
       const u128 V = (base - x3 * x3) * inv21;
@@ -157,6 +163,31 @@ int verify_device(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s
     S.c1 = p.c1; S.c2 = p.c2;
     W3 rhs;   // the peeled terms plus 42^6 times the core
     long long t[5];
+    if (U.cls == 1) {   // B^6 = u^6 + 42^6 (c1^6 + c2^6 + c3^6 + c4^6)
+      S.c3 = H.e; S.c4 = H.c4;
+      const u128 core = pow6_u128(p.c1) + pow6_u128(p.c2) + pow6_u128(H.e) + pow6_u128(H.c4);
+      rhs = mul_w3_u64(W3{{(u64)core, (u64)(core >> 64), 0}}, kM42);
+      if (U.kind == 1) {
+        if (!eq_w3(rhs, W3{{U.base[0], U.base[1], U.base[2]}})) continue;
+      } else {
+        add_w3(rhs, pow6_w3(U.u));
+        if (!eq_w3(rhs, pow6_w3(U.B))) continue;
+        t[0] = 42LL * p.c1; t[1] = 42LL * p.c2; t[2] = 42LL * H.e; t[3] = 42LL * H.c4;
+        t[4] = (long long)U.u;
+        std::sort(t, t + 5);
+        bool bad = false;
+        for (int i = 0; i < 4; ++i) if (t[i] == t[i + 1]) bad = true;
+        if (bad || t[4] >= (long long)U.B || t[0] < 1) continue;
+        long long g = t[0];
+        for (int i = 1; i < 5; ++i) g = std::gcd(g, t[i]);
+        g = std::gcd(g, (long long)U.B);
+        for (int i = 0; i < 5; ++i) S.a[i] = t[i];
+        S.gcd = g;
+      }
+      if (k < cap) out[k] = S;
+      ++k;
+      continue;
+    }
     if (U.cls == S615_CLS_617) {
       S.d = H.d; S.c3 = H.e; S.c4 = H.c4; S.w = U.w;
       rhs = pow6_w3(21ULL * H.d);

@@ -225,6 +225,16 @@ def candidates617(B: int):
     return arr, n.value
 
 
+def make_plant1(c: Sequence[int], lim: int, B: int = 0) -> Unit:
+    """A planted class-1 (find4) target: base = 42^6 (c1^6 + c2^6 + c3^6 + c4^6)."""
+    base = 42**6 * sum(x**6 for x in c)
+    x = Unit()
+    x.cls, x.kind, x.B, x.lim = 1, 1, B, lim
+    for i in range(3):
+        x.base[i] = (base >> (64 * i)) & (2**64 - 1)
+    return x
+
+
 def make_units617(triples: Iterable[Tuple[int, int, int]]) -> "C.Array":
     """(6,1,7) Branch-A class-5 candidates (B, u = 14u', w = 6v')."""
     triples = list(triples)
@@ -413,6 +423,8 @@ def solution_line(s: Solution) -> str:
         if s.cls == S615_CLS_617:
             return (f"PLANT cls=7 unit={s.unit} d={s.d} c1={s.c1} c2={s.c2} c3={s.c3} "
                     f"c4={s.c4}")
+        if s.cls == 1:
+            return f"PLANT cls=1 unit={s.unit} c1={s.c1} c2={s.c2} c3={s.c3} c4={s.c4}"
         return f"PLANT cls={s.cls} unit={s.unit} d={s.d} c1={s.c1} c2={s.c2} c3={s.c3}"
     a = list(s.a)
     if s.cls == S615_CLS_617:
