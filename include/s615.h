@@ -70,6 +70,12 @@ typedef struct s615_table_info {
  * + k_find4, fourcore_find_v4.cu:165-176,406-420,287-338),
  * B^6 = u^6 + 42^6 (c1^6 + c2^6 + c3^6 + c4^6); a cls 1 plant has
  * base = 42^6 (c1^6 + .. + c4^6) and lim < 2^21.
+ * cls 8 (S615_CLS_617_FIND4): one find4 job of the (6,1,7) Branch-A classes
+ * 1-4 (gen_class_cands + push_find5_cand + set_window4_gen + k_find4,
+ * solve_617_v1.cu:807-884,766-803,507-560), as s615_617_jobs makes them:
+ * base[0..1] = Q4 = c1^6 + .. + c4^6 (the target after the c5 peel), B, u, w
+ * (the sixth anchor term), lim, fmax2..fmax1 = the c4 window, res_e = c5 and
+ * res_d = the (6,1,7) class (1-4).
  * cls 7 (S615_CLS_617): the (6,1,7) Branch-A class-5 candidate of
  * solve_617_v1.cu:885-906, B^6 = u^6 + w^6 + (21d)^6 + 42^6 (c1^6+..+c4^6)
  * with u = 14u', w = 6v', d over residues mod 2^6 (d <= (B-1)/21) and the
@@ -85,8 +91,9 @@ typedef struct s615_table_info {
  * units with base <= 0 are dropped like the reference drops them.  A cls 7
  * plant (solve_617_v1.cu:1564-1582) has base < 2^127 and lim < 65536. */
 #define S615_CLS_617 7
+#define S615_CLS_617_FIND4 8
 typedef struct s615_unit {
-  uint32_t cls;      /* 1, 2, 3, 4, 5 or 7 */
+  uint32_t cls;      /* 1, 2, 3, 4, 5, 7 or 8 */
   uint32_t kind;     /* 0 = (B,u) or (B,u,w), 1 = planted base */
   uint64_t B, u;
   uint64_t base[3];  /* kind 1 only */
@@ -127,6 +134,8 @@ typedef struct s615_counters {
  *   cls 5  : B^6 = u^6 + (21d)^6 + (14e)^6 + 42^6 (c1^6 + c2^6)           n = 5
  *   cls 2-4: B^6 = u^6 + (f d)^6 + 42^6 (c1^6 + c2^6 + c3^6), f = 14, 21, 7 n = 5
  *   cls 7  : B^6 = u^6 + w^6 + (21d)^6 + 42^6 (c1^6 + .. + c4^6)         n = 7
+ *   cls 8  : B^6 = u^6 + w^6 + 42^6 (c1^6 + .. + c4^6 + c5^6)            n = 7
+ *            (d holds the (6,1,7) class 1-4 and e holds c5)
  * (for plants the left side is base + u^6, or base + u^6 + w^6).  cls 7
  * reports each distinct 7-tuple once per call, like the reference's reported
  * set (solve_617_v1.cu:1096). */
@@ -195,6 +204,11 @@ int s615_unit_candidates(uint64_t B, int cls, uint64_t* out, size_t cap, size_t*
  * then w, ascending).  Writes min(cap, count) records; *n = count;
  * S615_E_OVERFLOW when cap is short; S615_E_ARG for B > 2,353,973. */
 int s615_617_candidates(uint64_t B, s615_unit* out, size_t cap, size_t* n);
+/* gen_class_cands(cls in 1..4) of the (6,1,7) solver with its c5 expansion
+ * (solve_617_v1.cu:807-884 over the full u band, push_find5_cand and
+ * set_window4_gen :766-803): the cls 8 find4 jobs of one B, in the
+ * reference's order.  Same return rules as s615_617_candidates. */
+int s615_617_jobs(uint64_t B, int cls, s615_unit* out, size_t cap, size_t* n);
 /* What a run does with one unit: S615_OK = searched, 1 = dropped like
  * pack_unit5 drops it (u >= B or an empty residue class), S615_E_FORMAT =
  * rejected (outside the engine's exact-arithmetic range, or a planted base

@@ -49,6 +49,12 @@ class OrcHit4(C.Structure):
                 ("fp", C.c_uint64)]
 
 
+class OrcJob617(C.Structure):
+    _fields_ = [("Q4", C.c_uint64 * 2), ("B", C.c_uint32), ("u", C.c_uint32), ("w", C.c_uint32),
+                ("cls", C.c_uint32), ("c5", C.c_uint32), ("lim", C.c_uint32), ("lo", C.c_uint32),
+                ("hi", C.c_uint32)]
+
+
 class OrcCand617(C.Structure):
     _fields_ = [("base", C.c_uint64 * 2), ("B", C.c_uint32), ("u", C.c_uint32), ("w", C.c_uint32),
                 ("lim", C.c_uint32), ("mod1", C.c_uint32), ("fmax1", C.c_uint32),
@@ -92,6 +98,10 @@ _SIG = {
     "orc_expand_cls1": (C.c_size_t, [C.c_uint64, C.c_uint64, _P, C.c_size_t]),
     "orc_find4_run": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_int, _P, C.c_size_t,
                                    _P]),
+    "orc_617_jobs": (C.c_size_t, [C.c_uint64, C.c_int, _P, C.c_size_t]),
+    "orc_617_find4_run": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_int, _P,
+                                       C.c_size_t, _P]),
+    "orc_617_find4_verify": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_char_p, C.c_size_t, _P]),
     "orc_617_cands": (C.c_size_t, [C.c_uint64, _P, C.c_size_t]),
     "orc_617_run": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_int, _P,
                                  C.c_size_t, _P]),
@@ -328,3 +338,43 @@ def run_find4(table: Table, jobs, n: int, use_gate: bool = True, ref_tiles: bool
         raise RuntimeError("oracle hit buffer overflow")
     raw = np.frombuffer(C.string_at(C.addressof(hits), nh * C.sizeof(OrcHit4)), dtype=HIT4_DTYPE)
     return raw.copy(), [int(x) for x in ctr]
+
+
+def jobs617(B: int, cls: int):
+    """gen_class_cands(cls in 1..4) of solve_617_v1.cu with the c5 expansion: find4 jobs."""
+    n = lib().orc_617_jobs(B, cls, None, 0)
+    arr = (OrcJob617 * max(n, 1))()
+    lib().orc_617_jobs(B, cls, C.cast(arr, C.c_void_p), n)
+    return arr, n
+
+
+def concat_jobs617(parts):
+    n = sum(k for _, k in parts)
+    out = (OrcJob617 * max(n, 1))()
+    i = 0
+    for arr, k in parts:
+        C.memmove(C.byref(out, i * C.sizeof(OrcJob617)), arr, k * C.sizeof(OrcJob617))
+        i += k
+    return out, n
+
+
+def run617_find4(table: Table, jobs, n: int, use_gate: bool = True, use_tri: bool = True,
+                 ymax: int = 1, threads: int = 0, cap: int = 1 << 20):
+    hits = (OrcHit4 * cap)()
+    ctr = np.zeros(5, dtype=np.uint64)
+    nh = lib().orc_617_find4_run(table.h, C.cast(jobs, C.c_void_p), n, int(use_gate), int(use_tri),
+                                 ymax, threads, C.cast(hits, C.c_void_p), cap, _ptr(ctr))
+    if nh > cap:
+        raise RuntimeError("oracle hit buffer overflow")
+    raw = np.frombuffer(C.string_at(C.addressof(hits), nh * C.sizeof(OrcHit4)), dtype=HIT4_DTYPE)
+    return raw.copy(), [int(x) for x in ctr]
+
+
+def verify617_find4(jobs, hits: np.ndarray, N: int, stats: list = None):
+    h = np.ascontiguousarray(hits.astype(HIT4_DTYPE))
+    buf = C.create_string_buffer(1 << 20)
+    st = np.zeros(2, dtype=np.uint64)
+    lib().orc_617_find4_verify(C.cast(jobs, C.c_void_p), _ptr(h), h.size, N, buf, len(buf), _ptr(st))
+    if stats is not None:
+        stats[:] = [int(st[0]), int(st[1])]
+    return [l for l in buf.value.decode().splitlines() if l]

@@ -1112,3 +1112,248 @@ size_t orc_617_verify(const orc_cand617* cands, const orc_hit617* hits, size_t n
 }
 
 }  // extern "C"
+
+// ================================================ (6,1,7) Branch-A cls 1-4
+namespace {
+
+// exact floor sixth root (iroot6_i128, solve_617_v1.cu:192-201)
+long long o617_iroot6(i128 n) {
+  if (n <= 0) return 0;
+  long long lo = 0, hi = 1;
+  while ((i128)pow6_u128(hi) <= n) hi <<= 1;
+  while (hi - lo > 1) {
+    const long long mid = (lo + hi) >> 1;
+    if ((i128)pow6_u128(mid) <= n) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+// least c >= 1 with k c^6 >= Q (the estimate-and-fix loops of :773-776, :788-791)
+long long o617_least(i128 Q, int k) {
+  long long c = 1;
+  while ((i128)k * (i128)pow6_u128(c) < Q) ++c;
+  return c;
+}
+
+std::vector<long long> o617_seeds616(long long B, int cls) {   // :267-275
+  if (cls == 4) {                                              // classes_d_cls4 (:256-264)
+    const Roots& rt = roots();
+    const long long t2 = mod_pow6(B, kM2) * mod_inv(mod_pow6(7, kM2), kM2) % kM2;
+    const long long t3 = mod_pow6(B, kM3) * mod_inv(mod_pow6(7, kM3), kM3) % kM3;
+    std::vector<long long> out;
+    for (long long a : rt.r2[t2]) for (long long b : rt.r3[t3]) out.push_back(crt2(a, kM2, b, kM3));
+    std::sort(out.begin(), out.end());
+    return out;
+  }
+  return seeds_for_B(B, cls);
+}
+long long o617_mod616(int cls) {
+  return cls == 1 ? 5489031744LL : cls == 2 ? 7529536LL : cls == 3 ? 85766121LL : kM2 * kM3;
+}
+bool o617_unit_ok616(long long u, int cls) {                   // :282-290
+  switch (cls) {
+    case 1: return (u & 1) && std::gcd(u, 42LL) == 1;
+    case 2: return (u & 1) && (u % 3 == 0);
+    case 3: return !(u & 1) && std::gcd(u, 21LL) == 1;
+    case 4: return (u % 7 == 0);
+  }
+  return true;
+}
+
+// push_find5_cand + set_window4_gen (:766-803)
+void o617_push_find5(orc_job617 J0, i128 Q, long long c5cap, std::vector<orc_job617>& out) {
+  long long hi5 = std::min(o617_iroot6(Q), (long long)J0.lim);
+  if (hi5 > c5cap) hi5 = c5cap;
+  const long long lo5 = o617_least(Q, 5);
+  if (lo5 > hi5) return;
+  for (long long c5 = lo5; c5 <= hi5; ++c5) {
+    const i128 Q4 = Q - (i128)pow6_u128(c5);
+    if (Q4 < 4) continue;
+    long long hi4 = std::min(o617_iroot6(Q4), (long long)J0.lim);
+    if (hi4 > c5) hi4 = c5;
+    const long long lo4 = o617_least(Q4, 4);
+    if (lo4 > hi4) continue;
+    orc_job617 J = J0;
+    J.Q4[0] = (u64)(u128)Q4; J.Q4[1] = (u64)((u128)Q4 >> 64);
+    J.c5 = (u32)c5; J.lo = (u32)lo4; J.hi = (u32)hi4;
+    out.push_back(J);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t orc_617_jobs(uint64_t Bu, int cls, orc_job617* out, size_t cap) {   // :807-884, full band
+  const long long B = (long long)Bu;
+  const long long lo = 1, hi = B - 1;
+  const i128 B6 = (i128)pow6_u128(Bu);
+  const u32 lim = (u32)((B - 1) / 42);
+  const auto lift = [](const std::vector<long long>& res, long long m, long long maxv) {
+    return lift617(res, m, maxv);
+  };
+  std::vector<long long> uvals;
+  if (cls == 4) {
+    for (long long x : lift(o617_seeds616(B, 4), kM2 * kM3, (B - 1) / 7)) {
+      const long long u = 7 * x;
+      if (u >= lo && u <= hi) uvals.push_back(u);
+    }
+  } else {
+    const long long M = o617_mod616(cls);
+    for (long long s : o617_seeds616(B, cls)) {
+      long long u0 = s % M;
+      if (u0 < lo) u0 += (lo - u0 + M - 1) / M * M;
+      for (long long u = u0; u <= hi; u += M)
+        if (o617_unit_ok616(u, cls)) uvals.push_back(u);
+    }
+  }
+  std::sort(uvals.begin(), uvals.end());
+  uvals.erase(std::unique(uvals.begin(), uvals.end()), uvals.end());
+  std::vector<orc_job617> jobs;
+  for (long long u : uvals) {
+    const i128 u6 = (i128)pow6_u128((u64)u);
+    if (u6 >= B6) continue;
+    orc_job617 J0{};
+    J0.B = (u32)B; J0.u = (u32)u; J0.cls = (u32)cls; J0.lim = lim;
+    if (cls == 1) {
+      const i128 R = B6 - u6;
+      if (R % (i128)kM42 != 0) continue;
+      const i128 Q0 = R / (i128)kM42;
+      const long long wmax = std::min((long long)lim, o617_iroot6(Q0 - 5));
+      for (long long w = 1; w <= wmax; ++w) {
+        const i128 Q = Q0 - (i128)pow6_u128((u64)w);
+        if (Q < 5) break;
+        J0.w = (u32)(42 * w);
+        o617_push_find5(J0, Q, w, jobs);
+      }
+    } else {
+      long long f, vmod, vmax;
+      std::vector<long long> vres;
+      if (cls == 2) { f = 14; vres = classes_d_cls2(B); vmod = kM3; vmax = (B - 1) / 14; }
+      else if (cls == 3) { f = 21; vres = classes_d_cls3(B, u); vmod = kM2; vmax = (B - 1) / 21; }
+      else {
+        f = 6;
+        vres = roots().r7[mod_pow6(B, kM7) * mod_inv(mod_pow6(6, kM7), kM7) % kM7];
+        vmod = kM7; vmax = (B - 1) / 6;
+      }
+      for (long long v : lift(vres, vmod, vmax)) {
+        const i128 R = B6 - u6 - (i128)pow6_u128((u64)(f * v));
+        if (R <= 0 || R % (i128)kM42 != 0) continue;
+        const i128 Q = R / (i128)kM42;
+        if (Q < 5) continue;
+        J0.w = (u32)(f * v);
+        o617_push_find5(J0, Q, lim, jobs);
+      }
+    }
+  }
+  for (size_t i = 0; i < jobs.size() && i < cap; ++i) out[i] = jobs[i];
+  return jobs.size();
+}
+
+size_t orc_617_find4_run(const orc_table* t, const orc_job617* jobs, size_t n, int use_gate,
+                         int use_tri, int ymax, int threads, orc_hit4x* hits, size_t cap,
+                         uint64_t counters[5]) {   // k_find4 (:507-560)
+  const Gate& G = gate();
+  static const std::vector<uint8_t> t504 = tri_set(504), t247 = tri_set(247);
+  u64 c_calls = 0, c_gated = 0, c_tri_tot = 0, c_tri_skip = 0;
+  size_t nh = 0;
+#ifdef _OPENMP
+  const int nt = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nt) reduction(+ : c_calls, c_gated, c_tri_tot, c_tri_skip)
+#endif
+  for (long long ci = 0; ci < (long long)n; ++ci) {
+    const orc_job617& J = jobs[ci];
+    const u128 Q = ((u128)J.Q4[1] << 64) | J.Q4[0];
+    const u32 q504 = (u32)(Q % 504), q247 = (u32)(Q % 247);
+    std::vector<orc_hit4x> local;
+    for (u32 c4 = J.lo; c4 <= J.hi; ++c4) {
+      const u64 mult = ymax <= 1 ? 1 : std::min<u64>((u64)ymax, (c4 - J.lo) / 2048 + 1);
+      const u32 t4504 = (q504 + 504 - G.p6504[c4 % 504]) % 504;
+      const u32 t4247 = (q247 + 247 - G.p6247[c4 % 247]) % 247;
+      if (use_tri) {
+        c_tri_tot += mult;
+        if (!t504[t4504] || !t247[t4247]) { c_tri_skip += mult; continue; }
+      }
+      const u128 c46 = pow6_u128(c4);
+      if (c46 >= Q) continue;
+      const u128 R2 = Q - c46;
+      u32 hi3 = (u32)o617_iroot6((i128)R2);
+      const u32 capm = J.lim < c4 ? J.lim : c4;
+      if (hi3 > capm) hi3 = capm;
+      if (hi3 < 1) continue;
+      const u32 lo3 = (u32)o617_least((i128)R2, 3);
+      const u64 tfp = J.Q4[0] - (u64)c46;
+      for (u32 c3 = lo3; c3 <= hi3; ++c3) {
+        if (use_gate) {
+          const u32 x = (t4504 + 504 - G.p6504[c3 % 504]) % 504;
+          const u32 y = (t4247 + 247 - G.p6247[c3 % 247]) % 247;
+          if (!(G.g504[x] && G.g247[y])) { c_gated += mult; continue; }
+        }
+        c_calls += mult;
+        const u64 c32 = (u64)c3 * c3;
+        const u64 key = tfp - c32 * c32 * c32;
+        if (might_contain(*t, key))
+          for (u64 k = 0; k < mult; ++k) local.push_back(orc_hit4x{(u32)ci, c3, c4, 0, key});
+      }
+    }
+    if (!local.empty()) {
+#pragma omp critical(orc_hits4x)
+      {
+        for (const auto& h : local) { if (nh < cap) hits[nh] = h; ++nh; }
+      }
+    }
+  }
+  counters[0] = c_calls; counters[1] = c_gated; counters[2] = 3 * c_calls;
+  counters[3] = c_tri_tot; counters[4] = c_tri_skip;
+  return nh;
+}
+
+size_t orc_617_find4_verify(const orc_job617* jobs, const orc_hit4x* hits, size_t nh, int N,
+                            char* buf, size_t buflen, uint64_t stats[2]) {   // verify_hit cls <= 4
+  u64 n_exact = 0, n_false = 0;
+  PairRecover pr(N);
+  std::vector<std::pair<u32, u32>> pairs;
+  std::vector<std::array<long long, 7>> reported;
+  std::string text;
+  size_t lines = 0;
+  for (size_t k = 0; k < nh; ++k) {
+    const orc_hit4x& H = hits[k];
+    const orc_job617& J = jobs[H.job];
+    const u128 q = ((u128)J.Q4[1] << 64) | J.Q4[0];
+    pr.recover(H.fp, pairs);
+    for (auto [a, b] : pairs) {
+      if (pow6_u128(a) + pow6_u128(b) + pow6_u128(H.c3) + pow6_u128(H.c4) != q) { ++n_false; continue; }
+      ++n_exact;
+      std::array<long long, 7> t = {42LL * a, 42LL * b, 42LL * H.c3, 42LL * H.c4, 42LL * J.c5,
+                                    (long long)J.w, (long long)J.u};
+      std::sort(t.begin(), t.end());
+      bool bad = false;
+      for (int i = 0; i < 6; ++i) if (t[i] == t[i + 1]) bad = true;
+      if (bad || t[6] >= (long long)J.B || t[0] < 1) continue;
+      i128 lhs = (i128)pow6_u128(J.B);
+      for (long long x : t) { lhs -= (i128)pow6_u128((u64)x); if (lhs < 0) break; }
+      if (lhs != 0) continue;
+      if (std::find(reported.begin(), reported.end(), t) != reported.end()) continue;
+      reported.push_back(t);
+      long long g = std::gcd(t[0], t[1]);
+      for (int i = 2; i < 7; ++i) g = std::gcd(g, t[i]);
+      g = std::gcd(g, (long long)J.B);
+      char line[256];
+      std::snprintf(line, sizeof line,
+                    "SOLUTION cls=%u B=%u a1=%lld a2=%lld a3=%lld a4=%lld a5=%lld a6=%lld a7=%lld "
+                    "(anchor=%u) gcd=%lld %s\n",
+                    J.cls, J.B, t[0], t[1], t[2], t[3], t[4], t[5], t[6], J.u, g,
+                    g == 1 ? "primitive" : "NON-PRIMITIVE");
+      text += line;
+      ++lines;
+    }
+  }
+  if (stats) { stats[0] = n_exact; stats[1] = n_false; }
+  if (buf && buflen) {
+    const size_t c = std::min(buflen - 1, text.size());
+    std::memcpy(buf, text.data(), c);
+    buf[c] = 0;
+  }
+  return lines;
+}
+
+}  // extern "C"

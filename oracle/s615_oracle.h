@@ -160,6 +160,27 @@ size_t orc_617_run(const orc_table* t, const orc_cand617* cands, size_t n, int u
 size_t orc_617_verify(const orc_cand617* cands, const orc_hit617* hits, size_t nh, int N,
                       int planted, char* buf, size_t buflen, uint64_t stats[2]);
 
+/* ---- (6,1,7) Branch-A classes 1-4: find5 by c5 expansion, then find4
+ * (solve_617_v1.cu:807-884 gen_class_cands, :766-803 push_find5_cand /
+ * set_window4_gen, :507-560 k_find4, :1040-1110 verify_hit) ---- */
+typedef struct orc_job617 {
+  uint64_t Q4[2];          /* Q - c5^6 = c1^6 + .. + c4^6 */
+  uint32_t B, u, w, cls;   /* w: the sixth anchor term (42w', 14v', 21v' or 6v') */
+  uint32_t c5, lim, lo, hi;/* c4 window [lo, hi] */
+} orc_job617;
+typedef struct orc_hit4x {
+  uint32_t job, c3, c4, pad;
+  uint64_t fp;
+} orc_hit4x;
+size_t orc_617_jobs(uint64_t B, int cls, orc_job617* out, size_t cap);
+/* counters as orc_617_run; ymax > 1 repeats c4 as the reference's y tiles do
+ * (block y walks c4 >= lo + 2048 y, ymax = the batch's tile count). */
+size_t orc_617_find4_run(const orc_table* t, const orc_job617* jobs, size_t n, int use_gate,
+                         int use_tri, int ymax, int threads, orc_hit4x* hits, size_t cap,
+                         uint64_t counters[5]);
+size_t orc_617_find4_verify(const orc_job617* jobs, const orc_hit4x* hits, size_t nh, int N,
+                            char* buf, size_t buflen, uint64_t stats[2]);
+
 #ifdef __cplusplus
 }
 #endif

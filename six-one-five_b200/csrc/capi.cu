@@ -471,6 +471,14 @@ int s615_617_candidates(uint64_t B, s615_unit* out, size_t cap, size_t* n) {
   return v.size() > cap ? S615_E_OVERFLOW : S615_OK;
 }
 
+int s615_617_jobs(uint64_t B, int cls, s615_unit* out, size_t cap, size_t* n) {
+  if (!n || B > 2353973ULL || cls < 1 || cls > 4 || (cap && !out)) return S615_E_ARG;
+  const auto v = jobs617(B, cls);
+  for (size_t i = 0; i < v.size() && i < cap; ++i) out[i] = v[i];
+  *n = v.size();
+  return v.size() > cap ? S615_E_OVERFLOW : S615_OK;
+}
+
 // ---------------------------------------------------------- peel batches
 }  // extern "C"
 
@@ -504,7 +512,9 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
     if (s) return s;
     if (skip) continue;
     // classes 1 and 7 (c4 windows) run in the second kernel
-    unit_items(d, (u32)du.size(), (d.cls == S615_CLS_617 || d.cls == 1) ? items617 : b->host_items);
+    unit_items(d, (u32)du.size(),
+               (d.cls == S615_CLS_617 || d.cls == 1 || d.cls == S615_CLS_617_FIND4) ? items617
+                                                                                : b->host_items);
     du.push_back(d);
   }
   // heaviest first: a candidate's first rows (smallest d) have the largest T

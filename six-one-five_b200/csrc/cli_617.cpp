@@ -1,11 +1,13 @@
 // cli_617.cpp -- s615_617, a drop-in for solve_617_v1 restricted to what this
-// engine builds: Branch A (7 does not divide B), class 5.
+// engine builds: Branch A (7 does not divide B), classes 1-5.
 //
 // Same positional arguments, options, stderr progress lines, stdout SOLUTION
 // lines, summary and exit codes as solve_617_v1.cu:1686-2046 for
-//   s615_617 B_min B_max 5 [u_lo] [u_hi] --branch-a-only [options]
+//   s615_617 B_min B_max [classes] [u_lo] [u_hi] --branch-a-only [options]
 // The table is built on the device (or loaded), candidates come from
-// s615_617_candidates, the search is s615_run and the identities s615_verify.
+// s615_617_candidates (class 5) and s615_617_jobs (classes 1-4: the c5
+// expansion into find4 jobs), the search is s615_run and the identities
+// s615_verify.
 // The summary's exact / fp-false counts expand every raw hit into its pairs
 // the way expand_xor_hits does (:1019-1036): all i <= j <= N with
 // i^6 + j^6 = fp (mod 2^64); exact = pairs that satisfy the identity.
@@ -36,8 +38,8 @@ u128 pow6(u64 x) { const u128 a = (u128)x * x; return a * a * a; }
 void usage(const char* a0) {
   std::fprintf(stderr,
       "usage: %s <B_min> <B_max> [classes] [u_lo] [u_hi] [options]\n"
-      "  (6,1,7): a1^6+..+a7^6 = B^6, primitive; Branch A (7 does not divide B), class 5.\n"
-      "  classes: \"5\" (classes 1-4 and Branch B are not built by this engine);\n"
+      "  (6,1,7): a1^6+..+a7^6 = B^6, primitive; Branch A (7 does not divide B), classes 1-5.\n"
+      "  classes: \"all\" (default) or e.g. \"1,3\" (Branch B is not built by this engine);\n"
       "  u band as fractions of B.\n"
       "  options: --branch-a-only (required) --chunk K --device K --r R --hit-cap N\n"
       "           --save-table F --load-table F --bench [K] --quiet\n"
@@ -203,9 +205,11 @@ int main(int argc, char** argv) {
   if (pos.size() < 2 && bench_chunks > 0) { pos.push_back("1"); pos.push_back("10000"); }
   if (pos.size() < 2) { usage(argv[0]); return 1; }
   const long long B_min = std::atoll(pos[0].c_str()), B_max = std::atoll(pos[1].c_str());
-  if (pos.size() >= 3 && pos[2] != "5") {
-    std::fprintf(stderr, "classes \"%s\": only class 5 of Branch A is built by this engine\n", pos[2].c_str());
-    return 1;
+  std::vector<int> classes{1, 2, 3, 4, 5};   // the reference's "all" (:1767-1772)
+  if (pos.size() >= 3 && pos[2] != "all") {
+    classes.clear();
+    for (char c : pos[2]) if (c >= '1' && c <= '5') classes.push_back(c - '0');
+    if (classes.empty()) classes = {1, 2, 3, 4, 5};
   }
   if (!branch_a_only) {
     std::fprintf(stderr, "Branch B is not built by this engine: pass --branch-a-only\n");
@@ -250,9 +254,9 @@ int main(int argc, char** argv) {
   const size_t kBatchCap = 6000000;   // BRANCH_A_BATCH_CAP (:1896)
 
   long solutions = 0;
-  long long st_cands = 0, st_exact = 0, st_false = 0;
-  u64 st_probes = 0, st_calls = 0, st_gated = 0, st_tri_skip = 0, st_tri_tot = 0;
-  double st_ms = 0;
+  long long st_cands[6] = {0}, st_exact[6] = {0}, st_false[6] = {0};
+  u64 st_probes[6] = {0}, st_calls[6] = {0}, st_gated[6] = {0}, st_tri_skip[6] = {0}, st_tri_tot[6] = {0};
+  double st_ms[6] = {0};
   std::set<std::array<long long, 7>> reported;
   std::set<long long> found_B;
   std::vector<s615_hit> hits(hit_cap);
@@ -265,91 +269,111 @@ int main(int argc, char** argv) {
     for (long long B = std::max(c0, 11LL); B <= c1; ++B)
       if ((B & 1) && B % 3 && B % 7) Bl.push_back(B);
     if (!quiet) std::fprintf(stderr, "[chunk] B %lld..%lld: Branch A (%zu values)\n", c0, c1, Bl.size());
-    std::vector<s615_unit> batch;
-    auto flush = [&]() -> int {
-      if (batch.empty()) return 0;
-      size_t nh = 0;
-      s615_counters c{};
-      const auto t0 = Clock::now();
-      int s = s615_run(ctx, tid, batch.data(), batch.size(), flags, hits.data(), hits.size(), &nh, &c);
-      st_ms += std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
-      if (s == S615_E_OVERFLOW)
-        std::fprintf(stderr, "!! hit buffer overflow at B<=%lld — rerun with larger --hit-cap\n", c1);
-      else if (s) { std::fprintf(stderr, "[617] run failed: %s\n", s615_strerror(s)); return 1; }
-      st_cands += (long long)batch.size();
-      st_probes += 3 * c.probes; st_calls += c.probes; st_gated += c.gated;
-      st_tri_skip += 32 * c.tri_skipped; st_tri_tot += 32 * c.tri_total;   // the reference counts per thread
-      const size_t kept = std::min(nh, hits.size());
-      for (size_t k = 0; k < kept; ++k) {   // expanded (hit, pair) records, as expand_xor_hits
-        const s615_hit& H = hits[k];
-        const s615_unit& U = batch[H.unit];
-        u128 q = 0;
-        { const u128 b6 = pow6(U.B); q = b6 - pow6(U.u) - pow6(U.w); }
-        pr.each(H.fp, [&](unsigned a, unsigned b) {
-          const u128 g6 = pow6(21ULL * H.d);
-          bool ex = false;
-          if (g6 <= q) {
-            const u128 rhs = q - g6;
-            ex = rhs % kM42 == 0 && pow6(a) + pow6(b) + pow6(H.e) + pow6(H.c4) == rhs / kM42;
-          }
-          ex ? ++st_exact : ++st_false;
-        });
+    for (int cls : classes) {
+      std::vector<s615_unit> batch;
+      auto flush = [&]() -> int {
+        if (batch.empty()) return 0;
+        size_t nh = 0;
+        s615_counters c{};
+        const auto t0 = Clock::now();
+        int s = s615_run(ctx, tid, batch.data(), batch.size(), flags, hits.data(), hits.size(), &nh, &c);
+        st_ms[cls] += std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+        if (s == S615_E_OVERFLOW)
+          std::fprintf(stderr, "!! hit buffer overflow at B<=%lld — rerun with larger --hit-cap\n", c1);
+        else if (s) { std::fprintf(stderr, "[617] run failed: %s\n", s615_strerror(s)); return 1; }
+        st_cands[cls] += (long long)batch.size();
+        st_probes[cls] += 3 * c.probes; st_calls[cls] += c.probes; st_gated[cls] += c.gated;
+        st_tri_skip[cls] += 32 * c.tri_skipped; st_tri_tot[cls] += 32 * c.tri_total;   // per thread
+        const size_t kept = std::min(nh, hits.size());
+        for (size_t k = 0; k < kept; ++k) {   // expanded (hit, pair) records, as expand_xor_hits
+          const s615_hit& H = hits[k];
+          const s615_unit& U = batch[H.unit];
+          pr.each(H.fp, [&](unsigned a, unsigned b) {
+            bool ex = false;
+            if (U.cls == S615_CLS_617_FIND4) {   // the find4 identity against Q4
+              const u128 q4 = ((u128)U.base[1] << 64) | U.base[0];
+              ex = pow6(a) + pow6(b) + pow6(H.e) + pow6(H.c4) == q4;
+            } else {
+              const u128 q = pow6(U.B) - pow6(U.u) - pow6(U.w);
+              const u128 g6 = pow6(21ULL * H.d);
+              if (g6 <= q) {
+                const u128 rhs = q - g6;
+                ex = rhs % kM42 == 0 && pow6(a) + pow6(b) + pow6(H.e) + pow6(H.c4) == rhs / kM42;
+              }
+            }
+            ex ? ++st_exact[cls] : ++st_false[cls];
+          });
+        }
+        std::vector<s615_solution> sol(4 * kept + 64);
+        size_t ns = 0;
+        s = s615_verify(ctx, batch.data(), batch.size(), hits.data(), kept, N, sol.data(), sol.size(), &ns);
+        if (s) { std::fprintf(stderr, "[617] verify failed: %s\n", s615_strerror(s)); return 1; }
+        for (size_t k = 0; k < ns; ++k) {
+          const s615_solution& S = sol[k];
+          std::array<long long, 7> t;
+          for (int i = 0; i < 7; ++i) t[i] = S.a[i];
+          if (!reported.insert(t).second) continue;
+          const unsigned pcls = S.cls == S615_CLS_617_FIND4 ? S.d : 5u;
+          std::printf("SOLUTION cls=%u B=%llu a1=%lld a2=%lld a3=%lld a4=%lld a5=%lld a6=%lld a7=%lld (anchor=%llu) gcd=%lld %s\n",
+                      pcls, (u64)S.B, t[0], t[1], t[2], t[3], t[4], t[5], t[6], (u64)S.u, (long long)S.gcd,
+                      S.gcd == 1 ? "primitive" : "NON-PRIMITIVE");
+          std::fflush(stdout);
+          std::fprintf(stderr, "%llu\tSOLUTION\tcls=%u\n", (u64)S.B, pcls);
+          ++solutions;
+          found_B.insert((long long)S.B);
+        }
+        batch.clear();
+        return 0;
+      };
+      std::vector<s615_unit> tmp;
+      for (long long B : Bl) {
+        size_t n = 0;
+        if (cls == 5) {
+          s615_617_candidates((uint64_t)B, nullptr, 0, &n);
+          tmp.resize(n);
+          if (n) s615_617_candidates((uint64_t)B, tmp.data(), n, &n);
+        } else {
+          s615_617_jobs((uint64_t)B, cls, nullptr, 0, &n);
+          tmp.resize(n);
+          if (n) s615_617_jobs((uint64_t)B, cls, tmp.data(), n, &n);
+        }
+        const long long lo = std::max(1LL, (long long)(u_lo * B)), hi = std::min(B - 1, (long long)(u_hi * B));
+        for (const s615_unit& x : tmp) {
+          if ((long long)x.u < lo || (long long)x.u > hi) continue;   // band applies to the u term
+          batch.push_back(x);
+          if (batch.size() >= kBatchCap && (rc = flush())) break;
+        }
+        if (rc) break;
       }
-      std::vector<s615_solution> sol(4 * kept + 64);
-      size_t ns = 0;
-      s = s615_verify(ctx, batch.data(), batch.size(), hits.data(), kept, N, sol.data(), sol.size(), &ns);
-      if (s) { std::fprintf(stderr, "[617] verify failed: %s\n", s615_strerror(s)); return 1; }
-      for (size_t k = 0; k < ns; ++k) {
-        const s615_solution& S = sol[k];
-        std::array<long long, 7> t;
-        for (int i = 0; i < 7; ++i) t[i] = S.a[i];
-        if (!reported.insert(t).second) continue;
-        std::printf("SOLUTION cls=5 B=%llu a1=%lld a2=%lld a3=%lld a4=%lld a5=%lld a6=%lld a7=%lld (anchor=%llu) gcd=%lld %s\n",
-                    (u64)S.B, t[0], t[1], t[2], t[3], t[4], t[5], t[6], (u64)S.u, (long long)S.gcd,
-                    S.gcd == 1 ? "primitive" : "NON-PRIMITIVE");
-        std::fflush(stdout);
-        std::fprintf(stderr, "%llu\tSOLUTION\tcls=5\n", (u64)S.B);
-        ++solutions;
-        found_B.insert((long long)S.B);
-      }
-      batch.clear();
-      return 0;
-    };
-    std::vector<s615_unit> tmp;
-    for (long long B : Bl) {
-      size_t n = 0;
-      s615_617_candidates((uint64_t)B, nullptr, 0, &n);
-      tmp.resize(n);
-      if (n) s615_617_candidates((uint64_t)B, tmp.data(), n, &n);
-      const long long lo = std::max(1LL, (long long)(u_lo * B)), hi = std::min(B - 1, (long long)(u_hi * B));
-      for (const s615_unit& x : tmp) {
-        if ((long long)x.u < lo || (long long)x.u > hi) continue;   // band applies to the u term
-        batch.push_back(x);
-        if (batch.size() >= kBatchCap && (rc = flush())) break;
-      }
+      if (!rc) rc = flush();
       if (rc) break;
+      if (!quiet && st_cands[cls])
+        std::fprintf(stderr, "[chunk] cls%d done: cum cands=%lld probes=%.2e sol=%ld\n", cls, st_cands[cls],
+                     (double)st_probes[cls], solutions);
     }
-    if (!rc) rc = flush();
-    if (!quiet && st_cands)
-      std::fprintf(stderr, "[chunk] cls5 done: cum cands=%lld probes=%.2e sol=%ld\n", st_cands,
-                   (double)st_probes, solutions);
-    if (!quiet)
-      std::fprintf(stderr, "B %lld..%lld | cands c5=%lld | probes c5=%.2e | sol=%ld\n", c0, c1, st_cands,
-                   (double)st_probes, solutions);
+    if (!quiet) {
+      std::fprintf(stderr, "B %lld..%lld | cands", c0, c1);
+      for (int cls : classes) std::fprintf(stderr, " c%d=%lld", cls, st_cands[cls]);
+      std::fprintf(stderr, " | probes");
+      for (int cls : classes) std::fprintf(stderr, " c%d=%.2e", cls, (double)st_probes[cls]);
+      std::fprintf(stderr, " | sol=%ld\n", solutions);
+    }
     if (bench_chunks > 0 && ++chunks_done >= bench_chunks) break;
   }
   s615_close(ctx);
   if (rc) return 1;
   std::fprintf(stderr, "---- summary ----\n");
-  if (st_cands) {
-    std::fprintf(stderr, "cls5: cands=%lld probes=%.4e kernel=%.1fs rate=%.2e probes/s exact=%lld fp-false=%lld gate-kill=%.2f%%",
-                 st_cands, (double)st_probes, st_ms / 1e3, st_probes / std::max(1e-9, st_ms / 1e3), st_exact,
-                 st_false, 100.0 * (double)st_gated / std::max(1.0, (double)(st_gated + st_calls)));
-    if (st_tri_tot)
-      std::fprintf(stderr, " tri-skip=%.2f%% (%llu/%llu c4)", 100.0 * (double)st_tri_skip / (double)st_tri_tot,
-                   st_tri_skip, st_tri_tot);
-    std::fprintf(stderr, "\n");
-  }
+  for (int cls : classes)
+    if (st_cands[cls]) {
+      std::fprintf(stderr, "cls%d: cands=%lld probes=%.4e kernel=%.1fs rate=%.2e probes/s exact=%lld fp-false=%lld gate-kill=%.2f%%",
+                   cls, st_cands[cls], (double)st_probes[cls], st_ms[cls] / 1e3,
+                   st_probes[cls] / std::max(1e-9, st_ms[cls] / 1e3), st_exact[cls], st_false[cls],
+                   100.0 * (double)st_gated[cls] / std::max(1.0, (double)(st_gated[cls] + st_calls[cls])));
+      if (st_tri_tot[cls])
+        std::fprintf(stderr, " tri-skip=%.2f%% (%llu/%llu c4)",
+                     100.0 * (double)st_tri_skip[cls] / (double)st_tri_tot[cls], st_tri_skip[cls], st_tri_tot[cls]);
+      std::fprintf(stderr, "\n");
+    }
   std::fprintf(stderr, "total solutions: %ld (unique B=%zu)\n", solutions, found_B.size());
   if (check && !known.empty()) return check_known(found_B, known, B_min, B_max);
   return 0;

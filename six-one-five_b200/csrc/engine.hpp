@@ -24,6 +24,8 @@ namespace s615 {
 //   cls 1  : the find4 unit (fourcore_find_v4.cu:287-338): base holds
 //            T = (B^6-u^6)/42^6 itself, fmax2..fmax1 the c4 window [lo4, hi4];
 //            items are chunks of kC4Chunk c4 values.
+//   cls 8  : a (6,1,7) class 1-4 find4 job: base = Q4, fmax2..fmax1 the c4
+//            window, pad1 = c5, pad2 = the (6,1,7) class; c4 chunks as cls 1.
 //   cls 7  : the (6,1,7) class-5 shape: base = B^6-u^6-w^6 (< 2^127), rows
 //            d = res1[i] + 64 j (d <= fmax1), f = 21; each row's c4 window
 //            opens find3 rows T' = T - c4^6 over c3.
@@ -214,6 +216,8 @@ void root_csr(int which, std::vector<u32>& off, std::vector<u32>& roots);
 u32 inv_pow6_mod(u32 f, u32 m);   // (f^6)^-1 mod m
 // (u, w) anchor pairs of the (6,1,7) class-5 candidates of one B.
 std::vector<std::pair<u64, u64>> candidates617(u64 B);
+// find4 jobs of the (6,1,7) classes 1-4 for one B (cls 8 unit records).
+std::vector<s615_unit> jobs617(u64 B, int cls);
 int free_factor(int cls);
 
 // Build the device record of one caller unit; returns S615_OK (with *skip

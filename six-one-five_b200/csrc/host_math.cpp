@@ -230,6 +230,141 @@ std::vector<std::pair<u64, u64>> candidates617(u64 B) {
   return out;
 }
 
+// ---------------------------------------------- (6,1,7) classes 1-4 jobs
+namespace {
+using i128 = __int128;
+
+u64 iroot6_i(i128 n) {   // exact floor sixth root, n >= 0
+  if (n <= 0) return 0;
+  const double x = (double)n;
+  u64 a = (u64)std::pow(x, 1.0 / 6.0);
+  while ((i128)pow6_u128(a + 1) <= n) ++a;
+  while (a && (i128)pow6_u128(a) > n) --a;
+  return a;
+}
+u64 least_k(i128 Q, int k) {   // least c >= 1 with k c^6 >= Q
+  u64 c = (u64)std::pow((double)Q / k, 1.0 / 6.0);
+  if (c < 1) c = 1;
+  while ((i128)k * (i128)pow6_u128(c) < Q) ++c;
+  while (c > 1 && (i128)k * (i128)pow6_u128(c - 1) >= Q) --c;
+  return c;
+}
+std::vector<u64> lift_res(const std::vector<long long>& res, u64 m, u64 maxv) {
+  std::vector<u64> v;
+  for (long long r : res)
+    for (u64 x = (u64)r % m ? (u64)r % m : m; x <= maxv; x += m) v.push_back(x);
+  std::sort(v.begin(), v.end());
+  return v;
+}
+// the c5 peel and the find4 window of one find5 target (push_find5_cand,
+// set_window4_gen: c5 <= c5cap, c4 <= c5, 5 c5^6 >= Q, 4 c4^6 >= Q4)
+void push_find5(const s615_unit& J0, i128 Q, u64 c5cap, std::vector<s615_unit>& out) {
+  u64 hi5 = std::min<u64>(iroot6_i(Q), J0.lim);
+  if (hi5 > c5cap) hi5 = c5cap;
+  const u64 lo5 = least_k(Q, 5);
+  for (u64 c5 = lo5; c5 <= hi5; ++c5) {
+    const i128 Q4 = Q - (i128)pow6_u128(c5);
+    if (Q4 < 4) continue;
+    u64 hi4 = std::min<u64>(iroot6_i(Q4), J0.lim);
+    if (hi4 > c5) hi4 = c5;
+    const u64 lo4 = least_k(Q4, 4);
+    if (lo4 > hi4) continue;
+    s615_unit J = J0;
+    J.base[0] = (u64)(u128)Q4;
+    J.base[1] = (u64)((u128)Q4 >> 64);
+    J.res_e = (u32)c5;
+    J.fmax2 = (u32)lo4;
+    J.fmax1 = (u32)hi4;
+    out.push_back(J);
+  }
+}
+}  // namespace
+
+std::vector<s615_unit> jobs617(u64 B, int cls) {
+  std::vector<s615_unit> out;
+  if (B < 2 || cls < 1 || cls > 4) return out;
+  const i128 B6 = (i128)pow6_u128(B);
+  const u32 lim = (u32)((B - 1) / 42);
+  const long long b2 = mod_pow6((long long)(B % kM2), kM2), b3 = mod_pow6((long long)(B % kM3), kM3);
+  const long long b7 = mod_pow6((long long)(B % kM7), kM7);
+  // anchors u (seeds616 / mod616 / unit_ok616, solve_617_v1.cu:267-290,826-848)
+  std::vector<u64> us;
+  if (cls == 4) {
+    const long long t2 = b2 * mod_inv(mod_pow6(7, kM2), kM2) % kM2;
+    const long long t3 = b3 * mod_inv(mod_pow6(7, kM3), kM3) % kM3;
+    std::vector<long long> xs;
+    for (u32 a : roots2().by[(size_t)t2]) for (u32 b : roots3().by[(size_t)t3]) xs.push_back(crt_pair(a, kM2, b, kM3));
+    for (u64 x : lift_res(xs, (u64)(kM2 * kM3), (B - 1) / 7)) us.push_back(7 * x);
+  } else {
+    std::vector<long long> seeds;
+    long long M = 0;
+    if (cls == 1) {
+      M = kM2 * kM3 * kM7;
+      for (u32 a : roots2().by[(size_t)b2])
+        for (u32 c : roots3().by[(size_t)b3]) {
+          const long long s23 = crt_pair(a, kM2, c, kM3);
+          for (u32 d : roots7().by[(size_t)b7]) seeds.push_back(crt_pair(s23, kM2 * kM3, d, kM7));
+        }
+    } else if (cls == 2) {
+      M = kM2 * kM7;
+      for (u32 a : roots2().by[(size_t)b2]) for (u32 d : roots7().by[(size_t)b7]) seeds.push_back(crt_pair(a, kM2, d, kM7));
+    } else {
+      M = kM3 * kM7;
+      for (u32 c : roots3().by[(size_t)b3]) for (u32 d : roots7().by[(size_t)b7]) seeds.push_back(crt_pair(c, kM3, d, kM7));
+    }
+    for (long long sd : seeds)
+      for (u64 u = (u64)(sd % M) ? (u64)(sd % M) : (u64)M; u <= B - 1; u += (u64)M) {
+        const bool ok = cls == 1 ? ((u & 1) && std::gcd(u, (u64)42) == 1)
+                      : cls == 2 ? ((u & 1) && u % 3 == 0)
+                                 : (!(u & 1) && std::gcd(u, (u64)21) == 1);
+        if (ok) us.push_back(u);
+      }
+  }
+  std::sort(us.begin(), us.end());
+  us.erase(std::unique(us.begin(), us.end()), us.end());
+  for (u64 u : us) {
+    const i128 u6 = (i128)pow6_u128(u);
+    if (u6 >= B6) continue;
+    s615_unit J0{};
+    J0.cls = S615_CLS_617_FIND4; J0.kind = 0; J0.B = B; J0.u = u; J0.lim = lim; J0.res_d = (u32)cls;
+    if (cls == 1) {   // Q0 = (B^6-u^6)/42^6; the sixth 42-term 42w with c5 <= w
+      const i128 R = B6 - u6;
+      if (R % (i128)kM42 != 0) continue;
+      const i128 Q0 = R / (i128)kM42;
+      const u64 wmax = std::min<u64>(lim, iroot6_i(Q0 - 5));
+      for (u64 w = 1; w <= wmax; ++w) {
+        const i128 Q = Q0 - (i128)pow6_u128(w);
+        if (Q < 5) break;
+        J0.w = (u32)(42 * w);
+        push_find5(J0, Q, w, out);
+      }
+    } else {          // the sixth term f v over its residue classes
+      u64 f = 0, vmod = 0, vmax = 0;
+      std::vector<long long> vres;
+      if (cls == 2) {
+        f = 14; vmod = kM3; vmax = (B - 1) / 14;
+        for (u32 v : e_residues(B)) vres.push_back(v);
+      } else if (cls == 3) {
+        f = 21; vmod = kM2; vmax = (B - 1) / 21;
+        for (u32 v : d_residues(B, u)) vres.push_back(v);
+      } else {
+        f = 6; vmod = kM7; vmax = (B - 1) / 6;
+        const long long t = b7 * mod_inv(mod_pow6(6, kM7), kM7) % kM7;
+        for (u32 v : roots7().by[(size_t)t]) vres.push_back(v);
+      }
+      for (u64 v : lift_res(vres, vmod, vmax)) {
+        const i128 R = B6 - u6 - (i128)pow6_u128(f * v);
+        if (R <= 0 || R % (i128)kM42 != 0) continue;
+        const i128 Q = R / (i128)kM42;
+        if (Q < 5) continue;
+        J0.w = (u32)(f * v);
+        push_find5(J0, Q, lim, out);
+      }
+    }
+  }
+  return out;
+}
+
 // --------------------------------------------------------------- dev units
 namespace {
 constexpr u64 kMaxB = 40000000ULL;  // keeps d^3, (14e)^3 and the row values inside device words
@@ -382,10 +517,34 @@ static int make_dev_unit1(const s615_unit& in, DevUnit* out, bool* skip) {
   return S615_OK;
 }
 
+// cls 8: a (6,1,7) class 1-4 find4 job as jobs617 makes it (or a caller's
+// own: base = Q4 < 2^126, window inside [1, lim], lim < 2^21).
+static int make_dev_unit8(const s615_unit& in, DevUnit* out) {
+  if (in.kind != 0 || in.base[2] != 0 || (in.base[1] >> 62) != 0) return S615_E_FORMAT;
+  if (in.lim >= (1u << 21) || in.fmax2 < 1 || in.fmax1 < in.fmax2 || in.fmax1 > in.lim)
+    return S615_E_FORMAT;
+  out->cls = S615_CLS_617_FIND4;
+  out->B = in.B; out->u = in.u; out->w = in.w;
+  out->base_lo = in.base[0];
+  out->base_hi = in.base[1];
+  out->lim = in.lim;
+  out->fmax1 = in.fmax1;
+  out->fmax2 = in.fmax2;
+  out->nres1 = 1;
+  out->pad1 = in.res_e;   // c5
+  out->pad2 = in.res_d;   // the (6,1,7) class
+  return S615_OK;
+}
+
 int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip) {
   std::memset(out, 0, sizeof *out);
   *skip = false;
   const u32 cls = in.cls;
+  if (cls == S615_CLS_617_FIND4) {
+    const int s = make_dev_unit8(in, out);
+    out->id = id;
+    return s;
+  }
   if (cls == 1) {
     const int s = make_dev_unit1(in, out, skip);
     out->id = id;
@@ -468,7 +627,7 @@ int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip) {
 }
 
 void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out) {
-  if (d.cls == 1) {   // chunks of the c4 window
+  if (d.cls == 1 || d.cls == S615_CLS_617_FIND4) {   // chunks of the c4 window
     const u32 n = (d.fmax1 - d.fmax2) / kC4Chunk + 1;
     for (u32 c = 0; c < n; ++c) out.push_back(make_item(unit_index, 0, c));
     return;

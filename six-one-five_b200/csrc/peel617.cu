@@ -296,7 +296,8 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Par
     I.cls = U->cls;
     I.lim = U->lim;
     u32 nrows;
-    if (I.cls == 1) {   // one row, T = base; this item's c4 are a chunk of [fmax2, fmax1]
+    const bool single = I.cls == 1 || I.cls == S615_CLS_617_FIND4;
+    if (single) {   // one row, T = base; this item's c4 are a chunk of [fmax2, fmax1]
       I.r0 = 0; I.mod = 0; I.j0 = 0;
       nrows = 1;
     } else {
@@ -316,13 +317,15 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Par
       // ---- the row of this lane: T(d), its c4 window and T mod 504 / 247 ----
       u64 tl = 0, th = 0;
       u32 lo4 = 0, len4 = 0, q504 = 0, q247 = 0;
-      if (I.cls == 1) {
+      if (single) {
         if (lane == 0) {
           const u32 c0 = U->fmax2 + item_chunk(packed) * kC4Chunk;
           if (c0 <= U->fmax1) {
             tl = U->base_lo; th = U->base_hi;
             lo4 = c0;
             len4 = min(kC4Chunk, U->fmax1 - c0 + 1u);
+            q504 = mod_small<504>(th, tl);   // the triple-sum gate of cls 8 rows
+            q247 = mod_small<247>(th, tl);
           }
         }
       } else if (h + lane < nrows) {

@@ -39,7 +39,7 @@ __global__ void k_verify(const DevUnit* __restrict__ units, const s615_hit* __re
     const u128 base = ((u128)U.base_hi << 64) | U.base_lo;
     u128 S;
     u32 cmax;
-    if (U.cls == 1) {   // base holds T; S = T - c4^6 - c3^6, pairs up to N
+    if (U.cls == 1 || U.cls == S615_CLS_617_FIND4) {   // base holds T; S = T - c4^6 - c3^6, pairs up to N
       const u128 T = base;
       const u128 c46 = pow6_small(H.c4) + pow6_small(H.e);
       if (T <= c46) continue;
@@ -163,6 +163,34 @@ int verify_device(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s
     S.c1 = p.c1; S.c2 = p.c2;
     W3 rhs;   // the peeled terms plus 42^6 times the core
     long long t[5];
+    if (U.cls == S615_CLS_617_FIND4) {   // B^6 = u^6 + w^6 + 42^6 (c1^6 + .. + c5^6)
+      S.c3 = H.e; S.c4 = H.c4; S.w = U.w;
+      S.d = U.res_d;    // the (6,1,7) class
+      S.e = U.res_e;    // c5
+      const u128 core = pow6_u128(p.c1) + pow6_u128(p.c2) + pow6_u128(H.e) + pow6_u128(H.c4);
+      const u128 Q4 = ((u128)U.base[1] << 64) | U.base[0];
+      if (core != Q4) continue;   // the find4 identity (verify_hit, solve_617_v1.cu:1079-1082)
+      W3 r = mul_w3_u64(W3{{(u64)(core + pow6_u128(U.res_e)), (u64)((core + pow6_u128(U.res_e)) >> 64), 0}}, kM42);
+      add_w3(r, pow6_w3(U.u));
+      add_w3(r, pow6_w3(U.w));
+      if (!eq_w3(r, pow6_w3(U.B))) continue;
+      std::array<long long, 7> t7 = {42LL * p.c1, 42LL * p.c2, 42LL * H.e, 42LL * H.c4,
+                                     42LL * U.res_e, (long long)U.w, (long long)U.u};
+      std::sort(t7.begin(), t7.end());
+      bool bad = false;
+      for (int i = 0; i < 6; ++i) if (t7[i] == t7[i + 1]) bad = true;
+      if (bad || t7[6] >= (long long)U.B || t7[0] < 1) continue;
+      if (std::find(reported.begin(), reported.end(), t7) != reported.end()) continue;
+      reported.push_back(t7);
+      long long g = t7[0];
+      for (int i = 1; i < 7; ++i) g = std::gcd(g, t7[i]);
+      g = std::gcd(g, (long long)U.B);
+      for (int i = 0; i < 7; ++i) S.a[i] = t7[i];
+      S.gcd = g;
+      if (k < cap) out[k] = S;
+      ++k;
+      continue;
+    }
     if (U.cls == 1) {   // B^6 = u^6 + 42^6 (c1^6 + c2^6 + c3^6 + c4^6)
       S.c3 = H.e; S.c4 = H.c4;
       const u128 core = pow6_u128(p.c1) + pow6_u128(p.c2) + pow6_u128(H.e) + pow6_u128(H.c4);

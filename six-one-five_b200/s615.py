@@ -24,6 +24,7 @@ STATUS = {
 LAYOUT_AUTO, LAYOUT_PACKED, LAYOUT_WIDE = 0, 1, 2
 F_NO_GATE, F_PLAIN, F_NO_TRI, F_SHARP = 1, 2, 4, 8
 S615_CLS_617 = 7
+S615_CLS_617_FIND4 = 8
 
 
 class S615Error(RuntimeError):
@@ -112,6 +113,7 @@ SIGNATURES = {
                                        C.POINTER(C.c_size_t)]),
     "s615_unit_status": (C.c_int, [_P]),
     "s615_617_candidates": (C.c_int, [C.c_uint64, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "s615_617_jobs": (C.c_int, [C.c_uint64, C.c_int, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
     "s615_run": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.c_uint, _P, C.c_size_t,
                            C.POINTER(C.c_size_t), C.POINTER(Counters)]),
     "s615_cls5_run": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.c_uint, _P, C.c_size_t,
@@ -233,6 +235,17 @@ def make_plant1(c: Sequence[int], lim: int, B: int = 0) -> Unit:
     for i in range(3):
         x.base[i] = (base >> (64 * i)) & (2**64 - 1)
     return x
+
+
+def jobs617(B: int, cls: int):
+    """s615_617_jobs: the (6,1,7) class-`cls` (1-4) find4 jobs of one B (array, count)."""
+    n = C.c_size_t(0)
+    st = lib().s615_617_jobs(B, cls, None, 0, C.byref(n))
+    if st not in (S615_OK, -9):
+        _check(st, "617_jobs")
+    arr = (Unit * max(n.value, 1))()
+    _check(lib().s615_617_jobs(B, cls, C.cast(arr, C.c_void_p), n.value, C.byref(n)), "617_jobs")
+    return arr, n.value
 
 
 def make_units617(triples: Iterable[Tuple[int, int, int]]) -> "C.Array":
@@ -427,6 +440,10 @@ def solution_line(s: Solution) -> str:
             return f"PLANT cls=1 unit={s.unit} c1={s.c1} c2={s.c2} c3={s.c3} c4={s.c4}"
         return f"PLANT cls={s.cls} unit={s.unit} d={s.d} c1={s.c1} c2={s.c2} c3={s.c3}"
     a = list(s.a)
+    if s.cls == S615_CLS_617_FIND4:   # the (6,1,7) class is in d
+        terms = " ".join(f"a{i + 1}={a[i]}" for i in range(7))
+        return (f"SOLUTION cls={s.d} B={s.B} {terms} (anchor={s.u}) gcd={s.gcd} "
+                f"{'primitive' if s.gcd == 1 else 'NON-PRIMITIVE'}")
     if s.cls == S615_CLS_617:
         terms = " ".join(f"a{i + 1}={a[i]}" for i in range(7))
         return (f"SOLUTION cls=5 B={s.B} {terms} (anchor={s.u}) gcd={s.gcd} "

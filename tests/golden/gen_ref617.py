@@ -19,41 +19,51 @@ import sys
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 BIN = os.path.join(ROOT, "oracle", "_ref", "solve_617_v1")
 
-# (B_lo, B_hi, r, gate, tri)
+# (B_lo, B_hi, r, gate, tri, classes)
 CASES = [
-    (54301, 54400, 48, True, True),
-    (54301, 54400, 16, True, True),
-    (59801, 59900, 20, True, True),
-    (63601, 63700, 48, True, True),
-    (54301, 54400, 48, True, False),
-    (54301, 54340, 20, False, True),
+    (54301, 54400, 48, True, True, "5"),
+    (54301, 54400, 16, True, True, "5"),
+    (59801, 59900, 20, True, True, "5"),
+    (63601, 63700, 48, True, True, "5"),
+    (54301, 54400, 48, True, False, "5"),
+    (54301, 54340, 20, False, True, "5"),
+    (34701, 34800, 48, True, True, "1234"),
+    (38101, 38200, 16, True, True, "1234"),
+    (39701, 39800, 20, True, True, "1234"),
+    (39701, 39760, 48, True, False, "34"),
 ]
 
 SUMMARY = re.compile(
-    r"cls5: cands=(\d+) probes=(\S+) kernel=\S+ rate=\S+ probes/s exact=(\d+) fp-false=(\d+) "
+    r"cls(\d): cands=(\d+) probes=(\S+) kernel=\S+ rate=\S+ probes/s exact=(\d+) fp-false=(\d+) "
     r"gate-kill=([\d.]+)%(?: tri-skip=[\d.]+% \((\d+)/(\d+) c4\))?")
 
 
 def main():
     out = sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "ref617.json")
     cases = []
-    for lo, hi, r, gate, tri in CASES:
-        cmd = [BIN, str(lo), str(hi), "5", "--branch-a-only", "--r", str(r), "--quiet"]
+    for lo, hi, r, gate, tri, classes in CASES:
+        cmd = [BIN, str(lo), str(hi), classes, "--branch-a-only", "--r", str(r), "--quiet"]
         if not gate:
             cmd.append("--no-gate")
         if not tri:
             cmd.append("--no-tri-gate")
         p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
-        case = {"B_lo": lo, "B_hi": hi, "r": r, "gate": gate, "tri": tri, "rc": p.returncode,
-                "cmd": " ".join(["oracle/_ref/solve_617_v1"] + cmd[1:])}
-        m = SUMMARY.search(p.stderr)
-        if p.returncode != 0 or not m:
+        case = {"B_lo": lo, "B_hi": hi, "r": r, "gate": gate, "tri": tri, "classes": classes,
+                "rc": p.returncode, "cmd": " ".join(["oracle/_ref/solve_617_v1"] + cmd[1:])}
+        found = list(SUMMARY.finditer(p.stderr))
+        if p.returncode != 0:
             case["error"] = p.stderr.strip().splitlines()[-3:]
         else:
-            case.update(cands=int(m.group(1)), probes=m.group(2), exact=int(m.group(3)),
-                        fp_false=int(m.group(4)), gate_kill=m.group(5))
-            if m.group(6):
-                case.update(tri_skipped=int(m.group(6)), tri_total=int(m.group(7)))
+            per = {}
+            for m in found:
+                c = {"cands": int(m.group(2)), "probes": m.group(3), "exact": int(m.group(4)),
+                     "fp_false": int(m.group(5)), "gate_kill": m.group(6)}
+                if m.group(7):
+                    c.update(tri_skipped=int(m.group(7)), tri_total=int(m.group(8)))
+                per[m.group(1)] = c
+            case["per_class"] = per
+            if "5" in per:   # the class-5 fields at the top level, as the first fixtures had them
+                case.update(per["5"])
             case["solutions"] = [l for l in p.stdout.splitlines() if l.startswith("SOLUTION")]
         cases.append(case)
         print(json.dumps(case)[:300])
