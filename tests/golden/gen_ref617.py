@@ -1,5 +1,5 @@
 #!/usr/bin/env python3
-"""Record the reference's own (6,1,7) Branch-A class-5 counts as a fixture.
+"""Record the reference's own (6,1,7) Branch-A counts (classes 1-5) as a fixture.
 
 Runs the reference GPU binary oracle/_ref/solve_617_v1 (built from the
 reference sources by `make -C oracle ref`) on a few small B ranges and writes
@@ -31,6 +31,9 @@ CASES = [
     (38101, 38200, 16, True, True, "1234"),
     (39701, 39800, 20, True, True, "1234"),
     (39701, 39760, 48, True, False, "34"),
+    (24301, 24400, 48, True, True, "1"),
+    (24301, 24400, 20, False, True, "1"),
+    (28101, 28200, 16, True, False, "12"),
 ]
 
 SUMMARY = re.compile(

@@ -1,4 +1,4 @@
-"""(6,1,7) Branch-A class-5 search on the device against the CPU oracle (GPU).
+"""(6,1,7) Branch-A search (classes 1-5) on the device against the CPU oracle (GPU).
 
 The oracle restates gen_class_cands(cls=5), k_find4_cls5 and verify_hit of
 solve_617_v1.cu (:885-906, :563-657, :1040-1110); the device path is the
@@ -194,5 +194,37 @@ def test_bad_units_rejected(engine, oracle_table):
             with pytest.raises(s615.S615Error) as e:
                 engine.run(tid, units, n)
             assert e.value.status == -3
+    finally:
+        engine.free_table(tid)
+
+
+@pytest.mark.parametrize("lo,hi,r", [(34701, 34800, 48), (38101, 38200, 16), (39701, 39800, 20),
+                                      (24301, 24400, 48), (28101, 28200, 16)])
+def test_classes_1_to_4_parity(engine, oracle_table, lo, hi, r):
+    """(6,1,7) classes 1-4: the native find4 jobs equal the oracle's, and the
+    device run over them gives the oracle's hits, counters and lines."""
+    N = hi // 42
+    t, path = oracle_table(N, r)
+    tid = engine.load_table(path, N)
+    try:
+        for cls in (1, 2, 3, 4):
+            parts = [orc.jobs617(B, cls) for B in range(lo, hi + 1) if eligible617(B)]
+            oj, n = orc.concat_jobs617([p for p in parts if p[1]])
+            units = []
+            for B in range(lo, hi + 1):
+                if eligible617(B):
+                    a, k = s615.jobs617(B, cls)
+                    units += [a[i] for i in range(k)]
+            assert len(units) == n
+            if not n:
+                continue
+            arr = (s615.Unit * n)(*units)
+            hits, ctr = engine.run(tid, arr, n)
+            oh, oc = orc.run617_find4(t, oj, n)
+            check_counters(ctr, oc)
+            assert sorted((int(h["unit"]), int(h["e"]), int(h["c4"]), int(h["fp"])) for h in hits) == \
+                sorted((int(h["job"]), int(h["c3"]), int(h["c4"]), int(h["fp"])) for h in oh)
+            lines = sorted(s615.solution_line(s) for s in engine.verify(arr, n, hits, N))
+            assert lines == sorted(orc.verify617_find4(oj, oh, N))
     finally:
         engine.free_table(tid)

@@ -21,7 +21,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 BIN617 = os.path.join(ROOT, "six-one-five_b200", "bin", "s615_617")
 BIN5 = os.path.join(ROOT, "six-one-five_b200", "bin", "s615_cls5")
 SUMMARY = re.compile(
-    r"cls5: cands=(\d+) probes=(\S+) kernel=\S+ rate=\S+ probes/s exact=(\d+) fp-false=(\d+) "
+    r"cls(\d): cands=(\d+) probes=(\S+) kernel=\S+ rate=\S+ probes/s exact=(\d+) fp-false=(\d+) "
     r"gate-kill=([\d.]+)%(?: tri-skip=[\d.]+% \((\d+)/(\d+) c4\))?")
 
 
@@ -31,24 +31,28 @@ def ref_cases():
 
 
 @pytest.mark.parametrize("case", ref_cases(), ids=lambda c: f"{c['B_lo']}-{c['B_hi']}-r{c['r']}"
+                         f"-c{c.get('classes', '5')}"
                          f"{'' if c['gate'] else '-nogate'}{'' if c['tri'] else '-notri'}")
 def test_617_cli_prints_what_the_reference_printed(case):
-    cmd = [BIN617, str(case["B_lo"]), str(case["B_hi"]), "5", "--branch-a-only", "--r",
-           str(case["r"]), "--quiet"]
+    cmd = [BIN617, str(case["B_lo"]), str(case["B_hi"]), case.get("classes", "5"), "--branch-a-only",
+           "--r", str(case["r"]), "--quiet"]
     if not case["gate"]:
         cmd.append("--no-gate")
     if not case["tri"]:
         cmd.append("--no-tri-gate")
     p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
     assert p.returncode == 0, p.stderr
-    m = SUMMARY.search(p.stderr)
-    assert m, p.stderr
-    assert int(m.group(1)) == case["cands"]
-    assert m.group(2) == case["probes"]
-    assert (int(m.group(3)), int(m.group(4))) == (case["exact"], case["fp_false"])
-    assert m.group(5) == case["gate_kill"]
-    if case["tri"]:
-        assert (int(m.group(6)), int(m.group(7))) == (case["tri_skipped"], case["tri_total"])
+    per = {}
+    for m in SUMMARY.finditer(p.stderr):
+        c = {"cands": int(m.group(2)), "probes": m.group(3), "exact": int(m.group(4)),
+             "fp_false": int(m.group(5)), "gate_kill": m.group(6)}
+        if m.group(7):
+            c.update(tri_skipped=int(m.group(7)), tri_total=int(m.group(8)))
+        per[m.group(1)] = c
+    want = case.get("per_class", {"5": {k: case[k] for k in ("cands", "probes", "exact", "fp_false",
+                                                              "gate_kill", "tri_skipped", "tri_total")
+                                        if k in case}})
+    assert per == want, p.stderr
     sols = [l for l in p.stdout.splitlines() if l.startswith("SOLUTION")]
     assert sorted(sols) == sorted(case["solutions"])
 

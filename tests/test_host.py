@@ -73,6 +73,23 @@ def test_617_candidates_match_oracle():
         s615.candidates617(2353975)
 
 
+def test_617_find4_jobs_match_oracle():
+    # s615_617_jobs against the oracle's find5 expansion (classes 1-4): same
+    # jobs in the same order, c4 window [lo, hi] in fmax2 / fmax1
+    for B, cls in [(34781, 4), (38191, 4), (39779, 3), (34763, 1), (34763, 2), (38111, 3)]:
+        arr, n = s615.jobs617(B, cls)
+        oarr, on = orc.jobs617(B, cls)
+        assert n == on, (B, cls)
+        for i in range(n):
+            a, o = arr[i], oarr[i]
+            assert a.cls == s615.S615_CLS_617_FIND4 and a.B == B == o.B
+            assert (a.u, a.w, a.res_e, a.res_d, a.lim) == (o.u, o.w, o.c5, cls, o.lim), (B, cls, i)
+            assert (a.fmax2, a.fmax1) == (o.lo, o.hi), (B, cls, i)
+            assert (a.base[0], a.base[1], a.base[2]) == (o.Q4[0], o.Q4[1], 0), (B, cls, i)
+    with pytest.raises(s615.S615Error):
+        s615.jobs617(34781, 5)
+
+
 def test_open_without_gpu_fails_loudly():
     import torch
     if torch.cuda.is_available():

@@ -155,6 +155,43 @@ def test_tiles_repeat_wide_windows():
     assert b[3] > a[3] > 0 and a[3] == a[4] and b[3] == b[4]
 
 
+def oracle_case(case):
+    """The oracle over one recorded reference run: per class the summary
+    fields, plus all SOLUTION lines."""
+    lo, hi, r = case["B_lo"], case["B_hi"], case["r"]
+    N = hi // 42
+    t = orc.Table.build_pairs(N, r)
+    Bs = [B for B in range(lo, hi + 1) if eligible617(B)]
+    per, lines = {}, []
+    for cls in case.get("classes", "5"):
+        st = [0, 0]
+        if cls == "5":
+            parts = [orc.cands617(B) for B in Bs]
+            arr, n = orc.concat617([p for p in parts if p[1]])
+            if not n:
+                continue
+            zmax = max(1, min(32, (max(arr[i].lim for i in range(n)) + 2047) // 2048))
+            hits, c = orc.run617(t, arr, n, use_gate=case["gate"], use_tri=case["tri"], zmax=zmax)
+            lines += orc.verify617(arr, hits, N, stats=st)
+        else:
+            parts = [orc.jobs617(B, int(cls)) for B in Bs]
+            arr, n = orc.concat_jobs617([p for p in parts if p[1]])
+            if not n:
+                continue
+            span = max(arr[i].hi - arr[i].lo + 1 for i in range(n))
+            ymax = max(1, min(32, (span + 2047) // 2048))
+            hits, c = orc.run617_find4(t, arr, n, use_gate=case["gate"], use_tri=case["tri"], ymax=ymax)
+            lines += orc.verify617_find4(arr, hits, N, stats=st)
+        rec = {"cands": n, "probes": "%.4e" % c[2], "exact": st[0], "fp_false": st[1],
+               "gate_kill": "%.2f" % (100.0 * c[1] / max(1, c[1] + c[0]))}
+        if case["tri"]:
+            # every one of the 32 threads of the warp that walks a c4 counts it
+            # (++l_tri_tot / ++l_tri_skip run per thread, solve_617_v1.cu:527-536, 604-614)
+            rec.update(tri_skipped=32 * c[4], tri_total=32 * c[3])
+        per[cls] = rec
+    return per, lines
+
+
 @pytest.mark.skipif(not os.path.exists(REF617), reason="reference GPU fixture not generated")
 def test_counters_equal_reference_binary():
     """Counts printed by the reference's own solve_617_v1 (run on a GPU by
@@ -164,21 +201,9 @@ def test_counters_equal_reference_binary():
     cases = [c for c in ref["cases"] if "error" not in c]
     assert cases
     for case in cases:
-        lo, hi, r = case["B_lo"], case["B_hi"], case["r"]
-        parts = [orc.cands617(B) for B in range(lo, hi + 1) if eligible617(B)]
-        arr, n = orc.concat617([p for p in parts if p[1]])
-        N = hi // 42
-        t = orc.Table.build_pairs(N, r)
-        zmax = max(1, min(32, (max(arr[i].lim for i in range(n)) + 2047) // 2048))
-        hits, c = orc.run617(t, arr, n, use_gate=case["gate"], use_tri=case["tri"], zmax=zmax)
-        st = [0, 0]
-        lines = orc.verify617(arr, hits, N, stats=st)
-        assert n == case["cands"], case
-        assert "%.4e" % c[2] == case["probes"], case
-        if case["tri"]:
-            # every one of the 32 threads of the warp that walks a c4 counts it
-            # (++l_tri_tot / ++l_tri_skip run per thread, solve_617_v1.cu:604-614)
-            assert (32 * c[4], 32 * c[3]) == (case["tri_skipped"], case["tri_total"]), case
-        assert st == [case["exact"], case["fp_false"]], case
-        assert "%.2f" % (100.0 * c[1] / max(1, c[1] + c[0])) == case["gate_kill"], case
-        assert sorted(lines) == sorted(case["solutions"]), case
+        per, lines = oracle_case(case)
+        want = case.get("per_class", {"5": {k: case[k] for k in ("cands", "probes", "exact", "fp_false",
+                                                                  "gate_kill", "tri_skipped", "tri_total")
+                                            if k in case}})
+        assert per == want, case["cmd"]
+        assert sorted(lines) == sorted(case["solutions"]), case["cmd"]
