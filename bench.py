@@ -19,7 +19,8 @@ measures the (6,1,7) Branch-A class-5 search instead: one step is every
 candidate of the eligible B in [400,401, 400,441) (a slice of the band
 B in [400,000, 440,000]) plus 128 plants, against the N=10,476 r=48 table;
 `value` counts probes the way the reference's summary does (3 per post-gate
-xor probe).  Its reference arm runs the reference's own GPU binary
+xor probe).  `classes_1_4` times one pass over the same band's classes 1-4
+find4 jobs.  Its reference arm runs the reference's own GPU binary
 (oracle/_ref/solve_617_v1, built from the reference sources) on the same band.
 """
 import argparse
@@ -27,6 +28,7 @@ import ctypes as C
 import json
 import math
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -55,6 +57,7 @@ def parse():
     ap.add_argument("--r", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-find4", action="store_true", help="cls617: skip the classes 1-4 pass")
     ap.add_argument("--workload", default="cls5", choices=["cls5", "cls617", "mix", "serve"])
     ap.add_argument("--units", type=int, default=0, help="mix: units per step (default 200,000)")
     ap.add_argument("--seconds", type=float, default=10.0, help="serve: seconds of arrivals")
@@ -412,6 +415,10 @@ def run617(args, rank, world, local, dist):
                  "speedup_vs_default": (total_ms / args.steps) / sms,
                  "flag": "S615_F_SHARP (extra sound residue tests; raw hits a subset)"}
 
+    find4 = None
+    if rank == 0 and not args.no_find4:
+        find4 = run617_find4(lib, eng, tid, stream, Bs)
+
     peak, peak_kind = measured_peaks()
     achieved = ctr.probes * PROBE_BYTES / (statistics.mean(per_ms) / 1e3) / 1e9
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -462,6 +469,7 @@ def run617(args, rank, world, local, dist):
         "roofline": roof,
         "cpu_baseline": cpu,
         "sharp_gate": sharp,
+        "classes_1_4": find4,
         "clocks": cl,
     }
     s615._check(lib.s615_batch_free(eng._ctx, batch), "batch_free")
@@ -472,6 +480,28 @@ def run617(args, rank, world, local, dist):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def run617_find4(lib, eng, tid, stream, Bs):
+    """(6,1,7) classes 1-4 of the same B band: every find4 job of
+    s615_617_jobs (the reference's find5 expansion, solve_617_v1.cu:807-884)
+    in one batch, one CUDA-event timed pass after a warm pass."""
+    import s615
+    t0 = time.perf_counter()
+    units, n = s615.jobs617_band(Bs)
+    jobs_s = time.perf_counter() - t0
+    if not n:
+        return None
+    batch = C.c_void_p()
+    t0 = time.perf_counter()
+    s615._check(lib.s615_prepare(eng._ctx, C.cast(units, C.c_void_p), n, C.byref(batch)), "prepare")
+    prep_s = time.perf_counter() - t0
+    ms, ctr = timed_steps(lib, eng, tid, batch, stream, 0, 1)
+    s615._check(lib.s615_batch_free(eng._ctx, batch), "batch_free")
+    return {"jobs": n, "probes": 3 * ctr.probes, "ms_per_step": ms,
+            "probes_per_s": 3 * ctr.probes / (ms / 1e3), "c4_total": ctr.tri_total,
+            "c4_tri_skipped": ctr.tri_skipped, "c3_points": ctr.pos, "hits": ctr.hits,
+            "host_jobs_s": round(jobs_s, 2), "host_prepare_s": round(prep_s, 2)}
 
 
 def run617_reference(args, rank):
@@ -492,7 +522,6 @@ def run617_reference(args, rank):
     for s in range(max(1, args.steps)):
         p = subprocess.run([exe, str(lo), str(hi), "5", "--branch-a-only", "--r", str(args.r),
                             "--quiet"], capture_output=True, text=True, timeout=3600)
-        import re
         m = re.search(r"cls5: cands=(\d+) probes=(\S+) kernel=([\d.]+)s rate=(\S+) probes/s", p.stderr)
         if p.returncode != 0 or not m:
             print(json.dumps({**base, "unavailable": "solve_617_v1 failed: " +
@@ -501,6 +530,21 @@ def run617_reference(args, rank):
         rates.append(float(m.group(4)))
         secs.append(float(m.group(3)))
     v = statistics.mean(rates)
+    find4 = None
+    if not args.no_find4:
+        # classes 1-4 of the same band, one run: summed kernel time of its
+        # per-class k_find4 launches
+        p = subprocess.run([exe, str(lo), str(hi), "1234", "--branch-a-only", "--r", str(args.r),
+                            "--quiet"], capture_output=True, text=True, timeout=3600)
+        per = re.findall(r"cls(\d): cands=(\d+) probes=(\S+) kernel=([\d.]+)s", p.stderr)
+        if p.returncode == 0 and per:
+            probes = sum(float(x[2]) for x in per)
+            ksec = sum(float(x[3]) for x in per)
+            find4 = {"jobs": sum(int(x[1]) for x in per), "probes": probes, "ms_per_step": ksec * 1e3,
+                     "probes_per_s": probes / ksec if ksec else None,
+                     "per_class": {x[0]: {"jobs": int(x[1]), "probes": float(x[2]),
+                                          "kernel_s": float(x[3])} for x in per},
+                     "note": "kernel seconds as the summary prints them (0.1 s resolution)"}
     line = {**base, "value": v, "n_gpus": 1, "steps": len(rates), "warmup": 0,
             "ms_per_step": statistics.mean(secs) * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u128", "data": "synthetic",
@@ -508,6 +552,7 @@ def run617_reference(args, rank):
                                    f"--branch-a-only --r {args.r} (table N={hi // 42} built on the host)"},
             "cpu_baseline": None,
             "e2e": {"value": v, "unit": UNIT617, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "classes_1_4": find4,
             "note": "kernel time as the reference's summary prints it (k_find4_cls5 launches only)"}
     print(json.dumps(line), flush=True)
     return 0

@@ -248,6 +248,25 @@ def jobs617(B: int, cls: int):
     return arr, n.value
 
 
+def jobs617_band(Bs: Iterable[int], classes: Iterable[int] = (1, 2, 3, 4)):
+    """The find4 jobs of every B in `Bs` for each (6,1,7) class in `classes`,
+    concatenated class by class in B order (array, count)."""
+    Bs = list(Bs)
+    chunks, n = [], 0
+    sz = C.sizeof(Unit)
+    for cls in classes:
+        for B in Bs:
+            arr, k = jobs617(B, cls)
+            if k:
+                chunks.append(C.string_at(C.addressof(arr), k * sz))
+                n += k
+    buf = b"".join(chunks)
+    out = (Unit * max(n, 1))()
+    if n:
+        C.memmove(out, buf, len(buf))
+    return out, n
+
+
 def make_units617(triples: Iterable[Tuple[int, int, int]]) -> "C.Array":
     """(6,1,7) Branch-A class-5 candidates (B, u = 14u', w = 6v')."""
     triples = list(triples)
