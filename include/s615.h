@@ -89,15 +89,24 @@ typedef struct s615_table_info {
  * cls 2-4 and 7 use res_d/fmax1.  cls 7 kind 0 needs 14 | u, 6 | w,
  * u^6 = B^6 (mod 3^6), w^6 = B^6 (mod 7^6) and B <= 2,353,973 (B^6 < 2^127);
  * units with base <= 0 are dropped like the reference drops them.  A cls 7
- * plant (solve_617_v1.cu:1564-1582) has base < 2^127 and lim < 65536. */
+ * plant (solve_617_v1.cu:1564-1582) has base < 2^127 and lim < 65536.
+ * kind 2 (S615_KIND_JOB): a reduced-T job of fourcore_find_v4 (a .but line or
+ * .bbj record, fourcore_job_bin.hpp:30-39, read by job_from_bin
+ * fourcore_find_v4.cu:598-608): base[0..1] = T (base[2] = 0), B, u,
+ * res_d = free1 (d), res_e = free2 (e, cls 5 only); lim is (B-1)/42.  cls 1:
+ * find4 over T (make_cand mode 4); cls 2-4: one find3 row, c3 in
+ * [least c with 3c^6 >= T, min(iroot6 T, lim)] (mode 3); cls 5: one gated
+ * probe of key T (mode 2, k_find2 :233-252).  Jobs with an empty window are
+ * dropped like run_batch drops them (:486). */
 #define S615_CLS_617 7
 #define S615_CLS_617_FIND4 8
+#define S615_KIND_JOB 2
 typedef struct s615_unit {
   uint32_t cls;      /* 1, 2, 3, 4, 5, 7 or 8 */
-  uint32_t kind;     /* 0 = (B,u) or (B,u,w), 1 = planted base */
+  uint32_t kind;     /* 0 = (B,u) or (B,u,w), 1 = planted base, 2 = reduced-T job */
   uint64_t B, u;
-  uint64_t base[3];  /* kind 1 only */
-  uint32_t fmax1, fmax2, res_e, res_d, lim; /* kind 1 only */
+  uint64_t base[3];  /* kind 1; kind 2: T in base[0..1] */
+  uint32_t fmax1, fmax2, res_e, res_d, lim; /* kind 1; kind 2: res_d, res_e */
   uint32_t w;        /* cls 7: the x6 anchor term 6v'; otherwise 0 */
 } s615_unit;
 
@@ -209,6 +218,41 @@ int s615_617_candidates(uint64_t B, s615_unit* out, size_t cap, size_t* n);
  * set_window4_gen :766-803): the cls 8 find4 jobs of one B, in the
  * reference's order.  Same return rules as s615_617_candidates. */
 int s615_617_jobs(uint64_t B, int cls, s615_unit* out, size_t cap, size_t* n);
+/* expand_unit of fourcore_find_v4 (fourcore_find_v4.cu:164-205): the
+ * reduced-T jobs (kind 2) of one Stage-1 unit (kind 0).  cls 1: one job,
+ * T = (B^6 - u^6)/42^6; cls 2-4: one job per free term d of free_d_cls234
+ * (residue order, then d ascending), T = (B^6 - u^6 - (f d)^6)/42^6; cls 5:
+ * one job per (e, d) of free_de_cls5 (e outer), T = (B^6 - u^6 - (21d)^6 -
+ * (14e)^6)/42^6.  A d or (e, d) whose difference is not positive, or not
+ * divisible by 42^6, is counted in *fail_t (the reference's failT) and
+ * skipped.  Writes min(cap, count) jobs; *n = count; S615_E_OVERFLOW when cap
+ * is short.  B <= 40,000,000. */
+int s615_expand_unit(const s615_unit* unit, s615_unit* out, size_t cap, size_t* n,
+                     uint64_t* fail_t);
+
+/* Job files (fourcore_job_bin.hpp; load_jobs_but fourcore_find_v4.cu:125-145).
+ * A path ending in .bbj (any case) is the binary form: a 32-byte header
+ * {magic 'FCJB', version 2, n_jobs, rec_bytes 36, min_B, max_B, pad} and
+ * 36-byte records {u8 cls, 3 pad, u32 B, u, free1, free2, u64 T_lo, T_hi},
+ * little-endian.  Any other path is text, one job per line:
+ * "cls B u free1 free2 T_lo T_hi" (lines that do not parse are skipped and
+ * counted).  The reader streams: s615_jobs_next returns up to cap jobs (kind
+ * 2) and *n = 0 at the end. */
+typedef struct s615_jobs_file s615_jobs_file;
+typedef struct s615_jobs_info {
+  uint64_t n_jobs;        /* .bbj: the header's count; text: 0 */
+  uint32_t min_B, max_B;  /* .bbj: the header's range; text: 0 */
+  uint32_t binary;        /* 1 for .bbj */
+  uint32_t pad;
+  uint64_t bad_lines;     /* text lines skipped so far */
+} s615_jobs_info;
+int s615_jobs_open(const char* path, s615_jobs_file** out, s615_jobs_info* info);
+int s615_jobs_next(s615_jobs_file* f, s615_unit* out, size_t cap, size_t* n);
+int s615_jobs_close(s615_jobs_file* f, s615_jobs_info* info);
+/* Writes kind 2 units as a job file (.bbj header with n, min_B, max_B; or
+ * text lines).  S615_E_ARG for other kinds or fields wider than the format. */
+int s615_jobs_write(const char* path, const s615_unit* jobs, size_t n);
+
 /* What a run does with one unit: S615_OK = searched, 1 = dropped like
  * pack_unit5 drops it (u >= B or an empty residue class), S615_E_FORMAT =
  * rejected (outside the engine's exact-arithmetic range, or a planted base

@@ -49,6 +49,11 @@ class OrcHit4(C.Structure):
                 ("fp", C.c_uint64)]
 
 
+class OrcJob(C.Structure):
+    _fields_ = [("cls", C.c_uint32), ("lim", C.c_uint32), ("B", C.c_uint64), ("u", C.c_uint64),
+                ("free1", C.c_uint64), ("free2", C.c_uint64), ("T", C.c_uint64 * 2)]
+
+
 class OrcJob617(C.Structure):
     _fields_ = [("Q4", C.c_uint64 * 2), ("B", C.c_uint32), ("u", C.c_uint32), ("w", C.c_uint32),
                 ("cls", C.c_uint32), ("c5", C.c_uint32), ("lim", C.c_uint32), ("lo", C.c_uint32),
@@ -99,6 +104,10 @@ _SIG = {
     "orc_find4_run": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_int, _P, C.c_size_t,
                                    _P]),
     "orc_617_jobs": (C.c_size_t, [C.c_uint64, C.c_int, _P, C.c_size_t]),
+    "orc_expand_unit": (C.c_size_t, [C.c_uint64, C.c_uint64, C.c_int, _P, C.c_size_t, _P]),
+    "orc_jobs_run": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_int, _P, C.c_size_t,
+                                  _P]),
+    "orc_jobs_verify": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_char_p, C.c_size_t, _P]),
     "orc_617_find4_run": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_int, C.c_int, _P,
                                        C.c_size_t, _P]),
     "orc_617_find4_verify": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_char_p, C.c_size_t, _P]),
@@ -338,6 +347,52 @@ def run_find4(table: Table, jobs, n: int, use_gate: bool = True, ref_tiles: bool
         raise RuntimeError("oracle hit buffer overflow")
     raw = np.frombuffer(C.string_at(C.addressof(hits), nh * C.sizeof(OrcHit4)), dtype=HIT4_DTYPE)
     return raw.copy(), [int(x) for x in ctr]
+
+
+def expand_unit(B: int, u: int, cls: int):
+    """expand_unit of fourcore_find_v4: (jobs, n, failT) of one Stage-1 unit."""
+    fail = C.c_uint64(0)
+    n = lib().orc_expand_unit(B, u, cls, None, 0, C.byref(fail))
+    arr = (OrcJob * max(n, 1))()
+    lib().orc_expand_unit(B, u, cls, C.cast(arr, C.c_void_p), n, C.byref(fail))
+    return arr, n, fail.value
+
+
+def concat_jobs(parts):
+    """One OrcJob array from (array, n, ...) parts."""
+    n = sum(p[1] for p in parts)
+    out = (OrcJob * max(n, 1))()
+    k = 0
+    for p in parts:
+        C.memmove(C.byref(out, k * C.sizeof(OrcJob)), p[0], p[1] * C.sizeof(OrcJob))
+        k += p[1]
+    return out, n
+
+
+def run_jobs(table: Table, jobs, n: int, use_gate: bool = True, ref_tiles: bool = False,
+             threads: int = 0, cap: int = 1 << 20):
+    """run_batch over reduced-T jobs (find2/find3/find4 by class): (hits
+    {job, c3, c4, fp}, [calls, gated, probes])."""
+    hits = (OrcHit4 * cap)()
+    ctr = np.zeros(3, dtype=np.uint64)
+    nh = lib().orc_jobs_run(table.h, C.cast(jobs, C.c_void_p), n, int(use_gate), int(ref_tiles),
+                            threads, C.cast(hits, C.c_void_p), cap, _ptr(ctr))
+    if nh > cap:
+        raise RuntimeError("oracle hit buffer overflow")
+    raw = np.frombuffer(C.string_at(C.addressof(hits), nh * C.sizeof(OrcHit4)), dtype=HIT4_DTYPE)
+    return raw.copy(), [int(x) for x in ctr]
+
+
+def verify_jobs(jobs, hits: np.ndarray, N: int):
+    """(exact matches, SOLUTION lines) of run_batch's filter + report_solution."""
+    arr = (OrcHit4 * max(len(hits), 1))()
+    for i, h in enumerate(hits):
+        arr[i].job, arr[i].c3, arr[i].c4, arr[i].fp = int(h["job"]), int(h["c3"]), int(h["c4"]), int(h["fp"])
+    buf = C.create_string_buffer(1 << 20)
+    nl = C.c_size_t(0)
+    exact = lib().orc_jobs_verify(C.cast(jobs, C.c_void_p), C.cast(arr, C.c_void_p), len(hits), N,
+                                  buf, len(buf), C.byref(nl))
+    return exact, [l for l in buf.value.decode().splitlines() if l]
 
 
 def jobs617(B: int, cls: int):

@@ -873,6 +873,184 @@ size_t orc_find3_run(const orc_table* t, const orc_job3* jobs, size_t n, int use
   return nh;
 }
 
+// ------------------------------------------- reduced-T jobs (find2/3/4)
+// T = (B^6 - u^6 - sum of the peeled terms^6) / D^6 as compute_T_gmp /
+// compute_T_peel1_gmp / compute_T_peel2_gmp (fourcore_gmp.hpp:34-62):
+// false when the difference is not positive, not divisible, or T >= 2^128.
+static bool o_job_T(u64 B, u64 u, const u64* terms, int nt, u64 D6, u128* T) {
+  if (u >= B) return false;
+  W3 R = w3_pow6(B);
+  if (w3_sub(R, w3_pow6(u))) return false;
+  for (int i = 0; i < nt; ++i)
+    if (w3_sub(R, w3_pow6(terms[i]))) return false;
+  if (w3_zero(R) || w3_divmod(R, D6) != 0 || !w3_fits128(R)) return false;
+  *T = w3_to128(R);
+  return true;
+}
+
+size_t orc_expand_unit(uint64_t B, uint64_t u, int cls, orc_job* out, size_t cap,
+                       uint64_t* fail_t) {
+  size_t k = 0;
+  u64 fails = 0;
+  const u32 lim = (u32)((B - 1) / 42);
+  auto push = [&](u64 f1, u64 f2, u128 T) {
+    if (T == 0) return;
+    orc_job J{};
+    J.cls = (u32)cls; J.lim = lim; J.B = B; J.u = u; J.free1 = f1; J.free2 = f2;
+    J.T[0] = (u64)T; J.T[1] = (u64)(T >> 64);
+    if (k < cap) out[k] = J;
+    ++k;
+  };
+  // for_each_free (classes_v3.hpp:224-232)
+  auto each = [](const std::vector<long long>& res, u64 mod, u64 fmax, auto&& fn) {
+    if (mod == 0 || fmax < 1) return;
+    for (long long r : res)
+      for (u64 x = (u64)r; x <= fmax; x += mod)
+        if (x) fn(x);
+  };
+  u128 T = 0;
+  if (cls == 1) {
+    if (o_job_T(B, u, nullptr, 0, kM42, &T)) push(0, 0, T);   // D = 42 (:172-176)
+    else ++fails;
+  } else if (cls >= 2 && cls <= 4) {
+    u32 res[32]; u32 nres = 0; u64 mod = 0, fmax = 0;
+    orc_free_d_cls234(B, u, cls, res, &nres, &mod, &fmax);
+    const u64 f = cls == 2 ? 14 : cls == 3 ? 21 : 7;
+    std::vector<long long> rv(res, res + nres);
+    each(rv, mod, fmax, [&](u64 d) {
+      const u64 t1 = f * d;
+      if (o_job_T(B, u, &t1, 1, kM42, &T)) push(d, 0, T);
+      else ++fails;
+    });
+  } else if (cls == 5) {                                        // free_de_cls5, e outer (:191-203)
+    const auto er = classes_d_cls2((long long)B);
+    const auto dr = classes_d_cls3((long long)B, (long long)u);
+    each(er, kM3, (B - 1) / 14, [&](u64 e) {
+      each(dr, kM2, (B - 1) / 21, [&](u64 d) {
+        const u64 t2[2] = {21 * d, 14 * e};
+        if (o_job_T(B, u, t2, 2, kM42, &T)) push(d, e, T);
+        else ++fails;
+      });
+    });
+  }
+  if (fail_t) *fail_t = fails;
+  return k;
+}
+
+size_t orc_jobs_run(const orc_table* t, const orc_job* jobs, size_t n, int use_gate, int ref_tiles,
+                    int threads, orc_hit4* hits, size_t cap, uint64_t counters[3]) {
+  const Gate& G = gate();
+  std::vector<orc_job3> j3, j4;
+  std::vector<u32> i3, i4;
+  u64 c[3] = {0, 0, 0};
+  size_t nh = 0;
+  auto add = [&](u32 job, u32 c3, u32 c4, u64 fp) {
+    if (nh < cap) hits[nh] = orc_hit4{job, c3, c4, 0, fp};
+    ++nh;
+  };
+  for (size_t i = 0; i < n; ++i) {
+    const orc_job& J = jobs[i];
+    const u128 T = ((u128)J.T[1] << 64) | J.T[0];
+    if (J.cls == 5) {                                           // k_find2 (:233-252)
+      ++c[0];
+      if (use_gate && !(G.g504[(u32)(T % 504)] && G.g247[(u32)(T % 247)])) { ++c[1]; continue; }
+      ++c[2];
+      if (might_contain(*t, J.T[0])) add((u32)i, 0, 0, J.T[0]);
+      continue;
+    }
+    if (J.cls < 1 || J.cls > 4) continue;
+    const u32 k = J.cls == 1 ? 4 : 3;                          // make_cand (:401-425)
+    const u32 hi = std::min(iroot6_find(T), J.lim);
+    u64 lo = 1;
+    while (lo <= hi && pow6_u128(lo) * k < T) ++lo;
+    if (lo > hi) continue;
+    orc_job3 X{};
+    X.cls = J.cls; X.lim = J.lim; X.B = J.B; X.u = J.u; X.d = J.free1;
+    X.T[0] = J.T[0]; X.T[1] = J.T[1]; X.lo = (u32)lo; X.hi = hi;
+    (k == 4 ? j4 : j3).push_back(X);
+    (k == 4 ? i4 : i3).push_back((u32)i);
+  }
+  if (!j3.empty()) {
+    std::vector<orc_hit3> h(1 << 20);
+    u64 cc[3];
+    const size_t m = orc_find3_run(t, j3.data(), j3.size(), use_gate, threads, h.data(), h.size(), cc);
+    for (size_t q = 0; q < std::min(m, h.size()); ++q) add(i3[h[q].job], h[q].c3, 0, h[q].fp);
+    for (int q = 0; q < 3; ++q) c[q] += cc[q];
+  }
+  if (!j4.empty()) {
+    std::vector<orc_hit4> h(1 << 20);
+    u64 cc[3];
+    const size_t m = orc_find4_run(t, j4.data(), j4.size(), use_gate, ref_tiles, threads, h.data(),
+                                   h.size(), cc);
+    for (size_t q = 0; q < std::min(m, h.size()); ++q) add(i4[h[q].job], h[q].c3, h[q].c4, h[q].fp);
+    for (int q = 0; q < 3; ++q) c[q] += cc[q];
+  }
+  for (int q = 0; q < 3; ++q) counters[q] = c[q];
+  return nh;
+}
+
+size_t orc_jobs_verify(const orc_job* jobs, const orc_hit4* hits, size_t nh, int N, char* buf,
+                       size_t buflen, size_t* n_lines) {
+  PairRecover pr(N);
+  std::vector<std::pair<u32, u32>> pairs;
+  std::string text;
+  size_t exact = 0, lines = 0;
+  for (size_t q = 0; q < nh; ++q) {
+    const orc_hit4& H = hits[q];
+    const orc_job& J = jobs[H.job];
+    const u128 T = ((u128)J.T[1] << 64) | J.T[0];
+    pr.recover(H.fp, pairs);
+    for (auto [a, b] : pairs) {
+      u128 core = pow6_u128(a) + pow6_u128(b);
+      W3 rhs = w3_pow6(J.u);
+      long long t[5];
+      if (J.cls == 5) {                                         // mode 2 (:537-541)
+        if (a > J.lim || b > J.lim || core != T) continue;
+        w3_add(rhs, w3_pow6(21 * J.free1));                     // verify_cls5_gmp
+        w3_add(rhs, w3_pow6(14 * J.free2));
+        t[2] = 21LL * (long long)J.free1; t[3] = 14LL * (long long)J.free2;
+      } else if (J.cls >= 2 && J.cls <= 4) {                    // mode 3 (:542-547)
+        if (H.c3 < 1 || b > H.c3) continue;
+        core += pow6_u128(H.c3);
+        if (core != T) continue;
+        const u64 f = J.cls == 2 ? 14 : J.cls == 3 ? 21 : 7;
+        w3_add(rhs, w3_pow6(f * J.free1));                      // verify_cls234_gmp
+        t[2] = 42LL * H.c3; t[3] = (long long)(f * J.free1);
+      } else {                                                  // mode 4 (:548-554)
+        if (H.c3 < 1 || H.c4 < 1 || b > H.c3 || H.c3 > H.c4) continue;
+        core += pow6_u128(H.c3) + pow6_u128(H.c4);
+        if (core != T) continue;
+        t[2] = 42LL * H.c3; t[3] = 42LL * H.c4;                 // verify_fourcore_gmp, D = 42
+      }
+      ++exact;
+      w3_add(rhs, w3_mul_u64(w3_u128(core), kM42));
+      if (!w3_eq(rhs, w3_pow6(J.B))) continue;
+      t[0] = 42LL * a; t[1] = 42LL * b; t[4] = (long long)J.u;
+      std::sort(t, t + 5);                                      // report_solution (:427-457)
+      bool bad = false;
+      for (int i = 0; i < 4; ++i) if (t[i] == t[i + 1]) bad = true;
+      if (bad || t[4] >= (long long)J.B || t[0] < 1) continue;
+      long long g = t[0];
+      for (int i = 1; i < 5; ++i) g = std::gcd(g, t[i]);
+      g = std::gcd(g, (long long)J.B);
+      char line[256];
+      std::snprintf(line, sizeof line,
+                    "SOLUTION cls=%u B=%llu u=%llu a1=%lld a2=%lld a3=%lld a4=%lld a5=%lld gcd=%lld %s\n",
+                    J.cls, (unsigned long long)J.B, (unsigned long long)J.u, t[0], t[1], t[2], t[3],
+                    t[4], g, g == 1 ? "primitive" : "NON-PRIMITIVE");
+      text += line;
+      ++lines;
+    }
+  }
+  if (buf && buflen) {
+    const size_t m = std::min(text.size(), buflen - 1);
+    std::memcpy(buf, text.data(), m);
+    buf[m] = 0;
+  }
+  if (n_lines) *n_lines = lines;
+  return exact;
+}
+
 }  // extern "C"
 
 // ===================================================== (6,1,7) Branch-A cls5

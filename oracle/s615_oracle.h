@@ -128,6 +128,29 @@ size_t orc_expand_cls1(uint64_t B, uint64_t u, orc_job3* out, size_t cap);
 size_t orc_find4_run(const orc_table* t, const orc_job3* jobs, size_t n, int use_gate,
                      int ref_tiles, int threads, orc_hit4* hits, size_t cap, uint64_t counters[3]);
 
+/* ---- reduced-T jobs of fourcore_find_v4 (.but / .bbj; find2 / find3 / find4) ---- */
+typedef struct orc_job {
+  uint32_t cls, lim;    /* lim = (B-1)/42 (job_from_bin, fourcore_find_v4.cu:598-608) */
+  uint64_t B, u, free1, free2;
+  uint64_t T[2];
+} orc_job;
+/* expand_unit (fourcore_find_v4.cu:164-205) for cls 1-5: the jobs of one
+ * Stage-1 unit in the reference's order; *fail_t counts the d or (e, d) whose
+ * T cannot be formed (compute_T_*_gmp false). */
+size_t orc_expand_unit(uint64_t B, uint64_t u, int cls, orc_job* out, size_t cap,
+                       uint64_t* fail_t);
+/* run_batch over jobs: make_cand (:401-425) then k_find2 (:233-252), k_find3
+ * (:255-284) or k_find4 (:287-338) by class; empty find3/find4 windows are
+ * dropped (:486).  Hits {job, c3, c4, fp} (c3 = c4 = 0 for find2, c4 = 0 for
+ * find3); counters calls / gated / probes summed over the three modes. */
+size_t orc_jobs_run(const orc_table* t, const orc_job* jobs, size_t n, int use_gate, int ref_tiles,
+                    int threads, orc_hit4* hits, size_t cap, uint64_t counters[3]);
+/* The exact filter of run_batch (:536-560) over PairRecover's pairs: returns
+ * the exact matches (the reference's `sols`); the ones report_solution
+ * (:427-457) prints go to buf as SOLUTION lines, *n_lines of them. */
+size_t orc_jobs_verify(const orc_job* jobs, const orc_hit4* hits, size_t nh, int N, char* buf,
+                       size_t buflen, size_t* n_lines);
+
 /* ---- (6,1,7) Branch-A class 5 (solve_617_v1.cu) ---- */
 typedef struct orc_cand617 {
   uint64_t base[2];        /* B^6 - u^6 - w^6 (i128; B <= 2,353,973) */

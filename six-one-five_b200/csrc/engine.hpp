@@ -100,6 +100,14 @@ S615_HD u64 make_item(u32 unit, u32 ires, u32 chunk) {
 S615_HD u32 item_unit(u64 it) { return (u32)(it >> 32); }
 S615_HD u32 item_res(u64 it) { return (u32)(it >> 24) & 255u; }
 S615_HD u32 item_chunk(u64 it) { return (u32)it & 0xFFFFFFu; }
+// Reduced-T jobs (kind 2) of classes 2-5 become one-row units of this
+// internal class; consecutive ones share an item (first unit, kJobItemTag,
+// count | kJobFind2 for the one-probe rows of class-5 jobs).
+constexpr u32 kClsJobRow = 9;
+constexpr u32 kJobRows = 64;
+constexpr u32 kJobItemTag = 255;
+constexpr u32 kJobFind2 = 1u << 8;
+S615_HD u32 job_count(u64 it) { return (u32)it & 0xFFu; }
 // Rows of one residue class: x = r0 + mod j for j in [jmin, jend), x <= fmax.
 S615_HD void class_rows(u32 r0, u32 mod, u32 fmax, u32* jmin, u32* jend) {
   *jmin = (r0 == 0) ? 1u : 0u;

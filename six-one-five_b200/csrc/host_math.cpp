@@ -536,10 +536,68 @@ static int make_dev_unit8(const s615_unit& in, DevUnit* out) {
   return S615_OK;
 }
 
+// kind 2: one reduced-T job of fourcore_find_v4 (job_from_bin :598-608 with
+// make_cand :401-425).  lim defaults to (B-1)/42 and stays <= (kMaxB-1)/42,
+// so 3 lim^6 < 2^121 and 4 lim^6 < 2^122: a find3 job with T >= 2^121 or a
+// find4 job with T >= 2^122 has an empty window, dropped like run_batch drops
+// it (:486).  cls 2-4: a one-row unit (kClsJobRow) whose row value is T;
+// cls 5 (find2): the same row with W = T + 1 and the window [1, 1], so the
+// gate tests W - 1^6 = T and the key is T mod 2^64.  When T + 1 >= 2^121, W is
+// T + 1 reduced mod 15561 * 2^64 (15561 = 9 * 7 * 13 * 19), which keeps the key
+// and every gate residue.  cls 1: the class-1 find4 unit with T given.
+static int make_dev_job(const s615_unit& in, DevUnit* out, bool* skip) {
+  if (in.cls < 1 || in.cls > 5 || in.base[2] != 0) return S615_E_FORMAT;
+  const u128 T = ((u128)in.base[1] << 64) | in.base[0];
+  const u64 lim = in.lim ? in.lim : (in.B ? (in.B - 1) / 42 : 0);
+  if (lim > (kMaxB - 1) / 42) return S615_E_FORMAT;
+  out->B = in.B; out->u = in.u;
+  out->lim = (u32)lim;
+  if (in.cls == 1) {
+    if (T == 0 || (T >> 122) != 0) { *skip = true; return S615_OK; }
+    const u32 hi4 = std::min(iroot6_exact(T), (u32)lim);
+    const u32 lo4 = least_c_k(T, 4);
+    if (hi4 < 1 || lo4 > hi4) { *skip = true; return S615_OK; }
+    out->cls = 1;
+    out->base_lo = (u64)T;
+    out->base_hi = (u64)(T >> 64);
+    out->fmax1 = hi4;
+    out->fmax2 = lo4;
+    out->nres1 = 1;
+    return S615_OK;
+  }
+  u128 W;
+  if (in.cls == 5) {
+    const u128 M = (u128)15561 << 64;
+    W = (T >> 121) == 0 && T + 1 < ((u128)1 << 121) ? T + 1 : (T % M + 1) % M;
+    if (W == 0) W = M;
+    out->w = 1;
+  } else {
+    if (T == 0 || (T >> 121) != 0) { *skip = true; return S615_OK; }
+    const u32 hi = std::min(iroot6_exact(T), (u32)lim);
+    if (hi < 1 || least_c_k(T, 3) > hi) { *skip = true; return S615_OK; }
+    W = T;
+  }
+  out->cls = kClsJobRow;
+  out->f = 0;            // row x = 0: the row value is (base >> 6) / 21^6 = W
+  out->mod1 = 1;
+  out->fmax1 = 1;
+  out->nres1 = 1;
+  out->res1[0] = 1;
+  const u128 base = W * (u128)kM42;   // mod 2^128
+  out->base_lo = (u64)base;
+  out->base_hi = (u64)(base >> 64);
+  return S615_OK;
+}
+
 int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip) {
   std::memset(out, 0, sizeof *out);
   *skip = false;
   const u32 cls = in.cls;
+  if (in.kind == S615_KIND_JOB) {
+    const int s = make_dev_job(in, out, skip);
+    out->id = id;
+    return s;
+  }
   if (cls == S615_CLS_617_FIND4) {
     const int s = make_dev_unit8(in, out);
     out->id = id;
@@ -627,6 +685,19 @@ int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip) {
 }
 
 void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out) {
+  if (d.cls == kClsJobRow) {   // runs of up to kJobRows consecutive job rows of one kind
+    const u32 kind = d.w != 0 ? kJobFind2 : 0u;
+    if (!out.empty()) {
+      const u64 last = out.back();
+      if (item_res(last) == kJobItemTag && (item_chunk(last) & kJobFind2) == kind &&
+          item_unit(last) + job_count(last) == unit_index && job_count(last) < kJobRows) {
+        out.back() = last + 1;
+        return;
+      }
+    }
+    out.push_back(make_item(unit_index, kJobItemTag, kind | 1u));
+    return;
+  }
   if (d.cls == 1 || d.cls == S615_CLS_617_FIND4) {   // chunks of the c4 window
     const u32 n = (d.fmax1 - d.fmax2) / kC4Chunk + 1;
     for (u32 c = 0; c < n; ++c) out.push_back(make_item(unit_index, 0, c));

@@ -95,7 +95,7 @@ __device__ __forceinline__ u32 pow6_mod512(u32 x) {
 __device__ __forceinline__ u32 entry(u32 di, u32 r, u32 k) { return (di << 24) | (r << 18) | k; }
 
 struct ItemCtx {
-  u32 cls, unit_id, r0, mod, j0, f;
+  u32 cls, unit_id, r0, mod, j0, f, u0;   // u0: first unit of a job item
 };
 
 // Probe the ring entries [head, head+cnt) (one per lane).
@@ -124,6 +124,10 @@ __device__ __forceinline__ void probe_batch(const PeelParams& P, const WarpSmem&
       h.unit = I.unit_id; h.a = 0; h.b = 0; h.c4 = 0;
       if (I.cls == 5) { h.d = (u32)x; h.e = rowval; }
       else { h.d = rowval; h.e = (u32)x; }
+      if (I.cls == kClsJobRow) {   // row r is unit u0 + r (hits are rare: one load)
+        h.unit = P.units[I.u0 + r].id;
+        h.d = 0;
+      }
       h.fp = key;
       P.hits[idx] = h;
     }
@@ -176,13 +180,22 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
     ItemCtx I;
     I.cls = U->cls;
     I.unit_id = U->id;
-    I.r0 = U->res1[item_res(packed)];
-    I.mod = U->mod1;
+    I.u0 = item_unit(packed);
     I.f = U->f;
-    u32 jmin, jend;
-    class_rows(I.r0, I.mod, U->fmax1, &jmin, &jend);
-    I.j0 = jmin + item_chunk(packed) * kRows;
-    const u32 nrows = min(kRows, jend - I.j0);
+    u32 nrows;
+    if (I.cls == kClsJobRow) {   // job_count consecutive one-row units; row r is unit u0 + r
+      I.r0 = 0;
+      I.mod = 1;
+      I.j0 = 0;
+      nrows = job_count(packed);
+    } else {
+      I.r0 = U->res1[item_res(packed)];
+      I.mod = U->mod1;
+      u32 jmin, jend;
+      class_rows(I.r0, I.mod, U->fmax1, &jmin, &jend);
+      I.j0 = jmin + item_chunk(packed) * kRows;
+      nrows = min(kRows, jend - I.j0);
+    }
     const u128 base = ((u128)U->base_hi << 64) | U->base_lo;
     const u32 lim = U->lim;
     u32 head = 0, qlen = 0;
@@ -294,20 +307,24 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
         __syncwarp();
       }
     } else {
-      // ---- cls2-4 rows: T(d) and its find3 window [lo, hi] ----
+      // ---- cls2-4 rows: T(d) and its find3 window [lo, hi]; job rows: T given ----
+      const bool job = I.cls == kClsJobRow;
+      const bool find2 = job && U->w != 0;
       for (u32 r = lane; r < nrows; r += 32) {
+        const DevUnit* Ur = job ? U + r : U;
         const u64 x = (u64)I.f * ((u64)I.r0 + (u64)I.mod * (I.j0 + r));
         const u128 x3 = (u128)(x * x) * x;
-        const u128 Rm = base - x3 * x3;                         // R mod 2^128
+        const u128 Rm = (job ? (((u128)Ur->base_hi << 64) | Ur->base_lo) : base) - x3 * x3;
         const u128 T = ((Rm >> 6) * inv21) & ((~(u128)0) >> 6);  // T mod 2^122
+        const u32 rlim = job ? Ur->lim : lim;
         RowRec R;
         R.wlo = (u64)T; R.whi = (u64)(T >> 64);
         R.a = 0; R.b = 0;
         R.off[0] = R.off[1] = R.off[2] = R.off[3] = 0;
         if (T != 0 && (T >> 121) == 0) {
-          const u32 hi = min(iroot6_u128(T), lim);
+          const u32 hi = find2 ? 1u : min(iroot6_u128(T), rlim);
           const u128 third = T / 3 + ((T % 3) ? 1 : 0);         // ceil(T/3) >= 1
-          const u32 lo = iroot6_u128(third - 1) + 1;            // least c with 3 c^6 >= T
+          const u32 lo = find2 ? 1u : iroot6_u128(third - 1) + 1;  // least c with 3 c^6 >= T
           if (lo <= hi) {
             const u32 len = hi - lo + 1;
             u32 m4 = 0;
@@ -327,6 +344,22 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
         W.rows[r] = R;
       }
       __syncwarp();
+      if (find2) {   // one column per row: lane r takes row r
+        for (u32 r0 = 0; r0 < nrows; r0 += 32) {
+          const u32 r = r0 + lane;
+          u32 m = 0;
+          if (r < nrows) {
+            const RowRec& R = W.rows[r];
+            if (R.b & kLenMask) m = (R.b >> 28) & gate_word(s_pat3, R, 1, 1, 1, 1) & 1u;
+          }
+          my_probes += m;
+          push_bits(P, W, m, 0, r & 63u, 0, head, qlen, I, lane);
+        }
+        __syncwarp();
+        probe_batch(P, W, head, qlen, I, lane);
+        __syncwarp();
+        continue;
+      }
       for (u32 r = 0; r < nrows; ++r) {
         const RowRec& R = W.rows[r];
         const u32 len = R.b & kLenMask;

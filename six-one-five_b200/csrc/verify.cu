@@ -39,12 +39,14 @@ __global__ void k_verify(const DevUnit* __restrict__ units, const s615_hit* __re
     const u128 base = ((u128)U.base_hi << 64) | U.base_lo;
     u128 S;
     u32 cmax;
-    if (U.cls == 1 || U.cls == S615_CLS_617_FIND4) {   // base holds T; S = T - c4^6 - c3^6, pairs up to N
+    if (U.cls == 1 || U.cls == S615_CLS_617_FIND4) {   // base holds T; S = T - c4^6 - c3^6
       const u128 T = base;
       const u128 c46 = pow6_small(H.c4) + pow6_small(H.e);
       if (T <= c46) continue;
       S = T - c46;
-      cmax = N;
+      // cls 1: a <= b <= c3 (run_batch mode 4, fourcore_find_v4.cu:548-554);
+      // the (6,1,7) jobs take every pair up to N (expand_xor_hits)
+      cmax = U.cls == 1 ? min(N, H.e) : N;
     } else if (U.cls == 5) {
       const u64 x = 14ull * H.e;
       const u128 x3 = (u128)(x * x) * x;
@@ -63,6 +65,7 @@ __global__ void k_verify(const DevUnit* __restrict__ units, const s615_hit* __re
       if ((T >> 121) || T <= c6) continue;
       S = T - c6;
       cmax = min(N, H.e);
+      if (U.cls == kClsJobRow && U.w) cmax = min(N, U.lim);   // find2: a, b <= lim (:537-541)
       if (U.cls == S615_CLS_617) {   // T - c3^6 - c4^6; pairs up to N
         const u128 c46 = pow6_small(H.c4);
         if (S <= c46) continue;
@@ -163,6 +166,49 @@ int verify_device(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s
     S.c1 = p.c1; S.c2 = p.c2;
     W3 rhs;   // the peeled terms plus 42^6 times the core
     long long t[5];
+    if (U.kind == S615_KIND_JOB) {
+      // run_batch's exact filter (fourcore_find_v4.cu:536-560), then
+      // report_solution's identity and term rules (:427-457).  An exact match
+      // whose identity does not hold for (B, u, free terms) stays kind 2: the
+      // reference counts it in `sols` but prints nothing.
+      const u128 T = ((u128)U.base[1] << 64) | U.base[0];
+      u128 core = pow6_u128(p.c1) + pow6_u128(p.c2);
+      rhs = pow6_w3(U.u);
+      S.d = U.res_d;
+      S.e = U.res_e;
+      if (U.cls == 1) {
+        S.c3 = H.e; S.c4 = H.c4;
+        core += pow6_u128(H.e) + pow6_u128(H.c4);
+        t[2] = 42LL * H.e; t[3] = 42LL * H.c4;
+      } else if (U.cls == 5) {
+        add_w3(rhs, pow6_w3(21ULL * U.res_d));
+        add_w3(rhs, pow6_w3(14ULL * U.res_e));
+        t[2] = 21LL * U.res_d; t[3] = 14LL * U.res_e;
+      } else {
+        const u64 f = (u64)free_factor((int)U.cls);
+        S.c3 = H.e;
+        core += pow6_u128(H.e);
+        add_w3(rhs, pow6_w3(f * U.res_d));
+        t[2] = 42LL * H.e; t[3] = (long long)(f * U.res_d);
+      }
+      if (core != T) continue;
+      add_w3(rhs, mul_w3_u64(W3{{(u64)core, (u64)(core >> 64), 0}}, kM42));
+      t[0] = 42LL * p.c1; t[1] = 42LL * p.c2; t[4] = (long long)U.u;
+      std::sort(t, t + 5);
+      bool ok = eq_w3(rhs, pow6_w3(U.B)) && t[0] >= 1 && t[4] < (long long)U.B;
+      for (int i = 0; i < 4; ++i) if (t[i] == t[i + 1]) ok = false;
+      if (ok) {
+        long long g = t[0];
+        for (int i = 1; i < 5; ++i) g = std::gcd(g, t[i]);
+        g = std::gcd(g, (long long)U.B);
+        for (int i = 0; i < 5; ++i) S.a[i] = t[i];
+        S.gcd = g;
+        S.kind = 0;
+      }
+      if (k < cap) out[k] = S;
+      ++k;
+      continue;
+    }
     if (U.cls == S615_CLS_617_FIND4) {   // B^6 = u^6 + w^6 + 42^6 (c1^6 + .. + c5^6)
       S.c3 = H.e; S.c4 = H.c4; S.w = U.w;
       S.d = U.res_d;    // the (6,1,7) class

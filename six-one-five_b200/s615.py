@@ -25,6 +25,7 @@ LAYOUT_AUTO, LAYOUT_PACKED, LAYOUT_WIDE = 0, 1, 2
 F_NO_GATE, F_PLAIN, F_NO_TRI, F_SHARP = 1, 2, 4, 8
 S615_CLS_617 = 7
 S615_CLS_617_FIND4 = 8
+S615_KIND_JOB = 2
 
 
 class S615Error(RuntimeError):
@@ -114,6 +115,12 @@ SIGNATURES = {
     "s615_unit_status": (C.c_int, [_P]),
     "s615_617_candidates": (C.c_int, [C.c_uint64, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
     "s615_617_jobs": (C.c_int, [C.c_uint64, C.c_int, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "s615_expand_unit": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(C.c_size_t),
+                                   C.POINTER(C.c_uint64)]),
+    "s615_jobs_open": (C.c_int, [C.c_char_p, C.POINTER(_P), _P]),
+    "s615_jobs_next": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "s615_jobs_close": (C.c_int, [_P, _P]),
+    "s615_jobs_write": (C.c_int, [C.c_char_p, _P, C.c_size_t]),
     "s615_run": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.c_uint, _P, C.c_size_t,
                            C.POINTER(C.c_size_t), C.POINTER(Counters)]),
     "s615_cls5_run": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.c_uint, _P, C.c_size_t,
@@ -246,6 +253,62 @@ def jobs617(B: int, cls: int):
     arr = (Unit * max(n.value, 1))()
     _check(lib().s615_617_jobs(B, cls, C.cast(arr, C.c_void_p), n.value, C.byref(n)), "617_jobs")
     return arr, n.value
+
+
+class JobsInfo(C.Structure):
+    _fields_ = [("n_jobs", C.c_uint64), ("min_B", C.c_uint32), ("max_B", C.c_uint32),
+                ("binary", C.c_uint32), ("pad", C.c_uint32), ("bad_lines", C.c_uint64)]
+
+
+def make_job(cls: int, B: int, u: int, T: int, free1: int = 0, free2: int = 0, lim: int = 0) -> Unit:
+    """A reduced-T job (kind 2): fourcore_find_v4's Job{cls, B, u, free1, free2, T}."""
+    J = Unit()
+    J.cls, J.kind, J.B, J.u = cls, S615_KIND_JOB, B, u
+    J.base[0], J.base[1] = T % 2**64, T >> 64
+    J.res_d, J.res_e, J.lim = free1, free2, lim
+    return J
+
+
+def expand_unit(B: int, u: int, cls: int):
+    """s615_expand_unit: (jobs, n, failT) of one Stage-1 unit."""
+    unit = Unit()
+    unit.cls, unit.B, unit.u = cls, B, u
+    n, fail = C.c_size_t(0), C.c_uint64(0)
+    st = lib().s615_expand_unit(C.byref(unit), None, 0, C.byref(n), C.byref(fail))
+    if st not in (S615_OK, -9):
+        _check(st, "expand_unit")
+    arr = (Unit * max(n.value, 1))()
+    _check(lib().s615_expand_unit(C.byref(unit), C.cast(arr, C.c_void_p), n.value, C.byref(n),
+                                  C.byref(fail)), "expand_unit")
+    return arr, n.value, fail.value
+
+
+def jobs_write(path: str, jobs, n: int) -> None:
+    """s615_jobs_write: a .bbj (binary) or text job file."""
+    _check(lib().s615_jobs_write(path.encode(), C.cast(jobs, C.c_void_p), n), "jobs_write")
+
+
+def jobs_read(path: str, chunk: int = 1 << 16):
+    """Every job of a .bbj or text job file: (array, n, JobsInfo)."""
+    f = C.c_void_p()
+    info = JobsInfo()
+    _check(lib().s615_jobs_open(path.encode(), C.byref(f), C.byref(info)), "jobs_open")
+    parts, n = [], 0
+    try:
+        while True:
+            buf = (Unit * chunk)()
+            k = C.c_size_t(0)
+            _check(lib().s615_jobs_next(f, C.cast(buf, C.c_void_p), chunk, C.byref(k)), "jobs_next")
+            if not k.value:
+                break
+            parts.append(C.string_at(C.addressof(buf), k.value * C.sizeof(Unit)))
+            n += k.value
+    finally:
+        lib().s615_jobs_close(f, C.byref(info))
+    out = (Unit * max(n, 1))()
+    if n:
+        C.memmove(out, b"".join(parts), n * C.sizeof(Unit))
+    return out, n, info
 
 
 def jobs617_band(Bs: Iterable[int], classes: Iterable[int] = (1, 2, 3, 4)):
@@ -458,6 +521,9 @@ def solution_line(s: Solution) -> str:
         if s.cls == 1:
             return f"PLANT cls=1 unit={s.unit} c1={s.c1} c2={s.c2} c3={s.c3} c4={s.c4}"
         return f"PLANT cls={s.cls} unit={s.unit} d={s.d} c1={s.c1} c2={s.c2} c3={s.c3}"
+    if s.kind == S615_KIND_JOB:   # an exact T match whose full identity does not hold
+        return (f"EXACT cls={s.cls} unit={s.unit} d={s.d} e={s.e} c1={s.c1} c2={s.c2} "
+                f"c3={s.c3} c4={s.c4}")
     a = list(s.a)
     if s.cls == S615_CLS_617_FIND4:   # the (6,1,7) class is in d
         terms = " ".join(f"a{i + 1}={a[i]}" for i in range(7))
