@@ -14,6 +14,7 @@ Multi-GPU (torchrun): each rank owns its own 20,000-B band (weak scaling),
 no collective on the data path; rank 0 prints one JSON line.
 
   python bench.py --workload cls617 [--impl ours|reference]
+  python bench.py --workload jobs    (reduced-T jobs through a .bbj file)
 
 measures the (6,1,7) Branch-A class-5 search instead: one step is every
 candidate of the eligible B in [400,401, 400,441) (a slice of the band
@@ -58,7 +59,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-find4", action="store_true", help="cls617: skip the classes 1-4 pass")
-    ap.add_argument("--workload", default="cls5", choices=["cls5", "cls617", "mix", "serve"])
+    ap.add_argument("--workload", default="cls5", choices=["cls5", "cls617", "mix", "serve", "jobs"])
     ap.add_argument("--units", type=int, default=0, help="mix: units per step (default 200,000)")
     ap.add_argument("--seconds", type=float, default=10.0, help="serve: seconds of arrivals")
     return ap.parse_args()
@@ -643,6 +644,170 @@ def run_mix(args, rank, world, local, dist):
     return 0
 
 
+METRIC_JOBS = ("reduced-T jobs/s (.bbj file, classes 1-4 of the mixed stream, B log-uniform "
+               "[1M,4M]), 1 B200")
+
+
+def run_jobs(args, rank, world, local, dist):
+    """Stage-1 units of classes 1-4 drawn like the mixed stream (B log-uniform
+    on [1M, 4M]) expanded into reduced-T jobs (expand_unit), written to a .bbj
+    file and read back; one step = one device pass over every job (find3 rows
+    for classes 2-4, find4 for class 1) against the N = 95,239 table."""
+    import tempfile
+
+    import numpy as np
+    import torch
+
+    import s615
+    import workloads as W
+    torch.cuda.set_device(local)
+    n_units = args.units or 20_000
+    N = args.N or math.ceil(4_000_000 / 42)
+    eng = s615.Engine(local)
+    t0 = time.perf_counter()
+    tid = eng.build_table(N, args.r)
+    build_s = time.perf_counter() - t0
+    units = W.mixed_units(n_units, 5 + rank, 1_000_000, 4_000_000,
+                          mix={1: 0.01, 2: 0.04, 3: 0.01, 4: 0.48})
+    t0 = time.perf_counter()
+    jobs, n, fail_t = s615.expand_units(units)
+    expand_s = time.perf_counter() - t0
+    path = os.path.join(tempfile.gettempdir(), f"s615_bench_jobs_{rank}.bbj")
+    t0 = time.perf_counter()
+    s615.jobs_write(path, jobs, n)
+    write_s = time.perf_counter() - t0
+    file_bytes = os.path.getsize(path)
+    t0 = time.perf_counter()
+    jobs, n2, _ = s615.jobs_read(path)
+    read_s = time.perf_counter() - t0
+    assert n2 == n
+    log(f"rank {rank}: {len(units)} units -> {n} jobs ({file_bytes / 1e6:.1f} MB .bbj)")
+
+    lib = s615.lib()
+    stream = torch.cuda.Stream()
+    sptr = C.c_void_p(stream.cuda_stream)
+    batch = C.c_void_p()
+    s615._check(lib.s615_prepare(eng._ctx, C.cast(jobs, C.c_void_p), n, C.byref(batch)), "prepare")
+    for _ in range(args.warmup):
+        s615._check(lib.s615_run_batch(eng._ctx, tid, batch, 0, sptr), "run_batch")
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    launches0 = eng.launches
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev[0].record(stream)
+    for k in range(args.steps):
+        s615._check(lib.s615_run_batch(eng._ctx, tid, batch, 0, sptr), "run_batch")
+        ev[k + 1].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    cl = clocks.stop()
+    launches = eng.launches - launches0
+    per_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[args.steps])
+    hits = (s615.Hit * (1 << 20))()
+    nh = C.c_size_t(0)
+    ctr = s615.Counters()
+    s615._check(lib.s615_batch_results(eng._ctx, batch, C.cast(hits, C.c_void_p), 1 << 20,
+                                       C.byref(nh), C.byref(ctr)), "results")
+    sols = eng.verify(jobs, n, s615.hits_to_array(hits, nh.value), N, cap=65536)
+    h2d = batch_h2d(lib, batch)
+    s615._check(lib.s615_batch_free(eng._ctx, batch), "batch_free")
+
+    # the same Stage-1 units searched directly (no job format): same rows
+    uarr = (s615.Unit * len(units))()
+    for i, (c, B, u) in enumerate(units):
+        uarr[i].cls, uarr[i].B, uarr[i].u = c, B, u
+    s615._check(lib.s615_prepare(eng._ctx, C.cast(uarr, C.c_void_p), len(units), C.byref(batch)),
+                "prepare")
+    units_ms, uctr = timed_steps(lib, eng, tid, batch, stream, 0, 1)
+    s615._check(lib.s615_batch_free(eng._ctx, batch), "batch_free")
+    assert (uctr.pos, uctr.probes) == (ctr.calls, ctr.probes)
+
+    # e2e: the .bbj file read, then s615_run (host jobs in, hits + counters out)
+    e2e_steps = max(1, min(args.steps, 2))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        j3, n3, _ = s615.jobs_read(path)
+        h3, c3 = eng.run(tid, j3, n3, hit_cap=1 << 16)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    assert c3.probes == ctr.probes
+    os.remove(path)
+
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        import orc
+        cores = os.cpu_count() or 1
+        table = orc.Table.build_pairs(2000, args.r)
+
+        def sample(count):
+            idx = np.linspace(0, n - 1, min(n, count)).astype(int)
+            samp = (orc.OrcJob * len(idx))()
+            for k, i in enumerate(idx):
+                J = jobs[int(i)]
+                samp[k].cls, samp[k].lim, samp[k].B, samp[k].u = J.cls, (J.B - 1) // 42, J.B, J.u
+                samp[k].free1, samp[k].free2 = J.res_d, J.res_e
+                samp[k].T[0], samp[k].T[1] = J.base[0], J.base[1]
+            t0 = time.perf_counter()
+            _, oc = orc.run_jobs(table, samp, len(idx), threads=cores)
+            return idx, oc, time.perf_counter() - t0
+
+        idx, oc, took = sample(64 * cores)          # calibration, then ~10 s of CPU work
+        idx, oc, took = sample(int(len(idx) * 10.0 / max(took, 1e-3)))
+        cpu = {"value": len(idx) / took, "unit": "jobs/s", "cores": cores, "kind": "port",
+               "sample": f"{len(idx)} evenly spaced jobs of the step ({oc[0]:.3e} c3/c4 points in "
+                         f"{took:.1f} s; oracle restatement of run_batch, probing a host-built "
+                         f"N=2000 r={args.r} table)"}
+
+    import collections
+    import shard
+    total_ms, tot = shard.merge(dist, "cuda", total_ms, {"jobs": n})
+    step_s = total_ms / args.steps / 1e3
+    peak, peak_kind = measured_peaks()
+    achieved = ctr.probes * PROBE_BYTES / (statistics.mean(per_ms) / 1e3) / 1e9
+    mix = collections.Counter(c for c, _, _ in units)
+    jmix = collections.Counter(jobs[i].cls for i in range(0, n, max(1, n // 100000)))
+    line = {"metric": METRIC_JOBS, "value": tot["jobs"] / step_s, "unit": "jobs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u128",
+            "data": "synthetic",
+            "config": {"workload": f"{len(units)} Stage-1 units {dict(sorted(mix.items()))} expanded "
+                                   f"into {n} reduced-T jobs (.bbj {file_bytes / 1e6:.1f} MB); xor "
+                                   f"table N={N} r={args.r} on device",
+                       "N": N, "r": args.r,
+                       "l2": "table %.1f GB, larger than L2" % (eng.table_info(tid).device_bytes / 1e9),
+                       "parallelism": f"replicas x{world}"},
+            "points_per_s": ctr.calls / step_s,
+            "counters": {"calls": ctr.calls, "gated": ctr.gated, "probes": ctr.probes, "hits": ctr.hits},
+            "jobs_by_class_sampled": dict(sorted(jmix.items())),
+            "exact_matches": len(sols),
+            "solutions": [s615.solution_line(s) for s in sols if s.kind == 0],
+            "units_path": {"ms_per_step": units_ms, "jobs_over_units_time": (total_ms / args.steps) / units_ms},
+            "host": {"expand_s": round(expand_s, 2), "fail_t": fail_t, "bbj_write_s": round(write_s, 2),
+                     "bbj_read_s": round(read_s, 2), "bbj_bytes": file_bytes},
+            "table_build_s": round(build_s, 2),
+            "e2e": {"value": n / e2e_s, "unit": "jobs/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": C.sizeof(s615.Counters) + len(h3) * C.sizeof(s615.Hit),
+                    "includes": ".bbj read + s615_run"},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs (burst)",
+                         "traffic": None, "algorithmic_bytes_per_launch": ctr.probes * PROBE_BYTES},
+            "cpu_baseline": cpu, "clocks": cl}
+    eng.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def run_serve(args, rank, world, local, dist):
     """Serving with four resident tables: requests of 50 units arrive as a
     Poisson stream (5,000 units/s); B uniform on [1M, 5M], classes mixed
@@ -746,6 +911,15 @@ def main():
         return run_mix(args, rank, world, local, dist)
     if args.workload == "serve":
         return run_serve(args, rank, world, local, dist)
+    if args.workload == "jobs":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "metric": METRIC_JOBS, "unavailable":
+                                  "fourcore_find_v4 (the reference's job runner) includes <gmpxx.h>, "
+                                  "which is not installed; the line's cpu_baseline is the oracle port"}),
+                      flush=True)
+            return 0
+        return run_jobs(args, rank, world, local, dist)
     if args.workload == "cls617":
         if args.impl == "reference":
             return run617_reference(args, rank)

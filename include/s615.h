@@ -96,8 +96,9 @@ typedef struct s615_table_info {
  * res_d = free1 (d), res_e = free2 (e, cls 5 only); lim is (B-1)/42.  cls 1:
  * find4 over T (make_cand mode 4); cls 2-4: one find3 row, c3 in
  * [least c with 3c^6 >= T, min(iroot6 T, lim)] (mode 3); cls 5: one gated
- * probe of key T (mode 2, k_find2 :233-252).  Jobs with an empty window are
- * dropped like run_batch drops them (:486). */
+ * probe of key T (mode 2, k_find2 :233-252).  A job with an empty window
+ * searches nothing, as run_batch drops it (:486); s615_unit_status reports
+ * class 1 and out-of-range T (cls 2-4: T = 0 or T >= 2^121) as dropped. */
 #define S615_CLS_617 7
 #define S615_CLS_617_FIND4 8
 #define S615_KIND_JOB 2

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <memory>
 #include <random>
+#include <thread>
 #include <vector>
 
 #include "engine.hpp"
@@ -500,37 +501,71 @@ int arena_get(s615_ctx* ctx, int k, size_t bytes, void** p) {
   return S615_OK;
 }
 
+// make_dev_unit over every unit (on several host threads for large batches),
+// the kept records compacted in unit order.  Returns the error of the
+// lowest-index unit that has one, as a sequential pass would.
+static int pack_units(const s615_unit* units, size_t n, std::unique_ptr<DevUnit[]>& out,
+                      size_t* n_out) {
+  out.reset(new DevUnit[std::max<size_t>(n, 1)]);
+  std::vector<uint8_t> keep(n);
+  const size_t hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  const size_t nt = n < (1u << 16) ? 1 : std::min(hw, (n + 65535) / 65536);
+  std::vector<int> err(nt, 0);
+  auto work = [&](size_t t) {
+    for (size_t i = n * t / nt, hi = n * (t + 1) / nt; i < hi; ++i) {
+      bool skip = false;
+      const int s = make_dev_unit(units[i], (u32)i, &out[i], &skip);
+      if (s) { err[t] = s; return; }
+      keep[i] = !skip;
+    }
+  };
+  if (nt == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> th;
+    for (size_t t = 0; t < nt; ++t) th.emplace_back(work, t);
+    for (auto& x : th) x.join();
+  }
+  for (size_t t = 0; t < nt; ++t)
+    if (err[t]) return err[t];
+  size_t k = 0;
+  for (size_t i = 0; i < n; ++i)
+    if (keep[i]) {
+      if (k != i) out[k] = out[i];
+      ++k;
+    }
+  *n_out = k;
+  return S615_OK;
+}
+
 int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
   b->host_items.clear();
-  std::vector<DevUnit> du;
-  du.reserve(n);
+  std::unique_ptr<DevUnit[]> dp;
+  size_t nd = 0;
+  if (const int s = pack_units(units, n, dp, &nd)) return s;
+  const DevUnit* du = dp.get();
   std::vector<u64> items617;   // the (6,1,7) kernel's items go after the others
-  for (size_t i = 0; i < n; ++i) {
-    DevUnit d;
-    bool skip = false;
-    const int s = make_dev_unit(units[i], (u32)i, &d, &skip);
-    if (s) return s;
-    if (skip) continue;
-    // classes 1 and 7 (c4 windows) run in the second kernel
-    unit_items(d, (u32)du.size(),
+  for (size_t k = 0; k < nd; ++k) {
+    const DevUnit& d = du[k];
+    // classes 1, 7 and 8 (c4 windows) run in the second kernel
+    unit_items(d, (u32)k,
                (d.cls == S615_CLS_617 || d.cls == 1 || d.cls == S615_CLS_617_FIND4) ? items617
                                                                                 : b->host_items);
-    du.push_back(d);
   }
   // heaviest first: a candidate's first rows (smallest d) have the largest T
   // and windows, so every candidate's chunk 0 goes out before any chunk 1
   std::stable_sort(items617.begin(), items617.end(),
                    [](u64 a, u64 b) { return item_chunk(a) < item_chunk(b); });
-  b->n_units = du.size();
+  b->n_units = nd;
   b->n_main = b->host_items.size();
   b->host_items.insert(b->host_items.end(), items617.begin(), items617.end());
   b->n_items = b->host_items.size();
   int s = 0;
   void* p = nullptr;
-  if (!b->d_units || du.size() > b->cap_units) {
+  if (!b->d_units || nd > b->cap_units) {
     dev_free(ctx, b->d_units, b->cap_units * sizeof(DevUnit));
     b->d_units = nullptr;
-    const size_t cap = std::max<size_t>(du.size(), 1);
+    const size_t cap = std::max<size_t>(nd, 1);
     if ((s = dev_alloc(ctx, &p, cap * sizeof(DevUnit)))) { b->cap_units = 0; return s; }
     b->d_units = static_cast<DevUnit*>(p);
     b->cap_units = cap;
@@ -553,8 +588,8 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
     b->d_hits = static_cast<s615_hit*>(p);
     b->hit_cap = 1u << 20;
   }
-  if (!du.empty())
-    S615_CU(cudaMemcpy(b->d_units, du.data(), du.size() * sizeof(DevUnit), cudaMemcpyHostToDevice));
+  if (nd)
+    S615_CU(cudaMemcpy(b->d_units, du, nd * sizeof(DevUnit), cudaMemcpyHostToDevice));
   if (b->n_items)
     S615_CU(cudaMemcpy(b->d_items, b->host_items.data(), b->n_items * sizeof(u64), cudaMemcpyHostToDevice));
   return S615_OK;

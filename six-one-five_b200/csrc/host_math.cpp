@@ -539,8 +539,9 @@ static int make_dev_unit8(const s615_unit& in, DevUnit* out) {
 // kind 2: one reduced-T job of fourcore_find_v4 (job_from_bin :598-608 with
 // make_cand :401-425).  lim defaults to (B-1)/42 and stays <= (kMaxB-1)/42,
 // so 3 lim^6 < 2^121 and 4 lim^6 < 2^122: a find3 job with T >= 2^121 or a
-// find4 job with T >= 2^122 has an empty window, dropped like run_batch drops
-// it (:486).  cls 2-4: a one-row unit (kClsJobRow) whose row value is T;
+// find4 job with T >= 2^122 has an empty window and is dropped, as run_batch
+// drops it (:486); other empty find3 windows come out empty on the device.
+// cls 2-4: a one-row unit (kClsJobRow) whose row value is T;
 // cls 5 (find2): the same row with W = T + 1 and the window [1, 1], so the
 // gate tests W - 1^6 = T and the key is T mod 2^64.  When T + 1 >= 2^121, W is
 // T + 1 reduced mod 15561 * 2^64 (15561 = 9 * 7 * 13 * 19), which keeps the key
@@ -572,9 +573,8 @@ static int make_dev_job(const s615_unit& in, DevUnit* out, bool* skip) {
     if (W == 0) W = M;
     out->w = 1;
   } else {
+    // the device row computes the c3 window; an empty one searches nothing
     if (T == 0 || (T >> 121) != 0) { *skip = true; return S615_OK; }
-    const u32 hi = std::min(iroot6_exact(T), (u32)lim);
-    if (hi < 1 || least_c_k(T, 3) > hi) { *skip = true; return S615_OK; }
     W = T;
   }
   out->cls = kClsJobRow;

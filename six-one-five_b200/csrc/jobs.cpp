@@ -6,6 +6,7 @@
 // (:164-205) makes them from Stage-1 units; the binary file layout is
 // fourcore_job_bin.hpp:16-46 and the text one load_jobs_but (:125-145).  Jobs
 // enter the engine as kind 2 units (include/s615.h).
+#include <algorithm>
 #include <cctype>
 #include <cstdio>
 #include <cstring>
@@ -154,11 +155,18 @@ int s615_jobs_next(s615_jobs_file* f, s615_unit* out, size_t cap, size_t* n) {
   if (!f || !n || (cap && !out)) return S615_E_ARG;
   size_t k = 0;
   if (f->info.binary) {
-    uint8_t r[kBbjRecord];
-    while (k < cap && std::fread(r, 1, sizeof r, f->fp) == sizeof r) {
-      // JobBinRec {u8 cls, 3 pad, u32 B, u, free1, free2, u64 T_lo, T_hi}
-      out[k++] = make_job(r[0], get<uint32_t>(r + 4), get<uint32_t>(r + 8), get<uint32_t>(r + 12),
-                          get<uint32_t>(r + 16), get<uint64_t>(r + 20), get<uint64_t>(r + 28));
+    std::vector<uint8_t> buf;
+    while (k < cap) {   // whole blocks of records, decoded in place
+      const size_t want = std::min<size_t>(cap - k, 1u << 16);
+      buf.resize(want * kBbjRecord);
+      const size_t got = std::fread(buf.data(), kBbjRecord, want, f->fp);
+      for (size_t i = 0; i < got; ++i) {
+        // JobBinRec {u8 cls, 3 pad, u32 B, u, free1, free2, u64 T_lo, T_hi}
+        const uint8_t* r = buf.data() + i * kBbjRecord;
+        out[k++] = make_job(r[0], get<uint32_t>(r + 4), get<uint32_t>(r + 8), get<uint32_t>(r + 12),
+                            get<uint32_t>(r + 16), get<uint64_t>(r + 20), get<uint64_t>(r + 28));
+      }
+      if (got < want) break;
     }
   } else {
     char line[256];

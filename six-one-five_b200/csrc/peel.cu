@@ -95,7 +95,7 @@ __device__ __forceinline__ u32 pow6_mod512(u32 x) {
 __device__ __forceinline__ u32 entry(u32 di, u32 r, u32 k) { return (di << 24) | (r << 18) | k; }
 
 struct ItemCtx {
-  u32 cls, unit_id, r0, mod, j0, f, u0;   // u0: first unit of a job item
+  u32 cls, unit_id, r0, mod, j0, f;   // job items: unit_id = index of the first unit
 };
 
 // Probe the ring entries [head, head+cnt) (one per lane).
@@ -124,8 +124,8 @@ __device__ __forceinline__ void probe_batch(const PeelParams& P, const WarpSmem&
       h.unit = I.unit_id; h.a = 0; h.b = 0; h.c4 = 0;
       if (I.cls == 5) { h.d = (u32)x; h.e = rowval; }
       else { h.d = rowval; h.e = (u32)x; }
-      if (I.cls == kClsJobRow) {   // row r is unit u0 + r (hits are rare: one load)
-        h.unit = P.units[I.u0 + r].id;
+      if (I.cls == kClsJobRow) {   // row r is unit unit_id + r (hits are rare: one load)
+        h.unit = P.units[I.unit_id + r].id;
         h.d = 0;
       }
       h.fp = key;
@@ -179,8 +179,7 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
     const DevUnit* U = P.units + item_unit(packed);
     ItemCtx I;
     I.cls = U->cls;
-    I.unit_id = U->id;
-    I.u0 = item_unit(packed);
+    I.unit_id = I.cls == kClsJobRow ? item_unit(packed) : U->id;
     I.f = U->f;
     u32 nrows;
     if (I.cls == kClsJobRow) {   // job_count consecutive one-row units; row r is unit u0 + r
@@ -196,13 +195,12 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
       I.j0 = jmin + item_chunk(packed) * kRows;
       nrows = min(kRows, jend - I.j0);
     }
-    const u128 base = ((u128)U->base_hi << 64) | U->base_lo;
-    const u32 lim = U->lim;
     u32 head = 0, qlen = 0;
     __syncwarp();
 
     if (I.cls == 5) {
       // ---- cls5 rows: V, D and the residues of V (two rows per lane) ----
+      const u128 base = ((u128)U->base_hi << 64) | U->base_lo;
       for (u32 r = lane; r < nrows; r += 32) {
         const u64 x = 14ull * ((u64)I.r0 + (u64)I.mod * (I.j0 + r));
         const u128 x3 = (u128)(x * x) * x;           // (14e)^3 < 2^78
@@ -311,12 +309,12 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
       const bool job = I.cls == kClsJobRow;
       const bool find2 = job && U->w != 0;
       for (u32 r = lane; r < nrows; r += 32) {
-        const DevUnit* Ur = job ? U + r : U;
+        const DevUnit* Ur = job ? U + r : U;   // a job item's row r is its own unit
         const u64 x = (u64)I.f * ((u64)I.r0 + (u64)I.mod * (I.j0 + r));
         const u128 x3 = (u128)(x * x) * x;
-        const u128 Rm = (job ? (((u128)Ur->base_hi << 64) | Ur->base_lo) : base) - x3 * x3;
+        const u128 Rm = (((u128)Ur->base_hi << 64) | Ur->base_lo) - x3 * x3;
         const u128 T = ((Rm >> 6) * inv21) & ((~(u128)0) >> 6);  // T mod 2^122
-        const u32 rlim = job ? Ur->lim : lim;
+        const u32 rlim = Ur->lim;
         RowRec R;
         R.wlo = (u64)T; R.whi = (u64)(T >> 64);
         R.a = 0; R.b = 0;
@@ -344,39 +342,30 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
         W.rows[r] = R;
       }
       __syncwarp();
-      if (find2) {   // one column per row: lane r takes row r
-        for (u32 r0 = 0; r0 < nrows; r0 += 32) {
-          const u32 r = r0 + lane;
-          u32 m = 0;
-          if (r < nrows) {
-            const RowRec& R = W.rows[r];
-            if (R.b & kLenMask) m = (R.b >> 28) & gate_word(s_pat3, R, 1, 1, 1, 1) & 1u;
-          }
-          my_probes += m;
-          push_bits(P, W, m, 0, r & 63u, 0, head, qlen, I, lane);
-        }
-        __syncwarp();
-        probe_batch(P, W, head, qlen, I, lane);
-        __syncwarp();
-        continue;
-      }
-      for (u32 r = 0; r < nrows; ++r) {
-        const RowRec& R = W.rows[r];
-        const u32 len = R.b & kLenMask;
-        if (len == 0) continue;
-        const u32 m8 = (R.b >> 28) * 0x11111111u;
-        const u32 ntiles = (len + 1023u) / 1024u;
-        for (u32 wt = 0; wt < ntiles; ++wt) {
-          const u32 kbase = (wt * 32u + lane) * 32u;
-          u32 m = 0;
+      // Sieve steps: a row's window in tiles of 1024 columns (lane = 32
+      // columns), or for find2 items 32 one-column rows at once (lane = row).
+      u32 r = 0, wt = 0;
+      while (r < nrows) {
+        const u32 rr = find2 ? r + lane : r;
+        const u32 kbase = find2 ? 0u : (wt * 32u + lane) * 32u;
+        u32 m = 0, len = 0;
+        if (rr < nrows) {
+          const RowRec& R = W.rows[rr];
+          len = R.b & kLenMask;
           if (kbase < len) {
             const u32 xs = R.a + kbase;
-            m = m8 & gate_word(s_pat3, R, xs % 9, xs % 7, xs % 13, xs % 19);
+            m = ((R.b >> 28) * 0x11111111u) & gate_word(s_pat3, R, xs % 9, xs % 7, xs % 13, xs % 19);
             const u32 n = len - kbase;
             if (n < 32u) m &= (1u << n) - 1u;
           }
-          my_probes += __popc(m);
-          push_bits(P, W, m, 0, r, kbase, head, qlen, I, lane);
+        }
+        my_probes += __popc(m);
+        push_bits(P, W, m, 0, rr & 63u, kbase, head, qlen, I, lane);
+        if (find2) {
+          r += 32;
+        } else if (++wt >= (len + 1023u) / 1024u) {   // len is the same in every lane here
+          wt = 0;
+          ++r;
         }
       }
       __syncwarp();

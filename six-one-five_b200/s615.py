@@ -283,6 +283,32 @@ def expand_unit(B: int, u: int, cls: int):
     return arr, n.value, fail.value
 
 
+def expand_units(units):
+    """s615_expand_unit over (cls, B, u) Stage-1 units, concatenated in unit
+    order: (jobs array, n, failT)."""
+    chunks, n, fails = [], 0, 0
+    sz = C.sizeof(Unit)
+    unit = Unit()
+    cnt, fail = C.c_size_t(0), C.c_uint64(0)
+    buf = (Unit * 1)()
+    for c, B, u in units:
+        unit.cls, unit.B, unit.u = c, B, u
+        st = lib().s615_expand_unit(C.byref(unit), C.cast(buf, C.c_void_p), len(buf), C.byref(cnt),
+                                    C.byref(fail))
+        if st == -9:
+            buf = (Unit * (cnt.value + cnt.value // 2))()
+            st = lib().s615_expand_unit(C.byref(unit), C.cast(buf, C.c_void_p), len(buf), C.byref(cnt),
+                                        C.byref(fail))
+        _check(st, "expand_unit")
+        chunks.append(C.string_at(C.addressof(buf), cnt.value * sz))
+        n += cnt.value
+        fails += fail.value
+    out = (Unit * max(n, 1))()
+    if n:
+        C.memmove(out, b"".join(chunks), n * sz)
+    return out, n, fails
+
+
 def jobs_write(path: str, jobs, n: int) -> None:
     """s615_jobs_write: a .bbj (binary) or text job file."""
     _check(lib().s615_jobs_write(path.encode(), C.cast(jobs, C.c_void_p), n), "jobs_write")
@@ -295,6 +321,15 @@ def jobs_read(path: str, chunk: int = 1 << 16):
     _check(lib().s615_jobs_open(path.encode(), C.byref(f), C.byref(info)), "jobs_open")
     parts, n = [], 0
     try:
+        if info.binary and info.n_jobs:   # the header's count in one read, then anything after it
+            first = (Unit * info.n_jobs)()
+            k = C.c_size_t(0)
+            _check(lib().s615_jobs_next(f, C.cast(first, C.c_void_p), info.n_jobs, C.byref(k)),
+                   "jobs_next")
+            n = k.value
+            if n < info.n_jobs:
+                return first, n, info
+            parts.append(first)
         while True:
             buf = (Unit * chunk)()
             k = C.c_size_t(0)
@@ -305,9 +340,14 @@ def jobs_read(path: str, chunk: int = 1 << 16):
             n += k.value
     finally:
         lib().s615_jobs_close(f, C.byref(info))
+    if len(parts) == 1 and not isinstance(parts[0], bytes):
+        return parts[0], n, info
     out = (Unit * max(n, 1))()
-    if n:
-        C.memmove(out, b"".join(parts), n * C.sizeof(Unit))
+    off = 0
+    for p in parts:
+        size = len(p) if isinstance(p, bytes) else C.sizeof(p)
+        C.memmove(C.byref(out, off), p, size)
+        off += size
     return out, n, info
 
 
