@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-find4", action="store_true", help="cls617: skip the classes 1-4 pass")
+    ap.add_argument("--shards", type=int, default=1,
+                    help="cls5: a pair-space shard set of S tables (S >= 2) instead of one table")
+    ap.add_argument("--layout", default="auto", choices=["auto", "wide", "packed"])
     ap.add_argument("--workload", default="cls5", choices=["cls5", "cls617", "mix", "serve", "jobs"])
     ap.add_argument("--units", type=int, default=0, help="mix: units per step (default 200,000)")
     ap.add_argument("--seconds", type=float, default=10.0, help="serve: seconds of arrivals")
@@ -938,10 +941,14 @@ def main():
     lo, hi = shard.rank_band(args.band_lo, args.band_width, rank)
     N = args.N or shard.table_N(args.band_lo, args.band_width, world)
     eng = s615.Engine(local)
+    layout = {"auto": s615.LAYOUT_AUTO, "wide": s615.LAYOUT_WIDE, "packed": s615.LAYOUT_PACKED}[args.layout]
     t0 = time.perf_counter()
-    tid = eng.build_table(N, args.r)
+    if args.shards > 1:
+        tid = eng.build_table_sharded(N, args.r, args.shards, layout)
+    else:
+        tid = eng.build_table(N, args.r, layout)
     build_s = time.perf_counter() - t0
-    log(f"rank {rank}: table N={N} r={args.r} built in {build_s:.1f} s")
+    log(f"rank {rank}: table N={N} r={args.r} shards={args.shards} built in {build_s:.1f} s")
     units = band_units(lo, hi - 1)   # B in [lo, hi): bands of ranks do not overlap
     log(f"rank {rank}: {len(units)} units in [{lo}, {hi})")
     plants = W.plants(N_PLANTS, 1000 + rank, lo, hi, N)
@@ -1072,7 +1079,7 @@ def main():
         log(f"serving: p50 {serve['p50_ms']:.1f} ms, p99 {serve['p99_ms']:.1f} ms per unit")
 
     cpu = None
-    if not args.no_cpu_baseline and rank == 0 and world == 1:
+    if not args.no_cpu_baseline and rank == 0 and world == 1 and args.shards == 1:
         import orc
         hb, pk = eng.export_table(tid)
         ot = orc.Table.from_memory(hb, pk)
@@ -1085,7 +1092,9 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64", "data": "synthetic",
         "config": {"workload": f"cls5 band B in [{lo}, {hi}) per rank: {len(units)} Stage-1 units + "
-                               f"{N_PLANTS} plants; xor table N={N} r={args.r} built on device",
+                               f"{N_PLANTS} plants; xor table N={N} r={args.r} built on device"
+                               + (f" as {args.shards} pair-space shards" if args.shards > 1 else ""),
+                   "shards": args.shards,
                    "units_per_rank": n, "N": N, "r": args.r,
                    "l2": "inputs larger than L2 (table %.1f GB)" % (eng.table_info(tid).device_bytes / 1e9),
                    "parallelism": f"replicas-by-band x{world}"},

@@ -184,6 +184,22 @@ int s615_build_table_keys(s615_ctx* ctx, const uint64_t* keys, size_t n, int r,
                           uint64_t base_seed, int layout, int* table_id);
 /* xor_save_file (fourcore_xor_store.hpp:126-143): header + packed cells. */
 int s615_save_table(s615_ctx* ctx, int table_id, const char* path);
+/* Pair-space shard sets (spike/ribbon/shard.hpp:19-24, the shard fields of
+ * store_header.hpp:33-35): shard s of S is an xor table over the pair keys k
+ * with mix64(k + 0x615615615615615) % S == s (shard_mode 0); a probe of k
+ * queries only its own shard, so a set answers exactly like one table over
+ * all keys (no false negatives, FPR 2^-r).  Each shard is built on the device
+ * with scratch for its own keys only, so sets reach N that one build cannot
+ * (the single-table cap is N <= 120,000).  A set's header has shard_count S,
+ * the key and cell totals and the routing seed in mix_seed; 2 <= S <= 64.
+ * s615_load_table refuses a file that is one shard of a set;
+ * s615_load_table_shards takes the S files in shard order; s615_save_table
+ * and s615_export_table refuse a set, s615_save_table_shard writes one shard's
+ * file.  Every run and query entry point takes a set's table id. */
+int s615_build_table_sharded(s615_ctx* ctx, int N, int r, int shards, int layout, int* table_id);
+int s615_load_table_shards(s615_ctx* ctx, const char* const* paths, int n, int expected_N,
+                           int layout, int* table_id);
+int s615_save_table_shard(s615_ctx* ctx, int table_id, int shard, const char* path);
 /* The packed file bytes (after the 64-byte header) into a host buffer of
  * cap >= packed_bytes(m_cells, r) bytes; the in-memory form of the
  * reference's XorFilter::packed. *len receives the byte count. */

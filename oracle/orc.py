@@ -88,6 +88,9 @@ _SIG = {
     "orc_packed_bytes": (C.c_size_t, [C.c_uint64, C.c_uint32]),
     "orc_build_xor": (_P, [_P, C.c_size_t, C.c_int, C.c_uint64, C.c_int]),
     "orc_build_pairs": (_P, [C.c_int, C.c_int]),
+    "orc_build_pairs_shard": (_P, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64]),
+    "orc_shard_set": (_P, [_P, C.c_int, C.c_uint64]),
+    "orc_shard_of": (C.c_uint32, [C.c_uint64, C.c_uint64, C.c_uint32]),
     "orc_load": (_P, [C.c_char_p, C.c_int]),
     "orc_from_memory": (_P, [C.POINTER(OrcHeader), _P, C.c_size_t]),
     "orc_save": (C.c_int, [_P, C.c_char_p]),
@@ -140,6 +143,9 @@ def _ptr(a: np.ndarray):
     return C.c_void_p(a.ctypes.data)
 
 
+SHARD_SEED = 0x615615615615615   # the routing seed of pair-space shards
+
+
 class Table:
     def __init__(self, handle):
         if not handle:
@@ -149,6 +155,19 @@ class Table:
     @classmethod
     def build_pairs(cls, N: int, r: int) -> "Table":
         return cls(lib().orc_build_pairs(N, r))
+
+    @classmethod
+    def build_pairs_shard(cls, N: int, r: int, S: int, s: int, seed: int = SHARD_SEED) -> "Table":
+        """Shard s of S: the pair keys with mix64(key + seed) % S == s."""
+        return cls(lib().orc_build_pairs_shard(N, r, S, s, seed))
+
+    @classmethod
+    def shard_set(cls, parts, seed: int = SHARD_SEED) -> "Table":
+        """A table whose probes go to parts[mix64(key + seed) % S] (parts stay referenced)."""
+        arr = (C.c_void_p * len(parts))(*[p.h for p in parts])
+        t = cls(lib().orc_shard_set(arr, len(parts), seed))
+        t.parts = list(parts)
+        return t
 
     @classmethod
     def build_keys(cls, keys, r: int, base_seed: int = 0x615615615615615, tries: int = 64):
@@ -195,6 +214,11 @@ class Table:
                 lib().orc_free(self.h)
         except Exception:
             pass
+
+
+def shard_of(key: int, S: int, seed: int = SHARD_SEED) -> int:
+    """shard_of_key (spike/ribbon/shard.hpp:19-24)."""
+    return lib().orc_shard_of(key, seed, S)
 
 
 def pack_unit(B: int, u: int):

@@ -288,6 +288,9 @@ void hashes3(u64 h, u64 block, u64 out[3]) {
 struct orc_table {
   orc_header hdr;
   std::vector<uint8_t> packed;
+  // a shard set: the probe of key k goes to parts[mix64(k + shard_seed) % S]
+  std::vector<const orc_table*> parts;
+  u64 shard_seed = 0;
 };
 
 namespace {
@@ -351,7 +354,12 @@ bool construct(const std::vector<u64>& keys, u32 r, u64 seed, orc_table& out) {
   return true;
 }
 
+// shard_of_key (spike/ribbon/shard.hpp:19-24): mix64_seeded(key, seed) % S.
+u32 shard_of(u64 key, u64 seed, u32 S) { return S <= 1 ? 0u : (u32)(mix64(key + seed) % S); }
+
 bool might_contain(const orc_table& t, u64 key) {  // xor_filter.hpp:472-483
+  if (!t.parts.empty())   // residue-steered probe: one query, in the key's own shard
+    return might_contain(*t.parts[shard_of(key, t.shard_seed, (u32)t.parts.size())], key);
   if (t.hdr.n_keys == 0) return false;
   if (t.packed.empty() || t.hdr.m_cells < 3) return false;
   const u64 block = t.hdr.m_cells / 3;
@@ -573,6 +581,55 @@ orc_table* orc_build_pairs(int N, int r) {
   return nullptr;
 }
 
+// Shard s of S of the pair-key store: xor_build_pairs over the keys with
+// shard_of_key(key, seed, S) == s; the header records shard_count, shard_index
+// and shard_mode 0 (key % S after the mix, store_header.hpp:19-21, 33-35).
+orc_table* orc_build_pairs_shard(int N, int r, int S, int s, uint64_t seed) {
+  std::vector<u64> pw6((size_t)N + 1, 0);
+  for (int x = 1; x <= N; ++x) { const u64 x2 = (u64)x * (u64)x; pw6[x] = x2 * x2 * x2; }
+  std::vector<u64> keys;
+  for (int i = 1; i <= N; ++i)
+    for (int j = i; j <= N; ++j) {
+      const u64 k = pw6[i] + pw6[j];
+      if (shard_of(k, seed, (u32)S) == (u32)s) keys.push_back(k);
+    }
+  for (int o = 0; o < 4; ++o) {
+    orc_table* t = orc_build_xor(keys.data(), keys.size(), r, kSeedBase + (u64)o * kPhi, 64);
+    if (t) {
+      t->hdr.N = (u32)N;
+      t->hdr.shard_count = (u32)S;
+      t->hdr.shard_index = (u32)s;
+      t->hdr.shard_mode = 0;
+      return t;
+    }
+  }
+  return nullptr;
+}
+
+// A shard set over parts[0..S) (not owned; each part's header says which
+// shard it is).  Null unless the parts are shards 0..S-1 of one S.
+orc_table* orc_shard_set(const orc_table* const* parts, int S, uint64_t seed) {
+  if (S < 1) return nullptr;
+  auto* t = new orc_table();
+  for (int s = 0; s < S; ++s) {
+    const orc_header& h = parts[s]->hdr;
+    if ((int)h.shard_count != S || (int)h.shard_index != s || h.shard_mode != 0) {
+      delete t;
+      return nullptr;
+    }
+    t->parts.push_back(parts[s]);
+    t->hdr.n_keys += h.n_keys;
+    t->hdr.m_cells += h.m_cells;
+  }
+  t->hdr.magic = kMagic; t->hdr.version = 2; t->hdr.kind = 1;
+  t->hdr.r = parts[0]->hdr.r; t->hdr.N = parts[0]->hdr.N;
+  t->hdr.shard_count = (u32)S;
+  t->shard_seed = seed;
+  return t;
+}
+
+uint32_t orc_shard_of(uint64_t key, uint64_t seed, uint32_t S) { return shard_of(key, seed, S); }
+
 orc_table* orc_load(const char* path, int expected_N) {  // fourcore_xor_store.hpp:147-181
   FILE* f = std::fopen(path, "rb");
   if (!f) return nullptr;
@@ -620,7 +677,7 @@ void orc_query(const orc_table* t, const uint64_t* keys, size_t n, uint8_t* out)
   for (long long i = 0; i < (long long)n; ++i) out[i] = might_contain(*t, keys[i]) ? 1 : 0;
 }
 int orc_fpr_smoke(const orc_table* t) {  // fourcore_xor_store.hpp:54-65
-  if (t->packed.empty() || t->hdr.m_cells < 3 || t->hdr.r == 0) return -1;
+  if (t->parts.empty() && (t->packed.empty() || t->hdr.m_cells < 3 || t->hdr.r == 0)) return -1;
   int hits = 0;
   u64 x = 0x123456789abcdef0ULL;
   for (int i = 0; i < 200000; ++i) { x = x * kPhi + 1; if (might_contain(*t, x)) ++hits; }

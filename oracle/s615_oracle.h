@@ -73,6 +73,11 @@ orc_table* orc_build_xor(const uint64_t* keys, size_t n, int r, uint64_t base_se
 /* xor_build_pairs(N, r) (fourcore_xor_store.hpp:67-119). */
 orc_table* orc_build_pairs(int N, int r);
 /* xor_load_file (fourcore_xor_store.hpp:147-181); expected_N<=0 accepts any. */
+/* Pair-space shards (spike/ribbon/shard.hpp, store_header.hpp shard fields):
+ * shard s of S holds the pair keys with mix64(key + seed) % S == s. */
+orc_table* orc_build_pairs_shard(int N, int r, int S, int s, uint64_t seed);
+orc_table* orc_shard_set(const orc_table* const* parts, int S, uint64_t seed);
+uint32_t orc_shard_of(uint64_t key, uint64_t seed, uint32_t S);
 orc_table* orc_load(const char* path, int expected_N);
 orc_table* orc_from_memory(const orc_header* h, const uint8_t* bytes, size_t len);
 int orc_save(const orc_table* t, const char* path);

@@ -53,9 +53,54 @@ bool gate_product_matches();
 namespace {
 
 void free_table(s615_ctx* ctx, DevTable& t) {
+  for (DevTable& p : t.parts) free_table(ctx, p);
+  t.parts.clear();
+  dev_free(ctx, t.d_views, t.d_views ? sizeof(TableView) * 64 : 0);
+  t.d_views = nullptr;
   dev_free(ctx, t.d_cells, t.bytes);
   t.d_cells = nullptr;
   t.bytes = 0;
+}
+
+// Device bytes of a table or of every shard of a set.
+size_t table_bytes(const DevTable& t) {
+  size_t b = t.bytes;
+  for (const DevTable& p : t.parts) b += p.bytes;
+  return b;
+}
+
+// A shard set over parts (shards 0..S-1 of one N and r): header totals, the
+// parts' views uploaded for the routed probe.
+int make_set(s615_ctx* ctx, std::vector<DevTable>&& parts, DevTable* out) {
+  const u32 S = (u32)parts.size();
+  DevTable t;
+  t.hdr = parts[0].hdr;
+  t.hdr.n_keys = 0;
+  t.hdr.m_cells = 0;
+  t.hdr.mix_seed = kShardSeed;   // a set's header carries the routing seed
+  t.hdr.shard_count = S;
+  t.hdr.shard_index = 0;
+  t.hdr.shard_mode = 0;
+  for (const DevTable& p : parts) {
+    t.hdr.n_keys += p.hdr.n_keys;
+    t.hdr.m_cells += p.hdr.m_cells;
+  }
+  t.layout = parts[0].layout;
+  t.cell_bytes = parts[0].cell_bytes;
+  t.parts = std::move(parts);
+  std::vector<TableView> views;
+  for (const DevTable& p : t.parts) views.push_back(view_of(p));
+  void* d = nullptr;
+  int s = dev_alloc(ctx, &d, sizeof(TableView) * 64);   // S <= 64
+  if (s) { free_table(ctx, t); return s; }
+  t.d_views = d;
+  if (cudaMemcpy(d, views.data(), views.size() * sizeof(TableView), cudaMemcpyHostToDevice) !=
+      cudaSuccess) {
+    free_table(ctx, t);
+    return S615_E_DEVICE;
+  }
+  *out = std::move(t);
+  return S615_OK;
 }
 
 DevTable* find_table(s615_ctx* ctx, int id) {
@@ -207,7 +252,7 @@ int s615_get_table_info(s615_ctx* ctx, int id, s615_table_info* info) {
   info->hdr = t->hdr;
   info->layout = t->layout;
   info->cell_bytes = t->cell_bytes;
-  info->device_bytes = t->bytes;
+  info->device_bytes = table_bytes(*t);
   return S615_OK;
 }
 
@@ -264,7 +309,7 @@ int s615_fpr_smoke(s615_ctx* ctx, int id, int* hits) {
   DevTable* t = find_table(ctx, id);
   if (!t) return S615_E_NOTABLE;
   *hits = 200000;
-  if (t->hdr.m_cells < 3 || t->hdr.r == 0 || !t->d_cells) return S615_OK;
+  if (t->parts.empty() && (t->hdr.m_cells < 3 || t->hdr.r == 0 || !t->d_cells)) return S615_OK;
   const size_t n = 200000;
   std::vector<u64> keys(n);
   u64 x = 0x123456789abcdef0ULL;
@@ -286,13 +331,11 @@ static int smoke_table(s615_ctx* ctx, int id) {
   return hits > 16 ? S615_E_FPR_SMOKE : S615_OK;
 }
 
-int s615_load_table(s615_ctx* ctx, const char* path, int expected_N, int layout, int* table_id) {
-  if (!ctx || !path) return S615_E_ARG;
-  if (serving_blocks(ctx)) return S615_E_BUSY;
-  cudaSetDevice(ctx->device);
+// Read one table file into HBM (header checks, streamed upload, layout).
+static int load_part(s615_ctx* ctx, const char* path, int expected_N, int layout, DevTable* out) {
   FILE* f = std::fopen(path, "rb");
   if (!f) return S615_E_IO;
-  DevTable t;
+  DevTable& t = *out;
   if (std::fread(&t.hdr, sizeof t.hdr, 1, f) != 1) { std::fclose(f); return S615_E_IO; }
   if (!header_ok(t.hdr)) { std::fclose(f); return S615_E_FORMAT; }
   if (expected_N > 0 && (int)t.hdr.N != expected_N) { std::fclose(f); return S615_E_N_MISMATCH; }
@@ -328,9 +371,54 @@ int s615_load_table(s615_ctx* ctx, const char* path, int expected_N, int layout,
   std::fclose(f);
   for (int i = 0; i < 2; ++i) { if (pin[i]) cudaFreeHost(pin[i]); cudaEventDestroy(ev[i]); }
   if (!ok) { dev_free(ctx, d, alloc); return s ? s : S615_E_OOM; }
-  if ((s = finish_upload(ctx, t, d, alloc, lay, cell_bytes))) return s;
+  return finish_upload(ctx, t, d, alloc, lay, cell_bytes);
+}
+
+int s615_load_table(s615_ctx* ctx, const char* path, int expected_N, int layout, int* table_id) {
+  if (!ctx || !path) return S615_E_ARG;
+  if (serving_blocks(ctx)) return S615_E_BUSY;
+  cudaSetDevice(ctx->device);
+  DevTable t;
+  int s = load_part(ctx, path, expected_N, layout, &t);
+  if (s) return s;
+  if (t.hdr.shard_count != 1) { free_table(ctx, t); return S615_E_FORMAT; }   // one shard of a set
   int id = 0;
   add_table(ctx, t, &id);
+  if ((s = smoke_table(ctx, id))) { s615_free_table(ctx, id); return s; }
+  if (table_id) *table_id = id;
+  return S615_OK;
+}
+
+int s615_load_table_shards(s615_ctx* ctx, const char* const* paths, int n, int expected_N,
+                           int layout, int* table_id) {
+  if (!ctx || !paths || n < 2 || n > 64) return S615_E_ARG;
+  if (serving_blocks(ctx)) return S615_E_BUSY;
+  cudaSetDevice(ctx->device);
+  std::vector<DevTable> parts;
+  int s = S615_OK;
+  for (int k = 0; k < n && !s; ++k) {
+    DevTable t;
+    if (!paths[k]) { s = S615_E_ARG; break; }
+    s = load_part(ctx, paths[k], expected_N, layout, &t);
+    if (s) break;
+    // shard k of n, mode key % S, and one N and r for the whole set
+    const s615_header& h = t.hdr;
+    if ((int)h.shard_count != n || (int)h.shard_index != k || h.shard_mode != 0 ||
+        (k && (h.N != parts[0].hdr.N || h.r != parts[0].hdr.r))) {
+      free_table(ctx, t);
+      s = S615_E_FORMAT;
+      break;
+    }
+    parts.push_back(std::move(t));
+  }
+  if (s) {
+    for (DevTable& p : parts) free_table(ctx, p);
+    return s;
+  }
+  DevTable set;
+  if ((s = make_set(ctx, std::move(parts), &set))) return s;
+  int id = 0;
+  add_table(ctx, std::move(set), &id);
   if ((s = smoke_table(ctx, id))) { s615_free_table(ctx, id); return s; }
   if (table_id) *table_id = id;
   return S615_OK;
@@ -361,6 +449,7 @@ int s615_export_table(s615_ctx* ctx, int id, s615_header* hdr, uint8_t* buf, siz
   if (!ctx) return S615_E_ARG;
   DevTable* t = find_table(ctx, id);
   if (!t) return S615_E_NOTABLE;
+  if (!t->parts.empty()) return S615_E_ARG;   // a set: export or save its shards one by one
   cudaSetDevice(ctx->device);
   const u64 n = packed_bytes(t->hdr.m_cells, t->hdr.r);
   if (hdr) *hdr = t->hdr;
@@ -370,11 +459,28 @@ int s615_export_table(s615_ctx* ctx, int id, s615_header* hdr, uint8_t* buf, siz
   return export_packed(ctx, *t, buf, n);
 }
 
+static int save_part(s615_ctx* ctx, const DevTable* t, const char* path);
+
 int s615_save_table(s615_ctx* ctx, int id, const char* path) {
   if (!ctx || !path) return S615_E_ARG;
   DevTable* t = find_table(ctx, id);
   if (!t) return S615_E_NOTABLE;
+  if (!t->parts.empty()) return S615_E_ARG;
   cudaSetDevice(ctx->device);
+  return save_part(ctx, t, path);
+}
+
+int s615_save_table_shard(s615_ctx* ctx, int id, int shard, const char* path) {
+  if (!ctx || !path) return S615_E_ARG;
+  DevTable* t = find_table(ctx, id);
+  if (!t) return S615_E_NOTABLE;
+  if (shard < 0 || shard >= (int)t->parts.size()) return S615_E_ARG;
+  cudaSetDevice(ctx->device);
+  return save_part(ctx, &t->parts[(size_t)shard], path);
+}
+
+// One table's file: its header, then the packed cells.
+static int save_part(s615_ctx* ctx, const DevTable* t, const char* path) {
   const u64 len = packed_bytes(t->hdr.m_cells, t->hdr.r);
   std::vector<u8> host(len);
   const int s = export_packed(ctx, *t, host.data(), len);
@@ -409,6 +515,44 @@ int s615_build_table(s615_ctx* ctx, int N, int r, int layout, int* table_id) {
   if (s) return s;
   int id = 0;
   add_table(ctx, t, &id);
+  if ((s = smoke_table(ctx, id))) { s615_free_table(ctx, id); return s; }
+  if (table_id) *table_id = id;
+  return S615_OK;
+}
+
+int s615_build_table_sharded(s615_ctx* ctx, int N, int r, int shards, int layout, int* table_id) {
+  if (!ctx || N < 1 || N > 8 * kNSoftMax || r < 8 || r > 64 || shards < 2 || shards > 64)
+    return S615_E_ARG;
+  if (serving_blocks(ctx)) return S615_E_BUSY;
+  cudaSetDevice(ctx->device);
+  std::vector<u64> vals((size_t)N);
+  for (int i = 1; i <= N; ++i) { const u64 x2 = (u64)i * (u64)i; vals[i - 1] = x2 * x2 * x2; }
+  std::sort(vals.begin(), vals.end());
+  vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
+  void* dv = nullptr;
+  int s = dev_alloc(ctx, &dv, vals.size() * 8);
+  if (s) return s;
+  S615_CU(cudaMemcpy(dv, vals.data(), vals.size() * 8, cudaMemcpyHostToDevice));
+  u64 seeds[4];
+  for (int o = 0; o < 4; ++o) seeds[o] = kSeedBase + (u64)o * kPhi;
+  std::vector<DevTable> parts;
+  // one shard at a time: a build's scratch is sized for its shard's keys
+  for (int k = 0; k < shards && !s; ++k) {
+    DevTable t;
+    s = build_xor_device(ctx, static_cast<const u64*>(dv), vals.size(), nullptr, 0, r, seeds, 4, N,
+                         layout == S615_LAYOUT_AUTO ? S615_LAYOUT_WIDE : layout, &t, (u32)shards,
+                         (u32)k);
+    if (!s) parts.push_back(std::move(t));
+  }
+  dev_free(ctx, dv, vals.size() * 8);
+  if (s) {
+    for (DevTable& p : parts) free_table(ctx, p);
+    return s;
+  }
+  DevTable set;
+  if ((s = make_set(ctx, std::move(parts), &set))) return s;
+  int id = 0;
+  add_table(ctx, std::move(set), &id);
   if ((s = smoke_table(ctx, id))) { s615_free_table(ctx, id); return s; }
   if (table_id) *table_id = id;
   return S615_OK;

@@ -24,6 +24,9 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 constexpr int kNSoftMax = 120000;   // fourcore_xor_store.hpp:122
+// With pair-space shards each build holds one shard's keys; the set's limit
+// is HBM (a packed r=48 set at N = 240,000, B ~ 10.08M, is ~210 GB).
+constexpr int kNShardMax = 240000;
 
 void usage() {
   std::printf(
@@ -34,13 +37,16 @@ void usage() {
       "                 [--load-table F] [--save-table F]\n"
       "                 [--allow-rebuild] [--dump-survivors F] [--plain]\n"
       "                 [--layout packed|wide] [--batch K] [--plant COUNT[:SEED]]\n"
+      "                 [--shards S [--save-shards PREFIX]] [--load-shards F0,F1,..]\n"
       "   or: s615_cls5 --serve --N K [--load-table F] [--r BITS] [--batch K] < units.buc\n"
       "   or: s615_cls5 --check-table --N K --load-table F\n"
       "                 [--r BITS] [--save-table F] [--allow-rebuild]\n"
       "  --load-table F: packed xor from xor_build_save / --save-table.\n"
       "  --save-table F: write packed xor after build or successful load.\n"
       "  --allow-rebuild: if --load-table fails, build on the device (default: FATAL).\n"
-      "  --check-table: load + FPR smoke only.\n");
+      "  --check-table: load + FPR smoke only.\n"
+      "  --shards S: build the table as S pair-space shards (a probe asks only its\n"
+      "      key's shard); lifts the soft cap to N <= 240000 as HBM allows.\n");
 }
 
 int selftest_host() {
@@ -121,6 +127,59 @@ bool load_buc5(const char* path, std::vector<Line>& out) {  // fourcore_cls5_gpu
   return !out.empty();
 }
 
+std::vector<std::string> split_commas(const std::string& v) {
+  std::vector<std::string> out;
+  size_t a = 0;
+  while (a <= v.size()) {
+    const size_t b = v.find(',', a);
+    const std::string part = v.substr(a, b == std::string::npos ? std::string::npos : b - a);
+    if (!part.empty()) out.push_back(part);
+    if (b == std::string::npos) break;
+    a = b + 1;
+  }
+  return out;
+}
+
+// A pair-space shard set: loaded from its shard files in order, or built on
+// the device one shard at a time (and saved as <prefix>.shard<k>of<S>).
+bool acquire_shards(s615_ctx* ctx, int N, int r, int shards, const std::string& load,
+                    const std::string& save_prefix, int layout, int& tid) {
+  int s = 0;
+  if (!load.empty()) {
+    const auto files = split_commas(load);
+    std::vector<const char*> paths;
+    for (const auto& f : files) paths.push_back(f.c_str());
+    s = s615_load_table_shards(ctx, paths.data(), (int)paths.size(), N, layout, &tid);
+    if (s) {
+      std::fprintf(stderr, "[cls5-gpu] FATAL: --load-shards: %s\n", s615_strerror(s));
+      return false;
+    }
+  } else {
+    s = s615_build_table_sharded(ctx, N, r, shards, layout, &tid);
+    if (s) {
+      std::fprintf(stderr, "[cls5-gpu] FATAL: sharded xor build failed: %s\n", s615_strerror(s));
+      return false;
+    }
+  }
+  s615_table_info info;
+  s615_get_table_info(ctx, tid, &info);
+  std::fprintf(stderr, "[xor] N=%u keys=%llu cells=%llu r=%u in %u pair-space shards (%.2f GB in HBM)\n",
+               info.hdr.N, (unsigned long long)info.hdr.n_keys, (unsigned long long)info.hdr.m_cells,
+               info.hdr.r, info.hdr.shard_count, info.device_bytes / 1e9);
+  if (!save_prefix.empty()) {
+    for (unsigned k = 0; k < info.hdr.shard_count; ++k) {
+      const std::string path = save_prefix + ".shard" + std::to_string(k) + "of" +
+                               std::to_string(info.hdr.shard_count);
+      if ((s = s615_save_table_shard(ctx, tid, (int)k, path.c_str()))) {
+        std::fprintf(stderr, "[xor] cannot save %s: %s\n", path.c_str(), s615_strerror(s));
+        return false;
+      }
+      std::fprintf(stderr, "[xor] saved %s\n", path.c_str());
+    }
+  }
+  return true;
+}
+
 // acquire_xor_filter (fourcore_cls5_gpu_v4.cu:568-594) on the device.
 bool acquire(s615_ctx* ctx, int N, int& r, const std::string& load, const std::string& save,
              bool allow_rebuild, int layout, int& tid) {
@@ -172,8 +231,8 @@ bool acquire(s615_ctx* ctx, int N, int& r, const std::string& load, const std::s
 int main(int argc, char** argv) {
   std::setvbuf(stdout, nullptr, _IOLBF, 0);
   std::setvbuf(stderr, nullptr, _IOLBF, 0);
-  std::string units_path, load_table, save_table, dump_path;
-  int device = 0, N_override = 0, xor_r = 48, layout = S615_LAYOUT_AUTO;
+  std::string units_path, load_table, save_table, dump_path, load_shards, save_shards;
+  int device = 0, N_override = 0, xor_r = 48, layout = S615_LAYOUT_AUTO, shards = 1;
   size_t batch = 1 << 16;
   bool do_host = false, quiet = true, use_gate = true, stop_first = false;
   bool allow_rebuild = false, check_table = false, plain = false, serve = false;
@@ -196,6 +255,9 @@ int main(int argc, char** argv) {
     else if (s == "--load-table") load_table = next();
     else if (s == "--save-table") save_table = next();
     else if (s == "--allow-rebuild") allow_rebuild = true;
+    else if (s == "--shards") shards = std::atoi(next().c_str());
+    else if (s == "--load-shards") load_shards = next();
+    else if (s == "--save-shards") save_shards = next();
     else if (s == "--check-table") check_table = true;
     else if (s == "--dump-survivors") dump_path = next();
     else if (s == "--plain") plain = true;
@@ -215,11 +277,21 @@ int main(int argc, char** argv) {
   }
   if (do_host || argc == 1) return selftest_host();
   if (xor_r < 8 || xor_r > 64) { std::fprintf(stderr, "--r must be 8..64\n"); return 1; }
+  if (!load_shards.empty()) shards = std::max<int>(2, (int)split_commas(load_shards).size());
+  if (shards != 1 && (shards < 2 || shards > 64)) {
+    std::fprintf(stderr, "--shards must be 2..64\n");
+    return 1;
+  }
+  const int n_cap = shards > 1 ? kNShardMax : kNSoftMax;
+  auto get_table = [&](s615_ctx* c, int N, int& r, int& tid) {
+    if (shards > 1) return acquire_shards(c, N, r, shards, load_shards, save_shards, layout, tid);
+    return acquire(c, N, r, load_table, save_table, allow_rebuild, layout, tid);
+  };
 
   if (check_table) {
     if (N_override <= 0) { std::fprintf(stderr, "--check-table needs --N\n"); return 1; }
-    if (N_override > kNSoftMax) {
-      std::fprintf(stderr, "N=%d exceeds soft xor cap %d\n", N_override, kNSoftMax);
+    if (N_override > n_cap) {
+      std::fprintf(stderr, "N=%d exceeds soft xor cap %d\n", N_override, n_cap);
       return 1;
     }
   } else if (serve) {
@@ -239,7 +311,7 @@ int main(int argc, char** argv) {
 
   if (check_table) {
     int tid = 0;
-    if (!acquire(ctx, N_override, xor_r, load_table, save_table, allow_rebuild, layout, tid)) {
+    if (!get_table(ctx, N_override, xor_r, tid)) {
       s615_close(ctx);
       return 1;
     }
@@ -253,7 +325,7 @@ int main(int argc, char** argv) {
 
   if (serve) {   // units stream in on stdin; one request per --batch lines (or at EOF)
     int tid = 0;
-    if (!acquire(ctx, N_override, xor_r, load_table, save_table, allow_rebuild, layout, tid)) {
+    if (!get_table(ctx, N_override, xor_r, tid)) {
       s615_close(ctx);
       return 1;
     }
@@ -344,8 +416,9 @@ int main(int argc, char** argv) {
                units_path.c_str());
   if (units.empty()) { s615_close(ctx); return 1; }
   const int N = N_override > 0 ? N_override : (int)need;
-  if (N > kNSoftMax) {
-    std::fprintf(stderr, "N=%d exceeds soft xor cap %d\n", N, kNSoftMax);
+  if (N > n_cap) {
+    std::fprintf(stderr, "N=%d exceeds soft xor cap %d%s\n", N, n_cap,
+                 shards > 1 ? "" : " (past it: --shards S)");
     s615_close(ctx);
     return 1;
   }
@@ -360,7 +433,7 @@ int main(int argc, char** argv) {
   }
   std::vector<char> plant_got(plants.size(), 0);
   int tid = 0;
-  if (!acquire(ctx, N, xor_r, load_table, save_table, allow_rebuild, layout, tid)) {
+  if (!get_table(ctx, N, xor_r, tid)) {
     s615_close(ctx);
     return 1;
   }

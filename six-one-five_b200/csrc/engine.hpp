@@ -65,6 +65,12 @@ constexpr int kSharpWords = 7839;
 constexpr int kTriT504 = 0, kTriT247 = 16, kTriP504 = 24, kTriWords = 400;
 
 // Table resident in HBM.
+// Pair-space shards (spike/ribbon/shard.hpp:19-24): shard s of S holds the
+// pair keys k with mix64(k + kShardSeed) % S == s, and a probe of k queries
+// only that shard.  The reference's helper takes the seed as a parameter;
+// this store fixes it (every shard file of one set shares it).
+constexpr u64 kShardSeed = 0x615615615615615ULL;
+
 struct DevTable {
   s615_header hdr{};
   int layout = S615_LAYOUT_WIDE;
@@ -72,13 +78,17 @@ struct DevTable {
   void* d_cells = nullptr;
   size_t bytes = 0;
   u64 block = 0, recip = 0;
+  std::vector<DevTable> parts;   // a shard set (hdr.shard_count > 1): its shards in order
+  void* d_views = nullptr;       // the parts' TableViews in HBM
 };
 
-// Kernel-facing view of a table.
+// Kernel-facing view of a table (or of a shard set: shards > 1, parts).
 struct TableView {
   const void* cells;
   u64 block, recip, fpmask, seed;
-  u32 r, layout, cell_bytes, pad;
+  u32 r, layout, cell_bytes, shards;
+  const TableView* parts;
+  u64 shard_seed;
 };
 
 struct Cls5Counters {  // device accumulators (u64 atomics)
@@ -197,7 +207,7 @@ int launch_pack(s615_ctx* ctx, const void* d_wide, int cell_bytes, u64 m, u32 r,
 // Device xor build over a unique-value source; see xor_build.cu.
 int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u64* d_keys,
                      u64 n_keys, int r, const u64* seeds, int n_seeds, int N, int layout,
-                     DevTable* out);
+                     DevTable* out, u32 shards = 1, u32 shard = 0);
 
 // Device verifier; see verify.cu.
 int verify_device(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s615_hit* hits,

@@ -99,6 +99,7 @@ struct ItemCtx {
 };
 
 // Probe the ring entries [head, head+cnt) (one per lane).
+template <bool kSet>
 __device__ __forceinline__ void probe_batch(const PeelParams& P, const WarpSmem& W, u32 head,
                                             u32 cnt, const ItemCtx& I, u32 lane) {
   if (lane >= cnt) return;
@@ -117,7 +118,7 @@ __device__ __forceinline__ void probe_batch(const PeelParams& P, const WarpSmem&
     key = R.wlo - (u64)pow6_small(x);               // T - c3^6 mod 2^64
     rowval = I.r0 + I.mod * (I.j0 + r);             // d
   }
-  if (might_contain(P.tv, key)) {
+  if (probe_table<kSet>(P.tv, key)) {
     const unsigned long long idx = atomicAdd(&P.ctr->hits, 1ull);
     if (idx < P.hit_cap) {
       s615_hit h;
@@ -135,6 +136,7 @@ __device__ __forceinline__ void probe_batch(const PeelParams& P, const WarpSmem&
 }
 
 // Push the set bits of m into the ring; probe every full batch of 32.
+template <bool kSet>
 __device__ __forceinline__ void push_bits(const PeelParams& P, WarpSmem& W, u32 m, u32 di, u32 r,
                                           u32 kbase, u32& head, u32& qlen, const ItemCtx& I,
                                           u32 lane) {
@@ -147,7 +149,7 @@ __device__ __forceinline__ void push_bits(const PeelParams& P, WarpSmem& W, u32 
     qlen += __popc(ballot);
     if (qlen >= 32u) {
       __syncwarp();
-      probe_batch(P, W, head, 32u, I, lane);
+      probe_batch<kSet>(P, W, head, 32u, I, lane);
       __syncwarp();
       head = (head + 32u) & (kQ - 1);
       qlen -= 32u;
@@ -155,7 +157,7 @@ __device__ __forceinline__ void push_bits(const PeelParams& P, WarpSmem& W, u32 
   }
 }
 
-template <bool kSharp>
+template <bool kSharp, bool kSet>
 __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr u32 kP5 = kSharp ? (u32)kSharpWords : (u32)kPatWords;
@@ -294,12 +296,12 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
                 m &= lowmask;
               }
               my_probes += __popc(m);
-              push_bits(P, W, m, di, r, kbase, head, qlen, I, lane);
+              push_bits<kSet>(P, W, m, di, r, kbase, head, qlen, I, lane);
             }
           }
         }
         __syncwarp();
-        probe_batch(P, W, head, qlen, I, lane);   // drain before d0s change
+        probe_batch<kSet>(P, W, head, qlen, I, lane);   // drain before d0s change
         head = 0;
         qlen = 0;
         __syncwarp();
@@ -360,7 +362,7 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
           }
         }
         my_probes += __popc(m);
-        push_bits(P, W, m, 0, rr & 63u, kbase, head, qlen, I, lane);
+        push_bits<kSet>(P, W, m, 0, rr & 63u, kbase, head, qlen, I, lane);
         if (find2) {
           r += 32;
         } else if (++wt >= (len + 1023u) / 1024u) {   // len is the same in every lane here
@@ -369,7 +371,7 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
         }
       }
       __syncwarp();
-      probe_batch(P, W, head, qlen, I, lane);
+      probe_batch<kSet>(P, W, head, qlen, I, lane);
       __syncwarp();
     }
   }
@@ -389,13 +391,13 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
 }
 
 // k_peel over items [0, n) of the batch.
-template <bool kSharp>
+template <bool kSharp, bool kSet>
 int launch_main(s615_ctx* ctx, const TableView& tv, const s615_batch* b, size_t n,
                 unsigned flags, cudaStream_t st, int grid_blocks) {
   static bool attr_set = false;
   constexpr size_t kSmemTotal = smem_total<kSharp>();
   if (!attr_set) {
-    S615_CU(cudaFuncSetAttribute(k_peel<kSharp>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    S615_CU(cudaFuncSetAttribute(k_peel<kSharp, kSet>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kSmemTotal));
     attr_set = true;
   }
@@ -421,12 +423,12 @@ int launch_main(s615_ctx* ctx, const TableView& tv, const s615_batch* b, size_t 
   int grid = grid_blocks;
   if (grid <= 0) {
     int per_sm = 0;
-    S615_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel<kSharp>, kThreads, kSmemTotal));
+    S615_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel<kSharp, kSet>, kThreads, kSmemTotal));
     grid = ctx->num_sms * (per_sm > 0 ? per_sm : 1);
   }
   const size_t need = (n + kWarps - 1) / kWarps;
   if ((size_t)grid > need) grid = (int)need;
-  k_peel<kSharp><<<grid, kThreads, kSmemTotal, st>>>(P);
+  k_peel<kSharp, kSet><<<grid, kThreads, kSmemTotal, st>>>(P);
   ctx->launches++;
   S615_CU(cudaGetLastError());
   return S615_OK;
@@ -438,8 +440,12 @@ int launch_peel(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flag
                 cudaStream_t st, int grid_blocks) {
   if (b->n_main) {
     const bool sharp = (flags & S615_F_SHARP) && !(flags & S615_F_NO_GATE);
-    const int s = sharp ? launch_main<true>(ctx, tv, b, b->n_main, flags, st, grid_blocks)
-                        : launch_main<false>(ctx, tv, b, b->n_main, flags, st, grid_blocks);
+    const bool set = tv.shards > 1;
+    const int s =
+        set ? (sharp ? launch_main<true, true>(ctx, tv, b, b->n_main, flags, st, grid_blocks)
+                     : launch_main<false, true>(ctx, tv, b, b->n_main, flags, st, grid_blocks))
+            : (sharp ? launch_main<true, false>(ctx, tv, b, b->n_main, flags, st, grid_blocks)
+                     : launch_main<false, false>(ctx, tv, b, b->n_main, flags, st, grid_blocks));
     if (s) return s;
   }
   if (b->n_items > b->n_main) return launch_peel617(ctx, tv, b, flags, st, grid_blocks);

@@ -102,6 +102,7 @@ struct State617 {
   u64 pos, probes;
 };
 
+template <bool kSet>
 __device__ __forceinline__ void probe_batch(const Peel617Params& P, const WarpSmem617& W,
                                             u32 head, u32 cnt, const Item617& I, u32 lane) {
   if (lane >= cnt) return;
@@ -111,7 +112,7 @@ __device__ __forceinline__ void probe_batch(const Peel617Params& P, const WarpSm
   const u32 c3 = R.a + k;
   const u64 c33 = (u64)c3 * c3 * c3;
   const u64 key = R.wlo - c33 * c33;                // T' - c3^6 mod 2^64
-  if (might_contain(P.tv, key)) {
+  if (probe_table<kSet>(P.tv, key)) {
     const unsigned long long idx = atomicAdd(&P.ctr->hits, 1ull);
     if (idx < P.hit_cap) {
       const u32 aux = W.aux[r];
@@ -127,7 +128,7 @@ __device__ __forceinline__ void probe_batch(const Peel617Params& P, const WarpSm
 }
 
 // Sieve every buffered row, probe the survivors, empty the buffer.
-template <bool kSharp>
+template <bool kSharp, bool kSet>
 __device__ __forceinline__ void flush_rows(const Peel617Params& P, Warp617T<kSharp>& W,
                                            const u32* s_pat, State617& S, const Item617& I,
                                            u32 lane) {
@@ -180,7 +181,7 @@ __device__ __forceinline__ void flush_rows(const Peel617Params& P, Warp617T<kSha
       S.qlen += __popc(ballot);
       if (S.qlen >= 32u) {
         __syncwarp();
-        probe_batch(P, W, S.head, 32u, I, lane);
+        probe_batch<kSet>(P, W, S.head, 32u, I, lane);
         __syncwarp();
         S.head = (S.head + 32u) & (kQ - 1);
         S.qlen -= 32u;
@@ -188,7 +189,7 @@ __device__ __forceinline__ void flush_rows(const Peel617Params& P, Warp617T<kSha
     }
   }
   __syncwarp();
-  probe_batch(P, W, S.head, S.qlen, I, lane);   // drain before the rows change
+  probe_batch<kSet>(P, W, S.head, S.qlen, I, lane);   // drain before the rows change
   __syncwarp();
   S.head = 0;
   S.qlen = 0;
@@ -196,7 +197,7 @@ __device__ __forceinline__ void flush_rows(const Peel617Params& P, Warp617T<kSha
 }
 
 // Turn cnt queued c4 (from cq[ch]) into find3 rows, one per lane.
-template <bool kSharp>
+template <bool kSharp, bool kSet>
 __device__ __forceinline__ void make_rows(const Peel617Params& P, Warp617T<kSharp>& W,
                                           const u32* s_pat, State617& S, const Item617& I,
                                           u32 lane, u32 ch, u32 cnt, u32 h, u64 tl, u64 th) {
@@ -250,7 +251,7 @@ __device__ __forceinline__ void make_rows(const Peel617Params& P, Warp617T<kShar
   __syncwarp();
   const u32 bal = __ballot_sync(kFull, ok);
   const u32 nnew = __popc(bal);
-  if (S.nbuf + nnew > kBuf) flush_rows<kSharp>(P, W, s_pat, S, I, lane);
+  if (S.nbuf + nnew > kBuf) flush_rows<kSharp, kSet>(P, W, s_pat, S, I, lane);
   if (ok) {
     const u32 slot = S.nbuf + __popc(bal & lanemask_lt());
     W.rows[slot] = R;
@@ -265,7 +266,7 @@ __device__ __forceinline__ void make_rows(const Peel617Params& P, Warp617T<kShar
   __syncwarp();
 }
 
-template <bool kSharp>
+template <bool kSharp, bool kSet>
 __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Params P) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr u32 kPW = kSharp ? (u32)kSharpWords : (u32)kPatWords;
@@ -373,7 +374,7 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Par
           cl += __popc(bal);
           if (cl >= 32u) {
             __syncwarp();
-            make_rows<kSharp>(P, W, s_pat, S, I, lane, ch, 32u, h, tl, th);
+            make_rows<kSharp, kSet>(P, W, s_pat, S, I, lane, ch, 32u, h, tl, th);
             ch = (ch + 32u) & (kCQ - 1);
             cl -= 32u;
           }
@@ -381,10 +382,10 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Par
       }
       if (cl) {   // the queue refers to this half's lane rows: empty it now
         __syncwarp();
-        make_rows<kSharp>(P, W, s_pat, S, I, lane, ch, cl, h, tl, th);
+        make_rows<kSharp, kSet>(P, W, s_pat, S, I, lane, ch, cl, h, tl, th);
       }
     }
-    flush_rows<kSharp>(P, W, s_pat, S, I, lane);
+    flush_rows<kSharp, kSet>(P, W, s_pat, S, I, lane);
   }
 
   // ---- counters: warp reduce, one atomic per warp ----
@@ -409,13 +410,13 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Par
 
 namespace {
 
-template <bool kSharp>
+template <bool kSharp, bool kSet>
 int launch617(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
               cudaStream_t st, int grid_blocks) {
   static bool attr_set = false;
   constexpr size_t kSmemTotal = smem_total617<kSharp>();
   if (!attr_set) {
-    S615_CU(cudaFuncSetAttribute(k_peel617<kSharp>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    S615_CU(cudaFuncSetAttribute(k_peel617<kSharp, kSet>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kSmemTotal));
     attr_set = true;
   }
@@ -442,12 +443,12 @@ int launch617(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
   int grid = grid_blocks;
   if (grid <= 0) {
     int per_sm = 0;
-    S615_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel617<kSharp>, kThreads, kSmemTotal));
+    S615_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel617<kSharp, kSet>, kThreads, kSmemTotal));
     grid = ctx->num_sms * (per_sm > 0 ? per_sm : 1);
   }
   const size_t need = (n + kWarps - 1) / kWarps;
   if ((size_t)grid > need) grid = (int)need;
-  k_peel617<kSharp><<<grid, kThreads, kSmemTotal, st>>>(P);
+  k_peel617<kSharp, kSet><<<grid, kThreads, kSmemTotal, st>>>(P);
   ctx->launches++;
   S615_CU(cudaGetLastError());
   return S615_OK;
@@ -457,9 +458,12 @@ int launch617(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
 
 int launch_peel617(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
                    cudaStream_t st, int grid_blocks) {
-  if ((flags & S615_F_SHARP) && !(flags & S615_F_NO_GATE))
-    return launch617<true>(ctx, tv, b, flags, st, grid_blocks);
-  return launch617<false>(ctx, tv, b, flags, st, grid_blocks);
+  const bool sharp = (flags & S615_F_SHARP) && !(flags & S615_F_NO_GATE);
+  if (tv.shards > 1)
+    return sharp ? launch617<true, true>(ctx, tv, b, flags, st, grid_blocks)
+                 : launch617<false, true>(ctx, tv, b, flags, st, grid_blocks);
+  return sharp ? launch617<true, false>(ctx, tv, b, flags, st, grid_blocks)
+               : launch617<false, false>(ctx, tv, b, flags, st, grid_blocks);
 }
 
 }  // namespace s615

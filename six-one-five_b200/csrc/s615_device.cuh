@@ -26,23 +26,28 @@ __device__ __forceinline__ u32 ld_cell32(const unsigned int* p) {
   return v;
 }
 
-__device__ __forceinline__ u64 load_cell(const TableView& t, u64 i) {
-  if (t.layout == S615_LAYOUT_WIDE) {
-    if (t.cell_bytes == 8) return ld_cell64(static_cast<const unsigned long long*>(t.cells) + i);
-    return (u64)ld_cell32(static_cast<const unsigned int*>(t.cells) + i);
+__device__ __forceinline__ u64 load_cell_at(const void* cells, u32 layout, u32 cell_bytes, u32 r,
+                                             u64 fpmask, u64 i) {
+  if (layout == S615_LAYOUT_WIDE) {
+    if (cell_bytes == 8) return ld_cell64(static_cast<const unsigned long long*>(cells) + i);
+    return (u64)ld_cell32(static_cast<const unsigned int*>(cells) + i);
   }
-  const unsigned long long* p = static_cast<const unsigned long long*>(t.cells);
-  const u64 bit = i * (u64)t.r;
+  const unsigned long long* p = static_cast<const unsigned long long*>(cells);
+  const u64 bit = i * (u64)r;
   const u64 w = bit >> 6;
   const u32 o = (u32)(bit & 63);
   u64 v = ld_cell64(p + w) >> o;
-  if (o + t.r > 64) v |= ld_cell64(p + w + 1) << (64 - o);
-  return v & t.fpmask;
+  if (o + r > 64) v |= ld_cell64(p + w + 1) << (64 - o);
+  return v & fpmask;
+}
+
+__device__ __forceinline__ u64 load_cell(const TableView& t, u64 i) {
+  return load_cell_at(t.cells, t.layout, t.cell_bytes, t.r, t.fpmask, i);
 }
 
 // xor_might_contain: h = mix64(key + seed), three cells, compare with the
 // low r bits of h.
-__device__ __forceinline__ bool might_contain(const TableView& t, u64 key) {
+__device__ __forceinline__ bool might_contain_one(const TableView& t, u64 key) {
   if (t.block == 0) return false;
   const u64 h = mix64(key + t.seed);
   u64 c[3];
@@ -51,6 +56,22 @@ __device__ __forceinline__ bool might_contain(const TableView& t, u64 key) {
   const u64 b = load_cell(t, c[1]);
   const u64 d = load_cell(t, c[2]);
   return (a ^ b ^ d) == (h & t.fpmask);
+}
+
+// A shard set sends the probe to the key's own shard, mix64(key + seed) % S
+// (residue-steered probing: one query per probe, as for one table); a set's
+// view keeps S and its reciprocal in block / recip.  The hot kernels are
+// compiled once per case (kSet), so a single table's probe is unchanged.
+template <bool kSet>
+__device__ __forceinline__ bool probe_table(const TableView& t, u64 key) {
+  if constexpr (kSet)
+    return might_contain_one(t.parts[fast_mod(mix64(key + t.shard_seed), t.block, t.recip)], key);
+  else
+    return might_contain_one(t, key);
+}
+
+__device__ __forceinline__ bool might_contain(const TableView& t, u64 key) {
+  return t.shards > 1 ? probe_table<true>(t, key) : probe_table<false>(t, key);
 }
 
 // x^6 for x < 2^21 (exact, < 2^126).

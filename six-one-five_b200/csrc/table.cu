@@ -69,6 +69,17 @@ int grid_for(s615_ctx* ctx, u64 n, int threads) {
 
 TableView view_of(const DevTable& t) {
   TableView v{};
+  v.shards = 1;
+  if (!t.parts.empty()) {   // a shard set: the parts' views live in HBM
+    v.shards = (u32)t.parts.size();
+    v.block = v.shards;   // the shard index is fast_mod(mix, S, recip)
+    v.recip = mod_recip(v.shards);
+    v.parts = static_cast<const TableView*>(t.d_views);
+    v.shard_seed = kShardSeed;
+    v.r = t.hdr.r;
+    v.fpmask = fp_mask(t.hdr.r);
+    return v;
+  }
   v.cells = t.d_cells;
   v.block = t.hdr.m_cells / 3;
   v.recip = mod_recip(v.block);

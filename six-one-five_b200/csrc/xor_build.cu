@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -53,32 +54,42 @@ __device__ __forceinline__ void hset_insert(unsigned long long* table, u64 tmask
   }
 }
 
+// Which keys this build takes: the memory partition (top bits of mix64(key))
+// and, for one shard of a set, mix64(key + kShardSeed) % shards == shard.
+struct KeyFilter {
+  u32 part_bits, part, shards, shard;
+  u64 srecip;
+  __device__ __forceinline__ bool take(u64 key) const {
+    if (part_bits && (mix64(key) >> (64 - part_bits)) != part) return false;
+    return shards <= 1 || fast_mod(mix64(key + kShardSeed), shards, srecip) == shard;
+  }
+};
+
 // Pair keys u[a] + u[b], a <= b, one block-stride row per a.
 __global__ void k_insert_pairs(const u64* __restrict__ vals, u64 nv, unsigned long long* table,
-                               u64 tmask, u32 part_bits, u32 part, u32* has_empty_key) {
+                               u64 tmask, KeyFilter kf, u32* has_empty_key) {
   for (u64 a = blockIdx.x; a < nv; a += gridDim.x) {
     const u64 va = vals[a];
     for (u64 b = a + threadIdx.x; b < nv; b += blockDim.x) {
       const u64 key = va + vals[b];
-      if (part_bits && (mix64(key) >> (64 - part_bits)) != part) continue;
-      hset_insert(table, tmask, key, has_empty_key);
+      if (kf.take(key)) hset_insert(table, tmask, key, has_empty_key);
     }
   }
 }
 
 __global__ void k_insert_keys(const u64* __restrict__ keys, u64 n, unsigned long long* table,
-                              u64 tmask, u32 part_bits, u32 part, u32* has_empty_key) {
+                              u64 tmask, KeyFilter kf, u32* has_empty_key) {
   for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n;
        i += (u64)gridDim.x * blockDim.x) {
     const u64 key = keys[i];
-    if (part_bits && (mix64(key) >> (64 - part_bits)) != part) continue;
-    hset_insert(table, tmask, key, has_empty_key);
+    if (kf.take(key)) hset_insert(table, tmask, key, has_empty_key);
   }
 }
 
-// Append occupied slots to out (order irrelevant).
+// Append occupied slots to out (order irrelevant); slots past cap are
+// counted, not written.
 __global__ void k_compact(const unsigned long long* __restrict__ table, u64 tsize,
-                          u64* __restrict__ out, unsigned long long* n_out) {
+                          u64* __restrict__ out, u64 cap, unsigned long long* n_out) {
   const u32 lane = threadIdx.x & 31;
   for (u64 i0 = blockIdx.x * (u64)blockDim.x; i0 < tsize; i0 += (u64)gridDim.x * blockDim.x) {
     const u64 i = i0 + threadIdx.x;
@@ -87,7 +98,8 @@ __global__ void k_compact(const unsigned long long* __restrict__ table, u64 tsiz
     unsigned long long base = 0;
     if (lane == 0 && ballot) base = atomicAdd(n_out, (unsigned long long)__popc(ballot));
     base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (occ) out[base + __popc(ballot & ((1u << lane) - 1u))] = table[i];
+    const u64 k = base + __popc(ballot & ((1u << lane) - 1u));
+    if (occ && k < cap) out[k] = table[i];
   }
 }
 
@@ -195,10 +207,16 @@ u64 pow2_at_least(u64 x) { u64 p = 1; while (p < x) p <<= 1; return p; }
 
 int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u64* d_keys,
                      u64 n_keys, int r, const u64* seeds, int n_seeds, int N, int layout,
-                     DevTable* out) {
+                     DevTable* out, u32 shards, u32 shard) {
   cudaStream_t st = ctx->stream;
   const bool pairs = d_pair_vals != nullptr;
-  const u64 n_raw = pairs ? n_vals * (n_vals + 1) / 2 : n_keys;
+  if (shards < 1) shards = 1;
+  if (shard >= shards) return S615_E_ARG;
+  const u64 n_all = pairs ? n_vals * (n_vals + 1) / 2 : n_keys;
+  // one shard's share of the keys, with room for the binomial spread
+  const u64 n_raw = shards == 1 ? n_all
+                                : std::min<u64>(n_all, n_all / shards +
+                                                           8 * (u64)std::sqrt((double)n_all) + 4096);
 
   // ---- 1. unique keys ----
   Buf keys(ctx);
@@ -229,20 +247,21 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
     S615_CU(cudaMemsetAsync(scratch.p, 0, 64, st));
     for (u32 part = 0; part < (1u << part_bits); ++part) {
       S615_CU(cudaMemsetAsync(table.p, 0xFF, tsize * sizeof(u64), st));
+      const KeyFilter kf{part_bits, part, shards, shard, mod_recip(shards)};
       if (pairs) {
         const int grid = (int)std::min<u64>(n_vals ? n_vals : 1, (u64)ctx->num_sms * 32);
         k_insert_pairs<<<grid, 256, 0, st>>>(d_pair_vals, n_vals,
                                              static_cast<unsigned long long*>(table.p), tsize - 1,
-                                             part_bits, part, d_flag);
+                                             kf, d_flag);
       } else {
         k_insert_keys<<<grid_for(ctx, n_keys, 256), 256, 0, st>>>(
-            d_keys, n_keys, static_cast<unsigned long long*>(table.p), tsize - 1, part_bits, part,
-            d_flag);
+            d_keys, n_keys, static_cast<unsigned long long*>(table.p), tsize - 1, kf, d_flag);
       }
       ctx->launches++;
       S615_CU(cudaGetLastError());
       k_compact<<<grid_for(ctx, tsize, 256), 256, 0, st>>>(
-          static_cast<const unsigned long long*>(table.p), tsize, static_cast<u64*>(keys.p), d_n);
+          static_cast<const unsigned long long*>(table.p), tsize, static_cast<u64*>(keys.p), n_raw,
+          d_n);
       ctx->launches++;
       S615_CU(cudaGetLastError());
     }
@@ -252,6 +271,7 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
     S615_CU(cudaMemcpyAsync(&h_n, d_n, 8, cudaMemcpyDeviceToHost, st));
     S615_CU(cudaStreamSynchronize(st));
     n = h_n;
+    if (n > n_raw) return S615_E_BUILD;   // more keys in this shard than its buffer holds
     if (h_flag) {
       const u64 e = kEmpty;
       S615_CU(cudaMemcpy(static_cast<u64*>(keys.p) + n, &e, 8, cudaMemcpyHostToDevice));
@@ -262,7 +282,8 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
   std::memset(&out->hdr, 0, sizeof out->hdr);
   out->hdr.magic = kMagic; out->hdr.version = kVersion; out->hdr.kind = 1;
   out->hdr.r = (u32)r; out->hdr.N = (u32)(N > 0 ? N : 0);
-  out->hdr.shard_count = 1;
+  out->hdr.shard_count = shards;
+  out->hdr.shard_index = shard;
   if (n == 0) {
     out->hdr.mix_seed = seeds[0];
     out->layout = S615_LAYOUT_WIDE; out->cell_bytes = 8;

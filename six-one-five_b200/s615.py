@@ -102,6 +102,11 @@ SIGNATURES = {
     "s615_build_table_keys": (C.c_int, [_P, _P, C.c_size_t, C.c_int, C.c_uint64, C.c_int,
                                         C.POINTER(C.c_int)]),
     "s615_save_table": (C.c_int, [_P, C.c_int, C.c_char_p]),
+    "s615_build_table_sharded": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int,
+                                           C.POINTER(C.c_int)]),
+    "s615_load_table_shards": (C.c_int, [_P, C.POINTER(C.c_char_p), C.c_int, C.c_int, C.c_int,
+                                         C.POINTER(C.c_int)]),
+    "s615_save_table_shard": (C.c_int, [_P, C.c_int, C.c_int, C.c_char_p]),
     "s615_export_table": (C.c_int, [_P, C.c_int, C.POINTER(Header), _P, C.c_size_t,
                                     C.POINTER(C.c_size_t)]),
     "s615_get_table_info": (C.c_int, [_P, C.c_int, C.POINTER(TableInfo)]),
@@ -446,6 +451,23 @@ class Engine:
 
     def save_table(self, tid: int, path: str) -> None:
         _check(lib().s615_save_table(self._ctx, tid, path.encode()), "save_table")
+
+    def build_table_sharded(self, N: int, r: int, shards: int, layout: int = LAYOUT_AUTO) -> int:
+        """A pair-space shard set: S xor tables, a probe queries its key's shard."""
+        tid = C.c_int(0)
+        _check(lib().s615_build_table_sharded(self._ctx, N, r, shards, layout, C.byref(tid)),
+               "build_table_sharded")
+        return tid.value
+
+    def load_table_shards(self, paths, expected_N: int = 0, layout: int = LAYOUT_AUTO) -> int:
+        arr = (C.c_char_p * len(paths))(*[p.encode() for p in paths])
+        tid = C.c_int(0)
+        _check(lib().s615_load_table_shards(self._ctx, arr, len(paths), expected_N, layout,
+                                            C.byref(tid)), "load_table_shards")
+        return tid.value
+
+    def save_table_shard(self, tid: int, shard: int, path: str) -> None:
+        _check(lib().s615_save_table_shard(self._ctx, tid, shard, path.encode()), "save_table_shard")
 
     def export_table(self, tid: int):
         """(64 header bytes, packed cell bytes as uint8 ndarray)."""
