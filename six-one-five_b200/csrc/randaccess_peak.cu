@@ -2,7 +2,8 @@
 // xor probe (three random cells per probe).
 //
 // Reads `iters` 8-byte words at hashed (uniform, always in-bounds) positions of
-// a 2 GiB buffer with several load forms and prints reads/s.  The result is the
+// a buffer (2 GiB unless sizes are given) with several load forms and prints
+// reads/s.  The result is the
 // denominator for the probe kernel's random-access roofline.
 //   bin/randaccess_peak            (run under ncu with dram__sectors_read.sum to
 //                                   see the bytes each form moves per read)
@@ -10,6 +11,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 
 typedef unsigned long long u64;
 
@@ -35,39 +37,50 @@ __global__ void k_random_reads(const u64* __restrict__ p, u64 n, u64 iters, u64*
   if (acc == 0x123456789ULL) out[0] = acc;
 }
 
-int main() {
-  const u64 n = (2ull << 30) / 8;
+// Usage: randaccess_peak [GiB ...] -- one line per load form and buffer size
+// (default 2 GiB); larger buffers show how the rate falls with the footprint.
+int main(int argc, char** argv) {
   const u64 iters = 1ull << 27;
-  u64 *p = nullptr, *o = nullptr;
-  if (cudaMalloc(&p, n * 8) != cudaSuccess || cudaMalloc(&o, 8) != cudaSuccess) {
-    std::printf("alloc failed\n");
-    return 1;
-  }
-  cudaMemset(p, 1, n * 8);
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
   cudaEvent_t a, b;
   cudaEventCreate(&a);
   cudaEventCreate(&b);
+  u64* o = nullptr;
+  if (cudaMalloc(&o, 8) != cudaSuccess) { std::printf("alloc failed\n"); return 1; }
   const char* names[3] = {"ld.global.nc (L1)", "ld.global.cg", "ld.global.cg.L2::64B"};
-  for (int v = 0; v < 3; ++v) {
-    auto launch = [&]() {
-      if (v == 0) k_random_reads<0><<<sms * 8, 256>>>(p, n, iters, o);
-      else if (v == 1) k_random_reads<1><<<sms * 8, 256>>>(p, n, iters, o);
-      else k_random_reads<2><<<sms * 8, 256>>>(p, n, iters, o);
-    };
-    launch();
-    cudaEventRecord(a);
-    launch();
-    cudaEventRecord(b);
-    cudaEventSynchronize(b);
-    float ms = 0;
-    cudaEventElapsedTime(&ms, a, b);
-    std::printf("%-24s %.3f ms  %.3e random reads/s\n", names[v], ms, iters / (ms * 1e-3));
+  const int nsizes = argc > 1 ? argc - 1 : 1;
+  cudaError_t e = cudaSuccess;
+  for (int si = 0; si < nsizes && e == cudaSuccess; ++si) {
+    const double gib = argc > 1 ? std::atof(argv[1 + si]) : 2.0;
+    const u64 n = (u64)(gib * (double)(1ull << 30)) / 8;
+    u64* p = nullptr;
+    if (n < 1024 || cudaMalloc(&p, n * 8) != cudaSuccess) {
+      std::printf("%.1f GiB: alloc failed\n", gib);
+      cudaGetLastError();
+      continue;
+    }
+    cudaMemset(p, 1, n * 8);
+    for (int v = 0; v < 3; ++v) {
+      auto launch = [&]() {
+        if (v == 0) k_random_reads<0><<<sms * 8, 256>>>(p, n, iters, o);
+        else if (v == 1) k_random_reads<1><<<sms * 8, 256>>>(p, n, iters, o);
+        else k_random_reads<2><<<sms * 8, 256>>>(p, n, iters, o);
+      };
+      launch();
+      cudaEventRecord(a);
+      launch();
+      cudaEventRecord(b);
+      cudaEventSynchronize(b);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, a, b);
+      std::printf("%7.1f GiB  %-24s %.3f ms  %.3e random reads/s\n", gib, names[v], ms,
+                  iters / (ms * 1e-3));
+    }
+    cudaFree(p);
+    e = cudaGetLastError();
   }
-  const cudaError_t e = cudaGetLastError();
   std::printf("status: %s\n", cudaGetErrorString(e));
-  cudaFree(p);
   cudaFree(o);
   return e == cudaSuccess ? 0 : 1;
 }
