@@ -200,6 +200,14 @@ int s615_build_table_sharded(s615_ctx* ctx, int N, int r, int shards, int layout
 int s615_load_table_shards(s615_ctx* ctx, const char* const* paths, int n, int expected_N,
                            int layout, int* table_id);
 int s615_save_table_shard(s615_ctx* ctx, int table_id, int shard, const char* path);
+/* Probe passes over a shard set (no counterpart in the reference).  Random
+ * reads lose ~3x of their rate once their footprint passes ~64 GiB (the
+ * GPU's address-translation reach), so a larger set is probed in G passes:
+ * pass g sieves the whole batch again but probes only keys of the g-th group
+ * of shards.  Counters and hits are those of one pass over all shards.
+ * groups = 0 (the default) picks G = ceil(set bytes / 56 GiB); 1..S forces
+ * G.  S615_E_ARG for a single table. */
+int s615_set_probe_groups(s615_ctx* ctx, int table_id, int groups);
 /* The packed file bytes (after the 64-byte header) into a host buffer of
  * cap >= packed_bytes(m_cells, r) bytes; the in-memory form of the
  * reference's XorFilter::packed. *len receives the byte count. */

@@ -470,6 +470,16 @@ int s615_save_table(s615_ctx* ctx, int id, const char* path) {
   return save_part(ctx, t, path);
 }
 
+int s615_set_probe_groups(s615_ctx* ctx, int id, int groups) {
+  if (!ctx) return S615_E_ARG;
+  if (serving_blocks(ctx)) return S615_E_BUSY;
+  DevTable* t = find_table(ctx, id);
+  if (!t) return S615_E_NOTABLE;
+  if (t->parts.empty() || groups < 0 || groups > (int)t->parts.size()) return S615_E_ARG;
+  t->groups = (u32)groups;
+  return S615_OK;
+}
+
 int s615_save_table_shard(s615_ctx* ctx, int id, int shard, const char* path) {
   if (!ctx || !path) return S615_E_ARG;
   DevTable* t = find_table(ctx, id);

@@ -80,7 +80,17 @@ struct DevTable {
   u64 block = 0, recip = 0;
   std::vector<DevTable> parts;   // a shard set (hdr.shard_count > 1): its shards in order
   void* d_views = nullptr;       // the parts' TableViews in HBM
+  u32 groups = 0;                // probe passes over a set (0: from its size)
 };
+
+// Random reads keep their rate over footprints up to 64 GiB and lose ~3x at
+// 110 GiB on a B200 (bin/randaccess_peak 2 8 29 64 110).  A shard set larger
+// than this is probed in passes over groups of its shards, each pass
+// touching at most this many bytes.
+constexpr u64 kProbeGroupBytes = 56ull << 30;
+// Internal launch flag: a pass after the first adds no counters (it repeats
+// the first pass's points; only its probes differ).
+constexpr unsigned kFlagNoCount = 1u << 30;
 
 // Kernel-facing view of a table (or of a shard set: shards > 1, parts).
 struct TableView {
@@ -89,6 +99,8 @@ struct TableView {
   u32 r, layout, cell_bytes, shards;
   const TableView* parts;
   u64 shard_seed;
+  u32 grp_lo, grp_hi;   // this pass probes keys of shards [grp_lo, grp_hi)
+  u32 groups, pad;      // passes over the set
 };
 
 struct Cls5Counters {  // device accumulators (u64 atomics)

@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <cstddef>
 #include <mutex>
 
 #include "engine.hpp"
@@ -33,6 +34,8 @@ struct Scratch {
   Cls5Counters ctr;
   u32 work;
 };
+// launch_peel clears 8 bytes of work counters between passes over a shard set
+static_assert(offsetof(Scratch, work) + 8 <= sizeof(Scratch), "work counters");
 
 // The scratch: every GPU that loads the library holds these ~1.9 MB until the
 // process exits.  All calls share it; it keeps the last call's contents.

@@ -25,6 +25,7 @@
 //    items from one device-wide queue; nothing waits at a block barrier.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "peel_common.cuh"
@@ -72,6 +73,7 @@ struct PeelParams {
   u64 inv21_lo, inv21_hi;  // (21^6)^-1 mod 2^128
   u32 s8;                  // admissible values mod 8, as a bitmask
   u64 p64;                 // sharp gate: admissible values mod 64, as a bitmask
+  u32 count;               // add this launch's counters (0 for a repeat pass over a set)
 };
 
 // cls5 pattern words (sharp or not) then the find3 ones, then the warp slices
@@ -383,7 +385,7 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
     my_pos += __shfl_xor_sync(0xFFFFFFFFu, my_pos, o);
     my_probes += __shfl_xor_sync(0xFFFFFFFFu, my_probes, o);
   }
-  if (lane == 0) {
+  if (lane == 0 && P.count) {
     atomicAdd(&P.ctr->calls, (unsigned long long)my_calls);
     atomicAdd(&P.ctr->pos, (unsigned long long)my_pos);
     atomicAdd(&P.ctr->probes, (unsigned long long)my_probes);
@@ -414,6 +416,7 @@ int launch_main(s615_ctx* ctx, const TableView& tv, const s615_batch* b, size_t 
   // ctx->d_pat = [gate cls5 | open cls5 | gate find3 | open find3]
   P.pat5 = kSharp ? ctx->d_sharp : ctx->d_pat + (gated ? 0 : kPatWords);
   P.p64 = ctx->p64;
+  P.count = (flags & kFlagNoCount) ? 0u : 1u;
   P.pat3 = ctx->d_pat + 2 * kPatWords + (gated ? 0 : kPatWords);
   const u128 inv = inv_2adic_u128((u128)kM21);
   P.inv21_lo = (u64)inv;
@@ -436,8 +439,8 @@ int launch_main(s615_ctx* ctx, const TableView& tv, const s615_batch* b, size_t 
 
 }  // namespace
 
-int launch_peel(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
-                cudaStream_t st, int grid_blocks) {
+static int launch_pass(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
+                       cudaStream_t st, int grid_blocks) {
   if (b->n_main) {
     const bool sharp = (flags & S615_F_SHARP) && !(flags & S615_F_NO_GATE);
     const bool set = tv.shards > 1;
@@ -449,6 +452,25 @@ int launch_peel(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flag
     if (s) return s;
   }
   if (b->n_items > b->n_main) return launch_peel617(ctx, tv, b, flags, st, grid_blocks);
+  return S615_OK;
+}
+
+// One pass, or for a shard set of G probe groups G passes: pass g probes only
+// the keys of its group's shards; passes after the first restart the work
+// queues and add no counters, and every pass appends to the same hit list.
+int launch_peel(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
+                cudaStream_t st, int grid_blocks) {
+  const u32 G = tv.shards > 1 ? std::max(1u, tv.groups) : 1u;
+  for (u32 g = 0; g < G; ++g) {
+    TableView v = tv;
+    if (G > 1) {
+      v.grp_lo = (u32)((u64)tv.shards * g / G);
+      v.grp_hi = (u32)((u64)tv.shards * (g + 1) / G);
+    }
+    if (g > 0) S615_CU(cudaMemsetAsync(b->d_work, 0, 8, st));
+    const int s = launch_pass(ctx, v, b, g > 0 ? flags | kFlagNoCount : flags, st, grid_blocks);
+    if (s) return s;
+  }
   return S615_OK;
 }
 

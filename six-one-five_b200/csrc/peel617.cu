@@ -78,6 +78,7 @@ struct Peel617Params {
   u32 s8;                  // admissible values mod 8, as a bitmask
   u32 use_tri;
   u64 p64;                 // sharp gate: admissible values mod 64, as a bitmask
+  u32 count;               // add this launch's counters (0 for a repeat pass over a set)
 };
 
 // Pattern words, the triple-sum block, then the warp slices (16-byte aligned:
@@ -397,7 +398,7 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Par
     my_tri += __shfl_xor_sync(kFull, my_tri, o);
     my_skip += __shfl_xor_sync(kFull, my_skip, o);
   }
-  if (lane == 0) {
+  if (lane == 0 && P.count) {
     atomicAdd(&P.ctr->calls, (unsigned long long)pos);
     atomicAdd(&P.ctr->pos, (unsigned long long)pos);
     atomicAdd(&P.ctr->probes, (unsigned long long)probes);
@@ -434,6 +435,7 @@ int launch617(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
   const bool gated = !(flags & S615_F_NO_GATE);
   P.pat3 = kSharp ? ctx->d_sharp + kSharpWords : ctx->d_pat + 2 * kPatWords + (gated ? 0 : kPatWords);
   P.p64 = ctx->p64;
+  P.count = (flags & kFlagNoCount) ? 0u : 1u;
   P.tri = ctx->d_tri;
   const u128 inv = inv_2adic_u128((u128)kM21);
   P.inv21_lo = (u64)inv;

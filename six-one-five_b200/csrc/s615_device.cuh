@@ -62,12 +62,17 @@ __device__ __forceinline__ bool might_contain_one(const TableView& t, u64 key) {
 // (residue-steered probing: one query per probe, as for one table); a set's
 // view keeps S and its reciprocal in block / recip.  The hot kernels are
 // compiled once per case (kSet), so a single table's probe is unchanged.
+// A key whose shard is outside the pass's group [grp_lo, grp_hi) is left to
+// the pass that owns that group.
 template <bool kSet>
 __device__ __forceinline__ bool probe_table(const TableView& t, u64 key) {
-  if constexpr (kSet)
-    return might_contain_one(t.parts[fast_mod(mix64(key + t.shard_seed), t.block, t.recip)], key);
-  else
+  if constexpr (kSet) {
+    const u32 s = (u32)fast_mod(mix64(key + t.shard_seed), t.block, t.recip);
+    if (s - t.grp_lo >= t.grp_hi - t.grp_lo) return false;
+    return might_contain_one(t.parts[s], key);
+  } else {
     return might_contain_one(t, key);
+  }
 }
 
 __device__ __forceinline__ bool might_contain(const TableView& t, u64 key) {

@@ -7,6 +7,8 @@
 // wraps once 3*block > 2^32).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "s615_device.cuh"
 
 namespace s615 {
@@ -76,6 +78,12 @@ TableView view_of(const DevTable& t) {
     v.recip = mod_recip(v.shards);
     v.parts = static_cast<const TableView*>(t.d_views);
     v.shard_seed = kShardSeed;
+    size_t bytes = 0;
+    for (const DevTable& p : t.parts) bytes += p.bytes;
+    const u64 want = t.groups ? t.groups : (bytes + kProbeGroupBytes - 1) / kProbeGroupBytes;
+    v.groups = (u32)std::min<u64>(std::max<u64>(want, 1), v.shards);
+    v.grp_lo = 0;
+    v.grp_hi = v.shards;
     v.r = t.hdr.r;
     v.fpmask = fp_mask(t.hdr.r);
     return v;

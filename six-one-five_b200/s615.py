@@ -107,6 +107,7 @@ SIGNATURES = {
     "s615_load_table_shards": (C.c_int, [_P, C.POINTER(C.c_char_p), C.c_int, C.c_int, C.c_int,
                                          C.POINTER(C.c_int)]),
     "s615_save_table_shard": (C.c_int, [_P, C.c_int, C.c_int, C.c_char_p]),
+    "s615_set_probe_groups": (C.c_int, [_P, C.c_int, C.c_int]),
     "s615_export_table": (C.c_int, [_P, C.c_int, C.POINTER(Header), _P, C.c_size_t,
                                     C.POINTER(C.c_size_t)]),
     "s615_get_table_info": (C.c_int, [_P, C.c_int, C.POINTER(TableInfo)]),
@@ -465,6 +466,10 @@ class Engine:
         _check(lib().s615_load_table_shards(self._ctx, arr, len(paths), expected_N, layout,
                                             C.byref(tid)), "load_table_shards")
         return tid.value
+
+    def set_probe_groups(self, tid: int, groups: int) -> None:
+        """Probe a shard set in `groups` passes (0: from its size)."""
+        _check(lib().s615_set_probe_groups(self._ctx, tid, groups), "set_probe_groups")
 
     def save_table_shard(self, tid: int, shard: int, path: str) -> None:
         _check(lib().s615_save_table_shard(self._ctx, tid, shard, path.encode()), "save_table_shard")

@@ -166,3 +166,44 @@ def test_cli_shards(tmp_path):
         outs.append((m.groups(), sorted(l for l in p.stdout.splitlines() if l.startswith("SOLUTION"))))
     assert outs[0] == outs[1] == outs[2]
     assert "pair-space shards" in p.stderr
+
+
+@pytest.mark.parametrize("G", [2, 3, 4])
+def test_probe_groups_change_nothing(engine, oracle_shards, G):
+    """Probing a set in G passes (one group of shards each) gives the one-pass
+    counters and raw hits, for every unit kind in one mixed batch."""
+    N = 54400 // 42
+    _, paths = oracle_shards(N, 16, 4)
+    tid = engine.load_table_shards(paths, N)
+    try:
+        units = list(s615.make_units(W.cls5_units(54301, 54400))[0])
+        c7, n7 = s615.candidates617(54347)
+        units += [c7[i] for i in range(n7)]
+        for B, u, c in [(24329, orc.unit_candidates(24329, 1)[0], 1), (54301, 5856, 5)]:
+            a, k, _ = s615.expand_unit(B, u, c)
+            units += [a[i] for i in range(min(k, 3000))]
+        arr = (s615.Unit * len(units))(*units)
+        key = lambda hs: sorted(tuple(int(h[f]) for f in ("unit", "d", "e", "c4", "fp")) for h in hs)
+        fields = ("calls", "gated", "probes", "pos", "hits", "tri_total", "tri_skipped")
+        out = []
+        for g, flags in ((1, 0), (G, 0), (1, s615.F_SHARP), (G, s615.F_SHARP)):
+            engine.set_probe_groups(tid, g)
+            h, c = engine.run(tid, arr, len(units), flags)
+            out.append((key(h), tuple(getattr(c, f) for f in fields)))
+        assert out[0] == out[1] and out[2] == out[3]
+        engine.set_probe_groups(tid, G)                   # the plain form, a few units
+        hp, cp = engine.run(tid, arr, 40, s615.F_PLAIN)
+        engine.set_probe_groups(tid, 1)
+        h1, c1 = engine.run(tid, arr, 40, s615.F_PLAIN)
+        assert key(hp) == key(h1) and tuple(getattr(cp, f) for f in fields) == \
+            tuple(getattr(c1, f) for f in fields)
+        with pytest.raises(s615.S615Error):
+            engine.set_probe_groups(tid, 5)                # more groups than shards
+    finally:
+        engine.free_table(tid)
+    mono = engine.build_table(300, 16)
+    try:
+        with pytest.raises(s615.S615Error):
+            engine.set_probe_groups(mono, 2)               # a single table has no groups
+    finally:
+        engine.free_table(mono)
