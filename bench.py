@@ -11,7 +11,10 @@ points ("peel probes") per second with units already resident in HBM;
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Multi-GPU (torchrun): each rank owns its own 20,000-B band (weak scaling),
-no collective on the data path; rank 0 prints one JSON line.
+no collective on the data path; rank 0 prints one JSON line.  With
+--shards S the ranks instead split one pair-space shard set (a table too
+large for one GPU): each holds its range of shards and runs the whole band
+(strong scaling); the hits are gathered once at the end.
 
   python bench.py --workload cls617 [--impl ours|reference]
   python bench.py --workload jobs    (reduced-T jobs through a .bbj file)
@@ -938,12 +941,22 @@ def main():
     import workloads as W
 
     torch.cuda.set_device(local)
-    lo, hi = shard.rank_band(args.band_lo, args.band_width, rank)
-    N = args.N or shard.table_N(args.band_lo, args.band_width, world)
+    # --shards S over several GPUs splits the set: every rank runs the whole
+    # band on its own range of shards (a table too large for one GPU)
+    split = args.shards > 1 and world > 1
+    if split:
+        lo, hi = args.band_lo, args.band_lo + args.band_width
+        N = args.N or math.ceil(hi / 42)
+    else:
+        lo, hi = shard.rank_band(args.band_lo, args.band_width, rank)
+        N = args.N or shard.table_N(args.band_lo, args.band_width, world)
     eng = s615.Engine(local)
     layout = {"auto": s615.LAYOUT_AUTO, "wide": s615.LAYOUT_WIDE, "packed": s615.LAYOUT_PACKED}[args.layout]
     t0 = time.perf_counter()
-    if args.shards > 1:
+    if split:
+        s_lo, s_hi = shard.shard_range(rank, world, args.shards)
+        tid = eng.build_table_shard_range(N, args.r, args.shards, s_lo, s_hi, layout)
+    elif args.shards > 1:
         tid = eng.build_table_sharded(N, args.r, args.shards, layout)
     else:
         tid = eng.build_table(N, args.r, layout)
@@ -951,7 +964,7 @@ def main():
     log(f"rank {rank}: table N={N} r={args.r} shards={args.shards} built in {build_s:.1f} s")
     units = band_units(lo, hi - 1)   # B in [lo, hi): bands of ranks do not overlap
     log(f"rank {rank}: {len(units)} units in [{lo}, {hi})")
-    plants = W.plants(N_PLANTS, 1000 + rank, lo, hi, N)
+    plants = W.plants(N_PLANTS, 1000 + (0 if split else rank), lo, hi, N)
     arr, n = W.unit_array(units, plants, N)
 
     lib = s615.lib()
@@ -994,11 +1007,13 @@ def main():
     ctr = s615.Counters()
     s615._check(lib.s615_batch_results(eng._ctx, batch, C.cast(hits, C.c_void_p), 1 << 20,
                                             C.byref(nh), C.byref(ctr)), "results")
-    # slowest rank's time, counters summed over ranks
-    total_ms, tot = shard.merge(dist, "cuda", total_ms,
-                                {"calls": ctr.calls, "gated": ctr.gated, "probes": ctr.probes,
-                                 "pos": ctr.pos, "eligible": eligible_count(lo, hi - 1)})
     harr = s615.hits_to_array(hits, nh.value)
+    counts = {"calls": ctr.calls, "gated": ctr.gated, "probes": ctr.probes, "pos": ctr.pos,
+              "eligible": eligible_count(lo, hi - 1)}
+    if split:   # slowest rank's time; the same counters on every rank; the union of the hits
+        total_ms, tot, harr = shard.merge_split(dist, "cuda", total_ms, counts, harr)
+    else:       # slowest rank's time, counters summed over ranks
+        total_ms, tot = shard.merge(dist, "cuda", total_ms, counts)
     log(f"timed {args.steps} steps: {total_ms:.1f} ms; pos={ctr.pos} probes={ctr.probes} hits={nh.value}")
     sols = eng.verify(arr, n, harr, N)
     # a plant counts when its exact planted (d, e, c1, c2) is among the verified
@@ -1089,15 +1104,19 @@ def main():
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "strong" if split else "weak",
         "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-        "config": {"workload": f"cls5 band B in [{lo}, {hi}) per rank: {len(units)} Stage-1 units + "
+        "config": {"workload": f"cls5 band B in [{lo}, {hi}){' (all ranks)' if split else ' per rank'}: "
+                               f"{len(units)} Stage-1 units + "
                                f"{N_PLANTS} plants; xor table N={N} r={args.r} built on device"
                                + (f" as {args.shards} pair-space shards" if args.shards > 1 else ""),
                    "shards": args.shards,
                    "units_per_rank": n, "N": N, "r": args.r,
                    "l2": "inputs larger than L2 (table %.1f GB)" % (eng.table_info(tid).device_bytes / 1e9),
-                   "parallelism": f"replicas-by-band x{world}"},
+                   "parallelism": (f"shard-split x{world}: each rank holds {args.shards // world}+ of "
+                                   f"{args.shards} shards and runs the whole band" if split
+                                   else f"replicas-by-band x{world}")},
         "eligible_B_per_hour": eligible * args.steps / (total_ms / 1e3) * 3600,
         "p99_unit_latency_ms": serve["p99_ms"] if serve else None,
         "p50_unit_latency_ms": serve["p50_ms"] if serve else None,

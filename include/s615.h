@@ -193,10 +193,19 @@ int s615_save_table(s615_ctx* ctx, int table_id, const char* path);
  * (the single-table cap is N <= 120,000).  A set's header has shard_count S,
  * the key and cell totals and the routing seed in mix_seed; 2 <= S <= 64.
  * s615_load_table refuses a file that is one shard of a set;
- * s615_load_table_shards takes the S files in shard order; s615_save_table
+ * s615_load_table_shards takes the files in shard order; s615_save_table
  * and s615_export_table refuse a set, s615_save_table_shard writes one shard's
  * file.  Every run and query entry point takes a set's table id. */
 int s615_build_table_sharded(s615_ctx* ctx, int N, int r, int shards, int layout, int* table_id);
+/* Shards [lo, hi) of an S-shard set only (one GPU's part when the shards of
+ * a set are split over GPUs, no counterpart in the reference): probes of keys
+ * whose shard lies outside [lo, hi) find nothing here, so every GPU runs the
+ * same units and the union of their hits is the whole set's; each GPU's
+ * counters are the whole set's. */
+int s615_build_table_shard_range(s615_ctx* ctx, int N, int r, int shards, int lo, int hi,
+                                 int layout, int* table_id);
+/* paths: consecutive shards k, k+1, .. of one set, in order (all S of them,
+ * or a range as above). */
 int s615_load_table_shards(s615_ctx* ctx, const char* const* paths, int n, int expected_N,
                            int layout, int* table_id);
 int s615_save_table_shard(s615_ctx* ctx, int table_id, int shard, const char* path);

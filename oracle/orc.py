@@ -163,10 +163,11 @@ class Table:
 
     @classmethod
     def shard_set(cls, parts, seed: int = SHARD_SEED) -> "Table":
-        """A table whose probes go to parts[mix64(key + seed) % S] (parts stay referenced)."""
-        arr = (C.c_void_p * len(parts))(*[p.h for p in parts])
+        """A table whose probes go to parts[mix64(key + seed) % S] (parts stay
+        referenced; None marks a shard held elsewhere)."""
+        arr = (C.c_void_p * len(parts))(*[p.h if p is not None else None for p in parts])
         t = cls(lib().orc_shard_set(arr, len(parts), seed))
-        t.parts = list(parts)
+        t.parts = [p for p in parts if p is not None]
         return t
 
     @classmethod

@@ -358,8 +358,10 @@ bool construct(const std::vector<u64>& keys, u32 r, u64 seed, orc_table& out) {
 u32 shard_of(u64 key, u64 seed, u32 S) { return S <= 1 ? 0u : (u32)(mix64(key + seed) % S); }
 
 bool might_contain(const orc_table& t, u64 key) {  // xor_filter.hpp:472-483
-  if (!t.parts.empty())   // residue-steered probe: one query, in the key's own shard
-    return might_contain(*t.parts[shard_of(key, t.shard_seed, (u32)t.parts.size())], key);
+  if (!t.parts.empty()) {   // residue-steered probe: one query, in the key's own shard
+    const orc_table* p = t.parts[shard_of(key, t.shard_seed, (u32)t.parts.size())];
+    return p && might_contain(*p, key);   // a shard not held here answers nothing
+  }
   if (t.hdr.n_keys == 0) return false;
   if (t.packed.empty() || t.hdr.m_cells < 3) return false;
   const u64 block = t.hdr.m_cells / 3;
@@ -607,22 +609,27 @@ orc_table* orc_build_pairs_shard(int N, int r, int S, int s, uint64_t seed) {
 }
 
 // A shard set over parts[0..S) (not owned; each part's header says which
-// shard it is).  Null unless the parts are shards 0..S-1 of one S.
+// shard it is; a null part is a shard held elsewhere, whose keys find
+// nothing here).  Null unless the parts are shards 0..S-1 of one S.
 orc_table* orc_shard_set(const orc_table* const* parts, int S, uint64_t seed) {
   if (S < 1) return nullptr;
   auto* t = new orc_table();
+  const orc_table* any = nullptr;
   for (int s = 0; s < S; ++s) {
+    t->parts.push_back(parts[s]);
+    if (!parts[s]) continue;   // a shard held elsewhere
+    any = parts[s];
     const orc_header& h = parts[s]->hdr;
     if ((int)h.shard_count != S || (int)h.shard_index != s || h.shard_mode != 0) {
       delete t;
       return nullptr;
     }
-    t->parts.push_back(parts[s]);
     t->hdr.n_keys += h.n_keys;
     t->hdr.m_cells += h.m_cells;
   }
+  if (!any) { delete t; return nullptr; }
   t->hdr.magic = kMagic; t->hdr.version = 2; t->hdr.kind = 1;
-  t->hdr.r = parts[0]->hdr.r; t->hdr.N = parts[0]->hdr.N;
+  t->hdr.r = any->hdr.r; t->hdr.N = any->hdr.N;
   t->hdr.shard_count = (u32)S;
   t->shard_seed = seed;
   return t;

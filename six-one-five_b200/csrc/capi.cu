@@ -71,16 +71,16 @@ size_t table_bytes(const DevTable& t) {
 
 // A shard set over parts (shards 0..S-1 of one N and r): header totals, the
 // parts' views uploaded for the routed probe.
-int make_set(s615_ctx* ctx, std::vector<DevTable>&& parts, DevTable* out) {
-  const u32 S = (u32)parts.size();
+int make_set(s615_ctx* ctx, std::vector<DevTable>&& parts, u32 S, u32 lo, DevTable* out) {
   DevTable t;
   t.hdr = parts[0].hdr;
   t.hdr.n_keys = 0;
   t.hdr.m_cells = 0;
   t.hdr.mix_seed = kShardSeed;   // a set's header carries the routing seed
   t.hdr.shard_count = S;
-  t.hdr.shard_index = 0;
+  t.hdr.shard_index = lo;   // the first shard held
   t.hdr.shard_mode = 0;
+  t.shard_lo = lo;
   for (const DevTable& p : parts) {
     t.hdr.n_keys += p.hdr.n_keys;
     t.hdr.m_cells += p.hdr.m_cells;
@@ -88,8 +88,8 @@ int make_set(s615_ctx* ctx, std::vector<DevTable>&& parts, DevTable* out) {
   t.layout = parts[0].layout;
   t.cell_bytes = parts[0].cell_bytes;
   t.parts = std::move(parts);
-  std::vector<TableView> views;
-  for (const DevTable& p : t.parts) views.push_back(view_of(p));
+  std::vector<TableView> views(S);   // shards not held keep an empty view
+  for (size_t i = 0; i < t.parts.size(); ++i) views[lo + i] = view_of(t.parts[i]);
   void* d = nullptr;
   int s = dev_alloc(ctx, &d, sizeof(TableView) * 64);   // S <= 64
   if (s) { free_table(ctx, t); return s; }
@@ -391,7 +391,7 @@ int s615_load_table(s615_ctx* ctx, const char* path, int expected_N, int layout,
 
 int s615_load_table_shards(s615_ctx* ctx, const char* const* paths, int n, int expected_N,
                            int layout, int* table_id) {
-  if (!ctx || !paths || n < 2 || n > 64) return S615_E_ARG;
+  if (!ctx || !paths || n < 1 || n > 64) return S615_E_ARG;
   if (serving_blocks(ctx)) return S615_E_BUSY;
   cudaSetDevice(ctx->device);
   std::vector<DevTable> parts;
@@ -401,10 +401,15 @@ int s615_load_table_shards(s615_ctx* ctx, const char* const* paths, int n, int e
     if (!paths[k]) { s = S615_E_ARG; break; }
     s = load_part(ctx, paths[k], expected_N, layout, &t);
     if (s) break;
-    // shard k of n, mode key % S, and one N and r for the whole set
+    // consecutive shards of one S (all of them, or the range a rank holds),
+    // mode key % S, and one N and r for the whole set
     const s615_header& h = t.hdr;
-    if ((int)h.shard_count != n || (int)h.shard_index != k || h.shard_mode != 0 ||
-        (k && (h.N != parts[0].hdr.N || h.r != parts[0].hdr.r))) {
+    const bool first_ok = k || (h.shard_count >= 2 && h.shard_count <= 64 &&
+                                (int)(h.shard_count - h.shard_index) >= n);
+    if (!first_ok || h.shard_mode != 0 ||
+        (k && (h.shard_count != parts[0].hdr.shard_count ||
+               h.shard_index != parts[0].hdr.shard_index + (u32)k || h.N != parts[0].hdr.N ||
+               h.r != parts[0].hdr.r))) {
       free_table(ctx, t);
       s = S615_E_FORMAT;
       break;
@@ -415,8 +420,9 @@ int s615_load_table_shards(s615_ctx* ctx, const char* const* paths, int n, int e
     for (DevTable& p : parts) free_table(ctx, p);
     return s;
   }
+  const u32 S = parts[0].hdr.shard_count, lo = parts[0].hdr.shard_index;
   DevTable set;
-  if ((s = make_set(ctx, std::move(parts), &set))) return s;
+  if ((s = make_set(ctx, std::move(parts), S, lo, &set))) return s;
   int id = 0;
   add_table(ctx, std::move(set), &id);
   if ((s = smoke_table(ctx, id))) { s615_free_table(ctx, id); return s; }
@@ -475,7 +481,7 @@ int s615_set_probe_groups(s615_ctx* ctx, int id, int groups) {
   if (serving_blocks(ctx)) return S615_E_BUSY;
   DevTable* t = find_table(ctx, id);
   if (!t) return S615_E_NOTABLE;
-  if (t->parts.empty() || groups < 0 || groups > (int)t->parts.size()) return S615_E_ARG;
+  if (t->parts.empty() || groups < 0 || groups > (int)t->parts.size()) return S615_E_ARG;   // <= shards held
   t->groups = (u32)groups;
   return S615_OK;
 }
@@ -484,9 +490,10 @@ int s615_save_table_shard(s615_ctx* ctx, int id, int shard, const char* path) {
   if (!ctx || !path) return S615_E_ARG;
   DevTable* t = find_table(ctx, id);
   if (!t) return S615_E_NOTABLE;
-  if (shard < 0 || shard >= (int)t->parts.size()) return S615_E_ARG;
+  const int i = shard - (int)t->shard_lo;   // shard numbers are the set's own
+  if (t->parts.empty() || i < 0 || i >= (int)t->parts.size()) return S615_E_ARG;
   cudaSetDevice(ctx->device);
-  return save_part(ctx, &t->parts[(size_t)shard], path);
+  return save_part(ctx, &t->parts[(size_t)i], path);
 }
 
 // One table's file: its header, then the packed cells.
@@ -531,7 +538,13 @@ int s615_build_table(s615_ctx* ctx, int N, int r, int layout, int* table_id) {
 }
 
 int s615_build_table_sharded(s615_ctx* ctx, int N, int r, int shards, int layout, int* table_id) {
-  if (!ctx || N < 1 || N > 8 * kNSoftMax || r < 8 || r > 64 || shards < 2 || shards > 64)
+  return s615_build_table_shard_range(ctx, N, r, shards, 0, shards, layout, table_id);
+}
+
+int s615_build_table_shard_range(s615_ctx* ctx, int N, int r, int shards, int lo, int hi,
+                                 int layout, int* table_id) {
+  if (!ctx || N < 1 || N > 8 * kNSoftMax || r < 8 || r > 64 || shards < 2 || shards > 64 ||
+      lo < 0 || hi > shards || lo >= hi)
     return S615_E_ARG;
   if (serving_blocks(ctx)) return S615_E_BUSY;
   cudaSetDevice(ctx->device);
@@ -547,7 +560,7 @@ int s615_build_table_sharded(s615_ctx* ctx, int N, int r, int shards, int layout
   for (int o = 0; o < 4; ++o) seeds[o] = kSeedBase + (u64)o * kPhi;
   std::vector<DevTable> parts;
   // one shard at a time: a build's scratch is sized for its shard's keys
-  for (int k = 0; k < shards && !s; ++k) {
+  for (int k = lo; k < hi && !s; ++k) {
     DevTable t;
     s = build_xor_device(ctx, static_cast<const u64*>(dv), vals.size(), nullptr, 0, r, seeds, 4, N,
                          layout == S615_LAYOUT_AUTO ? S615_LAYOUT_WIDE : layout, &t, (u32)shards,
@@ -560,7 +573,7 @@ int s615_build_table_sharded(s615_ctx* ctx, int N, int r, int shards, int layout
     return s;
   }
   DevTable set;
-  if ((s = make_set(ctx, std::move(parts), &set))) return s;
+  if ((s = make_set(ctx, std::move(parts), (u32)shards, (u32)lo, &set))) return s;
   int id = 0;
   add_table(ctx, std::move(set), &id);
   if ((s = smoke_table(ctx, id))) { s615_free_table(ctx, id); return s; }

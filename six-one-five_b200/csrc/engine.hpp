@@ -79,7 +79,8 @@ struct DevTable {
   size_t bytes = 0;
   u64 block = 0, recip = 0;
   std::vector<DevTable> parts;   // a shard set (hdr.shard_count > 1): its shards in order
-  void* d_views = nullptr;       // the parts' TableViews in HBM
+  u32 shard_lo = 0;              // parts[i] is shard shard_lo + i of hdr.shard_count
+  void* d_views = nullptr;       // one TableView per shard of the set in HBM (owned ones set)
   u32 groups = 0;                // probe passes over a set (0: from its size)
 };
 

@@ -463,9 +463,10 @@ int launch_peel(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flag
   const u32 G = tv.shards > 1 ? std::max(1u, tv.groups) : 1u;
   for (u32 g = 0; g < G; ++g) {
     TableView v = tv;
-    if (G > 1) {
-      v.grp_lo = (u32)((u64)tv.shards * g / G);
-      v.grp_hi = (u32)((u64)tv.shards * (g + 1) / G);
+    if (G > 1) {   // the g-th slice of the shards this set holds
+      const u64 n = tv.grp_hi - tv.grp_lo;
+      v.grp_lo = tv.grp_lo + (u32)(n * g / G);
+      v.grp_hi = tv.grp_lo + (u32)(n * (g + 1) / G);
     }
     if (g > 0) S615_CU(cudaMemsetAsync(b->d_work, 0, 8, st));
     const int s = launch_pass(ctx, v, b, g > 0 ? flags | kFlagNoCount : flags, st, grid_blocks);

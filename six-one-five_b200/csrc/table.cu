@@ -73,7 +73,7 @@ TableView view_of(const DevTable& t) {
   TableView v{};
   v.shards = 1;
   if (!t.parts.empty()) {   // a shard set: the parts' views live in HBM
-    v.shards = (u32)t.parts.size();
+    v.shards = t.hdr.shard_count;
     v.block = v.shards;   // the shard index is fast_mod(mix, S, recip)
     v.recip = mod_recip(v.shards);
     v.parts = static_cast<const TableView*>(t.d_views);
@@ -81,9 +81,9 @@ TableView view_of(const DevTable& t) {
     size_t bytes = 0;
     for (const DevTable& p : t.parts) bytes += p.bytes;
     const u64 want = t.groups ? t.groups : (bytes + kProbeGroupBytes - 1) / kProbeGroupBytes;
-    v.groups = (u32)std::min<u64>(std::max<u64>(want, 1), v.shards);
-    v.grp_lo = 0;
-    v.grp_hi = v.shards;
+    v.groups = (u32)std::min<u64>(std::max<u64>(want, 1), t.parts.size());
+    v.grp_lo = t.shard_lo;   // the shards this set holds; other keys are not its to probe
+    v.grp_hi = t.shard_lo + (u32)t.parts.size();
     v.r = t.hdr.r;
     v.fpmask = fp_mask(t.hdr.r);
     return v;

@@ -108,6 +108,8 @@ SIGNATURES = {
                                          C.POINTER(C.c_int)]),
     "s615_save_table_shard": (C.c_int, [_P, C.c_int, C.c_int, C.c_char_p]),
     "s615_set_probe_groups": (C.c_int, [_P, C.c_int, C.c_int]),
+    "s615_build_table_shard_range": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                               C.c_int, C.POINTER(C.c_int)]),
     "s615_export_table": (C.c_int, [_P, C.c_int, C.POINTER(Header), _P, C.c_size_t,
                                     C.POINTER(C.c_size_t)]),
     "s615_get_table_info": (C.c_int, [_P, C.c_int, C.POINTER(TableInfo)]),
@@ -458,6 +460,14 @@ class Engine:
         tid = C.c_int(0)
         _check(lib().s615_build_table_sharded(self._ctx, N, r, shards, layout, C.byref(tid)),
                "build_table_sharded")
+        return tid.value
+
+    def build_table_shard_range(self, N: int, r: int, shards: int, lo: int, hi: int,
+                                layout: int = LAYOUT_AUTO) -> int:
+        """Shards [lo, hi) of an S-shard set: one GPU's part of a set split over GPUs."""
+        tid = C.c_int(0)
+        _check(lib().s615_build_table_shard_range(self._ctx, N, r, shards, lo, hi, layout,
+                                                  C.byref(tid)), "build_table_shard_range")
         return tid.value
 
     def load_table_shards(self, paths, expected_N: int = 0, layout: int = LAYOUT_AUTO) -> int:

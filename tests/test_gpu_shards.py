@@ -207,3 +207,43 @@ def test_probe_groups_change_nothing(engine, oracle_shards, G):
             engine.set_probe_groups(mono, 2)               # a single table has no groups
     finally:
         engine.free_table(mono)
+
+
+def test_shard_ranges_split_the_set(engine, oracle_shards, tmp_path):
+    """The parts two GPUs would hold of one set, run in turn on this GPU: each
+    part gives the whole set's counters, and their raw hits together are the
+    whole set's; a part answers exactly the keys of its own shards."""
+    N = 54400 // 42
+    _, paths = oracle_shards(N, 16, 4)
+    full = engine.load_table_shards(paths, N)
+    parts = [engine.load_table_shards(paths[:2], N), engine.load_table_shards(paths[2:], N)]
+    built = engine.build_table_shard_range(N, 48, 4, 1, 3)
+    key = lambda hs: sorted(tuple(int(h[f]) for f in ("unit", "d", "e", "c4", "fp")) for h in hs)
+    fields = ("calls", "gated", "probes", "pos", "tri_total", "tri_skipped")
+    try:
+        units = list(s615.make_units(W.cls5_units(54301, 54400))[0])
+        c7, n7 = s615.candidates617(54347)
+        units += [c7[i] for i in range(n7)]
+        arr = (s615.Unit * len(units))(*units)
+        hf, cf = engine.run(full, arr, len(units))
+        union = []
+        for tid, lo in zip(parts, (0, 2)):
+            info = engine.table_info(tid)
+            assert (info.hdr.shard_count, info.hdr.shard_index) == (4, lo)
+            h, c = engine.run(tid, arr, len(units))
+            assert tuple(getattr(c, f) for f in fields) == tuple(getattr(cf, f) for f in fields)
+            union += key(h)
+        assert sorted(union) == key(hf) and len(union) > 0
+        keys = pair_keys(N)
+        owner = np.array([orc.shard_of(int(k), 4) for k in keys])
+        for tid, lo in zip(parts + [built], (0, 2, 1)):
+            got = engine.query(tid, keys).astype(bool)
+            mine = (owner >= lo) & (owner < lo + 2)
+            assert got[mine].all() and not got[~mine].any()
+        engine.save_table_shard(built, 2, str(tmp_path / "s2.bin"))
+        assert orc.Table.load(str(tmp_path / "s2.bin"), N).header.shard_index == 2
+        with pytest.raises(s615.S615Error):
+            engine.save_table_shard(built, 0, str(tmp_path / "s0.bin"))   # not held here
+    finally:
+        for tid in [full, built] + parts:
+            engine.free_table(tid)
