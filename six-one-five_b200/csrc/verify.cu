@@ -102,14 +102,24 @@ int verify_device(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s
                   size_t n_hits, int N, s615_solution* out, size_t cap, size_t* n_out) {
   *n_out = 0;
   if (n_hits == 0) return S615_OK;
-  std::vector<DevUnit> du(n_units);
-  for (size_t i = 0; i < n_units; ++i) {
-    bool skip = false;
-    const int s = make_dev_unit(units[i], (u32)i, &du[i], &skip);
-    if (s && !skip) std::memset(&du[i], 0, sizeof du[i]);
-  }
   for (size_t i = 0; i < n_hits; ++i)
     if (hits[i].unit >= n_units) return S615_E_ARG;
+  // Device records for the units that have hits only (a batch can hold
+  // millions of units and a handful of hits); the kernel's copy of the hits
+  // indexes that short list, the host tail below keeps the caller's indices.
+  std::vector<u32> ids(n_hits);
+  for (size_t i = 0; i < n_hits; ++i) ids[i] = hits[i].unit;
+  std::sort(ids.begin(), ids.end());
+  ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+  std::vector<DevUnit> du(ids.size());
+  for (size_t k = 0; k < ids.size(); ++k) {
+    bool skip = false;
+    const int s = make_dev_unit(units[ids[k]], ids[k], &du[k], &skip);
+    if (s && !skip) std::memset(&du[k], 0, sizeof du[k]);
+  }
+  std::vector<s615_hit> kh(hits, hits + n_hits);
+  for (s615_hit& h : kh)
+    h.unit = (u32)(std::lower_bound(ids.begin(), ids.end(), h.unit) - ids.begin());
   const u32 pcap = (u32)std::min<size_t>(std::max<size_t>(4 * n_hits + 64, 1024), 1u << 26);
   // scratch from the context's grow-only arena: no cudaFree, so no
   // device-wide sync against kernels running on other streams
@@ -126,7 +136,7 @@ int verify_device(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s
   {
     const u128 inv = inv_2adic_u128((u128)kM21);
     cudaError_t e = cudaMemcpyAsync(d_u, du.data(), bu, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_h, hits, bh, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_h, kh.data(), bh, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_n, 0, 16, st);
     if (e == cudaSuccess) {
       const u32 blocks = (u32)std::min<size_t>((n_hits + 7) / 8, (size_t)ctx->num_sms * 32);
