@@ -614,6 +614,10 @@ def run_mix(args, rank, world, local, dist):
     ctr = s615.Counters()
     s615._check(lib.s615_batch_results(eng._ctx, batch, C.cast(hits, C.c_void_p), 1 << 20,
                                        C.byref(nh), C.byref(ctr)), "results")
+    sms, sctr = timed_steps(lib, eng, tid, batch, stream, s615.F_SHARP, 1)
+    sharp = {"ms_per_step": sms, "units_per_s": n / (sms / 1e3), "post_gate_probes": sctr.probes,
+             "speedup_vs_default": (ms / args.steps) / sms,
+             "flag": "S615_F_SHARP (extra sound residue tests; raw hits a subset)"}
     sols = eng.verify(arr, n, s615.hits_to_array(hits, nh.value), N, cap=65536)
     k5 = len(units)
     got5 = {(s.unit, s.d, s.e, s.c1, s.c2) for s in sols if s.kind == 1 and s.cls == 5}
@@ -642,7 +646,8 @@ def run_mix(args, rank, world, local, dist):
             "table_build_s": round(build_s, 2),
             "e2e": {"value": n / e2e_s, "unit": "units/s", "h2d_bytes_per_step": batch_h2d(lib, batch),
                     "d2h_bytes_per_step": C.sizeof(s615.Counters) + len(h2) * C.sizeof(s615.Hit)},
-            "gpu_launches": launches, "roofline": None, "cpu_baseline": None, "clocks": cl}
+            "gpu_launches": launches, "roofline": None, "cpu_baseline": None,
+            "sharp_gate": sharp, "clocks": cl}
     s615._check(lib.s615_batch_free(eng._ctx, batch), "batch_free")
     eng.close()
     if rank == 0:
@@ -721,6 +726,10 @@ def run_jobs(args, rank, world, local, dist):
     ctr = s615.Counters()
     s615._check(lib.s615_batch_results(eng._ctx, batch, C.cast(hits, C.c_void_p), 1 << 20,
                                        C.byref(nh), C.byref(ctr)), "results")
+    sms, sctr = timed_steps(lib, eng, tid, batch, stream, s615.F_SHARP, 1)
+    sharp = {"ms_per_step": sms, "jobs_per_s": n / (sms / 1e3), "post_gate_probes": sctr.probes,
+             "speedup_vs_default": (total_ms / args.steps) / sms,
+             "flag": "S615_F_SHARP (extra sound residue tests; raw hits a subset)"}
     sols = eng.verify(jobs, n, s615.hits_to_array(hits, nh.value), N, cap=65536)
     h2d = batch_h2d(lib, batch)
     s615._check(lib.s615_batch_free(eng._ctx, batch), "batch_free")
@@ -804,7 +813,7 @@ def run_jobs(args, rank, world, local, dist):
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs (burst)",
                          "traffic": None, "algorithmic_bytes_per_launch": ctr.probes * PROBE_BYTES},
-            "cpu_baseline": cpu, "clocks": cl}
+            "cpu_baseline": cpu, "sharp_gate": sharp, "clocks": cl}
     eng.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -297,13 +297,12 @@ int s615_unit_status(const s615_unit* unit);
 #define S615_F_NO_GATE 1u     /* --no-gate: probe every R>0 point */
 #define S615_F_PLAIN 2u       /* one unit per launch + sync (the plain form) */
 #define S615_F_NO_TRI 4u      /* cls 7: --no-tri-gate, every c4 of the window */
-/* Sharper sound gate (no counterpart in the reference): for cls 5 and cls 7
- * units the peel also requires the point value to be a sum of two sixth
- * powers mod 64, 27, 49, 31, 37 and 43.  Every true pair sum passes, so the
- * verified solutions are the same; the raw hits are a subset of the default
- * run's (the filter's false positives at rejected points are not probed) and
- * calls/gated/probes count the sharper gate.  Ignored with S615_F_NO_GATE;
- * cls 2-4 units run the reference gate. */
+/* Sharper sound gate (no counterpart in the reference): for every unit kind
+ * the peel also requires the point value to be a sum of two sixth powers mod
+ * 64, 27, 49, 31, 37 and 43.  Every true pair sum passes, so the verified
+ * solutions are the same; the raw hits are a subset of the default run's
+ * (the filter's false positives at rejected points are not probed) and
+ * calls/gated/probes count the sharper gate.  Ignored with S615_F_NO_GATE. */
 #define S615_F_SHARP 8u
 
 /* The peel of a mixed batch of units (classes 2-5 and 7) in one persistent

@@ -70,6 +70,7 @@ struct PeelParams {
   Cls5Counters* ctr;
   const u32* pat5;         // cls5 column patterns (step 64, scale 64)
   const u32* pat3;         // find3 column patterns (step 1, scale 1)
+  const u32* pat3s;        // sharp gate: find3 column patterns in HBM (read through L1)
   u64 inv21_lo, inv21_hi;  // (21^6)^-1 mod 2^128
   u32 s8;                  // admissible values mod 8, as a bitmask
   u64 p64;                 // sharp gate: admissible values mod 64, as a bitmask
@@ -338,7 +339,17 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
             }
             R.a = lo;
             R.b = len | (m4 << 28);
-            set_offsets(R);
+            if constexpr (kSharp) {   // q = 27, 49, 13, 19, 31, 37, 43 and T - c^6 mod 64
+              set_offsets_sharp(R, W.offx[r]);
+              u32 m32 = 0;
+              for (u32 i = 0; i < 32; ++i) {
+                const u32 t = ((u32)R.wlo - pow6_mod4096(lo + i)) & 63u;
+                m32 |= (u32)((P.p64 >> t) & 1ull) << i;
+              }
+              W.M32[0][r] = m32;
+            } else {
+              set_offsets(R);
+            }
             my_calls += len;
             my_pos += len;
           }
@@ -358,7 +369,11 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
           len = R.b & kLenMask;
           if (kbase < len) {
             const u32 xs = R.a + kbase;
-            m = ((R.b >> 28) * 0x11111111u) & gate_word(s_pat3, R, xs % 9, xs % 7, xs % 13, xs % 19);
+            if constexpr (kSharp)   // T - c^6 mod 64 has period 32 in c: one mask per row
+              m = W.M32[0][rr] & gate_word(P.pat3s, R, xs % 27, xs % 49, xs % 13, xs % 19) &
+                  gate_word3(P.pat3s, W.offx[rr], xs % 31, xs % 37, xs % 43);
+            else
+              m = ((R.b >> 28) * 0x11111111u) & gate_word(s_pat3, R, xs % 9, xs % 7, xs % 13, xs % 19);
             const u32 n = len - kbase;
             if (n < 32u) m &= (1u << n) - 1u;
           }
@@ -418,6 +433,7 @@ int launch_main(s615_ctx* ctx, const TableView& tv, const s615_batch* b, size_t 
   P.p64 = ctx->p64;
   P.count = (flags & kFlagNoCount) ? 0u : 1u;
   P.pat3 = ctx->d_pat + 2 * kPatWords + (gated ? 0 : kPatWords);
+  P.pat3s = ctx->d_sharp + kSharpWords;
   const u128 inv = inv_2adic_u128((u128)kM21);
   P.inv21_lo = (u64)inv;
   P.inv21_hi = (u64)(inv >> 64);

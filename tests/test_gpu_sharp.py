@@ -3,7 +3,7 @@
 It adds sound residue tests (sums of two sixth powers mod 64, 27, 49, 31, 37,
 43), so against the default run on the same units: the same in-range and R>0
 point counts, fewer probes, raw hits a subset, and exactly the same verified
-solutions and recovered plants.  cls 2-4 units are not affected.
+solutions and recovered plants, for every unit kind.
 """
 import numpy as np
 import pytest
@@ -109,18 +109,34 @@ def test_sharp_617_plants(engine):
         engine.free_table(tid)
 
 
-def test_sharp_leaves_cls234_alone(engine, oracle_table):
+def test_sharp_cls234_and_jobs(engine, oracle_table):
+    """Find3 rows (classes 2-4, reduced-T jobs, find2 jobs) take the sharper
+    gate too: fewer probes, raw hits a subset, the same verified results."""
     N = 2000
     _, path = oracle_table(N, 16)
     tid = engine.load_table(path, N)
     try:
         units = [(c, B, u) for B in range(400000, 400600) if W.eligible(B)
                  for c in (2, 3, 4) for u in s615.unit_candidates(B, c)]
-        arr = (s615.Unit * len(units))()
-        for i, (c, B, u) in enumerate(units):
-            arr[i].cls, arr[i].B, arr[i].u = c, B, u
-        (h0, c0, s0), (h1, c1, s1) = both(engine, tid, arr, len(units), N)
-        assert (c1.calls, c1.probes) == (c0.calls, c0.probes)
-        assert hit_set(h1) == hit_set(h0) and s1 == s0
+        p24 = W.plants234(12, 8, 400000, 400600, N)
+        arr0, n0 = W.mixed_unit_array(units, [], p24, N)
+        rows = [arr0[i] for i in range(n0)]
+        rng = np.random.RandomState(3)
+        for k in range(30):   # planted jobs: find2, find3 and find4
+            m = (2, 3, 4)[k % 3]
+            c = sorted(int(x) for x in rng.choice(np.arange(1, N + 1), m, replace=False))
+            cls = {2: 5, 3: 2 + (k // 3) % 3, 4: 1}[m]
+            rows.append(s615.make_job(cls, 999999 - k, 1, sum(x**6 for x in c), 1, 1, lim=N))
+        for c, B, u in [(4, 400003, s615.unit_candidates(400003, 4)[0]),
+                        (5, *W.cls5_units(100001, 100100)[0])]:
+            a, k, _ = s615.expand_unit(B, u, c)
+            rows += [a[i] for i in range(min(k, 4000))]
+        arr = (s615.Unit * len(rows))(*rows)
+        (h0, c0, s0), (h1, c1, s1) = both(engine, tid, arr, len(rows), N)
+        assert (c1.calls, c1.pos) == (c0.calls, c0.pos)
+        assert c1.probes < c0.probes / 4
+        assert hit_set(h1) <= hit_set(h0) and s1 == s0
+        assert sum(1 for x in s0 if x[1] == 1) >= len(p24)                  # plants
+        assert sum(1 for x in s0 if x[1] == s615.S615_KIND_JOB) >= 30        # planted jobs
     finally:
         engine.free_table(tid)
