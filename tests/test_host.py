@@ -105,3 +105,13 @@ def test_cli_built_and_selftest():
     r = subprocess.run([cli, "--selftest-host"], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "PASS" in r.stdout
+
+
+def test_band_unit_count_equals_reference_campaign():
+    # the reference's 4.5M -> 5.0M class-5 campaign ran units=5765343 (its README's
+    # coverage table); both band ends are even, so the count is the same for
+    # open or closed bounds.  The engine's host rule and the oracle's both give it.
+    import workloads as W
+    assert len(W.cls5_units(4_500_000, 5_000_000)) == 5_765_343
+    assert sum(len(orc.unit_candidates(B, 5)) for B in range(4_500_001, 5_000_000, 2)
+               if B % 3 and B % 7) == 5_765_343
