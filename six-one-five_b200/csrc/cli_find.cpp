@@ -6,7 +6,8 @@
 // find2 / find3 / find4 jobs on an N = 40 table, :808-892) and
 // --selftest-host.  The search runs on the engine (s615_run + s615_verify
 // with kind 2 units).  Extra flags: --load-table F (a table file instead of
-// the device build) and --emit-jobs F (with --units: write the expanded jobs
+// the device build), --shards S / --load-shards F0,F1,.. (a pair-space shard
+// set, past the single-table cap) and --emit-jobs F (with --units: write the expanded jobs
 // as a .bbj or text job file instead of searching, the hunt tool's
 // --expand --emit, fourcore_hunt_v3.cpp:347-447).  The per-batch "[gate]"
 // line counts a whole engine batch (every find mode together).
@@ -22,6 +23,15 @@
 namespace {
 
 constexpr int kNSoftMax = 120000;   // kXorNSoftMax of the reference's store
+constexpr int kNShardMax = 240000;  // with pair-space shards, as HBM allows
+
+// Table options beyond the reference's: a file, or a pair-space shard set
+// (built on the device, or loaded from its shard files in order).
+struct TableOpts {
+  std::string load;
+  int shards = 1;
+  std::vector<std::string> shard_files;
+};
 
 void usage() {
   std::printf(
@@ -31,6 +41,7 @@ void usage() {
       "   or: s615_find --units FILE.buc --emit-jobs FILE.bbj|FILE.but [--max-expand N]\n"
       " options: --N n --r BITS (xor rank, default 48) --batch N --max-expand N\n"
       "          --max-table-gb G (ignored) --S (ignored) --load-table F\n"
+      "          --shards S | --load-shards F0,F1,.. (pair-space shard set; N <= 240000)\n"
       "          --quiet --no-quiet --no-gate --stop-first --device K\n"
       "  .buc: cls B u\n"
       "  .but: ASCII jobs | .bbj: binary jobs (36 B/job; streamed)\n");
@@ -87,15 +98,23 @@ struct Run {
   }
 };
 
-bool start(Run& R, int device, int N, int r, const std::string& load) {
+bool start(Run& R, int device, int N, int r, const TableOpts& T) {
   int s = s615_open(device, 0, &R.ctx);
   if (s) {
     std::fprintf(stderr, "[find] cannot open device %d: %s\n", device, s615_strerror(s));
     return false;
   }
   R.N = N;
-  s = load.empty() ? s615_build_table(R.ctx, N, r, S615_LAYOUT_WIDE, &R.tid)
-                   : s615_load_table(R.ctx, load.c_str(), N, S615_LAYOUT_WIDE, &R.tid);
+  if (!T.shard_files.empty()) {
+    std::vector<const char*> paths;
+    for (const auto& f : T.shard_files) paths.push_back(f.c_str());
+    s = s615_load_table_shards(R.ctx, paths.data(), (int)paths.size(), N, S615_LAYOUT_WIDE, &R.tid);
+  } else if (T.shards > 1) {
+    s = s615_build_table_sharded(R.ctx, N, r, T.shards, S615_LAYOUT_WIDE, &R.tid);
+  } else {
+    s = T.load.empty() ? s615_build_table(R.ctx, N, r, S615_LAYOUT_WIDE, &R.tid)
+                       : s615_load_table(R.ctx, T.load.c_str(), N, S615_LAYOUT_WIDE, &R.tid);
+  }
   if (s) {
     std::fprintf(stderr, "[find] FATAL: xor table: %s\n", s615_strerror(s));
     return false;
@@ -114,7 +133,7 @@ int selftest_gpu(int device) {
   const int N = 40;
   Run R;
   R.quiet = true;
-  if (!start(R, device, N, 48, "")) return 1;
+  if (!start(R, device, N, 48, TableOpts{})) return 1;
   auto p6 = [](unsigned long long x) { return x * x * x * x * x * x; };
   struct Plant { int mode; uint32_t cls; uint64_t B; uint32_t f1, f2; unsigned long long T; };
   const Plant plants[3] = {
@@ -171,7 +190,8 @@ bool load_buc(const char* path, std::vector<s615_unit>& units) {
 int main(int argc, char** argv) {
   std::setvbuf(stdout, nullptr, _IOLBF, 0);
   std::setvbuf(stderr, nullptr, _IOLBF, 0);
-  std::string units_path, jobs_path, load, emit;
+  std::string units_path, jobs_path, emit;
+  TableOpts topt;
   int N = 0, device = 0, r = 48, quiet_flag = -1;
   unsigned long long max_expand = 0, batch = 1ULL << 20;
   bool use_gate = true, stop_first = false, do_host = false, do_gpu = false;
@@ -192,7 +212,19 @@ int main(int argc, char** argv) {
     else if (a == "--no-gate") use_gate = false;
     else if (a == "--stop-first") stop_first = true;
     else if (a == "--device") device = std::atoi(next().c_str());
-    else if (a == "--load-table") load = next();
+    else if (a == "--load-table") topt.load = next();
+    else if (a == "--shards") topt.shards = std::atoi(next().c_str());
+    else if (a == "--load-shards") {
+      const std::string v = next();
+      size_t p = 0;
+      while (p <= v.size()) {
+        const size_t q = v.find(',', p);
+        const std::string f = v.substr(p, q == std::string::npos ? std::string::npos : q - p);
+        if (!f.empty()) topt.shard_files.push_back(f);
+        if (q == std::string::npos) break;
+        p = q + 1;
+      }
+    }
     else if (a == "--emit-jobs") emit = next();
     else if (a == "-h" || a == "--help") { usage(); return 0; }
     else { std::fprintf(stderr, "unknown arg %s\n", a.c_str()); usage(); return 1; }
@@ -206,6 +238,11 @@ int main(int argc, char** argv) {
   }
   if (do_gpu) return selftest_gpu(device);
   if (r < 8 || r > 64) { std::fprintf(stderr, "--r must be 8..64\n"); return 1; }
+  if (topt.shards != 1 && (topt.shards < 2 || topt.shards > 64)) {
+    std::fprintf(stderr, "--shards must be 2..64\n");
+    return 1;
+  }
+  const int n_cap = (topt.shards > 1 || !topt.shard_files.empty()) ? kNShardMax : kNSoftMax;
   if (batch < 1) batch = 1;
   if (batch > (1ULL << 24)) batch = 1ULL << 24;
   const bool quiet = quiet_flag == 1;
@@ -245,12 +282,12 @@ int main(int argc, char** argv) {
       for (const auto& J : all) need = std::max(need, job_lim(J));
       if (N <= 0 || N < (int)need) N = (int)need;
     }
-    if (N > kNSoftMax) {
-      std::fprintf(stderr, "[fatal] N=%d exceeds soft xor cap %d\n", N, kNSoftMax);
+    if (N > n_cap) {
+      std::fprintf(stderr, "[fatal] N=%d exceeds soft xor cap %d\n", N, n_cap);
       if (f) s615_jobs_close(f, nullptr);
       return 1;
     }
-    if (!start(R, device, N, r, load)) { if (f) s615_jobs_close(f, nullptr); return 1; }
+    if (!start(R, device, N, r, topt)) { if (f) s615_jobs_close(f, nullptr); return 1; }
     if (info.binary) {
       std::fprintf(stderr, "[bbj] stream %s n_jobs=%llu B=[%u,%u]\n", jobs_path.c_str(),
                    (unsigned long long)info.n_jobs, info.min_B, info.max_B);
@@ -303,15 +340,15 @@ int main(int argc, char** argv) {
     uint32_t need = 0;
     for (const auto& U : units) need = std::max(need, (uint32_t)((U.B > 0 ? U.B - 1 : 0) / 42));
     if (N <= 0 || N < (int)need) N = (int)need;
-    if (N > kNSoftMax) {
-      std::fprintf(stderr, "[fatal] N=%d exceeds soft xor cap %d\n", N, kNSoftMax);
+    if (N > n_cap) {
+      std::fprintf(stderr, "[fatal] N=%d exceeds soft xor cap %d\n", N, n_cap);
       return 1;
     }
     const bool emitting = !emit.empty();
     if (!emitting) {
       std::fprintf(stderr, "[units] %zu from %s — stream-expand (max_expand=%llu) N=%d\n", units.size(),
                    units_path.c_str(), max_expand, N);
-      if (!start(R, device, N, r, load)) return 1;
+      if (!start(R, device, N, r, topt)) return 1;
     }
     std::vector<s615_unit> pending, emitted, tmp;
     bool cap = false, bad = false;

@@ -219,3 +219,20 @@ def test_cli_selftest_gpu():
     for mode in (2, 3, 4):
         assert re.search(rf"find{mode} plant exact_hits=1 ", p.stdout), p.stdout
     assert "[selftest-gpu] PASS (exact=3)" in p.stdout
+
+
+def test_cli_jobs_on_a_shard_set(tmp_path, band):
+    # the same job file against one table and against a 3-shard set: same lines
+    arr, _, _, n_real, _, N = band
+    path = str(tmp_path / "j.bbj")
+    s615.jobs_write(path, arr, n_real)
+    gate_re = re.compile(r"\[gate\] batch n=\d+ calls=(\d+) gated=(\d+) probes=(\d+)")
+    outs = []
+    for extra in ([], ["--shards", "3"]):
+        p = subprocess.run([FIND, "--jobs", path, "--r", "16", "--batch", "50000"] + extra,
+                           capture_output=True, text=True, timeout=600)
+        assert p.returncode == 0, p.stderr
+        g = [tuple(int(x) for x in m.groups()) for m in gate_re.finditer(p.stderr)]
+        sols = sorted(l for l in p.stdout.splitlines() if l.startswith("SOLUTION"))
+        outs.append((DONE.search(p.stdout).groups(), tuple(map(sum, zip(*g))), sols))
+    assert outs[0] == outs[1]

@@ -140,3 +140,37 @@ def test_sharp_cls234_and_jobs(engine, oracle_table):
         assert sum(1 for x in s0 if x[1] == s615.S615_KIND_JOB) >= 30        # planted jobs
     finally:
         engine.free_table(tid)
+
+
+def test_sharp_find4_kinds(engine, oracle_table):
+    """Class-1 find4 units and plants, and (6,1,7) classes 1-4 jobs with their
+    known identities, through the sharp gate: same tri counts and points,
+    fewer probes, raw hits a subset, the same verified lines."""
+    N = 40000 // 42
+    _, path = oracle_table(N, 16)
+    tid = engine.load_table(path, N)
+    try:
+        rows = []
+        for B in (24329, 28121, 32105, 33365):                 # class-1 units
+            for u in s615.unit_candidates(B, 1):
+                U = s615.Unit()
+                U.cls, U.B, U.u = 1, B, u
+                rows.append(U)
+        rng = np.random.RandomState(12)
+        for _ in range(16):                                    # class-1 plants
+            c = sorted(int(x) for x in rng.choice(np.arange(1, N + 1), 4, replace=False))
+            rows.append(s615.make_plant1(c, N, B=42 * N + 1))
+        for B, cls in ((34781, 4), (38191, 4), (39779, 3), (34763, 2)):   # (6,1,7) jobs
+            a, k = s615.jobs617(B, cls)
+            rows += [a[i] for i in range(k)]
+        arr = (s615.Unit * len(rows))(*rows)
+        (h0, c0, s0), (h1, c1, s1) = both(engine, tid, arr, len(rows), N)
+        assert (c1.tri_total, c1.tri_skipped, c1.pos) == (c0.tri_total, c0.tri_skipped, c0.pos)
+        assert c1.probes < c0.probes
+        assert hit_set(h1) <= hit_set(h0) and s1 == s0
+        lines = [s615.solution_line(s) for s in engine.verify(arr, len(rows), h1, N)]
+        for B in (34781, 38191, 39779):
+            assert any(f"B={B} " in l and l.startswith("SOLUTION") for l in lines), B
+        assert sum(l.startswith("PLANT cls=1") for l in lines) >= 16
+    finally:
+        engine.free_table(tid)
