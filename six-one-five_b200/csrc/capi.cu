@@ -712,12 +712,17 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
   if (const int s = pack_units(units, n, dp, &nd)) return s;
   const DevUnit* du = dp.get();
   std::vector<u64> items617;   // the (6,1,7) kernel's items go after the others
+  // Job rows per item: up to 64, fewer when the batch is small, so that its
+  // items still fill the GPU (about 64 warps per SM).
+  u32 job_rows = 8;
+  while (job_rows < kJobRows && (u64)job_rows * ctx->num_sms * 64 < nd) job_rows *= 2;
   for (size_t k = 0; k < nd; ++k) {
     const DevUnit& d = du[k];
     // classes 1, 7 and 8 (c4 windows) run in the second kernel
     unit_items(d, (u32)k,
                (d.cls == S615_CLS_617 || d.cls == 1 || d.cls == S615_CLS_617_FIND4) ? items617
-                                                                                : b->host_items);
+                                                                                : b->host_items,
+               job_rows);
   }
   // heaviest first: a candidate's first rows (smallest d) have the largest T
   // and windows, so every candidate's chunk 0 goes out before any chunk 1

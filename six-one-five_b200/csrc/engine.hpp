@@ -256,7 +256,8 @@ int free_factor(int cls);
 // cannot search exactly.
 int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip);
 // Work items of one packed unit (appended to out).
-void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out);
+// Job rows are grouped up to job_rows (<= kJobRows) per item.
+void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out, u32 job_rows = kJobRows);
 
 void gate_patterns(bool gated, int shape, u32 out[kPatWords]);
 void tri_tables(u32 out[kTriWords]);

@@ -684,13 +684,13 @@ int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip) {
   return S615_OK;
 }
 
-void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out) {
+void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out, u32 job_rows) {
   if (d.cls == kClsJobRow) {   // runs of up to kJobRows consecutive job rows of one kind
     const u32 kind = d.w != 0 ? kJobFind2 : 0u;
     if (!out.empty()) {
       const u64 last = out.back();
       if (item_res(last) == kJobItemTag && (item_chunk(last) & kJobFind2) == kind &&
-          item_unit(last) + job_count(last) == unit_index && job_count(last) < kJobRows) {
+          item_unit(last) + job_count(last) == unit_index && job_count(last) < job_rows) {
         out.back() = last + 1;
         return;
       }
