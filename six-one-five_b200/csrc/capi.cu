@@ -716,13 +716,32 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
   // items still fill the GPU (about 64 warps per SM).
   u32 job_rows = 8;
   while (job_rows < kJobRows && (u64)job_rows * ctx->num_sms * 64 < nd) job_rows *= 2;
+  // Rows per class 2-5 item: 64, or 32 / 16 when a batch would otherwise
+  // have fewer items than about 40 warps per SM (a small serving batch).
+  const u64 want_items = (u64)ctx->num_sms * 40;
+  u32 unit_rows = kItemRows;
+  while (unit_rows > 16) {
+    u64 items = 0;
+    for (size_t k = 0; k < nd && items < want_items; ++k) {
+      const DevUnit& d = du[k];
+      if (d.cls < 2 || d.cls > 5) continue;
+      for (u32 ir = 0; ir < d.nres1; ++ir) {
+        u32 jmin = 0, jend = 0;
+        class_rows(d.res1[ir], d.mod1, d.fmax1, &jmin, &jend);
+        if (jend > jmin) items += (jend - jmin + unit_rows - 1) / unit_rows;
+      }
+    }
+    if (items >= want_items) break;
+    unit_rows /= 2;
+  }
+  b->item_rows = unit_rows;
   for (size_t k = 0; k < nd; ++k) {
     const DevUnit& d = du[k];
     // classes 1, 7 and 8 (c4 windows) run in the second kernel
     unit_items(d, (u32)k,
                (d.cls == S615_CLS_617 || d.cls == 1 || d.cls == S615_CLS_617_FIND4) ? items617
                                                                                 : b->host_items,
-               job_rows);
+               job_rows, unit_rows);
   }
   // heaviest first: a candidate's first rows (smallest d) have the largest T
   // and windows, so every candidate's chunk 0 goes out before any chunk 1
@@ -820,6 +839,7 @@ int s615_run_batch(s615_ctx* ctx, int id, s615_batch* b, unsigned flags, void* s
   one.hit_cap = b->hit_cap;
   one.d_ctr = b->d_ctr;
   one.d_work = b->d_work;
+  one.item_rows = b->item_rows;
   size_t i = 0;
   while (i < b->n_items) {
     size_t j = i;

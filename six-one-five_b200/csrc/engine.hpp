@@ -153,6 +153,7 @@ struct s615_batch {
   size_t cap_units = 0, cap_items = 0;   // device capacity (a reused batch only grows)
   s615::Cls5Counters* d_ctr = nullptr;
   s615::u32* d_work = nullptr;   // persistent-queue cursors [classes 2-5, cls 7]
+  s615::u32 item_rows = s615::kItemRows;   // rows per class 2-5 item (smaller for small batches)
   std::vector<s615::u64> host_items;
 };
 
@@ -256,8 +257,10 @@ int free_factor(int cls);
 // cannot search exactly.
 int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip);
 // Work items of one packed unit (appended to out).
-// Job rows are grouped up to job_rows (<= kJobRows) per item.
-void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out, u32 job_rows = kJobRows);
+// Job rows are grouped up to job_rows (<= kJobRows) per item; the row chunks
+// of classes 2-5 have unit_rows (<= kItemRows) rows each.
+void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out, u32 job_rows = kJobRows,
+                u32 unit_rows = kItemRows);
 
 void gate_patterns(bool gated, int shape, u32 out[kPatWords]);
 void tri_tables(u32 out[kTriWords]);

@@ -684,7 +684,8 @@ int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip) {
   return S615_OK;
 }
 
-void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out, u32 job_rows) {
+void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out, u32 job_rows,
+                u32 unit_rows) {
   if (d.cls == kClsJobRow) {   // runs of up to kJobRows consecutive job rows of one kind
     const u32 kind = d.w != 0 ? kJobFind2 : 0u;
     if (!out.empty()) {
@@ -703,7 +704,7 @@ void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out, u32 job
     for (u32 c = 0; c < n; ++c) out.push_back(make_item(unit_index, 0, c));
     return;
   }
-  const u32 per = item_rows(d.cls);
+  const u32 per = d.cls == (u32)S615_CLS_617 ? item_rows(d.cls) : unit_rows;
   for (u32 ir = 0; ir < d.nres1; ++ir) {
     u32 jmin = 0, jend = 0;
     class_rows(d.res1[ir], d.mod1, d.fmax1, &jmin, &jend);

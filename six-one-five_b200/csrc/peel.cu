@@ -75,6 +75,7 @@ struct PeelParams {
   u32 s8;                  // admissible values mod 8, as a bitmask
   u64 p64;                 // sharp gate: admissible values mod 64, as a bitmask
   u32 count;               // add this launch's counters (0 for a repeat pass over a set)
+  u32 item_rows;           // rows per item of the batch (<= kRows)
 };
 
 // cls5 pattern words (sharp or not) then the find3 ones, then the warp slices
@@ -197,8 +198,8 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
       I.mod = U->mod1;
       u32 jmin, jend;
       class_rows(I.r0, I.mod, U->fmax1, &jmin, &jend);
-      I.j0 = jmin + item_chunk(packed) * kRows;
-      nrows = min(kRows, jend - I.j0);
+      I.j0 = jmin + item_chunk(packed) * P.item_rows;
+      nrows = min(P.item_rows, jend - I.j0);
     }
     u32 head = 0, qlen = 0;
     __syncwarp();
@@ -231,9 +232,8 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
         __syncwarp();
         // per (row, d residue): in-row limit and the mod-8 row mask
         u32 kmax = 0;
-        for (u32 idx = lane; idx < nd * kRows; idx += 32) {
-          const u32 di = idx / kRows, r = idx % kRows;
-          if (r >= nrows) continue;
+        for (u32 idx = lane; idx < nd * nrows; idx += 32) {   // the item's rows only
+          const u32 di = idx / nrows, r = idx - di * nrows;
           const u32 d0 = W.d0s[di];
           const RowRec& R = W.rows[r];
           const u32 kcap = (d0 <= fmax2) ? (fmax2 - d0) / 64u + 1u : 0u;
@@ -432,6 +432,7 @@ int launch_main(s615_ctx* ctx, const TableView& tv, const s615_batch* b, size_t 
   P.pat5 = kSharp ? ctx->d_sharp : ctx->d_pat + (gated ? 0 : kPatWords);
   P.p64 = ctx->p64;
   P.count = (flags & kFlagNoCount) ? 0u : 1u;
+  P.item_rows = b->item_rows ? std::min(b->item_rows, kRows) : kRows;
   P.pat3 = ctx->d_pat + 2 * kPatWords + (gated ? 0 : kPatWords);
   P.pat3s = ctx->d_sharp + kSharpWords;
   const u128 inv = inv_2adic_u128((u128)kM21);
