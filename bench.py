@@ -1098,6 +1098,19 @@ def main():
 
     # per-unit latency through the serving loop under a config-5-like stream
     serve = None
+    tune = None
+    if rank == 0 and not args.no_plain:
+        # the autotuner on a request-sized and a mid-sized sample of the band
+        # (its choices are forgotten again: the numbers above use the default rule)
+        tune = []
+        for k in (64, 1024):
+            idx = np.linspace(0, len(units) - 1, k).astype(int)
+            sarr, sn = W.unit_array([units[i] for i in idx], [], N)
+            table, best = eng.autotune(tid, sarr, sn)
+            tune.append({"units": k, "best": {"item_rows": best[0], "blocks_per_sm": best[1],
+                                              "ms": round(best[2], 3)},
+                         "trials": [[r, b, round(ms, 3)] for r, b, ms in table]})
+        eng.tune_reset()
     if rank == 0 and not args.no_plain:
         serve = serve_latency(eng, tid, units, N)
         log(f"serving: p50 {serve['p50_ms']:.1f} ms, p99 {serve['p99_ms']:.1f} ms per unit")
@@ -1130,6 +1143,7 @@ def main():
         "p99_unit_latency_ms": serve["p99_ms"] if serve else None,
         "p50_unit_latency_ms": serve["p50_ms"] if serve else None,
         "serving": serve,
+        "autotune": tune,
         "counters": {"calls": tot["calls"], "gated": tot["gated"], "probes": tot["probes"],
                      "pos": pos_all},
         "plants_recovered": f"{recovered}/{N_PLANTS}", "solutions": solutions,

@@ -287,6 +287,23 @@ int s615_jobs_close(s615_jobs_file* f, s615_jobs_info* info);
  * text lines).  S615_E_ARG for other kinds or fields wider than the format. */
 int s615_jobs_write(const char* path, const s615_unit* jobs, size_t n);
 
+/* Autotuner (no counterpart in the reference).  Times one pass of the peel
+ * over this batch of units under every candidate setting -- 16, 32 or 64 rows
+ * per class 2-5 work item, times 1 .. the kernel's occupancy limit of blocks
+ * per SM -- and keeps the fastest for later batches of the same size (units
+ * in [2^k, 2^(k+1))) on this context: s615_prepare, s615_run and the serving
+ * loop then use it.  Other sizes keep the default rule (64-row items, fewer
+ * for small batches; the occupancy limit).  Results never depend on the
+ * setting.  table receives every trial (S615_E_OVERFLOW when cap is short),
+ * best the chosen one.  s615_tune_reset forgets every choice. */
+typedef struct s615_tune_entry {
+  uint32_t item_rows, blocks_per_sm;
+  float ms;            /* one pass, CUDA events on the context's stream */
+} s615_tune_entry;
+int s615_autotune(s615_ctx* ctx, int table_id, const s615_unit* units, size_t n, unsigned flags,
+                  s615_tune_entry* table, size_t cap, size_t* n_entries, s615_tune_entry* best);
+int s615_tune_reset(s615_ctx* ctx);
+
 /* What a run does with one unit: S615_OK = searched, 1 = dropped like
  * pack_unit5 drops it (u >= B or an empty residue class), S615_E_FORMAT =
  * rejected (outside the engine's exact-arithmetic range, or a planted base

@@ -720,19 +720,27 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
   // have fewer items than about 40 warps per SM (a small serving batch).
   const u64 want_items = (u64)ctx->num_sms * 40;
   u32 unit_rows = kItemRows;
-  while (unit_rows > 16) {
-    u64 items = 0;
-    for (size_t k = 0; k < nd && items < want_items; ++k) {
-      const DevUnit& d = du[k];
-      if (d.cls < 2 || d.cls > 5) continue;
-      for (u32 ir = 0; ir < d.nres1; ++ir) {
-        u32 jmin = 0, jend = 0;
-        class_rows(d.res1[ir], d.mod1, d.fmax1, &jmin, &jend);
-        if (jend > jmin) items += (jend - jmin + unit_rows - 1) / unit_rows;
+  u32 bucket = 0;
+  while (bucket < 39 && (2ull << bucket) <= n) ++bucket;
+  const auto& tuned = ctx->tune[bucket];
+  b->blocks_per_sm = ctx->force_bps ? ctx->force_bps : tuned.blocks_per_sm;
+  if (ctx->force_rows || tuned.item_rows) {
+    unit_rows = ctx->force_rows ? ctx->force_rows : tuned.item_rows;
+  } else {
+    while (unit_rows > 16) {
+      u64 items = 0;
+      for (size_t k = 0; k < nd && items < want_items; ++k) {
+        const DevUnit& d = du[k];
+        if (d.cls < 2 || d.cls > 5) continue;
+        for (u32 ir = 0; ir < d.nres1; ++ir) {
+          u32 jmin = 0, jend = 0;
+          class_rows(d.res1[ir], d.mod1, d.fmax1, &jmin, &jend);
+          if (jend > jmin) items += (jend - jmin + unit_rows - 1) / unit_rows;
+        }
       }
+      if (items >= want_items) break;
+      unit_rows /= 2;
     }
-    if (items >= want_items) break;
-    unit_rows /= 2;
   }
   b->item_rows = unit_rows;
   for (size_t k = 0; k < nd; ++k) {
@@ -840,6 +848,7 @@ int s615_run_batch(s615_ctx* ctx, int id, s615_batch* b, unsigned flags, void* s
   one.d_ctr = b->d_ctr;
   one.d_work = b->d_work;
   one.item_rows = b->item_rows;
+  one.blocks_per_sm = b->blocks_per_sm;
   size_t i = 0;
   while (i < b->n_items) {
     size_t j = i;
@@ -892,6 +901,62 @@ int s615_run(s615_ctx* ctx, int id, const s615_unit* units, size_t n, unsigned f
   if (!s) s = s615_batch_results(ctx, b, hits, hit_cap, n_hits, counters);
   s615_batch_free(ctx, b);
   return s;
+}
+
+int s615_autotune(s615_ctx* ctx, int id, const s615_unit* units, size_t n, unsigned flags,
+                  s615_tune_entry* table, size_t cap, size_t* n_entries, s615_tune_entry* best) {
+  if (!ctx || !units || n == 0 || (cap && !table)) return S615_E_ARG;
+  if (serving_blocks(ctx)) return S615_E_BUSY;
+  if (!find_table(ctx, id)) return S615_E_NOTABLE;
+  cudaSetDevice(ctx->device);
+  u32 bucket = 0;
+  while (bucket < 39 && (2ull << bucket) <= n) ++bucket;
+  std::vector<s615_tune_entry> got;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int s = S615_OK;
+  const u32 max_bps = (flags & S615_F_SHARP) ? 3u : 5u;   // k_peel's launch bounds
+  for (u32 rows : {16u, 32u, 64u}) {
+    for (u32 bps = 1; bps <= max_bps && !s; ++bps) {
+      ctx->force_rows = rows;
+      ctx->force_bps = bps;
+      s615_batch* b = nullptr;
+      s = s615_prepare(ctx, units, n, &b);
+      ctx->force_rows = ctx->force_bps = 0;
+      if (s) break;
+      float ms = 0;
+      s = s615_run_batch(ctx, id, b, flags, nullptr);   // warm
+      if (!s) cudaEventRecord(e0, ctx->stream);
+      if (!s) s = s615_run_batch(ctx, id, b, flags, nullptr);
+      if (!s) {
+        cudaEventRecord(e1, ctx->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) s = S615_E_DEVICE;
+        else cudaEventElapsedTime(&ms, e0, e1);
+      }
+      s615_batch_free(ctx, b);
+      if (!s) got.push_back(s615_tune_entry{rows, bps, ms});
+    }
+    if (s) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (s) return s;
+  size_t k = 0;
+  for (size_t i = 1; i < got.size(); ++i)
+    if (got[i].ms < got[k].ms) k = i;
+  ctx->tune[bucket].item_rows = got[k].item_rows;
+  ctx->tune[bucket].blocks_per_sm = got[k].blocks_per_sm;
+  if (best) *best = got[k];
+  if (n_entries) *n_entries = got.size();
+  for (size_t i = 0; i < got.size() && i < cap; ++i) table[i] = got[i];
+  return got.size() > cap && table ? S615_E_OVERFLOW : S615_OK;
+}
+
+int s615_tune_reset(s615_ctx* ctx) {
+  if (!ctx) return S615_E_ARG;
+  for (auto& t : ctx->tune) t = s615_ctx::Tune{};
+  return S615_OK;
 }
 
 int s615_cls5_run(s615_ctx* ctx, int id, const s615_unit* units, size_t n, unsigned flags,

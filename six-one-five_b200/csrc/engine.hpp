@@ -154,6 +154,7 @@ struct s615_batch {
   s615::Cls5Counters* d_ctr = nullptr;
   s615::u32* d_work = nullptr;   // persistent-queue cursors [classes 2-5, cls 7]
   s615::u32 item_rows = s615::kItemRows;   // rows per class 2-5 item (smaller for small batches)
+  s615::u32 blocks_per_sm = 0;              // k_peel blocks per SM (0: the occupancy limit)
   std::vector<s615::u64> host_items;
 };
 
@@ -175,6 +176,11 @@ struct s615_ctx {
   s615::u32* d_roots = nullptr;     // device Stage-1 root tables (stage1.cu)
   size_t roots_bytes = 0;
   size_t arena_cap[4] = {};
+  // s615_autotune's choice per batch size (bucket k: 2^k <= units < 2^(k+1));
+  // zero fields fall back to the occupancy rule.  force_* hold a trial's
+  // setting while s615_autotune times it.
+  struct Tune { s615::u32 item_rows = 0, blocks_per_sm = 0; } tune[40];
+  s615::u32 force_rows = 0, force_bps = 0;
 };
 
 namespace s615 {

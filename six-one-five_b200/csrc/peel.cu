@@ -444,6 +444,7 @@ int launch_main(s615_ctx* ctx, const TableView& tv, const s615_batch* b, size_t 
   if (grid <= 0) {
     int per_sm = 0;
     S615_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_peel<kSharp, kSet>, kThreads, kSmemTotal));
+    if (b->blocks_per_sm && (int)b->blocks_per_sm < per_sm) per_sm = (int)b->blocks_per_sm;
     grid = ctx->num_sms * (per_sm > 0 ? per_sm : 1);
   }
   const size_t need = (n + kWarps - 1) / kWarps;

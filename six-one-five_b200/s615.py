@@ -108,6 +108,9 @@ SIGNATURES = {
                                          C.POINTER(C.c_int)]),
     "s615_save_table_shard": (C.c_int, [_P, C.c_int, C.c_int, C.c_char_p]),
     "s615_set_probe_groups": (C.c_int, [_P, C.c_int, C.c_int]),
+    "s615_autotune": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.c_uint, _P, C.c_size_t,
+                                C.POINTER(C.c_size_t), _P]),
+    "s615_tune_reset": (C.c_int, [_P]),
     "s615_build_table_shard_range": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                                C.c_int, C.POINTER(C.c_int)]),
     "s615_export_table": (C.c_int, [_P, C.c_int, C.POINTER(Header), _P, C.c_size_t,
@@ -261,6 +264,10 @@ def jobs617(B: int, cls: int):
     arr = (Unit * max(n.value, 1))()
     _check(lib().s615_617_jobs(B, cls, C.cast(arr, C.c_void_p), n.value, C.byref(n)), "617_jobs")
     return arr, n.value
+
+
+class TuneEntry(C.Structure):
+    _fields_ = [("item_rows", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("ms", C.c_float)]
 
 
 class JobsInfo(C.Structure):
@@ -476,6 +483,19 @@ class Engine:
         _check(lib().s615_load_table_shards(self._ctx, arr, len(paths), expected_N, layout,
                                             C.byref(tid)), "load_table_shards")
         return tid.value
+
+    def autotune(self, tid: int, units, n: int, flags: int = 0):
+        """s615_autotune: every trial (item_rows, blocks_per_sm, ms) and the chosen one."""
+        table = (TuneEntry * 64)()
+        k = C.c_size_t(0)
+        best = TuneEntry()
+        _check(lib().s615_autotune(self._ctx, tid, C.cast(units, C.c_void_p), n, flags,
+                                   C.cast(table, C.c_void_p), 64, C.byref(k), C.byref(best)), "autotune")
+        rows = [(table[i].item_rows, table[i].blocks_per_sm, table[i].ms) for i in range(k.value)]
+        return rows, (best.item_rows, best.blocks_per_sm, best.ms)
+
+    def tune_reset(self) -> None:
+        _check(lib().s615_tune_reset(self._ctx), "tune_reset")
 
     def set_probe_groups(self, tid: int, groups: int) -> None:
         """Probe a shard set in `groups` passes (0: from its size)."""
