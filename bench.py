@@ -139,6 +139,35 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+def random_read_ceiling(gib):
+    """Random 8-byte reads/s of this GPU over a buffer of `gib` GiB, the table's
+    footprint: the faster of bin/randaccess_peak's two `ld.global.cg.L2::64B`
+    forms, the load the xor probe issues (three per post-gate probe).  Run after
+    the timed region; None when the binary is missing or fails."""
+    exe = os.path.join(ROOT, "six-one-five_b200", "bin", "randaccess_peak")
+    try:
+        r = subprocess.run([exe, "%.2f" % max(gib, 0.01)], capture_output=True, text=True,
+                           timeout=300)
+    except (OSError, subprocess.TimeoutExpired):
+        return None
+    if r.returncode != 0:
+        return None
+    rates = [float(line.split()[-3]) for line in r.stdout.splitlines() if "L2::64B" in line]
+    return max(rates) if rates else None
+
+
+def random_access_roof(probes, dur_s, table_bytes):
+    """The probe's second roofline: cell reads/s (3 per post-gate probe) over the
+    measured random-read rate at the same footprint.  Above 1.0 means some cell
+    reads were L2 hits."""
+    ceil = random_read_ceiling(table_bytes / 2**30)
+    got = 3 * probes / dur_s
+    return {"achieved_reads_per_s": got, "ceiling_reads_per_s": ceil,
+            "frac": round(got / ceil, 4) if ceil else None,
+            "ceiling_source": "bin/randaccess_peak %.2f (same GPU, after the timed region)"
+                              % (table_bytes / 2**30)}
+
+
 def profiled_traffic():
     """DRAM bytes per post-gate probe from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", "k_peel_cls5_band3p2M.md")
@@ -444,6 +473,9 @@ def run617(args, rank, world, local, dist):
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs (burst)",
             "traffic": None, "algorithmic_bytes_per_launch": ctr.probes * PROBE_BYTES}
+    if rank == 0:
+        roof["random_access"] = random_access_roof(ctr.probes, statistics.mean(per_ms) / 1e3,
+                                                   eng.table_info(tid).device_bytes)
 
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and world == 1:
@@ -825,7 +857,10 @@ def run_jobs(args, rank, world, local, dist):
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs (burst)",
-                         "traffic": None, "algorithmic_bytes_per_launch": ctr.probes * PROBE_BYTES},
+                         "traffic": None, "algorithmic_bytes_per_launch": ctr.probes * PROBE_BYTES,
+                         "random_access": (random_access_roof(
+                             ctr.probes, statistics.mean(per_ms) / 1e3,
+                             eng.table_info(tid).device_bytes) if rank == 0 else None)},
             "cpu_baseline": cpu, "sharp_gate": sharp, "clocks": cl}
     eng.close()
     if rank == 0:
@@ -1069,6 +1104,14 @@ def main():
             "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs (burst)",
             "traffic": (tpp * ctr.probes if tpp else None),
             "algorithmic_bytes_per_launch": ctr.probes * PROBE_BYTES}
+    if rank == 0 and args.shards == 1:
+        roof["random_access"] = random_access_roof(ctr.probes, dur_s,
+                                                   eng.table_info(tid).device_bytes)
+        log("random-access roofline: %.3e cell reads/s of %s measured (%s)" % (
+            roof["random_access"]["achieved_reads_per_s"],
+            "%.3e" % roof["random_access"]["ceiling_reads_per_s"]
+            if roof["random_access"]["ceiling_reads_per_s"] else "n/a",
+            roof["random_access"]["frac"]))
 
     # plain per-unit-launch form on a bounded sample of the same band
     plain = None

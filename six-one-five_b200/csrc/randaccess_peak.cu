@@ -2,7 +2,7 @@
 // xor probe (three random cells per probe).
 //
 // Reads `iters` 8-byte words at hashed (uniform, always in-bounds) positions of
-// a buffer (2 GiB unless sizes are given) with several load forms and prints
+// a buffer (2 GiB unless sizes are given) with four load forms and prints
 // reads/s.  The result is the
 // denominator for the probe kernel's random-access roofline.
 //   bin/randaccess_peak            (run under ncu with dram__sectors_read.sum to
@@ -37,6 +37,25 @@ __global__ void k_random_reads(const u64* __restrict__ p, u64 n, u64 iters, u64*
   if (acc == 0x123456789ULL) out[0] = acc;
 }
 
+// The same random 64-B-fill reads with the index taken as the high half of
+// h * n (one multiply instead of a 64-bit remainder) and four independent loads
+// per thread per iteration, so that neither the index arithmetic nor a lack of
+// loads in flight limits the rate.
+__global__ void k_random_reads_ilp(const u64* __restrict__ p, u64 n, u64 iters, u64* out) {
+  u64 acc = 0;
+  const u64 tid = blockIdx.x * (u64)blockDim.x + threadIdx.x, nt = (u64)gridDim.x * blockDim.x;
+  for (u64 i = tid * 4; i < iters; i += nt * 4) {
+    u64 v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const u64 j = __umul64hi(mix((i + k) * 0x9E3779B97F4A7C15ULL + 3), n);   // j < n
+      asm volatile("ld.global.cg.L2::64B.u64 %0, [%1];" : "=l"(v[k]) : "l"(p + j));
+    }
+    acc ^= v[0] ^ v[1] ^ v[2] ^ v[3];
+  }
+  if (acc == 0x123456789ULL) out[0] = acc;
+}
+
 // Usage: randaccess_peak [GiB ...] -- one line per load form and buffer size
 // (default 2 GiB); larger buffers show how the rate falls with the footprint.
 int main(int argc, char** argv) {
@@ -48,7 +67,8 @@ int main(int argc, char** argv) {
   cudaEventCreate(&b);
   u64* o = nullptr;
   if (cudaMalloc(&o, 8) != cudaSuccess) { std::printf("alloc failed\n"); return 1; }
-  const char* names[3] = {"ld.global.nc (L1)", "ld.global.cg", "ld.global.cg.L2::64B"};
+  const char* names[4] = {"ld.global.nc (L1)", "ld.global.cg", "ld.global.cg.L2::64B",
+                          "ld.global.cg.L2::64B x4"};
   const int nsizes = argc > 1 ? argc - 1 : 1;
   cudaError_t e = cudaSuccess;
   for (int si = 0; si < nsizes && e == cudaSuccess; ++si) {
@@ -61,11 +81,12 @@ int main(int argc, char** argv) {
       continue;
     }
     cudaMemset(p, 1, n * 8);
-    for (int v = 0; v < 3; ++v) {
+    for (int v = 0; v < 4; ++v) {
       auto launch = [&]() {
         if (v == 0) k_random_reads<0><<<sms * 8, 256>>>(p, n, iters, o);
         else if (v == 1) k_random_reads<1><<<sms * 8, 256>>>(p, n, iters, o);
-        else k_random_reads<2><<<sms * 8, 256>>>(p, n, iters, o);
+        else if (v == 2) k_random_reads<2><<<sms * 8, 256>>>(p, n, iters, o);
+        else k_random_reads_ilp<<<sms * 8, 256>>>(p, n, iters, o);
       };
       launch();
       cudaEventRecord(a);
@@ -76,6 +97,18 @@ int main(int argc, char** argv) {
       cudaEventElapsedTime(&ms, a, b);
       std::printf("%7.1f GiB  %-24s %.3f ms  %.3e random reads/s\n", gib, names[v], ms,
                   iters / (ms * 1e-3));
+    }
+    // the x4 form with fewer resident blocks: fewer reads in flight per SM
+    for (int bps : {1, 2, 4}) {
+      k_random_reads_ilp<<<sms * bps, 256>>>(p, n, iters, o);
+      cudaEventRecord(a);
+      k_random_reads_ilp<<<sms * bps, 256>>>(p, n, iters, o);
+      cudaEventRecord(b);
+      cudaEventSynchronize(b);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, a, b);
+      std::printf("%7.1f GiB  %-17s bps=%d %.3f ms  %.3e random reads/s\n", gib,
+                  "ld.global.cg.L2::64B x4", bps, ms, iters / (ms * 1e-3));
     }
     cudaFree(p);
     e = cudaGetLastError();
