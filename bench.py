@@ -1095,6 +1095,26 @@ def main():
     log(f"e2e through s615_cls5_run: {e2e_s * 1e3:.1f} ms per step (device step {total_ms / args.steps:.1f} ms)")
     assert c2.pos == ctr.pos and c2.probes == ctr.probes
     d2h = C.sizeof(s615.Counters) + len(h2) * 32
+    # where the e2e step goes: the same work as s615_run, one C-ABI call per phase
+    e2e_phases = None
+    if rank == 0:
+        ph = {}
+        t0 = time.perf_counter()
+        b2 = C.c_void_p()
+        s615._check(lib.s615_prepare(eng._ctx, C.cast(arr, C.c_void_p), n, C.byref(b2)), "prepare")
+        ph["prepare_ms"] = (time.perf_counter() - t0) * 1e3
+        t0 = time.perf_counter()
+        s615._check(lib.s615_run_batch(eng._ctx, tid, b2, 0, None), "run_batch")
+        hb = (s615.Hit * (1 << 16))()
+        nh2, c3 = C.c_size_t(0), s615.Counters()
+        s615._check(lib.s615_batch_results(eng._ctx, b2, C.cast(hb, C.c_void_p), 1 << 16,
+                                           C.byref(nh2), C.byref(c3)), "results")
+        ph["run_and_results_ms"] = (time.perf_counter() - t0) * 1e3
+        t0 = time.perf_counter()
+        s615._check(lib.s615_batch_free(eng._ctx, b2), "batch_free")
+        ph["free_ms"] = (time.perf_counter() - t0) * 1e3
+        e2e_phases = {k: round(v, 1) for k, v in ph.items()}
+        log(f"e2e phases: {e2e_phases}")
 
     peak, peak_kind = measured_peaks()
     dur_s = statistics.mean(per_ms) / 1e3
@@ -1212,7 +1232,7 @@ def main():
         "plants_recovered": f"{recovered}/{N_PLANTS}", "solutions": solutions,
         "table_build_s": round(build_s, 2),
         "e2e": {"value": ctr.pos / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
+                "d2h_bytes_per_step": d2h, "phases": e2e_phases},
         "gpu_launches": launches,
         "roofline": roof,
         "cpu_baseline": cpu,

@@ -86,7 +86,8 @@ typedef struct s615_table_info {
  * (= target - u^6, 3 LE limbs) is taken as given with a single residue per
  * axis and fmax equal to the planted value (the reference's plant shape,
  * solve_516_v3.cu:1130-1170): cls 5 uses res_e/fmax1 and res_d/fmax2;
- * cls 2-4 and 7 use res_d/fmax1.  cls 7 kind 0 needs 14 | u, 6 | w,
+ * cls 2-4 and 7 use res_d/fmax1.  Classes 2-5: B <= 40,000,000 for kind 0,
+ * and for kind 1 base < 2^152 with f * fmax <= 40,000,000 on each axis.  cls 7 kind 0 needs 14 | u, 6 | w,
  * u^6 = B^6 (mod 3^6), w^6 = B^6 (mod 7^6) and B <= 2,353,973 (B^6 < 2^127);
  * units with base <= 0 are dropped like the reference drops them.  A cls 7
  * plant (solve_617_v1.cu:1564-1582) has base < 2^127 and lim < 65536.

@@ -655,7 +655,9 @@ int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip) {
     }
   } else if (in.kind == 1) {
     base = W3{{in.base[0], in.base[1], in.base[2]}};
-    if (zero_w3(base) || (in.base[2] >> 22) != 0) return S615_E_FORMAT;  // base < 2^150
+    // base < 2^152, like a Stage-1 unit's B^6 - u^6 at the largest B (kMaxB^6 < 2^151.6):
+    // the row values V = (base - x^6) / 21^6 stay below 2^126
+    if (zero_w3(base) || (in.base[2] >> 24) != 0) return S615_E_FORMAT;
     out->B = in.B; out->u = in.u;
     out->lim = in.lim;
     out->nres1 = 1;

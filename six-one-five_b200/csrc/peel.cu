@@ -7,7 +7,7 @@
 // raw hits and calls/gated/probes counters.
 //
 //  * Exact rows, no per-point big integers.
-//      cls5 row e:   V(e) = (base - (14e)^6) / 21^6 (exact, < 2^112);
+//      cls5 row e:   V(e) = (base - (14e)^6) / 21^6 (exact, < 2^126 for B <= 40M);
 //                    at column d, T = (V - d^6) / 64, and R > 0 <=> d <= D(e)
 //                    with D(e) = iroot6(V - 1).
 //      cls2-4 row d: T(d) = (base - (f d)^6) / 42^6 (exact, < 2^122); the

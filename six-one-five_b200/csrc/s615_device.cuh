@@ -79,18 +79,21 @@ __device__ __forceinline__ bool might_contain(const TableView& t, u64 key) {
   return t.shards > 1 ? probe_table<true>(t, key) : probe_table<false>(t, key);
 }
 
-// x^6 for x < 2^21 (exact, < 2^126).
+// x^6, exact for x <= 2,642,245 (the largest x with x^3 < 2^64; x^6 < 2^128).
 __device__ __forceinline__ u128 pow6_small(u64 x) {
   const u64 x3 = x * x * x;
   return (u128)x3 * x3;
 }
 
-// floor(v^(1/6)) for 0 <= v < 2^120: double estimate, then exact fix-up.
+// floor(v^(1/6)) for 0 <= v < 2^127 (root < 2,413,000): double estimate, off by at
+// most one, then exact fix-up.  The clamp keeps pow6_small(r + 1) exact; it is
+// above every root of the domain, so the fix-up takes a step or two.  (A class-5
+// row at B = 40,000,000 has V ~ 2^125 and D(e) up to 1.9M.)
 __device__ __forceinline__ u32 iroot6_u128(u128 v) {
   if (v == 0) return 0;
   const double x = (double)(u64)(v >> 64) * 18446744073709551616.0 + (double)(u64)v;
   u64 r = (u64)cbrt(sqrt(x));
-  if (r > (1ULL << 20)) r = 1ULL << 20;
+  if (r > 2642244ull) r = 2642244ull;
   while (r > 0 && pow6_small(r) > v) --r;
   while (pow6_small(r + 1) <= v) ++r;
   return (u32)r;
