@@ -72,14 +72,15 @@ __device__ __forceinline__ u32 gate_word(const u32* pat, const RowRec& R, u32 s9
          pat[(offs.y >> 16) + s19];
 }
 
-// Least c >= 1 with 3 c^6 >= T, for 1 <= T < 2^120 (min_c_fix,
+// Least c >= 1 with 3 c^6 >= T, for 1 <= T < 2^127 (min_c_fix,
 // solve_617_v1.cu:430-436, and the window start of make_cand mode 3,
-// fourcore_find_v4.cu:411-416): a double estimate, then an exact fix-up.
+// fourcore_find_v4.cu:411-416): a double estimate, then an exact fix-up.  The
+// answer is below 1.95M; the clamp at 2^21 keeps 3 c^6 < 2^128.
 __device__ __forceinline__ u32 least_c_3c6(u128 T) {
   const double x = ((double)(u64)(T >> 64) * 18446744073709551616.0 + (double)(u64)T) / 3.0;
   u64 c = (u64)cbrt(sqrt(x));
   if (c < 1) c = 1;
-  if (c > (1ULL << 20)) c = 1ULL << 20;
+  if (c > (1ULL << 21)) c = 1ULL << 21;
   while (3 * pow6_small(c) < T) ++c;
   while (c > 1 && 3 * pow6_small(c - 1) >= T) --c;
   return (u32)c;
