@@ -126,3 +126,107 @@ def test_top_of_range_plants(engine, table):
     for j, p in enumerate(plants):
         sel = (hits["unit"] == j) & (hits["d"] == p.d) & (hits["e"] == p.e)
         assert (hits["fp"][sel] == p.fp).any(), p
+
+
+F234 = {2: 14, 3: 21, 4: 7}
+MOD234 = {2: 729, 3: 64, 4: 46656}
+
+
+def iroot6(n):
+    if n <= 0:
+        return 0
+    x = int(round(n ** (1 / 6)))
+    while x**6 > n:
+        x -= 1
+    while (x + 1) ** 6 <= n:
+        x += 1
+    return x
+
+
+def find3_window(T, lim):
+    """make_cand mode 3 (fourcore_find_v4.cu:411-416): hi = min(iroot6 T, lim),
+    lo the least c with 3 c^6 >= T."""
+    hi = min(iroot6(T), lim)
+    lo = iroot6(-(-T // 3) - 1) + 1
+    return (lo, hi) if lo <= hi else (1, 0)
+
+
+def test_top_of_range_cls234_plants(engine, table):
+    # class 2-4 planted targets with f d near B = 40,000,000 (base ~ 2^151.6,
+    # T up to 2^119): the oracle's find3 rows over the plant's residue class
+    t, tid = table
+    rng = np.random.RandomState(21)
+    plants = []
+    for i, cls in enumerate([2, 3, 4] * 2):
+        B = B_TOP - 1 - 2 * i
+        f = F234[cls]
+        d = (B - 1) // f - int(rng.randint(0, 3 * MOD234[cls]))
+        c = sorted(int(x) for x in rng.choice(np.arange(1, N1 + 1), 3, replace=False))
+        plants.append(dict(cls=cls, B=B, d=d, c=c, base=(f * d) ** 6 + 42**6 * sum(x**6 for x in c)))
+    arr = (s615.Unit * len(plants))()
+    jobs, origin = [], []
+    for j, p in enumerate(plants):
+        arr[j] = s615.make_plant234(p["cls"], p["base"], p["d"], lim=N1, B=p["B"])
+        f, mod = F234[p["cls"]], MOD234[p["cls"]]
+        d = p["d"] % mod or mod
+        while d <= p["d"]:
+            R = p["base"] - (f * d) ** 6
+            if R > 0:
+                assert R % 42**6 == 0
+                T = R // 42**6
+                lo, hi = find3_window(T, N1)
+                if lo <= hi:
+                    J = orc.OrcJob3()
+                    J.cls, J.lim, J.B, J.u, J.d = p["cls"], N1, p["B"], 0, d
+                    J.T[0], J.T[1] = T % 2**64, T >> 64
+                    J.lo, J.hi = lo, hi
+                    jobs.append(J)
+                    origin.append((j, d))
+            d += mod
+    assert jobs
+    hits, ctr = engine.run(tid, arr, len(plants))
+    jarr = (orc.OrcJob3 * len(jobs))(*jobs)
+    hits3 = (orc.OrcHit3 * (1 << 16))()
+    c3 = np.zeros(3, dtype=np.uint64)
+    nh = orc.lib().orc_find3_run(t.h, orc.C.cast(jarr, orc.C.c_void_p), len(jobs), 1, 0,
+                                 orc.C.cast(hits3, orc.C.c_void_p), 1 << 16, orc._ptr(c3))
+    assert (ctr.calls, ctr.gated, ctr.probes) == tuple(int(x) for x in c3)
+    mine = sorted((int(h["unit"]), int(h["d"]), int(h["e"]), int(h["fp"])) for h in hits)
+    theirs = sorted((origin[hits3[k].job][0], origin[hits3[k].job][1], hits3[k].c3, hits3[k].fp)
+                    for k in range(nh))
+    assert mine == theirs
+    lines = {s615.solution_line(s) for s in engine.verify(arr, len(plants), hits, N1)}
+    for j, p in enumerate(plants):
+        c1, c2, c3v = p["c"]
+        assert f"PLANT cls={p['cls']} unit={j} d={p['d']} c1={c1} c2={c2} c3={c3v}" in lines
+
+
+def test_top_of_range_jobs(engine, table):
+    # reduced-T jobs of class 2-4 Stage-1 units at B ~ 40,000,000: T up to 2^119 and
+    # c3 windows up to ~150k wide (lim = (B-1)/42 = 952,380); a spread of each unit's
+    # jobs against the oracle's expand_unit + make_cand + k_find3 restatement
+    t, tid = table
+    picked, opicked = [], []
+    for cls in (2, 3, 4):
+        B = B_TOP + 1
+        while True:
+            B -= 2
+            if W.eligible(B) and s615.unit_candidates(B, cls):
+                break
+        u = s615.unit_candidates(B, cls)[0]
+        arr, n, fail = s615.expand_unit(B, u, cls)
+        oarr, on, ofail = orc.expand_unit(B, u, cls)
+        assert (n, fail) == (on, ofail) and n > 0
+        for i in range(0, n, max(1, n // 60)):
+            assert (arr[i].base[0], arr[i].base[1]) == (oarr[i].T[0], oarr[i].T[1])
+            picked.append(arr[i])
+            opicked.append(oarr[i])
+    jarr = (s615.Unit * len(picked))(*picked)
+    oj = (orc.OrcJob * len(opicked))(*opicked)
+    hits, ctr = engine.run(tid, jarr, len(picked))
+    oh, (calls, gated, probes) = orc.run_jobs(t, oj, len(opicked))
+    assert calls > 10**7 and len(oh) > 0          # r = 16: filter false positives
+    assert (ctr.calls, ctr.gated, ctr.probes) == (calls, gated, probes)
+    mine = sorted((int(h["unit"]), int(h["e"]), int(h["c4"]), int(h["fp"])) for h in hits)
+    theirs = sorted((int(h["job"]), int(h["c3"]), int(h["c4"]), int(h["fp"])) for h in oh)
+    assert mine == theirs
