@@ -230,3 +230,36 @@ def test_top_of_range_jobs(engine, table):
     mine = sorted((int(h["unit"]), int(h["e"]), int(h["c4"]), int(h["fp"])) for h in hits)
     theirs = sorted((int(h["job"]), int(h["c3"]), int(h["c4"]), int(h["fp"])) for h in oh)
     assert mine == theirs
+
+
+def test_top_of_range_617_plants(engine):
+    # (6,1,7) Branch-A class-5 plants just below the i128 wall (21 d up to
+    # B_HARD_MAX = 2,353,973, base up to 2^127): the c4 windows of the large-T
+    # rows, and the planted row, against the oracle's k_find4_cls5 restatement
+    import test_gpu_617 as T7
+    N, r = 600, 16
+    rng = np.random.RandomState(17)
+    plants = []
+    for k in range(12):
+        c = sorted(int(x) for x in rng.choice(np.arange(1, N + 1), 4, replace=False))
+        d = 2_353_973 // 21 - int(rng.randint(0, 2000))
+        plants.append((c, d))
+    cands = (orc.OrcCand617 * len(plants))()
+    units = (s615.Unit * len(plants))()
+    for i, (c, d) in enumerate(plants):
+        cands[i], units[i] = T7.plant(c, d, N)
+        assert (21 * d) ** 6 < 2**127 and (21 * d) ** 6 > 2**126
+    tid = engine.build_table(N, r)
+    try:
+        hdr, packed = engine.export_table(tid)
+        t = orc.Table.from_memory(hdr, packed)
+        hits, ctr = engine.run(tid, units, len(plants))
+        oh, oc = orc.run617(t, cands, len(plants))
+        T7.check_counters(ctr, oc)
+        assert T7.mine(hits) == T7.theirs(oh)
+        got = {(s.unit, tuple(sorted((s.c1, s.c2, s.c3, s.c4))))
+               for s in engine.verify(units, len(plants), hits, N) if s.kind == 1}
+        for i, (c, d) in enumerate(plants):
+            assert ((i, tuple(c)) in got) == T7.window_reaches(c, N), (i, c, d)
+    finally:
+        engine.free_table(tid)
