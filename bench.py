@@ -796,6 +796,27 @@ def run_jobs(args, rank, world, local, dist):
         j3, n3, _ = s615.jobs_read(path)
         h3, c3 = eng.run(tid, j3, n3, hit_cap=1 << 16)
     e2e_s = (time.perf_counter() - t0) / e2e_steps
+    # the same step one C-ABI call per phase
+    ph = {}
+    t0 = time.perf_counter()
+    j3, n3, _ = s615.jobs_read(path)
+    ph["bbj_read_ms"] = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    b3 = C.c_void_p()
+    s615._check(lib.s615_prepare(eng._ctx, C.cast(j3, C.c_void_p), n3, C.byref(b3)), "prepare")
+    ph["prepare_ms"] = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    s615._check(lib.s615_run_batch(eng._ctx, tid, b3, 0, None), "run_batch")
+    hb3 = (s615.Hit * (1 << 16))()
+    nh3, c4 = C.c_size_t(0), s615.Counters()
+    s615._check(lib.s615_batch_results(eng._ctx, b3, C.cast(hb3, C.c_void_p), 1 << 16,
+                                       C.byref(nh3), C.byref(c4)), "results")
+    ph["run_and_results_ms"] = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    s615._check(lib.s615_batch_free(eng._ctx, b3), "batch_free")
+    ph["free_ms"] = (time.perf_counter() - t0) * 1e3
+    e2e_phases = {k: round(v, 1) for k, v in ph.items()}
+    log(f"jobs e2e phases: {e2e_phases}")
     assert c3.probes == ctr.probes
     os.remove(path)
 
@@ -853,7 +874,7 @@ def run_jobs(args, rank, world, local, dist):
             "table_build_s": round(build_s, 2),
             "e2e": {"value": n / e2e_s, "unit": "jobs/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": C.sizeof(s615.Counters) + len(h3) * C.sizeof(s615.Hit),
-                    "includes": ".bbj read + s615_run"},
+                    "includes": ".bbj read + s615_run", "phases": e2e_phases},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs (burst)",

@@ -14,6 +14,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <new>
 #include <random>
 #include <thread>
 #include <vector>
@@ -29,14 +30,22 @@ int cuda_status(cudaError_t e) {
   return e == cudaSuccess ? S615_OK : S615_E_DEVICE;
 }
 
+// A failed allocation gives back s615_run's kept batch, if it holds one that
+// no run is using, and tries once more.
 int dev_alloc(s615_ctx* ctx, void** p, size_t bytes) {
   *p = nullptr;
   if (bytes == 0) bytes = 16;
-  if (ctx->budget && ctx->used + bytes > ctx->budget) return S615_E_OOM;
-  const cudaError_t e = cudaMalloc(p, bytes);
-  if (e != cudaSuccess) { cudaGetLastError(); *p = nullptr; return S615_E_OOM; }
-  ctx->used += bytes;
-  return S615_OK;
+  for (int attempt = 0;; ++attempt) {
+    if (!ctx->budget || ctx->used + bytes <= ctx->budget) {
+      if (cudaMalloc(p, bytes) == cudaSuccess) {
+        ctx->used += bytes;
+        return S615_OK;
+      }
+      cudaGetLastError();
+      *p = nullptr;
+    }
+    if (attempt > 0 || !release_run_batch(ctx)) return S615_E_OOM;
+  }
 }
 
 void dev_free(s615_ctx* ctx, void* p, size_t bytes) {
@@ -44,6 +53,38 @@ void dev_free(s615_ctx* ctx, void* p, size_t bytes) {
   if (bytes == 0) bytes = 16;
   cudaFree(p);
   ctx->used -= std::min(ctx->used, bytes);
+}
+
+bool release_run_batch(s615_ctx* ctx) {
+  if (!ctx->run_batch || ctx->run_busy) return false;
+  s615_batch* b = ctx->run_batch;
+  ctx->run_batch = nullptr;
+  s615_batch_free(ctx, b);
+  return true;
+}
+
+void* stage_get(HostStage& s, size_t bytes) {
+  if (bytes <= s.bytes) return s.p;
+  stage_free(s);
+  const size_t want = std::max<size_t>(bytes + bytes / 4, size_t(1) << 20);
+  if (cudaMallocHost(&s.p, want) == cudaSuccess) {
+    s.pinned = true;
+  } else {
+    cudaGetLastError();
+    s.p = ::operator new(want, std::nothrow);
+    s.pinned = false;
+    if (!s.p) return nullptr;
+  }
+  s.bytes = want;
+  return s.p;
+}
+
+void stage_free(HostStage& s) {
+  if (s.p) {
+    if (s.pinned) cudaFreeHost(s.p);
+    else ::operator delete(s.p);
+  }
+  s = HostStage{};
 }
 
 bool gate_product_matches();
@@ -125,6 +166,7 @@ int pick_layout(s615_ctx* ctx, int want, u64 m, u32 r, int* cell_bytes) {
   *cell_bytes = r <= 32 ? 4 : 8;
   if (want == S615_LAYOUT_PACKED) { *cell_bytes = 0; return S615_LAYOUT_PACKED; }
   if (want == S615_LAYOUT_WIDE) return S615_LAYOUT_WIDE;
+  release_run_batch(ctx);   // a table needs the room more than s615_run's kept buffers
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
   const size_t wide = m * (size_t)(*cell_bytes) + packed_bytes(m, r) + ((size_t)4 << 30);
@@ -223,6 +265,9 @@ int s615_close(s615_ctx* ctx) {
   if (!ctx) return S615_E_ARG;
   cudaSetDevice(ctx->device);
   server_destroy(ctx);
+  ctx->run_busy = false;
+  release_run_batch(ctx);
+  stage_free(ctx->unit_stage);
   for (int k = 0; k < 4; ++k) dev_free(ctx, ctx->arena[k], ctx->arena_cap[k]);
   dev_free(ctx, ctx->d_roots, ctx->roots_bytes);
   for (auto& kv : ctx->tables) free_table(ctx, kv.second);
@@ -671,10 +716,15 @@ int arena_get(s615_ctx* ctx, int k, size_t bytes, void** p) {
 // make_dev_unit over every unit (on several host threads for large batches),
 // the kept records compacted in unit order.  Returns the error of the
 // lowest-index unit that has one, as a sequential pass would.
-static int pack_units(const s615_unit* units, size_t n, std::unique_ptr<DevUnit[]>& out,
+// One device record per input unit, in input order.  A unit the reference
+// drops (u >= B, an empty residue class or window) stays in place as a class-0
+// record that gets no work items, so no pass compacts the array.
+static int pack_units(s615_ctx* ctx, const s615_unit* units, size_t n, DevUnit** out_p,
                       size_t* n_out) {
-  out.reset(new DevUnit[std::max<size_t>(n, 1)]);
-  std::vector<uint8_t> keep(n);
+  DevUnit* out = static_cast<DevUnit*>(
+      stage_get(ctx->unit_stage, std::max<size_t>(n, 1) * sizeof(DevUnit)));
+  if (!out) return S615_E_OOM;
+  *out_p = out;
   const size_t hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
   const size_t nt = n < (1u << 16) ? 1 : std::min(hw, (n + 65535) / 65536);
   std::vector<int> err(nt, 0);
@@ -683,7 +733,7 @@ static int pack_units(const s615_unit* units, size_t n, std::unique_ptr<DevUnit[
       bool skip = false;
       const int s = make_dev_unit(units[i], (u32)i, &out[i], &skip);
       if (s) { err[t] = s; return; }
-      keep[i] = !skip;
+      if (skip) out[i].cls = 0;
     }
   };
   if (nt == 1) {
@@ -695,22 +745,15 @@ static int pack_units(const s615_unit* units, size_t n, std::unique_ptr<DevUnit[
   }
   for (size_t t = 0; t < nt; ++t)
     if (err[t]) return err[t];
-  size_t k = 0;
-  for (size_t i = 0; i < n; ++i)
-    if (keep[i]) {
-      if (k != i) out[k] = out[i];
-      ++k;
-    }
-  *n_out = k;
+  *n_out = n;
   return S615_OK;
 }
 
 int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
   b->host_items.clear();
-  std::unique_ptr<DevUnit[]> dp;
+  DevUnit* du = nullptr;
   size_t nd = 0;
-  if (const int s = pack_units(units, n, dp, &nd)) return s;
-  const DevUnit* du = dp.get();
+  if (const int s = pack_units(ctx, units, n, &du, &nd)) return s;
   std::vector<u64> items617;   // the (6,1,7) kernel's items go after the others
   // Job rows per item: up to 64, fewer when the batch is small, so that its
   // items still fill the GPU (about 64 warps per SM).
@@ -745,6 +788,7 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
   b->item_rows = unit_rows;
   for (size_t k = 0; k < nd; ++k) {
     const DevUnit& d = du[k];
+    if (d.cls == 0) continue;   // dropped
     // classes 1, 7 and 8 (c4 windows) run in the second kernel
     unit_items(d, (u32)k,
                (d.cls == S615_CLS_617 || d.cls == 1 || d.cls == S615_CLS_617_FIND4) ? items617
@@ -889,17 +933,25 @@ int s615_batch_results(s615_ctx* ctx, s615_batch* b, s615_hit* hits, size_t hit_
   return S615_OK;
 }
 
+// One call = s615_prepare + s615_run_batch + s615_batch_results on the
+// context's kept batch: its device buffers are reused while they are large
+// enough, so repeated calls allocate nothing.
 int s615_run(s615_ctx* ctx, int id, const s615_unit* units, size_t n, unsigned flags,
              s615_hit* hits, size_t hit_cap, size_t* n_hits, s615_counters* counters) {
-  if (!ctx) return S615_E_ARG;
+  if (!ctx || (n && !units) || n > kMaxBatchUnits) return S615_E_ARG;
+  if (serving_blocks(ctx)) return S615_E_BUSY;
   if (!find_table(ctx, id)) return S615_E_NOTABLE;
   cudaSetDevice(ctx->device);
-  s615_batch* b = nullptr;
-  int s = s615_prepare(ctx, units, n, &b);
-  if (s) return s;
-  s = s615_run_batch(ctx, id, b, flags, nullptr);
+  if (!ctx->run_batch) ctx->run_batch = new s615_batch();
+  s615_batch* b = ctx->run_batch;
+  ctx->run_busy = true;
+  int s = fill_batch(ctx, units, n, b);
+  if (!s) s = s615_run_batch(ctx, id, b, flags, nullptr);
   if (!s) s = s615_batch_results(ctx, b, hits, hit_cap, n_hits, counters);
-  s615_batch_free(ctx, b);
+  ctx->run_busy = false;
+  // an overflow still returns counters and the hits that fit; any other
+  // failure keeps no device buffers
+  if (s && s != S615_E_OVERFLOW) release_run_batch(ctx);
   return s;
 }
 

@@ -158,6 +158,15 @@ struct s615_batch {
   std::vector<s615::u64> host_items;
 };
 
+namespace s615 {
+// A grow-only host buffer: pinned when the driver grants it, pageable if not.
+struct HostStage {
+  void* p = nullptr;
+  size_t bytes = 0;
+  bool pinned = false;
+};
+}  // namespace s615
+
 struct s615_ctx {
   int device = 0;
   size_t budget = 0, used = 0;
@@ -181,6 +190,14 @@ struct s615_ctx {
   // setting while s615_autotune times it.
   struct Tune { s615::u32 item_rows = 0, blocks_per_sm = 0; } tune[40];
   s615::u32 force_rows = 0, force_bps = 0;
+  // The unit records every fill_batch packs before its host-to-device copy
+  // (reused, so a large batch is neither page-faulted nor copied from pageable
+  // memory again), and s615_run's own batch, whose device buffers serve the
+  // next call.  Both live until s615_close; the batch is also given back when a
+  // device allocation runs out of room.
+  s615::HostStage unit_stage;
+  s615_batch* run_batch = nullptr;
+  bool run_busy = false;
 };
 
 namespace s615 {
@@ -197,6 +214,12 @@ int cuda_status(cudaError_t e);
 // its worker thread (calls that allocate or launch then return S615_E_BUSY).
 bool serving_blocks(s615_ctx* ctx);
 void server_destroy(s615_ctx* ctx);   // stops the loop (draining it) and frees it
+
+// Host staging (grow-only; nullptr if even a pageable buffer cannot be had).
+void* stage_get(HostStage& s, size_t bytes);
+void stage_free(HostStage& s);
+// Frees s615_run's kept batch unless a run is using it; true if one was freed.
+bool release_run_batch(s615_ctx* ctx);
 
 // Budgeted device allocation.
 int dev_alloc(s615_ctx* ctx, void** p, size_t bytes);

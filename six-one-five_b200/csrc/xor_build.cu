@@ -227,6 +227,7 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
     if (s) return s;
     // Hash set sized for load <= 1/2 per partition; partitions by the top bits
     // of mix64(key) bound the table when HBM is short.
+    release_run_batch(ctx);   // a table needs the room more than s615_run's kept buffers
     size_t free_b = 0, total_b = 0;
     S615_CU(cudaMemGetInfo(&free_b, &total_b));
     size_t avail = std::min(free_b, ctx->budget > ctx->used ? ctx->budget - ctx->used : (size_t)0);
