@@ -160,7 +160,9 @@ typedef struct s615_solution {
 } s615_solution;
 
 /* ------------------------------------------------------------- context */
-/* Open device `device` with an HBM admission budget (0 = all free memory). */
+/* Open device `device` with an HBM admission budget (0 = all free memory).
+ * s615_close frees every table, batch buffer and host staging buffer the
+ * context holds (batches from s615_prepare are the caller's to free first). */
 int s615_open(int device, size_t hbm_budget, s615_ctx** out);
 int s615_close(s615_ctx* ctx);
 /* Change the HBM admission budget of an open context (0 = all device memory):
@@ -330,7 +332,10 @@ int s615_unit_status(const s615_unit* unit);
  * verify step.  Class-7 units go to their own persistent kernel, launched
  * after the first on the same stream.  Host units in, raw hits + counters out (hits unordered).
  * Returns S615_E_OVERFLOW (*n_hits = the true count) when hit_cap is too
- * small; at most 2^24 units per call. */
+ * small; at most 2^24 units per call.  The context keeps the call's device
+ * buffers for the next call; they count against the HBM budget and are given
+ * back when a table is built or loaded, when another allocation runs out of
+ * room, or on s615_close. */
 int s615_run(s615_ctx* ctx, int table_id, const s615_unit* units, size_t n, unsigned flags,
              s615_hit* hits, size_t hit_cap, size_t* n_hits, s615_counters* counters);
 /* run_cls5_gpu (fourcore_cls5_gpu_v4.cu:412-563) without the verify step:
