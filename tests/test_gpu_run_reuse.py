@@ -1,0 +1,79 @@
+"""s615_run keeps its batch between calls: results must not depend on what ran
+before (smaller, larger, overflowing or failed calls, table builds that take the
+buffers back), and dropped units keep their input index (GPU)."""
+import numpy as np
+import pytest
+
+import s615
+import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+N1 = 715
+
+
+def key(hits, ctr):
+    a = sorted((int(h["unit"]), int(h["d"]), int(h["e"]), int(h["fp"])) for h in hits)
+    return (ctr.calls, ctr.gated, ctr.probes, ctr.pos), a
+
+
+@pytest.fixture(scope="module")
+def setup(engine, oracle_table):
+    _, path = oracle_table(N1, 16)
+    tid = engine.load_table(path, N1)
+    units = W.cls5_units(1000, 30000)
+    plants = W.plants(8, 0, 1000, 30000, N1)
+    small = W.unit_array(units[:40], [], N1)
+    large = W.unit_array(units, plants, N1)
+    yield tid, small, large
+    engine.free_table(tid)
+
+
+def test_results_do_not_depend_on_earlier_calls(engine, setup):
+    tid, (sa, sn), (la, ln) = setup
+    first_small = key(*engine.run(tid, sa, sn))
+    first_large = key(*engine.run(tid, la, ln))
+    assert first_large[0][2] > first_small[0][2] > 0
+    for _ in range(2):
+        assert key(*engine.run(tid, sa, sn)) == first_small     # a larger batch ran before
+        assert key(*engine.run(tid, la, ln)) == first_large     # buffers grow back
+    # an overflowing call reports the true count and leaves the next call intact
+    with pytest.raises(s615.S615Error) as ei:
+        engine.run(tid, la, ln, hit_cap=1)
+    assert ei.value.status == -9
+    assert key(*engine.run(tid, sa, sn)) == first_small
+    # a failed call (a refused unit) keeps nothing and breaks nothing
+    bad, bn = W.unit_array([(40_000_001, 6)], [], N1)
+    with pytest.raises(s615.S615Error):
+        engine.run(tid, bad, bn)
+    assert key(*engine.run(tid, la, ln)) == first_large
+    # a table build takes the kept buffers back
+    t2 = engine.build_table(300, 16)
+    engine.free_table(t2)
+    assert key(*engine.run(tid, la, ln)) == first_large
+    # the plain form and the kept batch agree
+    assert key(*engine.run(tid, sa, sn, flags=s615.F_PLAIN)) == first_small
+
+
+def test_dropped_units_keep_input_indices(engine, setup):
+    tid, _, (la, ln) = setup
+    base = key(*engine.run(tid, la, ln))
+    # the same units with a dropped unit (u >= B) after every third one
+    units = W.cls5_units(1000, 30000)
+    plants = W.plants(8, 0, 1000, 30000, N1)
+    arr, _ = W.unit_array(units, plants, N1)
+    mixed, where = [], []
+    for i in range(ln):
+        where.append(len(mixed))
+        mixed.append(arr[i])
+        if i % 3 == 0:
+            d = s615.Unit()
+            d.cls, d.kind, d.B, d.u = 5, 0, 1003, 1008
+            mixed.append(d)
+    marr = (s615.Unit * len(mixed))(*mixed)
+    hits, ctr = engine.run(tid, marr, len(mixed))
+    back = {w: i for i, w in enumerate(where)}
+    assert all(int(h["unit"]) in back for h in hits)
+    hits = hits.copy()
+    hits["unit"] = [back[int(u)] for u in hits["unit"]]
+    assert key(hits, ctr) == base
