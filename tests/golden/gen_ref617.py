@@ -8,7 +8,7 @@ tri-skip counts, SOLUTION lines) to a JSON file.  It needs a GPU; run it on a
 GPU machine and copy the output to tests/golden/ref617.json, which
 tests/test_oracle617.py compares with the oracle on the same inputs.
 
-  python tests/golden/gen_ref617.py [out.json]
+  python tests/golden/gen_ref617.py OUT.json
 """
 import json
 import os
@@ -42,7 +42,9 @@ SUMMARY = re.compile(
 
 
 def main():
-    out = sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "ref617.json")
+    if len(sys.argv) != 2:
+        sys.exit("usage: gen_ref617.py OUT.json")
+    out = sys.argv[1]
     cases = []
     for lo, hi, r, gate, tri, classes in CASES:
         cmd = [BIN, str(lo), str(hi), classes, "--branch-a-only", "--r", str(r), "--quiet"]
