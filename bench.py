@@ -333,7 +333,7 @@ def run_reference(args, rank):
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u64", "data": "synthetic",
-            "config": {"workload": f"cls5 band B in [{lo}, {hi}], Stage-1 units; reference arm: "
+            "config": {"workload": f"cls5 band B in [{lo}, {hi}), Stage-1 units; reference arm: "
                                    f"{samples[0]} units per step on the host cores, N=2000 r={args.r} table"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": f"{samples[0]} units per step x {args.steps} steps"},
