@@ -111,9 +111,12 @@ struct Cls5Counters {  // device accumulators (u64 atomics)
 
 // Work items: (unit, residue index, chunk of kItemRows rows) packed in a u64.
 constexpr u32 kItemRows = 64;
-// (6,1,7) rows carry a whole c4 window each: 8 rows per item keep the
-// heaviest item short next to a pass.
+// (6,1,7) rows carry a whole c4 window each: 8 rows per item, and each such
+// chunk goes out as kParts617 items (chunk field = chunk * kParts617 + part) of
+// which part p takes every kParts617-th 32-wide block of the rows' c4 windows,
+// so that the heaviest rows are shared by several warps.
 constexpr u32 kItemRows617 = 8;
+constexpr u32 kParts617 = 8;
 S615_HD u32 item_rows(u32 cls) { return cls == 7u ? kItemRows617 : kItemRows; }
 constexpr u32 kC4Chunk = 128;   // cls 1: c4 values per work item
 constexpr u32 kMaxBatchUnits = 1u << 24;

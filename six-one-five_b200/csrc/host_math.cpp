@@ -706,12 +706,15 @@ void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out, u32 job
     for (u32 c = 0; c < n; ++c) out.push_back(make_item(unit_index, 0, c));
     return;
   }
-  const u32 per = d.cls == (u32)S615_CLS_617 ? item_rows(d.cls) : unit_rows;
+  const bool c617 = d.cls == (u32)S615_CLS_617;
+  const u32 per = c617 ? item_rows(d.cls) : unit_rows;
+  const u32 parts = c617 ? kParts617 : 1u;
   for (u32 ir = 0; ir < d.nres1; ++ir) {
     u32 jmin = 0, jend = 0;
     class_rows(d.res1[ir], d.mod1, d.fmax1, &jmin, &jend);
     const u32 rows = jend > jmin ? jend - jmin : 0;
-    for (u32 c = 0; c * per < rows; ++c) out.push_back(make_item(unit_index, ir, c));
+    for (u32 c = 0; c * per < rows; ++c)
+      for (u32 p = 0; p < parts; ++p) out.push_back(make_item(unit_index, ir, c * parts + p));
   }
 }
 

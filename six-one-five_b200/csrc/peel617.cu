@@ -298,6 +298,7 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Par
     I.cls = U->cls;
     I.lim = U->lim;
     u32 nrows;
+    u32 part = 0, nparts = 1;   // cls 7: this item's share of the rows' c4 blocks
     const bool single = I.cls == 1 || I.cls == S615_CLS_617_FIND4;
     if (single) {   // one row, T = base; this item's c4 are a chunk of [fmax2, fmax1]
       I.r0 = 0; I.mod = 0; I.j0 = 0;
@@ -307,7 +308,9 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Par
       I.mod = U->mod1;
       u32 jmin, jend;
       class_rows(I.r0, I.mod, U->fmax1, &jmin, &jend);
-      I.j0 = jmin + item_chunk(packed) * kItemRows617;
+      part = item_chunk(packed) % kParts617;
+      nparts = kParts617;
+      I.j0 = jmin + (item_chunk(packed) / kParts617) * kItemRows617;
       nrows = min(kItemRows617, jend - I.j0);
     }
     const bool tri = P.use_tri && I.cls != 1;   // cls 1 (k_find4) has no triple-sum gate
@@ -349,7 +352,7 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Par
           }
         }
       }
-      if (tri) my_tri += len4;
+      if (tri && part == 0) my_tri += len4;   // a row's c4 are counted once
       // ---- c4 step: triple-sum gate, survivors to the c4 queue ----
       u32 ch = 0, cl = 0;
       const u32 nd = min(32u, nrows - h);
@@ -358,7 +361,7 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Par
         if (L == 0) continue;
         const u32 lo = __shfl_sync(kFull, lo4, j);
         const u32 a504 = __shfl_sync(kFull, q504, j), a247 = __shfl_sync(kFull, q247, j);
-        for (u32 c0 = 0; c0 < L; c0 += 32u) {
+        for (u32 c0 = 32u * part; c0 < L; c0 += 32u * nparts) {
           const u32 c4 = lo + c0 + lane;
           bool pass = c0 + lane < L;
           if (pass && tri) {
