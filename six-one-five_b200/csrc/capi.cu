@@ -786,6 +786,9 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
     }
   }
   b->item_rows = unit_rows;
+  // a batch too small to fill the GPU even with 16-row items (a serving
+  // request) also splits each class 2-4 row chunk four ways over its tiles
+  b->parts3 = (!ctx->force_rows && !tuned.item_rows && unit_rows == 16) ? 4u : 1u;
   for (size_t k = 0; k < nd; ++k) {
     const DevUnit& d = du[k];
     if (d.cls == 0) continue;   // dropped
@@ -793,7 +796,7 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
     unit_items(d, (u32)k,
                (d.cls == S615_CLS_617 || d.cls == 1 || d.cls == S615_CLS_617_FIND4) ? items617
                                                                                 : b->host_items,
-               job_rows, unit_rows);
+               job_rows, unit_rows, b->parts3);
   }
   // heaviest first: a candidate's first rows (smallest d) have the largest T
   // and windows, so every candidate's chunk 0 goes out before any chunk 1
@@ -892,6 +895,7 @@ int s615_run_batch(s615_ctx* ctx, int id, s615_batch* b, unsigned flags, void* s
   one.d_ctr = b->d_ctr;
   one.d_work = b->d_work;
   one.item_rows = b->item_rows;
+  one.parts3 = b->parts3;
   one.blocks_per_sm = b->blocks_per_sm;
   size_t i = 0;
   while (i < b->n_items) {

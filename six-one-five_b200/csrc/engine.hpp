@@ -157,6 +157,9 @@ struct s615_batch {
   s615::Cls5Counters* d_ctr = nullptr;
   s615::u32* d_work = nullptr;   // persistent-queue cursors [classes 2-5, cls 7]
   s615::u32 item_rows = s615::kItemRows;   // rows per class 2-5 item (smaller for small batches)
+  // items per class 2-4 row chunk, 1, 2 or 4 (chunk field = chunk * parts3 +
+  // part): part p sieves every parts3-th 1024-column tile of the rows' c3 windows
+  s615::u32 parts3 = 1;
   s615::u32 blocks_per_sm = 0;              // k_peel blocks per SM (0: the occupancy limit)
   std::vector<s615::u64> host_items;
 };
@@ -292,7 +295,7 @@ int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip);
 // Job rows are grouped up to job_rows (<= kJobRows) per item; the row chunks
 // of classes 2-5 have unit_rows (<= kItemRows) rows each.
 void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out, u32 job_rows = kJobRows,
-                u32 unit_rows = kItemRows);
+                u32 unit_rows = kItemRows, u32 parts3 = 1);
 
 void gate_patterns(bool gated, int shape, u32 out[kPatWords]);
 void tri_tables(u32 out[kTriWords]);

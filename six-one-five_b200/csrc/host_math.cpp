@@ -687,7 +687,7 @@ int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip) {
 }
 
 void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out, u32 job_rows,
-                u32 unit_rows) {
+                u32 unit_rows, u32 parts3) {
   if (d.cls == kClsJobRow) {   // runs of up to kJobRows consecutive job rows of one kind
     const u32 kind = d.w != 0 ? kJobFind2 : 0u;
     if (!out.empty()) {
@@ -708,7 +708,7 @@ void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out, u32 job
   }
   const bool c617 = d.cls == (u32)S615_CLS_617;
   const u32 per = c617 ? item_rows(d.cls) : unit_rows;
-  const u32 parts = c617 ? kParts617 : 1u;
+  const u32 parts = c617 ? kParts617 : (d.cls >= 2 && d.cls <= 4) ? std::max(parts3, 1u) : 1u;
   for (u32 ir = 0; ir < d.nres1; ++ir) {
     u32 jmin = 0, jend = 0;
     class_rows(d.res1[ir], d.mod1, d.fmax1, &jmin, &jend);

@@ -48,6 +48,7 @@ struct WarpSmem {                 // one warp's private slice
   u8 M4[kMaxD][kRows];            // cls5: mod-8 admissibility of k mod 4
   u32 ring[kQ];
   u32 d0s[kMaxD];                 // cls5: d residues of the current pass
+  u32 part, nparts;               // class 2-4 items: this item's share of the window tiles
 };
 
 // With the sharp gate a cls5 row also carries the offsets for 31, 37, 43 and
@@ -76,6 +77,7 @@ struct PeelParams {
   u64 p64;                 // sharp gate: admissible values mod 64, as a bitmask
   u32 count;               // add this launch's counters (0 for a repeat pass over a set)
   u32 item_rows;           // rows per item of the batch (<= kRows)
+  u32 parts3_log2;         // log2 of the items per class 2-4 row chunk (1 or 4 items)
 };
 
 // cls5 pattern words (sharp or not) then the find3 ones, then the warp slices
@@ -198,9 +200,15 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
       I.mod = U->mod1;
       u32 jmin, jend;
       class_rows(I.r0, I.mod, U->fmax1, &jmin, &jend);
-      I.j0 = jmin + item_chunk(packed) * P.item_rows;
+      u32 ch = item_chunk(packed);
+      if (I.cls != 5) {   // kept in the warp's slice: the find3 loop reads them there
+        if (lane == 0) { W.part = ch & ((1u << P.parts3_log2) - 1u); W.nparts = 1u << P.parts3_log2; }
+        ch >>= P.parts3_log2;
+      }
+      I.j0 = jmin + ch * P.item_rows;
       nrows = min(P.item_rows, jend - I.j0);
     }
+    if (I.cls == kClsJobRow && lane == 0) { W.part = 0; W.nparts = 1; }
     u32 head = 0, qlen = 0;
     __syncwarp();
 
@@ -350,8 +358,10 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
             } else {
               set_offsets(R);
             }
-            my_calls += len;
-            my_pos += len;
+            if (W.part == 0) {   // a row's window is counted once
+              my_calls += len;
+              my_pos += len;
+            }
           }
         }
         W.rows[r] = R;
@@ -359,7 +369,7 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
       __syncwarp();
       // Sieve steps: a row's window in tiles of 1024 columns (lane = 32
       // columns), or for find2 items 32 one-column rows at once (lane = row).
-      u32 r = 0, wt = 0;
+      u32 r = 0, wt = W.part;
       while (r < nrows) {
         const u32 rr = find2 ? r + lane : r;
         const u32 kbase = find2 ? 0u : (wt * 32u + lane) * 32u;
@@ -382,8 +392,8 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
         push_bits<kSet>(P, W, m, 0, rr & 63u, kbase, head, qlen, I, lane);
         if (find2) {
           r += 32;
-        } else if (++wt >= (len + 1023u) / 1024u) {   // len is the same in every lane here
-          wt = 0;
+        } else if ((wt += W.nparts) >= (len + 1023u) / 1024u) {   // len: the same in every lane
+          wt = W.part;
           ++r;
         }
       }
@@ -433,6 +443,7 @@ int launch_main(s615_ctx* ctx, const TableView& tv, const s615_batch* b, size_t 
   P.p64 = ctx->p64;
   P.count = (flags & kFlagNoCount) ? 0u : 1u;
   P.item_rows = b->item_rows ? std::min(b->item_rows, kRows) : kRows;
+  P.parts3_log2 = b->parts3 >= 4 ? 2u : b->parts3 >= 2 ? 1u : 0u;
   P.pat3 = ctx->d_pat + 2 * kPatWords + (gated ? 0 : kPatWords);
   P.pat3s = ctx->d_sharp + kSharpWords;
   const u128 inv = inv_2adic_u128((u128)kM21);
