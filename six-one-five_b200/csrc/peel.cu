@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <type_traits>
 
 #include "peel_common.cuh"
@@ -421,12 +422,14 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
 template <bool kSharp, bool kSet>
 int launch_main(s615_ctx* ctx, const TableView& tv, const s615_batch* b, size_t n,
                 unsigned flags, cudaStream_t st, int grid_blocks) {
-  static bool attr_set = false;
+  // the shared-memory attribute belongs to each device's context: one bit per device
+  static std::atomic<unsigned long long> attr_set{0};
   constexpr size_t kSmemTotal = smem_total<kSharp>();
-  if (!attr_set) {
+  const unsigned long long dev_bit = 1ull << (ctx->device & 63);
+  if (!(attr_set.load() & dev_bit)) {
     S615_CU(cudaFuncSetAttribute(k_peel<kSharp, kSet>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kSmemTotal));
-    attr_set = true;
+    attr_set.fetch_or(dev_bit);
   }
   PeelParams P{};
   P.tv = tv;

@@ -28,6 +28,7 @@
 //    (B above about 514,000); its counters and raw hits then repeat those c4.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <type_traits>
 
 #include "peel_common.cuh"
@@ -417,12 +418,14 @@ namespace {
 template <bool kSharp, bool kSet>
 int launch617(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
               cudaStream_t st, int grid_blocks) {
-  static bool attr_set = false;
+  // the shared-memory attribute belongs to each device's context: one bit per device
+  static std::atomic<unsigned long long> attr_set{0};
   constexpr size_t kSmemTotal = smem_total617<kSharp>();
-  if (!attr_set) {
+  const unsigned long long dev_bit = 1ull << (ctx->device & 63);
+  if (!(attr_set.load() & dev_bit)) {
     S615_CU(cudaFuncSetAttribute(k_peel617<kSharp, kSet>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kSmemTotal));
-    attr_set = true;
+    attr_set.fetch_or(dev_bit);
   }
   const size_t n = b->n_items - b->n_main;
   if (n == 0) return S615_OK;
