@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "engine.hpp"
@@ -155,17 +156,33 @@ int s615_jobs_next(s615_jobs_file* f, s615_unit* out, size_t cap, size_t* n) {
   if (!f || !n || (cap && !out)) return S615_E_ARG;
   size_t k = 0;
   if (f->info.binary) {
+    // blocks of records read whole (up to 2^22 at a time), each decoded by up
+    // to 16 threads when it is large
     std::vector<uint8_t> buf;
-    while (k < cap) {   // whole blocks of records, decoded in place
-      const size_t want = std::min<size_t>(cap - k, 1u << 16);
+    while (k < cap) {
+      const size_t want = std::min<size_t>(cap - k, 1u << 22);
       buf.resize(want * kBbjRecord);
       const size_t got = std::fread(buf.data(), kBbjRecord, want, f->fp);
-      for (size_t i = 0; i < got; ++i) {
-        // JobBinRec {u8 cls, 3 pad, u32 B, u, free1, free2, u64 T_lo, T_hi}
-        const uint8_t* r = buf.data() + i * kBbjRecord;
-        out[k++] = make_job(r[0], get<uint32_t>(r + 4), get<uint32_t>(r + 8), get<uint32_t>(r + 12),
-                            get<uint32_t>(r + 16), get<uint64_t>(r + 20), get<uint64_t>(r + 28));
+      auto decode = [&](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; ++i) {
+          // JobBinRec {u8 cls, 3 pad, u32 B, u, free1, free2, u64 T_lo, T_hi}
+          const uint8_t* r = buf.data() + i * kBbjRecord;
+          out[k + i] = make_job(r[0], get<uint32_t>(r + 4), get<uint32_t>(r + 8),
+                                get<uint32_t>(r + 12), get<uint32_t>(r + 16),
+                                get<uint64_t>(r + 20), get<uint64_t>(r + 28));
+        }
+      };
+      const size_t nt = got < (1u << 16) ? 1
+                        : std::min<size_t>({16, got >> 16,
+                                            std::max(1u, std::thread::hardware_concurrency())});
+      if (nt <= 1) {
+        decode(0, got);
+      } else {
+        std::vector<std::thread> th;
+        for (size_t t = 0; t < nt; ++t) th.emplace_back(decode, got * t / nt, got * (t + 1) / nt);
+        for (auto& x : th) x.join();
       }
+      k += got;
       if (got < want) break;
     }
   } else {
