@@ -213,13 +213,15 @@ def timed_steps(lib, eng, tid, batch, stream, flags, steps):
     return e0.elapsed_time(e1), ctr
 
 
-def serve_latency(eng, tid, units, N, rate=5000.0, secs=4.0, req_units=50, seed=5, tune=False):
+def serve_latency(eng, tid, units, N, rate=5000.0, secs=8.0, req_units=50, seed=5, tune=False,
+                  warmup_s=0.5):
     """Per-unit latency under a Poisson stream of requests through the serving
     loop (s615_submit / s615_poll): `rate` units/s in requests of `req_units`
     units drawn from the band; a unit's latency is its request's
-    submit-to-verified-result time.  With tune, s615_autotune first tunes
-    batches of one and two requests (the loop's usual batches) on samples of
-    the band."""
+    submit-to-verified-result time.  Requests submitted in the first
+    `warmup_s` seconds (while the loop's slots grow their buffers) are served
+    but not counted.  With tune, s615_autotune first tunes batches of one and
+    two requests (the loop's usual batches) on samples of the band."""
     import numpy as np
 
     import s615
@@ -234,7 +236,13 @@ def serve_latency(eng, tid, units, N, rate=5000.0, secs=4.0, req_units=50, seed=
             _, best = eng.autotune(tid, arr, n)
             tuned.append({"units": k, "item_rows": best[0], "blocks_per_sm": best[1]})
     eng.serve_start(slots=2)
-    lat, batch_reqs, sent = [], [], 0
+    lat, batch_reqs, sent, warm = [], [], 0, set()
+
+    def take(r):
+        if r["ticket"] not in warm:
+            lat.extend([r["latency_ms"]] * r["n_units"])
+            batch_reqs.append(r["batch_requests"])
+
     try:
         t0 = time.perf_counter()
         nxt = t0
@@ -244,18 +252,18 @@ def serve_latency(eng, tid, units, N, rate=5000.0, secs=4.0, req_units=50, seed=
             while nxt <= now:
                 pick = [units[i] for i in rng.randint(0, len(units), size=req_units)]
                 arr, n = W.unit_array(pick, [], N)
-                eng.submit(tid, arr, n)
+                t = eng.submit(tid, arr, n)
+                if now - t0 < warmup_s:
+                    warm.add(t)
                 sent += 1
                 nxt += rng.exponential(req_units / rate)
             for r in eng.poll(wait_ms=1):
-                lat += [r["latency_ms"]] * r["n_units"]
-                batch_reqs.append(r["batch_requests"])
+                take(r)
                 done += 1
             time.sleep(max(0.0, min(0.001, nxt - time.perf_counter())))
         while done < sent:
             for r in eng.poll(wait_ms=100):
-                lat += [r["latency_ms"]] * r["n_units"]
-                batch_reqs.append(r["batch_requests"])
+                take(r)
                 done += 1
     finally:
         eng.serve_stop()
@@ -263,7 +271,8 @@ def serve_latency(eng, tid, units, N, rate=5000.0, secs=4.0, req_units=50, seed=
             eng.tune_reset()
     lat = np.array(lat)
     return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-            "units": int(lat.size), "requests": sent, "offered_units_per_s": rate,
+            "units": int(lat.size), "requests": sent, "warmup_requests_not_counted": len(warm),
+            "seconds": secs, "offered_units_per_s": rate,
             "request_units": req_units, "mean_requests_per_batch": float(np.mean(batch_reqs)),
             "tuned": tuned,
             "loop": "s615_serve_start(slots=2) + s615_submit/s615_poll, Poisson arrivals"}
