@@ -1,13 +1,13 @@
 #!/usr/bin/env python3
 """Regenerate tests/golden/golden.json.
 
-Run in a container that has the reference tree at /root/reference (read
-only).  It builds the reference's own buildable programs into oracle/_ref
+Run in a container that has the reference tree (read only), given as the
+first argument or in S615_REFERENCE.  It builds the reference's own buildable programs into oracle/_ref
 (oracle/Makefile `ref`), runs them, and records their outputs next to exact
 Python-integer values for the known-answer checks the reference's self-tests
 make.  The GPU box never runs this script; tests read the JSON only.
 
-  python tests/golden/gen_golden.py
+  python tests/golden/gen_golden.py REFERENCE_DIR
 """
 import hashlib
 import json
@@ -20,7 +20,7 @@ import tempfile
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 REF_BIN = os.path.join(ROOT, "oracle", "_ref")
-REF = "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("S615_REFERENCE", "")
 OUT = os.path.join(ROOT, "tests", "golden", "golden.json")
 
 
@@ -29,7 +29,9 @@ def run(cmd, **kw):
 
 
 def main():
-    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True,
+    if not os.path.isdir(REF):
+        sys.exit("usage: gen_golden.py REFERENCE_DIR (or set S615_REFERENCE)")
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={REF}"], check=True,
                    stdout=subprocess.DEVNULL)
     g = {}
 
