@@ -324,6 +324,12 @@ int s615_unit_status(const s615_unit* unit);
  * (the filter's false positives at rejected points are not probed) and
  * calls/gated/probes count the sharper gate.  Ignored with S615_F_NO_GATE. */
 #define S615_F_SHARP 8u
+/* Launch the peel kernels without their L2-persisting access window (no
+ * counterpart in the reference).  By default a table whose cells fit the
+ * device's persisting L2 set-aside is marked persisting for the launch, and a
+ * larger table's launches mark the gate pattern block instead; results are
+ * the same either way.  This flag exists to measure the window. */
+#define S615_F_NO_L2_WINDOW 16u
 
 /* The peel of a mixed batch of units (classes 2-5 and 7) in one persistent
  * launch per kernel: run_cls5_gpu's chunk loop (fourcore_cls5_gpu_v4.cu:
@@ -377,10 +383,13 @@ int s615_batch_size(const s615_batch* b, size_t* n_units, size_t* n_items, size_
  * (about 1.9 MB, held by every GPU that loads the library until exit).
  * Limits: n <= 4096 units, <= 65536 work items (S615_E_ARG beyond either),
  * <= 16384 raw hits (S615_E_OVERFLOW beyond, *n_hits = true count); flags may
- * only hold S615_F_NO_GATE.  The first call on a device looks up the array's
- * device address; make that first call before any stream capture.  All calls
- * share the array: calls that overlap on the GPU race; each call clears the
- * counters and cursor it needs and waits for its own results. */
+ * only hold S615_F_NO_GATE (S615_E_ARG otherwise); S615_E_BUSY while a serving
+ * loop owns the context.  Work items are cut like s615_cls5_run's (the tuned
+ * rows per item for this batch size, else 64 rows, or 32 / 16 for small
+ * batches).  The first call on a device looks up the array's device address;
+ * make that first call before any stream capture.  All calls and contexts on
+ * a GPU share the array: calls that overlap on the GPU race; each call clears
+ * the counters and cursor it needs and waits for its own results. */
 int s615_cls5_run_noalloc(s615_ctx* ctx, int table_id, const s615_unit* units, size_t n,
                           unsigned flags, s615_hit* hits, size_t hit_cap, size_t* n_hits,
                           s615_counters* counters);

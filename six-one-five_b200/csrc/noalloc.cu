@@ -74,6 +74,7 @@ extern "C" int s615_cls5_run_noalloc(s615_ctx* ctx, int table_id, const s615_uni
                                      s615_counters* counters) {
   if (!ctx || (n && !units) || (flags & ~S615_F_NO_GATE)) return S615_E_ARG;
   if (n > kMaxUnits) return S615_E_ARG;
+  if (serving_blocks(ctx)) return S615_E_BUSY;   // the request loop owns the context
   auto it = ctx->tables.find(table_id);
   if (it == ctx->tables.end()) return S615_E_NOTABLE;
   S615_CU(cudaSetDevice(ctx->device));
@@ -81,6 +82,38 @@ extern "C" int s615_cls5_run_noalloc(s615_ctx* ctx, int table_id, const s615_uni
   int s = scratch_for(ctx->device, &S);
   if (s) return s;
   cudaStream_t st = ctx->stream;
+
+  // Rows per work item, by the rule s615_run uses: the autotuned choice for
+  // this batch size if there is one, else 64 rows, or 32 / 16 when 64-row
+  // items would give fewer than about 40 warps per SM.  A size whose items
+  // would not fit the scratch falls back to longer items.
+  u64 items_at[3] = {0, 0, 0};   // items with 64, 32 and 16 rows
+  for (size_t i = 0; i < n; ++i) {
+    if (units[i].cls != 5) return S615_E_FORMAT;
+    DevUnit d;
+    bool skip = false;
+    if ((s = make_dev_unit(units[i], (u32)i, &d, &skip))) return s;
+    if (skip) continue;
+    for (u32 ie = 0; ie < d.nres1; ++ie) {
+      u32 jmin = 0, jend = 0;
+      class_rows(d.res1[ie], d.mod1, d.fmax1, &jmin, &jend);
+      const u32 rows = jend > jmin ? jend - jmin : 0;
+      for (int k = 0; k < 3; ++k) items_at[k] += (rows + (kItemRows >> k) - 1) / (kItemRows >> k);
+    }
+  }
+  u32 bucket = 0;
+  while (bucket < 39 && (2ull << bucket) <= n) ++bucket;
+  const auto& tuned = ctx->tune[bucket];
+  u32 unit_rows = kItemRows;
+  if (tuned.item_rows) {
+    unit_rows = tuned.item_rows;
+  } else {
+    const u64 want_items = (u64)ctx->num_sms * 40;
+    while (unit_rows > 16 && items_at[unit_rows == 64 ? 0 : 1] < want_items) unit_rows /= 2;
+  }
+  while (unit_rows < kItemRows &&
+         items_at[unit_rows == 32 ? 1 : unit_rows == 16 ? 2 : 0] > kMaxItems)
+    unit_rows *= 2;
 
   // Unit records and work items, staged through small stack buffers (the
   // pageable copies have consumed a buffer by the time they return).
@@ -101,7 +134,6 @@ extern "C" int s615_cls5_run_noalloc(s615_ctx* ctx, int table_id, const s615_uni
     return S615_OK;
   };
   for (size_t i = 0; i < n; ++i) {
-    if (units[i].cls != 5) return S615_E_FORMAT;
     DevUnit d;
     bool skip = false;
     if ((s = make_dev_unit(units[i], (u32)i, &d, &skip))) return s;
@@ -110,7 +142,7 @@ extern "C" int s615_cls5_run_noalloc(s615_ctx* ctx, int table_id, const s615_uni
       u32 jmin = 0, jend = 0;
       class_rows(d.res1[ie], d.mod1, d.fmax1, &jmin, &jend);
       const u32 rows = jend > jmin ? jend - jmin : 0;
-      for (u32 c = 0; c * kItemRows < rows; ++c) {
+      for (u32 c = 0; c * unit_rows < rows; ++c) {
         if (ni == kMaxItems) return S615_E_ARG;
         istage[is++] = make_item((u32)nu, ie, c);
         ++ni;
@@ -136,6 +168,8 @@ extern "C" int s615_cls5_run_noalloc(s615_ctx* ctx, int table_id, const s615_uni
   b.hit_cap = (u32)kMaxHits;
   b.d_ctr = &S->ctr;
   b.d_work = &S->work;
+  b.item_rows = unit_rows;
+  b.blocks_per_sm = tuned.blocks_per_sm;
   if ((s = launch_peel(ctx, view_of(it->second), &b, flags, st, 0))) return s;
 
   Cls5Counters c{};
