@@ -201,6 +201,39 @@ int finish_upload(s615_ctx* ctx, DevTable& t, void* d_packed, size_t packed_allo
 }  // namespace
 
 // ======================================================================= ABI
+namespace s615 {
+
+int l2_window(s615_ctx* ctx, const TableView& tv, unsigned flags, cudaLaunchAttribute* attr) {
+  if ((flags & S615_F_NO_L2_WINDOW) || !ctx->l2_persist_max || !ctx->l2_window_max) return 0;
+  const void* base = nullptr;
+  size_t bytes = 0;
+  if (tv.shards <= 1 && tv.cells && tv.bytes && tv.bytes <= ctx->l2_persist_max &&
+      tv.bytes <= ctx->l2_window_max) {
+    base = tv.cells;   // the whole table stays in L2
+    bytes = tv.bytes;
+  } else {
+    base = ctx->d_pat;   // only the gate patterns (the table streams through L2)
+    bytes = (4 * kPatWords + kTriWords + 2 * kSharpWords) * sizeof(u32);
+  }
+  if (ctx->l2_limit < bytes) {   // reserve the set-aside once (this process only)
+    const size_t want = ctx->l2_persist_max;
+    if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    ctx->l2_limit = want;
+  }
+  attr->id = cudaLaunchAttributeAccessPolicyWindow;
+  attr->val.accessPolicyWindow.base_ptr = const_cast<void*>(base);
+  attr->val.accessPolicyWindow.num_bytes = bytes;
+  attr->val.accessPolicyWindow.hitRatio = 1.0f;
+  attr->val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+  attr->val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+  return 1;
+}
+
+}  // namespace s615
+
 extern "C" {
 
 const char* s615_strerror(int s) {
@@ -236,6 +269,14 @@ int s615_open(int device, size_t hbm_budget, s615_ctx** out) {
   S615_CU(cudaFree(nullptr));
   S615_CU(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
   S615_CU(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
+  int l2p = 0, l2w = 0;
+  if (cudaDeviceGetAttribute(&l2p, cudaDevAttrMaxPersistingL2CacheSize, device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&l2w, cudaDevAttrMaxAccessPolicyWindowSize, device) != cudaSuccess) {
+    cudaGetLastError();
+    l2p = l2w = 0;
+  }
+  ctx->l2_persist_max = (size_t)(l2p > 0 ? l2p : 0);
+  ctx->l2_window_max = (size_t)(l2w > 0 ? l2w : 0);
   size_t free_b = 0, total_b = 0;
   S615_CU(cudaMemGetInfo(&free_b, &total_b));
   ctx->budget = hbm_budget ? hbm_budget : total_b;

@@ -102,6 +102,7 @@ struct TableView {
   u64 shard_seed;
   u32 grp_lo, grp_hi;   // this pass probes keys of shards [grp_lo, grp_hi)
   u32 groups, pad;      // passes over the set
+  u64 bytes;            // bytes of cells (a single table; 0 for a set)
 };
 
 struct Cls5Counters {  // device accumulators (u64 atomics)
@@ -204,6 +205,10 @@ struct s615_ctx {
   s615::HostStage unit_stage;
   s615_batch* run_batch = nullptr;
   bool run_busy = false;
+  // L2-persisting access windows (cudaDevAttrMaxPersistingL2CacheSize,
+  // cudaDevAttrMaxAccessPolicyWindowSize) and the set-aside this context
+  // has asked for (cudaLimitPersistingL2CacheSize, per process).
+  size_t l2_persist_max = 0, l2_window_max = 0, l2_limit = 0;
 };
 
 namespace s615 {
@@ -238,6 +243,13 @@ int arena_get(s615_ctx* ctx, int k, size_t bytes, void** p);
 int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b);
 
 TableView view_of(const DevTable& t);
+
+// The launch attribute for a peel kernel's L2-persisting access window: the
+// table's cells when they fit the persisting set-aside (the window's lines
+// stay in L2 while other traffic streams past), else the gate pattern block
+// the kernels read.  Returns the number of attributes written (0 or 1); 0
+// with S615_F_NO_L2_WINDOW or when the device offers no persisting L2.
+int l2_window(s615_ctx* ctx, const TableView& tv, unsigned flags, cudaLaunchAttribute* attr);
 
 // Kernel launchers (each returns a status and counts its launches).
 // Launches k_peel over items [0, n_main) and, when present, the (6,1,7)

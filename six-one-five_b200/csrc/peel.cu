@@ -463,7 +463,15 @@ int launch_main(s615_ctx* ctx, const TableView& tv, const s615_batch* b, size_t 
   }
   const size_t need = (n + kWarps - 1) / kWarps;
   if ((size_t)grid > need) grid = (int)need;
-  k_peel<kSharp, kSet><<<grid, kThreads, kSmemTotal, st>>>(P);
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = kSmemTotal;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  cfg.attrs = attr;
+  cfg.numAttrs = (unsigned)l2_window(ctx, tv, flags, attr);
+  S615_CU(cudaLaunchKernelEx(&cfg, k_peel<kSharp, kSet>, P));
   ctx->launches++;
   S615_CU(cudaGetLastError());
   return S615_OK;

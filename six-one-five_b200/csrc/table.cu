@@ -89,6 +89,7 @@ TableView view_of(const DevTable& t) {
     return v;
   }
   v.cells = t.d_cells;
+  v.bytes = t.bytes;
   v.block = t.hdr.m_cells / 3;
   v.recip = mod_recip(v.block);
   v.fpmask = fp_mask(t.hdr.r);

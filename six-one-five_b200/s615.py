@@ -22,7 +22,7 @@ STATUS = {
     -7: "DEVICE", -8: "TIMEOUT", -9: "OVERFLOW", -10: "BUILD", -11: "NOTABLE", -12: "BUSY",
 }
 LAYOUT_AUTO, LAYOUT_PACKED, LAYOUT_WIDE = 0, 1, 2
-F_NO_GATE, F_PLAIN, F_NO_TRI, F_SHARP = 1, 2, 4, 8
+F_NO_GATE, F_PLAIN, F_NO_TRI, F_SHARP, F_NO_L2_WINDOW = 1, 2, 4, 8, 16
 S615_CLS_617 = 7
 S615_CLS_617_FIND4 = 8
 S615_KIND_JOB = 2
