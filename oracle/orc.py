@@ -99,6 +99,8 @@ _SIG = {
     "orc_table_bytes": (C.POINTER(C.c_uint8), [_P, C.POINTER(C.c_size_t)]),
     "orc_query": (None, [_P, _P, C.c_size_t, _P]),
     "orc_fpr_smoke": (C.c_int, [_P]),
+    "orc_residue": (None, [_P, _P, C.c_size_t, _P]),
+    "orc_mt64": (None, [C.c_uint64, C.c_size_t, _P]),
     "orc_cls5_run": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_int, _P, C.c_size_t, _P]),
     "orc_cls5_verify": (C.c_size_t, [_P, _P, C.c_size_t, C.c_int, C.c_int, C.c_char_p, C.c_size_t]),
     "orc_expand_cls234": (C.c_size_t, [C.c_uint64, C.c_uint64, C.c_int, _P, C.c_size_t]),
@@ -206,6 +208,13 @@ class Table:
         lib().orc_query(self.h, _ptr(k), k.size, _ptr(out))
         return out
 
+    def residue(self, keys) -> np.ndarray:
+        """cell(i0) ^ cell(i1) ^ cell(i2) ^ fingerprint per key (0 iff "maybe")."""
+        k = np.ascontiguousarray(np.asarray(keys, dtype=np.uint64))
+        out = np.zeros(k.size, dtype=np.uint64)
+        lib().orc_residue(self.h, _ptr(k), k.size, _ptr(out))
+        return out
+
     def fpr_smoke(self) -> int:
         return lib().orc_fpr_smoke(self.h)
 
@@ -215,6 +224,13 @@ class Table:
                 lib().orc_free(self.h)
         except Exception:
             pass
+
+
+def mt64(seed: int, n: int) -> np.ndarray:
+    """n draws of std::mt19937_64(seed) (the reference FPR test's non-key stream)."""
+    out = np.zeros(n, dtype=np.uint64)
+    lib().orc_mt64(seed, n, _ptr(out))
+    return out
 
 
 def shard_of(key: int, S: int, seed: int = SHARD_SEED) -> int:

@@ -25,6 +25,7 @@
 
 #ifdef _OPENMP
 #include <omp.h>
+#include <random>
 #endif
 
 typedef unsigned __int128 u128;
@@ -682,6 +683,28 @@ const uint8_t* orc_table_bytes(const orc_table* t, size_t* n) { *n = t->packed.s
 void orc_query(const orc_table* t, const uint64_t* keys, size_t n, uint8_t* out) {
 #pragma omp parallel for schedule(static)
   for (long long i = 0; i < (long long)n; ++i) out[i] = might_contain(*t, keys[i]) ? 1 : 0;
+}
+// The filter's residue for each key of a single table: cell(i0) ^ cell(i1) ^
+// cell(i2) ^ (h & mask), zero exactly when xor_might_contain answers "maybe"
+// (xor_filter.hpp:472-483).  For a non-key every r-bit residue is equally
+// likely, so the rate of residues whose low b bits are zero is 2^-b; this
+// measures the fingerprint statistics of a wide (r = 48) table, whose
+// false-positive rate 2^-48 no sample can reach.
+void orc_residue(const orc_table* t, const uint64_t* keys, size_t n, uint64_t* out) {
+  const u64 block = t->hdr.m_cells / 3;
+#pragma omp parallel for schedule(static)
+  for (long long i = 0; i < (long long)n; ++i) {
+    const u64 h = mix64(keys[i] + t->hdr.mix_seed);
+    u64 hs[3]; hashes3(h, block, hs);
+    out[i] = load_cell(t->packed.data(), hs[0], t->hdr.r) ^ load_cell(t->packed.data(), hs[1], t->hdr.r) ^
+             load_cell(t->packed.data(), hs[2], t->hdr.r) ^ (h & fp_mask(t->hdr.r));
+  }
+}
+// n draws of std::mt19937_64(seed): the non-key stream of the reference's FPR
+// test (spike/ribbon/xor_filter_test.cpp:67-75 seeds it with 0xF15EED + n).
+void orc_mt64(uint64_t seed, size_t n, uint64_t* out) {
+  std::mt19937_64 rng(seed);
+  for (size_t i = 0; i < n; ++i) out[i] = rng();
 }
 int orc_fpr_smoke(const orc_table* t) {  // fourcore_xor_store.hpp:54-65
   if (t->parts.empty() && (t->packed.empty() || t->hdr.m_cells < 3 || t->hdr.r == 0)) return -1;

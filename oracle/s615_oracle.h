@@ -88,6 +88,8 @@ const uint8_t* orc_table_bytes(const orc_table* t, size_t* n);
 void orc_query(const orc_table* t, const uint64_t* keys, size_t n, uint8_t* out);
 /* xor_fpr_smoke (fourcore_xor_store.hpp:54-65). */
 int orc_fpr_smoke(const orc_table* t);
+void orc_residue(const orc_table* t, const uint64_t* keys, size_t n, uint64_t* out);
+void orc_mt64(uint64_t seed, size_t n, uint64_t* out);
 
 /* ---- cls5 peel (k_cls5_192, fourcore_cls5_gpu_v4.cu:353-410) ---- */
 /* Runs every unit; hits (unit index, d, e, fp) appended up to cap; counters
