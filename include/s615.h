@@ -415,6 +415,30 @@ int s615_cls5_verify(s615_ctx* ctx, const s615_unit* units, size_t n_units,
  * Needs no GPU.  Returns 0 on success, else the number of the failed check. */
 int s615_selftest_host(void);
 
+/* ------------------------------------------------------------- journal */
+/* Restart journal of a campaign (no counterpart in the reference, whose
+ * restarts redo the whole band, fourcore_runbook_v3.md:162-170): an
+ * append-only text file of committed blocks, one per finished request or
+ * chunk, holding the block's units, their raw hits and their verified
+ * solutions (hit and solution unit indices refer to the block's units).  A
+ * block counts only once its closing checksum line is complete, so a block
+ * torn by a crash is ignored and its units are searched again; opening the
+ * journal cuts such a tail off before anything is appended.
+ * s615_journal_append flushes and fsyncs before it returns.  A journal
+ * handle is not thread-safe. */
+typedef struct s615_journal s615_journal;
+int s615_journal_open(const char* path, s615_journal** out);   /* creates the file if missing */
+/* 1 if the unit (every field equal) is in a committed block, else 0. */
+int s615_journal_has(const s615_journal* j, const s615_unit* unit);
+int s615_journal_stats(const s615_journal* j, size_t* units, size_t* hits, size_t* solutions);
+/* Committed units in file order, and the recorded solutions with `unit`
+ * indexing that list (to report them again after a restart). */
+int s615_journal_units(const s615_journal* j, s615_unit* out, size_t cap, size_t* n);
+int s615_journal_solutions(const s615_journal* j, s615_solution* out, size_t cap, size_t* n);
+int s615_journal_append(s615_journal* j, const s615_unit* units, size_t n, const s615_hit* hits,
+                        size_t n_hits, const s615_solution* sols, size_t n_sols);
+int s615_journal_close(s615_journal* j);
+
 /* ------------------------------------------------------------- serving */
 /* A long-running request loop on one context (no counterpart in the
  * reference, which runs one campaign per process).  s615_submit queues a copy

@@ -9,12 +9,17 @@
 // --plant COUNT[:SEED] (adds planted targets in the reference's plant shape,
 // solve_516_v3.cu:1130-1170, and reports how many were recovered) and
 // --serve (reads .buc lines from stdin and runs them through the serving
-// loop as they arrive, printing SOLUTION lines as their requests finish).
+// loop as they arrive, printing SOLUTION lines as their requests finish) and
+// --journal F (a restart journal: every finished chunk or request is
+// committed to F with its raw hits and solutions; a rerun with the same F
+// prints the recorded SOLUTION lines again and searches only the units that
+// are not committed yet).
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -38,7 +43,9 @@ void usage() {
       "                 [--allow-rebuild] [--dump-survivors F] [--plain]\n"
       "                 [--layout packed|wide] [--batch K] [--plant COUNT[:SEED]]\n"
       "                 [--shards S [--save-shards PREFIX]] [--load-shards F0,F1,..]\n"
-      "   or: s615_cls5 --serve --N K [--load-table F] [--r BITS] [--batch K] < units.buc\n"
+      "                 [--journal F]\n"
+      "   or: s615_cls5 --serve --N K [--load-table F] [--r BITS] [--batch K]\n"
+      "                 [--journal F] < units.buc\n"
       "   or: s615_cls5 --check-table --N K --load-table F\n"
       "                 [--r BITS] [--save-table F] [--allow-rebuild]\n"
       "  --load-table F: packed xor from xor_build_save / --save-table.\n"
@@ -46,7 +53,8 @@ void usage() {
       "  --allow-rebuild: if --load-table fails, build on the device (default: FATAL).\n"
       "  --check-table: load + FPR smoke only.\n"
       "  --shards S: build the table as S pair-space shards (a probe asks only its\n"
-      "      key's shard); lifts the soft cap to N <= 240000 as HBM allows.\n");
+      "      key's shard); lifts the soft cap to N <= 240000 as HBM allows.\n"
+      "  --journal F: commit finished units to F; a rerun resumes from it.\n");
 }
 
 int selftest_host() {
@@ -110,6 +118,41 @@ std::vector<Plant> make_plants(int count, u64 seed, u64 B_max, int N, std::vecto
     ps.push_back(p);
   }
   return ps;
+}
+
+void print_solution(const s615_solution& S) {   // fourcore_cls5_gpu_v4.cu:533-536
+  std::printf("SOLUTION cls=5 B=%llu u=%llu a1=%lld a2=%lld a3=%lld a4=%lld a5=%lld gcd=%lld %s\n",
+              (unsigned long long)S.B, (unsigned long long)S.u, (long long)S.a[0], (long long)S.a[1],
+              (long long)S.a[2], (long long)S.a[3], (long long)S.a[4], (long long)S.gcd,
+              S.gcd == 1 ? "primitive" : "NON-PRIMITIVE");
+}
+
+// Opens the journal and reports what it holds; nullptr (with a message) on error.
+s615_journal* open_journal(const std::string& path) {
+  s615_journal* j = nullptr;
+  const int s = s615_journal_open(path.c_str(), &j);
+  if (s) {
+    std::fprintf(stderr, "[journal] cannot open %s: %s\n", path.c_str(), s615_strerror(s));
+    return nullptr;
+  }
+  size_t nu = 0, nh = 0, ns = 0;
+  s615_journal_stats(j, &nu, &nh, &ns);
+  std::fprintf(stderr, "[journal] %s: %zu committed units, %zu raw hits, %zu solutions\n", path.c_str(),
+               nu, nh, ns);
+  return j;
+}
+
+// The journal's recorded solutions of kind 0, printed again (a resumed run's
+// stdout then holds every SOLUTION line of the campaign); returns how many.
+unsigned long long replay_solutions(s615_journal* j) {
+  size_t n = 0;
+  s615_journal_solutions(j, nullptr, 0, &n);
+  std::vector<s615_solution> v(n);
+  if (n) s615_journal_solutions(j, v.data(), v.size(), &n);
+  unsigned long long k = 0;
+  for (const s615_solution& S : v)
+    if (S.kind == 0) { print_solution(S); ++k; }
+  return k;
 }
 
 bool load_buc5(const char* path, std::vector<Line>& out) {  // fourcore_cls5_gpu_v4.cu:155-167
@@ -231,7 +274,7 @@ bool acquire(s615_ctx* ctx, int N, int& r, const std::string& load, const std::s
 int main(int argc, char** argv) {
   std::setvbuf(stdout, nullptr, _IOLBF, 0);
   std::setvbuf(stderr, nullptr, _IOLBF, 0);
-  std::string units_path, load_table, save_table, dump_path, load_shards, save_shards;
+  std::string units_path, load_table, save_table, dump_path, load_shards, save_shards, journal_path;
   int device = 0, N_override = 0, xor_r = 48, layout = S615_LAYOUT_AUTO, shards = 1;
   size_t batch = 1 << 16;
   bool do_host = false, quiet = true, use_gate = true, stop_first = false;
@@ -262,6 +305,7 @@ int main(int argc, char** argv) {
     else if (s == "--dump-survivors") dump_path = next();
     else if (s == "--plain") plain = true;
     else if (s == "--serve") serve = true;
+    else if (s == "--journal") journal_path = next();
     else if (s == "--plant") {
       const std::string v = next();
       plant_count = std::atoi(v.c_str());
@@ -336,9 +380,20 @@ int main(int argc, char** argv) {
       return 1;
     }
     std::vector<s615_unit> pend;
-    size_t submitted = 0, finished = 0, n_units = 0;
+    size_t submitted = 0, finished = 0, n_units = 0, resumed = 0;
     unsigned long long sols = 0, calls = 0, probes = 0;
     std::vector<s615_result> res(64);
+    s615_journal* jr = nullptr;
+    std::map<uint64_t, std::vector<s615_unit>> inflight;   // ticket -> units (journal)
+    bool jfail = false;
+    if (!journal_path.empty()) {
+      if (!(jr = open_journal(journal_path))) {
+        s615_serve_stop(ctx);
+        s615_close(ctx);
+        return 1;
+      }
+      sols += replay_solutions(jr);
+    }
     auto drain = [&](int wait_ms) {
       size_t k = 0;
       s615_poll(ctx, res.data(), res.size(), &k, wait_ms);
@@ -348,12 +403,18 @@ int main(int argc, char** argv) {
         for (u64 j = 0; j < R.n_solutions; ++j) {
           const s615_solution& S = R.solutions[j];
           if (S.kind != 0) continue;
-          std::printf("SOLUTION cls=5 B=%llu u=%llu a1=%lld a2=%lld a3=%lld a4=%lld a5=%lld gcd=%lld %s\n",
-                      (u64)S.B, (u64)S.u, (long long)S.a[0], (long long)S.a[1], (long long)S.a[2],
-                      (long long)S.a[3], (long long)S.a[4], (long long)S.gcd,
-                      S.gcd == 1 ? "primitive" : "NON-PRIMITIVE");
+          print_solution(S);
           ++sols;
         }
+        if (jr && R.status == S615_OK) {   // commit the request once it is reported
+          const auto& us = inflight[R.ticket];
+          if (s615_journal_append(jr, us.data(), us.size(), R.hits, R.n_hits, R.solutions,
+                                  R.n_solutions) != S615_OK) {
+            std::fprintf(stderr, "[journal] append failed\n");
+            jfail = true;
+          }
+        }
+        inflight.erase(R.ticket);
         if (!quiet)
           std::fprintf(stderr, "[cls5-gpu] request %llu: %llu units, %.1f ms\n", (u64)R.ticket,
                        (u64)R.n_units, R.latency_ms);
@@ -364,7 +425,10 @@ int main(int argc, char** argv) {
     auto submit = [&]() {
       if (pend.empty()) return;
       uint64_t t = 0;
-      if (s615_submit(ctx, tid, pend.data(), pend.size(), flags, &t) == S615_OK) ++submitted;
+      if (s615_submit(ctx, tid, pend.data(), pend.size(), flags, &t) == S615_OK) {
+        ++submitted;
+        if (jr) inflight[t] = pend;
+      }
       n_units += pend.size();
       pend.clear();
     };
@@ -377,6 +441,7 @@ int main(int argc, char** argv) {
       s615_unit U{};
       U.cls = 5; U.B = B; U.u = u;
       if (s615_unit_status(&U) != S615_OK) continue;
+      if (jr && s615_journal_has(jr, &U) == 1) { ++resumed; continue; }
       pend.push_back(U);
       if (pend.size() >= batch) submit();
       drain(0);
@@ -385,10 +450,14 @@ int main(int argc, char** argv) {
     while (finished < submitted) drain(100);
     s615_serve_stop(ctx);
     (void)calls; (void)probes;
+    if (jr) {
+      std::fprintf(stderr, "[journal] %zu units already committed, %zu searched now\n", resumed, n_units);
+      if (s615_journal_close(jr) != S615_OK) jfail = true;
+    }
     std::printf("---- done cls5-gpu serve: solutions=%llu units=%zu requests=%zu time=%.1fs ----\n", sols,
-                n_units, submitted, std::chrono::duration<double>(Clock::now() - t0).count());
+                n_units + resumed, submitted, std::chrono::duration<double>(Clock::now() - t0).count());
     s615_close(ctx);
-    return 0;
+    return jfail ? 1 : 0;
   }
 
   std::vector<Line> lines;
@@ -445,17 +514,53 @@ int main(int argc, char** argv) {
   }
   const unsigned flags = (use_gate ? 0u : S615_F_NO_GATE) | (plain ? S615_F_PLAIN : 0u);
   unsigned long long tot_calls = 0, tot_gated = 0, tot_probes = 0, sols = 0;
+  // With a journal, committed units are skipped (their solutions printed
+  // again) and the rest are searched in order; `order` holds the indices into
+  // `units` still to search, kept contiguous in `work`.
+  s615_journal* jr = nullptr;
+  std::vector<s615_unit> work;
+  std::vector<size_t> order;
+  if (!journal_path.empty()) {
+    if (!(jr = open_journal(journal_path))) { s615_close(ctx); return 1; }
+    sols += replay_solutions(jr);
+    size_t n = 0;
+    s615_journal_solutions(jr, nullptr, 0, &n);
+    std::vector<s615_solution> old(n);
+    if (n) s615_journal_solutions(jr, old.data(), n, &n);
+    size_t nu = 0;
+    s615_journal_units(jr, nullptr, 0, &nu);
+    std::vector<s615_unit> jus(nu);
+    if (nu) s615_journal_units(jr, jus.data(), nu, &nu);
+    for (const s615_solution& S : old) {   // plants recovered before the restart
+      if (S.kind != 1) continue;
+      for (size_t pi = 0; pi < plants.size(); ++pi) {
+        const Plant& P = plants[pi];
+        if (!std::memcmp(&jus[S.unit], &units[n_stage1 + pi], sizeof(s615_unit)) && S.e == P.e &&
+            S.d == P.d && S.c1 == P.c1 && S.c2 == P.c2)
+          plant_got[pi] = 1;
+      }
+    }
+    for (size_t i = 0; i < units.size(); ++i)
+      if (s615_journal_has(jr, &units[i]) != 1) order.push_back(i);
+    std::fprintf(stderr, "[journal] %zu of %zu units already committed; searching %zu\n",
+                 units.size() - order.size(), units.size(), order.size());
+  } else {
+    order.resize(units.size());
+    for (size_t i = 0; i < units.size(); ++i) order[i] = i;
+  }
+  work.reserve(order.size());
+  for (size_t i : order) work.push_back(units[i]);
   const auto t0 = Clock::now();
   std::vector<s615_hit> hits;
   std::vector<s615_solution> solv;
   size_t chunk_no = 0;
-  for (size_t off = 0; off < units.size(); off += batch, ++chunk_no) {
-    const size_t n = std::min(batch, units.size() - off);
+  for (size_t off = 0; off < work.size(); off += batch, ++chunk_no) {
+    const size_t n = std::min(batch, work.size() - off);
     size_t cap = std::max<size_t>(hits.size(), 1 << 16), nh = 0;
     s615_counters c{};
     for (;;) {
       hits.resize(cap);
-      s = s615_cls5_run(ctx, tid, units.data() + off, n, flags, hits.data(), cap, &nh, &c);
+      s = s615_cls5_run(ctx, tid, work.data() + off, n, flags, hits.data(), cap, &nh, &c);
       if (s == S615_E_OVERFLOW && nh > cap) { cap = nh + nh / 4; continue; }
       break;
     }
@@ -467,46 +572,57 @@ int main(int argc, char** argv) {
     tot_calls += c.calls; tot_gated += c.gated; tot_probes += c.probes;
     if (dump)
       for (size_t k = 0; k < nh; ++k) {
-        const s615_unit& U = units[off + hits[k].unit];
+        const s615_unit& U = work[off + hits[k].unit];
         std::fprintf(dump, "%llu %llu %u %u %llu\n", (unsigned long long)U.B, (unsigned long long)U.u,
                      hits[k].d, hits[k].e, (unsigned long long)hits[k].fp);
       }
+    size_t ns = 0;
     if (nh) {
-      size_t ns = 0;
       size_t scap = std::max<size_t>(16, nh);
       solv.resize(scap);
-      s = s615_cls5_verify(ctx, units.data() + off, n, hits.data(), nh, N, solv.data(), scap, &ns);
+      s = s615_cls5_verify(ctx, work.data() + off, n, hits.data(), nh, N, solv.data(), scap, &ns);
       if (s && s != S615_E_OVERFLOW) {
         std::fprintf(stderr, "[cls5-gpu] verify failed: %s\n", s615_strerror(s));
         s615_close(ctx);
         return 1;
       }
-      for (size_t k = 0; k < std::min(ns, scap); ++k) {
+      ns = std::min(ns, scap);
+      for (size_t k = 0; k < ns; ++k) {
         const s615_solution& S = solv[k];
         if (S.kind == 1) {   // a recovered plant: its exact planted (e, d, c1, c2)?
-          const size_t pi = off + S.unit - n_stage1;
-          if (off + S.unit >= n_stage1 && pi < plants.size()) {
+          const size_t ui = order[off + S.unit];
+          const size_t pi = ui - n_stage1;
+          if (ui >= n_stage1 && pi < plants.size()) {
             const Plant& P = plants[pi];
             if (S.e == P.e && S.d == P.d && S.c1 == P.c1 && S.c2 == P.c2) plant_got[pi] = 1;
           }
           continue;
         }
         if (S.kind != 0) continue;
-        std::printf("SOLUTION cls=5 B=%llu u=%llu a1=%lld a2=%lld a3=%lld a4=%lld a5=%lld gcd=%lld %s\n",
-                    (unsigned long long)S.B, (unsigned long long)S.u, (long long)S.a[0],
-                    (long long)S.a[1], (long long)S.a[2], (long long)S.a[3], (long long)S.a[4],
-                    (long long)S.gcd, S.gcd == 1 ? "primitive" : "NON-PRIMITIVE");
+        print_solution(S);
         ++sols;
         if (stop_first) break;
       }
+    }
+    if (jr && s615_journal_append(jr, work.data() + off, n, hits.data(), nh, solv.data(), ns) != S615_OK) {
+      std::fprintf(stderr, "[journal] append failed\n");
+      s615_journal_close(jr);
+      s615_close(ctx);
+      return 1;
     }
     const double sec = std::chrono::duration<double>(Clock::now() - t0).count();
     if (!quiet || chunk_no % 2 == 0 || off + n >= units.size()) {
       const double gate_pct = tot_calls ? 100.0 * (double)tot_gated / (double)tot_calls : 0.0;
       std::fprintf(stderr, "[cls5-gpu] units=%zu/%zu calls=%llu probes=%llu gate=%.1f%% sols=%llu %.1fs\n",
-                   off + n, units.size(), tot_calls, tot_probes, gate_pct, sols, sec);
+                   units.size() - work.size() + off + n, units.size(), tot_calls, tot_probes, gate_pct,
+                   sols, sec);
     }
     if (stop_first && sols) break;
+  }
+  if (jr && s615_journal_close(jr) != S615_OK) {
+    std::fprintf(stderr, "[journal] close failed\n");
+    s615_close(ctx);
+    return 1;
   }
   if (dump) std::fclose(dump);
   if (!plants.empty()) {

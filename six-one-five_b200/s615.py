@@ -152,6 +152,13 @@ SIGNATURES = {
     "s615_cls5_verify": (C.c_int, [_P, _P, C.c_size_t, _P, C.c_size_t, C.c_int, _P, C.c_size_t,
                                    C.POINTER(C.c_size_t)]),
     "s615_selftest_host": (C.c_int, []),
+    "s615_journal_open": (C.c_int, [C.c_char_p, C.POINTER(_P)]),
+    "s615_journal_has": (C.c_int, [_P, _P]),
+    "s615_journal_stats": (C.c_int, [_P, _P, _P, _P]),
+    "s615_journal_units": (C.c_int, [_P, _P, C.c_size_t, _P]),
+    "s615_journal_solutions": (C.c_int, [_P, _P, C.c_size_t, _P]),
+    "s615_journal_append": (C.c_int, [_P, _P, C.c_size_t, _P, C.c_size_t, _P, C.c_size_t]),
+    "s615_journal_close": (C.c_int, [_P]),
     "s615_serve_start": (C.c_int, [_P, C.c_int, C.c_size_t]),
     "s615_submit": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.c_uint, C.POINTER(C.c_uint64)]),
     "s615_poll": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(C.c_size_t), C.c_int]),
@@ -415,6 +422,59 @@ def s615_hits_copy(ptr, n: int) -> np.ndarray:
 def hits_to_array(hits, n: int) -> np.ndarray:
     raw = np.frombuffer(C.string_at(C.addressof(hits), n * C.sizeof(Hit)), dtype=HIT_DTYPE)
     return raw.copy()
+
+
+class Journal:
+    """s615_journal_*: the restart journal of a campaign (append-only, one
+    committed block per finished request or chunk)."""
+
+    def __init__(self, path: str):
+        self._j = C.c_void_p()
+        _check(lib().s615_journal_open(path.encode(), C.byref(self._j)), "journal_open")
+
+    def close(self) -> None:
+        if self._j:
+            _check(lib().s615_journal_close(self._j), "journal_close")
+            self._j = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def has(self, unit: "Unit") -> bool:
+        st = lib().s615_journal_has(self._j, C.byref(unit))
+        if st < 0:
+            _check(st, "journal_has")
+        return st == 1
+
+    def stats(self):
+        u, h, s = C.c_size_t(0), C.c_size_t(0), C.c_size_t(0)
+        _check(lib().s615_journal_stats(self._j, C.byref(u), C.byref(h), C.byref(s)), "journal_stats")
+        return u.value, h.value, s.value
+
+    def units(self):
+        n = C.c_size_t(0)
+        lib().s615_journal_units(self._j, None, 0, C.byref(n))
+        arr = (Unit * max(n.value, 1))()
+        _check(lib().s615_journal_units(self._j, C.cast(arr, C.c_void_p), n.value, C.byref(n)),
+               "journal_units")
+        return [arr[i] for i in range(n.value)]
+
+    def solutions(self):
+        n = C.c_size_t(0)
+        lib().s615_journal_solutions(self._j, None, 0, C.byref(n))
+        arr = (Solution * max(n.value, 1))()
+        _check(lib().s615_journal_solutions(self._j, C.cast(arr, C.c_void_p), n.value, C.byref(n)),
+               "journal_solutions")
+        return [arr[i] for i in range(n.value)]
+
+    def append(self, units, n: int, hits=None, sols=()) -> None:
+        h = np.ascontiguousarray(hits if hits is not None else np.zeros(0, dtype=HIT_DTYPE))
+        sarr = (Solution * max(len(sols), 1))(*sols)
+        _check(lib().s615_journal_append(self._j, C.cast(units, C.c_void_p), n, _ptr(h), h.size,
+                                         C.cast(sarr, C.c_void_p), len(sols)), "journal_append")
 
 
 class Engine:

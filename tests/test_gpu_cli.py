@@ -13,6 +13,7 @@ import subprocess
 import pytest
 
 import orc
+import s615
 import workloads as W
 
 pytestmark = pytest.mark.gpu
@@ -106,3 +107,40 @@ def test_cls5_cli_plants_and_serve(tmp_path, oracle_table):
     m = re.search(r"---- done cls5-gpu serve: solutions=(\d+) units=(\d+) requests=(\d+)", p.stdout)
     assert m and int(m.group(2)) == len(units) and int(m.group(3)) == (len(units) + 99) // 100
     assert int(m.group(1)) == 0
+
+
+def test_cls5_cli_journal_resumes(tmp_path, oracle_table):
+    # a run journals its chunks; after a crash (journal cut inside a block) the
+    # rerun searches only the units not committed, and every plant is still
+    # recovered once (before or after the restart)
+    N = 715
+    t, path = oracle_table(N, 20)
+    units = W.cls5_units(1000, 30000)
+    buc = tmp_path / "u.buc"
+    W.write_buc(str(buc), units)
+    jpath = tmp_path / "run.journal"
+    cmd = [BIN5, "--units", str(buc), "--N", str(N), "--load-table", path, "--plant", "8:3",
+           "--batch", "200", "--journal", str(jpath)]
+    p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr
+    total = len(units) + 8
+    assert "[plant] recovered 8/8" in p.stderr
+    full = jpath.read_bytes()
+    # cut inside the third block: two committed blocks of 200 units survive
+    starts = [i for i in range(len(full)) if full.startswith(b"B ", i) and (i == 0 or full[i - 1] == 10)]
+    assert len(starts) == (total + 199) // 200
+    jpath.write_bytes(full[:starts[2] + (starts[3] - starts[2]) // 2])
+    p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr
+    assert f"[journal] 400 of {total} units already committed; searching {total - 400}" in p.stderr
+    assert "[plant] recovered 8/8" in p.stderr
+    m = re.search(r"---- done cls5-gpu: solutions=(\d+) units=(\d+) calls=(\d+) probes=(\d+)", p.stdout)
+    assert m and int(m.group(1)) == 0 and int(m.group(2)) == total
+    # the journal now commits every unit exactly once
+    with s615.Journal(str(jpath)) as j:
+        assert j.stats()[0] == total
+        assert len({(u.kind, u.B, u.u, tuple(u.base)) for u in j.units()}) == total
+    p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr
+    assert f"[journal] {total} of {total} units already committed; searching 0" in p.stderr
+    assert "[plant] recovered 8/8" in p.stderr
