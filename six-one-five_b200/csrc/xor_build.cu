@@ -25,6 +25,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -124,6 +126,82 @@ __global__ void k_incidence(const u64* __restrict__ keys, u64 n, u64 seed, u64 b
   }
 }
 
+// ---- incidence through shared-memory radix bins ---------------------------
+// The cells are cut into slices of 2^sbits cells (about 19 MB of setxor and
+// counts: L2-sized).  Each block takes a fixed range of keys.  k_bin_count
+// counts the block's updates per slice in a shared-memory histogram; a host
+// scan over (slice, block) gives every block its own output range per slice;
+// k_bin_scatter bins the updates through shared-memory cursors into those
+// ranges (slice-local cell offset and hash), so the updates of a slice lie
+// together; k_bin_apply then walks the updates in slice order and its
+// atomics land on a slice that is resident in L2, instead of missing to DRAM
+// twice (xor word and count byte) per update.
+constexpr u32 kMaxSlices = 4608;
+constexpr int kBinThreads = 256;
+
+__global__ void k_bin_count(const u64* __restrict__ keys, u64 k0, u64 per, u64 k1, u64 seed,
+                            u64 block, u64 recip, u32 sbits, u32 S, u32* __restrict__ bhist) {
+  extern __shared__ u32 hist[];
+  for (u32 i = threadIdx.x; i < S; i += blockDim.x) hist[i] = 0;
+  __syncthreads();
+  const u64 lo = k0 + blockIdx.x * per, hi = min(k1, lo + per);
+  for (u64 i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const u64 h = mix64(keys[i] + seed);
+    u64 c[3];
+    cell_indices(h, block, recip, c);
+#pragma unroll
+    for (int t = 0; t < 3; ++t) atomicAdd(&hist[(u32)(c[t] >> sbits)], 1u);
+  }
+  __syncthreads();
+  for (u32 i = threadIdx.x; i < S; i += blockDim.x) bhist[(u64)blockIdx.x * S + i] = hist[i];
+}
+
+__global__ void k_bin_scatter(const u64* __restrict__ keys, u64 k0, u64 per, u64 k1, u64 seed,
+                              u64 block, u64 recip, u32 sbits, u32 S,
+                              const unsigned long long* __restrict__ bbase, u32* __restrict__ ent_off,
+                              u64* __restrict__ ent_h) {
+  extern __shared__ unsigned long long cur[];
+  for (u32 i = threadIdx.x; i < S; i += blockDim.x) cur[i] = bbase[(u64)blockIdx.x * S + i];
+  __syncthreads();
+  const u64 lo = k0 + blockIdx.x * per, hi = min(k1, lo + per);
+  const u64 lmask = (1ull << sbits) - 1;
+  for (u64 i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const u64 h = mix64(keys[i] + seed);
+    u64 c[3];
+    cell_indices(h, block, recip, c);
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+      const unsigned long long pos = atomicAdd(&cur[(u32)(c[t] >> sbits)], 1ull);
+      ent_off[pos] = (u32)(c[t] & lmask);
+      ent_h[pos] = h;
+    }
+  }
+}
+
+__global__ void k_bin_apply(const u32* __restrict__ ent_off, const u64* __restrict__ ent_h, u64 E,
+                            const unsigned long long* __restrict__ soff, u32 sbits, u32 S,
+                            unsigned long long* setxor, u32* counts, u32* overflow) {
+  extern __shared__ unsigned long long so[];   // S + 1 slice starts
+  for (u32 i = threadIdx.x; i <= S; i += blockDim.x) so[i] = soff[i];
+  __syncthreads();
+  u32 s = 0;
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < E; i += (u64)gridDim.x * blockDim.x) {
+    if (i < so[s] || i >= so[s + 1]) {   // the slice of entry i: so[s] <= i < so[s + 1]
+      u32 a = 0, b = S;
+      while (b - a > 1) {
+        const u32 mid = (a + b) / 2;
+        if (so[mid] <= i) a = mid; else b = mid;
+      }
+      s = a;
+    }
+    const u64 c = ((u64)s << sbits) + ent_off[i];
+    atomicXor(setxor + c, (unsigned long long)ent_h[i]);
+    const u32 sh = 8 * (u32)(c & 3);
+    const u32 old = atomicAdd(counts + (c >> 2), 1u << sh);
+    if (((old >> sh) & 0xFFu) == 0xFFu) *overflow = 1;
+  }
+}
+
 // Claim: a count-1 cell c claims its key iff no lower cell of that key has
 // count 1.  Counts are only read here, so the round sees one snapshot.
 __global__ void k_claim(const unsigned long long* __restrict__ setxor, const u32* __restrict__ counts,
@@ -203,6 +281,87 @@ struct Buf {
 
 u64 pow2_at_least(u64 x) { u64 p = 1; while (p < x) p <<= 1; return p; }
 
+// Incidence of keys [0, n) for one seed through the slice bins, in chunks of
+// keys whose updates fit the entry buffers (ent_cap updates).
+int incidence_binned(s615_ctx* ctx, const u64* keys, u64 n, u64 seed, u64 m, u64 block, u64 recip,
+                     u32* ent_off, u64* ent_h, u64 ent_cap, unsigned long long* setxor, u32* counts,
+                     u32* d_over, u32* bhist, unsigned long long* bbase, cudaStream_t st) {
+  u32 sbits = 21;
+  while (((m + (1ull << sbits) - 1) >> sbits) > kMaxSlices) ++sbits;
+  const u32 S = (u32)((m + (1ull << sbits) - 1) >> sbits);
+  const int G = ctx->num_sms * 2;
+  const u64 chunk = std::max<u64>(1, ent_cap / 3);
+  std::vector<u32> h_hist((size_t)G * S);
+  std::vector<unsigned long long> h_base((size_t)G * S), h_soff(S + 1);
+  for (u64 k0 = 0; k0 < n; k0 += chunk) {
+    const u64 k1 = std::min(n, k0 + chunk);
+    const u64 per = (k1 - k0 + G - 1) / G;
+    k_bin_count<<<G, kBinThreads, S * sizeof(u32), st>>>(keys, k0, per, k1, seed, block, recip, sbits,
+                                                         S, bhist);
+    ctx->launches++;
+    S615_CU(cudaGetLastError());
+    S615_CU(cudaMemcpyAsync(h_hist.data(), bhist, h_hist.size() * sizeof(u32), cudaMemcpyDeviceToHost, st));
+    S615_CU(cudaStreamSynchronize(st));
+    // exclusive scan in (slice, block) order: slice s's updates are contiguous
+    unsigned long long run = 0;
+    for (u32 sl = 0; sl < S; ++sl) {
+      h_soff[sl] = run;
+      for (int b = 0; b < G; ++b) {
+        h_base[(size_t)b * S + sl] = run;
+        run += h_hist[(size_t)b * S + sl];
+      }
+    }
+    h_soff[S] = run;
+    if (run != 3 * (k1 - k0)) return S615_E_DEVICE;
+    S615_CU(cudaMemcpyAsync(bbase, h_base.data(), h_base.size() * sizeof(unsigned long long),
+                            cudaMemcpyHostToDevice, st));
+    k_bin_scatter<<<G, kBinThreads, S * sizeof(unsigned long long), st>>>(
+        keys, k0, per, k1, seed, block, recip, sbits, S, bbase, ent_off, ent_h);
+    ctx->launches++;
+    S615_CU(cudaGetLastError());
+    // the slice starts go where the block bases were (read by the apply kernel)
+    S615_CU(cudaMemcpyAsync(bbase, h_soff.data(), (S + 1) * sizeof(unsigned long long),
+                            cudaMemcpyHostToDevice, st));
+    k_bin_apply<<<grid_for(ctx, run, 256), 256, (S + 1) * sizeof(unsigned long long), st>>>(
+        ent_off, ent_h, run, bbase, sbits, S, setxor, counts, d_over);
+    ctx->launches++;
+    S615_CU(cudaGetLastError());
+    S615_CU(cudaStreamSynchronize(st));   // h_base / h_soff are reused by the next chunk
+  }
+  return S615_OK;
+}
+
+// S615_TRACE: per-phase device times of a build on stderr (CUDA events on
+// the build stream).
+struct PhaseTrace {
+  bool on = std::getenv("S615_TRACE") != nullptr;
+  cudaStream_t st;
+  std::vector<std::pair<const char*, cudaEvent_t>> marks;
+  explicit PhaseTrace(cudaStream_t s) : st(s) {}
+  void mark(const char* name) {
+    if (!on) return;
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); return; }
+    cudaEventRecord(e, st);
+    marks.emplace_back(name, e);
+  }
+  void report(u64 n, u64 m, int rounds) {
+    if (!on || marks.size() < 2) return;
+    cudaEventSynchronize(marks.back().second);
+    std::fprintf(stderr, "[xor-build] keys=%llu cells=%llu rounds=%d", (unsigned long long)n,
+                 (unsigned long long)m, rounds);
+    for (size_t i = 1; i < marks.size(); ++i) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, marks[i - 1].second, marks[i].second);
+      std::fprintf(stderr, " %s=%.1fms", marks[i].first, ms);
+    }
+    std::fprintf(stderr, "\n");
+  }
+  ~PhaseTrace() {
+    for (auto& m : marks) cudaEventDestroy(m.second);
+  }
+};
+
 }  // namespace
 
 int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u64* d_keys,
@@ -218,6 +377,8 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
                                 : std::min<u64>(n_all, n_all / shards +
                                                            8 * (u64)std::sqrt((double)n_all) + 4096);
 
+  PhaseTrace trace(st);
+  trace.mark("start");
   // ---- 1. unique keys ----
   Buf keys(ctx);
   u64 n = 0;
@@ -292,6 +453,7 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
     return S615_OK;
   }
 
+  trace.mark("unique");
   // ---- 2-4. per seed: incidence, peel, fill ----
   const u64 m = capacity_for(n);
   const u64 block = m / 3, recip = mod_recip(block);
@@ -304,20 +466,60 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
   u32* d_over = static_cast<u32*>(scratch.p);
   unsigned long long* d_claimed = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch.p) + 8);
   const int g = grid_for(ctx, m, 256);
+  // Entry buffers of the binned incidence: all 3n updates when HBM allows,
+  // else chunks of keys; with no room for a useful chunk the incidence falls
+  // back to direct atomics (k_incidence).
+  Buf ent_off(ctx), ent_h(ctx), bins(ctx);
+  u64 ent_cap = 0;
+  {
+    size_t free_b = 0, total_b = 0;
+    S615_CU(cudaMemGetInfo(&free_b, &total_b));
+    size_t avail = std::min(free_b, ctx->budget > ctx->used ? ctx->budget - ctx->used : (size_t)0);
+    const size_t margin = (size_t)2 << 30;
+    avail = avail > margin ? avail - margin : 0;
+    const size_t bin_bytes = (size_t)ctx->num_sms * 2 * kMaxSlices * (4 + 8) + 64;
+    if (avail > bin_bytes) {
+      ent_cap = std::min<u64>(3 * n, (avail - bin_bytes) / 12);
+      ent_cap = ent_cap / 3 * 3;
+    }
+    if (ent_cap >= std::min<u64>(3 * n, 3ull << 20)) {
+      if ((s = ent_off.alloc(ent_cap * 4)) || (s = ent_h.alloc(ent_cap * 8)) ||
+          (s = bins.alloc(bin_bytes))) {
+        ent_off.release(); ent_h.release(); bins.release();
+        ent_cap = 0;
+      }
+    } else {
+      ent_cap = 0;
+    }
+  }
   bool built = false;
   u64 used_seed = 0;
+  int trace_rounds = 0;
   for (int si = 0; si < n_seeds && !built; ++si) {
     const u64 seed = seeds[si];
     S615_CU(cudaMemsetAsync(setxor.p, 0, m * sizeof(u64), st));
     S615_CU(cudaMemsetAsync(counts.p, 0, ((m + 3) / 4) * sizeof(u32), st));
     S615_CU(cudaMemsetAsync(rounds.p, 0, m * sizeof(u16), st));
     S615_CU(cudaMemsetAsync(scratch.p, 0, 64, st));
-    k_incidence<<<grid_for(ctx, n, 256), 256, 0, st>>>(static_cast<const u64*>(keys.p), n, seed,
-                                                       block, recip,
-                                                       static_cast<unsigned long long*>(setxor.p),
-                                                       static_cast<u32*>(counts.p), d_over);
-    ctx->launches++;
-    S615_CU(cudaGetLastError());
+    if (ent_cap) {
+      const size_t G = (size_t)ctx->num_sms * 2;
+      u32* bhist = static_cast<u32*>(bins.p);
+      auto* bbase = reinterpret_cast<unsigned long long*>(static_cast<char*>(bins.p) +
+                                                          (G * kMaxSlices * 4 + 7) / 8 * 8);
+      if ((s = incidence_binned(ctx, static_cast<const u64*>(keys.p), n, seed, m, block, recip,
+                                static_cast<u32*>(ent_off.p), static_cast<u64*>(ent_h.p), ent_cap,
+                                static_cast<unsigned long long*>(setxor.p),
+                                static_cast<u32*>(counts.p), d_over, bhist, bbase, st)))
+        return s;
+    } else {
+      k_incidence<<<grid_for(ctx, n, 256), 256, 0, st>>>(static_cast<const u64*>(keys.p), n, seed,
+                                                         block, recip,
+                                                         static_cast<unsigned long long*>(setxor.p),
+                                                         static_cast<u32*>(counts.p), d_over);
+      ctx->launches++;
+      S615_CU(cudaGetLastError());
+    }
+    trace.mark("incidence");
     u64 peeled = 0;
     u16 rr = 0;
     for (;;) {
@@ -343,6 +545,7 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
     S615_CU(cudaMemcpy(&over, d_over, 4, cudaMemcpyDeviceToHost));
     if (over) return S615_E_BUILD;
     if (peeled != n) continue;   // 2-core not empty: next seed
+    trace.mark("peel");
     const u64 mask = fp_mask((u32)r);
     for (u16 q = rr; q >= 1; --q) {
       k_fill<<<g, 256, 0, st>>>(static_cast<unsigned long long*>(setxor.p),
@@ -350,11 +553,14 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
       ctx->launches++;
     }
     S615_CU(cudaGetLastError());
+    trace.mark("fill");
+    trace_rounds = rr;
     built = true;
     used_seed = seed;
   }
   if (!built) return S615_E_BUILD;
   keys.release(); counts.release(); rounds.release();
+  ent_off.release(); ent_h.release(); bins.release();
 
   out->hdr.n_keys = n;
   out->hdr.m_cells = m;
@@ -385,6 +591,8 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
     out->d_cells = setxor.p; out->bytes = setxor.n;
     setxor.p = nullptr; setxor.n = 0;   // ownership moves to the table
   }
+  trace.mark("layout");
+  trace.report(n, m, trace_rounds);
   S615_CU(cudaStreamSynchronize(st));
   S615_CU(cudaGetLastError());
   return S615_OK;
