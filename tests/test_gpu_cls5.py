@@ -148,3 +148,30 @@ def test_band_3p2M_sample_parity(engine, oracle_table):
         np.testing.assert_array_equal(sorted_hits(hits), sorted_hits(ohits))
     finally:
         engine.free_table(tid)
+
+
+def test_band_production_table_parity(engine):
+    # the configuration the bench times, against the oracle: 64 evenly spaced
+    # Stage-1 units of the B ~ 3.2M band plus 8 plants on a table for
+    # N = 76,667 built on the device in its default layout, at r = 20 so that
+    # the filter gives raw hits; the table is exported (reference file bytes)
+    # and probed by the oracle
+    N, r = 76667, 20
+    band = W.cls5_units(3_200_000, 3_219_999)
+    idx = np.linspace(0, len(band) - 1, 64).astype(int)
+    units = [band[i] for i in idx]
+    plants = W.plants(8, 7, 3_200_000, 3_219_999, N)
+    tid = engine.build_table(N, r)
+    try:
+        arr, n = W.unit_array(units, plants, N)
+        hits, ctr = engine.cls5_run(tid, arr, n)
+        hb, pk = engine.export_table(tid)
+    finally:
+        engine.free_table(tid)
+    t = orc.Table.from_memory(hb, pk)
+    del pk
+    oarr, on = oracle_units(units, plants, N)
+    ohits, (calls, gated, probes) = orc.cls5_run(t, oarr, on)
+    assert (ctr.calls, ctr.gated, ctr.probes) == (calls, gated, probes)
+    assert len(ohits) > len(plants)   # filter false positives at r = 20 (~26 expected), and the plants
+    np.testing.assert_array_equal(sorted_hits(hits), sorted_hits(ohits))
