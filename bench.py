@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--workload", default="cls5", choices=["cls5", "cls617", "mix", "serve", "jobs"])
     ap.add_argument("--units", type=int, default=0, help="mix: units per step (default 200,000)")
     ap.add_argument("--seconds", type=float, default=10.0, help="serve: seconds of arrivals")
+    ap.add_argument("--reference-gpu", type=int, default=-1,
+                    help="cls5: run the reference's fourcore_cls5_gpu_v4 on K evenly spaced band "
+                         "units (0: the whole band; -1: skip)")
     return ap.parse_args()
 
 
@@ -289,6 +292,76 @@ def serve_latency(eng, tid, units, N, rate=5000.0, secs=8.0, req_units=50, seed=
             "request_units": req_units, "mean_requests_per_batch": float(np.mean(batch_reqs)),
             "tuned": tuned,
             "loop": "s615_serve_start(slots=2) + s615_submit/s615_poll, Poisson arrivals"}
+
+
+def reference_gpu_cls5(lib, eng, tid, units, N, r, stream, max_units=0):
+    """The reference's own class-5 program (fourcore_cls5_gpu_v4, compiled
+    from the reference sources into oracle/_ref) on the same Stage-1 units
+    and the same table bytes (the engine's table saved in the reference's
+    file format and given to it with --load-table), on this GPU: its summary
+    counters (calls=, probes=) must equal the engine's on the same units, and
+    its time= (the chunk loop: 16 units per launch, per-chunk sync and host
+    verify) is set against the engine's device time for those units."""
+    import shutil
+    import tempfile
+
+    import s615
+    import workloads as W
+    exe = os.path.join(ROOT, "oracle", "_ref", "fourcore_cls5_gpu_v4")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/fourcore_cls5_gpu_v4 not built"}
+    if max_units and len(units) > max_units:
+        idx = [round(i * (len(units) - 1) / (max_units - 1)) for i in range(max_units)]
+        units = [units[i] for i in idx]
+    info = eng.table_info(tid)
+    file_bytes = 64 + (info.hdr.m_cells * info.hdr.r + 7) // 8 + 8
+    tmp = os.environ.get("TMPDIR") or tempfile.gettempdir()
+    free = shutil.disk_usage(tmp).free
+    if free < file_bytes * 1.05 + (2 << 30):
+        return {"unavailable": f"the table file needs {file_bytes / 1e9:.1f} GB of disk, "
+                               f"{free / 1e9:.1f} GB free in {tmp}"}
+    try:
+        import psutil
+        if psutil.virtual_memory().available < file_bytes * 1.3 + (8 << 30):
+            return {"unavailable": "not enough host memory for the reference to read the table"}
+    except ImportError:
+        pass
+    d = tempfile.mkdtemp(dir=tmp)
+    try:
+        path = os.path.join(d, f"xor_N{N}_r{r}.bin")
+        t0 = time.perf_counter()
+        eng.save_table(tid, path)
+        save_s = time.perf_counter() - t0
+        buc = os.path.join(d, "band.buc")
+        W.write_buc(buc, units)
+        t0 = time.perf_counter()
+        p = subprocess.run([exe, "--units", buc, "--N", str(N), "--r", str(r), "--load-table", path,
+                            "--quiet"], capture_output=True, text=True, timeout=3600)
+        wall = time.perf_counter() - t0
+        m = re.search(r"---- done cls5-gpu: solutions=(\d+) units=(\d+) calls=(\d+) probes=(\d+) "
+                      r"time=([\d.]+)s", p.stdout)
+        if p.returncode != 0 or not m:
+            return {"unavailable": "fourcore_cls5_gpu_v4 failed: " +
+                                   " ".join(p.stderr.strip().splitlines()[-2:])}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    # the engine on exactly these units (no plants), device time
+    arr, n = W.unit_array(units, [], N)
+    b = C.c_void_p()
+    s615._check(lib.s615_prepare(eng._ctx, C.cast(arr, C.c_void_p), n, C.byref(b)), "prepare")
+    ms, c = timed_steps(lib, eng, tid, b, stream, 0, 1)
+    s615._check(lib.s615_batch_free(eng._ctx, b), "batch_free")
+    ref_s = float(m.group(5))
+    return {"program": "oracle/_ref/fourcore_cls5_gpu_v4 (reference sources, nvcc sm_100a)",
+            "units": int(m.group(2)), "calls": int(m.group(3)), "probes": int(m.group(4)),
+            "solutions": int(m.group(1)),
+            "counters_equal": (int(m.group(3)), int(m.group(4))) == (c.calls, c.probes),
+            "time_s": ref_s, "process_wall_s": round(wall, 1), "table_save_s": round(save_s, 1),
+            "peel_probes_per_s": c.pos / ref_s if ref_s else None,
+            "engine_ms_same_units": ms, "engine_over_reference": ref_s / (ms / 1e3) if ms else None,
+            "note": "time= is the reference's own summary figure (after table upload; its 16-unit "
+                    "chunk loop with per-chunk sync and host verify); R>0 points are the engine's "
+                    "count for the same units (the reference does not print them)"}
 
 
 def band_units(lo, hi):
@@ -1267,6 +1340,11 @@ def main():
         log(f"serving: p50 {serve['p50_ms']:.2f} ms, p99 {serve['p99_ms']:.2f} ms per unit; "
             f"tuned p50 {serve_tuned['p50_ms']:.2f} ms, p99 {serve_tuned['p99_ms']:.2f} ms")
 
+    ref_gpu = None
+    if rank == 0 and world == 1 and args.shards == 1 and args.reference_gpu >= 0:
+        ref_gpu = reference_gpu_cls5(lib, eng, tid, units, N, args.r, stream, args.reference_gpu)
+        log(f"reference GPU program: {ref_gpu}")
+
     cpu = None
     parity = None
     if not args.no_cpu_baseline and rank == 0 and world == 1 and args.shards == 1:
@@ -1326,6 +1404,7 @@ def main():
         "roofline": roof,
         "cpu_baseline": cpu,
         "parity_sample": parity,
+        "reference_gpu": ref_gpu,
         "plain_form": plain,
         "sharp_gate": sharp,
         "clocks": cl,
