@@ -263,6 +263,108 @@ __global__ void k_fill(unsigned long long* setxor, const u16* __restrict__ round
   }
 }
 
+// ---- peel over lists ---------------------------------------------------------
+// The same rounds, visiting only what can change.  Every count-1 cell at the
+// start of round r > 1 got its count 1 while round r-1 removed keys (a
+// count-1 cell of round r-1 either claimed its key or lost it to a lower
+// cell of the same key), so round r's candidates are exactly the cells whose
+// count went from 2 to 1 during round r-1's apply.  Claimed cells are
+// appended to one list in round order, which the fill then walks backwards.
+// Cell indices are u32 (used when m <= 2^32).
+
+// Append the flagged lanes' values (every lane of the warp calls this).
+__device__ __forceinline__ void warp_append(bool take, u32 val, u32* list,
+                                            unsigned long long* count, u64 cap, u32* over) {
+  const u32 ballot = __ballot_sync(0xFFFFFFFFu, take);
+  if (!ballot) return;
+  const u32 lane = threadIdx.x & 31;
+  const int leader = __ffs(ballot) - 1;
+  unsigned long long base = 0;
+  if ((int)lane == leader) base = atomicAdd(count, (unsigned long long)__popc(ballot));
+  base = __shfl_sync(0xFFFFFFFFu, base, leader);
+  if (take) {
+    const u64 k = base + __popc(ballot & ((1u << lane) - 1u));
+    if (k < cap) list[k] = val;
+    else *over = 1;
+  }
+}
+
+// Claim over the candidates cand[0, ncand), or over every cell when cand is
+// null: the lowest count-1 cell of a key claims it (appended to order).
+__global__ void k_claim_list(const u32* __restrict__ cand, u64 ncand,
+                             const unsigned long long* __restrict__ setxor,
+                             const u32* __restrict__ counts, u64 block, u64 recip, u32* order,
+                             unsigned long long* n_order, u64 order_cap, u32* over) {
+  for (u64 base = blockIdx.x * (u64)blockDim.x; base < ncand; base += (u64)gridDim.x * blockDim.x) {
+    const u64 i = base + threadIdx.x;
+    bool claim = false;
+    u32 c = 0;
+    if (i < ncand) {
+      c = cand ? cand[i] : (u32)i;
+      if (count_of(counts, c) == 1) {
+        const u64 h = setxor[c];
+        u64 cs[3];
+        cell_indices(h, block, recip, cs);
+        claim = true;
+#pragma unroll
+        for (int t = 0; t < 3; ++t)
+          if (cs[t] < c && count_of(counts, cs[t]) == 1) claim = false;
+      }
+    }
+    warp_append(claim, c, order, n_order, order_cap, over);
+  }
+}
+
+// Remove each claimed key from its two other cells; a cell whose count goes
+// from 2 to 1 becomes a candidate of the next round.
+__global__ void k_apply_list(const u32* __restrict__ claimed, u64 L, unsigned long long* setxor,
+                             u32* counts, u64 block, u64 recip, u32* next,
+                             unsigned long long* n_next, u64 next_cap, u32* over) {
+  for (u64 base = blockIdx.x * (u64)blockDim.x; base < L; base += (u64)gridDim.x * blockDim.x) {
+    const u64 i = base + threadIdx.x;
+    bool t0 = false, t1 = false;
+    u32 a0 = 0, a1 = 0;
+    if (i < L) {
+      const u32 c = claimed[i];
+      const u64 h = setxor[c];
+      u64 cs[3];
+      cell_indices(h, block, recip, cs);
+      int k = 0;
+#pragma unroll
+      for (int t = 0; t < 3; ++t) {
+        if (cs[t] == c) continue;
+        atomicXor(setxor + cs[t], (unsigned long long)h);
+        const u32 sh = 8 * (u32)(cs[t] & 3);
+        const u32 old = atomicSub(counts + (cs[t] >> 2), 1u << sh);
+        const bool to_one = ((old >> sh) & 0xFFu) == 2u;
+        if (k == 0) { t0 = to_one; a0 = (u32)cs[t]; }
+        else { t1 = to_one; a1 = (u32)cs[t]; }
+        ++k;
+      }
+      atomicAnd(counts + (c >> 2), ~(0xFFu << (8 * (c & 3))));
+    }
+    warp_append(t0, a0, next, n_next, next_cap, over);
+    warp_append(t1, a1, next, n_next, next_cap, over);
+  }
+}
+
+// Reverse fill of one round's claimed cells, in place.
+__global__ void k_fill_list(const u32* __restrict__ claimed, u64 L, unsigned long long* setxor,
+                            u64 block, u64 recip, u64 mask) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < L;
+       i += (u64)gridDim.x * blockDim.x) {
+    const u32 c = claimed[i];
+    const u64 h = setxor[c];
+    u64 cs[3];
+    cell_indices(h, block, recip, cs);
+    u64 v = h & mask;
+#pragma unroll
+    for (int t = 0; t < 3; ++t)
+      if (cs[t] != c) v ^= setxor[cs[t]];
+    setxor[c] = v & mask;
+  }
+}
+
 __global__ void k_narrow(const u64* __restrict__ in, u32* __restrict__ out, u64 m) {
   for (u64 c = blockIdx.x * (u64)blockDim.x + threadIdx.x; c < m;
        c += (u64)gridDim.x * blockDim.x)
@@ -457,11 +559,20 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
   // ---- 2-4. per seed: incidence, peel, fill ----
   const u64 m = capacity_for(n);
   const u64 block = m / 3, recip = mod_recip(block);
-  Buf setxor(ctx), counts(ctx), rounds(ctx), scratch(ctx);
+  Buf setxor(ctx), counts(ctx), rounds(ctx), scratch(ctx), order(ctx), front(ctx);
   int s = setxor.alloc(m * sizeof(u64));
   if (s) return s;
   if ((s = counts.alloc(((m + 3) / 4) * sizeof(u32)))) return s;
-  if ((s = rounds.alloc(m * sizeof(u16)))) return s;
+  // Peel over lists (claimed cells in round order, two candidate lists of
+  // m/8 cells each; a round whose candidates overflow scans every cell), or,
+  // for m > 2^32 or without room for the lists, over full scans by round tag.
+  const u64 fcap = std::max<u64>(4096, m / 8);
+  bool lists = m <= (1ull << 32);
+  if (lists && (order.alloc(n * sizeof(u32)) || front.alloc(2 * fcap * sizeof(u32)))) {
+    order.release(); front.release();
+    lists = false;
+  }
+  if (!lists && (s = rounds.alloc(m * sizeof(u16)))) return s;
   if ((s = scratch.alloc(64))) return s;
   u32* d_over = static_cast<u32*>(scratch.p);
   unsigned long long* d_claimed = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch.p) + 8);
@@ -499,7 +610,7 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
     const u64 seed = seeds[si];
     S615_CU(cudaMemsetAsync(setxor.p, 0, m * sizeof(u64), st));
     S615_CU(cudaMemsetAsync(counts.p, 0, ((m + 3) / 4) * sizeof(u32), st));
-    S615_CU(cudaMemsetAsync(rounds.p, 0, m * sizeof(u16), st));
+    if (!lists) S615_CU(cudaMemsetAsync(rounds.p, 0, m * sizeof(u16), st));
     S615_CU(cudaMemsetAsync(scratch.p, 0, 64, st));
     if (ent_cap) {
       const size_t G = (size_t)ctx->num_sms * 2;
@@ -520,6 +631,70 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
       S615_CU(cudaGetLastError());
     }
     trace.mark("incidence");
+    if (lists) {
+      // scratch: [0] incidence overflow, [4] list overflow, [8] n_order, [16] n_next
+      u32* d_lover = reinterpret_cast<u32*>(static_cast<char*>(scratch.p) + 4);
+      auto* d_norder = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch.p) + 8);
+      auto* d_nnext = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch.p) + 16);
+      u32* ord = static_cast<u32*>(order.p);
+      u32* fr[2] = {static_cast<u32*>(front.p), static_cast<u32*>(front.p) + fcap};
+      std::vector<u64> off{0};
+      u64 total = 0, ncand = m;
+      const u32* cand = nullptr;   // round 1 scans every cell
+      int cur = 0;
+      while (off.size() <= 0xFFFE) {
+        k_claim_list<<<grid_for(ctx, ncand, 256), 256, 0, st>>>(
+            cand, ncand, static_cast<const unsigned long long*>(setxor.p),
+            static_cast<const u32*>(counts.p), block, recip, ord, d_norder, n, d_lover);
+        ctx->launches++;
+        unsigned long long h_n[2] = {0, 0};
+        u32 h_lover = 0;
+        S615_CU(cudaMemcpyAsync(&h_n[0], d_norder, 8, cudaMemcpyDeviceToHost, st));
+        S615_CU(cudaStreamSynchronize(st));
+        const u64 L = h_n[0] - total;
+        if (L == 0) break;
+        S615_CU(cudaMemsetAsync(d_nnext, 0, 8, st));
+        S615_CU(cudaMemsetAsync(d_lover, 0, 4, st));
+        k_apply_list<<<grid_for(ctx, L, 256), 256, 0, st>>>(
+            ord + total, L, static_cast<unsigned long long*>(setxor.p), static_cast<u32*>(counts.p),
+            block, recip, fr[cur ^ 1], d_nnext, fcap, d_lover);
+        ctx->launches++;
+        S615_CU(cudaGetLastError());
+        S615_CU(cudaMemcpyAsync(&h_n[1], d_nnext, 8, cudaMemcpyDeviceToHost, st));
+        S615_CU(cudaMemcpyAsync(&h_lover, d_lover, 4, cudaMemcpyDeviceToHost, st));
+        S615_CU(cudaStreamSynchronize(st));
+        total += L;
+        off.push_back(total);
+        cur ^= 1;
+        if (h_lover) {   // candidates overflowed: the next round scans every cell
+          cand = nullptr;
+          ncand = m;
+          S615_CU(cudaMemsetAsync(d_lover, 0, 4, st));
+        } else {
+          cand = fr[cur];
+          ncand = h_n[1];
+          if (ncand == 0) break;   // nothing became count 1: the peel is over
+        }
+      }
+      u32 over = 0;
+      S615_CU(cudaMemcpy(&over, d_over, 4, cudaMemcpyDeviceToHost));
+      if (over) return S615_E_BUILD;
+      if (total != n) continue;   // 2-core not empty: next seed
+      trace.mark("peel");
+      const u64 mask = fp_mask((u32)r);
+      for (size_t q = off.size() - 1; q >= 1; --q) {
+        const u64 L = off[q] - off[q - 1];
+        k_fill_list<<<grid_for(ctx, L, 256), 256, 0, st>>>(
+            ord + off[q - 1], L, static_cast<unsigned long long*>(setxor.p), block, recip, mask);
+        ctx->launches++;
+      }
+      S615_CU(cudaGetLastError());
+      trace.mark("fill");
+      trace_rounds = (int)off.size() - 1;
+      built = true;
+      used_seed = seed;
+      continue;
+    }
     u64 peeled = 0;
     u16 rr = 0;
     for (;;) {
@@ -559,7 +734,7 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
     used_seed = seed;
   }
   if (!built) return S615_E_BUILD;
-  keys.release(); counts.release(); rounds.release();
+  keys.release(); counts.release(); rounds.release(); order.release(); front.release();
   ent_off.release(); ent_h.release(); bins.release();
 
   out->hdr.n_keys = n;
