@@ -9,10 +9,12 @@
 //     has i^6 = 0 mod 2^64), so this already removes most duplicate keys.
 //     Remaining duplicates are removed by an open-addressing hash set in HBM
 //     (the reference sorts + uniques).  The survivors are the unique keys.
-//  2. Incidence: setxor[c] ^= h and count[c]++ for the three cells of each key.
-//  3. Peel in rounds.  A cell with count 1 holds exactly one key; in round r
-//     every such key is claimed by the lowest of its count-1 cells (so a key
-//     is claimed once), recorded as round[c] = r, then removed from its other
+//  2. Incidence: every cell is one 64-bit word, count << 42 | sum of the
+//     indices of its keys, and each key adds (1 << 42) + index to its three
+//     cells (binned by L2-sized cell slice when HBM allows).
+//  3. Peel in rounds.  A cell with count 1 holds exactly one key, named by
+//     its index; in round r every such key is claimed by the lowest of its
+//     count-1 cells (so a key is claimed once), then removed from its other
 //     two cells.  The 2-core is unique, so peeling succeeds for exactly the
 //     seeds for which the reference's FIFO peel succeeds.
 //  4. Fill in reverse round order, in place: the claimed cell of a round-r key
@@ -105,37 +107,55 @@ __global__ void k_compact(const unsigned long long* __restrict__ table, u64 tsiz
   }
 }
 
-__device__ __forceinline__ u32 count_of(const u32* counts, u64 c) {
-  return (counts[c >> 2] >> (8 * (c & 3))) & 0xFFu;
+// ---- cell words -------------------------------------------------------------
+// During the build every cell is one 64-bit word: the number of unpeeled keys
+// in the cell above bit 42 and the sum of their key indices below it.  An
+// update of a cell is then one atomic add (the reference's incidence keeps an
+// xor of hashes and a count: two arrays, two read-modify-writes per update),
+// and a cell of count 1 names its key directly; the key's hash is
+// recomputed from the key array.  Indices are below 2^34 and a count above
+// 255 fails the build, so the sum never reaches bit 42.  After the peel the
+// word array is filled in place with the final r-bit cells.
+constexpr int kCntShift = 42;
+constexpr u64 kSumMask = (1ull << kCntShift) - 1;
+constexpr u64 kMaxKeys = 1ull << 34;
+__device__ __forceinline__ u64 cnt_of(u64 w) { return w >> kCntShift; }
+__device__ __forceinline__ u64 upd(u64 idx) { return (1ull << kCntShift) + idx; }
+
+__device__ __forceinline__ u64 key_hash(const u64* keys, u64 idx, u64 seed) {
+  return mix64(keys[idx] + seed);
 }
 
 __global__ void k_incidence(const u64* __restrict__ keys, u64 n, u64 seed, u64 block, u64 recip,
-                            unsigned long long* setxor, u32* counts, u32* overflow) {
+                            unsigned long long* W) {
   for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < n;
        i += (u64)gridDim.x * blockDim.x) {
-    const u64 h = mix64(keys[i] + seed);
     u64 c[3];
-    cell_indices(h, block, recip, c);
+    cell_indices(key_hash(keys, i, seed), block, recip, c);
 #pragma unroll
-    for (int t = 0; t < 3; ++t) {
-      atomicXor(setxor + c[t], (unsigned long long)h);
-      const u32 sh = 8 * (u32)(c[t] & 3);
-      const u32 old = atomicAdd(counts + (c[t] >> 2), 1u << sh);
-      if (((old >> sh) & 0xFFu) == 0xFFu) *overflow = 1;
-    }
+    for (int t = 0; t < 3; ++t) atomicAdd(W + c[t], (unsigned long long)upd(i));
   }
 }
 
+// The largest count of any cell (a count above 255 fails the build).
+__global__ void k_max_count(const unsigned long long* __restrict__ W, u64 m, unsigned* mx) {
+  unsigned local = 0;
+  for (u64 c = blockIdx.x * (u64)blockDim.x + threadIdx.x; c < m; c += (u64)gridDim.x * blockDim.x)
+    { const u64 k = cnt_of(W[c]); local = max(local, k > 0xFFFFFFFFull ? 0xFFFFFFFFu : (unsigned)k); }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) local = max(local, __shfl_xor_sync(0xFFFFFFFFu, local, o));
+  if ((threadIdx.x & 31) == 0 && local) atomicMax(mx, local);
+}
+
 // ---- incidence through shared-memory radix bins ---------------------------
-// The cells are cut into slices of 2^sbits cells (about 19 MB of setxor and
-// counts: L2-sized).  Each block takes a fixed range of keys.  k_bin_count
-// counts the block's updates per slice in a shared-memory histogram; a host
-// scan over (slice, block) gives every block its own output range per slice;
+// The cells are cut into slices of 2^sbits cells (16 MB of cell words:
+// L2-sized).  Each block takes a fixed range of keys.  k_bin_count counts the
+// block's updates per slice in a shared-memory histogram; a host scan over
+// (slice, block) gives every block its own output range per slice;
 // k_bin_scatter bins the updates through shared-memory cursors into those
-// ranges (slice-local cell offset and hash), so the updates of a slice lie
-// together; k_bin_apply then walks the updates in slice order and its
-// atomics land on a slice that is resident in L2, instead of missing to DRAM
-// twice (xor word and count byte) per update.
+// ranges (slice-local cell offset and key index, 8 B), so the updates of a
+// slice lie together; k_bin_apply walks them in slice order, and its atomic
+// adds land on a slice that is resident in L2.
 constexpr u32 kMaxSlices = 4608;
 constexpr int kBinThreads = 256;
 
@@ -146,9 +166,8 @@ __global__ void k_bin_count(const u64* __restrict__ keys, u64 k0, u64 per, u64 k
   __syncthreads();
   const u64 lo = k0 + blockIdx.x * per, hi = min(k1, lo + per);
   for (u64 i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    const u64 h = mix64(keys[i] + seed);
     u64 c[3];
-    cell_indices(h, block, recip, c);
+    cell_indices(key_hash(keys, i, seed), block, recip, c);
 #pragma unroll
     for (int t = 0; t < 3; ++t) atomicAdd(&hist[(u32)(c[t] >> sbits)], 1u);
   }
@@ -159,28 +178,27 @@ __global__ void k_bin_count(const u64* __restrict__ keys, u64 k0, u64 per, u64 k
 __global__ void k_bin_scatter(const u64* __restrict__ keys, u64 k0, u64 per, u64 k1, u64 seed,
                               u64 block, u64 recip, u32 sbits, u32 S,
                               const unsigned long long* __restrict__ bbase, u32* __restrict__ ent_off,
-                              u64* __restrict__ ent_h) {
+                              u32* __restrict__ ent_idx) {
   extern __shared__ unsigned long long cur[];
   for (u32 i = threadIdx.x; i < S; i += blockDim.x) cur[i] = bbase[(u64)blockIdx.x * S + i];
   __syncthreads();
   const u64 lo = k0 + blockIdx.x * per, hi = min(k1, lo + per);
   const u64 lmask = (1ull << sbits) - 1;
   for (u64 i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    const u64 h = mix64(keys[i] + seed);
     u64 c[3];
-    cell_indices(h, block, recip, c);
+    cell_indices(key_hash(keys, i, seed), block, recip, c);
 #pragma unroll
     for (int t = 0; t < 3; ++t) {
       const unsigned long long pos = atomicAdd(&cur[(u32)(c[t] >> sbits)], 1ull);
       ent_off[pos] = (u32)(c[t] & lmask);
-      ent_h[pos] = h;
+      ent_idx[pos] = (u32)(i - k0);
     }
   }
 }
 
-__global__ void k_bin_apply(const u32* __restrict__ ent_off, const u64* __restrict__ ent_h, u64 E,
-                            const unsigned long long* __restrict__ soff, u32 sbits, u32 S,
-                            unsigned long long* setxor, u32* counts, u32* overflow) {
+__global__ void k_bin_apply(const u32* __restrict__ ent_off, const u32* __restrict__ ent_idx, u64 E,
+                            u64 k0, const unsigned long long* __restrict__ soff, u32 sbits, u32 S,
+                            unsigned long long* W) {
   extern __shared__ unsigned long long so[];   // S + 1 slice starts
   for (u32 i = threadIdx.x; i <= S; i += blockDim.x) so[i] = soff[i];
   __syncthreads();
@@ -195,82 +213,21 @@ __global__ void k_bin_apply(const u32* __restrict__ ent_off, const u64* __restri
       s = a;
     }
     const u64 c = ((u64)s << sbits) + ent_off[i];
-    atomicXor(setxor + c, (unsigned long long)ent_h[i]);
-    const u32 sh = 8 * (u32)(c & 3);
-    const u32 old = atomicAdd(counts + (c >> 2), 1u << sh);
-    if (((old >> sh) & 0xFFu) == 0xFFu) *overflow = 1;
+    atomicAdd(W + c, (unsigned long long)upd(k0 + ent_idx[i]));
   }
 }
 
-// Claim: a count-1 cell c claims its key iff no lower cell of that key has
-// count 1.  Counts are only read here, so the round sees one snapshot.
-__global__ void k_claim(const unsigned long long* __restrict__ setxor, const u32* __restrict__ counts,
-                        u16* __restrict__ round, u64 m, u64 block, u64 recip, u16 r,
-                        unsigned long long* n_claimed) {
-  const u32 lane = threadIdx.x & 31;
-  for (u64 c0 = blockIdx.x * (u64)blockDim.x; c0 < m; c0 += (u64)gridDim.x * blockDim.x) {
-    const u64 c = c0 + threadIdx.x;
-    bool claim = false;
-    if (c < m && count_of(counts, c) == 1) {
-      const u64 h = setxor[c];
-      u64 cs[3];
-      cell_indices(h, block, recip, cs);
-      claim = true;
-#pragma unroll
-      for (int t = 0; t < 3; ++t)
-        if (cs[t] < c && count_of(counts, cs[t]) == 1) claim = false;
-      if (claim) round[c] = r;
-    }
-    const u32 ballot = __ballot_sync(0xFFFFFFFFu, claim);
-    if (lane == 0 && ballot) atomicAdd(n_claimed, (unsigned long long)__popc(ballot));
-  }
-}
-
-// Apply the round's claims: remove each claimed key from its other cells and
-// clear the claimed cell's count (its setxor keeps the key's hash).
-__global__ void k_apply(unsigned long long* setxor, u32* counts, const u16* __restrict__ round,
-                        u64 m, u64 block, u64 recip, u16 r) {
-  for (u64 c = blockIdx.x * (u64)blockDim.x + threadIdx.x; c < m;
-       c += (u64)gridDim.x * blockDim.x) {
-    if (round[c] != r) continue;
-    const u64 h = setxor[c];
-    u64 cs[3];
-    cell_indices(h, block, recip, cs);
-#pragma unroll
-    for (int t = 0; t < 3; ++t) {
-      if (cs[t] == c) continue;
-      atomicXor(setxor + cs[t], (unsigned long long)h);
-      atomicSub(counts + (cs[t] >> 2), 1u << (8 * (u32)(cs[t] & 3)));
-    }
-    atomicAnd(counts + (c >> 2), ~(0xFFu << (8 * (u32)(c & 3))));
-  }
-}
-
-// Reverse fill of one round, in place.
-__global__ void k_fill(unsigned long long* setxor, const u16* __restrict__ round, u64 m, u64 block,
-                       u64 recip, u16 r, u64 mask) {
-  for (u64 c = blockIdx.x * (u64)blockDim.x + threadIdx.x; c < m;
-       c += (u64)gridDim.x * blockDim.x) {
-    if (round[c] != r) continue;
-    const u64 h = setxor[c];
-    u64 cs[3];
-    cell_indices(h, block, recip, cs);
-    u64 v = h & mask;
-#pragma unroll
-    for (int t = 0; t < 3; ++t)
-      if (cs[t] != c) v ^= setxor[cs[t]];
-    setxor[c] = v & mask;
-  }
-}
-
-// ---- peel over lists ---------------------------------------------------------
-// The same rounds, visiting only what can change.  Every count-1 cell at the
-// start of round r > 1 got its count 1 while round r-1 removed keys (a
-// count-1 cell of round r-1 either claimed its key or lost it to a lower
-// cell of the same key), so round r's candidates are exactly the cells whose
-// count went from 2 to 1 during round r-1's apply.  Claimed cells are
-// appended to one list in round order, which the fill then walks backwards.
-// Cell indices are u32 (used when m <= 2^32).
+// ---- peel ------------------------------------------------------------------
+// Round r claims every key whose lowest count-1 cell is a count-1 cell (so a
+// key is claimed once), then removes each claimed key from its two other
+// cells; a claimed cell keeps its key's index with count 0.  Every count-1
+// cell at the start of round r > 1 got its count 1 while round r-1 removed
+// keys (a count-1 cell of round r-1 either claimed its key or lost it to a
+// lower cell of the same key), so after a full scan in round 1 each round
+// visits only the cells whose count went from 2 to 1 in the round before.
+// Claimed cells are appended in round order (u32 cell indices, m <= 2^32),
+// and the fill walks that list backwards.  For m > 2^32, or without room for
+// the lists, every round scans all cells and tags its claims with the round.
 
 // Append the flagged lanes' values (every lane of the warp calls this).
 __device__ __forceinline__ void warp_append(bool take, u32 val, u32* list,
@@ -289,80 +246,126 @@ __device__ __forceinline__ void warp_append(bool take, u32 val, u32* list,
   }
 }
 
-// Claim over the candidates cand[0, ncand), or over every cell when cand is
-// null: the lowest count-1 cell of a key claims it (appended to order).
+// Does cell c (count 1) claim its key?  The key's lower count-1 cells win.
+__device__ __forceinline__ bool claims(const unsigned long long* W, const u64* keys, u64 seed,
+                                       u64 block, u64 recip, u64 c, u64 w) {
+  u64 cs[3];
+  cell_indices(key_hash(keys, w & kSumMask, seed), block, recip, cs);
+#pragma unroll
+  for (int t = 0; t < 3; ++t)
+    if (cs[t] < c && cnt_of(W[cs[t]]) == 1) return false;
+  return true;
+}
+
+// Claims among cand[0, ncand), or among every cell when cand is null.
 __global__ void k_claim_list(const u32* __restrict__ cand, u64 ncand,
-                             const unsigned long long* __restrict__ setxor,
-                             const u32* __restrict__ counts, u64 block, u64 recip, u32* order,
-                             unsigned long long* n_order, u64 order_cap, u32* over) {
+                             const unsigned long long* __restrict__ W, const u64* __restrict__ keys,
+                             u64 seed, u64 block, u64 recip, u32* order, unsigned long long* n_order,
+                             u64 order_cap, u32* over) {
   for (u64 base = blockIdx.x * (u64)blockDim.x; base < ncand; base += (u64)gridDim.x * blockDim.x) {
     const u64 i = base + threadIdx.x;
     bool claim = false;
     u32 c = 0;
     if (i < ncand) {
       c = cand ? cand[i] : (u32)i;
-      if (count_of(counts, c) == 1) {
-        const u64 h = setxor[c];
-        u64 cs[3];
-        cell_indices(h, block, recip, cs);
-        claim = true;
-#pragma unroll
-        for (int t = 0; t < 3; ++t)
-          if (cs[t] < c && count_of(counts, cs[t]) == 1) claim = false;
-      }
+      const u64 w = W[c];
+      claim = cnt_of(w) == 1 && claims(W, keys, seed, block, recip, c, w);
     }
     warp_append(claim, c, order, n_order, order_cap, over);
   }
 }
 
-// Remove each claimed key from its two other cells; a cell whose count goes
-// from 2 to 1 becomes a candidate of the next round.
-__global__ void k_apply_list(const u32* __restrict__ claimed, u64 L, unsigned long long* setxor,
-                             u32* counts, u64 block, u64 recip, u32* next,
+// Removes the key of claimed cell c from its two other cells; returns the
+// cells whose count went from 2 to 1 (t0/t1 flags).
+__device__ __forceinline__ void remove_key(unsigned long long* W, const u64* keys, u64 seed,
+                                           u64 block, u64 recip, u64 c, bool& t0, u64& a0, bool& t1,
+                                           u64& a1) {
+  const u64 idx = W[c] & kSumMask;
+  u64 cs[3];
+  cell_indices(key_hash(keys, idx, seed), block, recip, cs);
+  int k = 0;
+#pragma unroll
+  for (int t = 0; t < 3; ++t) {
+    if (cs[t] == c) continue;
+    const u64 old = atomicAdd(W + cs[t], (unsigned long long)(0 - upd(idx)));
+    const bool to_one = cnt_of(old) == 2;
+    if (k == 0) { t0 = to_one; a0 = cs[t]; }
+    else { t1 = to_one; a1 = cs[t]; }
+    ++k;
+  }
+  W[c] = idx;   // count 0; the index stays for the fill
+}
+
+__global__ void k_apply_list(const u32* __restrict__ claimed, u64 L, unsigned long long* W,
+                             const u64* __restrict__ keys, u64 seed, u64 block, u64 recip, u32* next,
                              unsigned long long* n_next, u64 next_cap, u32* over) {
   for (u64 base = blockIdx.x * (u64)blockDim.x; base < L; base += (u64)gridDim.x * blockDim.x) {
     const u64 i = base + threadIdx.x;
     bool t0 = false, t1 = false;
-    u32 a0 = 0, a1 = 0;
-    if (i < L) {
-      const u32 c = claimed[i];
-      const u64 h = setxor[c];
-      u64 cs[3];
-      cell_indices(h, block, recip, cs);
-      int k = 0;
-#pragma unroll
-      for (int t = 0; t < 3; ++t) {
-        if (cs[t] == c) continue;
-        atomicXor(setxor + cs[t], (unsigned long long)h);
-        const u32 sh = 8 * (u32)(cs[t] & 3);
-        const u32 old = atomicSub(counts + (cs[t] >> 2), 1u << sh);
-        const bool to_one = ((old >> sh) & 0xFFu) == 2u;
-        if (k == 0) { t0 = to_one; a0 = (u32)cs[t]; }
-        else { t1 = to_one; a1 = (u32)cs[t]; }
-        ++k;
-      }
-      atomicAnd(counts + (c >> 2), ~(0xFFu << (8 * (c & 3))));
-    }
-    warp_append(t0, a0, next, n_next, next_cap, over);
-    warp_append(t1, a1, next, n_next, next_cap, over);
+    u64 a0 = 0, a1 = 0;
+    if (i < L) remove_key(W, keys, seed, block, recip, claimed[i], t0, a0, t1, a1);
+    warp_append(t0, (u32)a0, next, n_next, next_cap, over);
+    warp_append(t1, (u32)a1, next, n_next, next_cap, over);
   }
 }
 
-// Reverse fill of one round's claimed cells, in place.
-__global__ void k_fill_list(const u32* __restrict__ claimed, u64 L, unsigned long long* setxor,
-                            u64 block, u64 recip, u64 mask) {
-  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < L;
-       i += (u64)gridDim.x * blockDim.x) {
-    const u32 c = claimed[i];
-    const u64 h = setxor[c];
-    u64 cs[3];
-    cell_indices(h, block, recip, cs);
-    u64 v = h & mask;
+// Reverse fill of claimed cell c: fingerprint of its key xor its two other
+// cells, which are final already (filled in a later round, or never claimed
+// and 0).
+__device__ __forceinline__ void fill_cell(unsigned long long* W, const u64* keys, u64 seed,
+                                          u64 block, u64 recip, u64 mask, u64 c) {
+  const u64 h = key_hash(keys, W[c], seed);
+  u64 cs[3];
+  cell_indices(h, block, recip, cs);
+  u64 v = h & mask;
 #pragma unroll
-    for (int t = 0; t < 3; ++t)
-      if (cs[t] != c) v ^= setxor[cs[t]];
-    setxor[c] = v & mask;
+  for (int t = 0; t < 3; ++t)
+    if (cs[t] != c) v ^= W[cs[t]];
+  W[c] = v & mask;
+}
+
+__global__ void k_fill_list(const u32* __restrict__ claimed, u64 L, unsigned long long* W,
+                            const u64* __restrict__ keys, u64 seed, u64 block, u64 recip, u64 mask) {
+  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < L;
+       i += (u64)gridDim.x * blockDim.x)
+    fill_cell(W, keys, seed, block, recip, mask, claimed[i]);
+}
+
+// The scan form: claims of round r tagged in round[], apply and fill by tag.
+__global__ void k_claim_scan(const unsigned long long* __restrict__ W, const u64* __restrict__ keys,
+                             u64 seed, u16* __restrict__ round, u64 m, u64 block, u64 recip, u16 r,
+                             unsigned long long* n_claimed) {
+  const u32 lane = threadIdx.x & 31;
+  for (u64 c0 = blockIdx.x * (u64)blockDim.x; c0 < m; c0 += (u64)gridDim.x * blockDim.x) {
+    const u64 c = c0 + threadIdx.x;
+    bool claim = false;
+    if (c < m) {
+      const u64 w = W[c];
+      claim = cnt_of(w) == 1 && claims(W, keys, seed, block, recip, c, w);
+      if (claim) round[c] = r;
+    }
+    const u32 ballot = __ballot_sync(0xFFFFFFFFu, claim);
+    if (lane == 0 && ballot) atomicAdd(n_claimed, (unsigned long long)__popc(ballot));
   }
+}
+
+__global__ void k_apply_scan(unsigned long long* W, const u64* __restrict__ keys, u64 seed,
+                             const u16* __restrict__ round, u64 m, u64 block, u64 recip, u16 r) {
+  for (u64 c = blockIdx.x * (u64)blockDim.x + threadIdx.x; c < m;
+       c += (u64)gridDim.x * blockDim.x) {
+    if (round[c] != r) continue;
+    bool t0, t1;
+    u64 a0, a1;
+    remove_key(W, keys, seed, block, recip, c, t0, a0, t1, a1);
+  }
+}
+
+__global__ void k_fill_scan(unsigned long long* W, const u64* __restrict__ keys, u64 seed,
+                            const u16* __restrict__ round, u64 m, u64 block, u64 recip, u16 r,
+                            u64 mask) {
+  for (u64 c = blockIdx.x * (u64)blockDim.x + threadIdx.x; c < m;
+       c += (u64)gridDim.x * blockDim.x)
+    if (round[c] == r) fill_cell(W, keys, seed, block, recip, mask, c);
 }
 
 __global__ void k_narrow(const u64* __restrict__ in, u32* __restrict__ out, u64 m) {
@@ -386,13 +389,13 @@ u64 pow2_at_least(u64 x) { u64 p = 1; while (p < x) p <<= 1; return p; }
 // Incidence of keys [0, n) for one seed through the slice bins, in chunks of
 // keys whose updates fit the entry buffers (ent_cap updates).
 int incidence_binned(s615_ctx* ctx, const u64* keys, u64 n, u64 seed, u64 m, u64 block, u64 recip,
-                     u32* ent_off, u64* ent_h, u64 ent_cap, unsigned long long* setxor, u32* counts,
-                     u32* d_over, u32* bhist, unsigned long long* bbase, cudaStream_t st) {
+                     u32* ent_off, u32* ent_idx, u64 ent_cap, unsigned long long* W, u32* bhist,
+                     unsigned long long* bbase, cudaStream_t st) {
   u32 sbits = 21;
   while (((m + (1ull << sbits) - 1) >> sbits) > kMaxSlices) ++sbits;
   const u32 S = (u32)((m + (1ull << sbits) - 1) >> sbits);
   const int G = ctx->num_sms * 2;
-  const u64 chunk = std::max<u64>(1, ent_cap / 3);
+  const u64 chunk = std::max<u64>(1, std::min<u64>(ent_cap / 3, 1ull << 32));
   std::vector<u32> h_hist((size_t)G * S);
   std::vector<unsigned long long> h_base((size_t)G * S), h_soff(S + 1);
   for (u64 k0 = 0; k0 < n; k0 += chunk) {
@@ -418,14 +421,14 @@ int incidence_binned(s615_ctx* ctx, const u64* keys, u64 n, u64 seed, u64 m, u64
     S615_CU(cudaMemcpyAsync(bbase, h_base.data(), h_base.size() * sizeof(unsigned long long),
                             cudaMemcpyHostToDevice, st));
     k_bin_scatter<<<G, kBinThreads, S * sizeof(unsigned long long), st>>>(
-        keys, k0, per, k1, seed, block, recip, sbits, S, bbase, ent_off, ent_h);
+        keys, k0, per, k1, seed, block, recip, sbits, S, bbase, ent_off, ent_idx);
     ctx->launches++;
     S615_CU(cudaGetLastError());
     // the slice starts go where the block bases were (read by the apply kernel)
     S615_CU(cudaMemcpyAsync(bbase, h_soff.data(), (S + 1) * sizeof(unsigned long long),
                             cudaMemcpyHostToDevice, st));
     k_bin_apply<<<grid_for(ctx, run, 256), 256, (S + 1) * sizeof(unsigned long long), st>>>(
-        ent_off, ent_h, run, bbase, sbits, S, setxor, counts, d_over);
+        ent_off, ent_idx, run, k0, bbase, sbits, S, W);
     ctx->launches++;
     S615_CU(cudaGetLastError());
     S615_CU(cudaStreamSynchronize(st));   // h_base / h_soff are reused by the next chunk
@@ -559,10 +562,10 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
   // ---- 2-4. per seed: incidence, peel, fill ----
   const u64 m = capacity_for(n);
   const u64 block = m / 3, recip = mod_recip(block);
-  Buf setxor(ctx), counts(ctx), rounds(ctx), scratch(ctx), order(ctx), front(ctx);
-  int s = setxor.alloc(m * sizeof(u64));
+  if (n > kMaxKeys) return S615_E_BUILD;   // key indices must stay below 2^34
+  Buf cells(ctx), rounds(ctx), scratch(ctx), order(ctx), front(ctx);
+  int s = cells.alloc(m * sizeof(u64));
   if (s) return s;
-  if ((s = counts.alloc(((m + 3) / 4) * sizeof(u32)))) return s;
   // Peel over lists (claimed cells in round order, two candidate lists of
   // m/8 cells each; a round whose candidates overflow scans every cell), or,
   // for m > 2^32 or without room for the lists, over full scans by round tag.
@@ -574,13 +577,18 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
   }
   if (!lists && (s = rounds.alloc(m * sizeof(u16)))) return s;
   if ((s = scratch.alloc(64))) return s;
-  u32* d_over = static_cast<u32*>(scratch.p);
-  unsigned long long* d_claimed = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch.p) + 8);
+  auto* W = static_cast<unsigned long long*>(cells.p);
+  const u64* K = static_cast<const u64*>(keys.p);
+  // scratch: [0] max count, [4] list overflow, [8] n_order / n_claimed, [16] n_next
+  u32* d_max = static_cast<u32*>(scratch.p);
+  u32* d_lover = reinterpret_cast<u32*>(static_cast<char*>(scratch.p) + 4);
+  auto* d_norder = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch.p) + 8);
+  auto* d_nnext = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch.p) + 16);
   const int g = grid_for(ctx, m, 256);
   // Entry buffers of the binned incidence: all 3n updates when HBM allows,
-  // else chunks of keys; with no room for a useful chunk the incidence falls
-  // back to direct atomics (k_incidence).
-  Buf ent_off(ctx), ent_h(ctx), bins(ctx);
+  // else chunks of keys; with no room for a useful chunk the incidence adds
+  // directly into the cell words (k_incidence).
+  Buf ent_off(ctx), ent_idx(ctx), bins(ctx);
   u64 ent_cap = 0;
   {
     size_t free_b = 0, total_b = 0;
@@ -590,13 +598,13 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
     avail = avail > margin ? avail - margin : 0;
     const size_t bin_bytes = (size_t)ctx->num_sms * 2 * kMaxSlices * (4 + 8) + 64;
     if (avail > bin_bytes) {
-      ent_cap = std::min<u64>(3 * n, (avail - bin_bytes) / 12);
+      ent_cap = std::min<u64>(3 * n, (avail - bin_bytes) / 8);
       ent_cap = ent_cap / 3 * 3;
     }
     if (ent_cap >= std::min<u64>(3 * n, 3ull << 20)) {
-      if ((s = ent_off.alloc(ent_cap * 4)) || (s = ent_h.alloc(ent_cap * 8)) ||
+      if ((s = ent_off.alloc(ent_cap * 4)) || (s = ent_idx.alloc(ent_cap * 4)) ||
           (s = bins.alloc(bin_bytes))) {
-        ent_off.release(); ent_h.release(); bins.release();
+        ent_off.release(); ent_idx.release(); bins.release();
         ent_cap = 0;
       }
     } else {
@@ -608,8 +616,7 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
   int trace_rounds = 0;
   for (int si = 0; si < n_seeds && !built; ++si) {
     const u64 seed = seeds[si];
-    S615_CU(cudaMemsetAsync(setxor.p, 0, m * sizeof(u64), st));
-    S615_CU(cudaMemsetAsync(counts.p, 0, ((m + 3) / 4) * sizeof(u32), st));
+    S615_CU(cudaMemsetAsync(W, 0, m * sizeof(u64), st));
     if (!lists) S615_CU(cudaMemsetAsync(rounds.p, 0, m * sizeof(u16), st));
     S615_CU(cudaMemsetAsync(scratch.p, 0, 64, st));
     if (ent_cap) {
@@ -617,25 +624,23 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
       u32* bhist = static_cast<u32*>(bins.p);
       auto* bbase = reinterpret_cast<unsigned long long*>(static_cast<char*>(bins.p) +
                                                           (G * kMaxSlices * 4 + 7) / 8 * 8);
-      if ((s = incidence_binned(ctx, static_cast<const u64*>(keys.p), n, seed, m, block, recip,
-                                static_cast<u32*>(ent_off.p), static_cast<u64*>(ent_h.p), ent_cap,
-                                static_cast<unsigned long long*>(setxor.p),
-                                static_cast<u32*>(counts.p), d_over, bhist, bbase, st)))
+      if ((s = incidence_binned(ctx, K, n, seed, m, block, recip, static_cast<u32*>(ent_off.p),
+                                static_cast<u32*>(ent_idx.p), ent_cap, W, bhist, bbase, st)))
         return s;
     } else {
-      k_incidence<<<grid_for(ctx, n, 256), 256, 0, st>>>(static_cast<const u64*>(keys.p), n, seed,
-                                                         block, recip,
-                                                         static_cast<unsigned long long*>(setxor.p),
-                                                         static_cast<u32*>(counts.p), d_over);
+      k_incidence<<<grid_for(ctx, n, 256), 256, 0, st>>>(K, n, seed, block, recip, W);
       ctx->launches++;
       S615_CU(cudaGetLastError());
     }
+    k_max_count<<<g, 256, 0, st>>>(W, m, d_max);
+    ctx->launches++;
+    u32 mx = 0;
+    S615_CU(cudaMemcpyAsync(&mx, d_max, 4, cudaMemcpyDeviceToHost, st));
+    S615_CU(cudaStreamSynchronize(st));
+    if (mx > 255) return S615_E_BUILD;   // the index sums could reach the count bits
     trace.mark("incidence");
+    const u64 mask = fp_mask((u32)r);
     if (lists) {
-      // scratch: [0] incidence overflow, [4] list overflow, [8] n_order, [16] n_next
-      u32* d_lover = reinterpret_cast<u32*>(static_cast<char*>(scratch.p) + 4);
-      auto* d_norder = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch.p) + 8);
-      auto* d_nnext = reinterpret_cast<unsigned long long*>(static_cast<char*>(scratch.p) + 16);
       u32* ord = static_cast<u32*>(order.p);
       u32* fr[2] = {static_cast<u32*>(front.p), static_cast<u32*>(front.p) + fcap};
       std::vector<u64> off{0};
@@ -643,9 +648,8 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
       const u32* cand = nullptr;   // round 1 scans every cell
       int cur = 0;
       while (off.size() <= 0xFFFE) {
-        k_claim_list<<<grid_for(ctx, ncand, 256), 256, 0, st>>>(
-            cand, ncand, static_cast<const unsigned long long*>(setxor.p),
-            static_cast<const u32*>(counts.p), block, recip, ord, d_norder, n, d_lover);
+        k_claim_list<<<grid_for(ctx, ncand, 256), 256, 0, st>>>(cand, ncand, W, K, seed, block,
+                                                                recip, ord, d_norder, n, d_lover);
         ctx->launches++;
         unsigned long long h_n[2] = {0, 0};
         u32 h_lover = 0;
@@ -655,9 +659,8 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
         if (L == 0) break;
         S615_CU(cudaMemsetAsync(d_nnext, 0, 8, st));
         S615_CU(cudaMemsetAsync(d_lover, 0, 4, st));
-        k_apply_list<<<grid_for(ctx, L, 256), 256, 0, st>>>(
-            ord + total, L, static_cast<unsigned long long*>(setxor.p), static_cast<u32*>(counts.p),
-            block, recip, fr[cur ^ 1], d_nnext, fcap, d_lover);
+        k_apply_list<<<grid_for(ctx, L, 256), 256, 0, st>>>(ord + total, L, W, K, seed, block, recip,
+                                                            fr[cur ^ 1], d_nnext, fcap, d_lover);
         ctx->launches++;
         S615_CU(cudaGetLastError());
         S615_CU(cudaMemcpyAsync(&h_n[1], d_nnext, 8, cudaMemcpyDeviceToHost, st));
@@ -676,66 +679,50 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
           if (ncand == 0) break;   // nothing became count 1: the peel is over
         }
       }
-      u32 over = 0;
-      S615_CU(cudaMemcpy(&over, d_over, 4, cudaMemcpyDeviceToHost));
-      if (over) return S615_E_BUILD;
       if (total != n) continue;   // 2-core not empty: next seed
       trace.mark("peel");
-      const u64 mask = fp_mask((u32)r);
       for (size_t q = off.size() - 1; q >= 1; --q) {
         const u64 L = off[q] - off[q - 1];
-        k_fill_list<<<grid_for(ctx, L, 256), 256, 0, st>>>(
-            ord + off[q - 1], L, static_cast<unsigned long long*>(setxor.p), block, recip, mask);
+        k_fill_list<<<grid_for(ctx, L, 256), 256, 0, st>>>(ord + off[q - 1], L, W, K, seed, block,
+                                                           recip, mask);
         ctx->launches++;
       }
-      S615_CU(cudaGetLastError());
-      trace.mark("fill");
       trace_rounds = (int)off.size() - 1;
-      built = true;
-      used_seed = seed;
-      continue;
-    }
-    u64 peeled = 0;
-    u16 rr = 0;
-    for (;;) {
-      if (rr == 0xFFFE) break;
-      ++rr;
-      S615_CU(cudaMemsetAsync(d_claimed, 0, 8, st));
-      k_claim<<<g, 256, 0, st>>>(static_cast<const unsigned long long*>(setxor.p),
-                                 static_cast<const u32*>(counts.p), static_cast<u16*>(rounds.p), m,
-                                 block, recip, rr, d_claimed);
-      ctx->launches++;
-      k_apply<<<g, 256, 0, st>>>(static_cast<unsigned long long*>(setxor.p),
-                                 static_cast<u32*>(counts.p), static_cast<const u16*>(rounds.p), m,
-                                 block, recip, rr);
-      ctx->launches++;
-      S615_CU(cudaGetLastError());
-      unsigned long long c = 0;
-      S615_CU(cudaMemcpyAsync(&c, d_claimed, 8, cudaMemcpyDeviceToHost, st));
-      S615_CU(cudaStreamSynchronize(st));
-      if (c == 0) { --rr; break; }
-      peeled += c;
-    }
-    u32 over = 0;
-    S615_CU(cudaMemcpy(&over, d_over, 4, cudaMemcpyDeviceToHost));
-    if (over) return S615_E_BUILD;
-    if (peeled != n) continue;   // 2-core not empty: next seed
-    trace.mark("peel");
-    const u64 mask = fp_mask((u32)r);
-    for (u16 q = rr; q >= 1; --q) {
-      k_fill<<<g, 256, 0, st>>>(static_cast<unsigned long long*>(setxor.p),
-                                static_cast<const u16*>(rounds.p), m, block, recip, q, mask);
-      ctx->launches++;
+    } else {
+      u16* rt = static_cast<u16*>(rounds.p);
+      u64 peeled = 0;
+      u16 rr = 0;
+      for (;;) {
+        if (rr == 0xFFFE) break;
+        ++rr;
+        S615_CU(cudaMemsetAsync(d_norder, 0, 8, st));
+        k_claim_scan<<<g, 256, 0, st>>>(W, K, seed, rt, m, block, recip, rr, d_norder);
+        ctx->launches++;
+        k_apply_scan<<<g, 256, 0, st>>>(W, K, seed, rt, m, block, recip, rr);
+        ctx->launches++;
+        S615_CU(cudaGetLastError());
+        unsigned long long c = 0;
+        S615_CU(cudaMemcpyAsync(&c, d_norder, 8, cudaMemcpyDeviceToHost, st));
+        S615_CU(cudaStreamSynchronize(st));
+        if (c == 0) { --rr; break; }
+        peeled += c;
+      }
+      if (peeled != n) continue;   // 2-core not empty: next seed
+      trace.mark("peel");
+      for (u16 q = rr; q >= 1; --q) {
+        k_fill_scan<<<g, 256, 0, st>>>(W, K, seed, rt, m, block, recip, q, mask);
+        ctx->launches++;
+      }
+      trace_rounds = rr;
     }
     S615_CU(cudaGetLastError());
     trace.mark("fill");
-    trace_rounds = rr;
     built = true;
     used_seed = seed;
   }
   if (!built) return S615_E_BUILD;
-  keys.release(); counts.release(); rounds.release(); order.release(); front.release();
-  ent_off.release(); ent_h.release(); bins.release();
+  keys.release(); rounds.release(); order.release(); front.release();
+  ent_off.release(); ent_idx.release(); bins.release();
 
   out->hdr.n_keys = n;
   out->hdr.m_cells = m;
@@ -747,7 +734,7 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
     void* p = nullptr;
     if ((s = dev_alloc(ctx, &p, bytes))) return s;
     S615_CU(cudaMemsetAsync(p, 0, bytes, st));
-    if ((s = launch_pack(ctx, setxor.p, 8, m, (u32)r, static_cast<u8*>(p), len, st))) {
+    if ((s = launch_pack(ctx, cells.p, 8, m, (u32)r, static_cast<u8*>(p), len, st))) {
       dev_free(ctx, p, bytes);
       return s;
     }
@@ -757,14 +744,14 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
     void* p = nullptr;
     const size_t bytes = m * sizeof(u32);
     if ((s = dev_alloc(ctx, &p, bytes))) return s;
-    k_narrow<<<g, 256, 0, st>>>(static_cast<const u64*>(setxor.p), static_cast<u32*>(p), m);
+    k_narrow<<<g, 256, 0, st>>>(static_cast<const u64*>(cells.p), static_cast<u32*>(p), m);
     ctx->launches++;
     out->layout = S615_LAYOUT_WIDE; out->cell_bytes = 4;
     out->d_cells = p; out->bytes = bytes;
   } else {
     out->layout = S615_LAYOUT_WIDE; out->cell_bytes = 8;
-    out->d_cells = setxor.p; out->bytes = setxor.n;
-    setxor.p = nullptr; setxor.n = 0;   // ownership moves to the table
+    out->d_cells = cells.p; out->bytes = cells.n;
+    cells.p = nullptr; cells.n = 0;   // ownership moves to the table
   }
   trace.mark("layout");
   trace.report(n, m, trace_rounds);
