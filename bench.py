@@ -1275,6 +1275,12 @@ def main():
             "%.3e" % roof["random_access"]["ceiling_reads_per_s"]
             if roof["random_access"]["ceiling_reads_per_s"] else "n/a",
             roof["random_access"]["frac"]))
+    # DRAM bytes the probe moves: each cell read misses L2 and fills one 64-byte
+    # line (ld.global.cg.L2::64B; a one-pass ncu capture of the full pass
+    # measured 191.7 B per post-gate probe); against the same copy peak
+    dram = 3 * 64 * ctr.probes / dur_s / 1e9
+    roof["dram_fills"] = {"bytes_per_cell_read": 64, "achieved": round(dram, 1), "peak": peak,
+                          "unit": "GB/s", "frac": round(dram / peak, 4)}
 
     # plain per-unit-launch form on a bounded sample of the same band
     plain = None
