@@ -65,7 +65,8 @@ def parse():
     ap.add_argument("--shards", type=int, default=1,
                     help="cls5: a pair-space shard set of S tables (S >= 2) instead of one table")
     ap.add_argument("--layout", default="auto", choices=["auto", "wide", "packed"])
-    ap.add_argument("--workload", default="cls5", choices=["cls5", "cls617", "mix", "serve", "jobs"])
+    ap.add_argument("--workload", default="cls5",
+                    choices=["cls5", "cls617", "mix", "serve", "jobs", "cfg1"])
     ap.add_argument("--units", type=int, default=0, help="mix: units per step (default 200,000)")
     ap.add_argument("--seconds", type=float, default=10.0, help="serve: seconds of arrivals")
     ap.add_argument("--reference-gpu", type=int, default=-1,
@@ -721,6 +722,58 @@ METRIC_MIX = "mixed-class units/s (classes 2:4%/3:1%/4:48%/5:47%, B log-uniform 
 METRIC_SERVE = "per-unit latency p50/p99 through the serving loop (Poisson 5,000 units/s), 1 B200"
 
 
+def run_cfg1(args, rank, world, local, dist):
+    """--workload cfg1: the small CPU-runnable configuration -- every class-5
+    unit of B in [1000, 30000] (725) plus 8 plants against an N = 715, r = 48
+    table built on the device (1.9 MB) -- timed with and without the peel's
+    L2-persisting access window, and the oracle on the host cores beside it."""
+    import numpy as np
+    import torch
+
+    import orc
+    import s615
+    import workloads as W
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    N = 715
+    eng = s615.Engine(local)
+    tid = eng.build_table(N, args.r)
+    units = W.cls5_units(1000, 30000)
+    plants = W.plants(8, 0, 1000, 30000, N)
+    arr, n = W.unit_array(units, plants, N)
+    lib = s615.lib()
+    b = C.c_void_p()
+    s615._check(lib.s615_prepare(eng._ctx, C.cast(arr, C.c_void_p), n, C.byref(b)), "prepare")
+    stream = torch.cuda.Stream()
+    res = {}
+    for name, fl in (("window", 0), ("no_window", s615.F_NO_L2_WINDOW)):
+        for _ in range(args.warmup):
+            timed_steps(lib, eng, tid, b, stream, fl, 1)
+        ms, c = timed_steps(lib, eng, tid, b, stream, fl, max(args.steps, 50))
+        res[name] = {"ms_per_pass": ms / max(args.steps, 50), "pos": c.pos, "probes": c.probes}
+    s615._check(lib.s615_batch_free(eng._ctx, b), "batch_free")
+    hb, pk = eng.export_table(tid)
+    ot = orc.Table.from_memory(hb, pk)
+    oarr = orc.units_array([orc.pack_unit(B, u) for B, u in units])
+    t0 = time.perf_counter()
+    _, (calls, gated, probes) = orc.cls5_run(ot, oarr, len(units))
+    cpu_s = time.perf_counter() - t0
+    eng.close()
+    v = res["window"]["pos"] / (res["window"]["ms_per_pass"] / 1e3)
+    line = {"metric": "cls5 peel probes/sec, B in [1000, 30000] (config 1), 1 B200", "value": v,
+            "unit": UNIT, "n_gpus": 1, "steps": max(args.steps, 50), "warmup": args.warmup,
+            "ms_per_step": res["window"]["ms_per_pass"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": f"config 1: {len(units)} Stage-1 units + 8 plants, N={N} r={args.r} "
+                                   "table built on the device (1.9 MB: fits L2)"},
+            "l2_window": res,
+            "cpu_baseline": {"value": (gated + probes) / cpu_s, "unit": UNIT, "cores": os.cpu_count(),
+                             "kind": "port", "sample": f"all {len(units)} units once"}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_mix(args, rank, world, local, dist):
     """200,000 Stage-1 units of classes 2-5 in one persistent batch (the mixed
     queue), B log-uniform on [1M, 4M], 64 plants, N = 95,239 (B <= 4M)."""
@@ -1107,6 +1160,8 @@ def run_serve(args, rank, world, local, dist):
 def main():
     args = parse()
     rank, world, local, dist = dist_setup(args)
+    if args.workload == "cfg1":
+        return run_cfg1(args, rank, world, local, dist)
     if args.workload == "mix":
         return run_mix(args, rank, world, local, dist)
     if args.workload == "serve":

@@ -175,3 +175,19 @@ def test_band_production_table_parity(engine):
     assert (ctr.calls, ctr.gated, ctr.probes) == (calls, gated, probes)
     assert len(ohits) > len(plants)   # filter false positives at r = 20 (~26 expected), and the plants
     np.testing.assert_array_equal(sorted_hits(hits), sorted_hits(ohits))
+
+
+def test_l2_window_does_not_change_results(engine, oracle_table, config1):
+    # the peel launches mark config 1's table (1.9 MB) persisting in L2 by
+    # default; without the window the counters and raw hits are the same
+    units, plants = config1
+    _, path = oracle_table(N1, 20)
+    tid = engine.load_table(path, N1)
+    try:
+        arr, n = W.unit_array(units, plants, N1)
+        h0, c0 = engine.cls5_run(tid, arr, n)
+        h1, c1 = engine.cls5_run(tid, arr, n, flags=s615.F_NO_L2_WINDOW)
+        assert (c0.calls, c0.gated, c0.probes, c0.hits) == (c1.calls, c1.gated, c1.probes, c1.hits)
+        np.testing.assert_array_equal(sorted_hits(h0), sorted_hits(h1))
+    finally:
+        engine.free_table(tid)
