@@ -69,9 +69,9 @@ def parse():
                     choices=["cls5", "cls617", "mix", "serve", "jobs", "cfg1"])
     ap.add_argument("--units", type=int, default=0, help="mix: units per step (default 200,000)")
     ap.add_argument("--seconds", type=float, default=10.0, help="serve: seconds of arrivals")
-    ap.add_argument("--reference-gpu", type=int, default=-1,
+    ap.add_argument("--reference-gpu", type=int, default=15536,
                     help="cls5: run the reference's fourcore_cls5_gpu_v4 on K evenly spaced band "
-                         "units (0: the whole band; -1: skip)")
+                         "units (default: a tenth of the band; 0: the whole band; -1: skip)")
     return ap.parse_args()
 
 
