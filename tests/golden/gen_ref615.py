@@ -14,10 +14,12 @@ stand-in header oracle/gmpshim/gmpxx.h):
                         unit count, the summary counters calls= and probes=,
                         the gate percentage and the SOLUTION lines
                         (fourcore_cls5_gpu_v4.cu:545-562, 611-709).
-  fourcore_find_v4      --units on class 2-4 units (find3 leaf): per-mode sums
-                        of its [gate] batch counters, the job and failT counts
-                        and the SOLUTION lines (fourcore_find_v4.cu:504-508,
-                        1128-1158).
+  fourcore_find_v4      --units on class 2-4 units (find3 leaf) and on class-1
+                        units (find4), and --jobs on reduced-T job files (the
+                        hunt tool's .but, and the same jobs written as .bbj by
+                        the engine's s615_jobs_write): per-mode sums of its
+                        [gate] batch counters, the job and failT counts and the
+                        SOLUTION lines (fourcore_find_v4.cu:504-508, 1094-1222).
 
 Tables come from the reference's own host builder (oracle/_ref/xor_build_save),
 whose files the oracle reproduces byte for byte.  The counters of a class-5
@@ -72,24 +74,45 @@ CLS5_RUNS = [
     ("band_c", 3219993, 3219999, 2000, 16, True),
     ("band_a", 3200000, 3200006, 2000, 48, False),
 ]
-# find_v4 --units runs on class 2-4 units: (lo, hi, classes, r, gate)
+# find_v4 --units runs: (lo, hi, classes, r, gate).  Class 1 makes the
+# reference build an N = 23,809 table on the host (a few minutes).
 FIND_RUNS = [
     (150000, 150299, "2,3,4", 16, True),
     (150000, 150299, "2,3,4", 48, True),
     (150000, 150299, "2,3,4", 20, False),
+    (1000000, 1000999, "1", 48, True),
+    (1000000, 1000999, "1", 20, False),
+]
+# find_v4 --jobs runs on reduced-T job files: (format, lo, hi, classes, r, gate)
+JOB_FILE_RUNS = [
+    ("but", 150000, 150299, "2,3,4", 48, True),
+    ("but", 150000, 150299, "2,3,4", 16, True),
+    ("bbj", 150000, 150299, "2,3,4", 20, False),
 ]
 
 DONE5 = re.compile(r"---- done cls5-gpu: solutions=(\d+) units=(\d+) calls=(\d+) probes=(\d+) time=(\S+)s ----")
 PROG5 = re.compile(r"\[cls5-gpu\] units=\d+/\d+ calls=(\d+) probes=(\d+) gate=([\d.]+)%")
 PACKED = re.compile(r"\[cls5-gpu\] packed (\d+)/(\d+) units")
 GATE4 = re.compile(r"\[gate\] batch n=(\d+) mode=(\d) calls=(\d+) gated=(\d+) probes=(\d+)")
-DONE4 = re.compile(r"---- done: solutions=(\d+) jobs=(\d+) failT=(\d+) \(units stream\) ----")
+DONE4 = re.compile(r"---- done: solutions=(\d+) jobs=(\d+) failT=(\d+)(?: \((units|bbj) stream\))? ----")
 UNITS4 = re.compile(r"\[units\] (\d+) from .* N=(\d+)")
 
 
-def run(cmd, timeout=1800):
-    p = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+def run(cmd, timeout=1800, env=None):
+    p = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout, env=env)
     return p
+
+
+def find_modes(stderr):
+    """Per-mode sums of the [gate] batch lines (fourcore_find_v4.cu:504-508)."""
+    modes = {}
+    for m in GATE4.finditer(stderr):
+        c = modes.setdefault(m.group(2), {"cands": 0, "calls": 0, "gated": 0, "probes": 0})
+        c["cands"] += int(m.group(1))
+        c["calls"] += int(m.group(3))
+        c["gated"] += int(m.group(4))
+        c["probes"] += int(m.group(5))
+    return modes
 
 
 def sha(path):
@@ -176,12 +199,16 @@ def main():
             fx["cls5"].append(case)
             print(json.dumps(case)[:400])
 
+        # the reference's host table builder spills keys for large N
+        scratch = os.path.join(td, "spill")
+        os.makedirs(scratch, exist_ok=True)
+        env = dict(os.environ, XOR_PEEL_SCRATCH=scratch)
         for lo, hi, classes, r, gate in FIND_RUNS:
             ub = emit_units(td, lo, hi, classes)
             cmd = [FIND, "--units", ub, "--r", str(r)]
             if not gate:
                 cmd.append("--no-gate")
-            p = run(cmd)
+            p = run(cmd, env=env)
             case = {"lo": lo, "hi": hi, "classes": classes, "r": r, "gate": gate, "rc": p.returncode,
                     "cmd": " ".join(["oracle/_ref/fourcore_find_v4", "--units",
                                      f"<hunt_v3 --lo {lo} --hi {hi} --classes {classes}>", "--r", str(r)]
@@ -192,18 +219,51 @@ def main():
                 case["error"] = (p.stderr.strip().splitlines() or ["?"])[-3:]
                 ok = False
             else:
-                modes = {}
-                for m in GATE4.finditer(p.stderr):
-                    c = modes.setdefault(m.group(2), {"cands": 0, "calls": 0, "gated": 0, "probes": 0})
-                    c["cands"] += int(m.group(1))
-                    c["calls"] += int(m.group(3))
-                    c["gated"] += int(m.group(4))
-                    c["probes"] += int(m.group(5))
                 case.update(units=int(u.group(1)), N=int(u.group(2)), solutions=int(d.group(1)),
-                            jobs=int(d.group(2)), failT=int(d.group(3)), modes=modes,
+                            jobs=int(d.group(2)), failT=int(d.group(3)), modes=find_modes(p.stderr),
                             solution_lines=[l for l in p.stdout.splitlines() if l.startswith("SOLUTION")],
                             summary=d.group(0))
             fx["find"].append(case)
+            print(json.dumps(case)[:400])
+
+        fx["find_jobs"] = []
+        for fmt, lo, hi, classes, r, gate in JOB_FILE_RUNS:
+            but = os.path.join(td, f"j_{lo}_{hi}.but")
+            if not os.path.exists(but):
+                run([HUNT, "--lo", str(lo), "--hi", str(hi), "--classes", classes, "--expand",
+                     "--emit", but])
+            path = but
+            if fmt == "bbj":   # the same jobs in the binary format, written by the engine
+                sys.path.insert(0, os.path.join(ROOT, "six-one-five_b200"))
+                import s615
+                with open(but) as f:
+                    rows = [[int(x) for x in l.split()] for l in f if l.strip()]
+                arr = (s615.Unit * len(rows))()
+                for k, (c, B, u, f1, f2, tlo, thi) in enumerate(rows):
+                    arr[k] = s615.make_job(c, B, u, tlo | (thi << 64), f1, f2)
+                path = os.path.join(td, f"j_{lo}_{hi}.bbj")
+                s615.jobs_write(path, arr, len(rows))
+            cmd = [FIND, "--jobs", path, "--r", str(r)]
+            if not gate:
+                cmd.append("--no-gate")
+            p = run(cmd, env=env)
+            case = {"format": fmt, "lo": lo, "hi": hi, "classes": classes, "r": r, "gate": gate,
+                    "rc": p.returncode,
+                    "cmd": " ".join(["oracle/_ref/fourcore_find_v4", "--jobs",
+                                     f"<hunt_v3 --lo {lo} --hi {hi} --classes {classes} --expand"
+                                     + (" as .bbj by s615_jobs_write" if fmt == "bbj" else "") + ">",
+                                     "--r", str(r)] + ([] if gate else ["--no-gate"])),
+                    "file_sha256": sha(path)}
+            d = DONE4.search(p.stdout)
+            if p.returncode != 0 or not d:
+                case["error"] = (p.stderr.strip().splitlines() or ["?"])[-3:]
+                ok = False
+            else:
+                case.update(solutions=int(d.group(1)), jobs=int(d.group(2)), failT=int(d.group(3)),
+                            modes=find_modes(p.stderr),
+                            solution_lines=[l for l in p.stdout.splitlines() if l.startswith("SOLUTION")],
+                            summary=d.group(0))
+            fx["find_jobs"].append(case)
             print(json.dumps(case)[:400])
 
     os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
