@@ -154,8 +154,8 @@ __global__ void k_max_count(const unsigned long long* __restrict__ W, u64 m, uns
 // (slice, block) gives every block its own output range per slice;
 // k_bin_scatter bins the updates through shared-memory cursors into those
 // ranges (slice-local cell offset and key index, 8 B), so the updates of a
-// slice lie together; k_bin_apply walks them in slice order, and its atomic
-// adds land on a slice that is resident in L2.
+// slice lie together; k_bin_apply walks them slice by slice with the whole
+// grid, and its atomic adds land on a slice that is resident in L2.
 constexpr u32 kMaxSlices = 4608;
 constexpr int kBinThreads = 256;
 
@@ -196,24 +196,18 @@ __global__ void k_bin_scatter(const u64* __restrict__ keys, u64 k0, u64 per, u64
   }
 }
 
-__global__ void k_bin_apply(const u32* __restrict__ ent_off, const u32* __restrict__ ent_idx, u64 E,
-                            u64 k0, const unsigned long long* __restrict__ soff, u32 sbits, u32 S,
+// A persistent grid walks the slices in order and splits each slice's
+// entries over all its threads, so the whole GPU works on one or two slices
+// (a few tens of MB) at a time and the atomic adds hit in L2.
+__global__ void k_bin_apply(const u32* __restrict__ ent_off, const u32* __restrict__ ent_idx, u64 k0,
+                            const unsigned long long* __restrict__ soff, u32 sbits, u32 S,
                             unsigned long long* W) {
-  extern __shared__ unsigned long long so[];   // S + 1 slice starts
-  for (u32 i = threadIdx.x; i <= S; i += blockDim.x) so[i] = soff[i];
-  __syncthreads();
-  u32 s = 0;
-  for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < E; i += (u64)gridDim.x * blockDim.x) {
-    if (i < so[s] || i >= so[s + 1]) {   // the slice of entry i: so[s] <= i < so[s + 1]
-      u32 a = 0, b = S;
-      while (b - a > 1) {
-        const u32 mid = (a + b) / 2;
-        if (so[mid] <= i) a = mid; else b = mid;
-      }
-      s = a;
-    }
-    const u64 c = ((u64)s << sbits) + ent_off[i];
-    atomicAdd(W + c, (unsigned long long)upd(k0 + ent_idx[i]));
+  const u64 nt = (u64)gridDim.x * blockDim.x, tid = blockIdx.x * (u64)blockDim.x + threadIdx.x;
+  for (u32 sl = 0; sl < S; ++sl) {
+    unsigned long long* base = W + ((u64)sl << sbits);
+    const u64 e1 = soff[sl + 1];
+    for (u64 i = soff[sl] + tid; i < e1; i += nt)
+      atomicAdd(base + ent_off[i], (unsigned long long)upd(k0 + ent_idx[i]));
   }
 }
 
@@ -427,8 +421,10 @@ int incidence_binned(s615_ctx* ctx, const u64* keys, u64 n, u64 seed, u64 m, u64
     // the slice starts go where the block bases were (read by the apply kernel)
     S615_CU(cudaMemcpyAsync(bbase, h_soff.data(), (S + 1) * sizeof(unsigned long long),
                             cudaMemcpyHostToDevice, st));
-    k_bin_apply<<<grid_for(ctx, run, 256), 256, (S + 1) * sizeof(unsigned long long), st>>>(
-        ent_off, ent_idx, run, k0, bbase, sbits, S, W);
+    int per_sm = 0;
+    S615_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bin_apply, 256, 0));
+    k_bin_apply<<<ctx->num_sms * std::max(per_sm, 1), 256, 0, st>>>(ent_off, ent_idx, k0, bbase,
+                                                                     sbits, S, W);
     ctx->launches++;
     S615_CU(cudaGetLastError());
     S615_CU(cudaStreamSynchronize(st));   // h_base / h_soff are reused by the next chunk
