@@ -17,6 +17,7 @@ import subprocess
 
 import pytest
 
+import orc
 import s615
 import workloads as W
 
@@ -48,7 +49,9 @@ def write_buc(path, units):
 
 
 CLS5 = [c for c in fixture()["cls5"] if "error" not in c]
-FIND = [c for c in fixture()["find"] if "error" not in c]
+FIND = [c for c in fixture()["find"] if "error" not in c and c["classes"] != "1"]
+FIND1 = [c for c in fixture()["find"] if "error" not in c and c["classes"] == "1"]
+FINDJ = [c for c in fixture().get("find_jobs", []) if "error" not in c]
 
 
 def cid(c):
@@ -114,3 +117,70 @@ def test_find_cli_prints_what_the_reference_printed(case, tmp_path, oracle_table
     assert got == want, p.stderr[-2000:]
     sols = [l for l in p.stdout.splitlines() if l.startswith("SOLUTION")]
     assert sorted(sols) == sorted(case["solution_lines"])
+
+
+def gate_sums(stderr):
+    got = [0, 0, 0]
+    for m in GATE.finditer(stderr):
+        for k in range(3):
+            got[k] += int(m.group(k + 1))
+    return got
+
+
+@pytest.mark.parametrize("case", FIND1, ids=lambda c: f"cls1-r{c['r']}{'' if c['gate'] else '-nogate'}")
+def test_find_cli_class1(case, tmp_path):
+    # class-1 units (find4).  The reference's k_find4 y tiles re-walk every
+    # c4 >= lo + 2048 (fourcore_find_v4.cu:490-497, 300) and the engine visits
+    # each c4 once, so the counters are set against the oracle's one-visit
+    # form (its reference-tile form equals the fixture: tests/test_oracle615.py);
+    # jobs, failT and SOLUTION lines against the fixture.  The table is built on
+    # the device; the counters do not depend on its bytes.
+    units = units_of(case["lo"], case["hi"], [1])
+    assert len(units) == case["units"]
+    buc = str(tmp_path / "u.buc")
+    write_buc(buc, units)
+    cmd = [BINF, "--units", buc, "--r", str(case["r"])]
+    if not case["gate"]:
+        cmd.append("--no-gate")
+    p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr
+    d = DONEF.search(p.stdout)
+    assert d and tuple(int(x) for x in d.groups()) == (case["solutions"], case["jobs"], case["failT"])
+    parts = [orc.expand_unit(B, u, c) for c, B, u in units]
+    jobs, n = orc.concat_jobs([q for q in parts if q[1]])
+    _, once = orc.run_jobs(orc.Table.build_pairs(2000, case["r"]), jobs, n, use_gate=case["gate"],
+                           ref_tiles=False)
+    assert gate_sums(p.stderr) == once
+    assert [l for l in p.stdout.splitlines() if l.startswith("SOLUTION")] == case["solution_lines"]
+
+
+DONEJ = re.compile(r"---- done: solutions=(\d+) jobs=(\d+) failT=(\d+)(?: \(bbj stream\))? ----")
+
+
+@pytest.mark.parametrize("case", FINDJ, ids=lambda c: f"{c['format']}-r{c['r']}{'' if c['gate'] else '-nogate'}")
+def test_find_cli_job_files(case, tmp_path, oracle_table):
+    # --jobs on the same job file the reference read (.but lines of the hunt
+    # tool, or their .bbj form written by s615_jobs_write) and the same table bytes
+    units = units_of(case["lo"], case["hi"], [int(x) for x in case["classes"].split(",")])
+    jobs, n, _ = s615.expand_units(units)
+    path = str(tmp_path / f"j.{case['format']}")
+    if case["format"] == "bbj":
+        s615.jobs_write(path, jobs, n)
+    else:
+        with open(path, "w") as f:
+            for i in range(n):
+                J = jobs[i]
+                f.write(f"{J.cls} {J.B} {J.u} {J.res_d} {J.res_e} {J.base[0]} {J.base[1]}\n")
+    N = max((B - 1) // 42 for _, B, _ in units)
+    _, tpath = oracle_table(N, case["r"])
+    cmd = [BINF, "--jobs", path, "--r", str(case["r"]), "--N", str(N), "--load-table", tpath]
+    if not case["gate"]:
+        cmd.append("--no-gate")
+    p = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr
+    d = DONEJ.search(p.stdout)
+    assert d and tuple(int(x) for x in d.groups()) == (case["solutions"], case["jobs"], case["failT"])
+    want = [sum(m[k] for m in case["modes"].values()) for k in ("calls", "gated", "probes")]
+    assert gate_sums(p.stderr) == want
+    assert sorted(l for l in p.stdout.splitlines() if l.startswith("SOLUTION")) == \
+        sorted(case["solution_lines"])

@@ -13,9 +13,11 @@ reference sources by oracle/Makefile `ref`; tests/golden/gen_ref615.py).  Here:
     (config-1 window at r = 16, 20, 48 with and without the gate, and B ~ 3.2M
     slices), the same unit count and the same SOLUTION lines
     (fourcore_cls5_gpu_v4.cu:353-410, 472-562);
-  * the oracle's restatement of run_batch gives fourcore_find_v4 --units'
-    summed find3 counters, job and failT counts and SOLUTION lines
-    (fourcore_find_v4.cu:460-562, 1128-1158).
+  * the oracle's restatement of run_batch gives fourcore_find_v4's summed
+    find3 (classes 2-4) and find4 (class 1) counters, job and failT counts and
+    SOLUTION lines, for Stage-1 units (--units) and for reduced-T job files
+    (--jobs: the hunt tool's .but, and the engine's .bbj of the same jobs,
+    whose bytes the reference read) (fourcore_find_v4.cu:460-562, 1094-1222).
 
 The tables are the oracle's builds of the same (N, r); their bytes must
 equal the reference builder's files (the fixture records their sha256).
@@ -142,9 +144,19 @@ def test_cls5_counters_equal_the_reference_binary(ref615):
         assert case["solutions"] == len(case["solution_lines"])
 
 
-def test_find3_counters_equal_the_reference_binary(ref615):
+def find_table(N, r):
+    """The table a find run probes: the reference builder's bytes for N up to
+    5,000; for larger N (class-1 windows) an N = 2,000 table, since the
+    counters do not depend on the table and no raw hit is compared there."""
+    return table(N, r) if N <= 5000 else table(2000, r)
+
+
+def test_find_units_counters_equal_the_reference_binary(ref615):
+    # classes 2-4 (find3) and class 1 (find4, the reference's repeated c4 tiles
+    # restated by ref_tiles: fourcore_find_v4.cu:490-497, 300)
     cases = ref615["find"]
-    assert len(cases) >= 3 and all("error" not in c for c in cases)
+    assert len(cases) >= 5 and all("error" not in c for c in cases)
+    assert any(c["classes"] == "1" for c in cases)
     for case in cases:
         cl = classes_of(case["classes"])
         units = [(c, B, u) for B in range(case["lo"], case["hi"] + 1) if math.gcd(B, 42) == 1
@@ -154,8 +166,39 @@ def test_find3_counters_equal_the_reference_binary(ref615):
         assert sum(p[2] for p in parts) == case["failT"]
         jobs, n = orc.concat_jobs([p for p in parts if p[1]])
         assert n == case["jobs"]
-        hits, ctr = orc.run_jobs(table(case["N"], case["r"]), jobs, n, use_gate=case["gate"])
+        hits, ctr = orc.run_jobs(find_table(case["N"], case["r"]), jobs, n, use_gate=case["gate"],
+                                 ref_tiles=True)
         want = [sum(m[k] for m in case["modes"].values()) for k in ("calls", "gated", "probes")]
         assert ctr == want, (case["summary"], ctr, want)
-        exact, lines = orc.verify_jobs(jobs, hits, case["N"])
+        if case["N"] <= 5000:
+            exact, lines = orc.verify_jobs(jobs, hits, case["N"])
+            assert sorted(l for l in lines if l.startswith("SOLUTION")) == sorted(case["solution_lines"])
+        else:
+            assert case["solution_lines"] == []
+
+
+def test_find_job_files_equal_the_reference_binary(ref615, tmp_path):
+    # --jobs on the hunt tool's .but file and on the same jobs written as .bbj by
+    # the engine (fourcore_find_v4.cu:1094-1126, 1160-1222; fourcore_job_bin.hpp)
+    cases = ref615["find_jobs"]
+    assert {c["format"] for c in cases} == {"but", "bbj"} and all("error" not in c for c in cases)
+    for case in cases:
+        cl = classes_of(case["classes"])
+        units = [(c, B, u) for B in range(case["lo"], case["hi"] + 1) if math.gcd(B, 42) == 1
+                 for c in cl for u in orc.unit_candidates(B, c)]
+        parts = [orc.expand_unit(B, u, c) for c, B, u in units]
+        jobs, n = orc.concat_jobs([p for p in parts if p[1]])
+        assert n == case["jobs"] and case["failT"] == 0
+        if case["format"] == "bbj":   # the engine writes the bytes the reference read
+            mine, m, _ = s615.expand_units([(c, B, u) for c, B, u in units])
+            path = str(tmp_path / "j.bbj")
+            s615.jobs_write(path, mine, m)
+            with open(path, "rb") as f:
+                assert hashlib.sha256(f.read()).hexdigest() == case["file_sha256"]
+        N = max((B - 1) // 42 for _, B, _ in units)
+        hits, ctr = orc.run_jobs(find_table(N, case["r"]), jobs, n, use_gate=case["gate"],
+                                 ref_tiles=True)
+        want = [sum(m[k] for m in case["modes"].values()) for k in ("calls", "gated", "probes")]
+        assert ctr == want, (case["summary"], ctr, want)
+        exact, lines = orc.verify_jobs(jobs, hits, N)
         assert sorted(l for l in lines if l.startswith("SOLUTION")) == sorted(case["solution_lines"])
