@@ -240,11 +240,25 @@ __device__ __forceinline__ void warp_append(bool take, u32 val, u32* list,
   }
 }
 
+// The claimed cells of the peel, in round order.  With idx and hash set
+// (HBM permitting: they reuse the incidence's entry buffers) the claim also
+// records each claimed key's index and hash, so the apply and the fill read
+// them in order instead of fetching the cell word and the key again.
+struct ClaimList {
+  u32* cell;
+  u32* idx;                    // null: read from the cell word
+  unsigned long long* hash;    // null: recomputed from the key array
+  __host__ __device__ ClaimList at(u64 off) const {
+    return ClaimList{cell + off, idx ? idx + off : nullptr, hash ? hash + off : nullptr};
+  }
+};
+
 // Does cell c (count 1) claim its key?  The key's lower count-1 cells win.
 __device__ __forceinline__ bool claims(const unsigned long long* W, const u64* keys, u64 seed,
-                                       u64 block, u64 recip, u64 c, u64 w) {
+                                       u64 block, u64 recip, u64 c, u64 w, u64& h) {
+  h = key_hash(keys, w & kSumMask, seed);
   u64 cs[3];
-  cell_indices(key_hash(keys, w & kSumMask, seed), block, recip, cs);
+  cell_indices(h, block, recip, cs);
 #pragma unroll
   for (int t = 0; t < 3; ++t)
     if (cs[t] < c && cnt_of(W[cs[t]]) == 1) return false;
@@ -254,29 +268,47 @@ __device__ __forceinline__ bool claims(const unsigned long long* W, const u64* k
 // Claims among cand[0, ncand), or among every cell when cand is null.
 __global__ void k_claim_list(const u32* __restrict__ cand, u64 ncand,
                              const unsigned long long* __restrict__ W, const u64* __restrict__ keys,
-                             u64 seed, u64 block, u64 recip, u32* order, unsigned long long* n_order,
-                             u64 order_cap, u32* over) {
+                             u64 seed, u64 block, u64 recip, ClaimList out,
+                             unsigned long long* n_order, u64 order_cap, u32* over) {
   for (u64 base = blockIdx.x * (u64)blockDim.x; base < ncand; base += (u64)gridDim.x * blockDim.x) {
     const u64 i = base + threadIdx.x;
     bool claim = false;
     u32 c = 0;
+    u64 w = 0, h = 0;
     if (i < ncand) {
       c = cand ? cand[i] : (u32)i;
-      const u64 w = W[c];
-      claim = cnt_of(w) == 1 && claims(W, keys, seed, block, recip, c, w);
+      w = W[c];
+      claim = cnt_of(w) == 1 && claims(W, keys, seed, block, recip, c, w, h);
     }
-    warp_append(claim, c, order, n_order, order_cap, over);
+    const u32 ballot = __ballot_sync(0xFFFFFFFFu, claim);
+    if (!ballot) continue;
+    const u32 lane = threadIdx.x & 31;
+    const int leader = __ffs(ballot) - 1;
+    unsigned long long pos = 0;
+    if ((int)lane == leader) pos = atomicAdd(n_order, (unsigned long long)__popc(ballot));
+    pos = __shfl_sync(0xFFFFFFFFu, pos, leader);
+    if (claim) {
+      const u64 k = pos + __popc(ballot & ((1u << lane) - 1u));
+      if (k < order_cap) {
+        out.cell[k] = c;
+        if (out.hash) {
+          out.idx[k] = (u32)(w & kSumMask);
+          out.hash[k] = h;
+        }
+      } else {
+        *over = 1;
+      }
+    }
   }
 }
 
-// Removes the key of claimed cell c from its two other cells; returns the
+// Removes the key of claimed entry i from its two other cells; returns the
 // cells whose count went from 2 to 1 (t0/t1 flags).
 __device__ __forceinline__ void remove_key(unsigned long long* W, const u64* keys, u64 seed,
-                                           u64 block, u64 recip, u64 c, bool& t0, u64& a0, bool& t1,
-                                           u64& a1) {
-  const u64 idx = W[c] & kSumMask;
+                                           u64 block, u64 recip, u64 c, u64 idx, u64 h, bool& t0,
+                                           u64& a0, bool& t1, u64& a1) {
   u64 cs[3];
-  cell_indices(key_hash(keys, idx, seed), block, recip, cs);
+  cell_indices(h, block, recip, cs);
   int k = 0;
 #pragma unroll
   for (int t = 0; t < 3; ++t) {
@@ -287,17 +319,29 @@ __device__ __forceinline__ void remove_key(unsigned long long* W, const u64* key
     else { t1 = to_one; a1 = cs[t]; }
     ++k;
   }
-  W[c] = idx;   // count 0; the index stays for the fill
 }
 
-__global__ void k_apply_list(const u32* __restrict__ claimed, u64 L, unsigned long long* W,
+__global__ void k_apply_list(ClaimList in, u64 L, unsigned long long* W,
                              const u64* __restrict__ keys, u64 seed, u64 block, u64 recip, u32* next,
                              unsigned long long* n_next, u64 next_cap, u32* over) {
   for (u64 base = blockIdx.x * (u64)blockDim.x; base < L; base += (u64)gridDim.x * blockDim.x) {
     const u64 i = base + threadIdx.x;
     bool t0 = false, t1 = false;
     u64 a0 = 0, a1 = 0;
-    if (i < L) remove_key(W, keys, seed, block, recip, claimed[i], t0, a0, t1, a1);
+    if (i < L) {
+      const u32 c = in.cell[i];
+      u64 idx, h;
+      if (in.hash) {
+        idx = in.idx[i];
+        h = in.hash[i];
+      } else {
+        idx = W[c] & kSumMask;
+        h = key_hash(keys, idx, seed);
+      }
+      remove_key(W, keys, seed, block, recip, c, idx, h, t0, a0, t1, a1);
+      // count 0; without the recorded index the word keeps it for the fill
+      W[c] = in.hash ? 0ull : idx;
+    }
     warp_append(t0, (u32)a0, next, n_next, next_cap, over);
     warp_append(t1, (u32)a1, next, n_next, next_cap, over);
   }
@@ -306,9 +350,8 @@ __global__ void k_apply_list(const u32* __restrict__ claimed, u64 L, unsigned lo
 // Reverse fill of claimed cell c: fingerprint of its key xor its two other
 // cells, which are final already (filled in a later round, or never claimed
 // and 0).
-__device__ __forceinline__ void fill_cell(unsigned long long* W, const u64* keys, u64 seed,
-                                          u64 block, u64 recip, u64 mask, u64 c) {
-  const u64 h = key_hash(keys, W[c], seed);
+__device__ __forceinline__ void fill_cell(unsigned long long* W, u64 h, u64 block, u64 recip,
+                                          u64 mask, u64 c) {
   u64 cs[3];
   cell_indices(h, block, recip, cs);
   u64 v = h & mask;
@@ -318,11 +361,14 @@ __device__ __forceinline__ void fill_cell(unsigned long long* W, const u64* keys
   W[c] = v & mask;
 }
 
-__global__ void k_fill_list(const u32* __restrict__ claimed, u64 L, unsigned long long* W,
+__global__ void k_fill_list(ClaimList in, u64 L, unsigned long long* W,
                             const u64* __restrict__ keys, u64 seed, u64 block, u64 recip, u64 mask) {
   for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < L;
-       i += (u64)gridDim.x * blockDim.x)
-    fill_cell(W, keys, seed, block, recip, mask, claimed[i]);
+       i += (u64)gridDim.x * blockDim.x) {
+    const u32 c = in.cell[i];
+    const u64 h = in.hash ? (u64)in.hash[i] : key_hash(keys, W[c], seed);
+    fill_cell(W, h, block, recip, mask, c);
+  }
 }
 
 // The scan form: claims of round r tagged in round[], apply and fill by tag.
@@ -335,7 +381,8 @@ __global__ void k_claim_scan(const unsigned long long* __restrict__ W, const u64
     bool claim = false;
     if (c < m) {
       const u64 w = W[c];
-      claim = cnt_of(w) == 1 && claims(W, keys, seed, block, recip, c, w);
+      u64 h;
+      claim = cnt_of(w) == 1 && claims(W, keys, seed, block, recip, c, w, h);
       if (claim) round[c] = r;
     }
     const u32 ballot = __ballot_sync(0xFFFFFFFFu, claim);
@@ -350,7 +397,9 @@ __global__ void k_apply_scan(unsigned long long* W, const u64* __restrict__ keys
     if (round[c] != r) continue;
     bool t0, t1;
     u64 a0, a1;
-    remove_key(W, keys, seed, block, recip, c, t0, a0, t1, a1);
+    const u64 idx = W[c] & kSumMask;
+    remove_key(W, keys, seed, block, recip, c, idx, key_hash(keys, idx, seed), t0, a0, t1, a1);
+    W[c] = idx;   // count 0; the index stays for the fill
   }
 }
 
@@ -359,7 +408,7 @@ __global__ void k_fill_scan(unsigned long long* W, const u64* __restrict__ keys,
                             u64 mask) {
   for (u64 c = blockIdx.x * (u64)blockDim.x + threadIdx.x; c < m;
        c += (u64)gridDim.x * blockDim.x)
-    if (round[c] == r) fill_cell(W, keys, seed, block, recip, mask, c);
+    if (round[c] == r) fill_cell(W, key_hash(keys, W[c], seed), block, recip, mask, c);
 }
 
 __global__ void k_narrow(const u64* __restrict__ in, u32* __restrict__ out, u64 m) {
@@ -567,11 +616,10 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
   // for m > 2^32 or without room for the lists, over full scans by round tag.
   const u64 fcap = std::max<u64>(4096, m / 8);
   bool lists = m <= (1ull << 32);
-  if (lists && (order.alloc(n * sizeof(u32)) || front.alloc(2 * fcap * sizeof(u32)))) {
-    order.release(); front.release();
+  if (lists && front.alloc(2 * fcap * sizeof(u32))) {
+    front.release();
     lists = false;
   }
-  if (!lists && (s = rounds.alloc(m * sizeof(u16)))) return s;
   if ((s = scratch.alloc(64))) return s;
   auto* W = static_cast<unsigned long long*>(cells.p);
   const u64* K = static_cast<const u64*>(keys.p);
@@ -607,6 +655,19 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
       ent_cap = 0;
     }
   }
+  // The claim list: in the entry buffers (idle after the incidence) with each
+  // key's index and hash when they hold 2n entries, else cells only.
+  ClaimList claim_list{nullptr, nullptr, nullptr};
+  if (lists && ent_cap >= 2 * n) {
+    claim_list = ClaimList{static_cast<u32*>(ent_off.p), static_cast<u32*>(ent_off.p) + n,
+                           static_cast<unsigned long long*>(ent_idx.p)};
+  } else if (lists && !order.alloc(n * sizeof(u32))) {
+    claim_list.cell = static_cast<u32*>(order.p);
+  } else if (lists) {
+    order.release(); front.release();
+    lists = false;
+  }
+  if (!lists && (s = rounds.alloc(m * sizeof(u16)))) return s;
   bool built = false;
   u64 used_seed = 0;
   int trace_rounds = 0;
@@ -637,7 +698,7 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
     trace.mark("incidence");
     const u64 mask = fp_mask((u32)r);
     if (lists) {
-      u32* ord = static_cast<u32*>(order.p);
+
       u32* fr[2] = {static_cast<u32*>(front.p), static_cast<u32*>(front.p) + fcap};
       std::vector<u64> off{0};
       u64 total = 0, ncand = m;
@@ -645,7 +706,8 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
       int cur = 0;
       while (off.size() <= 0xFFFE) {
         k_claim_list<<<grid_for(ctx, ncand, 256), 256, 0, st>>>(cand, ncand, W, K, seed, block,
-                                                                recip, ord, d_norder, n, d_lover);
+                                                                recip, claim_list, d_norder, n,
+                                                                d_lover);
         ctx->launches++;
         unsigned long long h_n[2] = {0, 0};
         u32 h_lover = 0;
@@ -655,7 +717,8 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
         if (L == 0) break;
         S615_CU(cudaMemsetAsync(d_nnext, 0, 8, st));
         S615_CU(cudaMemsetAsync(d_lover, 0, 4, st));
-        k_apply_list<<<grid_for(ctx, L, 256), 256, 0, st>>>(ord + total, L, W, K, seed, block, recip,
+        k_apply_list<<<grid_for(ctx, L, 256), 256, 0, st>>>(claim_list.at(total), L, W, K, seed,
+                                                            block, recip,
                                                             fr[cur ^ 1], d_nnext, fcap, d_lover);
         ctx->launches++;
         S615_CU(cudaGetLastError());
@@ -679,8 +742,8 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
       trace.mark("peel");
       for (size_t q = off.size() - 1; q >= 1; --q) {
         const u64 L = off[q] - off[q - 1];
-        k_fill_list<<<grid_for(ctx, L, 256), 256, 0, st>>>(ord + off[q - 1], L, W, K, seed, block,
-                                                           recip, mask);
+        k_fill_list<<<grid_for(ctx, L, 256), 256, 0, st>>>(claim_list.at(off[q - 1]), L, W, K,
+                                                           seed, block, recip, mask);
         ctx->launches++;
       }
       trace_rounds = (int)off.size() - 1;
