@@ -23,6 +23,7 @@
 //     they are final already and a round needs no ordering inside it.
 // Cells then hold exactly the reference's cell relation (FN = 0, same FPR);
 // which key owns which cell differs from the FIFO order, so bytes differ.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,6 +38,8 @@
 namespace s615 {
 
 namespace {
+
+namespace cg = cooperative_groups;
 
 constexpr u64 kEmpty = ~0ULL;
 
@@ -196,18 +199,22 @@ __global__ void k_bin_scatter(const u64* __restrict__ keys, u64 k0, u64 per, u64
   }
 }
 
-// A persistent grid walks the slices in order and splits each slice's
-// entries over all its threads, so the whole GPU works on one or two slices
-// (a few tens of MB) at a time and the atomic adds hit in L2.
+// A cooperative grid walks the slices in order and splits each slice's
+// entries over all its threads, with a grid-wide sync after every slice, so
+// the whole GPU works on one slice (16 MB) at a time and its atomic adds hit
+// in L2.  (Without the syncs, blocks drift apart over the walk and the slices
+// in use outgrow L2.)
 __global__ void k_bin_apply(const u32* __restrict__ ent_off, const u32* __restrict__ ent_idx, u64 k0,
                             const unsigned long long* __restrict__ soff, u32 sbits, u32 S,
                             unsigned long long* W) {
+  cg::grid_group grid = cg::this_grid();
   const u64 nt = (u64)gridDim.x * blockDim.x, tid = blockIdx.x * (u64)blockDim.x + threadIdx.x;
   for (u32 sl = 0; sl < S; ++sl) {
     unsigned long long* base = W + ((u64)sl << sbits);
     const u64 e1 = soff[sl + 1];
     for (u64 i = soff[sl] + tid; i < e1; i += nt)
       atomicAdd(base + ent_off[i], (unsigned long long)upd(k0 + ent_idx[i]));
+    grid.sync();
   }
 }
 
@@ -472,8 +479,17 @@ int incidence_binned(s615_ctx* ctx, const u64* keys, u64 n, u64 seed, u64 m, u64
                             cudaMemcpyHostToDevice, st));
     int per_sm = 0;
     S615_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bin_apply, 256, 0));
-    k_bin_apply<<<ctx->num_sms * std::max(per_sm, 1), 256, 0, st>>>(ent_off, ent_idx, k0, bbase,
-                                                                     sbits, S, W);
+    {   // cooperative: every block resident at once (the launch fails otherwise)
+      const u32* a_off = ent_off;
+      const u32* a_idx = ent_idx;
+      const unsigned long long* a_soff = bbase;
+      u64 a_k0 = k0;
+      u32 a_sbits = sbits, a_S = S;
+      void* args[] = {(void*)&a_off, (void*)&a_idx, (void*)&a_k0, (void*)&a_soff, (void*)&a_sbits,
+                      (void*)&a_S, (void*)&W};
+      S615_CU(cudaLaunchCooperativeKernel((const void*)k_bin_apply, dim3(ctx->num_sms * std::max(per_sm, 1)),
+                                          dim3(256), args, 0, st));
+    }
     ctx->launches++;
     S615_CU(cudaGetLastError());
     S615_CU(cudaStreamSynchronize(st));   // h_base / h_soff are reused by the next chunk
