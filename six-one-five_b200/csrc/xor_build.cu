@@ -796,8 +796,12 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
     used_seed = seed;
   }
   if (!built) return S615_E_BUILD;
+  S615_CU(cudaStreamSynchronize(st));
+  trace.mark("sync");
   keys.release(); rounds.release(); order.release(); front.release();
+  trace.mark("free_keys");
   ent_off.release(); ent_idx.release(); bins.release();
+  trace.mark("free_bins");
 
   out->hdr.n_keys = n;
   out->hdr.m_cells = m;
