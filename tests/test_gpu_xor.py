@@ -130,3 +130,27 @@ def test_build_keys_matches_oracle_seed_outcome(engine, keys_n):
     assert (h.n_keys, h.m_cells, h.mix_seed) == (oh.n_keys, oh.m_cells, oh.mix_seed)
     assert engine.query(tid, keys).all()
     engine.free_table(tid)
+
+
+def test_device_build_past_u32_cells(engine):
+    # N = 84,000 gives m > 2^32 cells: the peel scans every cell each round
+    # (the candidate lists need u32 cell indices).  No false negative on a
+    # sample of pair keys, and the false-positive rate at r = 20 within four
+    # binomial standard deviations.
+    N, r = 84000, 20
+    tid = engine.build_table(N, r)
+    try:
+        h = engine.table_info(tid).hdr
+        assert h.m_cells > 2**32
+        rng = np.random.RandomState(84)
+        i = rng.randint(1, N + 1, size=2_000_000).astype(np.uint64)
+        j = rng.randint(1, N + 1, size=2_000_000).astype(np.uint64)
+        p6 = lambda x: x * x * x * x * x * x   # mod 2^64 in uint64 arithmetic
+        keys = p6(i) + p6(j)
+        assert engine.query(tid, keys).all()
+        n = 50_000_000
+        fp = int(engine.query(tid, orc.mt64(0xF15EED + h.n_keys, n)).sum())
+        mu, sd = n * 2.0**-r, (n * 2.0**-r * (1 - 2.0**-r)) ** 0.5
+        assert abs(fp - mu) <= 4 * sd, (fp, mu, sd)
+    finally:
+        engine.free_table(tid)
