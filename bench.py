@@ -581,8 +581,8 @@ def run617(args, rank, world, local, dist):
             "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs (burst)",
             "traffic": None, "algorithmic_bytes_per_launch": ctr.probes * PROBE_BYTES}
     if rank == 0:
-        roof["random_access"] = random_access_roof(ctr.probes, statistics.mean(per_ms) / 1e3,
-                                                   eng.table_info(tid).device_bytes)
+        roof["random_access"] = random_access_roof(lib, eng, tid, stream, ctr.probes,
+                                                   statistics.mean(per_ms) / 1e3)
 
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and world == 1:
@@ -842,8 +842,7 @@ def run_mix(args, rank, world, local, dist):
     mix_roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs (burst)",
                 "traffic": None, "algorithmic_bytes_per_launch": ctr.probes * PROBE_BYTES,
-                "random_access": random_access_roof(ctr.probes, per_s,
-                                                    eng.table_info(tid).device_bytes)
+                "random_access": random_access_roof(lib, eng, tid, stream, ctr.probes, per_s)
                 if rank == 0 else None}
     line = {"metric": METRIC_MIX, "value": n / step_s, "unit": "units/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -1049,8 +1048,8 @@ def run_jobs(args, rank, world, local, dist):
                          "frac": round(achieved / peak, 4), "peak_kind": f"{peak_kind} hbm_gbs (burst)",
                          "traffic": None, "algorithmic_bytes_per_launch": ctr.probes * PROBE_BYTES,
                          "random_access": (random_access_roof(
-                             ctr.probes, statistics.mean(per_ms) / 1e3,
-                             eng.table_info(tid).device_bytes) if rank == 0 else None)},
+                             lib, eng, tid, stream, ctr.probes, statistics.mean(per_ms) / 1e3)
+                             if rank == 0 else None)},
             "cpu_baseline": cpu, "sharp_gate": sharp, "clocks": cl}
     eng.close()
     if rank == 0:

@@ -647,16 +647,26 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
   const int g = grid_for(ctx, m, 256);
   // Entry buffers of the binned incidence: all 3n updates when HBM allows,
   // else chunks of keys; with no room for a useful chunk the incidence adds
-  // directly into the cell words (k_incidence).
+  // directly into the cell words (k_incidence).  The peel's own buffers come
+  // first: the round tags of the scan form, or (when the entry buffers will
+  // not hold 2n entries for the recorded claim list) the claimed-cell list.
+  auto avail_now = [&]() -> size_t {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { cudaGetLastError(); return 0; }
+    size_t a = std::min(free_b, ctx->budget > ctx->used ? ctx->budget - ctx->used : (size_t)0);
+    const size_t margin = (size_t)2 << 30;
+    return a > margin ? a - margin : 0;
+  };
+  const size_t bin_bytes = (size_t)ctx->num_sms * 2 * kMaxSlices * (4 + 8) + 64;
+  if (lists && avail_now() < bin_bytes + 16 * n && order.alloc(n * sizeof(u32))) {
+    order.release(); front.release();
+    lists = false;
+  }
+  if (!lists && (s = rounds.alloc(m * sizeof(u16)))) return s;
   Buf ent_off(ctx), ent_idx(ctx), bins(ctx);
   u64 ent_cap = 0;
   {
-    size_t free_b = 0, total_b = 0;
-    S615_CU(cudaMemGetInfo(&free_b, &total_b));
-    size_t avail = std::min(free_b, ctx->budget > ctx->used ? ctx->budget - ctx->used : (size_t)0);
-    const size_t margin = (size_t)2 << 30;
-    avail = avail > margin ? avail - margin : 0;
-    const size_t bin_bytes = (size_t)ctx->num_sms * 2 * kMaxSlices * (4 + 8) + 64;
+    const size_t avail = avail_now();
     if (avail > bin_bytes) {
       ent_cap = std::min<u64>(3 * n, (avail - bin_bytes) / 8);
       ent_cap = ent_cap / 3 * 3;
@@ -677,13 +687,16 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
   if (lists && ent_cap >= 2 * n) {
     claim_list = ClaimList{static_cast<u32*>(ent_off.p), static_cast<u32*>(ent_off.p) + n,
                            static_cast<unsigned long long*>(ent_idx.p)};
-  } else if (lists && !order.alloc(n * sizeof(u32))) {
+    order.release();   // not needed (it is only taken when HBM was short)
+  } else if (lists && (order.p || !order.alloc(n * sizeof(u32)))) {
     claim_list.cell = static_cast<u32*>(order.p);
-  } else if (lists) {
+  } else if (lists) {   // no room for any list: scan, with round tags in the entry buffers' place
     order.release(); front.release();
+    ent_off.release(); ent_idx.release(); bins.release();
+    ent_cap = 0;
     lists = false;
+    if ((s = rounds.alloc(m * sizeof(u16)))) return s;
   }
-  if (!lists && (s = rounds.alloc(m * sizeof(u16)))) return s;
   bool built = false;
   u64 used_seed = 0;
   int trace_rounds = 0;
