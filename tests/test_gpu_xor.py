@@ -154,3 +154,22 @@ def test_device_build_past_u32_cells(engine):
         assert abs(fp - mu) <= 4 * sd, (fp, mu, sd)
     finally:
         engine.free_table(tid)
+
+
+def test_device_build_same_bytes_under_a_tight_budget(engine):
+    # The builder picks its form by the HBM it may use: by default the binned
+    # incidence and the peel lists with each claimed key's index and hash; with
+    # a 400 MB budget the incidence adds straight into the cell words and the
+    # peel keeps only the claimed cells.  The rounds are the same, so the cells
+    # are too, byte for byte.
+    N, r = 3000, 20
+    tid = engine.build_table(N, r)
+    try:
+        h0, p0 = engine.export_table(tid)
+    finally:
+        engine.free_table(tid)
+    with s615.Engine(0, hbm_budget=400 << 20) as tight:
+        t2 = tight.build_table(N, r)
+        h1, p1 = tight.export_table(t2)
+    assert bytes(h0) == bytes(h1)
+    np.testing.assert_array_equal(p0, p1)
