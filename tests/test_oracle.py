@@ -138,3 +138,16 @@ def test_oracle_counters_small_unit():
     nd = sum(len(range(U.res[U.nres1 + i], U.fmax2 + 1, 64)) for i in range(U.nres2))
     assert calls == ne * nd
     assert probes + gated <= calls
+
+
+def test_residue_and_mt64_helpers():
+    # the FPR tests' helpers: std::mt19937_64's 10,000th draw from the default
+    # seed is the C++ standard's check value, and a table's residue
+    # (cell ^ cell ^ cell ^ fingerprint) is zero exactly where the query says "maybe"
+    assert int(orc.mt64(5489, 10000)[-1]) == 9981545732273789042
+    t = orc.Table.build_pairs(300, 8)
+    keys = np.concatenate([orc.mt64(7, 200_000), np.array([pow(3, 6, 2**64) + pow(5, 6, 2**64)],
+                                                           dtype=np.uint64)])
+    res = t.residue(keys)
+    np.testing.assert_array_equal((res == 0).astype(np.uint8), t.query(keys))
+    assert res[-1] == 0 and 0 < int((res == 0).sum()) < 200_000 // 64
