@@ -204,17 +204,20 @@ __global__ void k_bin_scatter(const u64* __restrict__ keys, u64 k0, u64 per, u64
 // the whole GPU works on one slice (16 MB) at a time and its atomic adds hit
 // in L2.  (Without the syncs, blocks drift apart over the walk and the slices
 // in use outgrow L2.)
+// kSync = false is the same walk without the syncs, for a device or setting
+// where a cooperative launch is refused (the result is the same; only the L2
+// hit rate suffers).
+template <bool kSync>
 __global__ void k_bin_apply(const u32* __restrict__ ent_off, const u32* __restrict__ ent_idx, u64 k0,
                             const unsigned long long* __restrict__ soff, u32 sbits, u32 S,
                             unsigned long long* W) {
-  cg::grid_group grid = cg::this_grid();
   const u64 nt = (u64)gridDim.x * blockDim.x, tid = blockIdx.x * (u64)blockDim.x + threadIdx.x;
   for (u32 sl = 0; sl < S; ++sl) {
     unsigned long long* base = W + ((u64)sl << sbits);
     const u64 e1 = soff[sl + 1];
     for (u64 i = soff[sl] + tid; i < e1; i += nt)
       atomicAdd(base + ent_off[i], (unsigned long long)upd(k0 + ent_idx[i]));
-    grid.sync();
+    if constexpr (kSync) cg::this_grid().sync();
   }
 }
 
@@ -478,8 +481,9 @@ int incidence_binned(s615_ctx* ctx, const u64* keys, u64 n, u64 seed, u64 m, u64
     S615_CU(cudaMemcpyAsync(bbase, h_soff.data(), (S + 1) * sizeof(unsigned long long),
                             cudaMemcpyHostToDevice, st));
     int per_sm = 0;
-    S615_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bin_apply, 256, 0));
-    {   // cooperative: every block resident at once (the launch fails otherwise)
+    S615_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bin_apply<true>, 256, 0));
+    const dim3 grid(ctx->num_sms * std::max(per_sm, 1));
+    {   // cooperative: every block resident at once (the launch is refused otherwise)
       const u32* a_off = ent_off;
       const u32* a_idx = ent_idx;
       const unsigned long long* a_soff = bbase;
@@ -487,8 +491,11 @@ int incidence_binned(s615_ctx* ctx, const u64* keys, u64 n, u64 seed, u64 m, u64
       u32 a_sbits = sbits, a_S = S;
       void* args[] = {(void*)&a_off, (void*)&a_idx, (void*)&a_k0, (void*)&a_soff, (void*)&a_sbits,
                       (void*)&a_S, (void*)&W};
-      S615_CU(cudaLaunchCooperativeKernel((const void*)k_bin_apply, dim3(ctx->num_sms * std::max(per_sm, 1)),
-                                          dim3(256), args, 0, st));
+      if (cudaLaunchCooperativeKernel((const void*)k_bin_apply<true>, grid, dim3(256), args, 0, st) !=
+          cudaSuccess) {
+        cudaGetLastError();
+        k_bin_apply<false><<<grid, 256, 0, st>>>(ent_off, ent_idx, k0, bbase, sbits, S, W);
+      }
     }
     ctx->launches++;
     S615_CU(cudaGetLastError());
