@@ -1169,8 +1169,10 @@ def main():
         if args.impl == "reference":
             if rank == 0:
                 print(json.dumps({"impl": "reference", "metric": METRIC_JOBS, "unavailable":
-                                  "fourcore_find_v4 (the reference's job runner) includes <gmpxx.h>, "
-                                  "which is not installed; the line's cpu_baseline is the oracle port"}),
+                                  "the reference's job runner (fourcore_find_v4) builds its N=95,239 "
+                                  "table on the host before searching (hours, ~100 GB); its counters on "
+                                  "job files are pinned on small windows by tests/golden/ref615.json, "
+                                  "and the line's cpu_baseline is the oracle port"}),
                       flush=True)
             return 0
         return run_jobs(args, rank, world, local, dist)
