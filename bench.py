@@ -69,6 +69,7 @@ def parse():
                     choices=["cls5", "cls617", "mix", "serve", "jobs", "cfg1"])
     ap.add_argument("--units", type=int, default=0, help="mix: units per step (default 200,000)")
     ap.add_argument("--seconds", type=float, default=10.0, help="serve: seconds of arrivals")
+    ap.add_argument("--slots", type=int, default=2, help="serve: batches in flight")
     ap.add_argument("--reference-gpu", type=int, default=15536,
                     help="cls5: run the reference's fourcore_cls5_gpu_v4 on K evenly spaced band "
                          "units (default: a tenth of the band; 0: the whole band; -1: skip)")
@@ -1097,7 +1098,7 @@ def run_serve(args, rank, world, local, dist):
     rate, req_units, secs = 5000.0, 50, args.seconds
     plants_left = 256
     planted = {}          # (ticket, index) -> expected solution key
-    eng.serve_start(slots=2)
+    eng.serve_start(slots=args.slots)
     lat, sent, done, got_plants = [], 0, 0, 0
     t_start = time.perf_counter()
     nxt = t_start
