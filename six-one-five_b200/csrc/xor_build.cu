@@ -229,25 +229,41 @@ __global__ void k_bin_apply(const u32* __restrict__ ent_off, const u32* __restri
 // keys (a count-1 cell of round r-1 either claimed its key or lost it to a
 // lower cell of the same key), so after a full scan in round 1 each round
 // visits only the cells whose count went from 2 to 1 in the round before.
-// Claimed cells are appended in round order (u32 cell indices, m <= 2^32),
-// and the fill walks that list backwards.  For m > 2^32, or without room for
-// the lists, every round scans all cells and tags its claims with the round.
+// Claimed cells are appended in round order (as offsets within their third
+// of the table), and the fill walks that list backwards.  Without room for
+// the lists every round scans all cells and tags its claims with the round.
 
-// Append the flagged lanes' values (every lane of the warp calls this).
-__device__ __forceinline__ void warp_append(bool take, u32 val, u32* list,
-                                            unsigned long long* count, u64 cap, u32* over) {
+// A list of cells, each entry a u32 offset within its third of the table and
+// the third (0, 1, 2) in a byte: a cell index needs more than 32 bits once m
+// passes 2^32, an offset within a third does not (block < 2^32 for every
+// single table).
+struct CellList {
+  u32* off;
+  u8* third;
+  __host__ __device__ CellList at(u64 k) const { return CellList{off + k, third + k}; }
+  __device__ __forceinline__ u64 cell(u64 k, u64 block) const { return third[k] * block + off[k]; }
+};
+
+// Append the flagged lanes' cells (every lane of the warp calls this).
+__device__ __forceinline__ u64 warp_append(bool take, u64 c, u64 block, CellList list,
+                                           unsigned long long* count, u64 cap, u32* over) {
   const u32 ballot = __ballot_sync(0xFFFFFFFFu, take);
-  if (!ballot) return;
+  if (!ballot) return ~0ull;
   const u32 lane = threadIdx.x & 31;
   const int leader = __ffs(ballot) - 1;
   unsigned long long base = 0;
   if ((int)lane == leader) base = atomicAdd(count, (unsigned long long)__popc(ballot));
   base = __shfl_sync(0xFFFFFFFFu, base, leader);
-  if (take) {
-    const u64 k = base + __popc(ballot & ((1u << lane) - 1u));
-    if (k < cap) list[k] = val;
-    else *over = 1;
+  if (!take) return ~0ull;
+  const u64 k = base + __popc(ballot & ((1u << lane) - 1u));
+  if (k >= cap) {
+    *over = 1;
+    return ~0ull;
   }
+  const u32 t = c >= 2 * block ? 2u : c >= block ? 1u : 0u;
+  list.off[k] = (u32)(c - t * block);
+  list.third[k] = (u8)t;
+  return k;
 }
 
 // The claimed cells of the peel, in round order.  With idx and hash set
@@ -255,11 +271,11 @@ __device__ __forceinline__ void warp_append(bool take, u32 val, u32* list,
 // records each claimed key's index and hash, so the apply and the fill read
 // them in order instead of fetching the cell word and the key again.
 struct ClaimList {
-  u32* cell;
+  CellList cells;
   u32* idx;                    // null: read from the cell word
   unsigned long long* hash;    // null: recomputed from the key array
-  __host__ __device__ ClaimList at(u64 off) const {
-    return ClaimList{cell + off, idx ? idx + off : nullptr, hash ? hash + off : nullptr};
+  __host__ __device__ ClaimList at(u64 k) const {
+    return ClaimList{cells.at(k), idx ? idx + k : nullptr, hash ? hash + k : nullptr};
   }
 };
 
@@ -275,71 +291,37 @@ __device__ __forceinline__ bool claims(const unsigned long long* W, const u64* k
   return true;
 }
 
-// Claims among cand[0, ncand), or among every cell when cand is null.
-__global__ void k_claim_list(const u32* __restrict__ cand, u64 ncand,
-                             const unsigned long long* __restrict__ W, const u64* __restrict__ keys,
-                             u64 seed, u64 block, u64 recip, ClaimList out,
-                             unsigned long long* n_order, u64 order_cap, u32* over) {
+// Claims among the candidate cells [0, ncand), or among every cell when the
+// candidate list is null.
+__global__ void k_claim_list(CellList cand, u64 ncand, const unsigned long long* __restrict__ W,
+                             const u64* __restrict__ keys, u64 seed, u64 block, u64 recip,
+                             ClaimList out, unsigned long long* n_order, u64 order_cap, u32* over) {
   for (u64 base = blockIdx.x * (u64)blockDim.x; base < ncand; base += (u64)gridDim.x * blockDim.x) {
     const u64 i = base + threadIdx.x;
     bool claim = false;
-    u32 c = 0;
-    u64 w = 0, h = 0;
+    u64 c = 0, w = 0, h = 0;
     if (i < ncand) {
-      c = cand ? cand[i] : (u32)i;
+      c = cand.off ? cand.cell(i, block) : i;
       w = W[c];
       claim = cnt_of(w) == 1 && claims(W, keys, seed, block, recip, c, w, h);
     }
-    const u32 ballot = __ballot_sync(0xFFFFFFFFu, claim);
-    if (!ballot) continue;
-    const u32 lane = threadIdx.x & 31;
-    const int leader = __ffs(ballot) - 1;
-    unsigned long long pos = 0;
-    if ((int)lane == leader) pos = atomicAdd(n_order, (unsigned long long)__popc(ballot));
-    pos = __shfl_sync(0xFFFFFFFFu, pos, leader);
-    if (claim) {
-      const u64 k = pos + __popc(ballot & ((1u << lane) - 1u));
-      if (k < order_cap) {
-        out.cell[k] = c;
-        if (out.hash) {
-          out.idx[k] = (u32)(w & kSumMask);
-          out.hash[k] = h;
-        }
-      } else {
-        *over = 1;
-      }
+    const u64 k = warp_append(claim, c, block, out.cells, n_order, order_cap, over);
+    if (k != ~0ull && out.hash) {
+      out.idx[k] = (u32)(w & kSumMask);
+      out.hash[k] = h;
     }
-  }
-}
-
-// Removes the key of claimed entry i from its two other cells; returns the
-// cells whose count went from 2 to 1 (t0/t1 flags).
-__device__ __forceinline__ void remove_key(unsigned long long* W, const u64* keys, u64 seed,
-                                           u64 block, u64 recip, u64 c, u64 idx, u64 h, bool& t0,
-                                           u64& a0, bool& t1, u64& a1) {
-  u64 cs[3];
-  cell_indices(h, block, recip, cs);
-  int k = 0;
-#pragma unroll
-  for (int t = 0; t < 3; ++t) {
-    if (cs[t] == c) continue;
-    const u64 old = atomicAdd(W + cs[t], (unsigned long long)(0 - upd(idx)));
-    const bool to_one = cnt_of(old) == 2;
-    if (k == 0) { t0 = to_one; a0 = cs[t]; }
-    else { t1 = to_one; a1 = cs[t]; }
-    ++k;
   }
 }
 
 __global__ void k_apply_list(ClaimList in, u64 L, unsigned long long* W,
-                             const u64* __restrict__ keys, u64 seed, u64 block, u64 recip, u32* next,
-                             unsigned long long* n_next, u64 next_cap, u32* over) {
+                             const u64* __restrict__ keys, u64 seed, u64 block, u64 recip,
+                             CellList next, unsigned long long* n_next, u64 next_cap, u32* over) {
   for (u64 base = blockIdx.x * (u64)blockDim.x; base < L; base += (u64)gridDim.x * blockDim.x) {
     const u64 i = base + threadIdx.x;
-    bool t0 = false, t1 = false;
-    u64 a0 = 0, a1 = 0;
+    bool to0 = false, to1 = false;
+    u64 nc0 = 0, nc1 = 0;
     if (i < L) {
-      const u32 c = in.cell[i];
+      const u64 c = in.cells.cell(i, block);
       u64 idx, h;
       if (in.hash) {
         idx = in.idx[i];
@@ -348,12 +330,20 @@ __global__ void k_apply_list(ClaimList in, u64 L, unsigned long long* W,
         idx = W[c] & kSumMask;
         h = key_hash(keys, idx, seed);
       }
-      remove_key(W, keys, seed, block, recip, c, idx, h, t0, a0, t1, a1);
+      // remove the key from its two other cells; a cell whose count goes from
+      // 2 to 1 is a candidate of the next round
+      u64 cs[3];
+      cell_indices(h, block, recip, cs);
+      const int own = cs[0] == c ? 0 : cs[1] == c ? 1 : 2;
+      nc0 = cs[own == 0 ? 1 : 0];
+      nc1 = cs[own == 2 ? 1 : 2];
+      to0 = cnt_of(atomicAdd(W + nc0, (unsigned long long)(0 - upd(idx)))) == 2;
+      to1 = cnt_of(atomicAdd(W + nc1, (unsigned long long)(0 - upd(idx)))) == 2;
       // count 0; without the recorded index the word keeps it for the fill
       W[c] = in.hash ? 0ull : idx;
     }
-    warp_append(t0, (u32)a0, next, n_next, next_cap, over);
-    warp_append(t1, (u32)a1, next, n_next, next_cap, over);
+    warp_append(to0, nc0, block, next, n_next, next_cap, over);
+    warp_append(to1, nc1, block, next, n_next, next_cap, over);
   }
 }
 
@@ -375,10 +365,22 @@ __global__ void k_fill_list(ClaimList in, u64 L, unsigned long long* W,
                             const u64* __restrict__ keys, u64 seed, u64 block, u64 recip, u64 mask) {
   for (u64 i = blockIdx.x * (u64)blockDim.x + threadIdx.x; i < L;
        i += (u64)gridDim.x * blockDim.x) {
-    const u32 c = in.cell[i];
+    const u64 c = in.cells.cell(i, block);
     const u64 h = in.hash ? (u64)in.hash[i] : key_hash(keys, W[c], seed);
     fill_cell(W, h, block, recip, mask, c);
   }
+}
+
+// remove_key for the scan form (index and hash from the cell word and keys).
+__device__ __forceinline__ void remove_key_scan(unsigned long long* W, const u64* keys, u64 seed,
+                                                u64 block, u64 recip, u64 c) {
+  const u64 idx = W[c] & kSumMask;
+  u64 cs[3];
+  cell_indices(key_hash(keys, idx, seed), block, recip, cs);
+#pragma unroll
+  for (int t = 0; t < 3; ++t)
+    if (cs[t] != c) atomicAdd(W + cs[t], (unsigned long long)(0 - upd(idx)));
+  W[c] = idx;   // count 0; the index stays for the fill
 }
 
 // The scan form: claims of round r tagged in round[], apply and fill by tag.
@@ -404,12 +406,7 @@ __global__ void k_apply_scan(unsigned long long* W, const u64* __restrict__ keys
                              const u16* __restrict__ round, u64 m, u64 block, u64 recip, u16 r) {
   for (u64 c = blockIdx.x * (u64)blockDim.x + threadIdx.x; c < m;
        c += (u64)gridDim.x * blockDim.x) {
-    if (round[c] != r) continue;
-    bool t0, t1;
-    u64 a0, a1;
-    const u64 idx = W[c] & kSumMask;
-    remove_key(W, keys, seed, block, recip, c, idx, key_hash(keys, idx, seed), t0, a0, t1, a1);
-    W[c] = idx;   // count 0; the index stays for the fill
+    if (round[c] == r) remove_key_scan(W, keys, seed, block, recip, c);
   }
 }
 
@@ -636,10 +633,11 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
   if (s) return s;
   // Peel over lists (claimed cells in round order, two candidate lists of
   // m/8 cells each; a round whose candidates overflow scans every cell), or,
-  // for m > 2^32 or without room for the lists, over full scans by round tag.
+  // without room for the lists, over full scans by round tag.
+  // Candidate lists: two of m/8 entries (5 bytes each: offset + third).
   const u64 fcap = std::max<u64>(4096, m / 8);
-  bool lists = m <= (1ull << 32);
-  if (lists && front.alloc(2 * fcap * sizeof(u32))) {
+  bool lists = block < (1ull << 32);
+  if (lists && front.alloc(2 * fcap * 5)) {
     front.release();
     lists = false;
   }
@@ -665,7 +663,11 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
     return a > margin ? a - margin : 0;
   };
   const size_t bin_bytes = (size_t)ctx->num_sms * 2 * kMaxSlices * (4 + 8) + 64;
-  if (lists && avail_now() < bin_bytes + 16 * n && order.alloc(n * sizeof(u32))) {
+  // the recorded claim list needs 17 bytes per key in the entry buffers
+  // (offset, third, u32 index, hash) and n < 2^32; otherwise the claimed
+  // cells alone (5 bytes per key) are taken now, before the entry buffers
+  const bool rich_possible = n < (1ull << 32);
+  if (lists && (!rich_possible || avail_now() < bin_bytes + 24 * n) && order.alloc(n * 5)) {
     order.release(); front.release();
     lists = false;
   }
@@ -690,13 +692,15 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
   }
   // The claim list: in the entry buffers (idle after the incidence) with each
   // key's index and hash when they hold 2n entries, else cells only.
-  ClaimList claim_list{nullptr, nullptr, nullptr};
-  if (lists && ent_cap >= 2 * n) {
-    claim_list = ClaimList{static_cast<u32*>(ent_off.p), static_cast<u32*>(ent_off.p) + n,
+  // ent_off holds offsets, indices and thirds (9n bytes), ent_idx the hashes (8n)
+  ClaimList claim_list{{nullptr, nullptr}, nullptr, nullptr};
+  if (lists && rich_possible && ent_cap * 4 >= 9 * n && !order.p) {
+    u32* o = static_cast<u32*>(ent_off.p);
+    claim_list = ClaimList{{o, reinterpret_cast<u8*>(o + 2 * n)}, o + n,
                            static_cast<unsigned long long*>(ent_idx.p)};
-    order.release();   // not needed (it is only taken when HBM was short)
-  } else if (lists && (order.p || !order.alloc(n * sizeof(u32)))) {
-    claim_list.cell = static_cast<u32*>(order.p);
+  } else if (lists && (order.p || !order.alloc(n * 5))) {
+    u32* o = static_cast<u32*>(order.p);
+    claim_list.cells = CellList{o, reinterpret_cast<u8*>(o + n)};
   } else if (lists) {   // no room for any list: scan, with round tags in the entry buffers' place
     order.release(); front.release();
     ent_off.release(); ent_idx.release(); bins.release();
@@ -735,10 +739,12 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
     const u64 mask = fp_mask((u32)r);
     if (lists) {
 
-      u32* fr[2] = {static_cast<u32*>(front.p), static_cast<u32*>(front.p) + fcap};
+      u32* fo = static_cast<u32*>(front.p);
+      u8* ft = reinterpret_cast<u8*>(fo + 2 * fcap);
+      const CellList fr[2] = {CellList{fo, ft}, CellList{fo + fcap, ft + fcap}};
       std::vector<u64> off{0};
       u64 total = 0, ncand = m;
-      const u32* cand = nullptr;   // round 1 scans every cell
+      CellList cand{nullptr, nullptr};   // round 1 scans every cell
       int cur = 0;
       while (off.size() <= 0xFFFE) {
         k_claim_list<<<grid_for(ctx, ncand, 256), 256, 0, st>>>(cand, ncand, W, K, seed, block,
@@ -765,7 +771,7 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
         off.push_back(total);
         cur ^= 1;
         if (h_lover) {   // candidates overflowed: the next round scans every cell
-          cand = nullptr;
+          cand = CellList{nullptr, nullptr};
           ncand = m;
           S615_CU(cudaMemsetAsync(d_lover, 0, 4, st));
         } else {
