@@ -133,10 +133,10 @@ def test_build_keys_matches_oracle_seed_outcome(engine, keys_n):
 
 
 def test_device_build_past_u32_cells(engine):
-    # N = 84,000 gives m > 2^32 cells: the peel scans every cell each round
-    # (the candidate lists need u32 cell indices).  No false negative on a
-    # sample of pair keys, and the false-positive rate at r = 20 within four
-    # binomial standard deviations.
+    # N = 84,000 gives m > 2^32 cells: the peel lists hold offsets within a
+    # third of the table (block < 2^32) and the cell words' key indices reach
+    # past 2^31.  No false negative on a sample of pair keys, and the
+    # false-positive rate at r = 20 within four binomial standard deviations.
     N, r = 84000, 20
     tid = engine.build_table(N, r)
     try:
@@ -159,17 +159,20 @@ def test_device_build_past_u32_cells(engine):
 def test_device_build_same_bytes_under_a_tight_budget(engine):
     # The builder picks its form by the HBM it may use: by default the binned
     # incidence and the peel lists with each claimed key's index and hash; with
-    # a 400 MB budget the incidence adds straight into the cell words and the
-    # peel keeps only the claimed cells.  The rounds are the same, so the cells
-    # are too, byte for byte.
+    # a 400 MB budget (N = 3,000: ~110 MB of build buffers) the incidence adds
+    # straight into the cell words and the peel keeps only the claimed cells;
+    # with 100 MB there is no room for the claimed-cell list (22.5 MB) and
+    # every round scans all cells.  The rounds are the same, so the cells are
+    # too, byte for byte.
     N, r = 3000, 20
     tid = engine.build_table(N, r)
     try:
         h0, p0 = engine.export_table(tid)
     finally:
         engine.free_table(tid)
-    with s615.Engine(0, hbm_budget=400 << 20) as tight:
-        t2 = tight.build_table(N, r)
-        h1, p1 = tight.export_table(t2)
-    assert bytes(h0) == bytes(h1)
-    np.testing.assert_array_equal(p0, p1)
+    for budget in (400 << 20, 100 << 20):
+        with s615.Engine(0, hbm_budget=budget) as tight:
+            t2 = tight.build_table(N, r)
+            h1, p1 = tight.export_table(t2)
+        assert bytes(h0) == bytes(h1), budget
+        np.testing.assert_array_equal(p0, p1)
