@@ -579,14 +579,17 @@ int main(int argc, char** argv) {
     size_t ns = 0;
     if (nh) {
       size_t scap = std::max<size_t>(16, nh);
-      solv.resize(scap);
-      s = s615_cls5_verify(ctx, work.data() + off, n, hits.data(), nh, N, solv.data(), scap, &ns);
-      if (s && s != S615_E_OVERFLOW) {
+      for (;;) {   // one hit can verify to several pairs: grow the buffer until it holds them
+        solv.resize(scap);
+        s = s615_cls5_verify(ctx, work.data() + off, n, hits.data(), nh, N, solv.data(), scap, &ns);
+        if (s == S615_E_OVERFLOW && ns > scap) { scap = ns; continue; }
+        break;
+      }
+      if (s) {
         std::fprintf(stderr, "[cls5-gpu] verify failed: %s\n", s615_strerror(s));
         s615_close(ctx);
         return 1;
       }
-      ns = std::min(ns, scap);
       for (size_t k = 0; k < ns; ++k) {
         const s615_solution& S = solv[k];
         if (S.kind == 1) {   // a recovered plant: its exact planted (e, d, c1, c2)?
