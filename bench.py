@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--units", type=int, default=0, help="mix: units per step (default 200,000)")
     ap.add_argument("--seconds", type=float, default=10.0, help="serve: seconds of arrivals")
     ap.add_argument("--slots", type=int, default=2, help="serve: batches in flight")
+    ap.add_argument("--no-l2-window", action="store_true",
+                    help="cls5: time the pass without the peel's L2-persisting access window")
     ap.add_argument("--reference-gpu", type=int, default=15536,
                     help="cls5: run the reference's fourcore_cls5_gpu_v4 on K evenly spaced band "
                          "units (default: a tenth of the band; 0: the whole band; -1: skip)")
@@ -1227,8 +1229,10 @@ def main():
     stream = torch.cuda.Stream()
     sptr = C.c_void_p(stream.cuda_stream)
 
+    run_flags = s615.F_NO_L2_WINDOW if args.no_l2_window else 0
+
     def step():
-        s615._check(lib.s615_run_batch(eng._ctx, tid, batch, 0, sptr), "run_batch")
+        s615._check(lib.s615_run_batch(eng._ctx, tid, batch, run_flags, sptr), "run_batch")
 
     for _ in range(args.warmup):
         step()
@@ -1446,6 +1450,7 @@ def main():
                    "shards": args.shards,
                    "units_per_rank": n, "N": N, "r": args.r,
                    "l2": "inputs larger than L2 (table %.1f GB)" % (eng.table_info(tid).device_bytes / 1e9),
+                   "l2_window": not args.no_l2_window,
                    "parallelism": (f"shard-split x{world}: each rank holds {args.shards // world}+ of "
                                    f"{args.shards} shards and runs the whole band" if split
                                    else f"replicas-by-band x{world}")},
