@@ -725,6 +725,36 @@ METRIC_MIX = "mixed-class units/s (classes 2:4%/3:1%/4:48%/5:47%, B log-uniform 
 METRIC_SERVE = "per-unit latency p50/p99 through the serving loop (Poisson 5,000 units/s), 1 B200"
 
 
+def solve_516_cfg1(points, runs=15):
+    """The reference's own CPU path on config 1 (`solve_516_v2 1000 30000 5`,
+    OpenMP over every host core; solve_516_v2.cpp:488-563), timed without
+    its pair-index build.  Its search is an exact pair-sum index rather than
+    the xor probe, so the rate is quoted per R>0 point of the same 725 units
+    (`points`, the oracle's count).  None when the program was not built."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "solve_516_v2")
+    if not os.path.exists(exe):
+        return None
+    search = []
+    units = sols = None
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        p = subprocess.run([exe, "1000", "30000", "5"], capture_output=True, text=True, timeout=120)
+        wall = time.perf_counter() - t0
+        if p.returncode != 0:
+            return None
+        m = re.search(r"index built in (\d+) ms", p.stderr)
+        search.append(wall - (int(m.group(1)) / 1e3 if m else 0.0))
+        mu = re.search(r"unit candidates tested: (\d+)", p.stderr)
+        ms = re.search(r"total solutions: (\d+)", p.stderr)
+        units = int(mu.group(1)) if mu else None
+        sols = int(ms.group(1)) if ms else None
+    t = statistics.median(search)
+    return {"value": points / t, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+            "sample": f"oracle/_ref/solve_516_v2 1000 30000 5, median of {runs} runs: "
+                      f"{t * 1e3:.1f} ms of search (process wall minus its printed index build) "
+                      f"for {units} units, {sols} solutions; rate per R>0 point of those units"}
+
+
 def run_cfg1(args, rank, world, local, dist):
     """--workload cfg1: the small CPU-runnable configuration -- every class-5
     unit of B in [1000, 30000] (725) plus 8 plants against an N = 715, r = 48
@@ -763,6 +793,9 @@ def run_cfg1(args, rank, world, local, dist):
     _, (calls, gated, probes) = orc.cls5_run(ot, oarr, len(units))
     cpu_s = time.perf_counter() - t0
     eng.close()
+    port = {"value": (gated + probes) / cpu_s, "unit": UNIT, "cores": os.cpu_count(),
+            "kind": "port", "sample": f"all {len(units)} units once"}
+    ref = solve_516_cfg1(gated + probes)
     v = res["window"]["pos"] / (res["window"]["ms_per_pass"] / 1e3)
     line = {"metric": "cls5 peel probes/sec, B in [1000, 30000] (config 1), 1 B200", "value": v,
             "unit": UNIT, "n_gpus": 1, "steps": max(args.steps, 50), "warmup": args.warmup,
@@ -771,8 +804,8 @@ def run_cfg1(args, rank, world, local, dist):
             "config": {"workload": f"config 1: {len(units)} Stage-1 units + 8 plants, N={N} r={args.r} "
                                    "table built on the device (1.9 MB: fits L2)"},
             "l2_window": res,
-            "cpu_baseline": {"value": (gated + probes) / cpu_s, "unit": UNIT, "cores": os.cpu_count(),
-                             "kind": "port", "sample": f"all {len(units)} units once"}}
+            "cpu_baseline": ref or port,
+            "cpu_port": port}
     print(json.dumps(line), flush=True)
     return 0
 
