@@ -754,6 +754,22 @@ int arena_get(s615_ctx* ctx, int k, size_t bytes, void** p) {
   return S615_OK;
 }
 
+// Host threads for a pass over n units: one per 8,192 units, at most the
+// machine's hardware threads (32 at most); one below 16,384 units.
+static size_t host_threads(size_t n) {
+  const size_t hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  return n < (1u << 14) ? 1 : std::min(hw, n / 8192);
+}
+
+// Run work(t) for t in [0, nt) on nt threads (inline when nt == 1).
+template <class F>
+static void run_threads(size_t nt, F&& work) {
+  if (nt == 1) { work(0); return; }
+  std::vector<std::thread> th;
+  for (size_t t = 0; t < nt; ++t) th.emplace_back(work, t);
+  for (auto& x : th) x.join();
+}
+
 // make_dev_unit over every unit (on several host threads for large batches),
 // the kept records compacted in unit order.  Returns the error of the
 // lowest-index unit that has one, as a sequential pass would.
@@ -766,8 +782,7 @@ static int pack_units(s615_ctx* ctx, const s615_unit* units, size_t n, DevUnit**
       stage_get(ctx->unit_stage, std::max<size_t>(n, 1) * sizeof(DevUnit)));
   if (!out) return S615_E_OOM;
   *out_p = out;
-  const size_t hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-  const size_t nt = n < (1u << 16) ? 1 : std::min(hw, (n + 65535) / 65536);
+  const size_t nt = host_threads(n);
   std::vector<int> err(nt, 0);
   auto work = [&](size_t t) {
     for (size_t i = n * t / nt, hi = n * (t + 1) / nt; i < hi; ++i) {
@@ -777,13 +792,7 @@ static int pack_units(s615_ctx* ctx, const s615_unit* units, size_t n, DevUnit**
       if (skip) out[i].cls = 0;
     }
   };
-  if (nt == 1) {
-    work(0);
-  } else {
-    std::vector<std::thread> th;
-    for (size_t t = 0; t < nt; ++t) th.emplace_back(work, t);
-    for (auto& x : th) x.join();
-  }
+  run_threads(nt, work);
   for (size_t t = 0; t < nt; ++t)
     if (err[t]) return err[t];
   *n_out = n;
@@ -795,7 +804,6 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
   DevUnit* du = nullptr;
   size_t nd = 0;
   if (const int s = pack_units(ctx, units, n, &du, &nd)) return s;
-  std::vector<u64> items617;   // the (6,1,7) kernel's items go after the others
   // Job rows per item: up to 64, fewer when the batch is small, so that its
   // items still fill the GPU (about 64 warps per SM).
   u32 job_rows = 8;
@@ -830,22 +838,50 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
   // a batch too small to fill the GPU even with 16-row items (a serving
   // request) also splits each class 2-4 row chunk four ways over its tiles
   b->parts3 = (!ctx->force_rows && !tuned.item_rows && unit_rows == 16) ? 4u : 1u;
-  for (size_t k = 0; k < nd; ++k) {
-    const DevUnit& d = du[k];
-    if (d.cls == 0) continue;   // dropped
-    // classes 1, 7 and 8 (c4 windows) run in the second kernel
-    unit_items(d, (u32)k,
-               (d.cls == S615_CLS_617 || d.cls == 1 || d.cls == S615_CLS_617_FIND4) ? items617
-                                                                                : b->host_items,
-               job_rows, unit_rows, b->parts3);
+  // Work items unit by unit in input order, on several host threads for a
+  // large batch.  Thread ranges are cut at multiples of job_rows, where a
+  // single pass starts a new item too (consecutive job rows share items, but
+  // never across such a multiple), so the items equal one sequential pass's.
+  const size_t nt = host_threads(nd);
+  std::vector<size_t> cut(nt + 1, nd);
+  cut[0] = 0;
+  for (size_t t = 1; t < nt; ++t)
+    cut[t] = std::max(cut[t - 1], std::min(nd, nd * t / nt / job_rows * job_rows));
+  b->part_main.resize(nt);
+  b->part_617.resize(nt);
+  run_threads(nt, [&](size_t t) {
+    auto& main = b->part_main[t];
+    auto& i617 = b->part_617[t];   // the (6,1,7) kernel's items go after the others
+    main.clear();
+    i617.clear();
+    for (size_t k = cut[t]; k < cut[t + 1]; ++k) {
+      const DevUnit& d = du[k];
+      if (d.cls == 0) continue;   // dropped
+      // classes 1, 7 and 8 (c4 windows) run in the second kernel
+      unit_items(d, (u32)k,
+                 (d.cls == S615_CLS_617 || d.cls == 1 || d.cls == S615_CLS_617_FIND4) ? i617 : main,
+                 job_rows, unit_rows, b->parts3);
+    }
+  });
+  std::vector<size_t> at(nt + 1, 0);
+  for (size_t t = 0; t < nt; ++t) at[t + 1] = at[t] + b->part_main[t].size();
+  size_t n617 = 0;
+  for (size_t t = 0; t < nt; ++t) n617 += b->part_617[t].size();
+  b->host_items.resize(at[nt] + n617);
+  run_threads(nt, [&](size_t t) {
+    std::copy(b->part_main[t].begin(), b->part_main[t].end(), b->host_items.begin() + at[t]);
+  });
+  if (n617) {
+    auto first617 = b->host_items.begin() + at[nt];
+    auto o = first617;
+    for (size_t t = 0; t < nt; ++t) o = std::copy(b->part_617[t].begin(), b->part_617[t].end(), o);
+    // heaviest first: a candidate's first rows (smallest d) have the largest T
+    // and windows, so every candidate's chunk 0 goes out before any chunk 1
+    std::stable_sort(first617, b->host_items.end(),
+                     [](u64 a, u64 b) { return item_chunk(a) < item_chunk(b); });
   }
-  // heaviest first: a candidate's first rows (smallest d) have the largest T
-  // and windows, so every candidate's chunk 0 goes out before any chunk 1
-  std::stable_sort(items617.begin(), items617.end(),
-                   [](u64 a, u64 b) { return item_chunk(a) < item_chunk(b); });
   b->n_units = nd;
-  b->n_main = b->host_items.size();
-  b->host_items.insert(b->host_items.end(), items617.begin(), items617.end());
+  b->n_main = at[nt];
   b->n_items = b->host_items.size();
   int s = 0;
   void* p = nullptr;

@@ -163,6 +163,8 @@ struct s615_batch {
   s615::u32 parts3 = 1;
   s615::u32 blocks_per_sm = 0;              // k_peel blocks per SM (0: the occupancy limit)
   std::vector<s615::u64> host_items;
+  // per host thread item lists of the last fill (kept for their capacity)
+  std::vector<std::vector<s615::u64>> part_main, part_617;
 };
 
 namespace s615 {

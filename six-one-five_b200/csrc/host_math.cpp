@@ -688,9 +688,11 @@ int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip) {
 
 void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out, u32 job_rows,
                 u32 unit_rows, u32 parts3) {
-  if (d.cls == kClsJobRow) {   // runs of up to kJobRows consecutive job rows of one kind
+  if (d.cls == kClsJobRow) {   // runs of up to job_rows consecutive job rows of one kind
     const u32 kind = d.w != 0 ? kJobFind2 : 0u;
-    if (!out.empty()) {
+    // an item also starts at every multiple of job_rows, so a batch can be
+    // itemised in ranges cut there and still give one pass's items
+    if (!out.empty() && unit_index % job_rows != 0) {
       const u64 last = out.back();
       if (item_res(last) == kJobItemTag && (item_chunk(last) & kJobFind2) == kind &&
           item_unit(last) + job_count(last) == unit_index && job_count(last) < job_rows) {

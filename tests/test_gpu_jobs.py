@@ -173,6 +173,48 @@ def test_jobs_in_a_mixed_batch(engine, oracle_table, band):
         engine.free_table(tid)
 
 
+def test_large_batch_threads_equal_chunks(engine, oracle_table, band):
+    """A batch of 16,384 units or more is packed and cut into work items on
+    several host threads; the same units in chunks below that size take one
+    thread each.  Job-row runs, Stage-1 units and (6,1,7) candidates are
+    interleaved so that thread ranges start beside every kind of unit."""
+    arr, _, n, _, _, N = band
+    _, path = oracle_table(N, 16)
+    tid = engine.load_table(path, N)
+    try:
+        u5 = W.cls5_units(24001, 26000)
+        c7, n7 = s615.candidates617(24329)
+        seq, k = [], 0
+        while len(seq) < 60_000:
+            run = 1 + (k * 7919) % 3000
+            seq += [arr[(k * 131 + i) % n] for i in range(run)]
+            B, u = u5[k % len(u5)]
+            x = s615.Unit()
+            x.cls, x.B, x.u = 5, B, u
+            seq.append(x)
+            seq.append(c7[k % n7])
+            k += 1
+        whole = (s615.Unit * len(seq))(*seq)
+        hw, cw = engine.run(tid, whole, len(seq))
+        parts, tot = [], {f: 0 for f in ("calls", "gated", "probes", "pos", "hits")}
+        for lo in range(0, len(seq), 9000):
+            m = min(9000, len(seq) - lo)
+            sub = (s615.Unit * m)(*seq[lo:lo + m])
+            h, c = engine.run(tid, sub, m)
+            h = h.copy()
+            h["unit"] += lo
+            parts.append(h)
+            for f in tot:
+                tot[f] += getattr(c, f)
+        for f in tot:
+            assert getattr(cw, f) == tot[f], f
+        key = lambda hs: sorted(tuple(int(h[f]) for f in ("unit", "d", "e", "c4", "fp")) for h in hs)
+        assert key(hw) == key(np.concatenate(parts))
+        assert cw.hits > 0
+    finally:
+        engine.free_table(tid)
+
+
 DONE = re.compile(r"---- done: solutions=(\d+) jobs=(\d+) failT=(\d+)( \(\w+ stream\))? ----")
 
 
