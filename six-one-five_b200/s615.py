@@ -336,15 +336,20 @@ def jobs_write(path: str, jobs, n: int) -> None:
     _check(lib().s615_jobs_write(path.encode(), C.cast(jobs, C.c_void_p), n), "jobs_write")
 
 
-def jobs_read(path: str, chunk: int = 1 << 16):
-    """Every job of a .bbj or text job file: (array, n, JobsInfo)."""
+def jobs_read(path: str, chunk: int = 1 << 16, out=None):
+    """Every job of a .bbj or text job file: (array, n, JobsInfo).
+
+    `out`, a Unit array, is filled and returned instead of a new array when a
+    .bbj file's jobs fit it (a caller reading file after file reuses one
+    buffer; a new array is allocated when they do not fit)."""
     f = C.c_void_p()
     info = JobsInfo()
     _check(lib().s615_jobs_open(path.encode(), C.byref(f), C.byref(info)), "jobs_open")
     parts, n = [], 0
     try:
         if info.binary and info.n_jobs:   # the header's count in one read, then anything after it
-            first = (Unit * info.n_jobs)()
+            fits = out is not None and len(out) >= info.n_jobs
+            first = out if fits else (Unit * info.n_jobs)()
             k = C.c_size_t(0)
             _check(lib().s615_jobs_next(f, C.cast(first, C.c_void_p), info.n_jobs, C.byref(k)),
                    "jobs_next")
@@ -364,13 +369,13 @@ def jobs_read(path: str, chunk: int = 1 << 16):
         lib().s615_jobs_close(f, C.byref(info))
     if len(parts) == 1 and not isinstance(parts[0], bytes):
         return parts[0], n, info
-    out = (Unit * max(n, 1))()
+    whole = (Unit * max(n, 1))()
     off = 0
-    for p in parts:
-        size = len(p) if isinstance(p, bytes) else C.sizeof(p)
-        C.memmove(C.byref(out, off), p, size)
+    for p in parts:   # the header-count read, then the chunks after it
+        size = len(p) if isinstance(p, bytes) else info.n_jobs * C.sizeof(Unit)
+        C.memmove(C.byref(whole, off), p, size)
         off += size
-    return out, n, info
+    return whole, n, info
 
 
 def jobs617_band(Bs: Iterable[int], classes: Iterable[int] = (1, 2, 3, 4)):

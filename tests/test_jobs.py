@@ -70,6 +70,13 @@ def test_job_files_round_trip(tmp_path):
         got, k, info = s615.jobs_read(path, chunk=4096)
         assert k == m and as_tuples(got, k) == as_tuples(jobs, m)
         assert info.binary == (name != "j.but")
+        if info.binary:   # a caller's buffer that fits is filled in place; one too small is not used
+            buf = (s615.Unit * (m + 5))()
+            got, k, _ = s615.jobs_read(path, out=buf)
+            assert got is buf and k == m and as_tuples(buf, k) == as_tuples(jobs, m)
+            small = (s615.Unit * (m - 1))()
+            got, k, _ = s615.jobs_read(path, out=small)
+            assert got is not small and k == m and as_tuples(got, k) == as_tuples(jobs, m)
     raw = open(str(tmp_path / "j.bbj"), "rb").read()
     magic, ver, nj, rec, lo, hi, pad = struct.unpack("<IIQIIII", raw[:32])
     assert (magic, ver, nj, rec, lo, hi) == (0x4A424346, 2, m, 36, 100003, 400471)
