@@ -8,6 +8,7 @@
 // device-wide sync per 16 units; a full hit buffer is reported
 // (S615_E_OVERFLOW) instead of silently truncated.
 #include <cuda_runtime.h>
+#include <sched.h>
 
 #include <algorithm>
 #include <cstdio>
@@ -755,10 +756,13 @@ int arena_get(s615_ctx* ctx, int k, size_t bytes, void** p) {
 }
 
 // Host threads for a pass over n units: one per 8,192 units, at most the
-// machine's hardware threads (32 at most); one below 16,384 units.
+// CPUs the process may run on (and 32); one below 16,384 units.
 static size_t host_threads(size_t n) {
-  const size_t hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-  return n < (1u << 14) ? 1 : std::min(hw, n / 8192);
+  if (n < (1u << 14)) return 1;
+  size_t hw = std::thread::hardware_concurrency();
+  cpu_set_t set;   // the CPUs this process may run on, when fewer than the machine's
+  if (sched_getaffinity(0, sizeof set, &set) == 0) hw = (size_t)CPU_COUNT(&set);
+  return std::max<size_t>(1, std::min<size_t>({hw, 32, n / 8192}));
 }
 
 // Run work(t) for t in [0, nt) on nt threads (inline when nt == 1).
@@ -800,7 +804,7 @@ static int pack_units(s615_ctx* ctx, const s615_unit* units, size_t n, DevUnit**
 }
 
 int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
-  b->host_items.clear();
+  b->n_items = b->n_main = 0;
   DevUnit* du = nullptr;
   size_t nd = 0;
   if (const int s = pack_units(ctx, units, n, &du, &nd)) return s;
@@ -839,50 +843,62 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
   // request) also splits each class 2-4 row chunk four ways over its tiles
   b->parts3 = (!ctx->force_rows && !tuned.item_rows && unit_rows == 16) ? 4u : 1u;
   // Work items unit by unit in input order, on several host threads for a
-  // large batch.  Thread ranges are cut at multiples of job_rows, where a
-  // single pass starts a new item too (consecutive job rows share items, but
-  // never across such a multiple), so the items equal one sequential pass's.
+  // large batch: each thread counts its range's items, then writes them in
+  // place.  Ranges are cut at multiples of job_rows, where a single pass
+  // starts a new item too (consecutive job rows share items, but never across
+  // such a multiple), so the items equal one sequential pass's.
   const size_t nt = host_threads(nd);
   std::vector<size_t> cut(nt + 1, nd);
   cut[0] = 0;
   for (size_t t = 1; t < nt; ++t)
     cut[t] = std::max(cut[t - 1], std::min(nd, nd * t / nt / job_rows * job_rows));
-  b->part_main.resize(nt);
-  b->part_617.resize(nt);
+  // classes 1, 7 and 8 (c4 windows) run in the second kernel, after the others
+  auto second = [](const DevUnit& d) {
+    return d.cls == S615_CLS_617 || d.cls == 1 || d.cls == S615_CLS_617_FIND4;
+  };
+  std::vector<size_t> cnt_main(nt, 0), cnt_617(nt, 0);
   run_threads(nt, [&](size_t t) {
-    auto& main = b->part_main[t];
-    auto& i617 = b->part_617[t];   // the (6,1,7) kernel's items go after the others
-    main.clear();
-    i617.clear();
+    ItemCount m, c;
     for (size_t k = cut[t]; k < cut[t + 1]; ++k) {
       const DevUnit& d = du[k];
       if (d.cls == 0) continue;   // dropped
-      // classes 1, 7 and 8 (c4 windows) run in the second kernel
-      unit_items(d, (u32)k,
-                 (d.cls == S615_CLS_617 || d.cls == 1 || d.cls == S615_CLS_617_FIND4) ? i617 : main,
-                 job_rows, unit_rows, b->parts3);
+      if (second(d)) unit_items(d, (u32)k, c, job_rows, unit_rows, b->parts3);
+      else unit_items(d, (u32)k, m, job_rows, unit_rows, b->parts3);
+    }
+    cnt_main[t] = m.n;
+    cnt_617[t] = c.n;
+  });
+  std::vector<size_t> at(nt + 1, 0), at617(nt + 1, 0);
+  for (size_t t = 0; t < nt; ++t) at[t + 1] = at[t] + cnt_main[t];
+  at617[0] = at[nt];
+  for (size_t t = 0; t < nt; ++t) at617[t + 1] = at617[t] + cnt_617[t];
+  const size_t total = at617[nt];
+  if (total > b->host_items_cap) {
+    b->host_items.reset();
+    b->host_items_cap = 0;
+    b->host_items.reset(new (std::nothrow) u64[std::max<size_t>(total, 1)]);
+    if (!b->host_items) return S615_E_OOM;
+    b->host_items_cap = std::max<size_t>(total, 1);
+  }
+  u64* items = b->host_items.get();
+  run_threads(nt, [&](size_t t) {
+    ItemWriter m, c;
+    m.p = items + at[t];
+    c.p = items + at617[t];
+    for (size_t k = cut[t]; k < cut[t + 1]; ++k) {
+      const DevUnit& d = du[k];
+      if (d.cls == 0) continue;
+      if (second(d)) unit_items(d, (u32)k, c, job_rows, unit_rows, b->parts3);
+      else unit_items(d, (u32)k, m, job_rows, unit_rows, b->parts3);
     }
   });
-  std::vector<size_t> at(nt + 1, 0);
-  for (size_t t = 0; t < nt; ++t) at[t + 1] = at[t] + b->part_main[t].size();
-  size_t n617 = 0;
-  for (size_t t = 0; t < nt; ++t) n617 += b->part_617[t].size();
-  b->host_items.resize(at[nt] + n617);
-  run_threads(nt, [&](size_t t) {
-    std::copy(b->part_main[t].begin(), b->part_main[t].end(), b->host_items.begin() + at[t]);
-  });
-  if (n617) {
-    auto first617 = b->host_items.begin() + at[nt];
-    auto o = first617;
-    for (size_t t = 0; t < nt; ++t) o = std::copy(b->part_617[t].begin(), b->part_617[t].end(), o);
-    // heaviest first: a candidate's first rows (smallest d) have the largest T
-    // and windows, so every candidate's chunk 0 goes out before any chunk 1
-    std::stable_sort(first617, b->host_items.end(),
-                     [](u64 a, u64 b) { return item_chunk(a) < item_chunk(b); });
-  }
+  // heaviest first: a candidate's first rows (smallest d) have the largest T
+  // and windows, so every candidate's chunk 0 goes out before any chunk 1
+  std::stable_sort(items + at[nt], items + total,
+                   [](u64 a, u64 c) { return item_chunk(a) < item_chunk(c); });
   b->n_units = nd;
   b->n_main = at[nt];
-  b->n_items = b->host_items.size();
+  b->n_items = total;
   int s = 0;
   void* p = nullptr;
   if (!b->d_units || nd > b->cap_units) {
@@ -914,7 +930,7 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
   if (nd)
     S615_CU(cudaMemcpy(b->d_units, du, nd * sizeof(DevUnit), cudaMemcpyHostToDevice));
   if (b->n_items)
-    S615_CU(cudaMemcpy(b->d_items, b->host_items.data(), b->n_items * sizeof(u64), cudaMemcpyHostToDevice));
+    S615_CU(cudaMemcpy(b->d_items, b->host_items.get(), b->n_items * sizeof(u64), cudaMemcpyHostToDevice));
   return S615_OK;
 }
 

@@ -2,7 +2,9 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -162,9 +164,10 @@ struct s615_batch {
   // part): part p sieves every parts3-th 1024-column tile of the rows' c3 windows
   s615::u32 parts3 = 1;
   s615::u32 blocks_per_sm = 0;              // k_peel blocks per SM (0: the occupancy limit)
-  std::vector<s615::u64> host_items;
-  // per host thread item lists of the last fill (kept for their capacity)
-  std::vector<std::vector<s615::u64>> part_main, part_617;
+  // host copy of the work items: grow-only and uninitialised, written in
+  // place by the fill's threads
+  std::unique_ptr<s615::u64[]> host_items;
+  size_t host_items_cap = 0;
 };
 
 namespace s615 {
@@ -305,11 +308,61 @@ int free_factor(int cls);
 // set for units the reference drops) or S615_E_FORMAT for units the engine
 // cannot search exactly.
 int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip);
+// Sinks for unit_items besides a std::vector<u64>: one that counts the items
+// a pass would append (it keeps the last one, which a run of job rows
+// extends), and one that appends into a window of a preallocated buffer.
+struct ItemCount {
+  size_t n = 0;
+  u64 last = 0;
+  bool empty() const { return n == 0; }
+  u64& back() { return last; }
+  void push_back(u64 it) { ++n; last = it; }
+};
+struct ItemWriter {
+  u64* p = nullptr;
+  size_t n = 0;
+  bool empty() const { return n == 0; }
+  u64& back() { return p[n - 1]; }
+  void push_back(u64 it) { p[n++] = it; }
+};
+
 // Work items of one packed unit (appended to out).
 // Job rows are grouped up to job_rows (<= kJobRows) per item; the row chunks
 // of classes 2-5 have unit_rows (<= kItemRows) rows each.
-void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out, u32 job_rows = kJobRows,
-                u32 unit_rows = kItemRows, u32 parts3 = 1);
+template <class Out>
+void unit_items(const DevUnit& d, u32 unit_index, Out& out, u32 job_rows = kJobRows,
+                u32 unit_rows = kItemRows, u32 parts3 = 1) {
+  if (d.cls == kClsJobRow) {   // runs of up to job_rows consecutive job rows of one kind
+    const u32 kind = d.w != 0 ? kJobFind2 : 0u;
+    // an item also starts at every multiple of job_rows, so a batch can be
+    // itemised in ranges cut there and still give one pass's items
+    if (!out.empty() && unit_index % job_rows != 0) {
+      const u64 last = out.back();
+      if (item_res(last) == kJobItemTag && (item_chunk(last) & kJobFind2) == kind &&
+          item_unit(last) + job_count(last) == unit_index && job_count(last) < job_rows) {
+        out.back() = last + 1;
+        return;
+      }
+    }
+    out.push_back(make_item(unit_index, kJobItemTag, kind | 1u));
+    return;
+  }
+  if (d.cls == 1 || d.cls == S615_CLS_617_FIND4) {   // chunks of the c4 window
+    const u32 n = (d.fmax1 - d.fmax2) / kC4Chunk + 1;
+    for (u32 c = 0; c < n; ++c) out.push_back(make_item(unit_index, 0, c));
+    return;
+  }
+  const bool c617 = d.cls == (u32)S615_CLS_617;
+  const u32 per = c617 ? item_rows(d.cls) : unit_rows;
+  const u32 parts = c617 ? kParts617 : (d.cls >= 2 && d.cls <= 4) ? std::max(parts3, 1u) : 1u;
+  for (u32 ir = 0; ir < d.nres1; ++ir) {
+    u32 jmin = 0, jend = 0;
+    class_rows(d.res1[ir], d.mod1, d.fmax1, &jmin, &jend);
+    const u32 rows = jend > jmin ? jend - jmin : 0;
+    for (u32 c = 0; c * per < rows; ++c)
+      for (u32 p = 0; p < parts; ++p) out.push_back(make_item(unit_index, ir, c * parts + p));
+  }
+}
 
 void gate_patterns(bool gated, int shape, u32 out[kPatWords]);
 void tri_tables(u32 out[kTriWords]);

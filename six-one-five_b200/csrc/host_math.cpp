@@ -686,40 +686,6 @@ int make_dev_unit(const s615_unit& in, u32 id, DevUnit* out, bool* skip) {
   return S615_OK;
 }
 
-void unit_items(const DevUnit& d, u32 unit_index, std::vector<u64>& out, u32 job_rows,
-                u32 unit_rows, u32 parts3) {
-  if (d.cls == kClsJobRow) {   // runs of up to job_rows consecutive job rows of one kind
-    const u32 kind = d.w != 0 ? kJobFind2 : 0u;
-    // an item also starts at every multiple of job_rows, so a batch can be
-    // itemised in ranges cut there and still give one pass's items
-    if (!out.empty() && unit_index % job_rows != 0) {
-      const u64 last = out.back();
-      if (item_res(last) == kJobItemTag && (item_chunk(last) & kJobFind2) == kind &&
-          item_unit(last) + job_count(last) == unit_index && job_count(last) < job_rows) {
-        out.back() = last + 1;
-        return;
-      }
-    }
-    out.push_back(make_item(unit_index, kJobItemTag, kind | 1u));
-    return;
-  }
-  if (d.cls == 1 || d.cls == S615_CLS_617_FIND4) {   // chunks of the c4 window
-    const u32 n = (d.fmax1 - d.fmax2) / kC4Chunk + 1;
-    for (u32 c = 0; c < n; ++c) out.push_back(make_item(unit_index, 0, c));
-    return;
-  }
-  const bool c617 = d.cls == (u32)S615_CLS_617;
-  const u32 per = c617 ? item_rows(d.cls) : unit_rows;
-  const u32 parts = c617 ? kParts617 : (d.cls >= 2 && d.cls <= 4) ? std::max(parts3, 1u) : 1u;
-  for (u32 ir = 0; ir < d.nres1; ++ir) {
-    u32 jmin = 0, jend = 0;
-    class_rows(d.res1[ir], d.mod1, d.fmax1, &jmin, &jend);
-    const u32 rows = jend > jmin ? jend - jmin : 0;
-    for (u32 c = 0; c * per < rows; ++c)
-      for (u32 p = 0; p < parts; ++p) out.push_back(make_item(unit_index, ir, c * parts + p));
-  }
-}
-
 // ------------------------------------------------------------ gate patterns
 // Admissible values mod q: sums of two sixth powers mod q (the factors of the
 // reference's mod-504 and mod-247 bitmaps, fourcore_cls5_gpu_v4.cu:124-137).
