@@ -1113,11 +1113,20 @@ def run_serve(args, rank, world, local, dist):
         return 0
     eng = s615.Engine(local)
     Ns = [24_000, 48_000, 76_000, 120_000]
+
+    def layout_for(N):
+        """--layout auto: WIDE (one sector per cell) while the table's WIDE
+        bytes (about 8 x 1.23 x N^2 / 2) stay under 56 GiB, which random reads
+        cover at their full rate; PACKED above that."""
+        if args.layout != "auto":
+            return s615.LAYOUT_WIDE if args.layout == "wide" else s615.LAYOUT_PACKED
+        return s615.LAYOUT_WIDE if 8 * 1.23 * N * N / 2 <= 56 * 2**30 else s615.LAYOUT_PACKED
+
     tids, builds = {}, {}
     for N in sorted(Ns, reverse=True):      # the largest build needs the most scratch
         t0 = time.perf_counter()
         try:
-            tids[N] = eng.build_table(N, args.r, layout=s615.LAYOUT_PACKED)
+            tids[N] = eng.build_table(N, args.r, layout=layout_for(N))
             builds[N] = round(time.perf_counter() - t0, 2)
         except s615.S615Error as e:
             log(f"table N={N}: {e}")
@@ -1181,7 +1190,9 @@ def run_serve(args, rank, world, local, dist):
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": f"Poisson {rate:.0f} units/s for {secs:.0f} s in {req_units}-unit requests, "
                                    "classes 2:4%/3:1%/4:48%/5:47%, B uniform [1M,5M]; resident tables "
-                                   + ", ".join(f"N={N}" for N in sorted(tids)) + " (packed, r=%d)" % args.r,
+                                   + ", ".join(f"N={N} " + ("wide" if eng.table_info(tids[N]).layout == s615.LAYOUT_WIDE
+                                                             else "packed") for N in sorted(tids))
+                                   + " (r=%d)" % args.r,
                        "hbm_budget_gb": 150, "resident_table_gb": round(resident / 1e9, 2)},
             "p50_unit_latency_ms": float(np.percentile(lat, 50)),
             "p99_unit_latency_ms": float(np.percentile(lat, 99)),
