@@ -57,11 +57,74 @@ void dev_free(s615_ctx* ctx, void* p, size_t bytes) {
 }
 
 bool release_run_batch(s615_ctx* ctx) {
-  if (!ctx->run_batch || ctx->run_busy) return false;
-  s615_batch* b = ctx->run_batch;
-  ctx->run_batch = nullptr;
-  s615_batch_free(ctx, b);
-  return true;
+  bool any = false;
+  if (ctx->run_batch && !ctx->run_busy) {
+    s615_batch* b = ctx->run_batch;
+    ctx->run_batch = nullptr;
+    s615_batch_free(ctx, b);
+    any = true;
+  }
+  {
+    std::lock_guard<std::mutex> lock(ctx->pool_mu);
+    any = any || !ctx->pool.empty();
+  }
+  pool_release(ctx);
+  return any;
+}
+
+// Batch buffers.  A freed batch's device buffers go to a pool on the context
+// (at most kPoolBytes and kPoolBuffers), and the next batch takes the
+// smallest pooled buffer that holds its request and is at most twice as large,
+// so a caller that prepares and frees batch after batch allocates and frees
+// no device memory once the pool holds its sizes.  The pool is given back
+// with s615_run's kept batch: when a table is built or loaded, when an
+// allocation runs out of room, and on s615_close.
+constexpr size_t kPoolBytes = size_t(8) << 30;
+constexpr size_t kPoolBuffers = 64;
+
+int pool_get(s615_ctx* ctx, size_t bytes, void** p, size_t* got) {
+  {
+    std::lock_guard<std::mutex> lock(ctx->pool_mu);   // never held across dev_alloc
+    size_t best = 0;
+    for (size_t i = 0; i < ctx->pool.size(); ++i) {
+      const size_t sz = ctx->pool[i].second;
+      if (sz >= bytes && sz <= 2 * std::max<size_t>(bytes, 4096) &&
+          (best == 0 || sz < ctx->pool[best - 1].second))
+        best = i + 1;
+    }
+    if (best) {
+      *p = ctx->pool[best - 1].first;
+      *got = ctx->pool[best - 1].second;
+      ctx->pool_bytes -= *got;
+      ctx->pool.erase(ctx->pool.begin() + (best - 1));
+      return S615_OK;
+    }
+  }
+  *got = bytes;
+  return dev_alloc(ctx, p, bytes);
+}
+
+void pool_put(s615_ctx* ctx, void* p, size_t bytes) {
+  if (!p) return;
+  {
+    std::lock_guard<std::mutex> lock(ctx->pool_mu);
+    if (ctx->pool.size() < kPoolBuffers && ctx->pool_bytes + bytes <= kPoolBytes) {
+      ctx->pool.emplace_back(p, bytes);
+      ctx->pool_bytes += bytes;
+      return;
+    }
+  }
+  dev_free(ctx, p, bytes);
+}
+
+void pool_release(s615_ctx* ctx) {
+  std::vector<std::pair<void*, size_t>> all;
+  {
+    std::lock_guard<std::mutex> lock(ctx->pool_mu);
+    all.swap(ctx->pool);
+    ctx->pool_bytes = 0;
+  }
+  for (auto& e : all) dev_free(ctx, e.first, e.second);
 }
 
 void* stage_get(HostStage& s, size_t bytes) {
@@ -901,31 +964,36 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
   b->n_items = total;
   int s = 0;
   void* p = nullptr;
+  size_t got = 0;
   if (!b->d_units || nd > b->cap_units) {
-    dev_free(ctx, b->d_units, b->cap_units * sizeof(DevUnit));
+    pool_put(ctx, b->d_units, b->units_bytes);
     b->d_units = nullptr;
-    const size_t cap = std::max<size_t>(nd, 1);
-    if ((s = dev_alloc(ctx, &p, cap * sizeof(DevUnit)))) { b->cap_units = 0; return s; }
+    b->cap_units = b->units_bytes = 0;
+    if ((s = pool_get(ctx, std::max<size_t>(nd, 1) * sizeof(DevUnit), &p, &got))) return s;
     b->d_units = static_cast<DevUnit*>(p);
-    b->cap_units = cap;
+    b->units_bytes = got;
+    b->cap_units = got / sizeof(DevUnit);
   }
   if (!b->d_items || b->n_items > b->cap_items) {
-    dev_free(ctx, b->d_items, b->cap_items * sizeof(u64));
+    pool_put(ctx, b->d_items, b->items_bytes);
     b->d_items = nullptr;
-    const size_t cap = std::max<size_t>(b->n_items, 1);
-    if ((s = dev_alloc(ctx, &p, cap * sizeof(u64)))) { b->cap_items = 0; return s; }
+    b->cap_items = b->items_bytes = 0;
+    if ((s = pool_get(ctx, std::max<size_t>(b->n_items, 1) * sizeof(u64), &p, &got))) return s;
     b->d_items = static_cast<u64*>(p);
-    b->cap_items = cap;
+    b->items_bytes = got;
+    b->cap_items = got / sizeof(u64);
   }
   if (!b->d_ctr) {
-    if ((s = dev_alloc(ctx, &p, sizeof(Cls5Counters) + 64))) return s;
+    if ((s = pool_get(ctx, sizeof(Cls5Counters) + 64, &p, &got))) return s;
     b->d_ctr = static_cast<Cls5Counters*>(p);
     b->d_work = reinterpret_cast<u32*>(static_cast<char*>(p) + sizeof(Cls5Counters));
+    b->ctr_bytes = got;
   }
   if (!b->d_hits) {
-    if ((s = dev_alloc(ctx, &p, (size_t)(1u << 20) * sizeof(s615_hit)))) return s;
+    if ((s = pool_get(ctx, (size_t)(1u << 20) * sizeof(s615_hit), &p, &got))) return s;
     b->d_hits = static_cast<s615_hit*>(p);
     b->hit_cap = 1u << 20;
+    b->hits_bytes = got;
   }
   if (nd)
     S615_CU(cudaMemcpy(b->d_units, du, nd * sizeof(DevUnit), cudaMemcpyHostToDevice));
@@ -962,10 +1030,11 @@ int s615_batch_size(const s615_batch* b, size_t* n_units, size_t* n_items, size_
 
 int s615_batch_free(s615_ctx* ctx, s615_batch* b) {
   if (!ctx || !b) return S615_E_ARG;
-  dev_free(ctx, b->d_units, b->cap_units * sizeof(DevUnit));
-  dev_free(ctx, b->d_items, b->cap_items * sizeof(u64));
-  dev_free(ctx, b->d_ctr, sizeof(Cls5Counters) + 64);
-  dev_free(ctx, b->d_hits, (size_t)b->hit_cap * sizeof(s615_hit));
+  // the device buffers go to the context's pool for the next batch
+  pool_put(ctx, b->d_units, b->units_bytes);
+  pool_put(ctx, b->d_items, b->items_bytes);
+  pool_put(ctx, b->d_ctr, b->ctr_bytes);
+  pool_put(ctx, b->d_hits, b->hits_bytes);
   delete b;
   return S615_OK;
 }

@@ -7,6 +7,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/s615.h"
@@ -157,6 +158,7 @@ struct s615_batch {
   s615_hit* d_hits = nullptr;
   s615::u32 hit_cap = 0;
   size_t cap_units = 0, cap_items = 0;   // device capacity (a reused batch only grows)
+  size_t units_bytes = 0, items_bytes = 0, ctr_bytes = 0, hits_bytes = 0;   // buffer sizes
   s615::Cls5Counters* d_ctr = nullptr;
   s615::u32* d_work = nullptr;   // persistent-queue cursors [classes 2-5, cls 7]
   s615::u32 item_rows = s615::kItemRows;   // rows per class 2-5 item (smaller for small batches)
@@ -209,6 +211,10 @@ struct s615_ctx {
   // device allocation runs out of room.
   s615::HostStage unit_stage;
   s615_batch* run_batch = nullptr;
+  // device buffers of freed batches, reused by the next batch (capi.cu)
+  std::vector<std::pair<void*, size_t>> pool;
+  size_t pool_bytes = 0;
+  std::mutex pool_mu;
   bool run_busy = false;
   // L2-persisting access windows (cudaDevAttrMaxPersistingL2CacheSize,
   // cudaDevAttrMaxAccessPolicyWindowSize) and the set-aside this context
@@ -234,12 +240,20 @@ void server_destroy(s615_ctx* ctx);   // stops the loop (draining it) and frees 
 // Host staging (grow-only; nullptr if even a pageable buffer cannot be had).
 void* stage_get(HostStage& s, size_t bytes);
 void stage_free(HostStage& s);
-// Frees s615_run's kept batch unless a run is using it; true if one was freed.
+// Frees s615_run's kept batch (unless a run is using it) and the pool of
+// freed batch buffers; true if either held anything.
 bool release_run_batch(s615_ctx* ctx);
 
 // Budgeted device allocation.
 int dev_alloc(s615_ctx* ctx, void** p, size_t bytes);
 void dev_free(s615_ctx* ctx, void* p, size_t bytes);
+// Batch buffers through the context's pool: pool_get hands out a pooled
+// buffer of at least `bytes` (at most twice that) or a new one, with its size
+// in *got; pool_put keeps a buffer for reuse (or frees it once the pool is
+// full); pool_release frees every pooled buffer.
+int pool_get(s615_ctx* ctx, size_t bytes, void** p, size_t* got);
+void pool_put(s615_ctx* ctx, void* p, size_t bytes);
+void pool_release(s615_ctx* ctx);
 // Grow-only scratch slot k of the context (no free, so no device-wide sync
 // once it is large enough).
 int arena_get(s615_ctx* ctx, int k, size_t bytes, void** p);

@@ -1,6 +1,9 @@
 """s615_run keeps its batch between calls: results must not depend on what ran
 before (smaller, larger, overflowing or failed calls, table builds that take the
-buffers back), and dropped units keep their input index (GPU)."""
+buffers back), and dropped units keep their input index; freed batches leave
+their device buffers in the context's pool for the next batch (GPU)."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -77,3 +80,41 @@ def test_dropped_units_keep_input_indices(engine, setup):
     hits = hits.copy()
     hits["unit"] = [back[int(u)] for u in hits["unit"]]
     assert key(hits, ctr) == base
+
+
+def test_prepare_free_cycles_reuse_the_pool(engine, setup):
+    tid, (sa, sn), (la, ln) = setup
+    lib = s615.lib()
+
+    def mem_free():
+        f, t = C.c_size_t(0), C.c_size_t(0)
+        s615._check(lib.s615_mem_info(engine._ctx, C.byref(f), C.byref(t)), "mem_info")
+        return f.value
+
+    def cycle(arr, n):
+        b = C.c_void_p()
+        s615._check(lib.s615_prepare(engine._ctx, C.cast(arr, C.c_void_p), n, C.byref(b)), "prepare")
+        s615._check(lib.s615_run_batch(engine._ctx, tid, b, 0, None), "run_batch")
+        hits = (s615.Hit * 4096)()
+        nh, ctr = C.c_size_t(0), s615.Counters()
+        s615._check(lib.s615_batch_results(engine._ctx, b, C.cast(hits, C.c_void_p), 4096,
+                                           C.byref(nh), C.byref(ctr)), "results")
+        s615._check(lib.s615_batch_free(engine._ctx, b), "batch_free")
+        return key(s615.hits_to_array(hits, nh.value), ctr)
+
+    t2 = engine.build_table(300, 16)   # gives back the kept batch and the pool
+    engine.free_table(t2)
+    want_l, want_s = key(*engine.run(tid, la, ln)), key(*engine.run(tid, sa, sn))
+    t2 = engine.build_table(300, 16)
+    engine.free_table(t2)
+    before = mem_free()
+    assert cycle(la, ln) == want_l
+    held = mem_free()
+    assert held < before          # the freed batch's buffers stay in the pool
+    for _ in range(3):
+        assert cycle(la, ln) == want_l
+        assert cycle(sa, sn) == want_s
+        assert mem_free() >= held - (4 << 20)   # taken from the pool, not allocated again
+    t2 = engine.build_table(300, 16)          # a table build empties the pool
+    engine.free_table(t2)
+    assert mem_free() > held
