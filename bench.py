@@ -1147,6 +1147,8 @@ def run_serve(args, rank, world, local, dist):
     planted = {}          # (ticket, index) -> expected solution key
     eng.serve_start(slots=args.slots)
     lat, sent, done, got_plants = [], 0, 0, 0
+    rows = []             # (submitted at, table N, latency ms, units) per request
+    sub_at = {}           # ticket -> (seconds after start, table N)
     t_start = time.perf_counter()
     nxt = t_start
     try:
@@ -1161,6 +1163,7 @@ def run_serve(args, rank, world, local, dist):
                     p5 = W.plants(1, int(rng.randint(1 << 30)), blo, bhi, N)
                 arr, n = W.mixed_unit_array(us, p5, [], N)
                 t = eng.submit(tids[N], arr, n)
+                sub_at[t] = (now - t_start, N)
                 if p5:
                     p = p5[0]
                     planted[t] = (len(us), p.d, p.e, p.c1, p.c2)
@@ -1169,6 +1172,7 @@ def run_serve(args, rank, world, local, dist):
                 nxt += rng.exponential(req_units / rate)
             for r in eng.poll(wait_ms=1):
                 lat += [r["latency_ms"]] * r["n_units"]
+                rows.append((*sub_at.pop(r["ticket"]), r["latency_ms"], r["n_units"]))
                 done += 1
                 if r["ticket"] in planted:
                     got = {(s.unit, s.d, s.e, s.c1, s.c2) for s in r["solutions"] if s.kind == 1}
@@ -1177,6 +1181,7 @@ def run_serve(args, rank, world, local, dist):
         while done < sent:
             for r in eng.poll(wait_ms=100):
                 lat += [r["latency_ms"]] * r["n_units"]
+                rows.append((*sub_at.pop(r["ticket"]), r["latency_ms"], r["n_units"]))
                 done += 1
                 if r["ticket"] in planted:
                     got = {(s.unit, s.d, s.e, s.c1, s.c2) for s in r["solutions"] if s.kind == 1}
@@ -1185,6 +1190,17 @@ def run_serve(args, rank, world, local, dist):
         eng.serve_stop()
     wall = time.perf_counter() - t_start
     lat = np.array(lat)
+
+    def pcts(sel):
+        """Unit-weighted p50 / p99 of the requests `sel` picks."""
+        v = np.repeat([r[2] for r in rows if sel(r)], [r[3] for r in rows if sel(r)])
+        return ({"units": int(v.size), "p50_ms": round(float(np.percentile(v, 50)), 3),
+                 "p99_ms": round(float(np.percentile(v, 99)), 3)} if v.size else None)
+
+    win = max(10.0, secs / 10)
+    windows = [dict(from_s=round(w0, 1), **pcts(lambda r, w0=w0: w0 <= r[0] < w0 + win))
+               for w0 in np.arange(0.0, secs, win) if pcts(lambda r, w0=w0: w0 <= r[0] < w0 + win)]
+    per_table = {str(N): pcts(lambda r, N=N: r[1] == N) for N in sorted(tids)}
     line = {"metric": METRIC_SERVE, "value": float(np.percentile(lat, 99)), "unit": "ms",
             "n_gpus": 1, "steps": sent, "warmup": 0, "ms_per_step": None, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
@@ -1196,6 +1212,7 @@ def run_serve(args, rank, world, local, dist):
                        "hbm_budget_gb": 150, "resident_table_gb": round(resident / 1e9, 2)},
             "p50_unit_latency_ms": float(np.percentile(lat, 50)),
             "p99_unit_latency_ms": float(np.percentile(lat, 99)),
+            "p99_ms_per_window": windows, "latency_per_table": per_table,
             "units_completed": int(lat.size), "requests": sent,
             "completed_units_per_s": lat.size / wall,
             "plants_recovered": f"{got_plants}/{len(planted)}",
