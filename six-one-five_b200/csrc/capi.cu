@@ -804,15 +804,18 @@ namespace s615 {
 
 int arena_get(s615_ctx* ctx, int k, size_t bytes, void** p) {
   if (bytes > ctx->arena_cap[k]) {
-    dev_free(ctx, ctx->arena[k], ctx->arena_cap[k]);
+    // the outgrown buffer goes to the batch pool rather than to cudaFree,
+    // whose device-wide sync (and occasional long stalls) would land on
+    // whatever else is in flight, e.g. the serving loop's other slot
+    pool_put(ctx, ctx->arena[k], ctx->arena_cap[k]);
     ctx->arena[k] = nullptr;
     ctx->arena_cap[k] = 0;
-    const size_t want = std::max<size_t>(bytes + bytes / 4, 4096);
     void* q = nullptr;
-    const int s = dev_alloc(ctx, &q, want);
+    size_t got = 0;
+    const int s = pool_get(ctx, std::max<size_t>(bytes + bytes / 4, 4096), &q, &got);
     if (s) return s;
     ctx->arena[k] = q;
-    ctx->arena_cap[k] = want;
+    ctx->arena_cap[k] = got;
   }
   *p = ctx->arena[k];
   return S615_OK;
