@@ -525,6 +525,7 @@ static int load_part(s615_ctx* ctx, const char* path, int expected_N, int layout
 }
 
 int s615_load_table(s615_ctx* ctx, const char* path, int expected_N, int layout, int* table_id) {
+  NvtxRange nvtx("s615_load_table");
   if (!ctx || !path) return S615_E_ARG;
   if (serving_blocks(ctx)) return S615_E_BUSY;
   cudaSetDevice(ctx->device);
@@ -661,6 +662,7 @@ static int save_part(s615_ctx* ctx, const DevTable* t, const char* path) {
 }
 
 int s615_build_table(s615_ctx* ctx, int N, int r, int layout, int* table_id) {
+  NvtxRange nvtx("s615_build_table");
   if (!ctx || N < 1 || N > 4 * kNSoftMax || r < 8 || r > 64) return S615_E_ARG;
   if (serving_blocks(ctx)) return S615_E_BUSY;
   cudaSetDevice(ctx->device);
@@ -873,7 +875,10 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
   b->n_items = b->n_main = 0;
   DevUnit* du = nullptr;
   size_t nd = 0;
-  if (const int s = pack_units(ctx, units, n, &du, &nd)) return s;
+  {
+    NvtxRange nvtx("pack units");
+    if (const int s = pack_units(ctx, units, n, &du, &nd)) return s;
+  }
   // Job rows per item: up to 64, fewer when the batch is small, so that its
   // items still fill the GPU (about 64 warps per SM).
   u32 job_rows = 8;
@@ -908,6 +913,7 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
   // a batch too small to fill the GPU even with 16-row items (a serving
   // request) also splits each class 2-4 row chunk four ways over its tiles
   b->parts3 = (!ctx->force_rows && !tuned.item_rows && unit_rows == 16) ? 4u : 1u;
+  nvtxRangePushA("work items");
   // Work items unit by unit in input order, on several host threads for a
   // large batch: each thread counts its range's items, then writes them in
   // place.  Ranges are cut at multiples of job_rows, where a single pass
@@ -943,7 +949,7 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
     b->host_items.reset();
     b->host_items_cap = 0;
     b->host_items.reset(new (std::nothrow) u64[std::max<size_t>(total, 1)]);
-    if (!b->host_items) return S615_E_OOM;
+    if (!b->host_items) { nvtxRangePop(); return S615_E_OOM; }
     b->host_items_cap = std::max<size_t>(total, 1);
   }
   u64* items = b->host_items.get();
@@ -962,6 +968,8 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
   // and windows, so every candidate's chunk 0 goes out before any chunk 1
   std::stable_sort(items + at[nt], items + total,
                    [](u64 a, u64 c) { return item_chunk(a) < item_chunk(c); });
+  nvtxRangePop();
+  NvtxRange upload("upload batch");
   b->n_units = nd;
   b->n_main = at[nt];
   b->n_items = total;
@@ -1010,6 +1018,7 @@ int fill_batch(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch* b) {
 extern "C" {
 
 int s615_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch** out) {
+  NvtxRange nvtx("s615_prepare");
   if (!ctx || !out || (n && !units) || n > kMaxBatchUnits) return S615_E_ARG;
   if (serving_blocks(ctx)) return S615_E_BUSY;
   cudaSetDevice(ctx->device);
@@ -1043,6 +1052,7 @@ int s615_batch_free(s615_ctx* ctx, s615_batch* b) {
 }
 
 int s615_run_batch(s615_ctx* ctx, int id, s615_batch* b, unsigned flags, void* stream) {
+  NvtxRange nvtx("s615_run_batch");
   if (!ctx || !b) return S615_E_ARG;
   DevTable* t = find_table(ctx, id);
   if (!t) return S615_E_NOTABLE;
@@ -1080,6 +1090,7 @@ int s615_run_batch(s615_ctx* ctx, int id, s615_batch* b, unsigned flags, void* s
 
 int s615_batch_results(s615_ctx* ctx, s615_batch* b, s615_hit* hits, size_t hit_cap,
                        size_t* n_hits, s615_counters* counters) {
+  NvtxRange nvtx("s615_batch_results");
   if (!ctx || !b) return S615_E_ARG;
   Cls5Counters c{};
   S615_CU(cudaStreamSynchronize(ctx->stream));
@@ -1107,6 +1118,7 @@ int s615_batch_results(s615_ctx* ctx, s615_batch* b, s615_hit* hits, size_t hit_
 // enough, so repeated calls allocate nothing.
 int s615_run(s615_ctx* ctx, int id, const s615_unit* units, size_t n, unsigned flags,
              s615_hit* hits, size_t hit_cap, size_t* n_hits, s615_counters* counters) {
+  NvtxRange nvtx("s615_run");
   if (!ctx || (n && !units) || n > kMaxBatchUnits) return S615_E_ARG;
   if (serving_blocks(ctx)) return S615_E_BUSY;
   if (!find_table(ctx, id)) return S615_E_NOTABLE;
@@ -1189,6 +1201,7 @@ int s615_cls5_run(s615_ctx* ctx, int id, const s615_unit* units, size_t n, unsig
 
 int s615_verify(s615_ctx* ctx, const s615_unit* units, size_t n_units, const s615_hit* hits,
                 size_t n_hits, int N, s615_solution* out, size_t cap, size_t* n_out) {
+  NvtxRange nvtx("s615_verify");
   if (!ctx || !n_out || N < 1) return S615_E_ARG;
   if (serving_blocks(ctx)) return S615_E_BUSY;
   cudaSetDevice(ctx->device);

@@ -1,6 +1,7 @@
 // engine.hpp -- internal types of the B200 engine (not part of the C ABI).
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <map>
@@ -14,6 +15,16 @@
 #include "s615_common.hpp"
 
 namespace s615 {
+
+// An NVTX range over a host scope, so a profiler's timeline shows the
+// engine's phases (prepare, run, results, verify, table build and load,
+// serving batches); a no-op unless a profiler is attached.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // ------------------------------------------------------------ device unit
 // One unit as the peel kernel consumes it.  Only base mod 2^128 is needed:

@@ -137,6 +137,7 @@ struct Server {
 
   // Download, verify and split one finished batch.
   void finish(Flight& f, int status) {
+    NvtxRange nvtx("serve: results + verify");
     const auto t_done = Clock::now();
     std::vector<s615_hit> hits;
     std::vector<s615_solution> sols;
@@ -228,7 +229,9 @@ struct Server {
         if (!slot_batch[slot]) slot_batch[slot] = new s615_batch();
         f.t_take = Clock::now();
         f.b = slot_batch[slot];
+        nvtxRangePushA("serve: prepare batch");
         int s = fill_batch(ctx, f.all.data(), f.all.size(), f.b);
+        nvtxRangePop();
         f.prep_ms = ms_between(f.t_take, Clock::now());
         if (s == S615_E_OOM && !flights.empty()) {   // wait for memory to free up
           put_back(f);

@@ -509,6 +509,7 @@ struct PhaseTrace {
   std::vector<std::pair<const char*, cudaEvent_t>> marks;
   explicit PhaseTrace(cudaStream_t s) : st(s) {}
   void mark(const char* name) {
+    nvtxMarkA(name);   // the phase boundary on a profiler's timeline
     if (!on) return;
     cudaEvent_t e;
     if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); return; }
