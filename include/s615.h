@@ -172,6 +172,20 @@ int s615_set_budget(s615_ctx* ctx, size_t hbm_budget);
 /* Kernel launches the engine issued since open (all of its own kernels). */
 uint64_t s615_launch_count(s615_ctx* ctx);
 
+/* Checked build (lib/libs615_checked.so, `make checked`): its kernels compare
+ * every table cell, work item, unit, shard and key index with its bound and,
+ * when one is out of range, skip the access and set a bit of
+ * S615_CHK_CELL / _ITEM / _HIT / _LIST instead.  s615_checked_build returns 1
+ * in that build and 0 in the default one; s615_check_flags waits for the
+ * device, returns the bits set since the last call in *flags and clears them
+ * (always 0 in the default build). */
+#define S615_CHK_CELL 1u   /* table cell index >= m, or shard index >= S */
+#define S615_CHK_ITEM 2u   /* work item: unit, residue or job run out of range */
+#define S615_CHK_HIT 4u    /* a hit's unit index out of range */
+#define S615_CHK_LIST 8u   /* xor build: a cell, list entry or key index out of range */
+int s615_checked_build(void);
+int s615_check_flags(s615_ctx* ctx, uint32_t* flags);
+
 /* -------------------------------------------------------------- tables */
 /* xor_load_file (fourcore_xor_store.hpp:147-181) + xor_fpr_smoke (:54-65) +
  * upload: header v2 checks, exact N (expected_N <= 0 accepts any), smoke <=16

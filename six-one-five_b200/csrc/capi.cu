@@ -385,6 +385,22 @@ int s615_close(s615_ctx* ctx) {
 
 uint64_t s615_launch_count(s615_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+int s615_checked_build(void) {
+#ifdef S615_CHECKED
+  return 1;
+#else
+  return 0;
+#endif
+}
+
+int s615_check_flags(s615_ctx* ctx, uint32_t* flags) {
+  if (!ctx || !flags) return S615_E_ARG;
+  cudaSetDevice(ctx->device);
+  S615_CU(cudaDeviceSynchronize());   // the kernels that may have set a flag are done
+  *flags = check_take_peel() | check_take_peel617() | check_take_table() | check_take_xor_build();
+  return S615_OK;
+}
+
 int s615_set_budget(s615_ctx* ctx, size_t hbm_budget) {
   if (!ctx) return S615_E_ARG;
   if (serving_blocks(ctx)) return S615_E_BUSY;

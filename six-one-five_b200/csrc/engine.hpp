@@ -265,6 +265,12 @@ void dev_free(s615_ctx* ctx, void* p, size_t bytes);
 int pool_get(s615_ctx* ctx, size_t bytes, void** p, size_t* got);
 void pool_put(s615_ctx* ctx, void* p, size_t bytes);
 void pool_release(s615_ctx* ctx);
+// The check words of the checked build (read and cleared; 0 in the default
+// build), one per compiled file whose kernels check their indices.
+unsigned check_take_peel();
+unsigned check_take_peel617();
+unsigned check_take_table();
+unsigned check_take_xor_build();
 // Grow-only scratch slot k of the context (no free, so no device-wide sync
 // once it is large enough).
 int arena_get(s615_ctx* ctx, int k, size_t bytes, void** p);

@@ -66,6 +66,7 @@ struct PeelParams {
   const DevUnit* units;
   const u64* items;
   u32 n_items;
+  u32 n_units;             // unit records (bound of every item's unit index)
   u32* work;
   s615_hit* hits;
   u32 hit_cap;
@@ -133,6 +134,7 @@ __device__ __forceinline__ void probe_batch(const PeelParams& P, const WarpSmem&
       if (I.cls == 5) { h.d = (u32)x; h.e = rowval; }
       else { h.d = rowval; h.e = (u32)x; }
       if (I.cls == kClsJobRow) {   // row r is unit unit_id + r (hits are rare: one load)
+        if (!S615_CHECK(I.unit_id + r < P.n_units, kChkHit)) return;
         h.unit = P.units[I.unit_id + r].id;
         h.d = 0;
       }
@@ -185,6 +187,7 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
     it = __shfl_sync(0xFFFFFFFFu, it, 0);
     if (it >= P.n_items) break;
     const u64 packed = P.items[it];
+    if (!S615_CHECK(item_unit(packed) < P.n_units, kChkItem)) continue;   // warp-uniform
     const DevUnit* U = P.units + item_unit(packed);
     ItemCtx I;
     I.cls = U->cls;
@@ -196,7 +199,9 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 5) k_peel(PeelParams P)
       I.mod = 1;
       I.j0 = 0;
       nrows = job_count(packed);
+      if (!S615_CHECK(item_unit(packed) + nrows <= P.n_units, kChkItem)) continue;
     } else {
+      if (!S615_CHECK(item_res(packed) < U->nres1 && U->nres1 <= 24, kChkItem)) continue;
       I.r0 = U->res1[item_res(packed)];
       I.mod = U->mod1;
       u32 jmin, jend;
@@ -436,6 +441,7 @@ int launch_main(s615_ctx* ctx, const TableView& tv, const s615_batch* b, size_t 
   P.units = b->d_units;
   P.items = b->d_items;
   P.n_items = (u32)n;
+  P.n_units = (u32)b->n_units;
   P.work = b->d_work;
   P.hits = b->d_hits;
   P.hit_cap = b->hit_cap;
@@ -514,5 +520,7 @@ int launch_peel(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flag
   }
   return S615_OK;
 }
+
+S615_CHECK_TAKE_DEFINE(check_take_peel)
 
 }  // namespace s615

@@ -69,6 +69,7 @@ struct Peel617Params {
   const DevUnit* units;
   const u64* items;
   u32 n_items;
+  u32 n_units;   // unit records (bound of every item's unit index)
   u32* work;
   s615_hit* hits;
   u32 hit_cap;
@@ -293,6 +294,7 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Par
     it = __shfl_sync(kFull, it, 0);
     if (it >= P.n_items) break;
     const u64 packed = P.items[it];
+    if (!S615_CHECK(item_unit(packed) < P.n_units, kChkItem)) continue;   // warp-uniform
     const DevUnit* U = P.units + item_unit(packed);
     Item617 I;
     I.unit_id = U->id;
@@ -305,6 +307,7 @@ __global__ void __launch_bounds__(kThreads, kSharp ? 3 : 4) k_peel617(Peel617Par
       I.r0 = 0; I.mod = 0; I.j0 = 0;
       nrows = 1;
     } else {
+      if (!S615_CHECK(item_res(packed) < U->nres1 && U->nres1 <= 24, kChkItem)) continue;
       I.r0 = U->res1[item_res(packed)];
       I.mod = U->mod1;
       u32 jmin, jend;
@@ -432,6 +435,7 @@ int launch617(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned flags,
   Peel617Params P{};
   P.tv = tv;
   P.units = b->d_units;
+  P.n_units = (u32)b->n_units;
   P.items = b->d_items + b->n_main;
   P.n_items = (u32)n;
   P.work = b->d_work + 1;
@@ -481,5 +485,7 @@ int launch_peel617(s615_ctx* ctx, const TableView& tv, s615_batch* b, unsigned f
   return sharp ? launch617<true, false>(ctx, tv, b, flags, st, grid_blocks)
                : launch617<false, false>(ctx, tv, b, flags, st, grid_blocks);
 }
+
+S615_CHECK_TAKE_DEFINE(check_take_peel617)
 
 }  // namespace s615

@@ -7,6 +7,39 @@
 
 namespace s615 {
 
+// Checked builds (-DS615_CHECKED, `make checked`: lib/libs615_checked.so).
+// Every table cell index, work item, unit index and shard index a kernel
+// uses is compared with its bound; a failed check sets a
+// bit in this file's check word (kChk*) and the access is skipped, so a bug
+// shows up as a flag the host reads (s615_check_flags), never as a trap or a
+// stray access.  In the default build S615_CHECK is `true` and costs nothing.
+// The word is per compiled file (no relocatable device code); each file
+// defines its reader with S615_CHECK_TAKE_DEFINE.
+constexpr unsigned kChkCell = 1u;      // table cell index >= m (or shard >= S)
+constexpr unsigned kChkItem = 2u;      // work item's unit / residue / job run out of range
+constexpr unsigned kChkHit = 4u;       // a hit's unit index out of range
+constexpr unsigned kChkList = 8u;      // a builder cell index (list entry, key's cells) out of range
+#ifdef S615_CHECKED
+static __device__ unsigned g_check_word;
+#define S615_CHECK(cond, bit) \
+  ((cond) ? true : (atomicOr(&::s615::g_check_word, (unsigned)(bit)), false))
+#define S615_CHECK_TAKE_DEFINE(name)                                          \
+  unsigned name() {                                                           \
+    unsigned v = 0;                                                           \
+    const unsigned z = 0;                                                     \
+    if (cudaMemcpyFromSymbol(&v, ::s615::g_check_word, sizeof v) != cudaSuccess || \
+        cudaMemcpyToSymbol(::s615::g_check_word, &z, sizeof z) != cudaSuccess) { \
+      cudaGetLastError();                                                     \
+      return 0;                                                               \
+    }                                                                         \
+    return v;                                                                 \
+  }
+#else
+#define S615_CHECK(cond, bit) true
+#define S615_CHECK_TAKE_DEFINE(name) \
+  unsigned name() { return 0; }
+#endif
+
 // Read one r-bit cell.  WIDE layouts hold one cell per aligned word, so a
 // cell is one load from one 32-byte sector.  PACKED is the file layout:
 // cell i starts at bit i*r; it is assembled from at most two aligned 64-bit
@@ -52,6 +85,8 @@ __device__ __forceinline__ bool might_contain_one(const TableView& t, u64 key) {
   const u64 h = mix64(key + t.seed);
   u64 c[3];
   cell_indices(h, t.block, t.recip, c);
+  if (!S615_CHECK(c[0] < 3 * t.block && c[1] < 3 * t.block && c[2] < 3 * t.block, kChkCell))
+    return false;
   const u64 a = load_cell(t, c[0]);
   const u64 b = load_cell(t, c[1]);
   const u64 d = load_cell(t, c[2]);
@@ -68,6 +103,7 @@ template <bool kSet>
 __device__ __forceinline__ bool probe_table(const TableView& t, u64 key) {
   if constexpr (kSet) {
     const u32 s = (u32)fast_mod(mix64(key + t.shard_seed), t.block, t.recip);
+    if (!S615_CHECK(s < t.block, kChkCell)) return false;
     if (s - t.grp_lo >= t.grp_hi - t.grp_lo) return false;
     return might_contain_one(t.parts[s], key);
   } else {

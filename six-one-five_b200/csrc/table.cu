@@ -136,4 +136,6 @@ int launch_pack(s615_ctx* ctx, const void* d_wide, int cell_bytes, u64 m, u32 r,
   return S615_OK;
 }
 
+S615_CHECK_TAKE_DEFINE(check_take_table)
+
 }  // namespace s615

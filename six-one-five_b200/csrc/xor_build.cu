@@ -125,8 +125,27 @@ constexpr u64 kMaxKeys = 1ull << 34;
 __device__ __forceinline__ u64 cnt_of(u64 w) { return w >> kCntShift; }
 __device__ __forceinline__ u64 upd(u64 idx) { return (1ull << kCntShift) + idx; }
 
+// Checked builds: the key and cell counts of the build in flight, set before
+// the incidence, bound every key index a kernel decodes (from a loop or from a
+// cell word's index sum) and the cells of the binned apply.  One build at a
+// time per process in such a build.
+#ifdef S615_CHECKED
+static __device__ u64 g_check_nkeys, g_check_ncells;
+#define S615_KEY_OK(idx) S615_CHECK((idx) < g_check_nkeys, kChkList)
+#define S615_CELL_OK(c) S615_CHECK((c) < g_check_ncells, kChkList)
+#else
+#define S615_KEY_OK(idx) true
+#define S615_CELL_OK(c) true
+#endif
+
 __device__ __forceinline__ u64 key_hash(const u64* keys, u64 idx, u64 seed) {
+  if (!S615_KEY_OK(idx)) return 0;
   return mix64(keys[idx] + seed);
+}
+
+// Checked builds: all three cells of a key lie in [0, 3 * block).
+__device__ __forceinline__ bool cells_ok(const u64* c, u64 block) {
+  return S615_CHECK(c[0] < 3 * block && c[1] < 3 * block && c[2] < 3 * block, kChkList);
 }
 
 __global__ void k_incidence(const u64* __restrict__ keys, u64 n, u64 seed, u64 block, u64 recip,
@@ -135,6 +154,7 @@ __global__ void k_incidence(const u64* __restrict__ keys, u64 n, u64 seed, u64 b
        i += (u64)gridDim.x * blockDim.x) {
     u64 c[3];
     cell_indices(key_hash(keys, i, seed), block, recip, c);
+    if (!cells_ok(c, block)) continue;
 #pragma unroll
     for (int t = 0; t < 3; ++t) atomicAdd(W + c[t], (unsigned long long)upd(i));
   }
@@ -171,6 +191,7 @@ __global__ void k_bin_count(const u64* __restrict__ keys, u64 k0, u64 per, u64 k
   for (u64 i = lo + threadIdx.x; i < hi; i += blockDim.x) {
     u64 c[3];
     cell_indices(key_hash(keys, i, seed), block, recip, c);
+    if (!cells_ok(c, block) || !S615_CHECK(((3 * block - 1) >> sbits) < S, kChkList)) continue;
 #pragma unroll
     for (int t = 0; t < 3; ++t) atomicAdd(&hist[(u32)(c[t] >> sbits)], 1u);
   }
@@ -190,6 +211,7 @@ __global__ void k_bin_scatter(const u64* __restrict__ keys, u64 k0, u64 per, u64
   for (u64 i = lo + threadIdx.x; i < hi; i += blockDim.x) {
     u64 c[3];
     cell_indices(key_hash(keys, i, seed), block, recip, c);
+    if (!cells_ok(c, block) || !S615_CHECK(((3 * block - 1) >> sbits) < S, kChkList)) continue;
 #pragma unroll
     for (int t = 0; t < 3; ++t) {
       const unsigned long long pos = atomicAdd(&cur[(u32)(c[t] >> sbits)], 1ull);
@@ -216,7 +238,8 @@ __global__ void k_bin_apply(const u32* __restrict__ ent_off, const u32* __restri
     unsigned long long* base = W + ((u64)sl << sbits);
     const u64 e1 = soff[sl + 1];
     for (u64 i = soff[sl] + tid; i < e1; i += nt)
-      atomicAdd(base + ent_off[i], (unsigned long long)upd(k0 + ent_idx[i]));
+      if (S615_KEY_OK(k0 + ent_idx[i]) && S615_CELL_OK(((u64)sl << sbits) + ent_off[i]))
+        atomicAdd(base + ent_off[i], (unsigned long long)upd(k0 + ent_idx[i]));
     if constexpr (kSync) cg::this_grid().sync();
   }
 }
@@ -285,6 +308,7 @@ __device__ __forceinline__ bool claims(const unsigned long long* W, const u64* k
   h = key_hash(keys, w & kSumMask, seed);
   u64 cs[3];
   cell_indices(h, block, recip, cs);
+  if (!cells_ok(cs, block)) return false;
 #pragma unroll
   for (int t = 0; t < 3; ++t)
     if (cs[t] < c && cnt_of(W[cs[t]]) == 1) return false;
@@ -302,8 +326,10 @@ __global__ void k_claim_list(CellList cand, u64 ncand, const unsigned long long*
     u64 c = 0, w = 0, h = 0;
     if (i < ncand) {
       c = cand.off ? cand.cell(i, block) : i;
-      w = W[c];
-      claim = cnt_of(w) == 1 && claims(W, keys, seed, block, recip, c, w, h);
+      if (S615_CHECK(c < 3 * block, kChkList)) {
+        w = W[c];
+        claim = cnt_of(w) == 1 && claims(W, keys, seed, block, recip, c, w, h);
+      }
     }
     const u64 k = warp_append(claim, c, block, out.cells, n_order, order_cap, over);
     if (k != ~0ull && out.hash) {
@@ -320,7 +346,7 @@ __global__ void k_apply_list(ClaimList in, u64 L, unsigned long long* W,
     const u64 i = base + threadIdx.x;
     bool to0 = false, to1 = false;
     u64 nc0 = 0, nc1 = 0;
-    if (i < L) {
+    if (i < L && S615_CHECK(in.cells.cell(i, block) < 3 * block, kChkList)) {
       const u64 c = in.cells.cell(i, block);
       u64 idx, h;
       if (in.hash) {
@@ -334,14 +360,17 @@ __global__ void k_apply_list(ClaimList in, u64 L, unsigned long long* W,
       // 2 to 1 is a candidate of the next round
       u64 cs[3];
       cell_indices(h, block, recip, cs);
-      const int own = cs[0] == c ? 0 : cs[1] == c ? 1 : 2;
-      nc0 = cs[own == 0 ? 1 : 0];
-      nc1 = cs[own == 2 ? 1 : 2];
-      to0 = cnt_of(atomicAdd(W + nc0, (unsigned long long)(0 - upd(idx)))) == 2;
-      to1 = cnt_of(atomicAdd(W + nc1, (unsigned long long)(0 - upd(idx)))) == 2;
-      // count 0; without the recorded index the word keeps it for the fill
-      W[c] = in.hash ? 0ull : idx;
+      if (cells_ok(cs, block) && S615_KEY_OK(idx)) {   // always true in the default build
+        const int own = cs[0] == c ? 0 : cs[1] == c ? 1 : 2;
+        nc0 = cs[own == 0 ? 1 : 0];
+        nc1 = cs[own == 2 ? 1 : 2];
+        to0 = cnt_of(atomicAdd(W + nc0, (unsigned long long)(0 - upd(idx)))) == 2;
+        to1 = cnt_of(atomicAdd(W + nc1, (unsigned long long)(0 - upd(idx)))) == 2;
+        // count 0; without the recorded index the word keeps it for the fill
+        W[c] = in.hash ? 0ull : idx;
+      }
     }
+    // every lane reaches both appends (they are warp-collective)
     warp_append(to0, nc0, block, next, n_next, next_cap, over);
     warp_append(to1, nc1, block, next, n_next, next_cap, over);
   }
@@ -354,6 +383,7 @@ __device__ __forceinline__ void fill_cell(unsigned long long* W, u64 h, u64 bloc
                                           u64 mask, u64 c) {
   u64 cs[3];
   cell_indices(h, block, recip, cs);
+  if (!cells_ok(cs, block) || !S615_CHECK(c < 3 * block, kChkList)) return;
   u64 v = h & mask;
 #pragma unroll
   for (int t = 0; t < 3; ++t)
@@ -377,6 +407,7 @@ __device__ __forceinline__ void remove_key_scan(unsigned long long* W, const u64
   const u64 idx = W[c] & kSumMask;
   u64 cs[3];
   cell_indices(key_hash(keys, idx, seed), block, recip, cs);
+  if (!cells_ok(cs, block) || !S615_KEY_OK(idx)) return;
 #pragma unroll
   for (int t = 0; t < 3; ++t)
     if (cs[t] != c) atomicAdd(W + cs[t], (unsigned long long)(0 - upd(idx)));
@@ -629,6 +660,10 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
   const u64 m = capacity_for(n);
   const u64 block = m / 3, recip = mod_recip(block);
   if (n > kMaxKeys) return S615_E_BUILD;   // key indices must stay below 2^34
+#ifdef S615_CHECKED
+  S615_CU(cudaMemcpyToSymbolAsync(g_check_nkeys, &n, sizeof n, 0, cudaMemcpyHostToDevice, st));
+  S615_CU(cudaMemcpyToSymbolAsync(g_check_ncells, &m, sizeof m, 0, cudaMemcpyHostToDevice, st));
+#endif
   Buf cells(ctx), rounds(ctx), scratch(ctx), order(ctx), front(ctx);
   int s = cells.alloc(m * sizeof(u64));
   if (s) return s;
@@ -865,5 +900,7 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
   S615_CU(cudaGetLastError());
   return S615_OK;
 }
+
+S615_CHECK_TAKE_DEFINE(check_take_xor_build)
 
 }  // namespace s615

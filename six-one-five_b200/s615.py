@@ -14,7 +14,10 @@ from typing import Iterable, List, Optional, Sequence, Tuple
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libs615.so")
+# S615_CHECKED=1 loads the checked build (`make -C six-one-five_b200 checked`):
+# the same library whose kernels check every index they use (s615_check_flags).
+LIB_PATH = os.path.join(HERE, "lib", "libs615_checked.so" if os.environ.get("S615_CHECKED") == "1"
+                        else "libs615.so")
 
 S615_OK = 0
 STATUS = {
@@ -96,6 +99,8 @@ SIGNATURES = {
     "s615_open": (C.c_int, [C.c_int, C.c_size_t, C.POINTER(_P)]),
     "s615_close": (C.c_int, [_P]),
     "s615_launch_count": (C.c_uint64, [_P]),
+    "s615_checked_build": (C.c_int, []),
+    "s615_check_flags": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
     "s615_set_budget": (C.c_int, [_P, C.c_size_t]),
     "s615_load_table": (C.c_int, [_P, C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_int)]),
     "s615_build_table": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int)]),
@@ -174,7 +179,8 @@ def lib() -> C.CDLL:
     global _lib
     if _lib is None:
         if not os.path.exists(LIB_PATH):
-            raise OSError(f"{LIB_PATH} missing: run `make -C six-one-five_b200`")
+            raise OSError(f"{LIB_PATH} missing: run `make -C six-one-five_b200`"
+                          + (" checked" if LIB_PATH.endswith("_checked.so") else ""))
         L = C.CDLL(LIB_PATH)
         for name, (res, args) in SIGNATURES.items():
             fn = getattr(L, name)
@@ -503,6 +509,13 @@ class Engine:
     @property
     def launches(self) -> int:
         return int(lib().s615_launch_count(self._ctx))
+
+    def check_flags(self) -> int:
+        """S615_CHK_* bits the checked build's kernels set since the last call
+        (0 in the default build)."""
+        f = C.c_uint32(0)
+        _check(lib().s615_check_flags(self._ctx, C.byref(f)), "check_flags")
+        return f.value
 
     # ---- tables ----
     def load_table(self, path: str, expected_N: int = 0, layout: int = LAYOUT_AUTO) -> int:
