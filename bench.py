@@ -554,7 +554,6 @@ def run617(args, rank, world, local, dist):
     import shard
     total_ms, tot = shard.merge(dist, "cuda", total_ms,
                                 {"probes": ctr.probes, "pos": ctr.pos, "B": len(Bs)})
-    ref_probes = 3 * ctr.probes                     # the reference's "probes" (3 per call)
     value = 3 * tot["probes"] * args.steps / (total_ms / 1e3)
     step_s = total_ms / args.steps / 1e3
 
@@ -565,6 +564,8 @@ def run617(args, rank, world, local, dist):
         h2, c2 = eng.run(tid, units, n, hit_cap=1 << 16)
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     assert c2.probes == ctr.probes and c2.tri_total == ctr.tri_total
+    # whole job over the ranks: the slowest rank's e2e step against all ranks' probes
+    e2e_ms, e2e_job = shard.merge(dist, "cuda", e2e_s * 1e3, {"probes": ctr.probes})
 
     sharp = None
     if rank == 0:
@@ -624,7 +625,7 @@ def run617(args, rank, world, local, dist):
                      "tri_total": ctr.tri_total, "tri_skipped": ctr.tri_skipped, "hits": ctr.hits},
         "plants_recovered": f"{recovered}/{len(plants)}", "solutions": solutions,
         "table_build_s": round(build_s, 2),
-        "e2e": {"value": ref_probes / e2e_s, "unit": UNIT617,
+        "e2e": {"value": 3 * e2e_job["probes"] / (e2e_ms / 1e3), "unit": UNIT617,
                 "h2d_bytes_per_step": batch_h2d(lib, batch),
                 "d2h_bytes_per_step": C.sizeof(s615.Counters) + len(h2) * 32},
         "gpu_launches": launches,
@@ -869,8 +870,13 @@ def run_mix(args, rank, world, local, dist):
     e2e_s = time.perf_counter() - t0
     assert c2.pos == ctr.pos and c2.probes == ctr.probes
     import collections
+
+    import shard
     mix = collections.Counter(c for c, _, _ in units)
-    step_s = ms / args.steps / 1e3
+    # whole job over the ranks: the slowest rank's time against all ranks' units
+    job_ms, job = shard.merge(dist, "cuda", ms, {"units": n})
+    e2e_ms, e2e_job = shard.merge(dist, "cuda", e2e_s * 1e3, {"units": n})
+    step_s = job_ms / args.steps / 1e3
     # the probe's roofline for one launch (all steps are the same pass)
     peak, peak_kind = measured_peaks()
     per_s = (ms / args.steps) / 1e3
@@ -880,8 +886,8 @@ def run_mix(args, rank, world, local, dist):
                 "traffic": None, "algorithmic_bytes_per_launch": ctr.probes * PROBE_BYTES,
                 "random_access": random_access_roof(lib, eng, tid, stream, ctr.probes, per_s)
                 if rank == 0 else None}
-    line = {"metric": METRIC_MIX, "value": n / step_s, "unit": "units/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+    line = {"metric": METRIC_MIX, "value": job["units"] / step_s, "unit": "units/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": job_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic",
             "config": {"workload": f"{len(units)} Stage-1 units {dict(sorted(mix.items()))} + 64 plants, "
@@ -893,7 +899,8 @@ def run_mix(args, rank, world, local, dist):
             "plants_recovered": f"{rec5 + rec24}/{len(p5) + len(p24)}",
             "solutions": [s615.solution_line(s) for s in sols if s.kind == 0],
             "table_build_s": round(build_s, 2),
-            "e2e": {"value": n / e2e_s, "unit": "units/s", "h2d_bytes_per_step": batch_h2d(lib, batch),
+            "e2e": {"value": e2e_job["units"] / (e2e_ms / 1e3), "unit": "units/s",
+                    "h2d_bytes_per_step": batch_h2d(lib, batch),
                     "d2h_bytes_per_step": C.sizeof(s615.Counters) + len(h2) * C.sizeof(s615.Hit)},
             "gpu_launches": launches, "roofline": mix_roof, "cpu_baseline": None,
             "sharp_gate": sharp, "clocks": cl}
@@ -1055,6 +1062,7 @@ def run_jobs(args, rank, world, local, dist):
     import collections
     import shard
     total_ms, tot = shard.merge(dist, "cuda", total_ms, {"jobs": n})
+    e2e_ms, e2e_job = shard.merge(dist, "cuda", e2e_s * 1e3, {"jobs": n})
     step_s = total_ms / args.steps / 1e3
     peak, peak_kind = measured_peaks()
     achieved = ctr.probes * PROBE_BYTES / (statistics.mean(per_ms) / 1e3) / 1e9
@@ -1079,7 +1087,7 @@ def run_jobs(args, rank, world, local, dist):
             "host": {"expand_s": round(expand_s, 2), "fail_t": fail_t, "bbj_write_s": round(write_s, 2),
                      "bbj_read_s": round(read_s, 2), "bbj_bytes": file_bytes},
             "table_build_s": round(build_s, 2),
-            "e2e": {"value": n / e2e_s, "unit": "jobs/s", "h2d_bytes_per_step": h2d,
+            "e2e": {"value": e2e_job["jobs"] / (e2e_ms / 1e3), "unit": "jobs/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": C.sizeof(s615.Counters) + len(h3) * C.sizeof(s615.Hit),
                     "includes": ".bbj read + s615_run", "phases": e2e_phases},
             "gpu_launches": launches,
@@ -1363,6 +1371,11 @@ def main():
         f"(device step {total_ms / args.steps:.1f} ms)")
     assert c2.pos == ctr.pos and c2.probes == ctr.probes and len(sols2) == len(sols)
     d2h = C.sizeof(s615.Counters) + len(h2) * 32
+    # whole-job e2e over the ranks: the slowest rank's e2e step (MAX) against
+    # the job's points (pos_all: summed over replica bands; a shard split's
+    # ranks search the same points), with every rank's copies counted
+    e2e_ms, e2e_bytes = shard.merge(dist, "cuda", e2e_s * 1e3, {"h2d": h2d, "d2h": d2h})
+    e2e_job_s = e2e_ms / 1e3
     # where the e2e step goes: the same work as s615_run, one C-ABI call per phase
     e2e_phases = None
     if rank == 0:
@@ -1522,7 +1535,7 @@ def main():
                                    else f"replicas-by-band x{world}")},
         "eligible_B_per_hour": eligible * args.steps / (total_ms / 1e3) * 3600,
         # the same through the C ABI with host buffers, exact verification included
-        "eligible_B_per_hour_e2e_with_verify": (eligible / world) / e2e_s * 3600,
+        "eligible_B_per_hour_e2e_with_verify": eligible / e2e_job_s * 3600,
         "p99_unit_latency_ms": serve["p99_ms"] if serve else None,
         "p50_unit_latency_ms": serve["p50_ms"] if serve else None,
         "serving": serve,
@@ -1532,8 +1545,8 @@ def main():
                      "pos": pos_all},
         "plants_recovered": f"{recovered}/{N_PLANTS}", "solutions": solutions,
         "table_build_s": round(build_s, 2),
-        "e2e": {"value": ctr.pos / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "phases": e2e_phases},
+        "e2e": {"value": pos_all / e2e_job_s, "unit": UNIT, "h2d_bytes_per_step": e2e_bytes["h2d"],
+                "d2h_bytes_per_step": e2e_bytes["d2h"], "phases": e2e_phases},
         "gpu_launches": launches,
         "roofline": roof,
         "cpu_baseline": cpu,
