@@ -191,3 +191,27 @@ def test_l2_window_does_not_change_results(engine, oracle_table, config1):
         np.testing.assert_array_equal(sorted_hits(h0), sorted_hits(h1))
     finally:
         engine.free_table(tid)
+
+
+def test_reference_selftest_plants(engine):
+    """The reference's GPU self-test recipe (solve_516_v3.cu:1149-1170): 512
+    class-5 plants, base = (14e)^6 + (21d)^6 + 42^6 (i^6 + j^6) with e in
+    [1, 280], d in [1, 190] and i != j <= 4096, each unit a single residue per
+    axis with fmax the planted value; every one must be found and verified."""
+    N = 4096
+    tid = engine.build_table(N, 48)
+    try:
+        rng = np.random.RandomState(1149)
+        ps = []
+        while len(ps) < 512:
+            e, d = int(rng.randint(1, 281)), int(rng.randint(1, 191))
+            i, j = (int(x) for x in rng.randint(1, N + 1, 2))
+            if i != j:
+                ps.append(W.Plant(172_049, 6, e, d, min(i, j), max(i, j)))
+        arr, n = W.unit_array([], ps, N)
+        hits, ctr = engine.cls5_run(tid, arr, n)
+        sols = engine.verify(arr, n, hits, N)
+        got = {(s.unit, s.d, s.e, s.c1, s.c2) for s in sols if s.kind == 1}
+        assert sum((k, p.d, p.e, p.c1, p.c2) in got for k, p in enumerate(ps)) == 512
+    finally:
+        engine.free_table(tid)
