@@ -37,13 +37,21 @@ int dev_alloc(s615_ctx* ctx, void** p, size_t bytes) {
   *p = nullptr;
   if (bytes == 0) bytes = 16;
   for (int attempt = 0;; ++attempt) {
-    if (!ctx->budget || ctx->used + bytes <= ctx->budget) {
-      if (cudaMalloc(p, bytes) == cudaSuccess) {
-        ctx->used += bytes;
-        return S615_OK;
+    // reserve the bytes against the budget first, so that threads allocating
+    // at once cannot overrun it together
+    bool reserved = false;
+    size_t cur = ctx->used.load();
+    while (!ctx->budget || cur + bytes <= ctx->budget) {
+      if (ctx->used.compare_exchange_weak(cur, cur + bytes)) {
+        reserved = true;
+        break;
       }
+    }
+    if (reserved) {
+      if (cudaMalloc(p, bytes) == cudaSuccess) return S615_OK;
       cudaGetLastError();
       *p = nullptr;
+      ctx->used.fetch_sub(bytes);
     }
     if (attempt > 0 || !release_run_batch(ctx)) return S615_E_OOM;
   }
@@ -53,7 +61,9 @@ void dev_free(s615_ctx* ctx, void* p, size_t bytes) {
   if (!p) return;
   if (bytes == 0) bytes = 16;
   cudaFree(p);
-  ctx->used -= std::min(ctx->used, bytes);
+  size_t cur = ctx->used.load();
+  while (!ctx->used.compare_exchange_weak(cur, cur - std::min(cur, bytes))) {
+  }
 }
 
 bool release_run_batch(s615_ctx* ctx) {
@@ -234,7 +244,7 @@ int pick_layout(s615_ctx* ctx, int want, u64 m, u32 r, int* cell_bytes) {
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
   const size_t wide = m * (size_t)(*cell_bytes) + packed_bytes(m, r) + ((size_t)4 << 30);
-  const size_t room = std::min(free_b, ctx->budget ? ctx->budget - std::min(ctx->budget, ctx->used) : free_b);
+  const size_t room = std::min(free_b, ctx->budget ? ctx->budget - std::min(ctx->budget, ctx->used.load()) : free_b);
   if (wide <= room) return S615_LAYOUT_WIDE;
   *cell_bytes = 0;
   return S615_LAYOUT_PACKED;

@@ -4,6 +4,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -194,7 +195,10 @@ struct HostStage {
 
 struct s615_ctx {
   int device = 0;
-  size_t budget = 0, used = 0;
+  size_t budget = 0;
+  // device bytes held against the budget; updated by the caller's threads and
+  // the serving worker (dev_alloc reserves before it allocates)
+  std::atomic<size_t> used{0};
   cudaStream_t stream = nullptr;
   std::map<int, s615::DevTable> tables;
   int next_table = 1;

@@ -43,6 +43,12 @@ namespace cg = cooperative_groups;
 
 constexpr u64 kEmpty = ~0ULL;
 
+// Bytes the context's HBM budget still allows (one read of the shared count).
+size_t budget_room(const s615_ctx* ctx) {
+  const size_t u = ctx->used.load();
+  return ctx->budget > u ? ctx->budget - u : 0;
+}
+
 int grid_for(s615_ctx* ctx, u64 n, int threads) {
   const u64 want = (n + threads - 1) / threads;
   const u64 cap = (u64)ctx->num_sms * 16;
@@ -593,7 +599,7 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
     release_run_batch(ctx);   // a table needs the room more than s615_run's kept buffers
     size_t free_b = 0, total_b = 0;
     S615_CU(cudaMemGetInfo(&free_b, &total_b));
-    size_t avail = std::min(free_b, ctx->budget > ctx->used ? ctx->budget - ctx->used : (size_t)0);
+    size_t avail = std::min(free_b, budget_room(ctx));
     if (avail > ((size_t)2 << 30)) avail -= (size_t)2 << 30;
     u32 part_bits = 0;
     u64 tsize = pow2_at_least(std::max<u64>(2 * n_raw, 1024));
@@ -694,7 +700,7 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
   auto avail_now = [&]() -> size_t {
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { cudaGetLastError(); return 0; }
-    size_t a = std::min(free_b, ctx->budget > ctx->used ? ctx->budget - ctx->used : (size_t)0);
+    size_t a = std::min(free_b, budget_room(ctx));
     const size_t margin = (size_t)2 << 30;
     return a > margin ? a - margin : 0;
   };
