@@ -859,12 +859,19 @@ static size_t host_threads(size_t n) {
   return std::max<size_t>(1, std::min<size_t>({hw, 32, n / 8192}));
 }
 
-// Run work(t) for t in [0, nt) on nt threads (inline when nt == 1).
+// Run work(t) for t in [0, nt) on nt threads (inline when nt == 1).  A range
+// whose thread cannot be started (the process is out of threads) runs on the
+// calling thread instead, so no exception leaves the C ABI.
 template <class F>
 static void run_threads(size_t nt, F&& work) {
   if (nt == 1) { work(0); return; }
   std::vector<std::thread> th;
-  for (size_t t = 0; t < nt; ++t) th.emplace_back(work, t);
+  size_t t = 0;
+  try {
+    for (; t < nt; ++t) th.emplace_back(work, t);
+  } catch (...) {
+  }
+  for (size_t k = t; k < nt; ++k) work(k);
   for (auto& x : th) x.join();
 }
 
