@@ -1075,6 +1075,11 @@ int s615_batch_size(const s615_batch* b, size_t* n_units, size_t* n_items, size_
 
 int s615_batch_free(s615_ctx* ctx, s615_batch* b) {
   if (!ctx || !b) return S615_E_ARG;
+  if (b->done) {   // its last launch has finished before another batch may reuse its buffers
+    cudaEventSynchronize(b->done);
+    cudaEventDestroy(b->done);
+    b->done = nullptr;
+  }
   // the device buffers go to the context's pool for the next batch
   pool_put(ctx, b->d_units, b->units_bytes);
   pool_put(ctx, b->d_items, b->items_bytes);
@@ -1091,13 +1096,27 @@ int s615_run_batch(s615_ctx* ctx, int id, s615_batch* b, unsigned flags, void* s
   if (!t) return S615_E_NOTABLE;
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
   const TableView tv = view_of(*t);
+  // after the launches: an event that s615_batch_free waits on before the
+  // batch's buffers go to the pool (the caller may free without a sync)
+  auto mark_done = [&]() {
+    if (!b->done && cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      b->done = nullptr;
+    }
+    if (b->done) cudaEventRecord(b->done, st);
+  };
   S615_CU(cudaMemsetAsync(b->d_ctr, 0, sizeof(Cls5Counters) + 64, st));
-  if (!(flags & S615_F_PLAIN)) return launch_peel(ctx, tv, b, flags, st, 0);
+  if (!(flags & S615_F_PLAIN)) {
+    const int s = launch_peel(ctx, tv, b, flags, st, 0);
+    mark_done();
+    return s;
+  }
   // Plain form: one unit per launch and a sync after each, like the
   // reference's per-chunk loop.  (cls 7 items go out heaviest first, so a
   // cls 7 unit's items are not contiguous: each run of them is one launch.)
   s615_batch one;   // a view of one unit's items; its vectors stay empty
   one.d_units = b->d_units;
+  one.n_units = b->n_units;
   one.d_hits = b->d_hits;
   one.hit_cap = b->hit_cap;
   one.d_ctr = b->d_ctr;
@@ -1114,10 +1133,11 @@ int s615_run_batch(s615_ctx* ctx, int id, s615_batch* b, unsigned flags, void* s
     one.n_main = i < b->n_main ? j - i : 0;   // a unit's items are all of one kernel
     S615_CU(cudaMemsetAsync(b->d_work, 0, 8, st));
     int s = launch_peel(ctx, tv, &one, flags, st, 0);
-    if (s) return s;
+    if (s) { mark_done(); return s; }
     S615_CU(cudaStreamSynchronize(st));
     i = j;
   }
+  mark_done();
   return S615_OK;
 }
 

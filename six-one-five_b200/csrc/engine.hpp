@@ -178,6 +178,7 @@ struct s615_batch {
   // part): part p sieves every parts3-th 1024-column tile of the rows' c3 windows
   s615::u32 parts3 = 1;
   s615::u32 blocks_per_sm = 0;              // k_peel blocks per SM (0: the occupancy limit)
+  cudaEvent_t done = nullptr;   // recorded after the last s615_run_batch's launches
   // host copy of the work items: grow-only and uninitialised, written in
   // place by the fill's threads
   std::unique_ptr<s615::u64[]> host_items;

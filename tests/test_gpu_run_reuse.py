@@ -118,3 +118,41 @@ def test_prepare_free_cycles_reuse_the_pool(engine, setup):
     t2 = engine.build_table(300, 16)          # a table build empties the pool
     engine.free_table(t2)
     assert mem_free() > held
+
+
+def test_free_without_sync_does_not_hand_over_live_buffers(engine):
+    """s615_batch_free right after an asynchronous s615_run_batch: the batch's
+    buffers go to the pool only once its kernel is done, so the next batch,
+    which takes them, gets its own results (a kernel still running would keep
+    writing its counters and hits into them)."""
+    import torch
+    N = 23810                                   # B <= 1,000,020
+    tid = engine.build_table(N, 48)
+    lib = s615.lib()
+    try:
+        ua = W.cls5_units(1_000_000, 1_004_000)    # ~2e10 points: tens of ms on the device
+        ub = W.cls5_units(990_000, 990_010)
+        aa, na = W.unit_array(ua, [], N)
+        ab, nb = W.unit_array(ub, [], N)
+        want = key(*engine.run(tid, ab, nb))
+        t2 = engine.build_table(300, 16)           # an empty pool and no kept batch
+        engine.free_table(t2)
+        stream = torch.cuda.Stream()
+        for _ in range(3):
+            a = C.c_void_p()
+            s615._check(lib.s615_prepare(engine._ctx, C.cast(aa, C.c_void_p), na, C.byref(a)), "prepare")
+            s615._check(lib.s615_run_batch(engine._ctx, tid, a, 0, C.c_void_p(stream.cuda_stream)),
+                        "run_batch")
+            s615._check(lib.s615_batch_free(engine._ctx, a), "batch_free")   # no sync before it
+            b = C.c_void_p()
+            s615._check(lib.s615_prepare(engine._ctx, C.cast(ab, C.c_void_p), nb, C.byref(b)), "prepare")
+            s615._check(lib.s615_run_batch(engine._ctx, tid, b, 0, None), "run_batch")
+            hits = (s615.Hit * 4096)()
+            nh, ctr = C.c_size_t(0), s615.Counters()
+            s615._check(lib.s615_batch_results(engine._ctx, b, C.cast(hits, C.c_void_p), 4096,
+                                               C.byref(nh), C.byref(ctr)), "results")
+            s615._check(lib.s615_batch_free(engine._ctx, b), "batch_free")
+            assert key(s615.hits_to_array(hits, nh.value), ctr) == want
+        torch.cuda.synchronize()
+    finally:
+        engine.free_table(tid)
