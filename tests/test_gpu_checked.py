@@ -3,7 +3,7 @@
 Its kernels compare every table cell, work item, unit, shard and key index
 with its bound and record a failed check in a flag word instead of making the
 access.  This runs the main paths through that build -- class-5 units and
-plants against an oracle-built table, a mixed queue of class 2-5 units, job
+plants against an oracle-built table, the one-launch-per-unit form, a mixed queue of class 2-5 units, job
 rows and (6,1,7) candidates, the device xor builder in its list and scan forms
 and a shard set -- and requires no flag set and the results of the default
 build (the oracle's for the class-5 batch).  The checked build is loaded in a
@@ -35,7 +35,8 @@ def test_checked_build_sets_no_flag(tmp_path):
     res = json.loads(p.stdout.strip().splitlines()[-1])
     assert res["checked_build"] == 1
     assert res["flags"] == {k: 0 for k in res["flags"]}, res
-    assert res["cls5_equal_oracle"] and res["mixed_equal_parts"] and res["build_fn0"]
+    assert res["cls5_equal_oracle"] and res["plain_equal"] and res["mixed_equal_parts"]
+    assert res["build_fn0"]
 
 
 def _child(tmp):
@@ -65,6 +66,12 @@ def _child(tmp):
         out["cls5_equal_oracle"] = bool((ctr.calls, ctr.gated, ctr.probes) == (calls, gated, probes)
                                         and np.array_equal(sorted_hits(hits), sorted_hits(ohits)))
         out["flags"]["cls5"] = eng.check_flags()
+        # the plain form (one launch per unit) on the first 40 units: the batched results
+        ph, pc = eng.cls5_run(tid, arr, 40, flags=s615.F_PLAIN)
+        dh, dc = eng.cls5_run(tid, arr, 40)
+        out["plain_equal"] = bool(np.array_equal(sorted_hits(ph), sorted_hits(dh))
+                                  and (pc.calls, pc.probes) == (dc.calls, dc.probes) and dc.probes > 0)
+        out["flags"]["plain"] = eng.check_flags()
 
         # one queue of class 2-5 units, job rows and (6,1,7) candidates == the parts alone
         Nm = 26000 // 42 + 1
