@@ -3,10 +3,10 @@
 Its kernels compare every table cell, work item, unit, shard and key index
 with its bound and record a failed check in a flag word instead of making the
 access.  This runs the main paths through that build -- class-5 units and
-plants against an oracle-built table, the one-launch-per-unit form, a mixed queue of class 2-5 units, job
-rows and (6,1,7) candidates, the device xor builder in its list and scan forms
-and a shard set -- and requires no flag set and the results of the default
-build (the oracle's for the class-5 batch).  The checked build is loaded in a
+plants against an oracle-built table, the one-launch-per-unit form, a mixed
+queue of class 2-5 units, job rows and (6,1,7) candidates, the device xor
+builder (binned incidence, list peel) and a shard set -- and requires no flag
+set and the results of the default build (the oracle's for the class-5 batch).  The checked build is loaded in a
 child process (the library is chosen when s615 is imported): this file run as
 a script with S615_CHECKED=1.
 """
