@@ -366,10 +366,12 @@ int s615_cls5_run(s615_ctx* ctx, int table_id, const s615_unit* units, size_t n,
 /* Device-resident form: the units are packed and uploaded once
  * (s615_prepare); each s615_run_batch is one launch on the caller's stream
  * (NULL = the context's stream); results stay on the device until
- * s615_batch_results.  s615_batch_free hands the batch's device buffers to a
- * pool on the context (up to 8 GiB), from which later batches take buffers of
- * a fitting size, so prepare/free loops stop allocating device memory; pooled
- * buffers count against the HBM budget and are given back like s615_run's. */
+ * s615_batch_results.  s615_batch_free first waits for the batch's last
+ * s615_run_batch to finish (it may be called right after the launch, with no
+ * sync), then hands the batch's device buffers to a pool on the context (up to
+ * 8 GiB), from which later batches take buffers of a fitting size, so
+ * prepare/free loops stop allocating device memory; pooled buffers count
+ * against the HBM budget and are given back like s615_run's. */
 typedef struct s615_batch s615_batch;
 int s615_prepare(s615_ctx* ctx, const s615_unit* units, size_t n, s615_batch** out);
 int s615_run_batch(s615_ctx* ctx, int table_id, s615_batch* b, unsigned flags, void* stream);
