@@ -404,6 +404,9 @@ def cpu_sample_rate(table, units, plants_n, N, budget_s=15.0, check=None):
             "_counters": (calls, gated, probes)}, sample, hits
 
 
+REF_TABLE_N = 8000   # the reference arm's host-built table (see run_reference)
+
+
 def run_reference(args, rank):
     """--impl reference: the reference's CPU path restated (oracle port of
     k_cls5_192 with the reference's per-point 192-bit peel, mod-192 gate and
@@ -418,9 +421,11 @@ def run_reference(args, rank):
     lo, hi = args.band_lo, args.band_lo + args.band_width
     units = [(B, u) for B in range(lo, hi) if math.gcd(B, 42) == 1 for u in orc.unit_candidates(B, 5)]
     # the reference's host table builder needs hours and ~100 GB at N=76,667;
-    # the reference arm probes a host-built N=2000 table (probes are ~3% of the
-    # points; the per-point 192-bit peel dominates CPU time)
-    table = orc.Table.build_pairs(2000, args.r)
+    # the reference arm probes a host-built N=8,000 table instead (~240 MB, past
+    # the host's last-level cache, so the probes are DRAM reads as they are on
+    # the band's table; probes are ~3% of the points and the per-point 192-bit
+    # peel dominates CPU time)
+    table = orc.Table.build_pairs(REF_TABLE_N, args.r)
     cores = os.cpu_count() or 1
     rates, samples = [], []
     for s in range(args.warmup + args.steps):
@@ -443,7 +448,7 @@ def run_reference(args, rank):
             "config": {"workload": f"cls5 band B in [{lo}, {hi}), Stage-1 units (oracle rule); "
                                    f"reference arm: the oracle port of k_cls5_192 on {samples[0]} "
                                    f"evenly spaced units per step ({samples[0] // cores} per host "
-                                   f"thread) against a host-built N=2000 r={args.r} table "
+                                   f"thread) against a host-built N={REF_TABLE_N} r={args.r} table "
                                    f"(the engine arm probes N=76,667)"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": f"{samples[0]} units per step x {args.steps} steps"},
