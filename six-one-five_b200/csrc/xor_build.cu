@@ -27,6 +27,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -788,7 +790,15 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
       u64 total = 0, ncand = m;
       CellList cand{nullptr, nullptr};   // round 1 scans every cell
       int cur = 0;
+      // S615_TRACE: per round, the candidates, the keys claimed and the host
+      // time of its claim and apply (each ends in a sync here anyway)
+      using TClock = std::chrono::steady_clock;
+      const auto ms_since = [](TClock::time_point a) {
+        return std::chrono::duration<double, std::milli>(TClock::now() - a).count();
+      };
+      std::vector<std::array<double, 4>> rounds_trace;
       while (off.size() <= 0xFFFE) {
+        const auto t_claim = TClock::now();
         k_claim_list<<<grid_for(ctx, ncand, 256), 256, 0, st>>>(cand, ncand, W, K, seed, block,
                                                                 recip, claim_list, d_norder, n,
                                                                 d_lover);
@@ -798,6 +808,8 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
         S615_CU(cudaMemcpyAsync(&h_n[0], d_norder, 8, cudaMemcpyDeviceToHost, st));
         S615_CU(cudaStreamSynchronize(st));
         const u64 L = h_n[0] - total;
+        const double claim_ms = trace.on ? ms_since(t_claim) : 0.0;
+        const auto t_apply = TClock::now();
         if (L == 0) break;
         S615_CU(cudaMemsetAsync(d_nnext, 0, 8, st));
         S615_CU(cudaMemsetAsync(d_lover, 0, 4, st));
@@ -809,6 +821,7 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
         S615_CU(cudaMemcpyAsync(&h_n[1], d_nnext, 8, cudaMemcpyDeviceToHost, st));
         S615_CU(cudaMemcpyAsync(&h_lover, d_lover, 4, cudaMemcpyDeviceToHost, st));
         S615_CU(cudaStreamSynchronize(st));
+        if (trace.on) rounds_trace.push_back({(double)ncand, (double)L, claim_ms, ms_since(t_apply)});
         total += L;
         off.push_back(total);
         cur ^= 1;
@@ -822,6 +835,11 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
           if (ncand == 0) break;   // nothing became count 1: the peel is over
         }
       }
+      if (trace.on)
+        for (size_t q = 0; q < rounds_trace.size(); ++q)
+          std::fprintf(stderr, "[xor-build] round %zu: candidates=%.0f claimed=%.0f claim=%.2fms apply=%.2fms\n",
+                       q + 1, rounds_trace[q][0], rounds_trace[q][1], rounds_trace[q][2],
+                       rounds_trace[q][3]);
       if (total != n) continue;   // 2-core not empty: next seed
       trace.mark("peel");
       for (size_t q = off.size() - 1; q >= 1; --q) {
