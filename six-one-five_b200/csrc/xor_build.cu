@@ -275,26 +275,57 @@ struct CellList {
   __device__ __forceinline__ u64 cell(u64 k, u64 block) const { return third[k] * block + off[k]; }
 };
 
-// Append the flagged lanes' cells (every lane of the warp calls this).
-__device__ __forceinline__ u64 warp_append(bool take, u64 c, u64 block, CellList list,
-                                           unsigned long long* count, u64 cap, u32* over) {
-  const u32 ballot = __ballot_sync(0xFFFFFFFFu, take);
-  if (!ballot) return ~0ull;
-  const u32 lane = threadIdx.x & 31;
-  const int leader = __ffs(ballot) - 1;
-  unsigned long long base = 0;
-  if ((int)lane == leader) base = atomicAdd(count, (unsigned long long)__popc(ballot));
-  base = __shfl_sync(0xFFFFFFFFu, base, leader);
-  if (!take) return ~0ull;
-  const u64 k = base + __popc(ballot & ((1u << lane) - 1u));
-  if (k >= cap) {
-    *over = 1;
-    return ~0ull;
+// Append up to two flagged cells per thread with ONE global atomic per block:
+// each warp's count goes to shared memory, thread 0 reserves the block's
+// total, and every lane writes at its offset.  All appends of a list go
+// through one counter, so per-warp atomics on it serialise in its L2 slice:
+// at ~1.7e8 such atomics/s they bound the round's apply (ncu: DRAM 11%, L2 5%,
+// 578 long-scoreboard stall cycles per issue); per block they are 8x fewer.
+// Every thread of the block calls this (it synchronises the block); it
+// returns the first entry's position, or ~0 when not taken or over capacity.
+__device__ __forceinline__ u64 block_append(bool take0, u64 c0, bool take1, u64 c1, u64 block,
+                                            CellList list, unsigned long long* count, u64 cap,
+                                            u32* over) {
+  __shared__ u32 s_cnt[32];
+  __shared__ unsigned long long s_base;
+  const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  const u32 b0 = __ballot_sync(0xFFFFFFFFu, take0), b1 = __ballot_sync(0xFFFFFFFFu, take1);
+  __syncthreads();   // the previous call's offsets have been read
+  if (lane == 0) s_cnt[wid] = __popc(b0) + __popc(b1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    u32 tot = 0;
+    for (u32 w = 0; w < nw; ++w) {
+      const u32 k = s_cnt[w];
+      s_cnt[w] = tot;
+      tot += k;
+    }
+    s_base = tot ? atomicAdd(count, (unsigned long long)tot) : 0ull;
   }
-  const u32 t = c >= 2 * block ? 2u : c >= block ? 1u : 0u;
-  list.off[k] = (u32)(c - t * block);
-  list.third[k] = (u8)t;
-  return k;
+  __syncthreads();
+  const u64 at0 = s_base + s_cnt[wid] + __popc(b0 & ((1u << lane) - 1u));
+  const u64 at1 = s_base + s_cnt[wid] + __popc(b0) + __popc(b1 & ((1u << lane) - 1u));
+  u64 first = ~0ull;
+  if (take0) {
+    if (at0 < cap) {
+      const u32 t = c0 >= 2 * block ? 2u : c0 >= block ? 1u : 0u;
+      list.off[at0] = (u32)(c0 - t * block);
+      list.third[at0] = (u8)t;
+      first = at0;
+    } else {
+      *over = 1;
+    }
+  }
+  if (take1) {
+    if (at1 < cap) {
+      const u32 t = c1 >= 2 * block ? 2u : c1 >= block ? 1u : 0u;
+      list.off[at1] = (u32)(c1 - t * block);
+      list.third[at1] = (u8)t;
+    } else {
+      *over = 1;
+    }
+  }
+  return first;
 }
 
 // The claimed cells of the peel, in round order.  With idx and hash set
@@ -339,7 +370,7 @@ __global__ void k_claim_list(CellList cand, u64 ncand, const unsigned long long*
         claim = cnt_of(w) == 1 && claims(W, keys, seed, block, recip, c, w, h);
       }
     }
-    const u64 k = warp_append(claim, c, block, out.cells, n_order, order_cap, over);
+    const u64 k = block_append(claim, c, false, 0, block, out.cells, n_order, order_cap, over);
     if (k != ~0ull && out.hash) {
       out.idx[k] = (u32)(w & kSumMask);
       out.hash[k] = h;
@@ -378,9 +409,8 @@ __global__ void k_apply_list(ClaimList in, u64 L, unsigned long long* W,
         W[c] = in.hash ? 0ull : idx;
       }
     }
-    // every lane reaches both appends (they are warp-collective)
-    warp_append(to0, nc0, block, next, n_next, next_cap, over);
-    warp_append(to1, nc1, block, next, n_next, next_cap, over);
+    // every thread of the block reaches the append (it synchronises the block)
+    block_append(to0, nc0, to1, nc1, block, next, n_next, next_cap, over);
   }
 }
 
