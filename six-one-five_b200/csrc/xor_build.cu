@@ -103,17 +103,38 @@ __global__ void k_insert_keys(const u64* __restrict__ keys, u64 n, unsigned long
 
 // Append occupied slots to out (order irrelevant); slots past cap are
 // counted, not written.
+// The flagged threads' positions in a list whose length is *count, with ONE
+// global atomic per block (a shared-memory scan of the warps' counts): the
+// lists' counters are single addresses, and per-warp atomics on them
+// serialise in their L2 slice.  Every thread of the block calls this (it
+// synchronises the block); ~0 for a thread that takes nothing.
+__device__ __forceinline__ u64 block_reserve(bool take, unsigned long long* count) {
+  __shared__ u32 s_cnt[32];
+  __shared__ unsigned long long s_base;
+  const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  const u32 b = __ballot_sync(0xFFFFFFFFu, take);
+  __syncthreads();   // the previous call's offsets have been read
+  if (lane == 0) s_cnt[wid] = __popc(b);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    u32 tot = 0;
+    for (u32 w = 0; w < nw; ++w) {
+      const u32 k = s_cnt[w];
+      s_cnt[w] = tot;
+      tot += k;
+    }
+    s_base = tot ? atomicAdd(count, (unsigned long long)tot) : 0ull;
+  }
+  __syncthreads();
+  return take ? s_base + s_cnt[wid] + __popc(b & ((1u << lane) - 1u)) : ~0ull;
+}
+
 __global__ void k_compact(const unsigned long long* __restrict__ table, u64 tsize,
                           u64* __restrict__ out, u64 cap, unsigned long long* n_out) {
-  const u32 lane = threadIdx.x & 31;
   for (u64 i0 = blockIdx.x * (u64)blockDim.x; i0 < tsize; i0 += (u64)gridDim.x * blockDim.x) {
     const u64 i = i0 + threadIdx.x;
     const bool occ = i < tsize && table[i] != kEmpty;
-    const u32 ballot = __ballot_sync(0xFFFFFFFFu, occ);
-    unsigned long long base = 0;
-    if (lane == 0 && ballot) base = atomicAdd(n_out, (unsigned long long)__popc(ballot));
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    const u64 k = base + __popc(ballot & ((1u << lane) - 1u));
+    const u64 k = block_reserve(occ, n_out);   // every thread of the block, every pass
     if (occ && k < cap) out[k] = table[i];
   }
 }
@@ -456,7 +477,6 @@ __device__ __forceinline__ void remove_key_scan(unsigned long long* W, const u64
 __global__ void k_claim_scan(const unsigned long long* __restrict__ W, const u64* __restrict__ keys,
                              u64 seed, u16* __restrict__ round, u64 m, u64 block, u64 recip, u16 r,
                              unsigned long long* n_claimed) {
-  const u32 lane = threadIdx.x & 31;
   for (u64 c0 = blockIdx.x * (u64)blockDim.x; c0 < m; c0 += (u64)gridDim.x * blockDim.x) {
     const u64 c = c0 + threadIdx.x;
     bool claim = false;
@@ -466,8 +486,7 @@ __global__ void k_claim_scan(const unsigned long long* __restrict__ W, const u64
       claim = cnt_of(w) == 1 && claims(W, keys, seed, block, recip, c, w, h);
       if (claim) round[c] = r;
     }
-    const u32 ballot = __ballot_sync(0xFFFFFFFFu, claim);
-    if (lane == 0 && ballot) atomicAdd(n_claimed, (unsigned long long)__popc(ballot));
+    block_reserve(claim, n_claimed);   // counts the claims (every thread, every pass)
   }
 }
 
