@@ -399,39 +399,103 @@ __global__ void k_claim_list(CellList cand, u64 ncand, const unsigned long long*
   }
 }
 
+// Claimed keys a thread applies per pass of k_apply_list: their eight atomics
+// are in flight together, and the block synchronises (in the append) once
+// per pass instead of once per key.
+constexpr int kApplyPer = 4;
+
+// block_append for K cells per thread (flags take[k], cells c[k]), one global
+// atomic per block; every thread of the block calls it.
+template <int K>
+__device__ __forceinline__ void block_append_n(const bool (&take)[K], const u64 (&c)[K], u64 block,
+                                               CellList list, unsigned long long* count, u64 cap,
+                                               u32* over) {
+  __shared__ u32 s_cnt[32];
+  __shared__ unsigned long long s_base;
+  const u32 lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  u32 b[K];
+  u32 wtot = 0;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    b[k] = __ballot_sync(0xFFFFFFFFu, take[k]);
+    wtot += __popc(b[k]);
+  }
+  __syncthreads();   // the previous call's offsets have been read
+  if (lane == 0) s_cnt[wid] = wtot;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    u32 tot = 0;
+    for (u32 w = 0; w < nw; ++w) {
+      const u32 n = s_cnt[w];
+      s_cnt[w] = tot;
+      tot += n;
+    }
+    s_base = tot ? atomicAdd(count, (unsigned long long)tot) : 0ull;
+  }
+  __syncthreads();
+  u64 at = s_base + s_cnt[wid];
+  const u32 below = (1u << lane) - 1u;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    if (take[k]) {
+      const u64 pos = at + __popc(b[k] & below);
+      if (pos < cap) {
+        const u32 t = c[k] >= 2 * block ? 2u : c[k] >= block ? 1u : 0u;
+        list.off[pos] = (u32)(c[k] - t * block);
+        list.third[pos] = (u8)t;
+      } else {
+        *over = 1;
+      }
+    }
+    at += __popc(b[k]);
+  }
+}
+
 __global__ void k_apply_list(ClaimList in, u64 L, unsigned long long* W,
                              const u64* __restrict__ keys, u64 seed, u64 block, u64 recip,
                              CellList next, unsigned long long* n_next, u64 next_cap, u32* over) {
-  for (u64 base = blockIdx.x * (u64)blockDim.x; base < L; base += (u64)gridDim.x * blockDim.x) {
-    const u64 i = base + threadIdx.x;
-    bool to0 = false, to1 = false;
-    u64 nc0 = 0, nc1 = 0;
-    if (i < L && S615_CHECK(in.cells.cell(i, block) < 3 * block, kChkList)) {
-      const u64 c = in.cells.cell(i, block);
-      u64 idx, h;
-      if (in.hash) {
-        idx = in.idx[i];
-        h = in.hash[i];
-      } else {
-        idx = W[c] & kSumMask;
-        h = key_hash(keys, idx, seed);
-      }
-      // remove the key from its two other cells; a cell whose count goes from
-      // 2 to 1 is a candidate of the next round
-      u64 cs[3];
-      cell_indices(h, block, recip, cs);
-      if (cells_ok(cs, block) && S615_KEY_OK(idx)) {   // always true in the default build
-        const int own = cs[0] == c ? 0 : cs[1] == c ? 1 : 2;
-        nc0 = cs[own == 0 ? 1 : 0];
-        nc1 = cs[own == 2 ? 1 : 2];
-        to0 = cnt_of(atomicAdd(W + nc0, (unsigned long long)(0 - upd(idx)))) == 2;
-        to1 = cnt_of(atomicAdd(W + nc1, (unsigned long long)(0 - upd(idx)))) == 2;
-        // count 0; without the recorded index the word keeps it for the fill
-        W[c] = in.hash ? 0ull : idx;
+  const u64 span = (u64)blockDim.x * kApplyPer;
+  for (u64 base = blockIdx.x * span; base < L; base += (u64)gridDim.x * span) {
+    bool to[2 * kApplyPer];
+    u64 nc[2 * kApplyPer];
+    u64 old[2 * kApplyPer];
+#pragma unroll
+    for (int q = 0; q < kApplyPer; ++q) {
+      to[2 * q] = to[2 * q + 1] = false;
+      nc[2 * q] = nc[2 * q + 1] = 0;
+      old[2 * q] = old[2 * q + 1] = 0;
+      const u64 i = base + (u64)q * blockDim.x + threadIdx.x;   // coalesced over the block
+      if (i < L && S615_CHECK(in.cells.cell(i, block) < 3 * block, kChkList)) {
+        const u64 c = in.cells.cell(i, block);
+        u64 idx, h;
+        if (in.hash) {
+          idx = in.idx[i];
+          h = in.hash[i];
+        } else {
+          idx = W[c] & kSumMask;
+          h = key_hash(keys, idx, seed);
+        }
+        // remove the key from its two other cells (results read below, so the
+        // atomics of all kApplyPer keys are in flight together)
+        u64 cs[3];
+        cell_indices(h, block, recip, cs);
+        if (cells_ok(cs, block) && S615_KEY_OK(idx)) {   // always true in the default build
+          const int own = cs[0] == c ? 0 : cs[1] == c ? 1 : 2;
+          nc[2 * q] = cs[own == 0 ? 1 : 0];
+          nc[2 * q + 1] = cs[own == 2 ? 1 : 2];
+          old[2 * q] = atomicAdd(W + nc[2 * q], (unsigned long long)(0 - upd(idx)));
+          old[2 * q + 1] = atomicAdd(W + nc[2 * q + 1], (unsigned long long)(0 - upd(idx)));
+          to[2 * q] = to[2 * q + 1] = true;   // pending: the count check follows
+          // count 0; without the recorded index the word keeps it for the fill
+          W[c] = in.hash ? 0ull : idx;
+        }
       }
     }
+    // a cell whose count went from 2 to 1 is a candidate of the next round
+#pragma unroll
+    for (int k = 0; k < 2 * kApplyPer; ++k) to[k] = to[k] && cnt_of(old[k]) == 2;
     // every thread of the block reaches the append (it synchronises the block)
-    block_append(to0, nc0, to1, nc1, block, next, n_next, next_cap, over);
+    block_append_n<2 * kApplyPer>(to, nc, block, next, n_next, next_cap, over);
   }
 }
 
@@ -862,7 +926,8 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
         if (L == 0) break;
         S615_CU(cudaMemsetAsync(d_nnext, 0, 8, st));
         S615_CU(cudaMemsetAsync(d_lover, 0, 4, st));
-        k_apply_list<<<grid_for(ctx, L, 256), 256, 0, st>>>(claim_list.at(total), L, W, K, seed,
+        k_apply_list<<<grid_for(ctx, (L + kApplyPer - 1) / kApplyPer, 256), 256, 0, st>>>(
+            claim_list.at(total), L, W, K, seed,
                                                             block, recip,
                                                             fr[cur ^ 1], d_nnext, fcap, d_lover);
         ctx->launches++;
