@@ -230,8 +230,8 @@ __global__ void k_bin_count(const u64* __restrict__ keys, u64 k0, u64 per, u64 k
 
 __global__ void k_bin_scatter(const u64* __restrict__ keys, u64 k0, u64 per, u64 k1, u64 seed,
                               u64 block, u64 recip, u32 sbits, u32 S,
-                              const unsigned long long* __restrict__ bbase, u32* __restrict__ ent_off,
-                              u32* __restrict__ ent_idx) {
+                              const unsigned long long* __restrict__ bbase,
+                              unsigned long long* __restrict__ ent) {
   extern __shared__ unsigned long long cur[];
   for (u32 i = threadIdx.x; i < S; i += blockDim.x) cur[i] = bbase[(u64)blockIdx.x * S + i];
   __syncthreads();
@@ -244,8 +244,7 @@ __global__ void k_bin_scatter(const u64* __restrict__ keys, u64 k0, u64 per, u64
 #pragma unroll
     for (int t = 0; t < 3; ++t) {
       const unsigned long long pos = atomicAdd(&cur[(u32)(c[t] >> sbits)], 1ull);
-      ent_off[pos] = (u32)(c[t] & lmask);
-      ent_idx[pos] = (u32)(i - k0);
+      ent[pos] = ((u64)(i - k0) << 32) | (c[t] & lmask);   // one 8-byte store per update
     }
   }
 }
@@ -259,16 +258,19 @@ __global__ void k_bin_scatter(const u64* __restrict__ keys, u64 k0, u64 per, u64
 // where a cooperative launch is refused (the result is the same; only the L2
 // hit rate suffers).
 template <bool kSync>
-__global__ void k_bin_apply(const u32* __restrict__ ent_off, const u32* __restrict__ ent_idx, u64 k0,
+__global__ void k_bin_apply(const unsigned long long* __restrict__ ent, u64 k0,
                             const unsigned long long* __restrict__ soff, u32 sbits, u32 S,
                             unsigned long long* W) {
   const u64 nt = (u64)gridDim.x * blockDim.x, tid = blockIdx.x * (u64)blockDim.x + threadIdx.x;
   for (u32 sl = 0; sl < S; ++sl) {
     unsigned long long* base = W + ((u64)sl << sbits);
     const u64 e1 = soff[sl + 1];
-    for (u64 i = soff[sl] + tid; i < e1; i += nt)
-      if (S615_KEY_OK(k0 + ent_idx[i]) && S615_CELL_OK(((u64)sl << sbits) + ent_off[i]))
-        atomicAdd(base + ent_off[i], (unsigned long long)upd(k0 + ent_idx[i]));
+    for (u64 i = soff[sl] + tid; i < e1; i += nt) {
+      const u64 e = ent[i];
+      const u32 off = (u32)e, idx = (u32)(e >> 32);
+      if (S615_KEY_OK(k0 + idx) && S615_CELL_OK(((u64)sl << sbits) + off))
+        atomicAdd(base + off, (unsigned long long)upd(k0 + idx));
+    }
     if constexpr (kSync) cg::this_grid().sync();
   }
 }
@@ -591,7 +593,7 @@ u64 pow2_at_least(u64 x) { u64 p = 1; while (p < x) p <<= 1; return p; }
 // Incidence of keys [0, n) for one seed through the slice bins, in chunks of
 // keys whose updates fit the entry buffers (ent_cap updates).
 int incidence_binned(s615_ctx* ctx, const u64* keys, u64 n, u64 seed, u64 m, u64 block, u64 recip,
-                     u32* ent_off, u32* ent_idx, u64 ent_cap, unsigned long long* W, u32* bhist,
+                     unsigned long long* ent, u64 ent_cap, unsigned long long* W, u32* bhist,
                      unsigned long long* bbase, cudaStream_t st) {
   u32 sbits = 21;
   while (((m + (1ull << sbits) - 1) >> sbits) > kMaxSlices) ++sbits;
@@ -623,7 +625,7 @@ int incidence_binned(s615_ctx* ctx, const u64* keys, u64 n, u64 seed, u64 m, u64
     S615_CU(cudaMemcpyAsync(bbase, h_base.data(), h_base.size() * sizeof(unsigned long long),
                             cudaMemcpyHostToDevice, st));
     k_bin_scatter<<<G, kBinThreads, S * sizeof(unsigned long long), st>>>(
-        keys, k0, per, k1, seed, block, recip, sbits, S, bbase, ent_off, ent_idx);
+        keys, k0, per, k1, seed, block, recip, sbits, S, bbase, ent);
     ctx->launches++;
     S615_CU(cudaGetLastError());
     // the slice starts go where the block bases were (read by the apply kernel)
@@ -633,17 +635,16 @@ int incidence_binned(s615_ctx* ctx, const u64* keys, u64 n, u64 seed, u64 m, u64
     S615_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bin_apply<true>, 256, 0));
     const dim3 grid(ctx->num_sms * std::max(per_sm, 1));
     {   // cooperative: every block resident at once (the launch is refused otherwise)
-      const u32* a_off = ent_off;
-      const u32* a_idx = ent_idx;
+      const unsigned long long* a_ent = ent;
       const unsigned long long* a_soff = bbase;
       u64 a_k0 = k0;
       u32 a_sbits = sbits, a_S = S;
-      void* args[] = {(void*)&a_off, (void*)&a_idx, (void*)&a_k0, (void*)&a_soff, (void*)&a_sbits,
-                      (void*)&a_S, (void*)&W};
+      void* args[] = {(void*)&a_ent, (void*)&a_k0, (void*)&a_soff, (void*)&a_sbits, (void*)&a_S,
+                      (void*)&W};
       if (cudaLaunchCooperativeKernel((const void*)k_bin_apply<true>, grid, dim3(256), args, 0, st) !=
           cudaSuccess) {
         cudaGetLastError();
-        k_bin_apply<false><<<grid, 256, 0, st>>>(ent_off, ent_idx, k0, bbase, sbits, S, W);
+        k_bin_apply<false><<<grid, 256, 0, st>>>(ent, k0, bbase, sbits, S, W);
       }
     }
     ctx->launches++;
@@ -829,7 +830,7 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
     lists = false;
   }
   if (!lists && (s = rounds.alloc(m * sizeof(u16)))) return s;
-  Buf ent_off(ctx), ent_idx(ctx), bins(ctx);
+  Buf ent(ctx), bins(ctx);   // ent: one 8-byte word per update (index << 32 | slice offset)
   u64 ent_cap = 0;
   {
     const size_t avail = avail_now();
@@ -838,29 +839,30 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
       ent_cap = ent_cap / 3 * 3;
     }
     if (ent_cap >= std::min<u64>(3 * n, 3ull << 20)) {
-      if ((s = ent_off.alloc(ent_cap * 4)) || (s = ent_idx.alloc(ent_cap * 4)) ||
-          (s = bins.alloc(bin_bytes))) {
-        ent_off.release(); ent_idx.release(); bins.release();
+      if ((s = ent.alloc(ent_cap * 8)) || (s = bins.alloc(bin_bytes))) {
+        ent.release(); bins.release();
         ent_cap = 0;
       }
     } else {
       ent_cap = 0;
     }
   }
-  // The claim list: in the entry buffers (idle after the incidence) with each
-  // key's index and hash when they hold 2n entries, else cells only.
-  // ent_off holds offsets, indices and thirds (9n bytes), ent_idx the hashes (8n)
+  // The claim list: in the entry buffer (idle after the incidence) with each
+  // key's index and hash when it has room, else cells only.  Its layout:
+  // offsets (4n bytes), indices (4n), thirds (n), then the hashes (8n) from
+  // the next 8-byte boundary.
   ClaimList claim_list{{nullptr, nullptr}, nullptr, nullptr};
-  if (lists && rich_possible && ent_cap * 4 >= 9 * n && !order.p) {
-    u32* o = static_cast<u32*>(ent_off.p);
+  const u64 hash_at = (9 * n + 7) / 8 * 8;
+  if (lists && rich_possible && ent_cap * 8 >= hash_at + 8 * n && !order.p) {
+    u32* o = static_cast<u32*>(ent.p);
     claim_list = ClaimList{{o, reinterpret_cast<u8*>(o + 2 * n)}, o + n,
-                           static_cast<unsigned long long*>(ent_idx.p)};
+                           reinterpret_cast<unsigned long long*>(static_cast<char*>(ent.p) + hash_at)};
   } else if (lists && (order.p || !order.alloc(n * 5))) {
     u32* o = static_cast<u32*>(order.p);
     claim_list.cells = CellList{o, reinterpret_cast<u8*>(o + n)};
   } else if (lists) {   // no room for any list: scan, with round tags in the entry buffers' place
     order.release(); front.release();
-    ent_off.release(); ent_idx.release(); bins.release();
+    ent.release(); bins.release();
     ent_cap = 0;
     lists = false;
     if ((s = rounds.alloc(m * sizeof(u16)))) return s;
@@ -878,8 +880,9 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
       u32* bhist = static_cast<u32*>(bins.p);
       auto* bbase = reinterpret_cast<unsigned long long*>(static_cast<char*>(bins.p) +
                                                           (G * kMaxSlices * 4 + 7) / 8 * 8);
-      if ((s = incidence_binned(ctx, K, n, seed, m, block, recip, static_cast<u32*>(ent_off.p),
-                                static_cast<u32*>(ent_idx.p), ent_cap, W, bhist, bbase, st)))
+      if ((s = incidence_binned(ctx, K, n, seed, m, block, recip,
+                                static_cast<unsigned long long*>(ent.p), ent_cap, W, bhist, bbase,
+                                st)))
         return s;
     } else {
       k_incidence<<<grid_for(ctx, n, 256), 256, 0, st>>>(K, n, seed, block, recip, W);
@@ -1000,7 +1003,7 @@ int build_xor_device(s615_ctx* ctx, const u64* d_pair_vals, u64 n_vals, const u6
   trace.mark("sync");
   keys.release(); rounds.release(); order.release(); front.release();
   trace.mark("free_keys");
-  ent_off.release(); ent_idx.release(); bins.release();
+  ent.release(); bins.release();
   trace.mark("free_bins");
 
   out->hdr.n_keys = n;
